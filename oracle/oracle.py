@@ -1,0 +1,531 @@
+"""The oracle: a CPU restatement of hdfe-stream's fixed-effects solve path.
+
+TEST INFRASTRUCTURE ONLY.  tests/, `__graft_entry__.smoke()` and bench.py's
+CPU-baseline leg use this as the checker and as the timed CPU baseline; the
+product (hdfe_stream_b200/) never imports it.
+
+The numba kernels of the reference are restated in C (hdfe_oracle.c, built by
+the Makefile beside it, bit-identical to the numba kernels); the numpy glue
+around them here restates the reference's own Python driver code, each
+function citing the reference file:line it follows.  Parity against the
+reference itself is pinned by tests/test_oracle.py on the golden vectors of
+tests/golden/, which tests/golden/make_golden.py produced by running the
+reference's kernels and mixins on the same panels.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libhdfe_oracle.so"
+
+# core/solve.py:44 and :49; core/passes.py:48
+RHS_ZERO_TOL = 1e-11
+CG_BLOCKS = 256
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile the oracle's C kernels (make), if not built already."""
+    src = HERE / "hdfe_oracle.c"
+    if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        for name in ("orc_peel", "orc_dense_labels", "orc_bfs_components"):
+            getattr(_lib, name).restype = ctypes.c_int64
+    return _lib
+
+
+def _p(a):
+    """ctypes pointer of a numpy array (None for None)."""
+    if a is None:
+        return None
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _i(x):
+    return ctypes.c_int64(int(x))
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(ctypes.c_int(int(n)))
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+# ---------------------------------------------------------------- pass 1
+
+@dataclass
+class Cells:
+    """Pass 1's output (core/passes.py:397-531, the plain case):
+    identifying cells and the level bookkeeping built with them."""
+
+    starts: np.ndarray          # (G'+1,) int64, groups with more than one cell
+    codes: np.ndarray           # (M, D) uint32
+    n: np.ndarray               # (M,) float64 cell weight
+    sums: np.ndarray            # (M, m) float64 centred sums
+    obs: np.ndarray             # (L,) weight per level, all cells
+    cnt: np.ndarray             # (L,) rows per level, all cells
+    diag: np.ndarray            # (L,) diagonal of S
+    rhs: np.ndarray             # (L, m) D_o' M_0 V
+    offs: np.ndarray            # (D,) int64
+    n_levels: list
+    n_cells: int
+    fe0_rank: int
+    means: np.ndarray
+    raw_ss: np.ndarray
+    pair_components: dict = field(default_factory=dict)
+
+    @property
+    def L(self) -> int:
+        return int(sum(self.n_levels))
+
+
+def cell_runs(rows):
+    """Cells of sorted rows (core/passes.py:533-589 `_cell_chunks`): runs of
+    equal (gcode, codes); cnt, n and the sums of the centred variables
+    (`_nb_run_sums`, core/kernels_base.py:375-422)."""
+    g = rows.gcode
+    n_rows = len(g)
+    same = g[1:] == g[:-1]
+    for d in range(rows.codes.shape[1]):
+        c = rows.codes[:, d]
+        same &= c[1:] == c[:-1]
+    cs = np.flatnonzero(np.concatenate(([True], ~same)))
+    bounds = np.append(cs, n_rows).astype(np.int64)
+    run = np.diff(bounds)
+    means = rows.V.mean(axis=0) if n_rows else np.zeros(rows.V.shape[1])
+    w = rows.w
+    weighted = w is not None
+    out = {"g": g[cs], "codes": rows.codes[cs], "cnt": run.astype(np.float64)}
+    out["n"] = np.add.reduceat(w, cs) if weighted else out["cnt"]
+    m = rows.V.shape[1]
+    ZT = np.empty((m, n_rows))
+    for j in range(m):
+        np.subtract(rows.V[:, j], means[j], out=ZT[j])
+    ST = np.empty((m, len(cs)))
+    lib().orc_run_sums(_p(bounds), _i(len(cs)), _p(ZT), _i(m), _i(n_rows),
+                       _p(np.ascontiguousarray(w) if weighted else None), _p(ST))
+    out["S"] = np.ascontiguousarray(ST.T)
+    return out, means
+
+
+def segments(g):
+    """core/utils.py:62-69 `_segments`: segment starts and local index."""
+    brk = np.flatnonzero(g[1:] != g[:-1]) + 1
+    starts = np.concatenate(([0], brk))
+    local = np.zeros(len(g), dtype=np.int64)
+    local[brk] = 1
+    np.cumsum(local, out=local)
+    return starts, local
+
+
+def pass1(rows) -> Cells:
+    """`_pass1_cells` (core/passes.py:397-531) over one chunk holding every
+    row: cells, obs/cnt per level, identifying cells (groups of more than one
+    cell), the Jacobi diagonal and the right-hand side D_o' M_0 V, and the
+    pair union-find for the degrees of freedom."""
+    ch, means = cell_runs(rows)
+    nl = list(rows.n_levels)
+    D = len(nl)
+    offs = np.concatenate(([0], np.cumsum(nl)[:-1])).astype(np.int64)
+    L = int(sum(nl))
+    m = rows.V.shape[1]
+    obs = np.zeros(L)
+    cnt = np.zeros(L)
+    diag = np.zeros(L)
+    rhs = np.zeros((L, m))
+    for d in range(D):
+        sl = slice(offs[d], offs[d] + nl[d])
+        obs[sl] += np.bincount(ch["codes"][:, d], weights=ch["n"], minlength=nl[d])
+        cnt[sl] += np.bincount(ch["codes"][:, d], weights=ch["cnt"], minlength=nl[d])
+    uf = {(i, j): np.arange(nl[i] + nl[j], dtype=np.int64)
+          for i in range(D) for j in range(i + 1, D)}
+    for (i, j), parent in uf.items():
+        a = np.ascontiguousarray(ch["codes"][:, i])
+        b = np.ascontiguousarray(ch["codes"][:, j])
+        lib().orc_union_pairs(_p(parent), _p(a), _p(b), _i(len(a)), _i(nl[i]))
+    starts, local = segments(ch["g"])
+    ncells = np.diff(np.append(starts, len(local)))
+    keep = ncells[local] > 1
+    fe0_rank = len(starts)
+    kept = ncells[ncells > 1]
+    kstarts = np.concatenate(([0], np.cumsum(kept))).astype(np.int64)
+    kcodes = np.ascontiguousarray(ch["codes"][keep]).astype(np.uint32)
+    kn = np.ascontiguousarray(ch["n"][keep]).astype(np.float64)
+    ksums = np.ascontiguousarray(ch["S"][keep])
+    G = len(kstarts) - 1
+    lib().orc_diag(_p(kstarts), _i(G), _p(kcodes), _i(D), _p(kn), _p(offs), _p(diag))
+    lib().orc_rhs(_p(kstarts), _i(G), _p(kcodes), _i(D), _p(kn), _p(ksums), _i(m),
+                  _p(offs), _p(rhs))
+    n_obs = rows.n_rows
+    raw_ss = (rows.V.var(axis=0, ddof=1) * max(n_obs - 1, 1)) if n_obs > 1 else np.zeros(m)
+    pair = {(i, j): int(np.count_nonzero(p == np.arange(len(p)))) for (i, j), p in uf.items()}
+    return Cells(starts=kstarts, codes=kcodes, n=kn, sums=ksums, obs=obs, cnt=cnt,
+                 diag=diag, rhs=rhs, offs=offs, n_levels=nl, n_cells=len(ch["g"]),
+                 fe0_rank=fe0_rank, means=means, raw_ss=raw_ss, pair_components=pair)
+
+
+# ------------------------------------------------------------ components
+
+def components(cells: Cells, col: int = 0):
+    """Union-find over dimension `col` (`_nb_components`,
+    core/kernels_base.py:156-174): the root of each level's component."""
+    nl = cells.n_levels[col]
+    parent = np.empty(nl, np.int64)
+    G = len(cells.starts) - 1
+    lib().orc_components(_p(cells.starts), _i(G), _p(cells.codes), _i(cells.codes.shape[1]),
+                         _i(col), _i(nl), _p(parent))
+    return parent
+
+
+def rank_components(root: np.ndarray, cnt_first: np.ndarray):
+    """core/passes.py:933-950 `_rank_components`: labels 0, 1, ... by rows,
+    ties to the component with the smallest level (a stable sort)."""
+    nl = len(root)
+    is_root = root == np.arange(nl)
+    dense = (np.cumsum(is_root) - 1)[root]
+    rows = np.bincount(dense, weights=cnt_first, minlength=int(is_root.sum()))
+    order = np.argsort(-rows, kind="stable")
+    rank = np.empty(len(order), np.int64)
+    rank[order] = np.arange(len(order))
+    return rank[dense], len(order)
+
+
+def component_labels(cells: Cells):
+    """(comp, n_components) for the first non-streamed dimension, as
+    `_components` (core/passes.py:952-979) computes them."""
+    root = components(cells, 0)
+    return rank_components(root, cells.cnt[cells.offs[0]:cells.offs[0] + cells.n_levels[0]])
+
+
+# ------------------------------------------------------------- explicit S
+
+def build_explicit(cells: Cells, n_threads: int | None = None):
+    """`_build_explicit` (core/solve.py:148-194) for the plain case:
+    S = D_o' M_0 D_o in CSR with sorted columns (indptr int64, indices
+    int32, data float64)."""
+    D = cells.codes.shape[1]
+    L = cells.L
+    G = len(cells.starts) - 1
+    lptr = np.empty(L + 1, np.int64)
+    lib().orc_level_groups(_p(cells.starts), _i(G), _p(cells.codes), _i(D), _p(cells.offs),
+                           _i(L), _p(lptr), None)
+    lgrp = np.empty(int(lptr[L]), np.int32)
+    lib().orc_level_groups(_p(cells.starts), _i(G), _p(cells.codes), _i(D), _p(cells.offs),
+                           _i(L), _p(lptr), _p(lgrp))
+    work = np.empty(L, np.int64)
+    lib().orc_row_work(_p(cells.starts), _p(lptr), _p(lgrp), _i(L), _p(work))
+    wide = max(L // (4 * D), 1)
+    rnnz = np.empty(L, np.int64)
+    lib().orc_row_nnz(_p(cells.starts), _p(cells.codes), _i(D), _p(cells.offs), _p(lptr),
+                      _p(lgrp), _p(work), _i(wide), _i(L), _p(rnnz))
+    nnz = int(rnnz.sum())
+    indptr = np.zeros(L + 1, np.int64)
+    np.cumsum(rnnz, out=indptr[1:])
+    indices = np.empty(nnz, np.int32)
+    data = np.empty(nnz)
+    ng = np.add.reduceat(cells.n, cells.starts[:-1]) if G else np.zeros(0)
+    ng = np.ascontiguousarray(ng)
+    lib().orc_row_fill(_p(cells.starts), _p(cells.codes), _i(D), _p(cells.n), _p(ng),
+                       _p(cells.offs), _i(D), _p(lptr), _p(lgrp), _p(work), _i(wide), _i(L),
+                       _p(indptr), _p(indices), _p(data))
+    return indptr, indices, data
+
+
+def jacobi(diag: np.ndarray) -> np.ndarray:
+    """core/solve.py:142-146 `_jacobi`."""
+    pos = diag > 1e-12
+    return np.where(pos, 1.0 / np.where(pos, diag, 1.0), 0.0)
+
+
+# ---------------------------------------------------------------- PCG
+
+def csr_matmat(S, X):
+    indptr, indices, data = S
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.empty_like(X)
+    lib().orc_csr_matmat(_p(indptr), _p(indices), _p(data), _i(len(indptr) - 1), _p(X),
+                         _i(X.shape[1]), _p(out))
+    return out
+
+
+def pcg(S, dinv, b, zero=None, x0=None, tol=1e-10, maxiter=5000):
+    """`_SolveMixin._pcg` (core/solve.py:66-140) with the Jacobi
+    preconditioner: block PCG, one CG per column in lockstep, column sums over
+    256 fixed row blocks.  Returns (X, iterations, converged, max rel)."""
+    b = np.asarray(b, dtype=np.float64)
+    bnorm = np.linalg.norm(b, axis=0)
+    bnorm[bnorm == 0] = 1.0
+    if x0 is None:
+        X = np.zeros_like(b)
+        R = b.copy()
+    else:
+        X = np.array(x0, dtype=np.float64, order="C")
+        R = b - csr_matmat(S, X)
+    if zero is not None and zero.any():
+        X[:, zero] = 0.0
+        R[:, zero] = 0.0
+        if zero.all():
+            return X, 0, True, 0.0
+    active = np.ones(b.shape[1], bool) if zero is None else ~zero
+    rel = np.zeros(b.shape[1])
+    if x0 is not None:
+        rel = np.linalg.norm(R, axis=0) / bnorm
+        active &= rel > tol
+        if not active.any():
+            return X, 0, True, float(rel.max())
+    X, R = np.ascontiguousarray(X), np.ascontiguousarray(R)
+    L, k = X.shape
+    dinv = np.ascontiguousarray(dinv, dtype=np.float64)
+    nblk = max(1, min(CG_BLOCKS, L))
+    parts = np.empty((nblk, 2, k))
+    dots = np.empty((nblk, k))
+    P = np.ascontiguousarray(R * dinv[:, None])
+    lib().orc_cg_dot(_p(R), _p(P), _i(L), _i(k), _i(nblk), _p(dots))
+    rz = dots.sum(axis=0)
+    it = 0
+    for it in range(1, maxiter + 1):
+        AP = csr_matmat(S, P)
+        lib().orc_cg_dot(_p(P), _p(AP), _i(L), _i(k), _i(nblk), _p(dots))
+        pAp = dots.sum(axis=0)
+        alpha = np.where(active & (pAp > 0), rz / np.where(pAp > 0, pAp, 1), 0.0)
+        alpha = np.ascontiguousarray(alpha)
+        lib().orc_cg_step(_p(X), _p(R), _p(P), _p(AP), _p(alpha), _p(dinv), _i(L), _i(k),
+                          _i(nblk), _p(parts))
+        sums = parts.sum(axis=0)
+        rel = np.sqrt(sums[0]) / bnorm
+        active = rel > tol
+        if not active.any():
+            break
+        rz_new = sums[1]
+        beta = np.ascontiguousarray(np.where(active, rz_new / np.where(rz != 0, rz, 1), 0.0))
+        lib().orc_cg_direction(_p(P), _p(R), _p(dinv), _p(beta), _i(L), _i(k))
+        rz = rz_new
+    return X, it, bool(not active.any()), float(rel.max())
+
+
+def normalize(Gamma, cells: Cells, comp):
+    """core/solve.py:383-399 `_normalize`: first dimension's effects have
+    obs-weighted mean zero within each component, further dimensions global
+    obs-weighted mean zero."""
+    nl, o = cells.n_levels[0], cells.offs[0]
+    w = cells.obs[o:o + nl]
+    cw = np.bincount(comp, weights=w, minlength=nl)
+    cw[cw == 0] = 1.0
+    mean = scatter(comp, w[:, None] * Gamma[o:o + nl], nl) / cw[:, None]
+    Gamma[o:o + nl] -= mean[comp]
+    for d in range(1, len(cells.n_levels)):
+        nl, o = cells.n_levels[d], cells.offs[d]
+        w = cells.obs[o:o + nl]
+        Gamma[o:o + nl] -= (w @ Gamma[o:o + nl]) / max(w.sum(), 1.0)
+    return Gamma
+
+
+def scatter(idx, vals, n):
+    """core/utils.py `_scatter`: column-wise bincount of `vals` (rows) by `idx`."""
+    out = np.zeros((n, vals.shape[1]))
+    for j in range(vals.shape[1]):
+        out[:, j] = np.bincount(idx, weights=vals[:, j], minlength=n)
+    return out
+
+
+def solve(cells: Cells, S, tol=1e-10, maxiter=5000, rhs_block=8, comp=None, x0=None):
+    """`_SolveMixin._solve` (core/solve.py:294-368) for the estimator's own
+    variables, whose right-hand side pass 1 built: zero-column detection
+    against each variable's total sum of squares, block PCG per rhs_block
+    columns, then `_normalize`.  Returns (Gamma, info)."""
+    L = cells.L
+    m = cells.rhs.shape[1]
+    if comp is None:
+        comp, _ = component_labels(cells)
+    dinv = jacobi(cells.diag)
+    gamma = np.empty((L, m))
+    its, conv, rel = [], True, 0.0
+    for j0 in range(0, m, rhs_block):
+        j1 = min(m, j0 + rhs_block)
+        b = cells.rhs[:, j0:j1]
+        scale = np.sqrt(np.maximum(cells.raw_ss[j0:j1], 0.0))
+        zero = np.linalg.norm(b, axis=0) <= RHS_ZERO_TOL * scale
+        X, it, c, r = pcg(S, dinv, b, zero, None if x0 is None else x0[:, j0:j1], tol, maxiter)
+        gamma[:, j0:j1] = normalize(X, cells, comp)
+        its.append(it)
+        conv &= c
+        rel = max(rel, r)
+    return gamma, {"iterations": its if len(its) > 1 else its[0], "converged": conv,
+                   "max_rel_residual": rel}
+
+
+# ---------------------------------------------------- random draws, rows
+
+def rademacher(ordinal, n_rows, draws, seed, first_draw=0):
+    """core/kernels_groups.py:53-76 `_nb_rademacher`."""
+    out = np.empty((n_rows, draws))
+    lib().orc_rademacher(_i(ordinal), _i(n_rows), _i(draws), ctypes.c_uint64(seed & (2**64 - 1)),
+                         _i(first_draw), _p(out))
+    return out
+
+
+def row_starts(gcode):
+    """Group boundaries of sorted rows (inverse.py:139-142 `_chunk_layout`)."""
+    n = len(gcode)
+    return np.concatenate(([0], np.flatnonzero(gcode[1:] != gcode[:-1]) + 1, [n])).astype(np.int64)
+
+
+def center_rows(starts, codes, offs, w, X, R, L, nt=1):
+    """kernels_inverse.py:35-71 `_nb_center_rows` with `nt` accumulator
+    copies; returns (acc.sum(0), acc_x.sum(0))."""
+    codes = np.ascontiguousarray(codes, dtype=np.int64)
+    G = len(starts) - 1
+    m = R.shape[1]
+    k = X.shape[1]
+    acc = np.zeros((nt, L, m))
+    acc_x = np.zeros((nt, k, m))
+    lib().orc_center_rows(_p(starts), _i(G), _p(codes), _i(codes.shape[1]), _p(offs),
+                          _p(np.ascontiguousarray(w, dtype=np.float64)),
+                          _p(np.ascontiguousarray(X, dtype=np.float64)), _i(k),
+                          _p(np.ascontiguousarray(R, dtype=np.float64)), _i(m), _i(nt), _i(L),
+                          _p(acc), _p(acc_x))
+    return acc.sum(axis=0), acc_x.sum(axis=0)
+
+
+def project_rows_kernel(starts, codes, offs, w, X, C, R, U):
+    """kernels_inverse.py:75-107 `_nb_project_rows`."""
+    codes = np.ascontiguousarray(codes, dtype=np.int64)
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    out = np.empty_like(R)
+    lib().orc_project_rows(_p(starts), _i(len(starts) - 1), _p(codes), _i(codes.shape[1]),
+                           _p(offs), _p(np.ascontiguousarray(w, dtype=np.float64)),
+                           _p(np.ascontiguousarray(X, dtype=np.float64)), _i(X.shape[1]),
+                           _p(np.ascontiguousarray(C, dtype=np.float64)), _p(R), _i(R.shape[1]),
+                           _p(np.ascontiguousarray(U, dtype=np.float64)), _p(out))
+    return out
+
+
+def reduce_rows(starts, codes, offs, w, X, R, L, nt=1):
+    """kernels_inverse.py:112-130 `_nb_reduce_rows`."""
+    codes = np.ascontiguousarray(codes, dtype=np.int64)
+    G = len(starts) - 1
+    m = R.shape[1]
+    k = X.shape[1]
+    acc = np.zeros((nt, L, m))
+    acc_x = np.zeros((nt, k, m))
+    lib().orc_reduce_rows(_p(starts), _i(G), _p(codes), _i(codes.shape[1]), _p(offs),
+                          _p(np.ascontiguousarray(w, dtype=np.float64)),
+                          _p(np.ascontiguousarray(X, dtype=np.float64)), _i(k),
+                          _p(np.ascontiguousarray(R, dtype=np.float64)), _i(m), _i(nt), _i(L),
+                          _p(acc), _p(acc_x))
+    return acc.sum(axis=0), acc_x.sum(axis=0)
+
+
+def spread_groups(starts, w, group_values):
+    """kernels_inverse.py:134-152 `_nb_spread_groups`."""
+    gv = np.ascontiguousarray(group_values, dtype=np.float64)
+    out = np.empty((int(starts[-1]), gv.shape[1]))
+    lib().orc_spread_groups(_p(starts), _i(len(starts) - 1),
+                            _p(np.ascontiguousarray(w, dtype=np.float64)), _p(gv),
+                            _i(gv.shape[1]), _p(out))
+    return out
+
+
+def project_coef(starts, codes, offs, w, X, C, RHO, U):
+    """kernels_inverse.py:157-188 `_nb_project_coef`: (rows, groups)."""
+    codes = np.ascontiguousarray(codes, dtype=np.int64)
+    RHO = np.ascontiguousarray(RHO, dtype=np.float64)
+    G = len(starts) - 1
+    rows = np.empty_like(RHO)
+    groups = np.empty((G, RHO.shape[1]))
+    lib().orc_project_coef(_p(starts), _i(G), _p(codes), _i(codes.shape[1]), _p(offs),
+                           _p(np.ascontiguousarray(w, dtype=np.float64)),
+                           _p(np.ascontiguousarray(X, dtype=np.float64)), _i(X.shape[1]),
+                           _p(np.ascontiguousarray(C, dtype=np.float64)), _p(RHO),
+                           _i(RHO.shape[1]), _p(np.ascontiguousarray(U, dtype=np.float64)),
+                           _p(rows), _p(groups))
+    return rows, groups
+
+
+def group_sums(starts, w, R):
+    """core/kernels_groups.py:17-27 `_nb_group_sums`."""
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    out = np.empty((len(starts) - 1, R.shape[1]))
+    lib().orc_group_sums(_p(starts), _i(len(starts) - 1),
+                         _p(np.ascontiguousarray(w, dtype=np.float64)), _p(R), _i(R.shape[1]),
+                         _p(out))
+    return out
+
+
+def trace_moments(starts, codes, psi_column, psi_offset, w, Zl, Zg, Ul, Ug, nt=1):
+    """kernels_inverse.py:192-231 `_nb_trace_moments`: acc (nt, m, 8)."""
+    codes = np.ascontiguousarray(codes, dtype=np.int64)
+    m = Zg.shape[1]
+    acc = np.zeros((nt, m, 8))
+    lib().orc_trace_moments(_p(starts), _i(len(starts) - 1), _p(codes), _i(codes.shape[1]),
+                            _i(psi_column), _i(psi_offset),
+                            _p(np.ascontiguousarray(w, dtype=np.float64)),
+                            *[_p(np.ascontiguousarray(a, dtype=np.float64))
+                              for a in (Zl, Zg, Ul, Ug)], _i(m), _i(nt), _p(acc))
+    return acc
+
+
+# -------------------------------------------------- bipartite network
+
+def distinct_pairs(a, b, n1):
+    """core/connected.py:656-687 `_DistinctPairs` in one batch: sorted
+    distinct keys a * n1 + b and the rows behind each."""
+    key = a.astype(np.uint64) * np.uint64(max(n1, 1)) + b.astype(np.uint64)
+    k, c = np.unique(key, return_counts=True)
+    return k, c.astype(np.uint32)
+
+
+def peel(keys, n1, k0, k1, alive0, alive1):
+    """core/kernels_graph.py:188-221 `_nb_peel` (in place); returns rounds."""
+    return int(lib().orc_peel(_p(keys), _i(len(keys)), ctypes.c_uint64(max(n1, 1)), _i(k0),
+                              _i(k1), _p(alive0), _i(len(alive0)), _p(alive1),
+                              _i(len(alive1))))
+
+
+def largest_connected(a, b, n0, n1, min_degree=(1, 1)):
+    """`_find_components` (core/connected.py:378-493) on coded pairs, for
+    `connected="largest"` with pruning: returns (alive levels of each
+    dimension in the largest component, labels (n0+n1), sizes by rows)."""
+    lib_ = lib()
+    alive = np.ones(n0 + n1, np.uint8)
+    keys, counts = distinct_pairs(a, b, n1)
+    n1u = max(n1, 1)
+    if tuple(min_degree) != (1, 1):
+        a0 = np.ascontiguousarray(alive[:n0])
+        a1 = np.ascontiguousarray(alive[n0:])
+        peel(keys, n1, min_degree[0], min_degree[1], a0, a1)
+        alive[:n0], alive[n0:] = a0, a1
+    parent = np.arange(n0 + n1, dtype=np.int64)
+    a0 = np.ascontiguousarray(alive[:n0])
+    a1 = np.ascontiguousarray(alive[n0:])
+    lib_.orc_union_keys(_p(parent), _p(keys), _i(len(keys)), ctypes.c_uint64(n1u), _p(a0),
+                        _i(n0), _p(a1))
+    nc = int(lib_.orc_dense_labels(_p(parent), _i(n0 + n1), _p(alive)))
+    rows = np.zeros(nc, np.int64)
+    lib_.orc_pair_rows(_p(keys), _p(counts), _i(len(keys)), ctypes.c_uint64(n1u), _p(parent),
+                       _i(n0 + n1), _p(rows))
+    order = np.argsort(-rows, kind="stable")
+    rank = np.empty(nc, np.int64)
+    rank[order] = np.arange(nc)
+    labels = np.where(parent >= 0, rank[np.maximum(parent, 0)], -1)
+    return labels == 0, labels, rows[order]
+

@@ -1,0 +1,119 @@
+"""The oracle against the reference's own outputs (tests/golden/, made by
+tests/golden/make_golden.py from the reference's numba kernels and mixins).
+
+Integer outputs (cell layout, counts, codes, CSR pattern, component labels)
+must be identical; floating-point outputs are compared to 1e-12 relative,
+and most are bit-identical since the oracle keeps the reference's order of
+operations."""
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from conftest import golden_rows
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)) if a.size else 0.0
+
+
+@pytest.fixture
+def cells(golden):
+    name, g = golden
+    return name, g, orc.pass1(golden_rows(g))
+
+
+def test_pass1_cells_match_reference(cells):
+    name, g, c = cells
+    assert np.array_equal(c.starts, g["starts"])
+    assert np.array_equal(c.codes, g["codes"])
+    assert c.n_cells == int(g["n_cells"])
+    assert c.fe0_rank == int(g["fe0_rank"])
+    assert np.array_equal(c.cnt, g["cnt"])
+    np.testing.assert_array_equal(c.n, g["n"])
+    assert rel(c.obs, g["obs"]) < 1e-13
+    assert rel(c.sums, g["sums"]) < 1e-12
+    assert rel(c.diag, g["diag"]) < 1e-12
+    assert rel(c.rhs, g["rhs"]) < 1e-12
+
+
+def test_pair_components_match_reference(cells):
+    name, g, c = cells
+    # the reference's keys, sorted: (firm, year), (worker, firm), (worker, year)
+    _, nc = orc.component_labels(c)
+    year_roots = orc.components(c, 1)
+    got = [c.pair_components[(0, 1)], nc,
+           int(np.count_nonzero(year_roots == np.arange(len(year_roots))))]
+    assert got == [int(x) for x in g["pair_components"]]
+
+
+def test_component_labels_match_reference(cells):
+    name, g, c = cells
+    comp, nc = orc.component_labels(c)
+    assert nc == int(g["n_components"])
+    assert np.array_equal(comp, g["comp"])
+
+
+def test_explicit_s_matches_reference(cells):
+    name, g, c = cells
+    indptr, indices, data = orc.build_explicit(c)
+    assert np.array_equal(indptr, g["S_indptr"])
+    assert np.array_equal(indices, g["S_indices"])
+    np.testing.assert_array_equal(data, g["S_data"])
+
+
+def test_pcg_matches_reference(golden):
+    name, g = golden
+    S = (g["S_indptr"], g["S_indices"], g["S_data"])
+    dinv = orc.jacobi(g["diag"])
+    X, it, ok, r = orc.pcg(S, dinv, g["pcg_b"], g["pcg_zero"], None, float(g["tol"]))
+    assert it == int(g["pcg_it"]) and ok == bool(g["pcg_ok"])
+    np.testing.assert_array_equal(X, g["pcg_X"])
+    X2, it2, ok2, r2 = orc.pcg(S, dinv, g["pcg_b"], g["pcg_zero"], g["pcg_x0"], float(g["tol"]))
+    assert it2 == int(g["pcg_it2"])
+    np.testing.assert_array_equal(X2, g["pcg_X2"])
+
+
+def test_step2_solve_matches_reference(cells):
+    name, g, c = cells
+    S = orc.build_explicit(c)
+    gamma, info = orc.solve(c, S, tol=float(g["tol"]))
+    assert list(np.atleast_1d(info["iterations"])) == list(g["gamma_iterations"])
+    assert rel(gamma, g["gamma"]) < 1e-12
+
+
+def test_rademacher_matches_reference(golden):
+    name, g = golden
+    np.testing.assert_array_equal(orc.rademacher(1000, 257, 5, 12345, 7), g["rademacher"])
+
+
+def _project(g, c, seed, n_vec, weighted):
+    """project_rows (inverse.py:240-309) restated on the oracle's kernels."""
+    rows = golden_rows(g)
+    nt = int(g["numba_threads"])
+    starts = orc.row_starts(rows.gcode)
+    w = rows.w if weighted else np.ones(rows.n_rows)
+    R = orc.rademacher(0, rows.n_rows, n_vec, seed, 0)
+    if weighted:
+        # inverse.py:280-281, 298-303: W^(1/2) A S^- A' W^(1/2) = rows scaled
+        # by w^(-1/2) on the way in, by w^(1/2) on the way out
+        root = np.sqrt(w)
+        R = R * (1.0 / root)[:, None]
+    rhs, _ = orc.center_rows(starts, rows.codes, c.offs, w, np.zeros((rows.n_rows, 0)), R,
+                             c.L, nt)
+    S = orc.build_explicit(c)
+    zero = np.linalg.norm(rhs, axis=0) <= orc.RHS_ZERO_TOL * np.sqrt(w @ (R * R))
+    U, *_ = orc.pcg(S, orc.jacobi(c.diag), rhs, zero, None, float(g["tol"]))
+    R2 = orc.rademacher(0, rows.n_rows, n_vec, seed, 0)
+    if weighted:
+        R2 = R2 * (1.0 / root)[:, None]
+    out = orc.project_rows_kernel(starts, rows.codes, c.offs, w, np.zeros((rows.n_rows, 0)),
+                                  np.zeros((0, n_vec)), R2, U)
+    return out * root[:, None] if weighted else out
+
+
+def test_project_rows_matches_reference(cells):
+    name, g, c = cells
+    out = _project(g, c, 11, 6, len(g["w"]) > 0)
+    assert rel(out, g["project_rows_seed11"]) < 1e-10
