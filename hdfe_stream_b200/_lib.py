@@ -1,0 +1,83 @@
+"""ctypes binding of libhdfe_b200.so (the C ABI declared in include/hdfe_b200.h).
+
+There is no fallback: if the library is missing this raises, and every
+device entry point of the package goes through it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libhdfe_b200.so"
+
+HDFE_OK = 0
+HDFE_ERR_ARG = 1
+HDFE_ERR_CUDA = 2
+HDFE_ERR_SPIN_LIMIT = 3
+HDFE_ERR_WORKSPACE = 4
+HDFE_ERR_BAD_CODE = 5
+HDFE_ERR_CAPACITY = 6
+PCG_MAX_K = 8
+
+_c = ctypes
+_vp = _c.c_void_p
+_i64 = _c.c_int64
+_i32 = _c.c_int32
+_f64 = _c.c_double
+
+# name -> (restype, argtypes); mirrors include/hdfe_b200.h
+SIGNATURES = {
+    "hdfe_error_string": (_c.c_char_p, []),
+    "hdfe_version": (_c.c_char_p, []),
+    "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
+    "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
+                                  _i64, _vp, _vp, _i64, _vp, _vp]),
+}
+
+
+class PcgInfo(ctypes.Structure):
+    """struct hdfe_pcg_info."""
+    _fields_ = [("iterations", _i64), ("converged", _i32), ("status", _i32),
+                ("max_rel", _f64)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises ImportError when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH.name} is not built; run "
+                              "`python -m hdfe_stream_b200.build` (needs nvcc)")
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+class HDFEError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"hdfe_b200 error {code}: {msg}")
+        self.code = code
+
+
+def check(status: int) -> None:
+    if status != HDFE_OK:
+        raise HDFEError(status, lib().hdfe_error_string().decode())
+
+
+def ptr(t) -> int | None:
+    """Device pointer of a torch tensor (None for None)."""
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(stream=None) -> int:
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return s.cuda_stream

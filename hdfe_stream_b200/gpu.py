@@ -1,0 +1,171 @@
+"""The drop-in for hdfe-stream's device solve seam.
+
+hdfe-stream's step 2 reaches the GPU through one function,
+`core/gpu.py:186-197 explicit_solver(S, dinv, tol, maxiter, debug) ->
+(solve, device_name)`, called from core/solve.py:221-229 when
+`device == "cuda"` and `solver == "explicit"`; `solve(b, zero, x0)` returns
+`(X, iterations, converged, max_rel)` with host arrays in and out.  This
+module provides the same two functions, and `cuda_backend()` (the seam the
+reference's tests monkeypatch, core/gpu.py:33-51), backed by the persistent
+CUDA block-PCG of libhdfe_b200 instead of CuPy:
+
+* S and the preconditioner go to the device once per solver, as there;
+* each call is one launch for up to 8 right-hand-side columns (wider blocks
+  run as independent launches of 8: each column's CG is independent, so the
+  result is the same as one lockstep solve), with no host round trip per
+  iteration;
+* errors follow the reference: ImportError naming what to build when the
+  library is missing, RuntimeError when there is no device; non-convergence
+  is reported in the return value (the caller warns), not raised.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import _lib
+
+_HINT = ("device='cuda' needs libhdfe_b200.so built for sm_100a "
+         "(`python -m hdfe_stream_b200.build`) and an NVIDIA B200 GPU")
+
+
+def cuda_backend():
+    """The device the solver runs on, as core/gpu.py:33-51 returns it: a
+    namespace with the device `name` (and the torch device)."""
+    try:
+        import torch
+    except ImportError as err:              # pragma: no cover - torch is a dependency
+        raise ImportError(_HINT) from err
+    try:
+        _lib.lib()
+    except ImportError as err:
+        raise ImportError(f"{_HINT}: {err}") from err
+    if not torch.cuda.is_available() or torch.cuda.device_count() < 1:
+        raise RuntimeError("device='cuda': no CUDA device found")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    return SimpleNamespace(name=torch.cuda.get_device_name(dev), device=dev)
+
+
+class DeviceCSR:
+    """S on the device: indptr int64 (L+1), indices int32 (nnz), data f64."""
+
+    def __init__(self, indptr, indices, data, L: int, nnz: int):
+        self.indptr, self.indices, self.data = indptr, indices, data
+        self.L, self.nnz = int(L), int(nnz)
+
+    @classmethod
+    def from_host(cls, indptr, indices, data, device=None):
+        import torch
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        ip = torch.as_tensor(np.ascontiguousarray(indptr, dtype=np.int64)).to(dev)
+        ix = torch.as_tensor(np.ascontiguousarray(indices, dtype=np.int32)).to(dev)
+        dt = torch.as_tensor(np.ascontiguousarray(data, dtype=np.float64)).to(dev)
+        return cls(ip, ix, dt, len(indptr) - 1, len(data))
+
+    @classmethod
+    def from_scipy(cls, S, device=None):
+        return cls.from_host(S.indptr, S.indices, S.data, device)
+
+    @property
+    def nbytes(self) -> int:
+        return self.nnz * 12 + (self.L + 1) * 8
+
+
+class BlockSolver:
+    """`solve(b, zero, x0) -> (X, iterations, converged, rel)` on the device.
+
+    `solve_device` takes and returns device tensors (what the device-resident
+    fit and the leave-out passes use); calling the object takes host arrays,
+    exactly as the reference's `solve` (core/gpu.py:194-196)."""
+
+    def __init__(self, S: DeviceCSR, dinv, tol: float, maxiter: int, debug=None):
+        import torch
+        self.S = S
+        self.dev = S.indptr.device
+        self.dinv = torch.as_tensor(np.asarray(dinv, dtype=np.float64)).to(self.dev) \
+            if not torch.is_tensor(dinv) else dinv.to(self.dev, torch.float64).contiguous()
+        self.tol, self.maxiter, self.debug = float(tol), int(maxiter), debug
+        self._ws = {}
+        self._info = torch.zeros(3, dtype=torch.float64, device=self.dev)   # 24 bytes
+        self._zero = torch.zeros(_lib.PCG_MAX_K, dtype=torch.uint8, device=self.dev)
+
+    def _workspace(self, k):
+        import torch
+        if k not in self._ws:
+            nbytes = _lib.lib().hdfe_pcg_workspace_bytes(self.S.L, self.S.nnz, k)
+            if nbytes < 0:
+                raise _lib.HDFEError(_lib.HDFE_ERR_CUDA, "could not size the PCG workspace")
+            self._ws[k] = torch.empty(int(nbytes), dtype=torch.uint8, device=self.dev)
+        return self._ws[k]
+
+    def launch(self, B, zero, X0, X, stream=None):
+        """Enqueue one solve of at most 8 columns on `stream` (no sync)."""
+        k = B.shape[1]
+        ws = self._workspace(k)
+        zp = None
+        if zero is not None:
+            import torch
+            self._zero[:k].copy_(torch.from_numpy(np.asarray(zero, bool).astype(np.uint8)))
+            zp = self._zero.data_ptr()
+        _lib.check(_lib.lib().hdfe_pcg_solve(
+            self.S.indptr.data_ptr(), self.S.indices.data_ptr(), self.S.data.data_ptr(),
+            self.S.L, self.S.nnz, self.dinv.data_ptr(), B.data_ptr(), k, zp,
+            None if X0 is None else X0.data_ptr(), self.tol, self.maxiter, X.data_ptr(),
+            ws.data_ptr(), ws.numel(), self._info.data_ptr(), _lib.stream_handle(stream)))
+
+    def read_info(self):
+        raw = self._info.cpu().numpy().tobytes()
+        info = _lib.PcgInfo.from_buffer_copy(raw)
+        if info.status != _lib.HDFE_OK:
+            why = {_lib.HDFE_ERR_SPIN_LIMIT: "a grid-wide wait timed out",
+                   _lib.HDFE_ERR_BAD_CODE: "a column index of S is out of range"}
+            raise _lib.HDFEError(info.status, "the PCG kernel stopped early: "
+                                 + why.get(info.status, "device error"))
+        return int(info.iterations), bool(info.converged), float(info.max_rel)
+
+    def solve_device(self, B, zero=None, X0=None):
+        import torch
+        B = B.to(self.dev, torch.float64).contiguous()
+        L, k = B.shape
+        X = torch.empty_like(B)
+        its, conv, rel = 0, True, 0.0
+        zero = None if zero is None else np.asarray(zero, bool)
+        for j0 in range(0, k, _lib.PCG_MAX_K):
+            j1 = min(k, j0 + _lib.PCG_MAX_K)
+            Bj = B[:, j0:j1].contiguous()
+            Xj = torch.empty_like(Bj)
+            X0j = None if X0 is None else X0[:, j0:j1].to(self.dev, torch.float64).contiguous()
+            zj = None if zero is None else zero[j0:j1]
+            self.launch(Bj, zj, X0j, Xj)
+            it, c, r = self.read_info()
+            X[:, j0:j1] = Xj
+            its, conv, rel = max(its, it), conv and c, max(rel, r)
+        if self.debug is not None:
+            self.debug(f"  CG iter {its}: max rel. residual {rel:.2e}")
+        return X, its, conv, rel
+
+    def __call__(self, b, zero=None, x0=None):
+        import torch
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        B = torch.as_tensor(b).to(self.dev)
+        X0 = None if x0 is None else torch.as_tensor(np.ascontiguousarray(x0, np.float64)).to(self.dev)
+        X, it, conv, rel = self.solve_device(B, zero, X0)
+        return X.cpu().numpy(), it, conv, rel
+
+
+def explicit_solver(S, dinv, tol, maxiter, debug=None):
+    """(solve(b, zero, x0) -> (X, iterations, converged, rel), device name):
+    S (scipy CSR) and the preconditioner are copied to the device here, once
+    (core/gpu.py:186-197)."""
+    be = cuda_backend()
+    A = DeviceCSR.from_scipy(S, be.device)
+    return BlockSolver(A, dinv, tol, maxiter, debug), be.name
+
+
+def pcg(A: DeviceCSR, dinv, b, zero=None, x0=None, tol=1e-10, maxiter=5000, debug=None):
+    """One block-PCG solve on a device matrix (core/gpu.py:199-253): host
+    arrays in and out, `(X, iterations, converged, max_rel)`."""
+    return BlockSolver(A, dinv, tol, maxiter, debug)(b, zero, x0)

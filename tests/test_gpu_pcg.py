@@ -1,0 +1,98 @@
+"""The device block-PCG against the oracle (the reference's _pcg restated),
+on the golden panels' S and on larger panels: zero columns, warm starts,
+iteration counts and solutions, with the tolerances of the reference's own
+device test (tests/test_gpu.py:56-81 there: |d iterations| <= 1,
+max|dX| < 1e-8 max|X|)."""
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from conftest import golden_rows, load_golden, GOLDEN_PANELS
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def _solvers(S, diag, tol, maxiter=5000):
+    from hdfe_stream_b200 import gpu
+    A = gpu.DeviceCSR.from_host(*S)
+    return gpu.BlockSolver(A, orc.jacobi(diag), tol, maxiter)
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_pcg_matches_oracle_on_golden(device, name):
+    g = load_golden(name)
+    S = (g["S_indptr"], g["S_indices"], g["S_data"])
+    tol = float(g["tol"])
+    solve = _solvers(S, g["diag"], tol)
+    for x0 in (None, g["pcg_x0"]):
+        X_ref, it_ref, ok_ref, _ = orc.pcg(S, orc.jacobi(g["diag"]), g["pcg_b"], g["pcg_zero"],
+                                           x0, tol)
+        X, it, ok, rel = solve(g["pcg_b"], g["pcg_zero"], x0)
+        assert ok and ok_ref
+        assert abs(it - it_ref) <= 1
+        assert np.all(X[:, 1] == 0.0)
+        assert np.max(np.abs(X - X_ref)) < 1e-8 * np.max(np.abs(X_ref))
+        assert rel <= tol
+
+
+@pytest.mark.parametrize("k", [1, 3, 8, 11])
+def test_pcg_widths(device, k):
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    rows = pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(8, 8), p_move=0.1, seed=7))
+    c = orc.pass1(rows)
+    S = orc.build_explicit(c)
+    rng = np.random.default_rng(k)
+    b = orc.csr_matmat(S, rng.standard_normal((c.L, k)))
+    X_ref, it_ref, ok_ref, _ = orc.pcg(S, orc.jacobi(c.diag), b, None, None, 1e-10)
+    X, it, ok, rel = _solvers(S, c.diag, 1e-10)(b)
+    assert ok and ok_ref and abs(it - it_ref) <= 1
+    assert np.max(np.abs(X - X_ref)) < 1e-8 * np.max(np.abs(X_ref))
+
+
+def test_pcg_is_deterministic(device):
+    g = load_golden("akm_small")
+    S = (g["S_indptr"], g["S_indices"], g["S_data"])
+    solve = _solvers(S, g["diag"], 1e-12)
+    X1, *_ = solve(g["pcg_b"])
+    X2, *_ = solve(g["pcg_b"])
+    assert np.array_equal(X1, X2)
+
+
+def test_pcg_maxiter_reports_not_converged(device):
+    g = load_golden("akm_small")
+    S = (g["S_indptr"], g["S_indices"], g["S_data"])
+    X, it, ok, rel = _solvers(S, g["diag"], 1e-12, maxiter=3)(g["pcg_b"])
+    X_ref, it_ref, ok_ref, rel_ref = orc.pcg(S, orc.jacobi(g["diag"]), g["pcg_b"], None, None,
+                                             1e-12, maxiter=3)
+    assert it == it_ref == 3 and not ok and not ok_ref
+    assert rel == pytest.approx(rel_ref, rel=1e-6)
+
+
+def test_pcg_all_zero_columns(device):
+    g = load_golden("akm_small")
+    S = (g["S_indptr"], g["S_indices"], g["S_data"])
+    b = np.zeros((len(g["diag"]), 2))
+    X, it, ok, rel = _solvers(S, g["diag"], 1e-10)(b, np.array([True, True]))
+    assert it == 0 and ok and rel == 0.0 and np.all(X == 0)
+
+
+def test_explicit_solver_seam(device):
+    import scipy.sparse as sp
+    from hdfe_stream_b200 import gpu
+    g = load_golden("akm_weighted")
+    L = len(g["diag"])
+    S = sp.csr_matrix((g["S_data"], g["S_indices"], g["S_indptr"]), shape=(L, L))
+    solve, name = gpu.explicit_solver(S, orc.jacobi(g["diag"]), 1e-11, 5000)
+    assert "B200" in name or "NVIDIA" in name
+    X, it, ok, rel = solve(g["pcg_b"], g["pcg_zero"], None)
+    assert ok
+    assert np.max(np.abs(X - g["pcg_X"])) < 1e-8 * np.max(np.abs(g["pcg_X"]))
