@@ -30,10 +30,38 @@ _f64 = _c.c_double
 SIGNATURES = {
     "hdfe_error_string": (_c.c_char_p, []),
     "hdfe_version": (_c.c_char_p, []),
+    "hdfe_pass1_workspace_bytes": (_i64, [_i64, _i32, _i32]),
+    "hdfe_pass1": (_c.c_int, [_vp, _vp, _i32, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
+                              _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
+    "hdfe_sbuild_workspace_bytes": (_i64, [_i64, _i64, _i32]),
+    "hdfe_sbuild_wide_workspace_bytes": (_i64, [_i64, _i64]),
+    "hdfe_sbuild_analyze": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _i64,
+                                       _vp, _vp]),
+    "hdfe_sbuild_count": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _i64, _vp,
+                                     _vp, _i64, _vp, _i64, _vp, _vp]),
+    "hdfe_sbuild_fill": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
+                                    _vp, _vp, _i64, _vp, _i64, _vp, _vp]),
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),
 }
+
+
+class Pass1Counts(ctypes.Structure):
+    """struct hdfe_pass1_counts."""
+    _fields_ = [(n, _i64) for n in ("n_rows", "n_groups", "n_cells", "n_ident_groups",
+                                    "n_ident_cells", "status")]
+
+
+class SbuildInfo(ctypes.Structure):
+    """struct hdfe_sbuild_info."""
+    _fields_ = [(n, _i64) for n in ("L", "nnz", "n_wide", "n_warp_rows", "n_block_rows",
+                                    "lgrp_len", "status")]
+
+
+def read_struct(cls, t):
+    """A ctypes struct from a device tensor holding it (synchronises)."""
+    return cls.from_buffer_copy(t.cpu().numpy().tobytes()[:ctypes.sizeof(cls)])
 
 
 class PcgInfo(ctypes.Structure):

@@ -1,0 +1,185 @@
+"""The fixed-effects solve path on the device, from pass 0's rows to Gamma.
+
+This is the host side of libhdfe_b200 for a whole fit's step 1-2:
+
+    rows (pass 0 layout, in HBM)
+      -> pass1()        cells, identifying cells, obs/cnt, diag, rhs
+                        (core/passes.py:397-589 `_pass1_cells`)
+      -> build_s()      S = D_o' M_0 D_o in CSR (core/solve.py:148-194)
+      -> BlockSolver    Jacobi block PCG (core/solve.py:66-140)
+      -> normalize      (core/solve.py:383-399)
+
+Every array lives in device memory as a torch tensor; the only host reads are
+the data-dependent sizes between kernels (a few int64 each).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .gpu import BlockSolver, DeviceCSR
+
+RHS_ZERO_TOL = 1e-11        # core/solve.py:44
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@dataclass
+class DeviceRows:
+    """Pass 0's rows on the device.
+
+    gcode (N,) uint32 (as int32), codes (N, D) uint32 (as int32), V (m, N)
+    float64 one contiguous row per variable, w (N,) float64 or None."""
+
+    gcode: object
+    codes: object
+    V: object
+    w: object
+    n_levels: list
+    names: list = field(default_factory=list)
+
+    @property
+    def n_rows(self) -> int:
+        return int(self.gcode.shape[0])
+
+    @property
+    def D(self) -> int:
+        return int(self.codes.shape[1])
+
+    @property
+    def m(self) -> int:
+        return int(self.V.shape[0])
+
+    @classmethod
+    def from_rows(cls, rows, device=None, pinned=False):
+        """Upload a `simulate.Rows` (host arrays)."""
+        torch = _torch()
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+
+        def up(a, dtype):
+            t = torch.from_numpy(np.ascontiguousarray(a).view(dtype))
+            if pinned:
+                t = t.pin_memory()
+            return t.to(dev, non_blocking=pinned)
+        gcode = up(rows.gcode.astype(np.uint32), np.int32)
+        codes = up(rows.codes.astype(np.uint32), np.int32)
+        V = up(np.ascontiguousarray(rows.V.T, dtype=np.float64), np.float64)
+        w = None if rows.w is None else up(rows.w.astype(np.float64), np.float64)
+        return cls(gcode, codes, V, w, list(rows.n_levels), list(rows.names))
+
+
+@dataclass
+class DeviceCells:
+    """Pass 1's output on the device (sizes trimmed to the actual counts)."""
+
+    starts: object          # (G'+1,) int64
+    codes: object           # (M, D) int32 (uint32 values)
+    n: object               # (M,) f64
+    sums: object            # (M, m) f64 or None
+    group_n: object         # (G',) f64
+    obs: object
+    cnt: object
+    diag: object
+    rhs: object             # (L, m)
+    means: object
+    raw_ss: object
+    n_levels: list
+    counts: dict
+
+    @property
+    def L(self) -> int:
+        return int(sum(self.n_levels))
+
+    @property
+    def offs(self):
+        return np.concatenate(([0], np.cumsum(self.n_levels)[:-1])).astype(np.int64)
+
+
+def pass1(rows: DeviceRows, keep_sums: bool = False, stream=None) -> DeviceCells:
+    torch = _torch()
+    lib = _lib.lib()
+    dev = rows.gcode.device
+    N, D, m = rows.n_rows, rows.D, rows.m
+    L = int(sum(rows.n_levels))
+    f64 = dict(dtype=torch.float64, device=dev)
+    nlev = np.asarray(rows.n_levels, dtype=np.int64)
+    ws_bytes = lib.hdfe_pass1_workspace_bytes(N, m, int(keep_sums))
+    ws = torch.empty(int(ws_bytes), dtype=torch.uint8, device=dev)
+    means, raw_ss = torch.empty(m, **f64), torch.empty(m, **f64)
+    starts = torch.empty(N + 1, dtype=torch.int64, device=dev)
+    ccodes = torch.empty((N, D), dtype=torch.int32, device=dev)
+    cn = torch.empty(N, **f64)
+    csums = torch.empty((N, m), **f64) if keep_sums else None
+    gn = torch.empty(N, **f64)
+    obs, cnt, diag = torch.empty(L, **f64), torch.empty(L, **f64), torch.empty(L, **f64)
+    rhs = torch.empty((L, m), **f64)
+    counts = torch.zeros(6, dtype=torch.int64, device=dev)
+    _lib.check(lib.hdfe_pass1(
+        rows.gcode.data_ptr(), rows.codes.data_ptr(), D, rows.V.data_ptr(), m,
+        None if rows.w is None else rows.w.data_ptr(), N, nlev.ctypes.data, means.data_ptr(),
+        raw_ss.data_ptr(), starts.data_ptr(), ccodes.data_ptr(), cn.data_ptr(),
+        None if csums is None else csums.data_ptr(), gn.data_ptr(), obs.data_ptr(),
+        cnt.data_ptr(), diag.data_ptr(), rhs.data_ptr(), counts.data_ptr(), ws.data_ptr(),
+        ws.numel(), _lib.stream_handle(stream)))
+    c = _lib.read_struct(_lib.Pass1Counts, counts)
+    if c.status != _lib.HDFE_OK:
+        raise _lib.HDFEError(c.status, "pass 1: a level code is out of range")
+    G, M = int(c.n_ident_groups), int(c.n_ident_cells)
+    return DeviceCells(starts=starts[:G + 1], codes=ccodes[:M], n=cn[:M],
+                       sums=None if csums is None else csums[:M], group_n=gn[:G], obs=obs,
+                       cnt=cnt, diag=diag, rhs=rhs, means=means, raw_ss=raw_ss,
+                       n_levels=list(rows.n_levels),
+                       counts={k: int(getattr(c, k)) for k in
+                               ("n_rows", "n_groups", "n_cells", "n_ident_groups",
+                                "n_ident_cells")})
+
+
+def build_s(cells: DeviceCells, stream=None) -> DeviceCSR:
+    """S in CSR from the identifying cells (three launches, two size reads)."""
+    torch = _torch()
+    lib = _lib.lib()
+    dev = cells.starts.device
+    G = int(cells.starts.shape[0]) - 1
+    M = int(cells.codes.shape[0])
+    D = len(cells.n_levels)
+    L = cells.L
+    nlev = np.asarray(cells.n_levels, dtype=np.int64)
+    sh = _lib.stream_handle(stream)
+    ws = torch.empty(int(lib.hdfe_sbuild_workspace_bytes(L, M, D)), dtype=torch.uint8, device=dev)
+    info = torch.zeros(7, dtype=torch.int64, device=dev)
+    args = (cells.starts.data_ptr(), G, cells.codes.data_ptr(), D, cells.n.data_ptr(),
+            cells.group_n.data_ptr(), M, nlev.ctypes.data)
+    _lib.check(lib.hdfe_sbuild_analyze(*args, ws.data_ptr(), ws.numel(), info.data_ptr(), sh))
+    inf = _lib.read_struct(_lib.SbuildInfo, info)
+    if inf.status != _lib.HDFE_OK:
+        raise _lib.HDFEError(inf.status, "S build: a level code is out of range")
+    W = int(inf.n_wide)
+    wide = torch.empty(max(int(lib.hdfe_sbuild_wide_workspace_bytes(L, W)), 1),
+                       dtype=torch.uint8, device=dev)
+    indptr = torch.empty(L + 1, dtype=torch.int64, device=dev)
+    _lib.check(lib.hdfe_sbuild_count(*args, W, indptr.data_ptr(), ws.data_ptr(), ws.numel(),
+                                     wide.data_ptr(), wide.numel(), info.data_ptr(), sh))
+    nnz = int(_lib.read_struct(_lib.SbuildInfo, info).nnz)
+    indices = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    data = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+    _lib.check(lib.hdfe_sbuild_fill(*args, W, indptr.data_ptr(), indices.data_ptr(),
+                                    data.data_ptr(), ws.data_ptr(), ws.numel(), wide.data_ptr(),
+                                    wide.numel(), info.data_ptr(), sh))
+    S = DeviceCSR(indptr, indices[:nnz], data[:nnz], L, nnz)
+    S.info = {k: int(getattr(inf, k)) for k in ("n_wide", "n_warp_rows", "n_block_rows")}
+    return S
+
+
+def jacobi(diag):
+    """core/solve.py:142-146 `_jacobi` on the device."""
+    torch = _torch()
+    pos = diag > 1e-12
+    return torch.where(pos, 1.0 / torch.where(pos, diag, torch.ones_like(diag)),
+                       torch.zeros_like(diag))

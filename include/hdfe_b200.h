@@ -43,6 +43,82 @@ const char *hdfe_error_string(void);
 /* Library version string. */
 const char *hdfe_version(void);
 
+/* Limits of the device path: non-streamed fixed-effect dimensions, and design
+ * variables (outcome + covariates) per pass. */
+#define HDFE_MAX_DIMS 4
+#define HDFE_MAX_VARS 16
+
+/* ------------------------------------------------------------------ pass 1
+ *
+ * Rows -> cells -> identifying cells, with the level bookkeeping: obs / cnt
+ * per level over all cells, the Jacobi diagonal of S and the right-hand side
+ * D_o' M_0 V over the identifying cells.  Replaces core/passes.py:397-531
+ * `_pass1_cells` with `_cell_chunks` (:533-589), `_nb_run_sums`
+ * (core/kernels_base.py:375-422), `_nb_diag` (:87-110) and `_nb_rhs`
+ * (:65-83), for the plain case (no varying slopes).
+ *
+ * Input rows are pass 0's layout: sorted by (gcode, codes...), gcode (N)
+ * uint32 the dense code of the streamed dimension, codes (N, D) uint32,
+ * V (m, N) float64 one contiguous row per variable (outcome first), w (N)
+ * float64 analytic weights or NULL.  n_levels (D) is a HOST array.
+ * Outputs are sized for the worst case (every row its own identifying cell):
+ * starts (N+1) int64, cell_codes (N, D), cell_n (N), cell_sums (N, m) or NULL,
+ * group_n (N): each identifying group's sum of n; obs, cnt, diag (L), rhs
+ * (L, m), means and raw_ss (m): the variables' means and sums of squared
+ * deviations; counts: DEVICE pointer, the actual sizes and a status
+ * (HDFE_ERR_BAD_CODE if a code is out of range).
+ */
+typedef struct hdfe_pass1_counts {
+    int64_t n_rows, n_groups, n_cells, n_ident_groups, n_ident_cells, status;
+} hdfe_pass1_counts;
+
+int64_t hdfe_pass1_workspace_bytes(int64_t n_rows, int32_t m, int32_t keep_sums);
+
+int hdfe_pass1(const uint32_t *gcode, const uint32_t *codes, int32_t D, const double *V,
+               int32_t m, const double *w, int64_t n_rows, const int64_t *n_levels,
+               double *means, double *raw_ss, int64_t *starts, uint32_t *cell_codes,
+               double *cell_n, double *cell_sums, double *group_n, double *obs, double *cnt,
+               double *diag, double *rhs, hdfe_pass1_counts *counts, void *workspace,
+               int64_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------- explicit S
+ *
+ * S = D_o' M_0 D_o in CSR with sorted columns, from the identifying cells.
+ * Replaces core/solve.py:148-194 `_build_explicit` and its kernels
+ * core/kernels_base.py:201-358 (`_nb_level_groups`, `_nb_row_work`,
+ * `_nb_row_nnz`, `_nb_row_fill`), plain case.  Three calls on one workspace
+ * (hdfe_sbuild_workspace_bytes), because the sizes are data-dependent:
+ *   analyze  per-level work and classes; info->n_wide = wide rows
+ *   count    needs a wide workspace (hdfe_sbuild_wide_workspace_bytes with
+ *            n_wide); writes indptr (L+1) and info->nnz
+ *   fill     writes indices (nnz) int32 and data (nnz) float64
+ * The caller reads info (a DEVICE pointer) between the calls.
+ */
+typedef struct hdfe_sbuild_info {
+    int64_t L, nnz, n_wide, n_warp_rows, n_block_rows, lgrp_len, status;
+} hdfe_sbuild_info;
+
+int64_t hdfe_sbuild_workspace_bytes(int64_t L, int64_t n_cells, int32_t D);
+int64_t hdfe_sbuild_wide_workspace_bytes(int64_t L, int64_t n_wide);
+
+int hdfe_sbuild_analyze(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                        int32_t D, const double *n, const double *group_n, int64_t n_cells,
+                        const int64_t *n_levels, void *workspace, int64_t workspace_bytes,
+                        hdfe_sbuild_info *info, void *stream);
+
+int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                      int32_t D, const double *n, const double *group_n, int64_t n_cells,
+                      const int64_t *n_levels, int64_t n_wide, int64_t *indptr,
+                      void *workspace, int64_t workspace_bytes, void *wide_workspace,
+                      int64_t wide_workspace_bytes, hdfe_sbuild_info *info, void *stream);
+
+int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                     int32_t D, const double *n, const double *group_n, int64_t n_cells,
+                     const int64_t *n_levels, int64_t n_wide, const int64_t *indptr,
+                     int32_t *indices, double *data, void *workspace, int64_t workspace_bytes,
+                     void *wide_workspace, int64_t wide_workspace_bytes,
+                     hdfe_sbuild_info *info, void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,
