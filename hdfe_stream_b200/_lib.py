@@ -41,6 +41,10 @@ SIGNATURES = {
                                      _vp, _i64, _vp, _i64, _vp, _vp]),
     "hdfe_sbuild_fill": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
                                     _vp, _vp, _i64, _vp, _i64, _vp, _vp]),
+    "hdfe_components_workspace_bytes": (_i64, []),
+    "hdfe_components": (_c.c_int, [_vp, _i64, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp]),
+    "hdfe_normalize_workspace_bytes": (_i64, [_i64, _i32]),
+    "hdfe_normalize": (_c.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),

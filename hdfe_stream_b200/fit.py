@@ -183,3 +183,100 @@ def jacobi(diag):
     pos = diag > 1e-12
     return torch.where(pos, 1.0 / torch.where(pos, diag, torch.ones_like(diag)),
                        torch.zeros_like(diag))
+
+
+def components(cells: DeviceCells, col: int = 0, stream=None):
+    """Component root of each level of dimension `col` (its smallest level),
+    and the number of components (core/kernels_base.py:156-174)."""
+    torch = _torch()
+    lib = _lib.lib()
+    dev = cells.starts.device
+    nl = int(cells.n_levels[col])
+    root = torch.empty(nl, dtype=torch.int32, device=dev)
+    out = torch.zeros(2, dtype=torch.int64, device=dev)
+    ws = torch.empty(int(lib.hdfe_components_workspace_bytes()), dtype=torch.uint8, device=dev)
+    G = int(cells.starts.shape[0]) - 1
+    _lib.check(lib.hdfe_components(cells.starts.data_ptr(), G, cells.codes.data_ptr(),
+                                   len(cells.n_levels), col, nl, root.data_ptr(), out.data_ptr(),
+                                   ws.data_ptr(), ws.numel(), _lib.stream_handle(stream)))
+    return root, out
+
+
+def rank_components(root, cnt_first):
+    """Labels 0, 1, ... by rows, ties to the smallest root (a stable sort):
+    core/passes.py:933-950 `_rank_components`, on host arrays."""
+    root = np.asarray(root, dtype=np.int64)
+    nl = len(root)
+    is_root = root == np.arange(nl)
+    dense = (np.cumsum(is_root) - 1)[root]
+    rows = np.bincount(dense, weights=cnt_first, minlength=int(is_root.sum()))
+    order = np.argsort(-rows, kind="stable")
+    rank = np.empty(len(order), np.int64)
+    rank[order] = np.arange(len(order))
+    return rank[dense], len(order)
+
+
+def normalize(gamma, cells: DeviceCells, root, stream=None):
+    """core/solve.py:383-399 `_normalize` on the device, Gamma (L, m) in place."""
+    torch = _torch()
+    lib = _lib.lib()
+    m = int(gamma.shape[1])
+    nlev = np.asarray(cells.n_levels, dtype=np.int64)
+    ws = torch.empty(int(lib.hdfe_normalize_workspace_bytes(int(nlev[0]), m)), dtype=torch.uint8,
+                     device=gamma.device)
+    _lib.check(lib.hdfe_normalize(gamma.data_ptr(), m, len(nlev), nlev.ctypes.data,
+                                  cells.obs.data_ptr(), root.data_ptr(), ws.data_ptr(),
+                                  ws.numel(), _lib.stream_handle(stream)))
+    return gamma
+
+
+@dataclass
+class FitResult:
+    """Step 2's output for the estimator's own variables."""
+
+    gamma: object               # (L, m) device tensor, normalised
+    info: dict
+    cells: DeviceCells
+    S: DeviceCSR
+    root: object
+
+
+def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
+          x0=None, normalize_fe=True) -> FitResult:
+    """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
+    right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
+    zero, block PCG per `rhs_block` columns, then `_normalize`."""
+    torch = _torch()
+    m = int(cells.rhs.shape[1])
+    dinv = jacobi(cells.diag)
+    solver = BlockSolver(S, dinv, tol, maxiter)
+    scale = torch.sqrt(torch.clamp(cells.raw_ss, min=0.0))
+    zero_all = (torch.linalg.vector_norm(cells.rhs, dim=0) <= RHS_ZERO_TOL * scale).cpu().numpy()
+    root, ncomp = components(cells, 0)
+    gamma = torch.empty_like(cells.rhs)
+    its, conv, rel = [], True, 0.0
+    for j0 in range(0, m, rhs_block):
+        j1 = min(m, j0 + rhs_block)
+        X, it, c, r = solver.solve_device(cells.rhs[:, j0:j1], zero_all[j0:j1],
+                                          None if x0 is None else x0[:, j0:j1])
+        gamma[:, j0:j1] = X
+        its.append(it)
+        conv &= c
+        rel = max(rel, r)
+    if normalize_fe:
+        normalize(gamma, cells, root)
+    n_comp = ncomp.cpu().numpy()
+    if int(n_comp[1]) != _lib.HDFE_OK:
+        raise _lib.HDFEError(int(n_comp[1]), "components: union-find failed")
+    info = {"solver": "explicit", "device": "cuda", "iterations": its if len(its) > 1 else its[0],
+            "converged": conv, "max_rel_residual": rel, "S_nnz": S.nnz,
+            "S_mb": round(S.nbytes / 1e6, 1), "n_components": int(n_comp[0]),
+            "fe_spanned": [j for j in range(m) if zero_all[j]]}
+    return FitResult(gamma=gamma, info=info, cells=cells, S=S, root=root)
+
+
+def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8) -> FitResult:
+    """Pass 1, the S build and step 2 on the device, for device rows."""
+    cells = pass1(rows)
+    S = build_s(cells)
+    return solve(cells, S, tol, maxiter, rhs_block)

@@ -119,6 +119,30 @@ int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const uint32_t *co
                      void *wide_workspace, int64_t wide_workspace_bytes,
                      hdfe_sbuild_info *info, void *stream);
 
+/* ------------------------------------------------ components, normalisation
+ *
+ * hdfe_components: union-find over dimension `col` of the identifying cells
+ * (levels sharing a group are connected).  Replaces core/kernels_base.py:
+ * 156-174 `_nb_components`: root (n_levels) int32 out is each level's
+ * component root, its smallest level, as the reference's; n_components is a
+ * DEVICE int64[2]: the number of components, then a status.  Ranking the
+ * roots by rows (core/passes.py:933-950) is left to the caller.
+ *
+ * hdfe_normalize: core/solve.py:383-399 `_normalize` on Gamma (L, m) in place:
+ * the first dimension's effects get obs-weighted mean zero within each
+ * component (root from hdfe_components), further dimensions obs-weighted mean
+ * zero.  n_levels (D) is a HOST array.
+ */
+int64_t hdfe_components_workspace_bytes(void);
+int hdfe_components(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                    int32_t col, int64_t n_levels, int32_t *root, int64_t *n_components,
+                    void *workspace, int64_t workspace_bytes, void *stream);
+
+int64_t hdfe_normalize_workspace_bytes(int64_t n_first, int32_t m);
+int hdfe_normalize(double *gamma, int32_t m, int32_t D, const int64_t *n_levels,
+                   const double *obs, const int32_t *root, void *workspace,
+                   int64_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,

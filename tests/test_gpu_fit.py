@@ -1,0 +1,72 @@
+"""The device fit's step 2 (components, PCG, normalisation) against the
+oracle's `_solve` (pinned to the reference's): fixed effects within 1e-8
+relative, component roots identical."""
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from conftest import golden_rows, load_golden, GOLDEN_PANELS
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def _panels():
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    out = [(n, golden_rows(load_golden(n))) for n in GOLDEN_PANELS]
+    out.append(("akm_20k", pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(8, 8),
+                                                        p_move=0.1, seed=21))))
+    out.append(("weighted", pass0_layout(simulate_panel(20_000, 1_000, 10, spell=(1, 10),
+                                                         p_move=0.1, weights=True, seed=22))))
+    return out
+
+
+PANELS = _panels()
+
+
+@pytest.mark.parametrize("name,rows", PANELS, ids=[p[0] for p in PANELS])
+def test_components_match_oracle(device, name, rows):
+    from hdfe_stream_b200 import fit
+    ref = orc.pass1(rows)
+    root_ref = orc.components(ref, 0)
+    cells = fit.pass1(fit.DeviceRows.from_rows(rows))
+    root, n = fit.components(cells, 0)
+    assert np.array_equal(root.cpu().numpy(), root_ref)
+    comp, nc = fit.rank_components(root.cpu().numpy(), ref.cnt[:ref.n_levels[0]])
+    comp_ref, nc_ref = orc.component_labels(ref)
+    assert nc == nc_ref == int(n.cpu().numpy()[0])
+    assert np.array_equal(comp, comp_ref)
+
+
+@pytest.mark.parametrize("name,rows", PANELS, ids=[p[0] for p in PANELS])
+def test_fixed_effects_match_oracle(device, name, rows):
+    from hdfe_stream_b200 import fit
+    ref = orc.pass1(rows)
+    S = orc.build_explicit(ref)
+    gamma_ref, info_ref = orc.solve(ref, S, tol=1e-12)
+    res = fit.fit(fit.DeviceRows.from_rows(rows), tol=1e-12)
+    gamma = res.gamma.cpu().numpy()
+    assert res.info["converged"]
+    err = np.max(np.abs(gamma - gamma_ref)) / np.max(np.abs(gamma_ref))
+    assert err < 1e-8, err
+    its = np.atleast_1d(res.info["iterations"])
+    assert np.all(np.abs(its - np.atleast_1d(info_ref["iterations"])) <= 1)
+
+
+def test_golden_gamma(device):
+    """Against the reference's own _solve output, stored in the golden file."""
+    from hdfe_stream_b200 import fit
+    for name in GOLDEN_PANELS:
+        g = load_golden(name)
+        res = fit.fit(fit.DeviceRows.from_rows(golden_rows(g)), tol=float(g["tol"]))
+        gamma = res.gamma.cpu().numpy()
+        err = np.max(np.abs(gamma - g["gamma"])) / np.max(np.abs(g["gamma"]))
+        assert err < 1e-8, (name, err)
