@@ -1,0 +1,350 @@
+"""Benchmark of the fixed-effects solve path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one AKM fit's hot path over the 5M-worker panel (5,000,000
+workers, 500,000 firms, 15 years, ~8.5 rows per worker, yearly move
+probability 0.08; largest connected set after min_degree = 2), model
+log_earn ~ age_squared + age_cubed | worker_id + firm_id + year:
+pass 1 (cells, identifying cells, obs/cnt, Jacobi diagonal, D_o'M_0V), the
+explicit S, the connected components, the FP64 block PCG to tol 1e-10 and the
+normalisation of the fixed effects -- on rows already in HBM (`value`), and
+through the public call with host rows and the effects copied back (`e2e`).
+The panel is built on the host first (generation and pass 0's layout and
+restriction are not timed).  Under torchrun each rank fits its own panel
+(weak scaling, no collective on the data path); rank 0 prints one JSON line.
+
+`--impl reference` times the reference's CPU implementation of the same path
+(the oracle's restatement of its numba kernels, all host threads) on the
+same panel, rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+WORKLOAD = "akm_5m"
+METRIC = "AKM fit throughput (pass 1 + S build + FP64 Jacobi PCG to 1e-10 + normalisation)"
+UNIT = "fits/s"
+PEAKS = REPO / "MEASURED_PEAKS.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(args, n, rows):
+    return {"workload": f"{args.workload}: 5M workers, 500k firms, 15 years, ~8.5 rows/worker, "
+                        "p_move 0.08, largest connected set with min_degree=2",
+            "rows": rows.n_rows, "workers": rows.n_groups, "levels": int(sum(rows.n_levels)),
+            "model": "log_earn ~ age_squared + age_cubed | worker_id + firm_id + year",
+            "tol": args.tol, "parallelism": f"replicas{n}" if n > 1 else "single",
+            "l2": "inputs (rows, S) larger than the 126 MB L2"}
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- algorithmic bytes
+
+def phase_bytes(rows, counts, S, iterations, m=3):
+    """Compulsory DRAM bytes per launch of each phase (written out in the
+    design notes): pass 1 reads each row once and writes the identifying
+    cells and level arrays; the S build reads the cells and writes S; one
+    PCG iteration reads S and streams the L x k vectors."""
+    N, D, L = rows.n_rows, rows.codes.shape[1], int(sum(rows.n_levels))
+    M, G = counts["n_ident_cells"], counts["n_ident_groups"]
+    w = 0 if rows.w is None else 8
+    p1 = N * (4 + 4 * D + 8 * m + w) + M * (4 * D + 8) + G * 16 + L * 8 * (3 + m)
+    sb = M * (4 * D + 8) + G * 16 + S.nnz * 12 + (L + 1) * 8
+    per_it = 12 * S.nnz + 8 * (L + 1) + 8 * L * m * 9
+    return {"pass1": p1, "sbuild": sb, "pcg_kernel": per_it * max(iterations, 1)}
+
+
+def measured_peak():
+    try:
+        d = json.loads(PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from hdfe_stream_b200 import _lib, fit
+    from hdfe_stream_b200.simulate import prepare
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    rows = prepare(args.workload, seed=rank)
+    drows = fit.DeviceRows.from_rows(rows)
+    torch.cuda.synchronize()
+    for _ in range(max(args.warmup, 0)):
+        res = fit.fit(drows, tol=args.tol)
+    torch.cuda.synchronize()
+    lib = _lib.lib()
+    timer = fit.PhaseTimer()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.hdfe_kernel_launches()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        res = fit.fit(drows, tol=args.tol, timer=timer)
+    t1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = lib.hdfe_kernel_launches() - launches0
+    clocks = sampler.stop()
+    ms = t0.elapsed_time(t1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    phases = timer.totals()
+    info = res.info
+    its = int(np.max(np.atleast_1d(info["iterations"])))
+
+    # e2e through the public call: pinned host rows up, fixed effects back
+    e2e = run_e2e(args, rows, dist)
+
+    out = None
+    if rank == 0:
+        value = world * args.steps / (ms / 1e3)
+        by = phase_bytes(rows, res.cells.counts, res.S, its)
+        peak, peak_kind = measured_peak()
+        roof = {}
+        for name in ("pass1", "sbuild", "pcg_kernel"):
+            tot, cnt = phases.get(name, (0.0, 0))
+            if cnt:
+                avg_ms = tot / cnt
+                gbs = by[name] / (avg_ms / 1e3) / 1e9
+                roof[name] = {"ms": round(avg_ms, 4), "bytes": int(by[name]),
+                              "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+        dom = max(roof, key=lambda k: roof[k]["ms"])
+        out = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, 5M-worker AKM panel per rank)",
+            "config": config(args, world, rows),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": roof[dom]["achieved_gbs"],
+                         "peak": peak, "unit": "GB/s",
+                         "frac": roof[dom]["frac"], "traffic": None,
+                         "peak_source": f"{peak_kind} hbm_gbs", "phases": roof},
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+            "solve": {"iterations": info["iterations"], "converged": info["converged"],
+                      "max_rel_residual": info["max_rel_residual"], "S_nnz": info["S_nnz"],
+                      "n_components": info["n_components"]},
+        }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out, rows
+
+
+def run_e2e(args, rows, dist):
+    """Same metric through fit.fit_rows-style calls with pinned host buffers:
+    every step copies the rows host->device and the fixed effects back."""
+    import torch
+    from hdfe_stream_b200 import fit
+
+    pinned = {
+        "gcode": torch.from_numpy(rows.gcode.view(np.int32)).pin_memory(),
+        "codes": torch.from_numpy(np.ascontiguousarray(rows.codes).view(np.int32)).pin_memory(),
+        "V": torch.from_numpy(np.ascontiguousarray(rows.V.T)).pin_memory(),
+    }
+    h2d = sum(t.numel() * t.element_size() for t in pinned.values())
+    out_host = None
+    d2h = 0
+
+    def step():
+        nonlocal out_host, d2h
+        dev = {k: v.to("cuda", non_blocking=True) for k, v in pinned.items()}
+        drows = fit.DeviceRows(dev["gcode"], dev["codes"], dev["V"], None, list(rows.n_levels))
+        res = fit.fit(drows, tol=args.tol)
+        if out_host is None:
+            out_host = torch.empty(res.gamma.shape, dtype=res.gamma.dtype, pin_memory=True)
+        out_host.copy_(res.gamma, non_blocking=True)
+        d2h = res.gamma.numel() * res.gamma.element_size()
+
+    step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    world = 1
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        world = dist.get_world_size()
+    return {"value": round(world * args.steps / (ms / 1e3), 4), "unit": UNIT,
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+
+# ------------------------------------------------------- the CPU baseline
+
+def oracle_fit(rows, tol):
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as orc
+    cells = orc.pass1(rows)
+    S = orc.build_explicit(cells)
+    gamma, info = orc.solve(cells, S, tol=tol)
+    return gamma, info
+
+
+def cpu_baseline(rows, tol, steps=1):
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as orc
+    orc.set_threads(os.cpu_count() or 1)
+    t = time.perf_counter()
+    for _ in range(steps):
+        oracle_fit(rows, tol)
+    dt = time.perf_counter() - t
+    return {"value": round(steps / dt, 5), "unit": UNIT, "cores": orc.num_threads(),
+            "kind": "port", "seconds_per_fit": round(dt / steps, 3),
+            "sample": f"{steps} full fit(s) of the same panel on the host cores (the oracle: "
+                      "the reference's numba kernels restated in C, OpenMP over all threads)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    from hdfe_stream_b200.simulate import prepare
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as orc
+    orc.set_threads(os.cpu_count() or 1)
+    rows = prepare(args.workload, seed=0)
+    for _ in range(max(args.warmup, 0)):
+        oracle_fit(rows, args.tol)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        _, info = oracle_fit(rows, args.tol)
+    dt = time.perf_counter() - t
+    value = args.steps / dt
+    return {"metric": METRIC, "value": round(value, 5), "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(dt / args.steps * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, 5M-worker AKM panel)",
+            "config": config(args, 1, rows),
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": orc.num_threads(),
+                             "kind": "port",
+                             "sample": "full fits of the panel, each step one fit"},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "solve": {"iterations": info["iterations"], "converged": info["converged"]}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    out, rows = run_ours(args, rank, world, local_rank)
+    if rank == 0 and out is not None:
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(rows, args.tol)
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

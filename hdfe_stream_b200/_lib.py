@@ -30,6 +30,7 @@ _f64 = _c.c_double
 SIGNATURES = {
     "hdfe_error_string": (_c.c_char_p, []),
     "hdfe_version": (_c.c_char_p, []),
+    "hdfe_kernel_launches": (_i64, []),
     "hdfe_pass1_workspace_bytes": (_i64, [_i64, _i32, _i32]),
     "hdfe_pass1": (_c.c_int, [_vp, _vp, _i32, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
                               _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),

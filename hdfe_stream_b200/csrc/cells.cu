@@ -573,6 +573,7 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     HDFE_CUDA_TRY(cudaGetLastError());
     write_counts<<<1, 32, 0, s>>>(totals, totals + 2, N, counts, status);
     HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(7);
     return HDFE_OK;
 }
 

@@ -1,5 +1,6 @@
 // Error reporting and version of libhdfe_b200.
 #include <cstdio>
+#include <atomic>
 #include <cstring>
 #include <cuda_runtime.h>
 
@@ -7,7 +8,12 @@
 
 namespace {
 thread_local char g_msg[512] = "no error";
+std::atomic<long long> g_launches{0};
 }
+
+void hdfe_add_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+extern "C" int64_t hdfe_kernel_launches(void) { return g_launches.load(); }
 
 int hdfe_set_cuda_error(cudaError_t e)
 {

@@ -115,3 +115,5 @@ __device__ __forceinline__ T block_sum(T v, T *scratch)
 int hdfe_set_cuda_error(cudaError_t e);
 int hdfe_set_error(int code, const char *msg);
 int hdfe_set_arg_error(const char *msg);
+// counts kernels launched by the library (hdfe_kernel_launches)
+void hdfe_add_launches(int n);

@@ -211,6 +211,7 @@ extern "C" int hdfe_components(const int64_t *starts, int64_t n_groups, const ui
         starts, n_groups, codes, D, col, n_levels, root, status);
     graph::k_flatten<<<graph::grid_for(n_levels), graph::kThreads, 0, s>>>(root, n_levels, roots);
     HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(3);
     // n_components[0] = roots, n_components[1] = status
     HDFE_CUDA_TRY(cudaMemcpyAsync(n_components, roots, 8, cudaMemcpyDeviceToDevice, s));
     HDFE_CUDA_TRY(cudaMemsetAsync(n_components + 1, 0, 8, s));
@@ -253,5 +254,6 @@ extern "C" int hdfe_normalize(double *gamma, int32_t m, int32_t D, const int64_t
         off += nl;
     }
     HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(2 + 2 * (D - 1));
     return HDFE_OK;
 }

@@ -478,7 +478,7 @@ int grid_blocks()
     return sms * (per_sm < 2 ? per_sm : 2);
 }
 
-int grid_blocks_for(int k)
+int grid_blocks_for_uncached(int k)
 {
     switch (k) {
     case 1: return grid_blocks<1>();
@@ -491,6 +491,16 @@ int grid_blocks_for(int k)
     case 8: return grid_blocks<8>();
     }
     return -1;
+}
+
+// occupancy per (device, k), computed once
+int grid_blocks_for(int k)
+{
+    static int cache[64][HDFE_PCG_MAX_K + 1] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return grid_blocks_for_uncached(k);
+    if (cache[dev][k] == 0) cache[dev][k] = grid_blocks_for_uncached(k);
+    return cache[dev][k];
 }
 
 template <int K>
@@ -568,5 +578,6 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     HDFE_CUDA_TRY(e);
     pcg::pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);
     HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(2);
     return HDFE_OK;
 }

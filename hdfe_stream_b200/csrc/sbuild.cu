@@ -713,6 +713,7 @@ extern "C" int hdfe_sbuild_analyze(const int64_t *starts, int64_t n_groups,
     k_fill_lists<<<grid_for(a.G, kThreads, cap), kThreads, 0, c.s>>>(a);
     k_write_info<<<1, 32, 0, c.s>>>(a, info);
     HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(8);
     return HDFE_OK;
 }
 
@@ -747,6 +748,7 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
     if (st != HDFE_OK) return st;
     k_write_info<<<1, 32, 0, c.s>>>(a, info);
     HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(n_wide > 0 ? 8 : 6);
     return HDFE_OK;
 }
 
@@ -775,5 +777,6 @@ extern "C" int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const u
     if (n_wide > 0) k_wide_fill<<<grid_for(n_wide, 1, c.sms * 4), kThreads, 0, c.s>>>(a);
     k_write_info<<<1, 32, 0, c.s>>>(a, info);
     HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(n_wide > 0 ? 4 : 3);
     return HDFE_OK;
 }

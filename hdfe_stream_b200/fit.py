@@ -242,14 +242,16 @@ class FitResult:
 
 
 def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
-          x0=None, normalize_fe=True) -> FitResult:
+          x0=None, normalize_fe=True, timer=None) -> FitResult:
     """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
     right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
     zero, block PCG per `rhs_block` columns, then `_normalize`."""
     torch = _torch()
+    timer = timer or _NoTimer()
     m = int(cells.rhs.shape[1])
     dinv = jacobi(cells.diag)
     solver = BlockSolver(S, dinv, tol, maxiter)
+    solver.timer = timer
     scale = torch.sqrt(torch.clamp(cells.raw_ss, min=0.0))
     zero_all = (torch.linalg.vector_norm(cells.rhs, dim=0) <= RHS_ZERO_TOL * scale).cpu().numpy()
     root, ncomp = components(cells, 0)
@@ -275,8 +277,58 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     return FitResult(gamma=gamma, info=info, cells=cells, S=S, root=root)
 
 
-def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8) -> FitResult:
+class PhaseTimer:
+    """CUDA events around the phases of a fit, on the current stream:
+    `with timer("pass1"): ...`; `totals()` gives milliseconds per phase."""
+
+    def __init__(self):
+        self.events = []
+
+    def __call__(self, name):
+        timer = self
+
+        class _Phase:
+            def __enter__(self_):
+                torch = _torch()
+                self_.a = torch.cuda.Event(enable_timing=True)
+                self_.b = torch.cuda.Event(enable_timing=True)
+                self_.a.record()
+
+            def __exit__(self_, *exc):
+                self_.b.record()
+                timer.events.append((name, self_.a, self_.b))
+        return _Phase()
+
+    def totals(self):
+        _torch().cuda.synchronize()
+        out = {}
+        for name, a, b in self.events:
+            t = out.setdefault(name, [0.0, 0])
+            t[0] += a.elapsed_time(b)
+            t[1] += 1
+        return out
+
+
+class _NoTimer:
+    def __call__(self, name):
+        import contextlib
+        return contextlib.nullcontext()
+
+
+def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None) -> FitResult:
     """Pass 1, the S build and step 2 on the device, for device rows."""
-    cells = pass1(rows)
-    S = build_s(cells)
-    return solve(cells, S, tol, maxiter, rhs_block)
+    timer = timer or _NoTimer()
+    with timer("pass1"):
+        cells = pass1(rows)
+    with timer("sbuild"):
+        S = build_s(cells)
+    with timer("solve"):
+        return solve(cells, S, tol, maxiter, rhs_block, timer=timer)
+
+
+def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):
+    """The fit from host rows (pass 0's layout, `simulate.Rows`): upload,
+    solve on the device, and the normalised fixed effects back on the host.
+    Returns (gamma (L, m) numpy, info)."""
+    res = fit(DeviceRows.from_rows(rows), tol, maxiter, rhs_block)
+    return res.gamma.cpu().numpy(), res.info

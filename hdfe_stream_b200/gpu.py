@@ -139,7 +139,12 @@ class BlockSolver:
             Xj = torch.empty_like(Bj)
             X0j = None if X0 is None else X0[:, j0:j1].to(self.dev, torch.float64).contiguous()
             zj = None if zero is None else zero[j0:j1]
-            self.launch(Bj, zj, X0j, Xj)
+            timer = getattr(self, "timer", None)
+            if timer is not None:
+                with timer("pcg_kernel"):
+                    self.launch(Bj, zj, X0j, Xj)
+            else:
+                self.launch(Bj, zj, X0j, Xj)
             it, c, r = self.read_info()
             X[:, j0:j1] = Xj
             its, conv, rel = max(its, it), conv and c, max(rel, r)

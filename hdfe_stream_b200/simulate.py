@@ -141,7 +141,14 @@ class Rows:
 
 def _rank_codes(values: np.ndarray):
     """Codes = rank of each value among the sorted distinct values
-    (core/passes.py:285-294: unique().sort() then a row index)."""
+    (core/passes.py:285-294: unique().sort() then a row index).  Ids are
+    small non-negative integers here, so a presence table does it in O(n)."""
+    values = np.asarray(values)
+    if len(values) and values.min() >= 0 and values.max() < 4 * len(values) + 1024:
+        present = np.zeros(int(values.max()) + 1, bool)
+        present[values] = True
+        rank = np.cumsum(present) - 1
+        return rank[values].astype(np.uint32), np.flatnonzero(present)
     levels, codes = np.unique(values, return_inverse=True)
     return codes.astype(np.uint32), levels
 
@@ -150,14 +157,18 @@ def pass0_layout(panel: Panel, keep: np.ndarray | None = None) -> Rows:
     """Rows of `panel` (optionally only those where `keep`) in pass 0's
     layout, sorted by (worker, firm, year, variables)."""
     sel = slice(None) if keep is None else np.asarray(keep, bool)
-    worker = panel.worker[sel]
-    g, wlev = _rank_codes(worker)
+    g, wlev = _rank_codes(panel.worker[sel])
     c1, flev = _rank_codes(panel.firm[sel])
     c2, ylev = _rank_codes(panel.year[sel])
     V = np.column_stack([panel.log_earn[sel], panel.age_squared[sel],
                          panel.age_cubed[sel]]).astype(np.float64)
     w = None if panel.weight is None else panel.weight[sel].astype(np.float64)
-    order = np.lexsort((V[:, 2], V[:, 1], V[:, 0], c2, c1, g))
+    key = (g.astype(np.int64) * len(flev) + c1) * len(ylev) + c2
+    order = np.argsort(key, kind="stable")
+    sk = key[order]
+    if len(sk) > 1 and bool(np.any(sk[1:] == sk[:-1])):
+        # rows sharing (worker, firm, year): the variables break the tie
+        order = np.lexsort((V[:, 2], V[:, 1], V[:, 0], c2, c1, g))
     return Rows(gcode=np.ascontiguousarray(g[order]),
                 codes=np.ascontiguousarray(np.column_stack([c1[order], c2[order]])),
                 V=np.ascontiguousarray(V[order]),
@@ -165,6 +176,54 @@ def pass0_layout(panel: Panel, keep: np.ndarray | None = None) -> Rows:
                 n_levels=[len(flev), len(ylev)], n_groups=len(wlev),
                 names=["log_earn", "age_squared", "age_cubed"],
                 ids={"worker": wlev, "firm": flev, "year": ylev})
+
+
+def restrict_connected(panel: Panel, min_degree=(1, 1)) -> np.ndarray:
+    """Rows kept by pass 0's `connected="largest"` restriction of the
+    (worker, firm) graph, after `min_degree` pruning: core/passes.py:780-857
+    `_connected_restriction` with core/connected.py:378-493
+    `_find_components` -- levels with fewer than k distinct partners are
+    removed until none is left, then the largest component by rows is kept
+    (ties to the component holding the smallest worker).  This is input
+    preparation on the host (pass 0), not a device kernel."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    _, wlev = _rank_codes(panel.worker)
+    a, _ = _rank_codes(panel.worker)
+    b, flev = _rank_codes(panel.firm)
+    n0, n1 = len(wlev), len(flev)
+    key = a.astype(np.int64) * n1 + b
+    run = np.concatenate(([True], key[1:] != key[:-1]))
+    keys, inv = np.unique(key[run], return_inverse=True)
+    counts = np.bincount(inv, weights=np.diff(np.append(np.flatnonzero(run), len(key))))
+    pa, pb = keys // n1, keys % n1
+    alive0, alive1 = np.ones(n0, bool), np.ones(n1, bool)
+    k0, k1 = (min_degree, min_degree) if np.isscalar(min_degree) else min_degree
+    if (k0, k1) != (1, 1):
+        while True:
+            e = alive0[pa] & alive1[pb]
+            d0 = np.bincount(pa[e], minlength=n0)
+            d1 = np.bincount(pb[e], minlength=n1)
+            drop0 = alive0 & (d0 < k0)
+            drop1 = alive1 & (d1 < k1)
+            if not (drop0.any() or drop1.any()):
+                break
+            alive0 &= ~drop0
+            alive1 &= ~drop1
+    e = alive0[pa] & alive1[pb]
+    nv = n0 + n1
+    adj = coo_matrix((np.ones(int(e.sum())), (pa[e], n0 + pb[e])), shape=(nv, nv))
+    nc, lab = connected_components(adj, directed=False)
+    alive = np.concatenate([alive0, alive1])
+    rows = np.bincount(lab[pa[e]], weights=counts[e], minlength=nc)
+    first = np.full(nc, nv, np.int64)
+    np.minimum.at(first, lab, np.where(alive, np.arange(nv), nv))
+    order = np.lexsort((first, -rows))
+    best = order[0]
+    ok0 = alive0 & (lab[:n0] == best)
+    ok1 = alive1 & (lab[n0:] == best)
+    return ok0[a] & ok1[b]
 
 
 # The panels the solve path is measured on, by what they are.
@@ -182,3 +241,12 @@ PANELS = {
     "akm_400k_w": dict(n_workers=400_000, n_firms=40_000, n_years=10, spell=(7, 10),
                        p_move=0.1, weights=True),
 }
+
+
+def prepare(name: str, seed: int = 0):
+    """The named panel's rows in pass 0's layout, restricted as its
+    specification says (akm_5m: largest connected set with min_degree 2)."""
+    spec = dict(PANELS[name])
+    panel = simulate_panel(seed=seed, **spec)
+    keep = restrict_connected(panel, (2, 2)) if name == "akm_5m" else None
+    return pass0_layout(panel, keep)

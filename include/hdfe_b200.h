@@ -43,6 +43,9 @@ const char *hdfe_error_string(void);
 /* Library version string. */
 const char *hdfe_version(void);
 
+/* Kernels this library has launched in this process (all entry points). */
+int64_t hdfe_kernel_launches(void);
+
 /* Limits of the device path: non-streamed fixed-effect dimensions, and design
  * variables (outcome + covariates) per pass. */
 #define HDFE_MAX_DIMS 4
