@@ -33,15 +33,18 @@ SIGNATURES = {
     "hdfe_kernel_launches": (_i64, []),
     "hdfe_pass1_workspace_bytes": (_i64, [_i64, _i32, _i32]),
     "hdfe_pass1": (_c.c_int, [_vp, _vp, _i32, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
-                              _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
+                              _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
+                              _vp]),
     "hdfe_sbuild_workspace_bytes": (_i64, [_i64, _i64, _i32]),
-    "hdfe_sbuild_wide_workspace_bytes": (_i64, [_i64, _i64]),
-    "hdfe_sbuild_analyze": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _i64,
-                                       _vp, _vp]),
-    "hdfe_sbuild_count": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _i64, _vp,
-                                     _vp, _i64, _vp, _i64, _vp, _vp]),
-    "hdfe_sbuild_fill": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
-                                    _vp, _vp, _i64, _vp, _i64, _vp, _vp]),
+    "hdfe_sbuild_wide_workspace_bytes": (_i64, [_i64, _i64, _i32, _i64]),
+    "hdfe_sbuild_analyze": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _vp,
+                                       _vp, _i64, _vp, _vp]),
+    "hdfe_sbuild_count": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _vp,
+                                     _i64, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp,
+                                     _vp]),
+    "hdfe_sbuild_fill": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _vp, _i64,
+                                    _i64, _vp, _vp, _vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp,
+                                    _vp]),
     "hdfe_components_workspace_bytes": (_i64, []),
     "hdfe_components": (_c.c_int, [_vp, _i64, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_normalize_workspace_bytes": (_i64, [_i64, _i32]),
@@ -61,7 +64,7 @@ class Pass1Counts(ctypes.Structure):
 class SbuildInfo(ctypes.Structure):
     """struct hdfe_sbuild_info."""
     _fields_ = [(n, _i64) for n in ("L", "nnz", "n_wide", "n_warp_rows", "n_block_rows",
-                                    "lgrp_len", "status")]
+                                    "lgrp_len", "temp_len", "status")]
 
 
 def read_struct(cls, t):

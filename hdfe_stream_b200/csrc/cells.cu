@@ -37,6 +37,8 @@ constexpr int kGroupTile = 1024;        // groups per tile (4 per thread)
 constexpr int kMaxDims = HDFE_MAX_DIMS;
 constexpr int kMaxVars = HDFE_MAX_VARS;
 constexpr int kSmemLevelBudget = 40 * 1024;   // bytes of level accumulators per CTA
+// a shared level slot: obs, cnt, diag, groups (lcount), work, then rhs[m]
+constexpr int kSlotFixed = 5;
 
 struct Dims {
     int D, m;
@@ -281,6 +283,8 @@ struct GroupArgs {
     double *cell_sums;          // (M, m) or null: then a scratch buffer is used
     double *group_n;            // (G') sum of n over the group's cells
     double *obs, *cnt, *diag, *rhs;
+    int32_t *lcount;            // identifying groups per level (or null)
+    int64_t *work;              // cells of those groups per level
     unsigned *status;
 };
 
@@ -330,7 +334,7 @@ __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, i
                 c[d] = 0;
             }
             if (dm.small[d]) {
-                double *slot = s_acc + (dm.soff[d] + c[d]) * (3 + m);
+                double *slot = s_acc + (dm.soff[d] + c[d]) * (kSlotFixed + m);
                 atomicAdd(slot + 0, n);
                 atomicAdd(slot + 1, cntv);
             } else {
@@ -362,12 +366,12 @@ __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, i
         const double n = a.cell_n[k];
 #pragma unroll
         for (int d = 0; d < D; d++) {
-            double *sl = dm.small[d] ? s_acc + (dm.soff[d] + c[d]) * (3 + m) : nullptr;
+            double *sl = dm.small[d] ? s_acc + (dm.soff[d] + c[d]) * (kSlotFixed + m) : nullptr;
             const int64_t lv = dm.offs[d] + c[d];
             if (sl) atomicAdd(sl + 2, n); else atomicAdd(a.diag + lv, n);
             for (int v = 0; v < m; v++) {
                 const double r = sums_buf[k * m + v] - n * vbar[v];
-                if (sl) atomicAdd(sl + 3 + v, r); else atomicAdd(a.rhs + lv * m + v, r);
+                if (sl) atomicAdd(sl + kSlotFixed + v, r); else atomicAdd(a.rhs + lv * m + v, r);
             }
         }
     }
@@ -384,8 +388,18 @@ __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, i
             for (int64_t k2 = k; k2 < q; k2++)
                 if (a.cell_codes[k2 * D + d] == ck) u += a.cell_n[k2];
             const double corr = -(u * u / Ng);
-            if (dm.small[d]) atomicAdd(s_acc + (dm.soff[d] + ck) * (3 + m) + 2, corr);
-            else atomicAdd(a.diag + dm.offs[d] + ck, corr);
+            if (dm.small[d]) {
+                double *sl = s_acc + (dm.soff[d] + ck) * (kSlotFixed + m);
+                atomicAdd(sl + 2, corr);
+                if (a.lcount) { atomicAdd(sl + 3, 1.0); atomicAdd(sl + 4, (double)(q - co)); }
+            } else {
+                atomicAdd(a.diag + dm.offs[d] + ck, corr);
+                if (a.lcount) {
+                    atomicAdd(a.lcount + dm.offs[d] + ck, 1);
+                    atomicAdd(reinterpret_cast<unsigned long long *>(a.work) + dm.offs[d] + ck,
+                              (unsigned long long)(q - co));
+                }
+            }
         }
     }
 }
@@ -397,7 +411,7 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
     __shared__ int s_scr[2][kThreads / 32 + 1];
     const Dims &dm = a.dims;
     const int m = dm.m;
-    const int64_t nsm = dm.n_small * (3 + m);
+    const int64_t nsm = dm.n_small * (kSlotFixed + m);
     for (int64_t k = threadIdx.x; k < nsm; k += kThreads) s_acc[k] = 0.0;
     __syncthreads();
     const int64_t G = a.totals[0];
@@ -425,13 +439,18 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
     for (int d = 0; d < dm.D; d++) {
         if (!dm.small[d]) continue;
         for (int64_t l = threadIdx.x; l < dm.nlev[d]; l += kThreads) {
-            const double *sl = s_acc + (dm.soff[d] + l) * (3 + m);
+            const double *sl = s_acc + (dm.soff[d] + l) * (kSlotFixed + m);
             const int64_t lv = dm.offs[d] + l;
             if (sl[0] != 0.0) atomicAdd(a.obs + lv, sl[0]);
             if (sl[1] != 0.0) atomicAdd(a.cnt + lv, sl[1]);
             if (sl[2] != 0.0) atomicAdd(a.diag + lv, sl[2]);
+            if (a.lcount && sl[3] != 0.0) {
+                atomicAdd(a.lcount + lv, (int)sl[3]);
+                atomicAdd(reinterpret_cast<unsigned long long *>(a.work) + lv,
+                          (unsigned long long)sl[4]);
+            }
             for (int v = 0; v < m; v++)
-                if (sl[3 + v] != 0.0) atomicAdd(a.rhs + lv * m + v, sl[3 + v]);
+                if (sl[kSlotFixed + v] != 0.0) atomicAdd(a.rhs + lv * m + v, sl[kSlotFixed + v]);
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -480,8 +499,8 @@ template <int D>
 int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, const double *w,
         int64_t N, const int64_t *n_levels, double *means, double *raw_ss, int64_t *starts,
         uint32_t *cell_codes, double *cell_n, double *cell_sums, double *group_n, double *obs,
-        double *cnt, double *diag, double *rhs, hdfe_pass1_counts *counts, char *ws,
-        cudaStream_t s)
+        double *cnt, double *diag, double *rhs, int32_t *lcount, int64_t *work,
+        hdfe_pass1_counts *counts, char *ws, cudaStream_t s)
 {
     Layout lay = layout(N, m, cell_sums == nullptr);
     int64_t *tile_cnt = (int64_t *)(ws + lay.tile_cnt);
@@ -503,7 +522,7 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
         L += n_levels[d];
     }
     // small dimensions: shared-memory accumulators, smallest first
-    const int64_t per_level = (3 + m) * 8;
+    const int64_t per_level = (kSlotFixed + m) * 8;
     for (int pass = 0; pass < D; pass++) {
         int best = -1;
         for (int d = 0; d < D; d++)
@@ -525,6 +544,10 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     HDFE_CUDA_TRY(cudaMemsetAsync(cnt, 0, L * 8, s));
     HDFE_CUDA_TRY(cudaMemsetAsync(diag, 0, L * 8, s));
     HDFE_CUDA_TRY(cudaMemsetAsync(rhs, 0, L * m * 8, s));
+    if (lcount) {
+        HDFE_CUDA_TRY(cudaMemsetAsync(lcount, 0, L * 4, s));
+        HDFE_CUDA_TRY(cudaMemsetAsync(work, 0, L * 8, s));
+    }
     const int64_t rtiles = (N + kRowTile - 1) / kRowTile;
     RowArgs ra{gcode, codes, V, N, m, tile_cnt, tile_mom, status};
     rows_count<D><<<(unsigned)rtiles, kThreads, 0, s>>>(ra);
@@ -560,6 +583,8 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     ga.cnt = cnt;
     ga.diag = diag;
     ga.rhs = rhs;
+    ga.lcount = lcount;
+    ga.work = work;
     ga.status = status;
     int dev = 0, sms = 0, per_sm = 0;
     HDFE_CUDA_TRY(cudaGetDevice(&dev));
@@ -593,12 +618,14 @@ extern "C" int hdfe_pass1(const uint32_t *gcode, const uint32_t *codes, int32_t 
                           const int64_t *n_levels, double *means, double *raw_ss,
                           int64_t *starts, uint32_t *cell_codes, double *cell_n,
                           double *cell_sums, double *group_n, double *obs, double *cnt,
-                          double *diag, double *rhs, hdfe_pass1_counts *counts, void *workspace,
-                          int64_t workspace_bytes, void *stream)
+                          double *diag, double *rhs, int32_t *lcount, int64_t *work,
+                          hdfe_pass1_counts *counts, void *workspace, int64_t workspace_bytes,
+                          void *stream)
 {
     if (D < 1 || D > HDFE_MAX_DIMS || m < 0 || m > HDFE_MAX_VARS || n_rows < 1 || !gcode ||
         !codes || (m > 0 && !V) || !n_levels || !starts || !cell_codes || !cell_n || !group_n ||
-        !obs || !cnt || !diag || (m > 0 && !rhs) || !counts || !workspace || !means || !raw_ss)
+        !obs || !cnt || !diag || (m > 0 && !rhs) || !counts || !workspace || !means || !raw_ss ||
+        ((lcount == nullptr) != (work == nullptr)))
         return hdfe_set_arg_error("hdfe_pass1: bad argument");
     for (int d = 0; d < D; d++)
         if (n_levels[d] < 1 || n_levels[d] > 0xffffffffll)
@@ -612,16 +639,16 @@ extern "C" int hdfe_pass1(const uint32_t *gcode, const uint32_t *codes, int32_t 
     switch (D) {
     case 1: return cells::run<1>(gcode, codes, V, m, w, n_rows, n_levels, means, raw_ss, starts,
                                  cell_codes, cell_n, cell_sums, group_n, obs, cnt, diag, rhs,
-                                 counts, ws, s);
+                                 lcount, work, counts, ws, s);
     case 2: return cells::run<2>(gcode, codes, V, m, w, n_rows, n_levels, means, raw_ss, starts,
                                  cell_codes, cell_n, cell_sums, group_n, obs, cnt, diag, rhs,
-                                 counts, ws, s);
+                                 lcount, work, counts, ws, s);
     case 3: return cells::run<3>(gcode, codes, V, m, w, n_rows, n_levels, means, raw_ss, starts,
                                  cell_codes, cell_n, cell_sums, group_n, obs, cnt, diag, rhs,
-                                 counts, ws, s);
+                                 lcount, work, counts, ws, s);
     case 4: return cells::run<4>(gcode, codes, V, m, w, n_rows, n_levels, means, raw_ss, starts,
                                  cell_codes, cell_n, cell_sums, group_n, obs, cnt, diag, rhs,
-                                 counts, ws, s);
+                                 lcount, work, counts, ws, s);
     }
     return hdfe_set_arg_error("hdfe_pass1: D out of range");
 }

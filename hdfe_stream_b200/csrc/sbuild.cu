@@ -9,29 +9,27 @@
 // out sorted, and the pattern (every level of every group the row's level is
 // in, explicit zeros included) is the reference's.
 //
-// B200 mapping:
-//   analyze     one thread per group: the distinct levels of the group (first
-//               occurrences) -> per-level group count and work (cells
-//               scanned to build the row), as `_nb_level_groups` /
-//               `_nb_row_work`.  Levels are then classed by work: "warp"
-//               rows (one warp each, a 512-slot shared hash), "block" rows
-//               (one CTA each, an 8192-slot hash) and "wide" rows (levels of
-//               small dimensions, e.g. years, in most groups).
-//   lists       the groups of each narrow level (level -> group index).
-//   count/fill  narrow rows: a warp streams the row's groups (sorted, so the
-//               sums have a fixed order) 32 cells at a time; lanes with the
-//               same column are combined with __match_any_sync by their
-//               lowest lane in lane order, then added to the row's hash
-//               slot.  The fill pass sorts the row's (column, value) pairs
-//               in shared memory (bitonic) and writes them at indptr[r].
-//   wide rows   S is symmetric: a wide row's entries at narrow columns are
-//               the narrow rows' entries at the wide column, stored into a
-//               dense (wide x L) buffer by the narrow fill; the wide x wide
-//               block is summed over all groups, privatised in shared memory
-//               per CTA.  Each wide row is then a stream compaction of its
-//               dense row, which leaves its columns sorted.
-// Values are FP64 sums in a fixed order per row (narrow) or atomic order
-// (wide x wide); the pattern and nnz are exact.
+// B200 mapping (three calls: analyze, count, fill):
+//   analyze   per-level group counts and work (from pass 1, or k_level_stats)
+//             -> each level's class: "warp" rows (one warp, a shared hash of
+//             32-512 slots), "block" rows (one CTA, up to 8192 slots), or
+//             "wide" rows (levels of small dimensions such as years, present
+//             in most groups); the groups of each narrow level (lists).
+//   count     narrow rows, ONE pass: a warp sorts the row's groups (fixed
+//             summation order), flattens the row's (group, cell) items over
+//             all 32 lanes, and adds each item's v into the hash slot of each
+//             of its columns -- lanes with the same column combined first by
+//             __match_any_sync in lane order, so the sums are deterministic.
+//             The row is compacted, sorted (bitonic) and parked in a temp
+//             buffer at a capacity bound; its entries at wide columns also go
+//             to a dense (wide x L) buffer.  Wide x wide block: each warp
+//             owns the W^2 entries in registers over a fixed set of groups,
+//             then fixed-order sums over warps and CTAs (no atomics).  Row
+//             nnz -> indptr.
+//   fill      narrow rows copied from the temp buffer to their final place;
+//             each wide row is the compaction of its dense row (S is
+//             symmetric: the narrow rows' entries at the wide column), in
+//             column segments processed in parallel.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -40,21 +38,27 @@ namespace hdfe {
 namespace sbuild {
 
 constexpr int kThreads = 256;
-constexpr int kWarpSlots = 512;                 // hash slots per warp (warp rows)
-constexpr int kBlockSlots = 8192;               // hash slots per CTA (block rows)
-constexpr int kWarpListCap = 256;               // groups per warp row (sorted in smem)
-constexpr int kBlockListCap = 4096;             // groups per block row
+constexpr int kWarpSlots = 512;                 // max hash slots per warp (warp rows)
+constexpr int kBlockSlots = 8192;               // max hash slots per CTA (block rows)
+constexpr int kWarpListCap = 128;               // groups per warp row
+constexpr int kBlockListCap = 2048;             // groups per block row
 constexpr int32_t kEmptyKey = -1;
-constexpr int32_t kKindEmpty = -1, kKindWarp = -2, kKindBlock = -3;
-constexpr int kWideSmem = 64;                   // wide x wide block in smem up to this W
+constexpr int32_t kKindEmpty = -1, kKindWarp = -2, kKindBlock = -3, kKindWide = -100;
+constexpr int kWideWarp = 16;                   // wide x wide in warp registers up to this W
+constexpr int kWideEntries = (kWideWarp * kWideWarp + 31) / 32;   // entries per lane
 constexpr int kScanTile = 4096;
+constexpr int64_t kSeg = 16384;                 // columns per wide-row segment
+constexpr int kWarpsPerCta = 4;
 
 // work thresholds: distinct columns <= work * D must stay <= 3/4 of a table
 __host__ __device__ inline int64_t warp_work(int D) { return (kWarpSlots * 3 / 4) / D; }
-__host__ __device__ inline int64_t block_work(int D)
+__host__ __device__ inline int64_t block_work(int D) { return (kBlockSlots * 3 / 4) / D; }
+
+__host__ __device__ inline int ceil_log2(int64_t x)
 {
-    int64_t by_slots = (kBlockSlots * 3 / 4) / D;
-    return by_slots < kBlockListCap ? by_slots : kBlockListCap;
+    int b = 0;
+    while ((int64_t(1) << b) < x) b++;
+    return b;
 }
 
 struct Args {
@@ -68,23 +72,35 @@ struct Args {
     int64_t L;
     int64_t offs[HDFE_MAX_DIMS];
     int64_t nlev[HDFE_MAX_DIMS];
+    // per-level statistics (pass 1's, or computed here)
+    const int32_t *lcount;
+    const unsigned long long *work;
     // main workspace
-    int32_t *lcount;
-    unsigned long long *work;
+    int32_t *lcount_ws;
+    unsigned long long *work_ws;
     int32_t *kind;              // kKind* or the wide index
     int64_t *lptr;              // (L+1)
     int32_t *fillpos;
     int32_t *lgrp;
-    int64_t *rnnz;              // (L+1) row nnz, then scanned
+    int64_t *rnnz;              // (L+1) row nnz
+    int64_t *toff;              // (L+1) temp offsets of the narrow rows
     int32_t *wide_list;         // wide index -> level
     int32_t *warp_rows, *block_rows;
     int64_t *tiles;             // scan partials
-    int64_t *ctr;               // [0] W, [1] warp rows, [2] block rows, [3] lgrp len, [4] nnz
+    int64_t *ctr;               // [0] W, [1] warp rows, [2] block rows, [3] lgrp len,
+                                // [4] nnz, [5] temp len
     unsigned *status;
-    // wide workspace (count/fill only)
+    // wide workspace
     double *dval;               // (W, L)
     uint8_t *dpres;             // (W, L)
-    int64_t W;
+    int32_t *cell_widx;         // (M, D) wide index of each cell's level, or -1
+    double *wpart;              // (CTAs, W*W) per-CTA wide x wide sums
+    uint8_t *wpres;             // (CTAs, W*W)
+    int64_t *segcnt;            // (W, nseg)
+    int64_t W, nseg, wide_ctas;
+    // temp
+    int32_t *tcol;
+    double *tval;
     // output
     int64_t *indptr;
     int32_t *indices;
@@ -100,6 +116,7 @@ __device__ __forceinline__ int level_dim(const Args &a, int64_t r)
 
 // ------------------------------------------------------------- analyze
 
+// per-level group counts and work, when the caller has no pass-1 statistics
 __global__ void __launch_bounds__(kThreads) k_level_stats(Args a)
 {
     for (int64_t g = (int64_t)blockIdx.x * kThreads + threadIdx.x; g < a.G;
@@ -115,8 +132,8 @@ __global__ void __launch_bounds__(kThreads) k_level_stats(Args a)
                 if (!first) continue;
                 if ((int64_t)c >= a.nlev[d]) { atomicCAS(a.status, 0u, (unsigned)HDFE_ERR_BAD_CODE); continue; }
                 const int64_t lv = a.offs[d] + c;
-                atomicAdd(a.lcount + lv, 1);
-                atomicAdd(a.work + lv, size);
+                atomicAdd(a.lcount_ws + lv, 1);
+                atomicAdd(a.work_ws + lv, size);
             }
         }
     }
@@ -128,26 +145,29 @@ __global__ void __launch_bounds__(kThreads) k_classify(Args a)
     for (int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x; r < a.L;
          r += (int64_t)gridDim.x * kThreads) {
         const unsigned long long w = a.work[r];
+        const int32_t lc = a.lcount[r];
         int32_t k;
         if (w == 0) k = kKindEmpty;
-        else if ((int64_t)w <= ww && a.lcount[r] <= kWarpListCap) k = kKindWarp;
-        else if ((int64_t)w <= bw && a.lcount[r] <= kBlockListCap) k = kKindBlock;
-        else k = -100;
+        else if ((int64_t)w <= ww && lc <= kWarpListCap) k = kKindWarp;
+        else if ((int64_t)w <= bw && lc <= kBlockListCap) k = kKindBlock;
+        else k = kKindWide;
         if (k == kKindWarp) a.warp_rows[atomicAdd((unsigned long long *)(a.ctr + 1), 1ull)] = (int32_t)r;
         if (k == kKindBlock) a.block_rows[atomicAdd((unsigned long long *)(a.ctr + 2), 1ull)] = (int32_t)r;
-        if (k == -100) {
+        if (k == kKindWide) {
             const int64_t wi = (int64_t)atomicAdd((unsigned long long *)a.ctr, 1ull);
             a.wide_list[wi] = (int32_t)r;
             k = (int32_t)wi;
         }
         a.kind[r] = k;
-        // narrow levels keep their group lists
-        a.lptr[r] = (k == kKindWarp || k == kKindBlock) ? a.lcount[r] : 0;
+        const bool narrow = k == kKindWarp || k == kKindBlock;
+        a.lptr[r] = narrow ? lc : 0;
+        // capacity of the row in the temp buffer: its distinct columns at most
+        const int64_t cap = (int64_t)w * a.D < a.L ? (int64_t)w * a.D : a.L;
+        a.toff[r] = narrow ? cap : 0;
     }
 }
 
-// The wide list in level order, so a wide row's index does not depend on
-// the atomic order above (one CTA; W is small).
+// the wide list in level order, so wide indices do not depend on atomics
 __global__ void k_sort_wide(Args a)
 {
     if (threadIdx.x != 0) return;
@@ -169,8 +189,7 @@ __global__ void __launch_bounds__(kThreads) k_scan_tiles(const int64_t *x, int64
     const int64_t t0 = (int64_t)blockIdx.x * kScanTile, t1 = min(t0 + kScanTile, n);
     int64_t s = 0;
     for (int64_t i = t0 + threadIdx.x; i < t1; i += kThreads) s += x[i];
-    // integer sums stay exact in double up to 2^53
-    double t = block_sum((double)s, s_red);
+    double t = block_sum((double)s, s_red);     // integer sums stay exact below 2^53
     if (threadIdx.x == 0) tiles[blockIdx.x] = (int64_t)t;
 }
 
@@ -247,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) k_fill_lists(Args a)
                 const int32_t k = a.kind[lv];
                 if (k == kKindWarp || k == kKindBlock) {
                     const int32_t at = atomicAdd(a.fillpos + lv, 1);
-                    a.lgrp[a.lptr[lv] + at] = (int32_t)g;
+                    if (a.lptr[lv] + at < a.lptr[lv + 1]) a.lgrp[a.lptr[lv] + at] = (int32_t)g;
                 }
             }
         }
@@ -261,18 +280,17 @@ __device__ __forceinline__ uint32_t slot_of(int32_t col, int bits)
     return ((uint32_t)col * 2654435761u) >> (32 - bits);
 }
 
-// Sorts n (<= cap, cap a power of two) int32 keys in smem ascending, with
-// an optional double payload; the tail up to cap is padded with INT32_MAX.
-__device__ void bitonic_sort(int32_t *key, double *val, int n, int cap, int lane, int lanes,
-                             bool block)
+// Sort n int32 keys (ascending, n <= the buffer's power-of-two capacity) in
+// warp-shared memory, with an optional double payload.
+__device__ void warp_bitonic(int32_t *key, double *val, int n, int lane)
 {
     int size = 1;
     while (size < n) size <<= 1;
-    for (int i = n + lane; i < size; i += lanes) key[i] = INT32_MAX;
-    if (block) __syncthreads(); else __syncwarp();
+    for (int i = n + lane; i < size; i += 32) key[i] = INT32_MAX;
+    __syncwarp();
     for (int k = 2; k <= size; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = lane; i < size; i += lanes) {
+            for (int i = lane; i < size; i += 32) {
                 const int ixj = i ^ j;
                 if (ixj > i) {
                     const bool up = (i & k) == 0;
@@ -284,242 +302,412 @@ __device__ void bitonic_sort(int32_t *key, double *val, int n, int cap, int lane
                     }
                 }
             }
-            if (block) __syncthreads(); else __syncwarp();
+            __syncwarp();
         }
     }
-    (void)cap;
 }
 
-// One narrow row, processed by one warp.  `fill` false: count its distinct
-// columns (and mark its wide columns); true: accumulate, sort, write.
-// Shared buffers: keys/vals (slots), list (list_cap ints), stage (32 doubles).
-__device__ void narrow_row(const Args &a, int64_t r, bool fill, int32_t *keys, double *vals,
-                           int bits, int32_t *list, double *stage, int *s_cnt)
+struct RowSmem {
+    int32_t *keys;
+    double *vals;
+    int32_t *list;      // the row's groups
+    int32_t *loff;      // (nl+1) item offsets
+    int64_t *gs;        // first cell of each listed group
+    double *wv;         // u_r / N_g of each listed group
+    double *stage;      // 32
+    int *cnt;
+};
+
+// One narrow row by one warp: accumulate, compact, sort, park in temp.
+__device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_bits)
 {
     const int lane = threadIdx.x & 31;
-    const int slots = 1 << bits;
     const int dr = level_dim(a, r);
     const uint32_t lr = (uint32_t)(r - a.offs[dr]);
-    for (int i = lane; i < slots; i += 32) { keys[i] = kEmptyKey; if (fill) vals[i] = 0.0; }
+    const int64_t cap = a.toff[r + 1] - a.toff[r];
+    int bits = ceil_log2((cap * 4 + 2) / 3);
+    bits = bits < 5 ? 5 : (bits > max_bits ? max_bits : bits);
+    const int slots = 1 << bits;
+    for (int i = lane; i < slots; i += 32) { sm.keys[i] = kEmptyKey; sm.vals[i] = 0.0; }
     // the row's groups, ascending
     const int64_t l0 = a.lptr[r];
     const int nl = (int)(a.lptr[r + 1] - l0);
-    for (int i = lane; i < nl; i += 32) list[i] = a.lgrp[l0 + i];
-    if (lane == 0) *s_cnt = 0;
+    for (int i = lane; i < nl; i += 32) sm.list[i] = a.lgrp[l0 + i];
+    if (lane == 0) *sm.cnt = 0;
     __syncwarp();
-    bitonic_sort(list, nullptr, nl, 0, lane, 32, false);
-    for (int li = 0; li < nl; li++) {
-        const int64_t g = list[li];
+    warp_bitonic(sm.list, nullptr, nl, lane);
+    // per group: first cell, cell count, u_r / N_g (one lane per group)
+    for (int k = lane; k < nl; k += 32) {
+        const int64_t g = sm.list[k];
         const int64_t s = a.starts[g], e = a.starts[g + 1];
-        // u_r over the group's cells
         double ur = 0.0;
-        for (int64_t i = s + lane; i < e; i += 32)
+        for (int64_t i = s; i < e; i++)
             if (a.codes[i * a.D + dr] == lr) ur += a.n[i];
-        ur = warp_sum(ur);
-        const double wv = ur / a.group_n[g];
-        for (int64_t base = s; base < e; base += 32) {
-            const int64_t i = base + lane;
-            const bool valid = i < e;
-            double v = 0.0;
-            if (valid) {
-                const double ni = a.n[i];
-                v -= ni * wv;
-                if (a.codes[i * a.D + dr] == lr) v += ni;
+        sm.gs[k] = s;
+        sm.loff[k] = (int32_t)(e - s);
+        sm.wv[k] = ur / a.group_n[g];
+    }
+    __syncwarp();
+    // exclusive offsets of the groups' cells (the row's items)
+    int32_t carry = 0;
+    for (int base = 0; base < nl; base += 32) {
+        const int k = base + lane;
+        const int32_t v = k < nl ? sm.loff[k] : 0;
+        int32_t inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        __syncwarp();
+        if (k < nl) sm.loff[k] = carry + inc - v;
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+        __syncwarp();
+    }
+    if (lane == 0) sm.loff[nl] = carry;
+    __syncwarp();
+    const int32_t items = carry;
+    for (int32_t base = 0; base < items; base += 32) {
+        const int32_t j = base + lane;
+        const bool valid = j < items;
+        int64_t i = 0;
+        double v = 0.0;
+        if (valid) {
+            int lo = 0, hi = nl;            // last group with loff <= j
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (sm.loff[mid] <= j) lo = mid; else hi = mid;
             }
-            for (int d = 0; d < a.D; d++) {
-                const int32_t col = valid ? (int32_t)(a.offs[d] + a.codes[i * a.D + d]) : -1;
-                const unsigned peers = __match_any_sync(0xffffffffu, col);
-                const int leader = __ffs(peers) - 1;
-                stage[lane] = v;
-                __syncwarp();
-                if (valid && lane == leader) {
-                    double sum = 0.0;
-                    for (unsigned p = peers; p; p &= p - 1) sum += stage[__ffs(p) - 1];
-                    uint32_t h = slot_of(col, bits);
-                    for (int probe = 0; probe < slots; probe++) {
-                        const int32_t old = atomicCAS(keys + h, kEmptyKey, col);
-                        if (old == kEmptyKey || old == col) {
-                            if (old == kEmptyKey) atomicAdd(s_cnt, 1);
-                            if (fill) vals[h] += sum;
-                            break;
-                        }
-                        h = (h + 1) & (slots - 1);
+            i = sm.gs[lo] + (j - sm.loff[lo]);
+            const double ni = a.n[i];
+            v -= ni * sm.wv[lo];
+            if (a.codes[i * a.D + dr] == lr) v += ni;
+        }
+        for (int d = 0; d < a.D; d++) {
+            const int32_t col = valid ? (int32_t)(a.offs[d] + a.codes[i * a.D + d]) : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, col);
+            const int leader = __ffs(peers) - 1;
+            sm.stage[lane] = v;
+            __syncwarp();
+            if (valid && lane == leader) {
+                double sum = 0.0;
+                for (unsigned p = peers; p; p &= p - 1) sum += sm.stage[__ffs(p) - 1];
+                uint32_t h = slot_of(col, bits);
+                for (int probe = 0; probe < slots; probe++) {
+                    const int32_t old = atomicCAS(sm.keys + h, kEmptyKey, col);
+                    if (old == kEmptyKey || old == col) {
+                        if (old == kEmptyKey) atomicAdd(sm.cnt, 1);
+                        sm.vals[h] += sum;
+                        break;
                     }
+                    h = (h + 1) & (slots - 1);
                 }
-                __syncwarp();
             }
+            __syncwarp();
         }
     }
     __syncwarp();
-    const int cnt = *s_cnt;
-    if (!fill) {
-        if (lane == 0) a.rnnz[r] = cnt;
-        // mark the row's wide columns: the wide rows' entries at column r
-        for (int i = lane; i < slots; i += 32) {
-            const int32_t c = keys[i];
-            if (c == kEmptyKey) continue;
-            const int32_t k = a.kind[c];
-            if (k >= 0) a.dpres[(int64_t)k * a.L + r] = 1;
-        }
-        return;
-    }
-    // compact the table to its first cnt slots, sort by column, write
+    const int cnt = *sm.cnt;
+    // compact the table to its first cnt slots (entries never overtake unread slots)
     __syncwarp();
-    if (lane == 0) *s_cnt = 0;
+    if (lane == 0) *sm.cnt = 0;
     __syncwarp();
     for (int base = 0; base < slots; base += 32) {
         const int i = base + lane;
-        const int32_t c = keys[i];
-        const double v = vals[i];
+        const int32_t c = sm.keys[i];
+        const double v = sm.vals[i];
         const bool has = c != kEmptyKey;
         const unsigned m = __ballot_sync(0xffffffffu, has);
         const int before = __popc(m & ((1u << lane) - 1));
-        int at0 = 0;
-        if (lane == 0) at0 = *s_cnt;
-        at0 = __shfl_sync(0xffffffffu, at0, 0);
+        const int at0 = *sm.cnt;
         __syncwarp();
-        // compacted entries never overtake the slots still to be read
-        if (has) { keys[at0 + before] = c; vals[at0 + before] = v; }
+        if (has) { sm.keys[at0 + before] = c; sm.vals[at0 + before] = v; }
         __syncwarp();
-        if (lane == 0) *s_cnt = at0 + __popc(m);
+        if (lane == 0) *sm.cnt = at0 + __popc(m);
         __syncwarp();
     }
-    bitonic_sort(keys, vals, cnt, slots, lane, 32, false);
-    const int64_t p0 = a.indptr[r];
+    warp_bitonic(sm.keys, sm.vals, cnt, lane);
+    const int64_t t0 = a.toff[r];
     for (int i = lane; i < cnt; i += 32) {
-        a.indices[p0 + i] = keys[i];
-        a.data[p0 + i] = vals[i];
-        const int32_t k = a.kind[keys[i]];
-        if (k >= 0) a.dval[(int64_t)k * a.L + r] = vals[i];
+        const int32_t c = sm.keys[i];
+        a.tcol[t0 + i] = c;
+        a.tval[t0 + i] = sm.vals[i];
+        const int32_t k = a.kind[c];
+        if (k >= 0) {
+            a.dpres[(int64_t)k * a.L + r] = 1;
+            a.dval[(int64_t)k * a.L + r] = sm.vals[i];
+        }
     }
+    if (lane == 0) a.rnnz[r] = cnt;
+    __syncwarp();
 }
 
-constexpr int kWarpsPerCta = 4;      // 4 x 7.4 KB of tables: static smem < 48 KB
-
-__global__ void __launch_bounds__(kWarpsPerCta * 32) k_warp_rows(Args a, bool fill)
+__global__ void __launch_bounds__(kWarpsPerCta * 32) k_warp_rows(Args a)
 {
     __shared__ int32_t s_keys[kWarpsPerCta][kWarpSlots];
     __shared__ double s_vals[kWarpsPerCta][kWarpSlots];
     __shared__ int32_t s_list[kWarpsPerCta][kWarpListCap];
+    __shared__ int32_t s_loff[kWarpsPerCta][kWarpListCap + 1];
+    __shared__ int64_t s_gs[kWarpsPerCta][kWarpListCap];
+    __shared__ double s_wv[kWarpsPerCta][kWarpListCap];
     __shared__ double s_stage[kWarpsPerCta][32];
     __shared__ int s_cnt[kWarpsPerCta];
     const int w = threadIdx.x >> 5;
+    RowSmem sm{s_keys[w], s_vals[w], s_list[w], s_loff[w], s_gs[w], s_wv[w], s_stage[w], &s_cnt[w]};
     const int64_t nrows = a.ctr[1];
-    const int bits = 9;     // log2(kWarpSlots)
     for (int64_t k = (int64_t)blockIdx.x * kWarpsPerCta + w; k < nrows;
          k += (int64_t)gridDim.x * kWarpsPerCta)
-        narrow_row(a, a.warp_rows[k], fill, s_keys[w], s_vals[w], bits, s_list[w], s_stage[w],
-                   &s_cnt[w]);
+        narrow_row(a, a.warp_rows[k], sm, 9);
 }
 
-// block rows: one warp per CTA with the large table in dynamic smem
-__global__ void __launch_bounds__(32) k_block_rows(Args a, bool fill)
+// block rows: one warp per CTA with the large table in dynamic shared memory
+__global__ void __launch_bounds__(32) k_block_rows(Args a)
 {
     extern __shared__ unsigned char s_raw[];
     double *vals = reinterpret_cast<double *>(s_raw);
-    int32_t *keys = reinterpret_cast<int32_t *>(vals + kBlockSlots);
+    double *wv = vals + kBlockSlots;
+    int64_t *gs = reinterpret_cast<int64_t *>(wv + kBlockListCap);
+    int32_t *keys = reinterpret_cast<int32_t *>(gs + kBlockListCap);
     int32_t *list = keys + kBlockSlots;
+    int32_t *loff = list + kBlockListCap;
     __shared__ double s_stage[32];
     __shared__ int s_cnt;
+    RowSmem sm{keys, vals, list, loff, gs, wv, s_stage, &s_cnt};
     const int64_t nrows = a.ctr[2];
-    const int bits = 13;    // log2(kBlockSlots)
     for (int64_t k = blockIdx.x; k < nrows; k += gridDim.x)
-        narrow_row(a, a.block_rows[k], fill, keys, vals, bits, list, s_stage, &s_cnt);
+        narrow_row(a, a.block_rows[k], sm, 13);
+}
+
+constexpr size_t kBlockSmem = (size_t)kBlockSlots * 12 + (size_t)kBlockListCap * (8 + 8 + 4 + 4) + 16;
+
+// narrow rows from the temp buffer to their place in the CSR
+__global__ void __launch_bounds__(kThreads) k_copy_narrow(Args a)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
+    const int64_t n1 = a.ctr[1], n2 = a.ctr[2];
+    for (int64_t k = gw; k < n1 + n2; k += nw) {
+        const int64_t r = k < n1 ? a.warp_rows[k] : a.block_rows[k - n1];
+        const int64_t src = a.toff[r], dst = a.indptr[r], cnt = a.rnnz[r];
+        for (int64_t i = lane; i < cnt; i += 32) {
+            a.indices[dst + i] = a.tcol[src + i];
+            a.data[dst + i] = a.tval[src + i];
+        }
+    }
 }
 
 // ------------------------------------------------------- wide rows
 
-// The wide x wide block: over all groups, for each wide level a in the group
-// (first occurrence) and each cell i, v_i = n_i [i has a] - n_i u_a / N_g
-// added to the wide columns of cell i.  Privatised per CTA when W <= 64.
-__global__ void __launch_bounds__(kThreads) k_wide_block(Args a)
+__global__ void __launch_bounds__(kThreads) k_cell_widx(Args a)
 {
-    __shared__ double s_acc[kWideSmem * kWideSmem];
-    __shared__ uint8_t s_pres[kWideSmem * kWideSmem];
-    const int64_t W = a.W;
-    const bool priv = W <= kWideSmem;
-    if (priv) {
-        for (int i = threadIdx.x; i < W * W; i += kThreads) { s_acc[i] = 0.0; s_pres[i] = 0; }
-        __syncthreads();
+    const int64_t total = a.M * a.D;
+    for (int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x; q < total;
+         q += (int64_t)gridDim.x * kThreads) {
+        const int d = (int)(q % a.D);
+        const uint32_t c = a.codes[q];
+        int32_t k = -1;
+        if ((int64_t)c < a.nlev[d]) {
+            const int32_t kk = a.kind[a.offs[d] + c];
+            k = kk >= 0 ? kk : -1;
+        }
+        a.cell_widx[q] = k;
     }
+}
+
+// The wide x wide block for W <= 16: warp w of the grid takes groups
+// w, w + warps, ... in order; lane owns entries lane + 32 t (a = e / W,
+// b = e % W).  Per group: u of each wide level (lane a), then each present
+// entry adds sum over cells with b of (n [has a] - n u_a / N_g).  Warps are
+// summed in order per CTA into wpart.
+__global__ void __launch_bounds__(kThreads) k_wide_block_warp(Args a)
+{
+    __shared__ double s_n[kThreads / 32][32];
+    __shared__ int32_t s_w[kThreads / 32][32 * HDFE_MAX_DIMS];
+    __shared__ double s_acc[kThreads / 32][kWideWarp * kWideWarp];
+    __shared__ uint8_t s_pr[kThreads / 32][kWideWarp * kWideWarp];
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int W = (int)a.W;
+    const int E = W * W;
+    const int64_t gwarp = (int64_t)blockIdx.x * (kThreads / 32) + wl;
+    const int64_t nwarps = (int64_t)gridDim.x * (kThreads / 32);
+    double acc[kWideEntries];
+    unsigned pres = 0;
+#pragma unroll
+    for (int t = 0; t < kWideEntries; t++) acc[t] = 0.0;
+    for (int64_t g = gwarp; g < a.G; g += nwarps) {
+        const int64_t s = a.starts[g], e = a.starts[g + 1];
+        const double Ng = a.group_n[g];
+        // u of each wide level over the group's cells, lane a owns level a
+        double u = 0.0;
+        for (int64_t base = s; base < e; base += 32) {
+            const int64_t i = base + lane;
+            const int nc = (int)min((int64_t)32, e - base);
+            if (i < e) {
+                s_n[wl][lane] = a.n[i];
+                for (int d = 0; d < a.D; d++) s_w[wl][lane * a.D + d] = a.cell_widx[i * a.D + d];
+            }
+            __syncwarp();
+            if (lane < W)
+                for (int c = 0; c < nc; c++) {
+                    bool has = false;
+                    for (int d = 0; d < a.D; d++) has |= s_w[wl][c * a.D + d] == lane;
+                    if (has) u += s_n[wl][c];
+                }
+            __syncwarp();
+        }
+        // entries
+        for (int64_t base = s; base < e; base += 32) {
+            const int64_t i = base + lane;
+            const int nc = (int)min((int64_t)32, e - base);
+            if (i < e) {
+                s_n[wl][lane] = a.n[i];
+                for (int d = 0; d < a.D; d++) s_w[wl][lane * a.D + d] = a.cell_widx[i * a.D + d];
+            }
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < kWideEntries; t++) {
+                const int en = lane + 32 * t;
+                const int ea = en < E ? en / W : 0, eb = en < E ? en % W : 0;
+                const double ua = __shfl_sync(0xffffffffu, u, ea);
+                const double ub = __shfl_sync(0xffffffffu, u, eb);
+                if (en < E && ua > 0.0 && ub > 0.0) {
+                    const double wa = ua / Ng;
+                    double sum = acc[t];
+                    for (int c = 0; c < nc; c++) {
+                        bool ha = false, hb = false;
+                        for (int d = 0; d < a.D; d++) {
+                            const int32_t k = s_w[wl][c * a.D + d];
+                            ha |= k == ea;
+                            hb |= k == eb;
+                        }
+                        if (hb) {
+                            const double ni = s_n[wl][c];
+                            double v = 0.0;
+                            v -= ni * wa;
+                            if (ha) v += ni;
+                            sum += v;
+                        }
+                    }
+                    acc[t] = sum;
+                    pres |= 1u << t;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    // warps of the CTA summed in order
+#pragma unroll
+    for (int t = 0; t < kWideEntries; t++) {
+        const int en = lane + 32 * t;
+        if (en < E) {
+            s_acc[wl][en] = acc[t];
+            s_pr[wl][en] = (pres >> t) & 1u;
+        }
+    }
+    __syncthreads();
+    for (int en = threadIdx.x; en < E; en += kThreads) {
+        double sum = 0.0;
+        uint8_t p = 0;
+        for (int w = 0; w < kThreads / 32; w++) { sum += s_acc[w][en]; p |= s_pr[w][en]; }
+        a.wpart[(int64_t)blockIdx.x * E + en] = sum;
+        a.wpres[(int64_t)blockIdx.x * E + en] = p;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_wide_block_reduce(Args a)
+{
+    const int64_t E = a.W * a.W;
+    for (int64_t en = (int64_t)blockIdx.x * kThreads + threadIdx.x; en < E;
+         en += (int64_t)gridDim.x * kThreads) {
+        double sum = 0.0;
+        uint8_t p = 0;
+        for (int64_t b = 0; b < a.wide_ctas; b++) {
+            sum += a.wpart[b * E + en];
+            p |= a.wpres[b * E + en];
+        }
+        if (!p) continue;
+        const int64_t wa = en / a.W, wb = en % a.W;
+        const int64_t lb = a.wide_list[wb];
+        a.dval[wa * a.L + lb] = sum;
+        a.dpres[wa * a.L + lb] = 1;
+    }
+}
+
+// the wide x wide block for W > 16: atomics into the dense buffer
+__global__ void __launch_bounds__(kThreads) k_wide_block_atomic(Args a)
+{
     for (int64_t g = (int64_t)blockIdx.x * kThreads + threadIdx.x; g < a.G;
          g += (int64_t)gridDim.x * kThreads) {
         const int64_t s = a.starts[g], e = a.starts[g + 1];
         const double Ng = a.group_n[g];
         for (int da = 0; da < a.D; da++) {
             for (int64_t ia = s; ia < e; ia++) {
-                const uint32_t ca = a.codes[ia * a.D + da];
-                if ((int64_t)ca >= a.nlev[da]) continue;
-                const int32_t wa = a.kind[a.offs[da] + ca];
+                const int32_t wa = a.cell_widx[ia * a.D + da];
                 if (wa < 0) continue;
                 bool first = true;
                 for (int64_t j = s; j < ia; j++)
-                    if (a.codes[j * a.D + da] == ca) { first = false; break; }
+                    if (a.cell_widx[j * a.D + da] == wa) { first = false; break; }
                 if (!first) continue;
                 double u = 0.0;
                 for (int64_t i = s; i < e; i++)
-                    if (a.codes[i * a.D + da] == ca) u += a.n[i];
+                    if (a.cell_widx[i * a.D + da] == wa) u += a.n[i];
                 const double wv = u / Ng;
                 for (int64_t i = s; i < e; i++) {
                     const double ni = a.n[i];
                     double v = 0.0;
                     v -= ni * wv;
-                    if (a.codes[i * a.D + da] == ca) v += ni;
+                    if (a.cell_widx[i * a.D + da] == wa) v += ni;
                     for (int d = 0; d < a.D; d++) {
-                        const uint32_t cb = a.codes[i * a.D + d];
-                        if ((int64_t)cb >= a.nlev[d]) continue;
-                        const int64_t lb = a.offs[d] + cb;
-                        const int32_t wb = a.kind[lb];
+                        const int32_t wb = a.cell_widx[i * a.D + d];
                         if (wb < 0) continue;
-                        if (priv) {
-                            atomicAdd(s_acc + wa * W + wb, v);
-                            s_pres[wa * W + wb] = 1;
-                        } else {
-                            atomicAdd(a.dval + (int64_t)wa * a.L + lb, v);
-                            a.dpres[(int64_t)wa * a.L + lb] = 1;
-                        }
+                        const int64_t lb = a.wide_list[wb];
+                        atomicAdd(a.dval + (int64_t)wa * a.L + lb, v);
+                        a.dpres[(int64_t)wa * a.L + lb] = 1;
                     }
                 }
             }
         }
     }
-    if (!priv) return;
-    __syncthreads();
-    for (int i = threadIdx.x; i < W * W; i += kThreads) {
-        if (!s_pres[i]) continue;
-        const int64_t wa = i / W, wb = i % W;
-        const int64_t lb = a.wide_list[wb];
-        atomicAdd(a.dval + wa * a.L + lb, s_acc[i]);
-        a.dpres[wa * a.L + lb] = 1;
-    }
 }
 
-// nnz of each wide row: its present columns (one CTA per wide row)
+// present columns of each wide row, per segment of kSeg columns
 __global__ void __launch_bounds__(kThreads) k_wide_count(Args a)
 {
     __shared__ double s_red[kThreads / 32];
-    for (int64_t wi = blockIdx.x; wi < a.W; wi += gridDim.x) {
+    const int64_t jobs = a.W * a.nseg;
+    for (int64_t job = blockIdx.x; job < jobs; job += gridDim.x) {
+        const int64_t wi = job / a.nseg, sg = job % a.nseg;
         const uint8_t *p = a.dpres + wi * a.L;
+        const int64_t c0 = sg * kSeg, c1 = min(c0 + kSeg, a.L);
         int64_t c = 0;
-        for (int64_t j = threadIdx.x; j < a.L; j += kThreads) c += p[j];
-        double t = block_sum((double)c, s_red);
-        if (threadIdx.x == 0) a.rnnz[a.wide_list[wi]] = (int64_t)t;
+        for (int64_t j = c0 + threadIdx.x; j < c1; j += kThreads) c += p[j];
+        const double t = block_sum((double)c, s_red);
+        if (threadIdx.x == 0) {
+            a.segcnt[job] = (int64_t)t;
+            atomicAdd(reinterpret_cast<unsigned long long *>(a.rnnz + a.wide_list[wi]),
+                      (unsigned long long)t);
+        }
     }
 }
 
-// write each wide row: compaction of its dense row, in column order
+// each (wide row, segment): compaction of the dense segment, in column order
 __global__ void __launch_bounds__(kThreads) k_wide_fill(Args a)
 {
     __shared__ int s_scr[kThreads / 32 + 1];
-    for (int64_t wi = blockIdx.x; wi < a.W; wi += gridDim.x) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t jobs = a.W * a.nseg;
+    for (int64_t job = blockIdx.x; job < jobs; job += gridDim.x) {
+        const int64_t wi = job / a.nseg, sg = job % a.nseg;
         const int64_t r = a.wide_list[wi];
+        int64_t at = a.indptr[r];
+        for (int64_t s2 = 0; s2 < sg; s2++) at += a.segcnt[wi * a.nseg + s2];
         const uint8_t *p = a.dpres + wi * a.L;
         const double *v = a.dval + wi * a.L;
-        int64_t at = a.indptr[r];
-        for (int64_t base = 0; base < a.L; base += kThreads) {
+        const int64_t c0 = sg * kSeg, c1 = min(c0 + kSeg, a.L);
+        for (int64_t base = c0; base < c1; base += kThreads) {
             const int64_t j = base + threadIdx.x;
-            const int has = (j < a.L) ? p[j] : 0;
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            const int has = (j < c1) ? p[j] : 0;
             const unsigned m = __ballot_sync(0xffffffffu, has);
             if (lane == 0) s_scr[warp] = __popc(m);
             __syncthreads();
@@ -549,14 +737,15 @@ __global__ void k_write_info(Args a, hdfe_sbuild_info *info)
     info->n_block_rows = a.ctr[2];
     info->lgrp_len = a.ctr[3];
     info->nnz = a.ctr[4];
+    info->temp_len = a.ctr[5];
     info->status = (int64_t)*a.status;
 }
 
 // --------------------------------------------------------------- host
 
 struct Layout {
-    int64_t lcount, work, kind, lptr, fillpos, lgrp, rnnz, wide_list, warp_rows, block_rows,
-        tiles, ctr, status, total;
+    int64_t lcount, work, kind, lptr, fillpos, lgrp, rnnz, toff, wide_list, warp_rows,
+        block_rows, tiles, ctr, status, total;
 };
 
 inline Layout layout(int64_t L, int64_t M, int D)
@@ -571,6 +760,7 @@ inline Layout layout(int64_t L, int64_t M, int D)
     o.fillpos = take(L * 4);
     o.lgrp = take(M * (int64_t)D * 4);
     o.rnnz = take((L + 1) * 8);
+    o.toff = take((L + 1) * 8);
     o.wide_list = take(L * 4);
     o.warp_rows = take(L * 4);
     o.block_rows = take(L * 4);
@@ -581,7 +771,27 @@ inline Layout layout(int64_t L, int64_t M, int D)
     return o;
 }
 
-inline int64_t wide_bytes(int64_t W, int64_t L) { return W * L * 9 + 256; }
+struct WideLayout {
+    int64_t dval, dpres, widx, wpart, wpres, segcnt, total;
+};
+
+inline int64_t wide_ctas_for(int sms) { return (int64_t)sms * 2; }
+
+inline WideLayout wide_layout(int64_t W, int64_t L, int64_t M, int D, int64_t ctas)
+{
+    WideLayout o;
+    int64_t p = 0;
+    auto take = [&](int64_t bytes) { int64_t at = p; p += (bytes + 255) / 256 * 256; return at; };
+    const int64_t nseg = (L + kSeg - 1) / kSeg;
+    o.dval = take(W * L * 8);
+    o.dpres = take(W * L);
+    o.widx = take(M * (int64_t)D * 4);
+    o.wpart = take(ctas * W * W * 8);
+    o.wpres = take(ctas * W * W);
+    o.segcnt = take(W * nseg * 8);
+    o.total = p + 256;
+    return o;
+}
 
 struct Ctx {
     Args a;
@@ -590,11 +800,11 @@ struct Ctx {
 };
 
 int setup(Ctx &c, const int64_t *starts, int64_t G, const uint32_t *codes, int32_t D,
-          const double *n, const double *group_n, int64_t M, const int64_t *n_levels, void *ws,
-          int64_t ws_bytes, void *wide_ws, int64_t wide_ws_bytes, int64_t W, void *stream)
+          const double *n, const double *group_n, int64_t M, const int64_t *n_levels,
+          const int32_t *lcount, const int64_t *work, void *ws, int64_t ws_bytes)
 {
     if (D < 1 || D > HDFE_MAX_DIMS || G < 0 || M < 0 || !starts || !codes || !n || !group_n ||
-        !n_levels || !ws)
+        !n_levels || !ws || ((lcount == nullptr) != (work == nullptr)))
         return hdfe_set_arg_error("hdfe_sbuild: bad argument");
     Args &a = c.a;
     a = Args{};
@@ -617,41 +827,60 @@ int setup(Ctx &c, const int64_t *starts, int64_t G, const uint32_t *codes, int32
     Layout lay = layout(L, M, D);
     if (ws_bytes < lay.total) return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_sbuild: workspace too small");
     char *b = (char *)ws;
-    a.lcount = (int32_t *)(b + lay.lcount);
-    a.work = (unsigned long long *)(b + lay.work);
+    a.lcount_ws = (int32_t *)(b + lay.lcount);
+    a.work_ws = (unsigned long long *)(b + lay.work);
+    a.lcount = lcount ? lcount : a.lcount_ws;
+    a.work = work ? reinterpret_cast<const unsigned long long *>(work) : a.work_ws;
     a.kind = (int32_t *)(b + lay.kind);
     a.lptr = (int64_t *)(b + lay.lptr);
     a.fillpos = (int32_t *)(b + lay.fillpos);
     a.lgrp = (int32_t *)(b + lay.lgrp);
     a.rnnz = (int64_t *)(b + lay.rnnz);
+    a.toff = (int64_t *)(b + lay.toff);
     a.wide_list = (int32_t *)(b + lay.wide_list);
     a.warp_rows = (int32_t *)(b + lay.warp_rows);
     a.block_rows = (int32_t *)(b + lay.block_rows);
     a.tiles = (int64_t *)(b + lay.tiles);
     a.ctr = (int64_t *)(b + lay.ctr);
     a.status = (unsigned *)(b + lay.status);
-    a.W = W;
-    if (W >= 0) {
-        if (W > 0 && (!wide_ws || wide_ws_bytes < wide_bytes(W, L)))
-            return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_sbuild: wide workspace too small");
-        a.dval = (double *)wide_ws;
-        a.dpres = (uint8_t *)((char *)wide_ws + W * L * 8);
-    }
-    c.s = (cudaStream_t)stream;
     int dev = 0;
     HDFE_CUDA_TRY(cudaGetDevice(&dev));
     HDFE_CUDA_TRY(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev));
     return HDFE_OK;
 }
 
+int set_wide(Ctx &c, int64_t W, void *wide_ws, int64_t wide_bytes_given)
+{
+    Args &a = c.a;
+    a.W = W;
+    a.nseg = (a.L + kSeg - 1) / kSeg;
+    a.wide_ctas = wide_ctas_for(c.sms);
+    if (W == 0) return HDFE_OK;
+    WideLayout wl = wide_layout(W, a.L, a.M, a.D, a.wide_ctas);
+    if (!wide_ws || wide_bytes_given < wl.total)
+        return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_sbuild: wide workspace too small");
+    char *b = (char *)wide_ws;
+    a.dval = (double *)(b + wl.dval);
+    a.dpres = (uint8_t *)(b + wl.dpres);
+    a.cell_widx = (int32_t *)(b + wl.widx);
+    a.wpart = (double *)(b + wl.wpart);
+    a.wpres = (uint8_t *)(b + wl.wpres);
+    a.segcnt = (int64_t *)(b + wl.segcnt);
+    return HDFE_OK;
+}
+
+int set_temp(Ctx &c, void *temp, int64_t temp_bytes, int64_t temp_len)
+{
+    if (temp_len < 0 || (temp_len > 0 && (!temp || temp_bytes < temp_len * 12)))
+        return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_sbuild: temp buffer too small");
+    c.a.tval = (double *)temp;
+    c.a.tcol = (int32_t *)((char *)temp + temp_len * 8);
+    return HDFE_OK;
+}
+
 int scan_exclusive(Ctx &c, int64_t *x, int64_t n, int64_t *out, int64_t *total)
 {
     const int64_t nt = (n + kScanTile - 1) / kScanTile;
-    if (nt == 0) {
-        HDFE_CUDA_TRY(cudaMemsetAsync(out, 0, 8, c.s));
-        HDFE_CUDA_TRY(cudaMemsetAsync(total, 0, 8, c.s));
-        return HDFE_OK;
-    }
     k_scan_tiles<<<(unsigned)nt, kThreads, 0, c.s>>>(x, n, c.a.tiles);
     k_scan_top<<<1, 1024, 0, c.s>>>(c.a.tiles, nt, total);
     k_scan_apply<<<(unsigned)nt, kThreads, 0, c.s>>>(x, n, c.a.tiles, out, total);
@@ -678,105 +907,137 @@ extern "C" int64_t hdfe_sbuild_workspace_bytes(int64_t L, int64_t n_cells, int32
     return layout(L, n_cells, D).total;
 }
 
-extern "C" int64_t hdfe_sbuild_wide_workspace_bytes(int64_t L, int64_t n_wide)
+extern "C" int64_t hdfe_sbuild_wide_workspace_bytes(int64_t L, int64_t n_cells, int32_t D,
+                                                    int64_t n_wide)
 {
-    if (L < 1 || n_wide < 0) return -1;
-    return wide_bytes(n_wide, L);
+    if (L < 1 || n_cells < 0 || D < 1 || D > HDFE_MAX_DIMS || n_wide < 0) return -1;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return -1;
+    return wide_layout(n_wide, L, n_cells, D, wide_ctas_for(sms)).total;
 }
 
 extern "C" int hdfe_sbuild_analyze(const int64_t *starts, int64_t n_groups,
                                    const uint32_t *codes, int32_t D, const double *n,
                                    const double *group_n, int64_t n_cells,
-                                   const int64_t *n_levels, void *workspace,
+                                   const int64_t *n_levels, const int32_t *lcount,
+                                   const int64_t *work, void *workspace,
                                    int64_t workspace_bytes, hdfe_sbuild_info *info, void *stream)
 {
     Ctx c;
-    int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, workspace,
-                   workspace_bytes, nullptr, 0, -1, stream);
+    c.s = (cudaStream_t)stream;
+    int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                   workspace, workspace_bytes);
     if (st != HDFE_OK) return st;
     Args &a = c.a;
     Layout lay = layout(a.L, n_cells, D);
     char *b = (char *)workspace;
-    HDFE_CUDA_TRY(cudaMemsetAsync(b + lay.lcount, 0, a.L * 4, c.s));
-    HDFE_CUDA_TRY(cudaMemsetAsync(b + lay.work, 0, a.L * 8, c.s));
+    int launched = 0;
+    if (!lcount) {
+        HDFE_CUDA_TRY(cudaMemsetAsync(b + lay.lcount, 0, a.L * 4, c.s));
+        HDFE_CUDA_TRY(cudaMemsetAsync(b + lay.work, 0, a.L * 8, c.s));
+    }
     HDFE_CUDA_TRY(cudaMemsetAsync(b + lay.fillpos, 0, a.L * 4, c.s));
     HDFE_CUDA_TRY(cudaMemsetAsync(b + lay.ctr, 0, 64, c.s));
     HDFE_CUDA_TRY(cudaMemsetAsync(b + lay.status, 0, 8, c.s));
     const int cap = c.sms * 8;
-    k_level_stats<<<grid_for(a.G, kThreads, cap), kThreads, 0, c.s>>>(a);
+    if (!lcount) {
+        k_level_stats<<<grid_for(a.G, kThreads, cap), kThreads, 0, c.s>>>(a);
+        launched++;
+    }
     k_classify<<<grid_for(a.L, kThreads, cap), kThreads, 0, c.s>>>(a);
     k_sort_wide<<<1, 32, 0, c.s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
-    // group lists of the narrow levels
-    st = scan_exclusive(c, a.lptr, a.L, a.lptr, a.ctr + 3);
-    if (st != HDFE_OK) return st;
+    if ((st = scan_exclusive(c, a.lptr, a.L, a.lptr, a.ctr + 3)) != HDFE_OK) return st;
+    if ((st = scan_exclusive(c, a.toff, a.L, a.toff, a.ctr + 5)) != HDFE_OK) return st;
     k_fill_lists<<<grid_for(a.G, kThreads, cap), kThreads, 0, c.s>>>(a);
     k_write_info<<<1, 32, 0, c.s>>>(a, info);
     HDFE_CUDA_TRY(cudaGetLastError());
-    hdfe_add_launches(8);
+    hdfe_add_launches(launched + 11);
     return HDFE_OK;
 }
 
 extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
                                  int32_t D, const double *n, const double *group_n,
-                                 int64_t n_cells, const int64_t *n_levels, int64_t n_wide,
+                                 int64_t n_cells, const int64_t *n_levels, const int32_t *lcount,
+                                 const int64_t *work, int64_t n_wide, int64_t temp_len,
                                  int64_t *indptr, void *workspace, int64_t workspace_bytes,
-                                 void *wide_workspace, int64_t wide_workspace_bytes,
-                                 hdfe_sbuild_info *info, void *stream)
+                                 void *wide_workspace, int64_t wide_workspace_bytes, void *temp,
+                                 int64_t temp_bytes, hdfe_sbuild_info *info, void *stream)
 {
     Ctx c;
-    int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, workspace,
-                   workspace_bytes, wide_workspace, wide_workspace_bytes, n_wide, stream);
+    c.s = (cudaStream_t)stream;
+    int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                   workspace, workspace_bytes);
     if (st != HDFE_OK) return st;
+    if ((st = set_wide(c, n_wide, wide_workspace, wide_workspace_bytes)) != HDFE_OK) return st;
+    if ((st = set_temp(c, temp, temp_bytes, temp_len)) != HDFE_OK) return st;
     if (!indptr) return hdfe_set_arg_error("hdfe_sbuild_count: indptr is null");
     Args &a = c.a;
     a.indptr = indptr;
-    if (n_wide > 0) HDFE_CUDA_TRY(cudaMemsetAsync(wide_workspace, 0, wide_bytes(n_wide, a.L), c.s));
-    HDFE_CUDA_TRY(cudaMemsetAsync(a.rnnz, 0, (a.L + 1) * 8, c.s));
-    const int cap = c.sms * 8;
-    k_warp_rows<<<(unsigned)(c.sms * 4), kWarpsPerCta * 32, 0, c.s>>>(a, false);
-    const size_t bsm = (size_t)kBlockSlots * 12 + kBlockListCap * 4;
-    HDFE_CUDA_TRY(cudaFuncSetAttribute(k_block_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)bsm));
-    k_block_rows<<<(unsigned)(c.sms * 2), 32, bsm, c.s>>>(a, false);
+    int launched = 0;
     if (n_wide > 0) {
-        k_wide_block<<<(unsigned)cap, kThreads, 0, c.s>>>(a);
-        k_wide_count<<<grid_for(n_wide, 1, c.sms * 4), kThreads, 0, c.s>>>(a);
+        WideLayout wl = wide_layout(n_wide, a.L, a.M, a.D, a.wide_ctas);
+        HDFE_CUDA_TRY(cudaMemsetAsync(wide_workspace, 0, wl.dpres + n_wide * a.L, c.s));
+        k_cell_widx<<<grid_for(a.M * a.D, kThreads, c.sms * 8), kThreads, 0, c.s>>>(a);
+        launched++;
+    }
+    HDFE_CUDA_TRY(cudaMemsetAsync(a.rnnz, 0, (a.L + 1) * 8, c.s));
+    k_warp_rows<<<(unsigned)(c.sms * 8), kWarpsPerCta * 32, 0, c.s>>>(a);
+    HDFE_CUDA_TRY(cudaFuncSetAttribute(k_block_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kBlockSmem));
+    k_block_rows<<<(unsigned)(c.sms), 32, kBlockSmem, c.s>>>(a);
+    launched += 2;
+    if (n_wide > 0) {
+        if (n_wide <= kWideWarp) {
+            k_wide_block_warp<<<(unsigned)a.wide_ctas, kThreads, 0, c.s>>>(a);
+            k_wide_block_reduce<<<grid_for(n_wide * n_wide, kThreads, 64), kThreads, 0, c.s>>>(a);
+            launched += 2;
+        } else {
+            k_wide_block_atomic<<<(unsigned)(c.sms * 8), kThreads, 0, c.s>>>(a);
+            launched++;
+        }
+        k_wide_count<<<grid_for(n_wide * a.nseg, 1, c.sms * 8), kThreads, 0, c.s>>>(a);
+        launched++;
     }
     HDFE_CUDA_TRY(cudaGetLastError());
-    st = scan_exclusive(c, a.rnnz, a.L, indptr, a.ctr + 4);
-    if (st != HDFE_OK) return st;
+    if ((st = scan_exclusive(c, a.rnnz, a.L, indptr, a.ctr + 4)) != HDFE_OK) return st;
     k_write_info<<<1, 32, 0, c.s>>>(a, info);
     HDFE_CUDA_TRY(cudaGetLastError());
-    hdfe_add_launches(n_wide > 0 ? 8 : 6);
+    hdfe_add_launches(launched + 4);
     return HDFE_OK;
 }
 
 extern "C" int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
                                 int32_t D, const double *n, const double *group_n,
-                                int64_t n_cells, const int64_t *n_levels, int64_t n_wide,
+                                int64_t n_cells, const int64_t *n_levels, const int32_t *lcount,
+                                const int64_t *work, int64_t n_wide, int64_t temp_len,
                                 const int64_t *indptr, int32_t *indices, double *data,
                                 void *workspace, int64_t workspace_bytes, void *wide_workspace,
-                                int64_t wide_workspace_bytes, hdfe_sbuild_info *info,
-                                void *stream)
+                                int64_t wide_workspace_bytes, void *temp, int64_t temp_bytes,
+                                hdfe_sbuild_info *info, void *stream)
 {
     Ctx c;
-    int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, workspace,
-                   workspace_bytes, wide_workspace, wide_workspace_bytes, n_wide, stream);
+    c.s = (cudaStream_t)stream;
+    int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                   workspace, workspace_bytes);
     if (st != HDFE_OK) return st;
+    if ((st = set_wide(c, n_wide, wide_workspace, wide_workspace_bytes)) != HDFE_OK) return st;
+    if ((st = set_temp(c, temp, temp_bytes, temp_len)) != HDFE_OK) return st;
     if (!indptr || !indices || !data) return hdfe_set_arg_error("hdfe_sbuild_fill: null output");
     Args &a = c.a;
     a.indptr = const_cast<int64_t *>(indptr);
     a.indices = indices;
     a.data = data;
-    k_warp_rows<<<(unsigned)(c.sms * 4), kWarpsPerCta * 32, 0, c.s>>>(a, true);
-    const size_t bsm = (size_t)kBlockSlots * 12 + kBlockListCap * 4;
-    HDFE_CUDA_TRY(cudaFuncSetAttribute(k_block_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)bsm));
-    k_block_rows<<<(unsigned)(c.sms * 2), 32, bsm, c.s>>>(a, true);
-    if (n_wide > 0) k_wide_fill<<<grid_for(n_wide, 1, c.sms * 4), kThreads, 0, c.s>>>(a);
+    k_copy_narrow<<<(unsigned)(c.sms * 8), kThreads, 0, c.s>>>(a);
+    int launched = 1;
+    if (n_wide > 0) {
+        k_wide_fill<<<grid_for(n_wide * a.nseg, 1, c.sms * 8), kThreads, 0, c.s>>>(a);
+        launched++;
+    }
     k_write_info<<<1, 32, 0, c.s>>>(a, info);
     HDFE_CUDA_TRY(cudaGetLastError());
-    hdfe_add_launches(n_wide > 0 ? 4 : 3);
+    hdfe_add_launches(launched + 1);
     return HDFE_OK;
 }

@@ -84,6 +84,8 @@ class DeviceCells:
     n: object               # (M,) f64
     sums: object            # (M, m) f64 or None
     group_n: object         # (G',) f64
+    lcount: object          # (L,) int32 identifying groups per level
+    work: object            # (L,) int64 their cells
     obs: object
     cnt: object
     diag: object
@@ -120,20 +122,23 @@ def pass1(rows: DeviceRows, keep_sums: bool = False, stream=None) -> DeviceCells
     gn = torch.empty(N, **f64)
     obs, cnt, diag = torch.empty(L, **f64), torch.empty(L, **f64), torch.empty(L, **f64)
     rhs = torch.empty((L, m), **f64)
+    lcount = torch.empty(L, dtype=torch.int32, device=dev)
+    work = torch.empty(L, dtype=torch.int64, device=dev)
     counts = torch.zeros(6, dtype=torch.int64, device=dev)
     _lib.check(lib.hdfe_pass1(
         rows.gcode.data_ptr(), rows.codes.data_ptr(), D, rows.V.data_ptr(), m,
         None if rows.w is None else rows.w.data_ptr(), N, nlev.ctypes.data, means.data_ptr(),
         raw_ss.data_ptr(), starts.data_ptr(), ccodes.data_ptr(), cn.data_ptr(),
         None if csums is None else csums.data_ptr(), gn.data_ptr(), obs.data_ptr(),
-        cnt.data_ptr(), diag.data_ptr(), rhs.data_ptr(), counts.data_ptr(), ws.data_ptr(),
-        ws.numel(), _lib.stream_handle(stream)))
+        cnt.data_ptr(), diag.data_ptr(), rhs.data_ptr(), lcount.data_ptr(), work.data_ptr(),
+        counts.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream_handle(stream)))
     c = _lib.read_struct(_lib.Pass1Counts, counts)
     if c.status != _lib.HDFE_OK:
         raise _lib.HDFEError(c.status, "pass 1: a level code is out of range")
     G, M = int(c.n_ident_groups), int(c.n_ident_cells)
     return DeviceCells(starts=starts[:G + 1], codes=ccodes[:M], n=cn[:M],
-                       sums=None if csums is None else csums[:M], group_n=gn[:G], obs=obs,
+                       sums=None if csums is None else csums[:M], group_n=gn[:G],
+                       lcount=lcount, work=work, obs=obs,
                        cnt=cnt, diag=diag, rhs=rhs, means=means, raw_ss=raw_ss,
                        n_levels=list(rows.n_levels),
                        counts={k: int(getattr(c, k)) for k in
@@ -142,7 +147,8 @@ def pass1(rows: DeviceRows, keep_sums: bool = False, stream=None) -> DeviceCells
 
 
 def build_s(cells: DeviceCells, stream=None) -> DeviceCSR:
-    """S in CSR from the identifying cells (three launches, two size reads)."""
+    """S in CSR from the identifying cells: three launches (analyze, count,
+    fill) with two size reads between them."""
     torch = _torch()
     lib = _lib.lib()
     dev = cells.starts.device
@@ -153,27 +159,33 @@ def build_s(cells: DeviceCells, stream=None) -> DeviceCSR:
     nlev = np.asarray(cells.n_levels, dtype=np.int64)
     sh = _lib.stream_handle(stream)
     ws = torch.empty(int(lib.hdfe_sbuild_workspace_bytes(L, M, D)), dtype=torch.uint8, device=dev)
-    info = torch.zeros(7, dtype=torch.int64, device=dev)
+    info = torch.zeros(8, dtype=torch.int64, device=dev)
+    lc = None if cells.lcount is None else cells.lcount.data_ptr()
+    wk = None if cells.work is None else cells.work.data_ptr()
     args = (cells.starts.data_ptr(), G, cells.codes.data_ptr(), D, cells.n.data_ptr(),
-            cells.group_n.data_ptr(), M, nlev.ctypes.data)
+            cells.group_n.data_ptr(), M, nlev.ctypes.data, lc, wk)
     _lib.check(lib.hdfe_sbuild_analyze(*args, ws.data_ptr(), ws.numel(), info.data_ptr(), sh))
     inf = _lib.read_struct(_lib.SbuildInfo, info)
     if inf.status != _lib.HDFE_OK:
         raise _lib.HDFEError(inf.status, "S build: a level code is out of range")
-    W = int(inf.n_wide)
-    wide = torch.empty(max(int(lib.hdfe_sbuild_wide_workspace_bytes(L, W)), 1),
+    W, T = int(inf.n_wide), int(inf.temp_len)
+    wide = torch.empty(max(int(lib.hdfe_sbuild_wide_workspace_bytes(L, M, D, W)), 256),
                        dtype=torch.uint8, device=dev)
+    temp = torch.empty(max(T * 12, 16), dtype=torch.uint8, device=dev)
     indptr = torch.empty(L + 1, dtype=torch.int64, device=dev)
-    _lib.check(lib.hdfe_sbuild_count(*args, W, indptr.data_ptr(), ws.data_ptr(), ws.numel(),
-                                     wide.data_ptr(), wide.numel(), info.data_ptr(), sh))
+    _lib.check(lib.hdfe_sbuild_count(*args, W, T, indptr.data_ptr(), ws.data_ptr(), ws.numel(),
+                                     wide.data_ptr(), wide.numel(), temp.data_ptr(),
+                                     temp.numel(), info.data_ptr(), sh))
     nnz = int(_lib.read_struct(_lib.SbuildInfo, info).nnz)
     indices = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
     data = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
-    _lib.check(lib.hdfe_sbuild_fill(*args, W, indptr.data_ptr(), indices.data_ptr(),
+    _lib.check(lib.hdfe_sbuild_fill(*args, W, T, indptr.data_ptr(), indices.data_ptr(),
                                     data.data_ptr(), ws.data_ptr(), ws.numel(), wide.data_ptr(),
-                                    wide.numel(), info.data_ptr(), sh))
+                                    wide.numel(), temp.data_ptr(), temp.numel(),
+                                    info.data_ptr(), sh))
     S = DeviceCSR(indptr, indices[:nnz], data[:nnz], L, nnz)
-    S.info = {k: int(getattr(inf, k)) for k in ("n_wide", "n_warp_rows", "n_block_rows")}
+    S.info = {k: int(getattr(inf, k)) for k in ("n_wide", "n_warp_rows", "n_block_rows",
+                                                "temp_len")}
     return S
 
 

@@ -68,8 +68,11 @@ int64_t hdfe_kernel_launches(void);
  * starts (N+1) int64, cell_codes (N, D), cell_n (N), cell_sums (N, m) or NULL,
  * group_n (N): each identifying group's sum of n; obs, cnt, diag (L), rhs
  * (L, m), means and raw_ss (m): the variables' means and sums of squared
- * deviations; counts: DEVICE pointer, the actual sizes and a status
- * (HDFE_ERR_BAD_CODE if a code is out of range).
+ * deviations; lcount (L) int32 and work (L) int64, or both NULL: per level the
+ * identifying groups containing it and their cells (what the S build's
+ * analysis needs, `_nb_level_groups` / `_nb_row_work`, collected here while
+ * the cells are at hand); counts: DEVICE pointer, the actual sizes and a
+ * status (HDFE_ERR_BAD_CODE if a code is out of range).
  */
 typedef struct hdfe_pass1_counts {
     int64_t n_rows, n_groups, n_cells, n_ident_groups, n_ident_cells, status;
@@ -81,8 +84,9 @@ int hdfe_pass1(const uint32_t *gcode, const uint32_t *codes, int32_t D, const do
                int32_t m, const double *w, int64_t n_rows, const int64_t *n_levels,
                double *means, double *raw_ss, int64_t *starts, uint32_t *cell_codes,
                double *cell_n, double *cell_sums, double *group_n, double *obs, double *cnt,
-               double *diag, double *rhs, hdfe_pass1_counts *counts, void *workspace,
-               int64_t workspace_bytes, void *stream);
+               double *diag, double *rhs, int32_t *lcount, int64_t *work,
+               hdfe_pass1_counts *counts, void *workspace, int64_t workspace_bytes,
+               void *stream);
 
 /* ------------------------------------------------------------- explicit S
  *
@@ -90,37 +94,46 @@ int hdfe_pass1(const uint32_t *gcode, const uint32_t *codes, int32_t D, const do
  * Replaces core/solve.py:148-194 `_build_explicit` and its kernels
  * core/kernels_base.py:201-358 (`_nb_level_groups`, `_nb_row_work`,
  * `_nb_row_nnz`, `_nb_row_fill`), plain case.  Three calls on one workspace
- * (hdfe_sbuild_workspace_bytes), because the sizes are data-dependent:
- *   analyze  per-level work and classes; info->n_wide = wide rows
- *   count    needs a wide workspace (hdfe_sbuild_wide_workspace_bytes with
- *            n_wide); writes indptr (L+1) and info->nnz
+ * (hdfe_sbuild_workspace_bytes), because the sizes are data-dependent; the
+ * caller reads info (a DEVICE pointer) between them:
+ *   analyze  levels' classes and group lists; info->n_wide (wide rows) and
+ *            info->temp_len (entries of the temp buffer)
+ *   count    needs the wide workspace (hdfe_sbuild_wide_workspace_bytes with
+ *            n_wide) and a temp buffer of temp_len * 12 bytes; writes indptr
+ *            (L+1) and info->nnz
  *   fill     writes indices (nnz) int32 and data (nnz) float64
- * The caller reads info (a DEVICE pointer) between the calls.
+ * lcount / work: pass 1's per-level statistics (hdfe_pass1), or both NULL to
+ * compute them here.  The same workspace, wide workspace and temp buffer go
+ * to all three calls.
  */
 typedef struct hdfe_sbuild_info {
-    int64_t L, nnz, n_wide, n_warp_rows, n_block_rows, lgrp_len, status;
+    int64_t L, nnz, n_wide, n_warp_rows, n_block_rows, lgrp_len, temp_len, status;
 } hdfe_sbuild_info;
 
 int64_t hdfe_sbuild_workspace_bytes(int64_t L, int64_t n_cells, int32_t D);
-int64_t hdfe_sbuild_wide_workspace_bytes(int64_t L, int64_t n_wide);
+int64_t hdfe_sbuild_wide_workspace_bytes(int64_t L, int64_t n_cells, int32_t D, int64_t n_wide);
 
 int hdfe_sbuild_analyze(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
                         int32_t D, const double *n, const double *group_n, int64_t n_cells,
-                        const int64_t *n_levels, void *workspace, int64_t workspace_bytes,
-                        hdfe_sbuild_info *info, void *stream);
+                        const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                        void *workspace, int64_t workspace_bytes, hdfe_sbuild_info *info,
+                        void *stream);
 
 int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
                       int32_t D, const double *n, const double *group_n, int64_t n_cells,
-                      const int64_t *n_levels, int64_t n_wide, int64_t *indptr,
-                      void *workspace, int64_t workspace_bytes, void *wide_workspace,
-                      int64_t wide_workspace_bytes, hdfe_sbuild_info *info, void *stream);
+                      const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                      int64_t n_wide, int64_t temp_len, int64_t *indptr, void *workspace,
+                      int64_t workspace_bytes, void *wide_workspace,
+                      int64_t wide_workspace_bytes, void *temp, int64_t temp_bytes,
+                      hdfe_sbuild_info *info, void *stream);
 
 int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
                      int32_t D, const double *n, const double *group_n, int64_t n_cells,
-                     const int64_t *n_levels, int64_t n_wide, const int64_t *indptr,
-                     int32_t *indices, double *data, void *workspace, int64_t workspace_bytes,
-                     void *wide_workspace, int64_t wide_workspace_bytes,
-                     hdfe_sbuild_info *info, void *stream);
+                     const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                     int64_t n_wide, int64_t temp_len, const int64_t *indptr, int32_t *indices,
+                     double *data, void *workspace, int64_t workspace_bytes,
+                     void *wide_workspace, int64_t wide_workspace_bytes, void *temp,
+                     int64_t temp_bytes, hdfe_sbuild_info *info, void *stream);
 
 /* ------------------------------------------------ components, normalisation
  *

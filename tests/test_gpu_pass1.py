@@ -24,16 +24,16 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)) if a.size else 0.0
 
 
-def three_dim_rows(seed=5):
+def three_dim_rows(seed=5, regions=7):
     """A panel with a third non-streamed dimension (a region of the firm)."""
     from hdfe_stream_b200.simulate import Rows, pass0_layout, simulate_panel
     r = pass0_layout(simulate_panel(3_000, 300, 8, spell=(2, 8), p_move=0.2, seed=seed))
-    region = (r.codes[:, 0] % 7).astype(np.uint32)
+    region = (r.codes[:, 0] % regions).astype(np.uint32)
     codes = np.column_stack([r.codes, region])
     order = np.lexsort((r.V[:, 2], r.V[:, 1], r.V[:, 0], codes[:, 2], codes[:, 1],
                         codes[:, 0], r.gcode))
     return Rows(gcode=r.gcode[order], codes=np.ascontiguousarray(codes[order]),
-                V=r.V[order], w=None, n_levels=r.n_levels + [7], n_groups=r.n_groups,
+                V=r.V[order], w=None, n_levels=r.n_levels + [regions], n_groups=r.n_groups,
                 names=r.names)
 
 
@@ -45,6 +45,8 @@ def panels():
     out.append(("weighted_uneven", pass0_layout(simulate_panel(
         30_000, 1_500, 12, spell=(1, 12), p_move=0.12, weights=True, seed=12))))
     out.append(("three_dims", three_dim_rows()))
+    # more than 16 wide rows: the wide x wide block takes its atomic path
+    out.append(("many_wide", three_dim_rows(seed=6, regions=30)))
     return out
 
 
@@ -92,6 +94,40 @@ def test_sbuild_matches_oracle(device, name, rows):
     zero = dt == 0.0
     if zero.any():
         assert np.max(np.abs(d[zero])) <= 1e-12 * np.max(np.abs(dt))
+
+
+def test_sbuild_without_pass1_statistics(device):
+    """The S build computes the per-level statistics itself when not given."""
+    from hdfe_stream_b200 import fit
+    rows = PANELS[3][1]
+    ip, ix, dt = orc.build_explicit(orc.pass1(rows))
+    cells = fit.pass1(fit.DeviceRows.from_rows(rows))
+    cells.lcount = None
+    cells.work = None
+    S = fit.build_s(cells)
+    assert np.array_equal(S.indptr.cpu().numpy(), ip)
+    assert np.array_equal(S.indices.cpu().numpy(), ix)
+    assert np.max(np.abs(S.data.cpu().numpy() - dt)) <= 1e-12 * np.max(np.abs(dt))
+
+
+def test_pass1_level_statistics(device):
+    """lcount / work: identifying groups per level and their cells
+    (`_nb_level_groups` / `_nb_row_work`)."""
+    from hdfe_stream_b200 import fit
+    rows = PANELS[4][1]
+    c = orc.pass1(rows)
+    cells = fit.pass1(fit.DeviceRows.from_rows(rows))
+    L = c.L
+    lcount = np.zeros(L, np.int64)
+    work = np.zeros(L, np.int64)
+    for g in range(len(c.starts) - 1):
+        s, e = c.starts[g], c.starts[g + 1]
+        for d in range(c.codes.shape[1]):
+            for lv in np.unique(c.codes[s:e, d]):
+                lcount[c.offs[d] + lv] += 1
+                work[c.offs[d] + lv] += e - s
+    assert np.array_equal(cells.lcount.cpu().numpy(), lcount)
+    assert np.array_equal(cells.work.cpu().numpy(), work)
 
 
 def test_sbuild_is_deterministic(device):
