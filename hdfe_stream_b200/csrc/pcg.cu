@@ -118,71 +118,89 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
     double carry[K];
 #pragma unroll
     for (int k = 0; k < K; k++) carry[k] = 0.0;
-
+    // the next chunk's indices and values are loaded one chunk ahead
+    int64_t c_nx = 0;
+    double d_nx = 0.0;
+    if (lo + lane < hi) {
+        c_nx = __ldg(a.indices + lo + lane);
+        d_nx = __ldg(a.data + lo + lane);
+    }
     for (int64_t base = lo; base < hi; base += 32) {
         const int64_t e = base + lane;
         const bool valid = e < hi;
-        // the row of nonzero e: r_cur + #(row ends <= e), over windows of 32 rows
-        int64_t rr = -1;
-        for (int64_t ws = r_cur;; ws += 32) {
-            const int64_t q = ws + 1 + lane;
-            const int64_t Eq = q <= a.L ? __ldg(indptr + q) : INT64_MAX;
-            int pos = 0;
-#pragma unroll
-            for (int step = 16; step >= 1; step >>= 1) {
-                int64_t v = __shfl_sync(kFull, Eq, pos + step - 1);
-                if (v <= e) pos += step;
-            }
-            if (__shfl_sync(kFull, Eq, 31) <= e) pos = 32;
-            if (rr < 0 && pos < 32) rr = ws + pos;
-            if (!__any_sync(kFull, valid && rr < 0)) break;
-        }
-        double v[K];
+        int64_t c = c_nx;
+        const double d = d_nx;
+        double g[K];
         if (valid) {
-            int64_t c = __ldg(a.indices + e);
             if (c < 0 || c >= a.L) {            // not a CSR of this size: record, skip
                 GridBarrier{a.bar}.fail(HDFE_ERR_BAD_CODE);
                 c = 0;
             }
-            const double d = __ldg(a.data + e);
 #pragma unroll
-            for (int k = 0; k < K; k++) v[k] = d * V[c * K + k];
+            for (int k = 0; k < K; k++) g[k] = V[c * K + k];
+        }
+        if (e + 32 < hi) {
+            c_nx = __ldg(a.indices + e + 32);
+            d_nx = __ldg(a.data + e + 32);
+        }
+        // the row of nonzero e, as an offset from r_cur: #(row ends <= e),
+        // row ends taken relative to `base` in windows of 32 rows
+        int rr = -1;
+        for (int64_t ws = r_cur;; ws += 32) {
+            const int64_t q = ws + 1 + lane;
+            const int64_t Eq = q <= a.L ? __ldg(indptr + q) : INT64_MAX;
+            const int Er = (int)min(Eq - base, (int64_t)INT32_MAX);
+            int pos = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int v = __shfl_sync(kFull, Er, pos + step - 1);
+                if (v <= lane) pos += step;
+            }
+            if (__shfl_sync(kFull, Er, 31) <= lane) pos = 32;
+            if (rr < 0 && pos < 32) rr = (int)(ws - r_cur) + pos;
+            if (!__any_sync(kFull, valid && rr < 0)) break;
+        }
+        double v[K];
+        if (valid) {
+#pragma unroll
+            for (int k = 0; k < K; k++) v[k] = d * g[k];
         } else {
-            rr = INT64_MAX;
+            rr = INT32_MAX;
 #pragma unroll
             for (int k = 0; k < K; k++) v[k] = 0.0;
         }
         // segmented inclusive scan over lanes of equal row
 #pragma unroll
         for (int s = 1; s < 32; s <<= 1) {
-            const int64_t ro = __shfl_up_sync(kFull, rr, s);
+            const int ro = __shfl_up_sync(kFull, rr, s);
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 const double o = __shfl_up_sync(kFull, v[k], s);
                 if (lane >= s && ro == rr) v[k] += o;
             }
         }
-        const int64_t rnext = __shfl_down_sync(kFull, rr, 1);
+        const int rnext = __shfl_down_sync(kFull, rr, 1);
         const bool tail = valid && (lane == 31 || rnext != rr);
-        if (tail && rr == row_open) {
+        const int64_t row = r_cur + rr;
+        if (tail && row == row_open) {
 #pragma unroll
             for (int k = 0; k < K; k++) v[k] += carry[k];
         }
         // the last lane's row and sum carry into the next chunk when it goes on
-        const int64_t r31 = __shfl_sync(kFull, rr, 31);
+        const int r31 = __shfl_sync(kFull, rr, 31);
         bool goes_on = false;
         if (tail) {
-            const int64_t rs = __ldg(indptr + rr), re = __ldg(indptr + rr + 1);
+            const int64_t rs = __ldg(indptr + row), re = __ldg(indptr + row + 1);
             const bool ends_here = re == e + 1;
             goes_on = !ends_here && e + 1 < hi;                 // into the next chunk
             if (!goes_on) {
                 if (want_dot) {
 #pragma unroll
-                    for (int k = 0; k < K; k++) dot[k] += V[rr * K + k] * v[k];
+                    for (int k = 0; k < K; k++) dot[k] += V[row * K + k] * v[k];
                 }
                 if (ends_here && rs >= lo) {
 #pragma unroll
-                    for (int k = 0; k < K; k++) out[rr * K + k] = v[k];
+                    for (int k = 0; k < K; k++) out[row * K + k] = v[k];
                 } else {
                     // cut row: slot 1 in the warp where it starts, 0 elsewhere
                     const int slot = rs >= lo ? 1 : 0;
@@ -193,13 +211,13 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
             }
         }
         if (__shfl_sync(kFull, (int)goes_on, 31)) {
-            row_open = r31;
+            row_open = r_cur + r31;
 #pragma unroll
             for (int k = 0; k < K; k++) carry[k] = __shfl_sync(kFull, v[k], 31);
         } else {
             row_open = -1;
         }
-        r_cur = r31 == INT64_MAX ? r_cur : r31;
+        if (r31 != INT32_MAX) r_cur += r31;
     }
 }
 
@@ -239,7 +257,7 @@ __device__ __forceinline__ bool row_is_cut(const int64_t *indptr, int64_t r, int
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads) pcg_kernel(Params a)
+__global__ void __launch_bounds__(kThreads, 3) pcg_kernel(Params a)
 {
     __shared__ double s_red[4 * K];
     __shared__ double s_scratch[kWarps];
@@ -475,7 +493,7 @@ int grid_blocks()
         cudaSuccess)
         return -1;
     if (per_sm < 1) return -1;
-    return sms * (per_sm < 2 ? per_sm : 2);
+    return sms * (per_sm < 3 ? per_sm : 3);
 }
 
 int grid_blocks_for_uncached(int k)

@@ -96,6 +96,7 @@ struct Args {
     int32_t *cell_widx;         // (M, D) wide index of each cell's level, or -1
     double *wpart;              // (CTAs, W*W) per-CTA wide x wide sums
     uint8_t *wpres;             // (CTAs, W*W)
+    double *wcross;             // (W*W) n of cells with two wide levels
     int64_t *segcnt;            // (W, nseg)
     int64_t W, nseg, wide_ctas;
     // temp
@@ -515,86 +516,80 @@ __global__ void __launch_bounds__(kThreads) k_cell_widx(Args a)
     }
 }
 
-// The wide x wide block for W <= 16: warp w of the grid takes groups
-// w, w + warps, ... in order; lane owns entries lane + 32 t (a = e / W,
-// b = e % W).  Per group: u of each wide level (lane a), then each present
-// entry adds sum over cells with b of (n [has a] - n u_a / N_g).  Warps are
-// summed in order per CTA into wpart.
-__global__ void __launch_bounds__(kThreads) k_wide_block_warp(Args a)
+// The wide x wide block for W <= 16.  Per group g the block adds
+//     C_g(a, b) - (u_a / N_g) u_b
+// (the reference's per-cell sum  sum_{i has b} (n_i [i has a] - n_i u_a / N_g)
+// regrouped), with u_a = sum of n over g's cells with wide level a and
+// C_g(a, b) = sum of n over its cells having both (C_g(a, a) = u_a).  Each
+// thread forms its group's u and u / N_g in shared memory; each lane of the
+// warp then owns W^2 / 32 entries and adds the 32 groups' outer products in
+// lane order.  Cells with two wide levels (two small dimensions) add their
+// off-diagonal C into its own array.  Warps and CTAs are summed in a fixed
+// order, so the block is deterministic.
+constexpr int kWideThreads = 128;   // static shared memory stays under 48 KB
+
+__global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
 {
-    __shared__ double s_n[kThreads / 32][32];
-    __shared__ int32_t s_w[kThreads / 32][32 * HDFE_MAX_DIMS];
-    __shared__ double s_acc[kThreads / 32][kWideWarp * kWideWarp];
-    __shared__ uint8_t s_pr[kThreads / 32][kWideWarp * kWideWarp];
+    __shared__ double s_u[kWideThreads][kWideWarp + 1];
+    __shared__ double s_w[kWideThreads][kWideWarp + 1];
+    __shared__ double s_acc[kWideThreads / 32][kWideWarp * kWideWarp];
+    __shared__ uint8_t s_pr[kWideThreads / 32][kWideWarp * kWideWarp];
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const int W = (int)a.W;
     const int E = W * W;
-    const int64_t gwarp = (int64_t)blockIdx.x * (kThreads / 32) + wl;
-    const int64_t nwarps = (int64_t)gridDim.x * (kThreads / 32);
     double acc[kWideEntries];
     unsigned pres = 0;
 #pragma unroll
     for (int t = 0; t < kWideEntries; t++) acc[t] = 0.0;
-    for (int64_t g = gwarp; g < a.G; g += nwarps) {
-        const int64_t s = a.starts[g], e = a.starts[g + 1];
-        const double Ng = a.group_n[g];
-        // u of each wide level over the group's cells, lane a owns level a
-        double u = 0.0;
-        for (int64_t base = s; base < e; base += 32) {
-            const int64_t i = base + lane;
-            const int nc = (int)min((int64_t)32, e - base);
-            if (i < e) {
-                s_n[wl][lane] = a.n[i];
-                for (int d = 0; d < a.D; d++) s_w[wl][lane * a.D + d] = a.cell_widx[i * a.D + d];
-            }
-            __syncwarp();
-            if (lane < W)
-                for (int c = 0; c < nc; c++) {
-                    bool has = false;
-                    for (int d = 0; d < a.D; d++) has |= s_w[wl][c * a.D + d] == lane;
-                    if (has) u += s_n[wl][c];
+    double *u = s_u[threadIdx.x];
+    double *wv = s_w[threadIdx.x];
+    const int64_t stride = (int64_t)gridDim.x * kWideThreads;
+    for (int64_t base = (int64_t)blockIdx.x * kWideThreads; base < a.G; base += stride) {
+        const int64_t g = base + threadIdx.x;
+        for (int k = 0; k < W; k++) u[k] = 0.0;
+        if (g < a.G) {
+            const int64_t s = a.starts[g], e = a.starts[g + 1];
+            for (int64_t i = s; i < e; i++) {
+                const double ni = a.n[i];
+                int nw = 0, k0 = -1;
+                for (int d = 0; d < a.D; d++) {
+                    const int32_t k = a.cell_widx[i * a.D + d];
+                    if (k < 0) continue;
+                    u[k] += ni;
+                    if (nw++ == 0) k0 = k;
+                    else {
+                        // a cell with two wide levels: C(k0, k) and C(k, k0)
+                        atomicAdd(a.wcross + (int64_t)k0 * W + k, ni);
+                        atomicAdd(a.wcross + (int64_t)k * W + k0, ni);
+                    }
                 }
-            __syncwarp();
-        }
-        // entries
-        for (int64_t base = s; base < e; base += 32) {
-            const int64_t i = base + lane;
-            const int nc = (int)min((int64_t)32, e - base);
-            if (i < e) {
-                s_n[wl][lane] = a.n[i];
-                for (int d = 0; d < a.D; d++) s_w[wl][lane * a.D + d] = a.cell_widx[i * a.D + d];
             }
-            __syncwarp();
+            const double Ng = a.group_n[g];
+            for (int k = 0; k < W; k++) wv[k] = u[k] / Ng;
+        } else {
+            for (int k = 0; k < W; k++) wv[k] = 0.0;
+        }
+        __syncwarp();
+        // the warp's 32 groups, in lane order, into the lane-owned entries
+        const int src0 = wl * 32;
+        for (int q = 0; q < 32; q++) {
+            const double *us = s_u[src0 + q];
+            const double *ws = s_w[src0 + q];
 #pragma unroll
             for (int t = 0; t < kWideEntries; t++) {
                 const int en = lane + 32 * t;
-                const int ea = en < E ? en / W : 0, eb = en < E ? en % W : 0;
-                const double ua = __shfl_sync(0xffffffffu, u, ea);
-                const double ub = __shfl_sync(0xffffffffu, u, eb);
-                if (en < E && ua > 0.0 && ub > 0.0) {
-                    const double wa = ua / Ng;
-                    double sum = acc[t];
-                    for (int c = 0; c < nc; c++) {
-                        bool ha = false, hb = false;
-                        for (int d = 0; d < a.D; d++) {
-                            const int32_t k = s_w[wl][c * a.D + d];
-                            ha |= k == ea;
-                            hb |= k == eb;
-                        }
-                        if (hb) {
-                            const double ni = s_n[wl][c];
-                            double v = 0.0;
-                            v -= ni * wa;
-                            if (ha) v += ni;
-                            sum += v;
-                        }
+                if (en < E) {
+                    const int ea = en / W, eb = en % W;
+                    const double ua = us[ea], ub = us[eb];
+                    if (ua > 0.0 && ub > 0.0) {
+                        double c = ea == eb ? ua : 0.0;
+                        acc[t] += c - ws[ea] * ub;
+                        pres |= 1u << t;
                     }
-                    acc[t] = sum;
-                    pres |= 1u << t;
                 }
             }
-            __syncwarp();
         }
+        __syncwarp();
     }
     // warps of the CTA summed in order
 #pragma unroll
@@ -606,10 +601,10 @@ __global__ void __launch_bounds__(kThreads) k_wide_block_warp(Args a)
         }
     }
     __syncthreads();
-    for (int en = threadIdx.x; en < E; en += kThreads) {
+    for (int en = threadIdx.x; en < E; en += kWideThreads) {
         double sum = 0.0;
         uint8_t p = 0;
-        for (int w = 0; w < kThreads / 32; w++) { sum += s_acc[w][en]; p |= s_pr[w][en]; }
+        for (int w = 0; w < kWideThreads / 32; w++) { sum += s_acc[w][en]; p |= s_pr[w][en]; }
         a.wpart[(int64_t)blockIdx.x * E + en] = sum;
         a.wpres[(int64_t)blockIdx.x * E + en] = p;
     }
@@ -629,7 +624,7 @@ __global__ void __launch_bounds__(kThreads) k_wide_block_reduce(Args a)
         if (!p) continue;
         const int64_t wa = en / a.W, wb = en % a.W;
         const int64_t lb = a.wide_list[wb];
-        a.dval[wa * a.L + lb] = sum;
+        a.dval[wa * a.L + lb] = sum + a.wcross[en];
         a.dpres[wa * a.L + lb] = 1;
     }
 }
@@ -772,10 +767,10 @@ inline Layout layout(int64_t L, int64_t M, int D)
 }
 
 struct WideLayout {
-    int64_t dval, dpres, widx, wpart, wpres, segcnt, total;
+    int64_t dval, dpres, widx, wpart, wpres, wcross, segcnt, total;
 };
 
-inline int64_t wide_ctas_for(int sms) { return (int64_t)sms * 2; }
+inline int64_t wide_ctas_for(int sms) { return (int64_t)sms * 4; }
 
 inline WideLayout wide_layout(int64_t W, int64_t L, int64_t M, int D, int64_t ctas)
 {
@@ -788,6 +783,7 @@ inline WideLayout wide_layout(int64_t W, int64_t L, int64_t M, int D, int64_t ct
     o.widx = take(M * (int64_t)D * 4);
     o.wpart = take(ctas * W * W * 8);
     o.wpres = take(ctas * W * W);
+    o.wcross = take(W * W * 8);
     o.segcnt = take(W * nseg * 8);
     o.total = p + 256;
     return o;
@@ -865,6 +861,7 @@ int set_wide(Ctx &c, int64_t W, void *wide_ws, int64_t wide_bytes_given)
     a.cell_widx = (int32_t *)(b + wl.widx);
     a.wpart = (double *)(b + wl.wpart);
     a.wpres = (uint8_t *)(b + wl.wpres);
+    a.wcross = (double *)(b + wl.wcross);
     a.segcnt = (int64_t *)(b + wl.segcnt);
     return HDFE_OK;
 }
@@ -980,6 +977,8 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
     if (n_wide > 0) {
         WideLayout wl = wide_layout(n_wide, a.L, a.M, a.D, a.wide_ctas);
         HDFE_CUDA_TRY(cudaMemsetAsync(wide_workspace, 0, wl.dpres + n_wide * a.L, c.s));
+        HDFE_CUDA_TRY(cudaMemsetAsync((char *)wide_workspace + wl.wcross, 0,
+                                      n_wide * n_wide * 8, c.s));
         k_cell_widx<<<grid_for(a.M * a.D, kThreads, c.sms * 8), kThreads, 0, c.s>>>(a);
         launched++;
     }
@@ -991,7 +990,7 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
     launched += 2;
     if (n_wide > 0) {
         if (n_wide <= kWideWarp) {
-            k_wide_block_warp<<<(unsigned)a.wide_ctas, kThreads, 0, c.s>>>(a);
+            k_wide_block_warp<<<(unsigned)a.wide_ctas, kWideThreads, 0, c.s>>>(a);
             k_wide_block_reduce<<<grid_for(n_wide * n_wide, kThreads, 64), kThreads, 0, c.s>>>(a);
             launched += 2;
         } else {
