@@ -289,14 +289,17 @@ struct GroupArgs {
 };
 
 // One group: cells from its rows, level scatter, identifying-cell output.
-template <int D>
+// MV > 0 fixes the number of variables at compile time (registers, unrolled
+// loops); MV == 0 takes it from the arguments.
+template <int D, int MV>
 __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, int64_t co,
                          double *s_acc, double *sums_buf)
 {
     const Dims &dm = a.dims;
-    const int m = dm.m;
+    const int m = MV > 0 ? MV : dm.m;
+    constexpr int kV = MV > 0 ? MV : kMaxVars;
     const int64_t r0 = a.grow[g], r1 = a.grow[g + 1];
-    double Ng = 0.0, vsum[kMaxVars];
+    double Ng = 0.0, vsum[kV];
     for (int j = 0; j < m; j++) vsum[j] = 0.0;
     int64_t q = co;     // next identifying cell slot
     // the cells are runs of rows with equal codes
@@ -306,7 +309,8 @@ __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, i
         load_codes<D>(a.codes, i, c);
         int64_t j = i + 1;
         double n = a.w ? a.w[i] : 1.0;
-        double s[kMaxVars];
+        double s[kV];
+#pragma unroll
         for (int v = 0; v < m; v++) s[v] = a.w ? a.w[i] * (a.V[(int64_t)v * a.N + i] - a.means[v])
                                               : (a.V[(int64_t)v * a.N + i] - a.means[v]);
         while (j < r1) {
@@ -357,7 +361,7 @@ __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, i
     if (!keep) return;
     a.starts[gi] = co;
     a.group_n[gi] = Ng;
-    double vbar[kMaxVars];
+    double vbar[kV];
     for (int v = 0; v < m; v++) vbar[v] = vsum[v] / Ng;
     // rhs and the diagonal's n over the identifying cells (_nb_rhs, _nb_diag)
     for (int64_t k = co; k < q; k++) {
@@ -404,7 +408,7 @@ __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, i
     }
 }
 
-template <int D>
+template <int D, int MV>
 __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sums_scratch)
 {
     extern __shared__ double s_acc[];
@@ -429,7 +433,7 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
             int tg, tc;
             const int eg = block_exclusive(keep ? 1 : 0, s_scr[0], tg);
             const int ec = block_exclusive(keep ? (int)nc : 0, s_scr[1], tc);
-            if (g < t1) do_group<D>(a, g, keep, gi_run + eg, co_run + ec, s_acc, sums_buf);
+            if (g < t1) do_group<D, MV>(a, g, keep, gi_run + eg, co_run + ec, s_acc, sums_buf);
             gi_run += tg;
             co_run += tc;
         }
@@ -590,11 +594,13 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     HDFE_CUDA_TRY(cudaGetDevice(&dev));
     HDFE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const size_t smem = (size_t)(slots * per_level);
-    HDFE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, groups_work<D>, kThreads,
-                                                               smem));
+    void (*kern)(GroupArgs, double *) = m == 1 ? groups_work<D, 1> : m == 2 ? groups_work<D, 2>
+                                       : m == 3 ? groups_work<D, 3> : m == 4 ? groups_work<D, 4>
+                                       : groups_work<D, 0>;
+    HDFE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
     int64_t blocks = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
     if (blocks > gtiles) blocks = gtiles > 0 ? gtiles : 1;
-    groups_work<D><<<(unsigned)blocks, kThreads, smem, s>>>(ga, sums_scratch);
+    kern<<<(unsigned)blocks, kThreads, smem, s>>>(ga, sums_scratch);
     HDFE_CUDA_TRY(cudaGetLastError());
     write_counts<<<1, 32, 0, s>>>(totals, totals + 2, N, counts, status);
     HDFE_CUDA_TRY(cudaGetLastError());

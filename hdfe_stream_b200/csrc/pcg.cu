@@ -114,6 +114,7 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
     if (lo >= hi) return;
     const int64_t *__restrict__ indptr = a.indptr;
     int64_t r_cur = upper_bound(indptr, a.L + 1, lo) - 1;    // row of nonzero `lo`
+    int64_t rcur_start = __ldg(indptr + r_cur);              // its first nonzero
     int64_t row_open = -1;                                   // row continued from the last chunk
     double carry[K];
 #pragma unroll
@@ -146,9 +147,13 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
         // the row of nonzero e, as an offset from r_cur: #(row ends <= e),
         // row ends taken relative to `base` in windows of 32 rows
         int rr = -1;
+        int64_t Eq_last = 0;
+        int nwin = 0;
         for (int64_t ws = r_cur;; ws += 32) {
             const int64_t q = ws + 1 + lane;
             const int64_t Eq = q <= a.L ? __ldg(indptr + q) : INT64_MAX;
+            Eq_last = Eq;
+            nwin++;
             const int Er = (int)min(Eq - base, (int64_t)INT32_MAX);
             int pos = 0;
 #pragma unroll
@@ -182,6 +187,12 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
         const int rnext = __shfl_down_sync(kFull, rr, 1);
         const bool tail = valid && (lane == 31 || rnext != rr);
         const int64_t row = r_cur + rr;
+        // with one window (the usual case) lane q holds the end of row r_cur + q,
+        // so a row's bounds come from shuffles instead of loads
+        const bool single = nwin == 1;
+        const int64_t re_w = __shfl_sync(kFull, Eq_last, min(max(rr, 0), 31));
+        int64_t rs_w = __shfl_sync(kFull, Eq_last, min(max(rr - 1, 0), 31));
+        if (rr == 0) rs_w = rcur_start;
         if (tail && row == row_open) {
 #pragma unroll
             for (int k = 0; k < K; k++) v[k] += carry[k];
@@ -190,7 +201,8 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
         const int r31 = __shfl_sync(kFull, rr, 31);
         bool goes_on = false;
         if (tail) {
-            const int64_t rs = __ldg(indptr + row), re = __ldg(indptr + row + 1);
+            const int64_t rs = single ? rs_w : __ldg(indptr + row);
+            const int64_t re = single ? re_w : __ldg(indptr + row + 1);
             const bool ends_here = re == e + 1;
             goes_on = !ends_here && e + 1 < hi;                 // into the next chunk
             if (!goes_on) {
@@ -217,7 +229,11 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
         } else {
             row_open = -1;
         }
-        if (r31 != INT32_MAX) r_cur += r31;
+        if (r31 != INT32_MAX) {
+            const int64_t next_start = __shfl_sync(kFull, Eq_last, min(max(r31 - 1, 0), 31));
+            if (r31 > 0) rcur_start = single ? next_start : __ldg(indptr + r_cur + r31);
+            r_cur += r31;
+        }
     }
 }
 
@@ -257,7 +273,7 @@ __device__ __forceinline__ bool row_is_cut(const int64_t *indptr, int64_t r, int
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads, 3) pcg_kernel(Params a)
+__global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
 {
     __shared__ double s_red[4 * K];
     __shared__ double s_scratch[kWarps];
@@ -493,7 +509,7 @@ int grid_blocks()
         cudaSuccess)
         return -1;
     if (per_sm < 1) return -1;
-    return sms * (per_sm < 3 ? per_sm : 3);
+    return sms * (per_sm < 4 ? per_sm : 4);
 }
 
 int grid_blocks_for_uncached(int k)

@@ -308,6 +308,49 @@ __device__ void warp_bitonic(int32_t *key, double *val, int n, int lane)
     }
 }
 
+// Sort n <= 128 distinct int32 keys (with an optional double payload) in
+// warp-shared memory by rank: each key's position is the number of keys
+// below it.  Keys are distinct (columns of a row, groups of a list).
+__device__ void warp_rank_sort(int32_t *key, double *val, int n, int lane)
+{
+    int32_t k[4];
+    double v[4];
+    int rank[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const int i = lane + 32 * t;
+        k[t] = i < n ? key[i] : INT32_MAX;
+        v[t] = (val && i < n) ? val[i] : 0.0;
+        rank[t] = 0;
+    }
+    const int chunks = (n + 31) >> 5;
+    for (int c = 0; c < chunks; c++) {
+        // chunk c's keys, one per lane (selected without indexing the array)
+        const int32_t kc = c == 0 ? k[0] : c == 1 ? k[1] : c == 2 ? k[2] : k[3];
+        for (int j = 0; j < 32; j++) {
+            const int32_t other = __shfl_sync(0xffffffffu, kc, j);
+#pragma unroll
+            for (int t = 0; t < 4; t++) rank[t] += other < k[t];
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const int i = lane + 32 * t;
+        if (i < n) {
+            key[rank[t]] = k[t];
+            if (val) val[rank[t]] = v[t];
+        }
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void warp_sort(int32_t *key, double *val, int n, int lane)
+{
+    if (n <= 128) warp_rank_sort(key, val, n, lane);
+    else warp_bitonic(key, val, n, lane);
+}
+
 struct RowSmem {
     int32_t *keys;
     double *vals;
@@ -336,7 +379,7 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
     for (int i = lane; i < nl; i += 32) sm.list[i] = a.lgrp[l0 + i];
     if (lane == 0) *sm.cnt = 0;
     __syncwarp();
-    warp_bitonic(sm.list, nullptr, nl, lane);
+    warp_sort(sm.list, nullptr, nl, lane);
     // per group: first cell, cell count, u_r / N_g (one lane per group)
     for (int k = lane; k < nl; k += 32) {
         const int64_t g = sm.list[k];
@@ -427,7 +470,7 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
         if (lane == 0) *sm.cnt = at0 + __popc(m);
         __syncwarp();
     }
-    warp_bitonic(sm.keys, sm.vals, cnt, lane);
+    warp_sort(sm.keys, sm.vals, cnt, lane);
     const int64_t t0 = a.toff[r];
     for (int i = lane; i < cnt; i += 32) {
         const int32_t c = sm.keys[i];
@@ -538,9 +581,16 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
     const int W = (int)a.W;
     const int E = W * W;
     double acc[kWideEntries];
-    unsigned pres = 0;
+    int ea[kWideEntries], eb[kWideEntries];
+    unsigned pres = 0, owned = 0;
 #pragma unroll
-    for (int t = 0; t < kWideEntries; t++) acc[t] = 0.0;
+    for (int t = 0; t < kWideEntries; t++) {
+        acc[t] = 0.0;
+        const int en = lane + 32 * t;
+        ea[t] = en < E ? en / W : 0;
+        eb[t] = en < E ? en % W : 0;
+        if (en < E) owned |= 1u << t;
+    }
     double *u = s_u[threadIdx.x];
     double *wv = s_w[threadIdx.x];
     const int64_t stride = (int64_t)gridDim.x * kWideThreads;
@@ -577,15 +627,11 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
             const double *ws = s_w[src0 + q];
 #pragma unroll
             for (int t = 0; t < kWideEntries; t++) {
-                const int en = lane + 32 * t;
-                if (en < E) {
-                    const int ea = en / W, eb = en % W;
-                    const double ua = us[ea], ub = us[eb];
-                    if (ua > 0.0 && ub > 0.0) {
-                        double c = ea == eb ? ua : 0.0;
-                        acc[t] += c - ws[ea] * ub;
-                        pres |= 1u << t;
-                    }
+                const double ua = us[ea[t]], ub = us[eb[t]];
+                if (((owned >> t) & 1u) && ua > 0.0 && ub > 0.0) {
+                    const double c = ea[t] == eb[t] ? ua : 0.0;
+                    acc[t] += c - ws[ea[t]] * ub;
+                    pres |= 1u << t;
                 }
             }
         }
