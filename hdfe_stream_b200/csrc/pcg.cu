@@ -13,13 +13,15 @@
 // Phases per iteration (3 grid barriers):
 //   A  AP = S P.  The nonzeros are split evenly over all warps of the grid
 //      (chunk = ceil(nnz / warps)), so a row of 500k nonzeros (a year level)
-//      and rows of 10 (firm levels) cost the same per nonzero.  A warp walks
-//      its range 32 nonzeros at a time with coalesced index/value loads,
-//      finds each lane's row by a shuffle binary search over the row ends,
-//      and reduces by row with a segmented shuffle scan.  Rows inside the
-//      warp's range are written to AP; a row cut by a range boundary leaves a
-//      partial sum in the warp's two carry slots.  p'Ap accumulates per warp
-//      (linear in the partials, so cut rows need no fix-up for it).
+//      and rows of 30 (firm levels) cost the same per nonzero.  A warp walks
+//      the rows of its range 32 at a time: a row with at least kLong nonzeros
+//      in the range takes the whole warp, shorter rows go four at a time to
+//      8-lane subgroups; each lane accumulates in registers and the group
+//      reduces once per row.  The vector is gathered as 16-byte pairs (P's
+//      rows are padded to an even width).  Rows inside the range are written
+//      to AP; a row cut by a range boundary leaves a partial sum in the
+//      warp's two carry slots.  p'Ap accumulates per row (linear in the
+//      partials, so cut rows need no fix-up for it).
 //   B  alpha from the reduced p'Ap.  Per row: X += alpha P, R -= alpha AP and
 //      the partial sums of R^2 and R^2 dinv.  A row cut across warps is
 //      finished by the warp holding its last nonzero, which sums the carry
@@ -39,6 +41,13 @@ namespace pcg {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kLong = 64;           // nonzeros in a warp's range that make a row "long"
+
+// P's row stride: even, so a row's pairs of values are 16-byte aligned
+template <int K>
+struct Stride {
+    static constexpr int P = K == 1 ? 1 : ((K + 1) / 2) * 2;
+};
 
 struct Params {
     const int64_t *indptr;
@@ -54,28 +63,33 @@ struct Params {
     double *X, *R, *P, *AP;
     double *carry;      // (total warps, 2, K)
     double *part;       // (quantities, gridDim.x)
+    int64_t *wfirst;    // (total warps) row of each warp's first nonzero
+    uint8_t *cut;       // (L) row spans two or more warps
     unsigned *bar;
     hdfe_pcg_info *info;
 };
 
-// Workspace layout, in doubles: R, P, AP (L*K each), carry (warps*2*K),
-// part (4*K*blocks), then the barrier words.
+// Workspace layout in bytes: R (L*K), P (L*KP), AP (L*K), carry, part,
+// wfirst, cut flags, then the barrier words.
 struct Layout {
-    int64_t r, p, ap, carry, part, bar_bytes_off, total_bytes;
+    int64_t r, p, ap, carry, part, wfirst, cut, bar, total;
 };
 
-__host__ __device__ inline Layout layout(int64_t L, int k, int64_t blocks)
+inline Layout layout(int64_t L, int k, int64_t blocks)
 {
     Layout o;
-    int64_t lk = L * k;
-    o.r = 0;
-    o.p = lk;
-    o.ap = 2 * lk;
-    o.carry = 3 * lk;
-    o.part = o.carry + blocks * kWarps * 2 * k;
-    int64_t doubles = o.part + 4 * (int64_t)k * blocks;
-    o.bar_bytes_off = ((doubles * 8 + 255) / 256) * 256;
-    o.total_bytes = o.bar_bytes_off + 256;
+    const int kp = k == 1 ? 1 : ((k + 1) / 2) * 2;
+    int64_t p = 0;
+    auto take = [&](int64_t bytes) { int64_t at = p; p += (bytes + 255) / 256 * 256; return at; };
+    o.r = take(L * k * 8);
+    o.p = take(L * kp * 8);
+    o.ap = take(L * k * 8);
+    o.carry = take(blocks * kWarps * 2 * k * 8);
+    o.part = take(4 * (int64_t)k * blocks * 8);
+    o.wfirst = take(blocks * kWarps * 8);
+    o.cut = take(L);
+    o.bar = take(64);
+    o.total = p;
     return o;
 }
 
@@ -100,140 +114,149 @@ __device__ __forceinline__ double reduce_part(const double *part, int q)
     return warp_sum(s);
 }
 
-// AP-type product of the nonzeros in this warp's range: out = S * V for
-// rows inside the range, partial sums of cut rows to the carry slots, and
-// dot[k] += V[r] . (S V)[r] over the range when want_dot.
-template <int K>
+// Row c of V (stride VS) into g[0..K): pairs of doubles when the rows are
+// 16-byte aligned (VS even, V 16-byte aligned), scalars otherwise.  Plain
+// loads: V may be written by this kernel between grid barriers.
+template <int K, int VS, bool PAIRS>
+__device__ __forceinline__ void gather(const double *V, int64_t c, double (&g)[K])
+{
+    const double *p = V + c * VS;
+    if constexpr (PAIRS) {
+#pragma unroll
+        for (int k = 0; k < K; k += 2) {
+            const double2 t = *reinterpret_cast<const double2 *>(p + k);
+            g[k] = t.x;
+            if (k + 1 < K) g[k + 1] = t.y;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; k++) g[k] = p[k];
+    }
+}
+
+// acc += sum over e = e0, e0 + STEP, ... < re of data[e] * V[indices[e]]:
+// U nonzeros per lane per round, their index/value loads and then their
+// gathers all issued before the multiply-adds, so U round trips overlap.
+template <int K, int VS, bool PAIRS, int STEP>
+__device__ __forceinline__ void row_products(const Params &a, const double *V, int64_t e0,
+                                             int64_t re, double (&acc)[K])
+{
+    constexpr int U = K <= 4 ? 4 : 2;
+    for (; e0 < re; e0 += STEP * U) {
+        int64_t c[U];
+        double d[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t e = e0 + STEP * u;
+            c[u] = 0;
+            d[u] = 0.0;
+            if (e < re) {
+                c[u] = __ldg(a.indices + e);
+                d[u] = __ldg(a.data + e);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (c[u] < 0 || c[u] >= a.L) { GridBarrier{a.bar}.fail(HDFE_ERR_BAD_CODE); c[u] = 0; }
+        double g[U][K];
+#pragma unroll
+        for (int u = 0; u < U; u++) gather<K, VS, PAIRS>(V, c[u], g[u]);
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int k = 0; k < K; k++) acc[k] += d[u] * g[u][k];
+    }
+}
+
+template <int K, int VS>
+__device__ __forceinline__ void finish_row(const Params &a, int64_t row, const double (&acc)[K],
+                                           int64_t row_st, int64_t row_en, int64_t lo,
+                                           int64_t hi, int64_t gw, const double *V,
+                                           double *out, double (&dot)[K], bool want_dot)
+{
+    if (want_dot) {
+#pragma unroll
+        for (int k = 0; k < K; k++) dot[k] += V[row * VS + k] * acc[k];
+    }
+    if (row_st >= lo && row_en <= hi) {
+#pragma unroll
+        for (int k = 0; k < K; k++) out[row * K + k] = acc[k];
+    } else {
+        // cut row: slot 1 in the warp where it starts, 0 elsewhere
+        double *cs = a.carry + (gw * 2 + (row_st >= lo ? 1 : 0)) * K;
+#pragma unroll
+        for (int k = 0; k < K; k++) cs[k] = acc[k];
+    }
+}
+
+// out = S V over this warp's range of nonzeros (rows inside the range),
+// partial sums of cut rows to the carry slots, dot[k] += V[r] . (S V)[r].
+template <int K, int VS, bool PAIRS>
 __device__ void spmm_range(const Params &a, const double *__restrict__ V, double *__restrict__ out,
                            double (&dot)[K], bool want_dot)
 {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, sub = lane >> 3, sl = lane & 7;
     const int64_t gw = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
     const int64_t lo = gw * a.chunk;
     const int64_t hi = min(lo + a.chunk, a.nnz);
     if (lo >= hi) return;
-    const int64_t *__restrict__ indptr = a.indptr;
-    int64_t r_cur = upper_bound(indptr, a.L + 1, lo) - 1;    // row of nonzero `lo`
-    int64_t rcur_start = __ldg(indptr + r_cur);              // its first nonzero
-    int64_t row_open = -1;                                   // row continued from the last chunk
-    double carry[K];
+    int64_t r0 = a.wfirst[gw];
+    for (;;) {
+        // bounds of rows r0 .. r0+31 (lane j: row r0+j)
+        const int64_t q = r0 + lane;
+        const int64_t st = q < a.L ? __ldg(a.indptr + q) : INT64_MAX;
+        const int64_t en = q < a.L ? __ldg(a.indptr + q + 1) : INT64_MAX;
+        const bool inr = st < hi;
+        const unsigned inmask = __ballot_sync(kFull, inr);
+        const int nrows = __popc(inmask);           // a prefix of the lanes: starts increase
+        if (nrows == 0) break;
+        const int64_t cs = max(st, lo), ce = min(en, hi);
+        const int len = inr ? (int)(ce - cs) : 0;
+        const unsigned longmask = __ballot_sync(kFull, inr && len >= kLong);
+        int j = 0;
+        while (j < nrows) {
+            if ((longmask >> j) & 1u) {
+                // one long row, the whole warp
+                const int64_t rs = __shfl_sync(kFull, cs, j), re = __shfl_sync(kFull, ce, j);
+                double acc[K];
 #pragma unroll
-    for (int k = 0; k < K; k++) carry[k] = 0.0;
-    // the next chunk's indices and values are loaded one chunk ahead
-    int64_t c_nx = 0;
-    double d_nx = 0.0;
-    if (lo + lane < hi) {
-        c_nx = __ldg(a.indices + lo + lane);
-        d_nx = __ldg(a.data + lo + lane);
-    }
-    for (int64_t base = lo; base < hi; base += 32) {
-        const int64_t e = base + lane;
-        const bool valid = e < hi;
-        int64_t c = c_nx;
-        const double d = d_nx;
-        double g[K];
-        if (valid) {
-            if (c < 0 || c >= a.L) {            // not a CSR of this size: record, skip
-                GridBarrier{a.bar}.fail(HDFE_ERR_BAD_CODE);
-                c = 0;
-            }
+                for (int k = 0; k < K; k++) acc[k] = 0.0;
+                row_products<K, VS, PAIRS, 32>(a, V, rs + lane, re, acc);
 #pragma unroll
-            for (int k = 0; k < K; k++) g[k] = V[c * K + k];
-        }
-        if (e + 32 < hi) {
-            c_nx = __ldg(a.indices + e + 32);
-            d_nx = __ldg(a.data + e + 32);
-        }
-        // the row of nonzero e, as an offset from r_cur: #(row ends <= e),
-        // row ends taken relative to `base` in windows of 32 rows
-        int rr = -1;
-        int64_t Eq_last = 0;
-        int nwin = 0;
-        for (int64_t ws = r_cur;; ws += 32) {
-            const int64_t q = ws + 1 + lane;
-            const int64_t Eq = q <= a.L ? __ldg(indptr + q) : INT64_MAX;
-            Eq_last = Eq;
-            nwin++;
-            const int Er = (int)min(Eq - base, (int64_t)INT32_MAX);
-            int pos = 0;
+                for (int k = 0; k < K; k++) acc[k] = warp_sum(acc[k]);
+                const int64_t row_st = __shfl_sync(kFull, st, j), row_en = __shfl_sync(kFull, en, j);
+                if (lane == 0)
+                    finish_row<K, VS>(a, r0 + j, acc, row_st, row_en, lo, hi, gw, V, out, dot,
+                                      want_dot);
+                j++;
+            } else {
+                // up to four short rows, one per 8-lane subgroup, up to the next long row
+                const unsigned ahead = longmask & (0xffffffffu << j);
+                int batch = ahead ? (__ffs(ahead) - 1 - j) : 4;
+                batch = min(min(batch, 4), nrows - j);
+                const int src = min(j + sub, 31);
+                const bool mine = sub < batch;
+                const int64_t rs = __shfl_sync(kFull, cs, src), re = __shfl_sync(kFull, ce, src);
+                const int64_t row_st = __shfl_sync(kFull, st, src);
+                const int64_t row_en = __shfl_sync(kFull, en, src);
+                double acc[K];
 #pragma unroll
-            for (int step = 16; step >= 1; step >>= 1) {
-                const int v = __shfl_sync(kFull, Er, pos + step - 1);
-                if (v <= lane) pos += step;
-            }
-            if (__shfl_sync(kFull, Er, 31) <= lane) pos = 32;
-            if (rr < 0 && pos < 32) rr = (int)(ws - r_cur) + pos;
-            if (!__any_sync(kFull, valid && rr < 0)) break;
-        }
-        double v[K];
-        if (valid) {
+                for (int k = 0; k < K; k++) acc[k] = 0.0;
+                if (mine) row_products<K, VS, PAIRS, 8>(a, V, rs + sl, re, acc);
 #pragma unroll
-            for (int k = 0; k < K; k++) v[k] = d * g[k];
-        } else {
-            rr = INT32_MAX;
-#pragma unroll
-            for (int k = 0; k < K; k++) v[k] = 0.0;
-        }
-        // segmented inclusive scan over lanes of equal row
-#pragma unroll
-        for (int s = 1; s < 32; s <<= 1) {
-            const int ro = __shfl_up_sync(kFull, rr, s);
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                const double o = __shfl_up_sync(kFull, v[k], s);
-                if (lane >= s && ro == rr) v[k] += o;
-            }
-        }
-        const int rnext = __shfl_down_sync(kFull, rr, 1);
-        const bool tail = valid && (lane == 31 || rnext != rr);
-        const int64_t row = r_cur + rr;
-        // with one window (the usual case) lane q holds the end of row r_cur + q,
-        // so a row's bounds come from shuffles instead of loads
-        const bool single = nwin == 1;
-        const int64_t re_w = __shfl_sync(kFull, Eq_last, min(max(rr, 0), 31));
-        int64_t rs_w = __shfl_sync(kFull, Eq_last, min(max(rr - 1, 0), 31));
-        if (rr == 0) rs_w = rcur_start;
-        if (tail && row == row_open) {
-#pragma unroll
-            for (int k = 0; k < K; k++) v[k] += carry[k];
-        }
-        // the last lane's row and sum carry into the next chunk when it goes on
-        const int r31 = __shfl_sync(kFull, rr, 31);
-        bool goes_on = false;
-        if (tail) {
-            const int64_t rs = single ? rs_w : __ldg(indptr + row);
-            const int64_t re = single ? re_w : __ldg(indptr + row + 1);
-            const bool ends_here = re == e + 1;
-            goes_on = !ends_here && e + 1 < hi;                 // into the next chunk
-            if (!goes_on) {
-                if (want_dot) {
-#pragma unroll
-                    for (int k = 0; k < K; k++) dot[k] += V[row * K + k] * v[k];
+                for (int k = 0; k < K; k++) {
+                    acc[k] += __shfl_xor_sync(kFull, acc[k], 4);
+                    acc[k] += __shfl_xor_sync(kFull, acc[k], 2);
+                    acc[k] += __shfl_xor_sync(kFull, acc[k], 1);
                 }
-                if (ends_here && rs >= lo) {
-#pragma unroll
-                    for (int k = 0; k < K; k++) out[row * K + k] = v[k];
-                } else {
-                    // cut row: slot 1 in the warp where it starts, 0 elsewhere
-                    const int slot = rs >= lo ? 1 : 0;
-                    double *cs = a.carry + (gw * 2 + slot) * K;
-#pragma unroll
-                    for (int k = 0; k < K; k++) cs[k] = v[k];
-                }
+                if (mine && sl == 0 && re > rs)
+                    finish_row<K, VS>(a, r0 + j + sub, acc, row_st, row_en, lo, hi, gw, V, out,
+                                      dot, want_dot);
+                j += batch;
             }
         }
-        if (__shfl_sync(kFull, (int)goes_on, 31)) {
-            row_open = r_cur + r31;
-#pragma unroll
-            for (int k = 0; k < K; k++) carry[k] = __shfl_sync(kFull, v[k], 31);
-        } else {
-            row_open = -1;
-        }
-        if (r31 != INT32_MAX) {
-            const int64_t next_start = __shfl_sync(kFull, Eq_last, min(max(r31 - 1, 0), 31));
-            if (r31 > 0) rcur_start = single ? next_start : __ldg(indptr + r_cur + r31);
-            r_cur += r31;
-        }
+        if (nrows < 32) break;
+        r0 += 32;
     }
 }
 
@@ -248,7 +271,7 @@ __device__ bool finish_cut_row(const Params &a, int64_t &row, double (&ap)[K])
     const int64_t lo = gw * a.chunk;
     const int64_t hi = min(lo + a.chunk, a.nnz);
     if (lo >= hi) return false;
-    const int64_t r = upper_bound(a.indptr, a.L + 1, lo) - 1;
+    const int64_t r = a.wfirst[gw];
     const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
     if (!(rs < lo && re <= hi)) return false;
     const int64_t w0 = rs / a.chunk;
@@ -266,15 +289,10 @@ __device__ bool finish_cut_row(const Params &a, int64_t &row, double (&ap)[K])
     return true;
 }
 
-__device__ __forceinline__ bool row_is_cut(const int64_t *indptr, int64_t r, int64_t chunk)
-{
-    const int64_t rs = indptr[r], re = indptr[r + 1];
-    return re > rs && (rs / chunk) != ((re - 1) / chunk);
-}
-
 template <int K>
 __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
 {
+    constexpr int KP = Stride<K>::P;
     __shared__ double s_red[4 * K];
     __shared__ double s_scratch[kWarps];
     GridBarrier gb{a.bar};
@@ -293,12 +311,24 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
         rel[k] = 0.0;
     }
 
-    // ---- set-up: R = B - S X0 (or B), the zero columns, ||B||, rz
+    // ---- set-up: each warp's first row and the cut flags (used by the same
+    // warps / threads later, so no barrier is needed for them)
+    {
+        const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
+        const int64_t lo = gw * a.chunk;
+        if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
+        __syncwarp();
+        for (int64_t r = gtid; r < L; r += gstride) {
+            const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
+            a.cut[r] = (re > rs && (rs / a.chunk) != ((re - 1) / a.chunk)) ? 1 : 0;
+        }
+    }
+    // ---- R = B - S X0 (or B), the zero columns, ||B||, rz
     double dot[K];
 #pragma unroll
     for (int k = 0; k < K; k++) dot[k] = 0.0;
     if (a.X0 != nullptr) {
-        spmm_range<K>(a, a.X0, a.AP, dot, false);
+        spmm_range<K, K, false>(a, a.X0, a.AP, dot, false);
         if (!gb.sync()) return;
     }
     {
@@ -315,16 +345,17 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
                 if (zero[k]) { x = 0.0; res = 0.0; }
                 a.X[r * K + k] = x;
                 a.R[r * K + k] = res;
-                a.P[r * K + k] = res * di;
+                a.P[r * KP + k] = res * di;
                 sb[k] += b * b;
                 sr[k] += res * res;
                 sz[k] += res * res * di;
             }
+#pragma unroll
+            for (int k = K; k < KP; k++) a.P[r * KP + k] = 0.0;
         };
         for (int64_t r = gtid; r < L; r += gstride) {
             double ap[K];
-            const bool cut = a.X0 != nullptr && row_is_cut(a.indptr, r, a.chunk);
-            if (cut) continue;
+            if (a.X0 != nullptr && a.cut[r]) continue;
             const bool empty = a.indptr[r + 1] == a.indptr[r];
 #pragma unroll
             for (int k = 0; k < K; k++) ap[k] = (a.X0 != nullptr && !empty) ? a.AP[r * K + k] : 0.0;
@@ -372,12 +403,12 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
     bool done = all_zero || (a.X0 != nullptr && !any_active);
     __syncthreads();
     if (!done) {
-        if (!gb.sync()) return;     // P complete before the first SpMM
+        if (!gb.sync()) return;     // the set-up partials are read before phase A reuses them
         for (it = 1; it <= a.maxiter; it++) {
             // ---- A: AP = S P, p'Ap
 #pragma unroll
             for (int k = 0; k < K; k++) dot[k] = 0.0;
-            spmm_range<K>(a, a.P, a.AP, dot, true);
+            spmm_range<K, KP, (KP % 2 == 0)>(a, a.P, a.AP, dot, true);
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 double t = block_sum(dot[k], s_scratch);
@@ -406,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
                 const double di = a.dinv[r];
 #pragma unroll
                 for (int k = 0; k < K; k++) {
-                    const double p = a.P[r * K + k];
+                    const double p = a.P[r * KP + k];
                     a.X[r * K + k] += alpha[k] * p;
                     const double res = a.R[r * K + k] - alpha[k] * ap[k];
                     a.R[r * K + k] = res;
@@ -415,7 +446,7 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
                 }
             };
             for (int64_t r = gtid; r < L; r += gstride) {
-                if (row_is_cut(a.indptr, r, a.chunk)) continue;
+                if (a.cut[r]) continue;
                 double ap[K];
                 const bool empty = a.indptr[r + 1] == a.indptr[r];
 #pragma unroll
@@ -465,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
                 const double di = a.dinv[r];
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    a.P[r * K + k] = a.R[r * K + k] * di + beta[k] * a.P[r * K + k];
+                    a.P[r * KP + k] = a.R[r * K + k] * di + beta[k] * a.P[r * KP + k];
             }
             if (!gb.sync()) return;
         }
@@ -487,8 +518,8 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
     }
 }
 
-// Writes the barrier's error code (if any) into info->status after the
-// persistent kernel, so a caller reading info sees a timed-out solve.
+// Writes the barrier's error code (if any) into info after the persistent
+// kernel, so a caller reading info sees a solve that stopped early.
 __global__ void pcg_status_kernel(const unsigned *bar, hdfe_pcg_info *info)
 {
     if (threadIdx.x == 0 && bar[2] != 0) {
@@ -556,7 +587,7 @@ extern "C" int64_t hdfe_pcg_workspace_bytes(int64_t L, int64_t nnz, int32_t k)
     if (k < 1 || k > HDFE_PCG_MAX_K || L < 0) return -1;
     int blocks = pcg::grid_blocks_for(k);
     if (blocks < 1) return -1;
-    return pcg::layout(L, k, blocks).total_bytes;
+    return pcg::layout(L, k, blocks).total;
 }
 
 extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *data,
@@ -568,13 +599,15 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     if (k < 1 || k > HDFE_PCG_MAX_K || L < 1 || nnz < 0 || !indptr || !dinv || !B || !X ||
         !info || !workspace || maxiter < 0 || (nnz > 0 && (!indices || !data)))
         return hdfe_set_arg_error("hdfe_pcg_solve: bad argument");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return hdfe_set_arg_error("hdfe_pcg_solve: workspace must be 256-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
     int blocks = pcg::grid_blocks_for(k);
     if (blocks < 1) return hdfe_set_cuda_error(cudaGetLastError());
     pcg::Layout lay = pcg::layout(L, k, blocks);
-    if (workspace_bytes < lay.total_bytes)
+    if (workspace_bytes < lay.total)
         return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_pcg_solve: workspace too small");
-    double *ws = (double *)workspace;
+    char *ws = (char *)workspace;
     pcg::Params p;
     p.indptr = indptr;
     p.indices = indices;
@@ -590,12 +623,14 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     p.tol = tol;
     p.maxiter = maxiter;
     p.X = X;
-    p.R = ws + lay.r;
-    p.P = ws + lay.p;
-    p.AP = ws + lay.ap;
-    p.carry = ws + lay.carry;
-    p.part = ws + lay.part;
-    p.bar = (unsigned *)((char *)workspace + lay.bar_bytes_off);
+    p.R = (double *)(ws + lay.r);
+    p.P = (double *)(ws + lay.p);
+    p.AP = (double *)(ws + lay.ap);
+    p.carry = (double *)(ws + lay.carry);
+    p.part = (double *)(ws + lay.part);
+    p.wfirst = (int64_t *)(ws + lay.wfirst);
+    p.cut = (uint8_t *)(ws + lay.cut);
+    p.bar = (unsigned *)(ws + lay.bar);
     p.info = info;
     HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
     cudaError_t e = cudaErrorInvalidValue;
