@@ -650,3 +650,48 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     hdfe_add_launches(2);
     return HDFE_OK;
 }
+
+// ------------------------------------------------ allocation-free variant
+//
+// Some callers cannot allocate device memory for the solver's scratch: a
+// host binding that has no CUDA allocator of its own (a thin FFI layer from
+// another language runtime), or code that must not call cudaMalloc because
+// it synchronises the device and would stall other work in flight.  For
+// them hdfe_pcg_solve_noalloc keeps the scratch in this file-scope device
+// array instead of a caller-provided workspace.  Every GPU that loads the
+// library holds the array until the process exits.
+
+static __device__ __align__(256) unsigned char g_pcg_scratch[HDFE_PCG_NOALLOC_BYTES];
+
+namespace {
+// the array's device address, looked up once per device (with that device
+// current): in host code the symbol is only a host-side stand-in
+void *g_scratch_addr[64] = {};
+}
+
+extern "C" int hdfe_pcg_solve_noalloc(const int64_t *indptr, const int32_t *indices,
+                                      const double *data, int64_t L, int64_t nnz,
+                                      const double *dinv, const double *B, int32_t k,
+                                      const uint8_t *zero, const double *X0, double tol,
+                                      int64_t maxiter, double *X, hdfe_pcg_info *info,
+                                      void *stream)
+{
+    if (k < 1 || k > HDFE_PCG_MAX_K || L < 1)
+        return hdfe_set_arg_error("hdfe_pcg_solve_noalloc: bad argument");
+    const int64_t need = hdfe_pcg_workspace_bytes(L, nnz, k);
+    if (need < 0) return hdfe_set_cuda_error(cudaGetLastError());
+    if (need > (int64_t)HDFE_PCG_NOALLOC_BYTES)
+        return hdfe_set_error(HDFE_ERR_WORKSPACE,
+                              "hdfe_pcg_solve_noalloc: L x k too large for the built-in scratch "
+                              "(HDFE_PCG_NOALLOC_BYTES); use hdfe_pcg_solve with a workspace");
+    int dev = 0;
+    HDFE_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return hdfe_set_arg_error("hdfe_pcg_solve_noalloc: device index");
+    if (g_scratch_addr[dev] == nullptr) {
+        void *ptr = nullptr;
+        HDFE_CUDA_TRY(cudaGetSymbolAddress(&ptr, g_pcg_scratch));
+        g_scratch_addr[dev] = ptr;
+    }
+    return hdfe_pcg_solve(indptr, indices, data, L, nnz, dinv, B, k, zero, X0, tol, maxiter, X,
+                          g_scratch_addr[dev], (int64_t)HDFE_PCG_NOALLOC_BYTES, info, stream);
+}

@@ -200,6 +200,28 @@ int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *
                    double *X, void *workspace, int64_t workspace_bytes,
                    hdfe_pcg_info *info, void *stream);
 
+/* The same solve for callers that cannot allocate device memory -- a host
+ * binding with no CUDA allocator of its own, or code that must not call
+ * cudaMalloc because it synchronises the device.  No counterpart in the
+ * reference: it is an addition of this library.  The scratch that
+ * hdfe_pcg_solve takes as `workspace` lives instead in a device array inside
+ * the library, HDFE_PCG_NOALLOC_BYTES (16 MiB) on every GPU that loads it,
+ * held until the process exits.  Sizes whose scratch exceeds it
+ * (hdfe_pcg_workspace_bytes(L, nnz, k) > HDFE_PCG_NOALLOC_BYTES; about
+ * L * k <= 600,000 values) are rejected with HDFE_ERR_WORKSPACE.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * with that device current, so make it before any stream capture.  Every
+ * call shares the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and corrupt each other; serialise them.  Nothing
+ * in the array needs clearing between calls: each solve rewrites what it
+ * reads.  No memory is allocated by this call. */
+#define HDFE_PCG_NOALLOC_BYTES (16ll << 20)
+
+int hdfe_pcg_solve_noalloc(const int64_t *indptr, const int32_t *indices, const double *data,
+                           int64_t L, int64_t nnz, const double *dinv, const double *B,
+                           int32_t k, const uint8_t *zero, const double *X0, double tol,
+                           int64_t maxiter, double *X, hdfe_pcg_info *info, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
