@@ -38,7 +38,7 @@
 namespace hdfe {
 namespace pcg {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 1024;    // one CTA per SM: fewer arrivals at each grid barrier
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kLong = 64;           // nonzeros in a warp's range that make a row "long"
@@ -289,12 +289,35 @@ __device__ bool finish_cut_row(const Params &a, int64_t &row, double (&ap)[K])
     return true;
 }
 
+// Per-CTA sums of N values per thread, written as partials q0 .. q0+N-1 of
+// this CTA: warp trees, then one thread per value over the warps in order.
+// One pair of __syncthreads for all N values.
+template <int N>
+__device__ __forceinline__ void block_partials(double (&v)[N], double *scratch, double *part,
+                                               int q0, int nb)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < N; i++) v[i] = warp_sum(v[i]);
+    if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < N; i++) scratch[warp * N + i] = v[i];
+    }
+    __syncthreads();
+    if (threadIdx.x < N) {
+        double t = 0.0;
+        for (int w = 0; w < kWarps; w++) t += scratch[w * N + threadIdx.x];
+        part[(int64_t)(q0 + threadIdx.x) * nb + blockIdx.x] = t;
+    }
+    __syncthreads();
+}
+
 template <int K>
-__global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
+__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(Params a)
 {
     constexpr int KP = Stride<K>::P;
     __shared__ double s_red[4 * K];
-    __shared__ double s_scratch[kWarps];
+    __shared__ double s_scratch[kWarps * 3 * K];
     GridBarrier gb{a.bar};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t gtid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
@@ -366,16 +389,11 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
             double ap[K];
             if (finish_cut_row<K>(a, r, ap) && lane == 0) setup_row(r, ap);
         }
+        {
+            double v[3 * K];
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            double t0 = block_sum(sb[k], s_scratch);
-            double t1 = block_sum(sr[k], s_scratch);
-            double t2 = block_sum(sz[k], s_scratch);
-            if (threadIdx.x == 0) {
-                a.part[(int64_t)(0 * K + k) * nb + blockIdx.x] = t0;
-                a.part[(int64_t)(1 * K + k) * nb + blockIdx.x] = t1;
-                a.part[(int64_t)(2 * K + k) * nb + blockIdx.x] = t2;
-            }
+            for (int k = 0; k < K; k++) { v[k] = sb[k]; v[K + k] = sr[k]; v[2 * K + k] = sz[k]; }
+            block_partials<3 * K>(v, s_scratch, a.part, 0, nb);
         }
         if (!gb.sync()) return;
         if (warp < 3) {
@@ -409,11 +427,7 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
 #pragma unroll
             for (int k = 0; k < K; k++) dot[k] = 0.0;
             spmm_range<K, KP, (KP % 2 == 0)>(a, a.P, a.AP, dot, true);
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                double t = block_sum(dot[k], s_scratch);
-                if (threadIdx.x == 0) a.part[(int64_t)k * nb + blockIdx.x] = t;
-            }
+            block_partials<K>(dot, s_scratch, a.part, 0, nb);
             if (!gb.sync()) return;
             if (warp == 0) {
                 for (int k = 0; k < K; k++) {
@@ -458,14 +472,11 @@ __global__ void __launch_bounds__(kThreads, 4) pcg_kernel(Params a)
                 double ap[K];
                 if (finish_cut_row<K>(a, r, ap) && lane == 0) step_row(r, ap);
             }
+            {
+                double v[2 * K];
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-                double t1 = block_sum(sr[k], s_scratch);
-                double t2 = block_sum(sz[k], s_scratch);
-                if (threadIdx.x == 0) {
-                    a.part[(int64_t)(1 * K + k) * nb + blockIdx.x] = t1;
-                    a.part[(int64_t)(2 * K + k) * nb + blockIdx.x] = t2;
-                }
+                for (int k = 0; k < K; k++) { v[k] = sr[k]; v[K + k] = sz[k]; }
+                block_partials<2 * K>(v, s_scratch, a.part, K, nb);
             }
             if (!gb.sync()) return;
             if (warp < 2) {
@@ -540,7 +551,7 @@ int grid_blocks()
         cudaSuccess)
         return -1;
     if (per_sm < 1) return -1;
-    return sms * (per_sm < 4 ? per_sm : 4);
+    return sms * (per_sm < 1 ? per_sm : 1);
 }
 
 int grid_blocks_for_uncached(int k)
