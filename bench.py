@@ -190,6 +190,31 @@ def run_ours(args, rank, world, local_rank):
     info = res.info
     its = int(np.max(np.atleast_1d(info["iterations"])))
 
+    # accuracy: FP64 and the mixed-precision solve (FP32 inner CG, FP64
+    # refinement) at tol 1e-12, each against an FP64 solve at 1e-13; the
+    # solves (components, PCG, normalisation) are timed on the same cells and S
+    cells, S = res.cells, res.S
+    ref = fit.solve(cells, S, tol=1e-13)
+    accuracy = {"tol": 1e-12, "oracle": "FP64 PCG at 1e-13"}
+    for prec in ("fp64", "mixed"):
+        for _ in range(2):
+            r = fit.solve(cells, S, tol=1e-12, precision=prec)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        reps = max(args.steps, 3)
+        a0.record()
+        for _ in range(reps):
+            r = fit.solve(cells, S, tol=1e-12, precision=prec)
+        a1.record()
+        torch.cuda.synchronize()
+        err = float((r.gamma - ref.gamma).abs().max() / ref.gamma.abs().max())
+        accuracy[prec] = {"solve_ms": round(a0.elapsed_time(a1) / reps, 3),
+                          "iterations": r.info["iterations"],
+                          "max_rel_residual": r.info["max_rel_residual"],
+                          "rel_fe_err": err}
+    accuracy["mixed_speedup"] = round(accuracy["fp64"]["solve_ms"] / accuracy["mixed"]["solve_ms"], 3)
+
     # e2e through the public call: pinned host rows up, fixed effects back
     e2e = run_e2e(args, rows, dist)
 
@@ -218,6 +243,7 @@ def run_ours(args, rank, world, local_rank):
                          "frac": roof[dom]["frac"], "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs", "phases": roof},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+            "accuracy_1e-8": accuracy,
             "solve": {"iterations": info["iterations"], "converged": info["converged"],
                       "max_rel_residual": info["max_rel_residual"], "S_nnz": info["S_nnz"],
                       "n_components": info["n_components"]},

@@ -52,6 +52,9 @@ SIGNATURES = {
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),
+    "hdfe_pcg_mixed_workspace_bytes": (_i64, [_i64, _i64, _i32]),
+    "hdfe_pcg_solve_mixed": (_c.c_int, [_vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp,
+                                        _vp, _f64, _f64, _i64, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_pcg_solve_noalloc": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp,
                                           _f64, _i64, _vp, _vp, _vp]),
 }

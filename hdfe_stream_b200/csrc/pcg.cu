@@ -31,6 +31,7 @@
 // Determinism: the grid size, the warp ranges and every reduction order are
 // fixed for a given GPU and build, so repeated solves give identical bits.
 #include <cstdio>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -114,17 +115,27 @@ __device__ __forceinline__ double reduce_part(const double *part, int q)
     return warp_sum(s);
 }
 
-// Row c of V (stride VS) into g[0..K): pairs of doubles when the rows are
-// 16-byte aligned (VS even, V 16-byte aligned), scalars otherwise.  Plain
-// loads: V may be written by this kernel between grid barriers.
-template <int K, int VS, bool PAIRS>
-__device__ __forceinline__ void gather(const double *V, int64_t c, double (&g)[K])
+// Row c of V (stride VS) into g[0..K), with vector loads of VW elements
+// (2 doubles, or 2 or 4 floats: 8- or 16-byte aligned rows) or scalars.
+// Plain loads: V may be written by this kernel between grid barriers.
+template <int K, int VS, int VW, typename T>
+__device__ __forceinline__ void gather(const T *V, int64_t c, T (&g)[K])
 {
-    const double *p = V + c * VS;
-    if constexpr (PAIRS) {
+    const T *p = V + c * VS;
+    if constexpr (VW == 4) {
+#pragma unroll
+        for (int k = 0; k < K; k += 4) {
+            const float4 t = *reinterpret_cast<const float4 *>(p + k);
+            g[k] = t.x;
+            if (k + 1 < K) g[k + 1] = t.y;
+            if (k + 2 < K) g[k + 2] = t.z;
+            if (k + 3 < K) g[k + 3] = t.w;
+        }
+    } else if constexpr (VW == 2) {
+        using T2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
 #pragma unroll
         for (int k = 0; k < K; k += 2) {
-            const double2 t = *reinterpret_cast<const double2 *>(p + k);
+            const T2 t = *reinterpret_cast<const T2 *>(p + k);
             g[k] = t.x;
             if (k + 1 < K) g[k + 1] = t.y;
         }
@@ -134,33 +145,33 @@ __device__ __forceinline__ void gather(const double *V, int64_t c, double (&g)[K
     }
 }
 
-// acc += sum over e = e0, e0 + STEP, ... < re of data[e] * V[indices[e]]:
+// acc += sum over e = e0, e0 + STEP, ... < re of vals[e] * V[indices[e]]:
 // U nonzeros per lane per round, their index/value loads and then their
 // gathers all issued before the multiply-adds, so U round trips overlap.
-template <int K, int VS, bool PAIRS, int STEP>
-__device__ __forceinline__ void row_products(const Params &a, const double *V, int64_t e0,
-                                             int64_t re, double (&acc)[K])
+template <int K, int VS, int VW, int STEP, typename T>
+__device__ __forceinline__ void row_products(const Params &a, const T *vals, const T *V,
+                                             int64_t e0, int64_t re, T (&acc)[K])
 {
     constexpr int U = K <= 4 ? 4 : 2;
     for (; e0 < re; e0 += STEP * U) {
         int64_t c[U];
-        double d[U];
+        T d[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const int64_t e = e0 + STEP * u;
             c[u] = 0;
-            d[u] = 0.0;
+            d[u] = T(0);
             if (e < re) {
                 c[u] = __ldg(a.indices + e);
-                d[u] = __ldg(a.data + e);
+                d[u] = __ldg(vals + e);
             }
         }
 #pragma unroll
         for (int u = 0; u < U; u++)
             if (c[u] < 0 || c[u] >= a.L) { GridBarrier{a.bar}.fail(HDFE_ERR_BAD_CODE); c[u] = 0; }
-        double g[U][K];
+        T g[U][K];
 #pragma unroll
-        for (int u = 0; u < U; u++) gather<K, VS, PAIRS>(V, c[u], g[u]);
+        for (int u = 0; u < U; u++) gather<K, VS, VW, T>(V, c[u], g[u]);
 #pragma unroll
         for (int u = 0; u < U; u++)
 #pragma unroll
@@ -168,32 +179,33 @@ __device__ __forceinline__ void row_products(const Params &a, const double *V, i
     }
 }
 
-template <int K, int VS>
-__device__ __forceinline__ void finish_row(const Params &a, int64_t row, const double (&acc)[K],
-                                           int64_t row_st, int64_t row_en, int64_t lo,
-                                           int64_t hi, int64_t gw, const double *V,
-                                           double *out, double (&dot)[K], bool want_dot)
+template <int K, int VS, typename T>
+__device__ __forceinline__ void finish_row(int64_t row, const T (&acc)[K], int64_t row_st,
+                                           int64_t row_en, int64_t lo, int64_t hi, int64_t gw,
+                                           const T *V, T *out, T *carry, double (&dot)[K],
+                                           bool want_dot)
 {
     if (want_dot) {
 #pragma unroll
-        for (int k = 0; k < K; k++) dot[k] += V[row * VS + k] * acc[k];
+        for (int k = 0; k < K; k++) dot[k] += (double)V[row * VS + k] * (double)acc[k];
     }
     if (row_st >= lo && row_en <= hi) {
 #pragma unroll
         for (int k = 0; k < K; k++) out[row * K + k] = acc[k];
     } else {
         // cut row: slot 1 in the warp where it starts, 0 elsewhere
-        double *cs = a.carry + (gw * 2 + (row_st >= lo ? 1 : 0)) * K;
+        T *cs = carry + (gw * 2 + (row_st >= lo ? 1 : 0)) * K;
 #pragma unroll
         for (int k = 0; k < K; k++) cs[k] = acc[k];
     }
 }
 
 // out = S V over this warp's range of nonzeros (rows inside the range),
-// partial sums of cut rows to the carry slots, dot[k] += V[r] . (S V)[r].
-template <int K, int VS, bool PAIRS>
-__device__ void spmm_range(const Params &a, const double *__restrict__ V, double *__restrict__ out,
-                           double (&dot)[K], bool want_dot)
+// partial sums of cut rows to the carry slots, dot[k] += V[r] . (S V)[r]
+// (in FP64 whatever T is).  vals are S's values in T.
+template <int K, int VS, int VW, typename T>
+__device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T *__restrict__ V,
+                           T *__restrict__ out, T *carry, double (&dot)[K], bool want_dot)
 {
     const int lane = threadIdx.x & 31, sub = lane >> 3, sl = lane & 7;
     const int64_t gw = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
@@ -218,16 +230,16 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
             if ((longmask >> j) & 1u) {
                 // one long row, the whole warp
                 const int64_t rs = __shfl_sync(kFull, cs, j), re = __shfl_sync(kFull, ce, j);
-                double acc[K];
+                T acc[K];
 #pragma unroll
-                for (int k = 0; k < K; k++) acc[k] = 0.0;
-                row_products<K, VS, PAIRS, 32>(a, V, rs + lane, re, acc);
+                for (int k = 0; k < K; k++) acc[k] = T(0);
+                row_products<K, VS, VW, 32, T>(a, vals, V, rs + lane, re, acc);
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = warp_sum(acc[k]);
                 const int64_t row_st = __shfl_sync(kFull, st, j), row_en = __shfl_sync(kFull, en, j);
                 if (lane == 0)
-                    finish_row<K, VS>(a, r0 + j, acc, row_st, row_en, lo, hi, gw, V, out, dot,
-                                      want_dot);
+                    finish_row<K, VS, T>(r0 + j, acc, row_st, row_en, lo, hi, gw, V, out, carry,
+                                         dot, want_dot);
                 j++;
             } else {
                 // up to four short rows, one per 8-lane subgroup, up to the next long row
@@ -239,10 +251,10 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
                 const int64_t rs = __shfl_sync(kFull, cs, src), re = __shfl_sync(kFull, ce, src);
                 const int64_t row_st = __shfl_sync(kFull, st, src);
                 const int64_t row_en = __shfl_sync(kFull, en, src);
-                double acc[K];
+                T acc[K];
 #pragma unroll
-                for (int k = 0; k < K; k++) acc[k] = 0.0;
-                if (mine) row_products<K, VS, PAIRS, 8>(a, V, rs + sl, re, acc);
+                for (int k = 0; k < K; k++) acc[k] = T(0);
+                if (mine) row_products<K, VS, VW, 8, T>(a, vals, V, rs + sl, re, acc);
 #pragma unroll
                 for (int k = 0; k < K; k++) {
                     acc[k] += __shfl_xor_sync(kFull, acc[k], 4);
@@ -250,8 +262,8 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
                     acc[k] += __shfl_xor_sync(kFull, acc[k], 1);
                 }
                 if (mine && sl == 0 && re > rs)
-                    finish_row<K, VS>(a, r0 + j + sub, acc, row_st, row_en, lo, hi, gw, V, out,
-                                      dot, want_dot);
+                    finish_row<K, VS, T>(r0 + j + sub, acc, row_st, row_en, lo, hi, gw, V, out,
+                                         carry, dot, want_dot);
                 j += batch;
             }
         }
@@ -263,8 +275,8 @@ __device__ void spmm_range(const Params &a, const double *__restrict__ V, double
 // AP[r] for a row whose nonzeros span several warps: summed from their carry
 // slots in a fixed order by the warp holding the row's last nonzero.  Returns
 // true (in all lanes) when this warp finishes such a row, with its AP in ap[].
-template <int K>
-__device__ bool finish_cut_row(const Params &a, int64_t &row, double (&ap)[K])
+template <int K, typename T>
+__device__ bool finish_cut_row(const Params &a, const T *carry, int64_t &row, T (&ap)[K])
 {
     const int lane = threadIdx.x & 31;
     const int64_t gw = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
@@ -275,11 +287,11 @@ __device__ bool finish_cut_row(const Params &a, int64_t &row, double (&ap)[K])
     const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
     if (!(rs < lo && re <= hi)) return false;
     const int64_t w0 = rs / a.chunk;
-    double s[K];
+    T s[K];
 #pragma unroll
-    for (int k = 0; k < K; k++) s[k] = 0.0;
+    for (int k = 0; k < K; k++) s[k] = T(0);
     for (int64_t w = w0 + lane; w <= gw; w += 32) {
-        const double *cs = a.carry + (w * 2 + (w == w0 ? 1 : 0)) * K;
+        const T *cs = carry + (w * 2 + (w == w0 ? 1 : 0)) * K;
 #pragma unroll
         for (int k = 0; k < K; k++) s[k] += __ldcg(cs + k);
     }
@@ -351,7 +363,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(Params a)
 #pragma unroll
     for (int k = 0; k < K; k++) dot[k] = 0.0;
     if (a.X0 != nullptr) {
-        spmm_range<K, K, false>(a, a.X0, a.AP, dot, false);
+        spmm_range<K, K, 1, double>(a, a.data, a.X0, a.AP, a.carry, dot, false);
         if (!gb.sync()) return;
     }
     {
@@ -387,7 +399,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(Params a)
         if (a.X0 != nullptr) {
             int64_t r;
             double ap[K];
-            if (finish_cut_row<K>(a, r, ap) && lane == 0) setup_row(r, ap);
+            if (finish_cut_row<K, double>(a, a.carry, r, ap) && lane == 0) setup_row(r, ap);
         }
         {
             double v[3 * K];
@@ -426,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(Params a)
             // ---- A: AP = S P, p'Ap
 #pragma unroll
             for (int k = 0; k < K; k++) dot[k] = 0.0;
-            spmm_range<K, KP, (KP % 2 == 0)>(a, a.P, a.AP, dot, true);
+            spmm_range<K, KP, (KP % 2 == 0) ? 2 : 1, double>(a, a.data, a.P, a.AP, a.carry, dot, true);
             block_partials<K>(dot, s_scratch, a.part, 0, nb);
             if (!gb.sync()) return;
             if (warp == 0) {
@@ -470,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(Params a)
             {
                 int64_t r;
                 double ap[K];
-                if (finish_cut_row<K>(a, r, ap) && lane == 0) step_row(r, ap);
+                if (finish_cut_row<K, double>(a, a.carry, r, ap) && lane == 0) step_row(r, ap);
             }
             {
                 double v[2 * K];
@@ -705,4 +717,432 @@ extern "C" int hdfe_pcg_solve_noalloc(const int64_t *indptr, const int32_t *indi
     }
     return hdfe_pcg_solve(indptr, indices, data, L, nnz, dinv, B, k, zero, X0, tol, maxiter, X,
                           g_scratch_addr[dev], (int64_t)HDFE_PCG_NOALLOC_BYTES, info, stream);
+}
+
+// ---------------------------------------------- mixed precision (refined)
+//
+// The same solve with the inner CG in FP32 and iterative refinement in FP64:
+//   outer:  R = B - S X in FP64 (S's FP64 values); rel = ||R|| / ||B||; stop
+//           when every column meets tol;
+//   inner:  Jacobi PCG on S D = R with S's values, the vectors and the
+//           products in FP32 (half the bytes per iteration), its dot products
+//           and norms accumulated in FP64, until ||R_inner|| <= inner_tol ||R||;
+//   update: X += D in FP64.
+// Columns, zero columns, warm starts and the reported relative residual follow
+// hdfe_pcg_solve; `iterations` counts inner iterations, bounded by maxiter.
+namespace hdfe {
+namespace pcg {
+
+template <int K>
+struct FStride {     // FP32 P's row stride: 1, 2, or a multiple of 4 (16-byte rows)
+    static constexpr int P = K == 1 ? 1 : (K == 2 ? 2 : ((K + 3) / 4) * 4);
+    static constexpr int VW = P % 4 == 0 ? 4 : (P % 2 == 0 ? 2 : 1);
+};
+
+struct Mixed {
+    const float *data32;
+    float *R, *P, *AP, *D;      // inner vectors
+    double *AX;                 // FP64 S X, then the FP64 residual
+    double inner_tol;
+};
+
+struct MixedLayout {
+    int64_t r, p, ap, d, ax, carry, part, wfirst, cut, bar, total;
+};
+
+inline MixedLayout mixed_layout(int64_t L, int k, int64_t blocks)
+{
+    MixedLayout o;
+    const int kf = k == 1 ? 1 : (k == 2 ? 2 : ((k + 3) / 4) * 4);
+    int64_t p = 0;
+    auto take = [&](int64_t bytes) { int64_t at = p; p += (bytes + 255) / 256 * 256; return at; };
+    o.r = take(L * k * 4);
+    o.p = take(L * kf * 4);
+    o.ap = take(L * k * 4);
+    o.d = take(L * k * 4);
+    o.ax = take(L * k * 8);
+    o.carry = take(blocks * kWarps * 2 * k * 8);
+    o.part = take(4 * (int64_t)k * blocks * 8);
+    o.wfirst = take(blocks * kWarps * 8);
+    o.cut = take(L);
+    o.bar = take(64);
+    o.total = p;
+    return o;
+}
+
+template <int K>
+__global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Params a, Mixed f)
+{
+    constexpr int KF = FStride<K>::P;
+    constexpr int VWF = FStride<K>::VW;
+    __shared__ double s_red[4 * K];
+    __shared__ double s_scratch[kWarps * 3 * K];
+    GridBarrier gb{a.bar};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t gtid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * kThreads;
+    const int64_t L = a.L;
+    const int nb = gridDim.x;
+    float *carry32 = reinterpret_cast<float *>(a.carry);
+
+    double bnorm[K], rel[K];
+    bool active[K], zero[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        zero[k] = a.zero != nullptr && a.zero[k] != 0;
+        active[k] = !zero[k];
+        rel[k] = 0.0;
+    }
+    // each warp's first row and the cut flags, X = X0 (or 0), ||B||
+    {
+        const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
+        const int64_t lo = gw * a.chunk;
+        if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
+        __syncwarp();
+        double sb[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) sb[k] = 0.0;
+        for (int64_t r = gtid; r < L; r += gstride) {
+            const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
+            a.cut[r] = (re > rs && (rs / a.chunk) != ((re - 1) / a.chunk)) ? 1 : 0;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const double b = a.B[r * K + k];
+                sb[k] += b * b;
+                a.X[r * K + k] = (a.X0 != nullptr && !zero[k]) ? a.X0[r * K + k] : 0.0;
+            }
+        }
+        block_partials<K>(sb, s_scratch, a.part, 0, nb);
+        if (!gb.sync()) return;
+        if (warp == 0) {
+            for (int k = 0; k < K; k++) {
+                const double t = reduce_part(a.part, k);
+                if (lane == 0) s_red[k] = t;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double bn = sqrt(s_red[k]);
+            bnorm[k] = bn == 0.0 ? 1.0 : bn;
+        }
+    }
+    int64_t total = 0;
+    bool any_active = false;
+    double dot[K];
+    for (int64_t outer = 0;; outer++) {
+        // ---- FP64 residual R = B - S X (into AX)
+        const bool have_x = outer > 0 || a.X0 != nullptr;
+        if (have_x) {
+#pragma unroll
+            for (int k = 0; k < K; k++) dot[k] = 0.0;
+            spmm_range<K, K, 1, double>(a, a.data, a.X, f.AX, a.carry, dot, false);
+            if (!gb.sync()) return;
+        }
+        double sr[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) sr[k] = 0.0;
+        auto resid_row = [&](int64_t r, const double (&ax)[K]) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const double res = zero[k] ? 0.0 : a.B[r * K + k] - ax[k];
+                f.AX[r * K + k] = res;
+                sr[k] += res * res;
+            }
+        };
+        for (int64_t r = gtid; r < L; r += gstride) {
+            if (have_x && a.cut[r]) continue;
+            const bool empty = a.indptr[r + 1] == a.indptr[r];
+            double ax[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) ax[k] = (have_x && !empty) ? f.AX[r * K + k] : 0.0;
+            resid_row(r, ax);
+        }
+        if (have_x) {
+            int64_t r;
+            double ax[K];
+            if (finish_cut_row<K, double>(a, a.carry, r, ax) && lane == 0) resid_row(r, ax);
+        }
+        block_partials<K>(sr, s_scratch, a.part, K, nb);
+        if (!gb.sync()) return;
+        if (warp == 0) {
+            for (int k = 0; k < K; k++) {
+                const double t = reduce_part(a.part, K + k);
+                if (lane == 0) s_red[K + k] = t;
+            }
+        }
+        __syncthreads();
+        any_active = false;
+        double rnorm[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            rnorm[k] = sqrt(s_red[K + k]);
+            rel[k] = rnorm[k] / bnorm[k];
+            active[k] = !zero[k] && rel[k] > a.tol;
+            any_active |= active[k];
+        }
+        if (!any_active || total >= a.maxiter) break;
+        // ---- inner FP32 PCG on S D = R
+        double rz[K];
+        {
+            double sz[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) sz[k] = 0.0;
+            for (int64_t r = gtid; r < L; r += gstride) {
+                const float di = (float)a.dinv[r];
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const float res = active[k] ? (float)f.AX[r * K + k] : 0.0f;
+                    f.R[r * K + k] = res;
+                    f.D[r * K + k] = 0.0f;
+                    const float z = res * di;
+                    f.P[r * KF + k] = z;
+                    sz[k] += (double)res * (double)z;
+                }
+#pragma unroll
+                for (int k = K; k < KF; k++) f.P[r * KF + k] = 0.0f;
+            }
+            block_partials<K>(sz, s_scratch, a.part, 2 * K, nb);
+            if (!gb.sync()) return;
+            if (warp == 0) {
+                for (int k = 0; k < K; k++) {
+                    const double t = reduce_part(a.part, 2 * K + k);
+                    if (lane == 0) s_red[2 * K + k] = t;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < K; k++) rz[k] = s_red[2 * K + k];
+        }
+        bool inner_active[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) inner_active[k] = active[k];
+        while (total < a.maxiter) {
+            total++;
+            // A: AP = S P (FP32), p'Ap in FP64
+#pragma unroll
+            for (int k = 0; k < K; k++) dot[k] = 0.0;
+            spmm_range<K, KF, VWF, float>(a, f.data32, f.P, f.AP, carry32, dot, true);
+            block_partials<K>(dot, s_scratch, a.part, 0, nb);
+            if (!gb.sync()) return;
+            if (warp == 0) {
+                for (int k = 0; k < K; k++) {
+                    const double t = reduce_part(a.part, k);
+                    if (lane == 0) s_red[k] = t;
+                }
+            }
+            __syncthreads();
+            float alpha[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const double pap = s_red[k];
+                alpha[k] = (inner_active[k] && pap > 0.0) ? (float)(rz[k] / pap) : 0.0f;
+            }
+            __syncthreads();
+            // B: D += alpha P, R -= alpha AP; sums of R^2 and R^2 dinv in FP64
+            double s1[K], s2[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) s1[k] = s2[k] = 0.0;
+            auto step_row = [&](int64_t r, const float (&ap)[K]) {
+                const double di = a.dinv[r];
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    f.D[r * K + k] += alpha[k] * f.P[r * KF + k];
+                    const float res = f.R[r * K + k] - alpha[k] * ap[k];
+                    f.R[r * K + k] = res;
+                    const double rd = (double)res;
+                    s1[k] += rd * rd;
+                    s2[k] += rd * rd * di;
+                }
+            };
+            for (int64_t r = gtid; r < L; r += gstride) {
+                if (a.cut[r]) continue;
+                float ap[K];
+                const bool empty = a.indptr[r + 1] == a.indptr[r];
+#pragma unroll
+                for (int k = 0; k < K; k++) ap[k] = empty ? 0.0f : f.AP[r * K + k];
+                step_row(r, ap);
+            }
+            {
+                int64_t r;
+                float ap[K];
+                if (finish_cut_row<K, float>(a, carry32, r, ap) && lane == 0) step_row(r, ap);
+            }
+            {
+                double v[2 * K];
+#pragma unroll
+                for (int k = 0; k < K; k++) { v[k] = s1[k]; v[K + k] = s2[k]; }
+                block_partials<2 * K>(v, s_scratch, a.part, K, nb);
+            }
+            if (!gb.sync()) return;
+            if (warp < 2) {
+                for (int k = 0; k < K; k++) {
+                    const double t = reduce_part(a.part, (warp + 1) * K + k);
+                    if (lane == 0) s_red[(warp + 1) * K + k] = t;
+                }
+            }
+            __syncthreads();
+            // C: inner convergence, beta, P = dinv R + beta P
+            bool any_inner = false;
+            float beta[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                inner_active[k] = inner_active[k] && sqrt(s_red[K + k]) > f.inner_tol * rnorm[k];
+                any_inner |= inner_active[k];
+            }
+            if (!any_inner) break;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const double rzn = s_red[2 * K + k];
+                beta[k] = inner_active[k] ? (float)(rzn / (rz[k] != 0.0 ? rz[k] : 1.0)) : 0.0f;
+                rz[k] = rzn;
+            }
+            __syncthreads();
+            for (int64_t r = gtid; r < L; r += gstride) {
+                const float di = (float)a.dinv[r];
+#pragma unroll
+                for (int k = 0; k < K; k++)
+                    f.P[r * KF + k] = f.R[r * K + k] * di + beta[k] * f.P[r * KF + k];
+            }
+            if (!gb.sync()) return;
+        }
+        // ---- X += D in FP64, then a barrier before the next product reads X
+        for (int64_t r = gtid; r < L; r += gstride) {
+#pragma unroll
+            for (int k = 0; k < K; k++)
+                if (active[k]) a.X[r * K + k] += (double)f.D[r * K + k];
+        }
+        if (!gb.sync()) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double mx = 0.0;
+#pragma unroll
+        for (int k = 0; k < K; k++) mx = fmax(mx, rel[k]);
+        a.info->iterations = total;
+        a.info->converged = any_active ? 0 : 1;
+        a.info->status = HDFE_OK;
+        a.info->max_rel = mx;
+    }
+}
+
+template <int K>
+int mixed_grid()
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel<K>, kThreads, 0) !=
+        cudaSuccess)
+        return -1;
+    return per_sm < 1 ? -1 : sms;
+}
+
+int mixed_grid_for(int k)
+{
+    static int cache[64][HDFE_PCG_MAX_K + 1] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    if (cache[dev][k] == 0) {
+        switch (k) {
+        case 1: cache[dev][k] = mixed_grid<1>(); break;
+        case 2: cache[dev][k] = mixed_grid<2>(); break;
+        case 3: cache[dev][k] = mixed_grid<3>(); break;
+        case 4: cache[dev][k] = mixed_grid<4>(); break;
+        case 5: cache[dev][k] = mixed_grid<5>(); break;
+        case 6: cache[dev][k] = mixed_grid<6>(); break;
+        case 7: cache[dev][k] = mixed_grid<7>(); break;
+        case 8: cache[dev][k] = mixed_grid<8>(); break;
+        default: return -1;
+        }
+    }
+    return cache[dev][k];
+}
+
+template <int K>
+cudaError_t launch_mixed(Params p, Mixed m, int blocks, cudaStream_t s)
+{
+    void *args[] = {&p, &m};
+    return cudaLaunchCooperativeKernel((const void *)mixed_kernel<K>, dim3(blocks),
+                                       dim3(kThreads), args, 0, s);
+}
+
+}  // namespace pcg
+}  // namespace hdfe
+
+extern "C" int64_t hdfe_pcg_mixed_workspace_bytes(int64_t L, int64_t nnz, int32_t k)
+{
+    (void)nnz;
+    if (k < 1 || k > HDFE_PCG_MAX_K || L < 0) return -1;
+    const int blocks = pcg::mixed_grid_for(k);
+    if (blocks < 1) return -1;
+    return pcg::mixed_layout(L, k, blocks).total;
+}
+
+extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indices,
+                                    const double *data, const float *data32, int64_t L,
+                                    int64_t nnz, const double *dinv, const double *B, int32_t k,
+                                    const uint8_t *zero, const double *X0, double tol,
+                                    double inner_tol, int64_t maxiter, double *X,
+                                    void *workspace, int64_t workspace_bytes,
+                                    hdfe_pcg_info *info, void *stream)
+{
+    if (k < 1 || k > HDFE_PCG_MAX_K || L < 1 || nnz < 0 || !indptr || !dinv || !B || !X ||
+        !info || !workspace || maxiter < 0 || !(inner_tol > 0.0 && inner_tol < 1.0) ||
+        (nnz > 0 && (!indices || !data || !data32)))
+        return hdfe_set_arg_error("hdfe_pcg_solve_mixed: bad argument");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return hdfe_set_arg_error("hdfe_pcg_solve_mixed: workspace must be 256-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int blocks = pcg::mixed_grid_for(k);
+    if (blocks < 1) return hdfe_set_cuda_error(cudaGetLastError());
+    const pcg::MixedLayout lay = pcg::mixed_layout(L, k, blocks);
+    if (workspace_bytes < lay.total)
+        return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_pcg_solve_mixed: workspace too small");
+    char *ws = (char *)workspace;
+    pcg::Params p{};
+    p.indptr = indptr;
+    p.indices = indices;
+    p.data = data;
+    p.L = L;
+    p.nnz = nnz;
+    const int64_t warps = (int64_t)blocks * pcg::kWarps;
+    p.chunk = nnz > 0 ? (nnz + warps - 1) / warps : 1;
+    p.dinv = dinv;
+    p.B = B;
+    p.zero = zero;
+    p.X0 = X0;
+    p.tol = tol;
+    p.maxiter = maxiter;
+    p.X = X;
+    p.carry = (double *)(ws + lay.carry);
+    p.part = (double *)(ws + lay.part);
+    p.wfirst = (int64_t *)(ws + lay.wfirst);
+    p.cut = (uint8_t *)(ws + lay.cut);
+    p.bar = (unsigned *)(ws + lay.bar);
+    p.info = info;
+    pcg::Mixed m;
+    m.data32 = data32;
+    m.R = (float *)(ws + lay.r);
+    m.P = (float *)(ws + lay.p);
+    m.AP = (float *)(ws + lay.ap);
+    m.D = (float *)(ws + lay.d);
+    m.AX = (double *)(ws + lay.ax);
+    m.inner_tol = inner_tol;
+    HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (k) {
+    case 1: e = pcg::launch_mixed<1>(p, m, blocks, s); break;
+    case 2: e = pcg::launch_mixed<2>(p, m, blocks, s); break;
+    case 3: e = pcg::launch_mixed<3>(p, m, blocks, s); break;
+    case 4: e = pcg::launch_mixed<4>(p, m, blocks, s); break;
+    case 5: e = pcg::launch_mixed<5>(p, m, blocks, s); break;
+    case 6: e = pcg::launch_mixed<6>(p, m, blocks, s); break;
+    case 7: e = pcg::launch_mixed<7>(p, m, blocks, s); break;
+    case 8: e = pcg::launch_mixed<8>(p, m, blocks, s); break;
+    }
+    HDFE_CUDA_TRY(e);
+    pcg::pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);
+    HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(2);
+    return HDFE_OK;
 }

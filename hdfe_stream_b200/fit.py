@@ -254,7 +254,7 @@ class FitResult:
 
 
 def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
-          x0=None, normalize_fe=True, timer=None) -> FitResult:
+          x0=None, normalize_fe=True, timer=None, precision="fp64") -> FitResult:
     """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
     right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
     zero, block PCG per `rhs_block` columns, then `_normalize`."""
@@ -262,7 +262,7 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     timer = timer or _NoTimer()
     m = int(cells.rhs.shape[1])
     dinv = jacobi(cells.diag)
-    solver = BlockSolver(S, dinv, tol, maxiter)
+    solver = BlockSolver(S, dinv, tol, maxiter, precision=precision)
     solver.timer = timer
     scale = torch.sqrt(torch.clamp(cells.raw_ss, min=0.0))
     zero_all = (torch.linalg.vector_norm(cells.rhs, dim=0) <= RHS_ZERO_TOL * scale).cpu().numpy()
@@ -327,15 +327,18 @@ class _NoTimer:
         return contextlib.nullcontext()
 
 
-def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None) -> FitResult:
-    """Pass 1, the S build and step 2 on the device, for device rows."""
+def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None,
+        precision="fp64") -> FitResult:
+    """Pass 1, the S build and step 2 on the device, for device rows.
+    precision "mixed": the PCG's inner iterations in FP32 with FP64
+    refinement to the same FP64 tolerance."""
     timer = timer or _NoTimer()
     with timer("pass1"):
         cells = pass1(rows)
     with timer("sbuild"):
         S = build_s(cells)
     with timer("solve"):
-        return solve(cells, S, tol, maxiter, rhs_block, timer=timer)
+        return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision)
 
 
 def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):

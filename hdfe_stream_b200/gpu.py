@@ -81,9 +81,17 @@ class BlockSolver:
     fit and the leave-out passes use); calling the object takes host arrays,
     exactly as the reference's `solve` (core/gpu.py:194-196)."""
 
-    def __init__(self, S: DeviceCSR, dinv, tol: float, maxiter: int, debug=None):
+    def __init__(self, S: DeviceCSR, dinv, tol: float, maxiter: int, debug=None,
+                 precision: str = "fp64", inner_tol: float = 1e-6):
+        """precision "fp64" is the reference's solve; "mixed" runs the inner
+        CG in FP32 with FP64 iterative refinement (hdfe_pcg_solve_mixed),
+        stopping on the same FP64 relative residual `tol`."""
         import torch
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision, self.inner_tol = precision, float(inner_tol)
         self.S = S
+        self._data32 = S.data.float() if precision == "mixed" else None
         self.dev = S.indptr.device
         self.dinv = torch.as_tensor(np.asarray(dinv, dtype=np.float64)).to(self.dev) \
             if not torch.is_tensor(dinv) else dinv.to(self.dev, torch.float64).contiguous()
@@ -95,7 +103,9 @@ class BlockSolver:
     def _workspace(self, k):
         import torch
         if k not in self._ws:
-            nbytes = _lib.lib().hdfe_pcg_workspace_bytes(self.S.L, self.S.nnz, k)
+            size = (_lib.lib().hdfe_pcg_mixed_workspace_bytes if self.precision == "mixed"
+                    else _lib.lib().hdfe_pcg_workspace_bytes)
+            nbytes = size(self.S.L, self.S.nnz, k)
             if nbytes < 0:
                 raise _lib.HDFEError(_lib.HDFE_ERR_CUDA, "could not size the PCG workspace")
             self._ws[k] = torch.empty(int(nbytes), dtype=torch.uint8, device=self.dev)
@@ -110,11 +120,20 @@ class BlockSolver:
             import torch
             self._zero[:k].copy_(torch.from_numpy(np.asarray(zero, bool).astype(np.uint8)))
             zp = self._zero.data_ptr()
+        x0p = None if X0 is None else X0.data_ptr()
+        if self.precision == "mixed":
+            _lib.check(_lib.lib().hdfe_pcg_solve_mixed(
+                self.S.indptr.data_ptr(), self.S.indices.data_ptr(), self.S.data.data_ptr(),
+                self._data32.data_ptr(), self.S.L, self.S.nnz, self.dinv.data_ptr(),
+                B.data_ptr(), k, zp, x0p, self.tol, self.inner_tol, self.maxiter,
+                X.data_ptr(), ws.data_ptr(), ws.numel(), self._info.data_ptr(),
+                _lib.stream_handle(stream)))
+            return
         _lib.check(_lib.lib().hdfe_pcg_solve(
             self.S.indptr.data_ptr(), self.S.indices.data_ptr(), self.S.data.data_ptr(),
-            self.S.L, self.S.nnz, self.dinv.data_ptr(), B.data_ptr(), k, zp,
-            None if X0 is None else X0.data_ptr(), self.tol, self.maxiter, X.data_ptr(),
-            ws.data_ptr(), ws.numel(), self._info.data_ptr(), _lib.stream_handle(stream)))
+            self.S.L, self.S.nnz, self.dinv.data_ptr(), B.data_ptr(), k, zp, x0p, self.tol,
+            self.maxiter, X.data_ptr(), ws.data_ptr(), ws.numel(), self._info.data_ptr(),
+            _lib.stream_handle(stream)))
 
     def read_info(self):
         raw = self._info.cpu().numpy().tobytes()

@@ -200,6 +200,23 @@ int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *
                    double *X, void *workspace, int64_t workspace_bytes,
                    hdfe_pcg_info *info, void *stream);
 
+/* Mixed precision: the same solve with the inner CG in FP32 and iterative
+ * refinement in FP64 -- the outer residual B - S X (S's FP64 values in
+ * `data`), the update X += D and every dot product and norm are FP64; the
+ * inner PCG on S D = R runs on S's values as FP32 (`data32`, nnz floats) and
+ * FP32 vectors until ||R_inner|| <= inner_tol ||R||.  It stops, like
+ * hdfe_pcg_solve, when every column's ||B - S X|| / ||B|| <= tol (checked in
+ * FP64); info->iterations counts inner iterations, bounded by maxiter.  An
+ * addition of this library (the reference's solve is FP64 only). */
+int64_t hdfe_pcg_mixed_workspace_bytes(int64_t L, int64_t nnz, int32_t k);
+
+int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indices, const double *data,
+                         const float *data32, int64_t L, int64_t nnz, const double *dinv,
+                         const double *B, int32_t k, const uint8_t *zero, const double *X0,
+                         double tol, double inner_tol, int64_t maxiter, double *X,
+                         void *workspace, int64_t workspace_bytes, hdfe_pcg_info *info,
+                         void *stream);
+
 /* The same solve for callers that cannot allocate device memory -- a host
  * binding with no CUDA allocator of its own, or code that must not call
  * cudaMalloc because it synchronises the device.  No counterpart in the

@@ -70,3 +70,16 @@ def test_golden_gamma(device):
         gamma = res.gamma.cpu().numpy()
         err = np.max(np.abs(gamma - g["gamma"])) / np.max(np.abs(g["gamma"]))
         assert err < 1e-8, (name, err)
+
+
+@pytest.mark.parametrize("name,rows", PANELS[:4], ids=[p[0] for p in PANELS[:4]])
+def test_mixed_precision_fit(device, name, rows):
+    """The fit with the mixed-precision solve: fixed effects within 1e-8 of
+    the FP64 oracle at the same residual tolerance."""
+    from hdfe_stream_b200 import fit
+    ref = orc.pass1(rows)
+    gamma_ref, _ = orc.solve(ref, orc.build_explicit(ref), tol=1e-13)
+    res = fit.fit(fit.DeviceRows.from_rows(rows), tol=1e-11, precision="mixed")
+    gamma = res.gamma.cpu().numpy()
+    assert res.info["converged"]
+    assert np.max(np.abs(gamma - gamma_ref)) / np.max(np.abs(gamma_ref)) < 1e-8
