@@ -49,6 +49,14 @@ SIGNATURES = {
     "hdfe_components": (_c.c_int, [_vp, _i64, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_normalize_workspace_bytes": (_i64, [_i64, _i32]),
     "hdfe_normalize": (_c.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _i64, _vp]),
+    "hdfe_row_groups_workspace_bytes": (_i64, [_i64]),
+    "hdfe_row_groups": (_c.c_int, [_vp, _i64, _vp, _vp, _vp, _i64, _vp]),
+    "hdfe_rows_center": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _i32,
+                                    _c.c_uint64, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _i64,
+                                    _vp]),
+    "hdfe_rows_project": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
+                                     _i32, _c.c_uint64, _i64, _i64, _i32, _i64, _vp, _vp, _vp]),
+    "hdfe_jla_combine": (_c.c_int, [_vp, _i64, _i64, _vp]),
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),

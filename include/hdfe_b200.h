@@ -159,6 +159,47 @@ int hdfe_normalize(double *gamma, int32_t m, int32_t D, const int64_t *n_levels,
                    const double *obs, const int32_t *root, void *workspace,
                    int64_t workspace_bytes, void *stream);
 
+/* ------------------------------------------------------- inverse operator
+ *
+ * Row passes of A S^- A' for the leave-out estimators.  Rows are pass 0's
+ * (sorted by the streamed group), `starts` (G+1) their group boundaries
+ * (hdfe_row_groups).  The vectors are either explicit, R (N, B) row-major, or
+ * (R NULL) Rademacher draws regenerated from (seed, ordinal0 + row,
+ * first_draw + j) -- core/kernels_groups.py:53-76 `_nb_rademacher`,
+ * bit-identical.  B <= 32 vectors per pass; X (N, c) covariates, c <= 8, or
+ * NULL; w (N) weights or NULL for ones; sqrt_weights: the square-root weight
+ * metric (vectors scaled by w^(-1/2) going in and w^(1/2) coming out,
+ * inverse.py:280-303).  n_levels is a HOST array.
+ *
+ * hdfe_row_groups: `starts` of rows sorted by gcode; n_groups a DEVICE int64.
+ * hdfe_rows_center: kernels_inverse.py:35-71 `_nb_center_rows`: acc (L, B)
+ *   = D_o' W M_0 R, acc_x (c, B) = X' W M_0 R, squares (B) = sum w R^2.
+ * hdfe_rows_project: kernels_inverse.py:75-107 `_nb_project_rows` given the
+ *   solution U (L, B) and covariate block C (c, B): out (N, B) = (A u)_i, and
+ *   / or moments (5, N) += the JLA sink's five sums per row over the block
+ *   (leaveout.py:181-190).
+ * hdfe_jla_combine: leaveout.py:210-282 `_combine_moments` in place: slots
+ *   0, 1, 2 of moments become the leverage, its complement and the
+ *   non-linearity factor.
+ */
+int64_t hdfe_row_groups_workspace_bytes(int64_t n_rows);
+int hdfe_row_groups(const uint32_t *gcode, int64_t n_rows, int64_t *starts, int64_t *n_groups,
+                    void *workspace, int64_t workspace_bytes, void *stream);
+
+int hdfe_rows_center(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                     const int64_t *n_levels, const double *w, const double *X, int32_t c,
+                     const double *R, int32_t B, uint64_t seed, int64_t first_draw,
+                     int64_t ordinal0, int32_t sqrt_weights, double *acc, double *acc_x,
+                     double *squares, void *workspace, int64_t workspace_bytes, void *stream);
+
+int hdfe_rows_project(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                      const int64_t *n_levels, const double *w, const double *X, int32_t c,
+                      const double *C, const double *U, const double *R, int32_t B,
+                      uint64_t seed, int64_t first_draw, int64_t ordinal0, int32_t sqrt_weights,
+                      int64_t n_rows, double *out, double *moments, void *stream);
+
+int hdfe_jla_combine(double *moments, int64_t n_rows, int64_t n_draws, void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,

@@ -529,3 +529,97 @@ def largest_connected(a, b, n0, n1, min_degree=(1, 1)):
     labels = np.where(parent >= 0, rank[np.maximum(parent, 0)], -1)
     return labels == 0, labels, rows[order]
 
+
+
+# ------------------------------------------------- inverse operator, JLA
+
+class Design:
+    """Row-level view the inverse operator needs: group boundaries of the
+    rows, their level codes, weights (ones when unweighted) and covariates
+    (inverse.py:105-160 `_chunks`, `_covariate_matrix`)."""
+
+    def __init__(self, rows, cells, S, X=None, tol=1e-10, nt=1):
+        self.rows, self.cells, self.S, self.tol, self.nt = rows, cells, S, tol, nt
+        self.starts = row_starts(rows.gcode)
+        self.codes = rows.codes
+        self.w = rows.w if rows.w is not None else np.ones(rows.n_rows)
+        self.X = np.zeros((rows.n_rows, 0)) if X is None else np.ascontiguousarray(X, np.float64)
+        self.dinv = jacobi(cells.diag)
+        self._border = None
+
+    def solve_reduced(self, rhs, scale):
+        """inverse.py:86-103 `_solve_reduced`: zero columns, then the PCG."""
+        rhs = np.ascontiguousarray(rhs)
+        zero = np.linalg.norm(rhs, axis=0) <= RHS_ZERO_TOL * np.asarray(scale)
+        U, *_ = pcg(self.S, self.dinv, rhs, zero, None, self.tol)
+        return U
+
+    def border(self):
+        """inverse.py:182-218 `_border` (and `_reduce_design`)."""
+        if self._border is None:
+            c = self.X.shape[1]
+            if c == 0:
+                self._border = (None, None)
+            else:
+                T_dx, T_xx = center_rows(self.starts, self.codes, self.cells.offs, self.w,
+                                         self.X, self.X, self.cells.L, self.nt)
+                scale = np.sqrt(self.w @ (self.X * self.X))
+                Z = self.solve_reduced(T_dx, scale)
+                schur = T_xx - T_dx.T @ Z
+                self._border = (Z, np.linalg.pinv(schur, hermitian=True))
+        return self._border
+
+    def project_rows(self, n_vec, seed, first_draw=0, sqrt_weights=False):
+        """inverse.py:240-309 `project_rows` for Rademacher vectors: the rows'
+        (A S^- A' r_j)_i, all rows in one chunk."""
+        N = self.rows.n_rows
+        R = rademacher(0, N, n_vec, seed, first_draw)
+        if sqrt_weights:
+            root = np.sqrt(self.w)
+            inv = np.divide(1.0, root, out=np.zeros_like(root), where=root > 0)
+            R = R * inv[:, None]
+        Z, schur_inv = self.border()
+        rhs, rhs_x = center_rows(self.starts, self.codes, self.cells.offs, self.w, self.X, R,
+                                 self.cells.L, self.nt)
+        scale = np.sqrt(self.w @ (R * R))
+        U = self.solve_reduced(rhs, scale)
+        if Z is not None:
+            C = schur_inv @ (rhs_x - Z.T @ rhs)
+            U = U - Z @ C
+        else:
+            C = np.zeros((0, n_vec))
+        out = project_rows_kernel(self.starts, self.codes, self.cells.offs, self.w, self.X, C,
+                                  R, U)
+        return out * root[:, None] if sqrt_weights else out
+
+    def jla_leverages(self, n_draws, block, seed):
+        """leaveout.py:130-198 `jla_leverages` and :210-282
+        `_combine_moments`: (leverage, complement, factor)."""
+        N = self.rows.n_rows
+        mom = np.zeros((5, N))
+        drawn = 0
+        sq = self.rows.w is not None
+        while drawn < n_draws:
+            size = min(block, n_draws - drawn)
+            proj = self.project_rows(size, seed, drawn, sqrt_weights=sq)
+            r = rademacher(0, N, size, seed, drawn)
+            P = proj ** 2
+            M = (r - proj) ** 2
+            mom[0] += P.sum(axis=1)
+            mom[1] += M.sum(axis=1)
+            mom[2] += (P ** 2).sum(axis=1)
+            mom[3] += (M ** 2).sum(axis=1)
+            mom[4] += (P * M).sum(axis=1)
+            drawn += size
+        P, M, m_PP, m_MM, m_PM = (m / n_draws for m in mom)
+        total = P + M
+        P_bar = np.divide(P, total, out=np.zeros_like(P), where=total > 0)
+        M_bar = 1.0 - P_bar
+        V = (M_bar ** 2 * m_PP + P_bar ** 2 * m_MM - 2 * P_bar * M_bar * m_PM) / n_draws
+        B = (M_bar * m_PP - P_bar * m_MM + (M_bar - P_bar) * m_PM) / n_draws
+        usable = M_bar > 0
+        factor = np.ones_like(M_bar)
+        np.divide(V, M_bar ** 2, out=factor, where=usable)
+        factor = np.where(usable, 1.0 - factor + np.divide(B, M_bar, out=np.zeros_like(B),
+                                                             where=usable), 1.0)
+        return P_bar, M_bar, factor

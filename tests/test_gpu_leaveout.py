@@ -1,0 +1,102 @@
+"""The inverse operator's row passes and the JLA leverages on the device,
+against the reference's own outputs (tests/golden, made by the reference's
+project_rows / jla_leverages) and against the oracle with covariates."""
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from conftest import golden_rows, load_golden, GOLDEN_PANELS
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def operator(rows, tol, covariates=False, precision="fp64"):
+    from hdfe_stream_b200 import fit, leaveout
+    drows = fit.DeviceRows.from_rows(rows)
+    cells = fit.pass1(drows)
+    S = fit.build_s(cells)
+    X = drows.V[1:].T.contiguous() if covariates else None
+    return leaveout.InverseOperator(drows, cells, S, X, tol=tol, precision=precision)
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_project_rows_matches_reference(device, name):
+    g = load_golden(name)
+    rows = golden_rows(g)
+    op = operator(rows, float(g["tol"]))
+    out, info = op.project(6, seed=11, sqrt_weights=rows.w is not None)
+    assert info["converged"]
+    assert rel(out.cpu().numpy(), g["project_rows_seed11"]) < 1e-8
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_jla_leverages_match_reference(device, name):
+    g = load_golden(name)
+    rows = golden_rows(g)
+    op = operator(rows, float(g["tol"]))
+    lev, comp, factor = op.jla_leverages(24, block=8, seed=2)
+    assert rel(lev.cpu().numpy(), g["jla_leverage"]) < 1e-8
+    assert rel(factor.cpu().numpy(), g["jla_factor"]) < 1e-8
+    assert np.allclose(lev.cpu().numpy() + comp.cpu().numpy(), 1.0)
+
+
+def test_jla_blocking_does_not_change_the_answer(device):
+    g = load_golden("akm_small")
+    op = operator(golden_rows(g), 1e-12)
+    a = op.jla_leverages(24, block=8, seed=2)[0].cpu().numpy().copy()
+    b = op.jla_leverages(24, block=24, seed=2)[0].cpu().numpy().copy()
+    c = op.jla_leverages(24, block=5, seed=2)[0].cpu().numpy().copy()
+    assert rel(a, b) < 1e-9 and rel(a, c) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["akm_small", "akm_weighted"])
+def test_projection_with_covariates_matches_oracle(device, name):
+    """The design with the model's covariates (age_squared, age_cubed): the
+    Schur border of inverse.py:182-218."""
+    g = load_golden(name)
+    rows = golden_rows(g)
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), X=rows.V[:, 1:], tol=1e-12)
+    ref = des.project_rows(20, 5, 3, sqrt_weights=rows.w is not None)
+    op = operator(rows, 1e-12, covariates=True)
+    out, _ = op.project(20, seed=5, first_draw=3, sqrt_weights=rows.w is not None)
+    assert rel(out.cpu().numpy(), ref) < 1e-8
+    lev_ref, _, f_ref = des.jla_leverages(40, 16, 7)
+    lev, _, f = op.jla_leverages(40, block=32, seed=7)
+    assert rel(lev.cpu().numpy(), lev_ref) < 1e-8
+    assert rel(f.cpu().numpy(), f_ref) < 1e-8
+
+
+def test_projection_is_idempotent(device):
+    """A S^- A' is a projection: applying it to its own output returns it
+    (tests/test_inverse.py:128 of the reference checks the same)."""
+    import torch
+    g = load_golden("akm_components")
+    rows = golden_rows(g)
+    op = operator(rows, 1e-13)
+    out, _ = op.project(4, seed=3)
+    again, _ = op.center(4, R=out.contiguous()), None
+    rhs, _, sq = again
+    U, _ = op.solve_reduced(rhs, torch.sqrt(sq))
+    out2 = torch.empty_like(out)
+    from hdfe_stream_b200 import _lib
+    _lib.check(_lib.lib().hdfe_rows_project(
+        op.starts.data_ptr(), op.G, op.rows.codes.data_ptr(), len(op.nlev),
+        op.nlev.ctypes.data, None, None, 0, None, U.contiguous().data_ptr(),
+        out.contiguous().data_ptr(), 4, 0, 0, 0, 0, op.N, out2.data_ptr(), None,
+        _lib.stream_handle()))
+    assert rel(out2.cpu().numpy(), out.cpu().numpy()) < 1e-8

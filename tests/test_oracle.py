@@ -117,3 +117,22 @@ def test_project_rows_matches_reference(cells):
     name, g, c = cells
     out = _project(g, c, 11, 6, len(g["w"]) > 0)
     assert rel(out, g["project_rows_seed11"]) < 1e-10
+
+
+def test_design_projection_matches_reference(cells):
+    """The oracle's project_rows (inverse.py:240-309 restated) on the golden
+    projection of seed 11, 6 draws."""
+    name, g, c = cells
+    rows = golden_rows(g)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g["tol"]), nt=int(g["numba_threads"]))
+    out = des.project_rows(6, 11, 0, sqrt_weights=rows.w is not None)
+    assert rel(out, g["project_rows_seed11"]) < 1e-10
+
+
+def test_jla_leverages_match_reference(cells):
+    name, g, c = cells
+    rows = golden_rows(g)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g["tol"]), nt=int(g["numba_threads"]))
+    lev, comp, factor = des.jla_leverages(24, 8, 2)
+    assert rel(lev, g["jla_leverage"]) < 1e-9
+    assert rel(factor, g["jla_factor"]) < 1e-9
