@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-jla", dest="jla", action="store_false",
+                    help="skip the KSS-JLA leverage measurement")
     return ap.parse_args()
 
 
@@ -215,6 +217,9 @@ def run_ours(args, rank, world, local_rank):
                           "rel_fe_err": err}
     accuracy["mixed_speedup"] = round(accuracy["fp64"]["solve_ms"] / accuracy["mixed"]["solve_ms"], 3)
 
+    # KSS-JLA: p = 256 Rademacher probes through A S^- A' on the 1M-worker panel
+    jla = run_jla(args, rank, world, dist) if args.jla else None
+
     # e2e through the public call: pinned host rows up, fixed effects back
     e2e = run_e2e(args, rows, dist)
 
@@ -243,7 +248,7 @@ def run_ours(args, rank, world, local_rank):
                          "frac": roof[dom]["frac"], "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs", "phases": roof},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
-            "accuracy_1e-8": accuracy,
+            "accuracy_1e-8": accuracy, "kss_jla": jla,
             "solve": {"iterations": info["iterations"], "converged": info["converged"],
                       "max_rel_residual": info["max_rel_residual"], "S_nnz": info["S_nnz"],
                       "n_components": info["n_components"]},
@@ -252,6 +257,60 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return out, rows
+
+
+def run_jla(args, rank, world, dist):
+    """JLA leverages for p = 256 probes (blocks of 32) on the 1M-worker panel,
+    the design with the model's covariates: RHS solves per second."""
+    import torch
+    from hdfe_stream_b200 import fit, leaveout
+    from hdfe_stream_b200.simulate import prepare
+
+    rows = prepare("kss_1m", seed=100 + rank)
+    drows = fit.DeviceRows.from_rows(rows)
+    cells = fit.pass1(drows)
+    S = fit.build_s(cells)
+    X = drows.V[1:].T.contiguous()
+    op = leaveout.InverseOperator(drows, cells, S, X, tol=args.tol)
+    p = 256
+    op.jla_leverages(p, block=32, seed=1)          # warm-up (and the border)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    reps = 2
+    a.record()
+    for _ in range(reps):
+        lev, comp, factor = op.jla_leverages(p, block=32, seed=1)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    out = {"workload": "kss_1m: 1M workers, 100k firms, 10 years, largest connected set; "
+                       "log_earn ~ age_squared + age_cubed | worker_id + firm_id",
+           "rows": rows.n_rows, "levels": int(sum(rows.n_levels)), "S_nnz": S.nnz, "draws": p,
+           "block": 32, "ms": round(ms, 3), "value": round(world * p / (ms / 1e3), 2),
+           "unit": "RHS solves/s", "note": "leverages only (the Hutchinson trace's "
+           "two applications per draw are not in this number)",
+           "max_leverage": float(lev.max()), "iterations_last_block": op.jla_info["iterations"]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(REPO / "oracle"))
+        import oracle as orc
+        orc.set_threads(os.cpu_count() or 1)
+        c = orc.pass1(rows)
+        des = orc.Design(rows, c, orc.build_explicit(c), X=rows.V[:, 1:], tol=args.tol)
+        des.border()
+        t0 = time.perf_counter()
+        des.jla_leverages(32, 32, 1)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(32 / dt, 3), "unit": "RHS solves/s",
+                               "cores": orc.num_threads(), "kind": "port",
+                               "sample": "32 of the 256 probes (one block) on the same panel"}
+    return out
 
 
 def run_e2e(args, rows, dist):

@@ -153,9 +153,10 @@ def _rank_codes(values: np.ndarray):
     return codes.astype(np.uint32), levels
 
 
-def pass0_layout(panel: Panel, keep: np.ndarray | None = None) -> Rows:
+def pass0_layout(panel: Panel, keep: np.ndarray | None = None, year_fe: bool = True) -> Rows:
     """Rows of `panel` (optionally only those where `keep`) in pass 0's
-    layout, sorted by (worker, firm, year, variables)."""
+    layout, sorted by (worker, firm, year, variables).  year_fe False: the
+    model has worker and firm effects only (codes (N, 1))."""
     sel = slice(None) if keep is None else np.asarray(keep, bool)
     g, wlev = _rank_codes(panel.worker[sel])
     c1, flev = _rank_codes(panel.firm[sel])
@@ -169,12 +170,12 @@ def pass0_layout(panel: Panel, keep: np.ndarray | None = None) -> Rows:
     if len(sk) > 1 and bool(np.any(sk[1:] == sk[:-1])):
         # rows sharing (worker, firm, year): the variables break the tie
         order = np.lexsort((V[:, 2], V[:, 1], V[:, 0], c2, c1, g))
-    return Rows(gcode=np.ascontiguousarray(g[order]),
-                codes=np.ascontiguousarray(np.column_stack([c1[order], c2[order]])),
+    codes = np.column_stack([c1[order], c2[order]]) if year_fe else c1[order][:, None]
+    return Rows(gcode=np.ascontiguousarray(g[order]), codes=np.ascontiguousarray(codes),
                 V=np.ascontiguousarray(V[order]),
                 w=None if w is None else np.ascontiguousarray(w[order]),
-                n_levels=[len(flev), len(ylev)], n_groups=len(wlev),
-                names=["log_earn", "age_squared", "age_cubed"],
+                n_levels=[len(flev), len(ylev)] if year_fe else [len(flev)],
+                n_groups=len(wlev), names=["log_earn", "age_squared", "age_cubed"],
                 ids={"worker": wlev, "firm": flev, "year": ylev})
 
 
@@ -245,8 +246,15 @@ PANELS = {
 
 def prepare(name: str, seed: int = 0):
     """The named panel's rows in pass 0's layout, restricted as its
-    specification says (akm_5m: largest connected set with min_degree 2)."""
+    specification says: akm_5m the largest connected set after min_degree 2;
+    kss_1m the largest connected set (the leave-one-out pruning's removal of
+    single-observation and articulation-point workers is not applied), with
+    worker and firm effects only (log_earn ~ age_squared + age_cubed |
+    worker_id + firm_id)."""
     spec = dict(PANELS[name])
     panel = simulate_panel(seed=seed, **spec)
-    keep = restrict_connected(panel, (2, 2)) if name == "akm_5m" else None
-    return pass0_layout(panel, keep)
+    if name == "akm_5m":
+        return pass0_layout(panel, restrict_connected(panel, (2, 2)))
+    if name == "kss_1m":
+        return pass0_layout(panel, restrict_connected(panel, (1, 1)), year_fe=False)
+    return pass0_layout(panel)
