@@ -39,8 +39,16 @@
 namespace hdfe {
 namespace pcg {
 
-constexpr int kThreads = 1024;    // one CTA per SM: fewer arrivals at each grid barrier
-constexpr int kWarps = kThreads / 32;
+// One CTA per SM (fewer arrivals at each grid barrier).  Narrow blocks run
+// 1024 threads (64 registers a thread: the most warps in flight); from
+// HDFE_PCG_WIDE_K columns on, a thread's K-wide accumulators and gathered
+// rows no longer fit in 64 registers, so those blocks run 512 threads with up
+// to 128 registers each instead of spilling to local memory.
+#ifndef HDFE_PCG_WIDE_K
+#define HDFE_PCG_WIDE_K 3
+#endif
+__host__ __device__ constexpr int threads_for(int k) { return k >= HDFE_PCG_WIDE_K ? 512 : 1024; }
+constexpr int kMaxWarps = 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kLong = 64;           // nonzeros in a warp's range that make a row "long"
 
@@ -85,9 +93,10 @@ inline Layout layout(int64_t L, int k, int64_t blocks)
     o.r = take(L * k * 8);
     o.p = take(L * kp * 8);
     o.ap = take(L * k * 8);
-    o.carry = take(blocks * kWarps * 2 * k * 8);
+    const int64_t warps = blocks * (threads_for(k) / 32);
+    o.carry = take(warps * 2 * k * 8);
     o.part = take(4 * (int64_t)k * blocks * 8);
-    o.wfirst = take(blocks * kWarps * 8);
+    o.wfirst = take(warps * 8);
     o.cut = take(L);
     o.bar = take(64);
     o.total = p;
@@ -113,6 +122,39 @@ __device__ __forceinline__ double reduce_part(const double *part, int q)
     const double *p = part + (int64_t)q * gridDim.x;
     for (int b = lane; b < (int)gridDim.x; b += 32) s += __ldcg(p + b);
     return warp_sum(s);
+}
+
+constexpr int kRedLoads = 8;            // CTAs per lane in reduce_range: grids up to 256 CTAs
+
+// s_red[q] = sum over CTAs of partial q, for q in [q0, q1): one warp per
+// quantity, the same fixed order in every CTA
+__device__ __forceinline__ void reduce_range(const double *part, int q0, int q1, double *s_red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int nb = gridDim.x;
+    for (int qb = q0 + warp; qb < q1; qb += 4 * nw) {
+        // four quantities per warp at a time, every load issued before the sums
+        double v[4][kRedLoads];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int q = qb + i * nw;
+#pragma unroll
+            for (int u = 0; u < kRedLoads; u++) {
+                const int b = lane + 32 * u;
+                v[i][u] = (q < q1 && b < nb) ? __ldcg(part + (int64_t)q * nb + b) : 0.0;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            double t = 0.0;
+#pragma unroll
+            for (int u = 0; u < kRedLoads; u++) t += v[i][u];
+            t = warp_sum(t);
+            const int q = qb + i * nw;
+            if (lane == 0 && q < q1) s_red[q] = t;
+        }
+    }
+    __syncthreads();
 }
 
 // Row c of V (stride VS) into g[0..K), with vector loads of VW elements
@@ -179,15 +221,16 @@ __device__ __forceinline__ void row_products(const Params &a, const T *vals, con
     }
 }
 
-template <int K, int VS, typename T>
+// vrow: V[row, 0..K), loaded before the row's products (for p'Ap)
+template <int K, typename T>
 __device__ __forceinline__ void finish_row(int64_t row, const T (&acc)[K], int64_t row_st,
                                            int64_t row_en, int64_t lo, int64_t hi, int64_t gw,
-                                           const T *V, T *out, T *carry, double (&dot)[K],
-                                           bool want_dot)
+                                           const T (&vrow)[K], T *out, T *carry,
+                                           double (&dot)[K], bool want_dot)
 {
     if (want_dot) {
 #pragma unroll
-        for (int k = 0; k < K; k++) dot[k] += (double)V[row * VS + k] * (double)acc[k];
+        for (int k = 0; k < K; k++) dot[k] += (double)vrow[k] * (double)acc[k];
     }
     if (row_st >= lo && row_en <= hi) {
 #pragma unroll
@@ -208,7 +251,7 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
                            T *__restrict__ out, T *carry, double (&dot)[K], bool want_dot)
 {
     const int lane = threadIdx.x & 31, sub = lane >> 3, sl = lane & 7;
-    const int64_t gw = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int64_t lo = gw * a.chunk;
     const int64_t hi = min(lo + a.chunk, a.nnz);
     if (lo >= hi) return;
@@ -230,6 +273,10 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
             if ((longmask >> j) & 1u) {
                 // one long row, the whole warp
                 const int64_t rs = __shfl_sync(kFull, cs, j), re = __shfl_sync(kFull, ce, j);
+                T vrow[K];
+#pragma unroll
+                for (int k = 0; k < K; k++)
+                    vrow[k] = (want_dot && lane == 0) ? V[(r0 + j) * VS + k] : T(0);
                 T acc[K];
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = T(0);
@@ -238,8 +285,8 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
                 for (int k = 0; k < K; k++) acc[k] = warp_sum(acc[k]);
                 const int64_t row_st = __shfl_sync(kFull, st, j), row_en = __shfl_sync(kFull, en, j);
                 if (lane == 0)
-                    finish_row<K, VS, T>(r0 + j, acc, row_st, row_en, lo, hi, gw, V, out, carry,
-                                         dot, want_dot);
+                    finish_row<K, T>(r0 + j, acc, row_st, row_en, lo, hi, gw, vrow, out, carry,
+                                     dot, want_dot);
                 j++;
             } else {
                 // up to four short rows, one per 8-lane subgroup, up to the next long row
@@ -251,6 +298,10 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
                 const int64_t rs = __shfl_sync(kFull, cs, src), re = __shfl_sync(kFull, ce, src);
                 const int64_t row_st = __shfl_sync(kFull, st, src);
                 const int64_t row_en = __shfl_sync(kFull, en, src);
+                T vrow[K];
+#pragma unroll
+                for (int k = 0; k < K; k++)
+                    vrow[k] = (want_dot && mine && sl == 0) ? V[(r0 + j + sub) * VS + k] : T(0);
                 T acc[K];
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = T(0);
@@ -262,8 +313,8 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
                     acc[k] += __shfl_xor_sync(kFull, acc[k], 1);
                 }
                 if (mine && sl == 0 && re > rs)
-                    finish_row<K, VS, T>(r0 + j + sub, acc, row_st, row_en, lo, hi, gw, V, out,
-                                         carry, dot, want_dot);
+                    finish_row<K, T>(r0 + j + sub, acc, row_st, row_en, lo, hi, gw, vrow, out,
+                                     carry, dot, want_dot);
                 j += batch;
             }
         }
@@ -279,7 +330,7 @@ template <int K, typename T>
 __device__ bool finish_cut_row(const Params &a, const T *carry, int64_t &row, T (&ap)[K])
 {
     const int lane = threadIdx.x & 31;
-    const int64_t gw = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int64_t lo = gw * a.chunk;
     const int64_t hi = min(lo + a.chunk, a.nnz);
     if (lo >= hi) return false;
@@ -318,22 +369,22 @@ __device__ __forceinline__ void block_partials(double (&v)[N], double *scratch, 
     __syncthreads();
     if (threadIdx.x < N) {
         double t = 0.0;
-        for (int w = 0; w < kWarps; w++) t += scratch[w * N + threadIdx.x];
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += scratch[w * N + threadIdx.x];
         part[(int64_t)(q0 + threadIdx.x) * nb + blockIdx.x] = t;
     }
     __syncthreads();
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(Params a)
+__global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 {
     constexpr int KP = Stride<K>::P;
     __shared__ double s_red[4 * K];
-    __shared__ double s_scratch[kWarps * 3 * K];
+    __shared__ double s_scratch[kMaxWarps * 3 * K];
     GridBarrier gb{a.bar};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t gtid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-    const int64_t gstride = (int64_t)gridDim.x * kThreads;
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
     const int64_t L = a.L;
     const int nb = gridDim.x;
 
@@ -349,7 +400,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(Params a)
     // ---- set-up: each warp's first row and the cut flags (used by the same
     // warps / threads later, so no barrier is needed for them)
     {
-        const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
+        const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
         const int64_t lo = gw * a.chunk;
         if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
         __syncwarp();
@@ -559,7 +610,7 @@ int grid_blocks()
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<K>, kThreads, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<K>, threads_for(K), 0) !=
         cudaSuccess)
         return -1;
     if (per_sm < 1) return -1;
@@ -584,8 +635,9 @@ int grid_blocks_for_uncached(int k)
 // occupancy per (device, k), computed once
 int grid_blocks_for(int k)
 {
-    static int cache[64][HDFE_PCG_MAX_K + 1] = {};
+    static int cache[64][9] = {};
     int dev = 0;
+    if (k < 1 || k > 8) return -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return grid_blocks_for_uncached(k);
     if (cache[dev][k] == 0) cache[dev][k] = grid_blocks_for_uncached(k);
     return cache[dev][k];
@@ -595,8 +647,544 @@ template <int K>
 cudaError_t launch(Params p, int blocks, cudaStream_t s)
 {
     void *args[] = {&p};
-    return cudaLaunchCooperativeKernel((const void *)pcg_kernel<K>, dim3(blocks), dim3(kThreads),
+    return cudaLaunchCooperativeKernel((const void *)pcg_kernel<K>, dim3(blocks), dim3(threads_for(K)),
                                        args, 0, s);
+}
+
+// ------------------------------------------------ one column per lane
+//
+// Wide blocks (the JLA's blocks of probe vectors: up to 32 columns) run with
+// one column per lane instead of K accumulators per thread.  The block is
+// padded to K = 8, 16 or 32 columns (padding columns are zero columns); a
+// row of a vector is then one coalesced load of 8K bytes, a thread holds one
+// accumulator, and all columns share one pass over S's indices and values
+// and one set of grid barriers per iteration.
+//   SpMM: a warp streams its range of nonzeros 32 at a time, H = 32 / K
+//   nonzeros side by side (one per group of K lanes), the rows of V it needs
+//   staged in shared memory by asynchronous copies, several windows ahead.  Row
+//   boundaries are the same in every lane, so the row walk is warp-uniform;
+//   the row ends come 32 at a time from one coalesced load.  A row finishing
+//   inside the range is summed over the H groups and written; a row cut by the
+//   range boundary goes to the warp's carry slots as in pcg_kernel.
+//   Vector phases: one thread per (row, column) element; a thread's column is
+//   fixed (the grid stride is a multiple of 32), so each thread keeps its
+//   column's alpha, beta and partial sums in registers, and the per-column
+//   sums reduce over the lanes of that column, then over warps and CTAs in a
+//   fixed order.
+#ifndef HDFE_PCG_LANE_FROM
+#define HDFE_PCG_LANE_FROM 5            // blocks of at least this many columns
+#endif
+// CTA size per block width: the K = 32 kernel stages 24 KB of gathers per
+// warp, so it runs 8 warps per CTA; narrower ones run 16.
+__host__ __device__ constexpr int lane_threads(int K) { return K >= 32 ? 256 : 512; }
+__host__ __device__ constexpr int lane_ru(int K) { return K >= 32 ? 4 : 2; }  // vector elements per trip
+constexpr int kLaneStages = 3;          // windows of 32 nonzeros in flight per warp
+constexpr uint8_t kRowCut = 1, kRowEmpty = 2;   // per-row flags
+// dynamic shared memory: per warp, kLaneStages x 32 gathered rows of K values
+// and their 32 matrix values
+inline int lane_smem_bytes(int K) { return (lane_threads(K) / 32) * kLaneStages * 32 * (K + 1) * 8; }
+
+inline bool use_lanes(int k) { return k >= HDFE_PCG_LANE_FROM || k > 8; }
+inline int lane_width(int k) { return k <= 8 ? 8 : (k <= 16 ? 16 : 32); }
+
+struct LaneLayout {
+    int64_t r, p, ap, x, carry, part, wfirst, cut, bar, total;
+};
+
+// R, P, AP (L, K); X (L, K) unless the caller's X has K columns already
+inline LaneLayout lane_layout(int64_t L, int k, int64_t blocks)
+{
+    LaneLayout o;
+    const int kw = lane_width(k);
+    const int64_t warps = blocks * (lane_threads(kw) / 32);
+    int64_t p = 0;
+    auto take = [&](int64_t bytes) { int64_t at = p; p += (bytes + 255) / 256 * 256; return at; };
+    o.r = take(L * kw * 8);
+    o.p = take(L * kw * 8);
+    o.ap = take(L * kw * 8);
+    o.x = k == kw ? -1 : take(L * kw * 8);
+    o.carry = take(warps * 2 * kw * 8);
+    o.part = take(3 * (int64_t)kw * blocks * 8);
+    o.wfirst = take(warps * 8);
+    o.cut = take(L);
+    o.bar = take(64);
+    o.total = p;
+    return o;
+}
+
+struct LaneArgs {
+    double *Xw;     // (L, K): the iterate (the caller's X when k == K)
+    int32_t k;      // the caller's columns (B, X0, X have stride k)
+};
+
+// vr = V[r, lane] (lanes < K), loaded when row r began
+template <int K>
+__device__ __forceinline__ void lane_flush(int64_t r, int64_t st, int64_t en, int64_t lo,
+                                           int64_t hi, int64_t gw, double acc, double vr,
+                                           double *out, double *carry, double &dot,
+                                           bool want_dot)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = K; o < 32; o <<= 1) acc += __shfl_xor_sync(kFull, acc, o);
+    if (lane < K) {
+        if (want_dot) dot += vr * acc;
+        if (st >= lo && en <= hi)
+            out[r * K + lane] = acc;
+        else    // cut row: slot 1 in the warp where it starts, 0 elsewhere
+            carry[(gw * 2 + (st >= lo ? 1 : 0)) * K + lane] = acc;
+    }
+}
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// out = S V over this warp's range of nonzeros (rows inside the range); cut
+// rows to the carry slots; dot += V[r, col] (S V)[r, col] in lanes < K.
+// The gathers go through shared memory: for each window of 32 nonzeros the
+// warp issues asynchronous copies (cp.async) of the 32 rows of V it needs,
+// lane (sub, col) copying column col of the rows it will itself multiply,
+// plus the window's matrix values, and keeps kLaneStages windows in flight,
+// so the bytes in flight per SM do not depend on registers.  Row walk and
+// flushes as described above; V[r] for p'Ap is loaded as row r begins.
+template <int K>
+__device__ void lane_spmm(const Params &a, const double *__restrict__ V, double *__restrict__ out,
+                          double *carry, double &dot, bool want_dot, double *stage)
+{
+    constexpr int H = 32 / K, NS = kLaneStages;
+    const int lane = threadIdx.x & 31, col = lane % K, sub = lane / K;
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t lo = gw * a.chunk;
+    const int64_t hi = min(lo + a.chunk, a.nnz);
+    if (lo >= hi) return;
+    double *vals = stage;                   // [NS][32][K]
+    double *wts = stage + NS * 32 * K;      // [NS][32]
+    const int64_t nwin = (hi - lo + 31) / 32;
+    auto load_idx = [&](int64_t w) -> int32_t {
+        const int64_t e = lo + w * 32 + lane;
+        int32_t c = 0;
+        if (w < nwin && e < hi) {
+            c = __ldg(a.indices + e);
+            if (c < 0 || c >= a.L) { GridBarrier{a.bar}.fail(HDFE_ERR_BAD_CODE); c = 0; }
+        }
+        return c;
+    };
+    auto issue = [&](int64_t w, int32_t c) {    // window w's rows and values into its stage
+        if (w < nwin) {
+            const int sgi = (int)(w % NS);
+            const int64_t base = lo + w * 32;
+            const int n = (int)min((int64_t)32, hi - base);
+            double *vs = vals + sgi * 32 * K;
+#pragma unroll
+            for (int u = 0; u < K; u++) {
+                const int t = u * H + sub;
+                const int cc = __shfl_sync(kFull, c, t);
+                if (t < n) cp_async8(vs + t * K + col, V + (int64_t)cc * K + col);
+            }
+            if (lane < n) cp_async8(wts + sgi * 32 + lane, a.data + base + lane);
+        }
+        cp_async_commit();                      // one group per window, empty past the end
+    };
+    int32_t cnext = load_idx(0);
+#pragma unroll
+    for (int w = 0; w < NS - 1; w++) {
+        const int32_t c = cnext;
+        cnext = load_idx(w + 1);
+        issue(w, c);
+    }
+    int64_t r = a.wfirst[gw];
+    int64_t st = a.indptr[r];
+    int64_t rw = r;     // row-end window: lane i holds indptr[rw + 1 + i]
+    int64_t rend = rw + 1 + lane <= a.L ? a.indptr[rw + 1 + lane] : INT64_MAX;
+    int64_t en = __shfl_sync(kFull, rend, 0);
+    double vr = want_dot ? V[r * K + col] : 0.0;
+    double acc = 0.0;
+    for (int64_t w = 0; w < nwin; w++) {
+        {
+            const int32_t c = cnext;
+            cnext = load_idx(w + NS);
+            issue(w + NS - 1, c);
+        }
+        cp_async_wait<NS - 1>();        // window w has landed (this lane's copies) ...
+        __syncwarp();                   // ... and every lane's (the values)
+        const int sgi = (int)(w % NS);
+        const int64_t base = lo + w * 32;
+        const double *vs = vals + sgi * 32 * K;
+        const double *ws = wts + sgi * 32;
+#pragma unroll 8
+        for (int u = 0; u < K; u++) {
+            const int64_t sb = base + u * H;             // this step's first nonzero
+            if (sb >= hi) break;
+            const int t = u * H + sub;
+            const bool valid = sb + sub < hi;
+            const double g = valid ? vs[t * K + col] : 0.0;
+            const double wv = valid ? ws[t] : 0.0;
+            if (sb + H <= en) {                          // the whole step in row r
+                acc += wv * g;
+                continue;
+            }
+            for (int h = 0; h < H; h++) {
+                const int64_t el = sb + h;
+                if (el >= hi) break;
+                while (el >= en) {                       // rows ending before el (empty ones too)
+                    lane_flush<K>(r, st, en, lo, hi, gw, acc, vr, out, carry, dot, want_dot);
+                    acc = 0.0;
+                    r++;
+                    st = en;
+                    if (want_dot) vr = V[r * K + col];
+                    if (r - rw >= 32) {
+                        rw = r;
+                        rend = rw + 1 + lane <= a.L ? a.indptr[rw + 1 + lane] : INT64_MAX;
+                    }
+                    en = __shfl_sync(kFull, rend, (int)(r - rw));
+                }
+                if (sub == h) acc += wv * g;
+            }
+        }
+        __syncwarp();                   // every lane is done with this stage before it is refilled
+    }
+    cp_async_wait<0>();
+    lane_flush<K>(r, st, en, lo, hi, gw, acc, vr, out, carry, dot, want_dot);
+}
+
+// The cut row this warp finishes (its first row, when that row started in an
+// earlier warp and ends in this one): the carry slots of the warps it spans
+// summed in warp order, lane col holding column col.
+template <int K>
+__device__ bool lane_finish_cut(const Params &a, const double *carry, int64_t &row, double &ap)
+{
+    const int col = (threadIdx.x & 31) % K;
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t lo = gw * a.chunk;
+    const int64_t hi = min(lo + a.chunk, a.nnz);
+    if (lo >= hi) return false;
+    const int64_t r = a.wfirst[gw];
+    const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
+    if (!(rs < lo && re <= hi)) return false;
+    const int64_t w0 = rs / a.chunk;
+    double s = 0.0;
+    for (int64_t w = w0; w <= gw; w++) s += __ldcg(carry + (w * 2 + (w == w0 ? 1 : 0)) * K + col);
+    ap = s;
+    row = r;
+    return true;
+}
+
+// Per-CTA sums of N quantities per column: v[i] is this thread's partial of
+// quantity i for its column (lane % K); written as partials (q0 + i) * K + col.
+template <int K, int N>
+__device__ __forceinline__ void column_partials(double (&v)[N], double *scratch, double *part,
+                                                int q0, int nb)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int o = K; o < 32; o <<= 1) v[i] += __shfl_xor_sync(kFull, v[i], o);
+    if (lane < K) {
+#pragma unroll
+        for (int i = 0; i < N; i++) scratch[(i * nw + warp) * K + lane] = v[i];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < N * K; t += blockDim.x) {
+        const int i = t / K, c = t % K;
+        double s = 0.0;
+        for (int w = 0; w < nw; w++) s += scratch[(i * nw + w) * K + c];
+        part[(int64_t)(q0 * K + t) * nb + blockIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+template <int K>
+__global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, LaneArgs x)
+{
+    constexpr int RU = lane_ru(K);
+    extern __shared__ double s_stage[];
+    __shared__ double s_red[3 * K];
+    __shared__ double s_scratch[(lane_threads(K) / 32) * 3 * K];
+    __shared__ double s_bnorm[K], s_rel[K];
+    __shared__ int s_active[K];
+    GridBarrier gb{a.bar};
+    const int lane = threadIdx.x & 31, col = lane % K;
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t L = a.L, LK = a.L * K;
+    const int nb = gridDim.x;
+    const int kc = x.k;
+    double *Xw = x.Xw;
+    const bool zero_c = col >= kc || (a.zero != nullptr && a.zero[col] != 0);
+    double *stage = s_stage + (threadIdx.x >> 5) * kLaneStages * 32 * (K + 1);
+
+    // ---- set-up: each warp's first row and the cut flags
+    {
+        const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        const int64_t lo = gw * a.chunk;
+        if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
+        __syncwarp();
+        for (int64_t r = gtid; r < L; r += gstride) {
+            const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
+            a.cut[r] = (re > rs && (rs / a.chunk) != ((re - 1) / a.chunk) ? kRowCut : 0) |
+                       (re == rs ? kRowEmpty : 0);
+        }
+    }
+    // ---- R = B - S X0 (or B), the zero and padding columns, ||B||, rz
+    double dot = 0.0;
+    if (a.X0 != nullptr) {
+        for (int64_t t = gtid; t < LK; t += gstride)
+            Xw[t] = zero_c ? 0.0 : a.X0[(t / K) * kc + col];
+        if (!gb.sync()) return;
+        lane_spmm<K>(a, Xw, a.AP, a.carry, dot, false, stage);
+        if (!gb.sync()) return;
+    }
+    double rel_c = 0.0, rz_c, bnorm_c;
+    bool active_c = !zero_c;
+    {
+        double v[3] = {0.0, 0.0, 0.0};      // b^2, r^2, r^2 dinv
+        auto setup_row = [&](int64_t r, double ap) {
+            const double di = a.dinv[r];
+            const double b = col < kc ? a.B[r * kc + col] : 0.0;
+            double xv = 0.0, res = b;
+            if (a.X0 != nullptr) { xv = Xw[r * K + col]; res = b - ap; }
+            if (zero_c) { xv = 0.0; res = 0.0; }
+            Xw[r * K + col] = xv;
+            a.R[r * K + col] = res;
+            a.P[r * K + col] = res * di;
+            v[0] += b * b;
+            v[1] += res * res;
+            v[2] += res * res * di;
+        };
+        for (int64_t t = gtid; t < LK; t += gstride) {
+            const int64_t r = t / K;
+            const uint8_t f = a.cut[r];
+            if (a.X0 != nullptr && (f & kRowCut)) continue;
+            setup_row(r, (a.X0 != nullptr && !(f & kRowEmpty)) ? a.AP[t] : 0.0);
+        }
+        if (a.X0 != nullptr) {
+            int64_t r;
+            double ap;
+            if (lane_finish_cut<K>(a, a.carry, r, ap) && lane < K) setup_row(r, ap);
+        }
+        column_partials<K, 3>(v, s_scratch, a.part, 0, nb);
+        if (!gb.sync()) return;
+        reduce_range(a.part, 0, 3 * K, s_red);
+        const double bn = sqrt(s_red[col]);
+        bnorm_c = bn == 0.0 ? 1.0 : bn;
+        rz_c = s_red[2 * K + col];
+        if (a.X0 != nullptr) {
+            rel_c = sqrt(s_red[K + col]) / bnorm_c;
+            active_c = active_c && rel_c > a.tol;
+        }
+        if (threadIdx.x < K) {
+            s_bnorm[col] = bnorm_c;
+            s_rel[col] = rel_c;
+            s_active[col] = active_c ? 1 : 0;
+        }
+    }
+    const bool all_zero = __syncthreads_and(zero_c) != 0;
+    const bool any_active0 = __syncthreads_or(active_c) != 0;
+    int64_t it = 0;
+    const bool done = all_zero || (a.X0 != nullptr && !any_active0);
+    if (!done) {
+        if (!gb.sync()) return;     // the set-up partials are read before phase A reuses them
+        for (it = 1; it <= a.maxiter; it++) {
+            // ---- A: AP = S P, p'Ap
+            dot = 0.0;
+            lane_spmm<K>(a, a.P, a.AP, a.carry, dot, true, stage);
+            {
+                double v[1] = {dot};
+                column_partials<K, 1>(v, s_scratch, a.part, 0, nb);
+            }
+            if (!gb.sync()) return;
+            reduce_range(a.part, 0, K, s_red);
+            const double pap = s_red[col];
+            const double alpha = (active_c && pap > 0.0) ? rz_c / pap : 0.0;
+            // ---- B: X += alpha P, R -= alpha AP, sums of R^2, R^2 dinv
+            double v[2] = {0.0, 0.0};
+            auto step_row = [&](int64_t r, double ap) {
+                const double di = a.dinv[r];
+                const int64_t t = r * K + col;
+                Xw[t] += alpha * a.P[t];
+                const double res = a.R[t] - alpha * ap;
+                a.R[t] = res;
+                v[0] += res * res;
+                v[1] += res * res * di;
+            };
+            // RU elements per thread per trip, all loads first
+            for (int64_t t0 = gtid; t0 < LK; t0 += RU * gstride) {
+                uint8_t f[RU];
+                double ap[RU], pv[RU], xv[RU], rv[RU], di[RU];
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    const int64_t t = t0 + u * gstride;
+                    f[u] = kRowCut;
+                    if (t < LK) {
+                        const int64_t r = t / K;
+                        f[u] = a.cut[r];
+                        ap[u] = a.AP[t];
+                        pv[u] = a.P[t];
+                        xv[u] = Xw[t];
+                        rv[u] = a.R[t];
+                        di[u] = a.dinv[r];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    if (f[u] & kRowCut) continue;       // also the slots past the end
+                    const int64_t t = t0 + u * gstride;
+                    Xw[t] = xv[u] + alpha * pv[u];
+                    const double res = rv[u] - alpha * ((f[u] & kRowEmpty) ? 0.0 : ap[u]);
+                    a.R[t] = res;
+                    v[0] += res * res;
+                    v[1] += res * res * di[u];
+                }
+            }
+            {
+                int64_t r;
+                double ap;
+                if (lane_finish_cut<K>(a, a.carry, r, ap) && lane < K) step_row(r, ap);
+            }
+            column_partials<K, 2>(v, s_scratch, a.part, 1, nb);
+            if (!gb.sync()) return;
+            reduce_range(a.part, K, 3 * K, s_red);
+            // ---- C: convergence, beta, P = dinv R + beta P
+            rel_c = sqrt(s_red[K + col]) / bnorm_c;
+            active_c = rel_c > a.tol;
+            if (threadIdx.x < K) {
+                s_rel[col] = rel_c;
+                s_active[col] = active_c ? 1 : 0;
+            }
+            if (!__syncthreads_or(active_c)) break;
+            const double rzn = s_red[2 * K + col];
+            const double beta = active_c ? rzn / (rz_c != 0.0 ? rz_c : 1.0) : 0.0;
+            rz_c = rzn;
+            for (int64_t t0 = gtid; t0 < LK; t0 += RU * gstride) {
+                double rv[RU], pv[RU], di[RU];
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    const int64_t t = t0 + u * gstride;
+                    if (t < LK) {
+                        rv[u] = a.R[t];
+                        pv[u] = a.P[t];
+                        di[u] = a.dinv[t / K];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    const int64_t t = t0 + u * gstride;
+                    if (t < LK) a.P[t] = rv[u] * di[u] + beta * pv[u];
+                }
+            }
+            if (!gb.sync()) return;
+        }
+        if (it > a.maxiter) it = a.maxiter;
+    }
+    // ---- the iterate to the caller's X (stride k)
+    if (Xw != a.X) {
+        for (int64_t t = gtid; t < LK; t += gstride)
+            if (col < kc) a.X[(t / K) * kc + col] = Xw[t];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double mx = 0.0;
+        bool conv = true;
+        for (int c = 0; c < kc; c++) {
+            mx = fmax(mx, s_rel[c]);
+            conv &= s_active[c] == 0;
+        }
+        if (all_zero) { conv = true; mx = 0.0; }
+        a.info->iterations = it;
+        a.info->converged = conv ? 1 : 0;
+        a.info->status = HDFE_OK;
+        a.info->max_rel = mx;
+    }
+}
+
+template <int K>
+int lane_grid()
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+    if (cudaFuncSetAttribute(lane_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             lane_smem_bytes(K)) != cudaSuccess)
+        return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel<K>, lane_threads(K),
+                                                      lane_smem_bytes(K)) != cudaSuccess)
+        return -1;
+    return per_sm < 1 ? -1 : sms;
+}
+
+int lane_grid_for(int kw)
+{
+    static int cache[64][3] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    const int i = kw == 8 ? 0 : (kw == 16 ? 1 : 2);
+    if (cache[dev][i] == 0)
+        cache[dev][i] = kw == 8 ? lane_grid<8>() : (kw == 16 ? lane_grid<16>() : lane_grid<32>());
+    return cache[dev][i];
+}
+
+template <int K>
+cudaError_t launch_lanes(Params p, LaneArgs x, int blocks, cudaStream_t s)
+{
+    void *args[] = {&p, &x};
+    return cudaLaunchCooperativeKernel((const void *)lane_kernel<K>, dim3(blocks),
+                                       dim3(lane_threads(K)), args, lane_smem_bytes(K), s);
+}
+
+int solve_lanes(const int64_t *indptr, const int32_t *indices, const double *data, int64_t L,
+                int64_t nnz, const double *dinv, const double *B, int32_t k, const uint8_t *zero,
+                const double *X0, double tol, int64_t maxiter, double *X, void *workspace,
+                int64_t workspace_bytes, hdfe_pcg_info *info, cudaStream_t s)
+{
+    const int kw = lane_width(k);
+    const int blocks = lane_grid_for(kw);
+    if (blocks < 1) return hdfe_set_cuda_error(cudaGetLastError());
+    const LaneLayout lay = lane_layout(L, k, blocks);
+    if (workspace_bytes < lay.total)
+        return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_pcg_solve: workspace too small");
+    char *ws = (char *)workspace;
+    Params p{};
+    p.indptr = indptr;
+    p.indices = indices;
+    p.data = data;
+    p.L = L;
+    p.nnz = nnz;
+    const int64_t warps = (int64_t)blocks * (lane_threads(kw) / 32);
+    p.chunk = nnz > 0 ? (nnz + warps - 1) / warps : 1;
+    p.dinv = dinv;
+    p.B = B;
+    p.zero = zero;
+    p.X0 = X0;
+    p.tol = tol;
+    p.maxiter = maxiter;
+    p.X = X;
+    p.R = (double *)(ws + lay.r);
+    p.P = (double *)(ws + lay.p);
+    p.AP = (double *)(ws + lay.ap);
+    p.carry = (double *)(ws + lay.carry);
+    p.part = (double *)(ws + lay.part);
+    p.wfirst = (int64_t *)(ws + lay.wfirst);
+    p.cut = (uint8_t *)(ws + lay.cut);
+    p.bar = (unsigned *)(ws + lay.bar);
+    p.info = info;
+    LaneArgs x;
+    x.Xw = lay.x < 0 ? X : (double *)(ws + lay.x);
+    x.k = k;
+    HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
+    cudaError_t e = kw == 8 ? launch_lanes<8>(p, x, blocks, s)
+                  : kw == 16 ? launch_lanes<16>(p, x, blocks, s)
+                             : launch_lanes<32>(p, x, blocks, s);
+    HDFE_CUDA_TRY(e);
+    pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);
+    HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(2);
+    return HDFE_OK;
 }
 
 }  // namespace pcg
@@ -608,6 +1196,10 @@ extern "C" int64_t hdfe_pcg_workspace_bytes(int64_t L, int64_t nnz, int32_t k)
 {
     (void)nnz;
     if (k < 1 || k > HDFE_PCG_MAX_K || L < 0) return -1;
+    if (pcg::use_lanes(k)) {
+        const int blocks = pcg::lane_grid_for(pcg::lane_width(k));
+        return blocks < 1 ? -1 : pcg::lane_layout(L, k, blocks).total;
+    }
     int blocks = pcg::grid_blocks_for(k);
     if (blocks < 1) return -1;
     return pcg::layout(L, k, blocks).total;
@@ -625,6 +1217,9 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
         return hdfe_set_arg_error("hdfe_pcg_solve: workspace must be 256-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
+    if (pcg::use_lanes(k)) return pcg::solve_lanes(indptr, indices, data, L, nnz, dinv, B, k, zero,
+                                                   X0, tol, maxiter, X, workspace,
+                                                   workspace_bytes, info, s);
     int blocks = pcg::grid_blocks_for(k);
     if (blocks < 1) return hdfe_set_cuda_error(cudaGetLastError());
     pcg::Layout lay = pcg::layout(L, k, blocks);
@@ -637,7 +1232,7 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     p.data = data;
     p.L = L;
     p.nnz = nnz;
-    const int64_t warps = (int64_t)blocks * pcg::kWarps;
+    const int64_t warps = (int64_t)blocks * (pcg::threads_for(k) / 32);
     p.chunk = nnz > 0 ? (nnz + warps - 1) / warps : 1;
     p.dinv = dinv;
     p.B = B;
@@ -761,9 +1356,10 @@ inline MixedLayout mixed_layout(int64_t L, int k, int64_t blocks)
     o.ap = take(L * k * 4);
     o.d = take(L * k * 4);
     o.ax = take(L * k * 8);
-    o.carry = take(blocks * kWarps * 2 * k * 8);
+    const int64_t warps = blocks * (threads_for(k) / 32);
+    o.carry = take(warps * 2 * k * 8);
     o.part = take(4 * (int64_t)k * blocks * 8);
-    o.wfirst = take(blocks * kWarps * 8);
+    o.wfirst = take(warps * 8);
     o.cut = take(L);
     o.bar = take(64);
     o.total = p;
@@ -771,16 +1367,16 @@ inline MixedLayout mixed_layout(int64_t L, int k, int64_t blocks)
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Params a, Mixed f)
+__global__ void __launch_bounds__(threads_for(K), 1) mixed_kernel(Params a, Mixed f)
 {
     constexpr int KF = FStride<K>::P;
     constexpr int VWF = FStride<K>::VW;
     __shared__ double s_red[4 * K];
-    __shared__ double s_scratch[kWarps * 3 * K];
+    __shared__ double s_scratch[kMaxWarps * 3 * K];
     GridBarrier gb{a.bar};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t gtid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-    const int64_t gstride = (int64_t)gridDim.x * kThreads;
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
     const int64_t L = a.L;
     const int nb = gridDim.x;
     float *carry32 = reinterpret_cast<float *>(a.carry);
@@ -795,7 +1391,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(Params a, Mixed f)
     }
     // each warp's first row and the cut flags, X = X0 (or 0), ||B||
     {
-        const int64_t gw = (int64_t)blockIdx.x * kWarps + warp;
+        const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
         const int64_t lo = gw * a.chunk;
         if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
         __syncwarp();
@@ -1031,7 +1627,7 @@ int mixed_grid()
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel<K>, kThreads, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel<K>, threads_for(K), 0) !=
         cudaSuccess)
         return -1;
     return per_sm < 1 ? -1 : sms;
@@ -1039,7 +1635,7 @@ int mixed_grid()
 
 int mixed_grid_for(int k)
 {
-    static int cache[64][HDFE_PCG_MAX_K + 1] = {};
+    static int cache[64][HDFE_PCG_MIXED_MAX_K + 1] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
     if (cache[dev][k] == 0) {
@@ -1063,7 +1659,7 @@ cudaError_t launch_mixed(Params p, Mixed m, int blocks, cudaStream_t s)
 {
     void *args[] = {&p, &m};
     return cudaLaunchCooperativeKernel((const void *)mixed_kernel<K>, dim3(blocks),
-                                       dim3(kThreads), args, 0, s);
+                                       dim3(threads_for(K)), args, 0, s);
 }
 
 }  // namespace pcg
@@ -1072,7 +1668,7 @@ cudaError_t launch_mixed(Params p, Mixed m, int blocks, cudaStream_t s)
 extern "C" int64_t hdfe_pcg_mixed_workspace_bytes(int64_t L, int64_t nnz, int32_t k)
 {
     (void)nnz;
-    if (k < 1 || k > HDFE_PCG_MAX_K || L < 0) return -1;
+    if (k < 1 || k > HDFE_PCG_MIXED_MAX_K || L < 0) return -1;
     const int blocks = pcg::mixed_grid_for(k);
     if (blocks < 1) return -1;
     return pcg::mixed_layout(L, k, blocks).total;
@@ -1086,7 +1682,7 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
                                     void *workspace, int64_t workspace_bytes,
                                     hdfe_pcg_info *info, void *stream)
 {
-    if (k < 1 || k > HDFE_PCG_MAX_K || L < 1 || nnz < 0 || !indptr || !dinv || !B || !X ||
+    if (k < 1 || k > HDFE_PCG_MIXED_MAX_K || L < 1 || nnz < 0 || !indptr || !dinv || !B || !X ||
         !info || !workspace || maxiter < 0 || !(inner_tol > 0.0 && inner_tol < 1.0) ||
         (nnz > 0 && (!indices || !data || !data32)))
         return hdfe_set_arg_error("hdfe_pcg_solve_mixed: bad argument");
@@ -1105,7 +1701,7 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
     p.data = data;
     p.L = L;
     p.nnz = nnz;
-    const int64_t warps = (int64_t)blocks * pcg::kWarps;
+    const int64_t warps = (int64_t)blocks * (pcg::threads_for(k) / 32);
     p.chunk = nnz > 0 ? (nnz + warps - 1) / warps : 1;
     p.dinv = dinv;
     p.B = B;

@@ -152,8 +152,9 @@ class BlockSolver:
         X = torch.empty_like(B)
         its, conv, rel = 0, True, 0.0
         zero = None if zero is None else np.asarray(zero, bool)
-        for j0 in range(0, k, _lib.PCG_MAX_K):
-            j1 = min(k, j0 + _lib.PCG_MAX_K)
+        width = _lib.PCG_MIXED_MAX_K if self.precision == "mixed" else _lib.PCG_MAX_K
+        for j0 in range(0, k, width):
+            j1 = min(k, j0 + width)
             Bj = B[:, j0:j1].contiguous()
             Xj = torch.empty_like(Bj)
             X0j = None if X0 is None else X0[:, j0:j1].to(self.dev, torch.float64).contiguous()

@@ -221,8 +221,15 @@ typedef struct hdfe_pcg_info {
     double max_rel;       /* max over columns of ||R|| / ||B|| at exit */
 } hdfe_pcg_info;
 
-/* Largest k (right-hand-side columns per solve) hdfe_pcg_solve accepts. */
-#define HDFE_PCG_MAX_K 8
+/* Largest k (right-hand-side columns per solve) hdfe_pcg_solve accepts.
+ * Blocks of up to 4 columns keep each row's k values in one thread's
+ * registers; wider blocks (the JLA's probe blocks) run one column per lane,
+ * padded to 8, 16 or 32 columns, so every column of the block shares one
+ * pass over S per iteration. */
+#define HDFE_PCG_MAX_K 32
+
+/* Largest k hdfe_pcg_solve_mixed accepts. */
+#define HDFE_PCG_MIXED_MAX_K 8
 
 /* Device workspace bytes hdfe_pcg_solve needs (for the current device). */
 int64_t hdfe_pcg_workspace_bytes(int64_t L, int64_t nnz, int32_t k);

@@ -40,6 +40,7 @@ def test_bad_arguments_are_rejected_without_a_device():
     # k out of range: rejected before any CUDA call
     assert _lib.lib().hdfe_pcg_workspace_bytes(10, 10, 0) == -1
     assert _lib.lib().hdfe_pcg_workspace_bytes(10, 10, _lib.PCG_MAX_K + 1) == -1
+    assert _lib.lib().hdfe_pcg_mixed_workspace_bytes(10, 10, _lib.PCG_MIXED_MAX_K + 1) == -1
     st = _lib.lib().hdfe_pcg_solve(None, None, None, 0, 0, None, None, 3, None, None, 1e-10,
                                    10, None, None, 0, None, None)
     assert st == _lib.HDFE_ERR_ARG

@@ -44,7 +44,7 @@ def test_pcg_matches_oracle_on_golden(device, name):
         assert rel <= tol
 
 
-@pytest.mark.parametrize("k", [1, 3, 8, 11])
+@pytest.mark.parametrize("k", [1, 3, 4, 5, 8, 11, 16, 23, 32])
 def test_pcg_widths(device, k):
     from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
     rows = pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(8, 8), p_move=0.1, seed=7))
@@ -55,6 +55,57 @@ def test_pcg_widths(device, k):
     X_ref, it_ref, ok_ref, _ = orc.pcg(S, orc.jacobi(c.diag), b, None, None, 1e-10)
     X, it, ok, rel = _solvers(S, c.diag, 1e-10)(b)
     assert ok and ok_ref and abs(it - it_ref) <= 1
+    assert np.max(np.abs(X - X_ref)) < 1e-8 * np.max(np.abs(X_ref))
+
+
+@pytest.mark.parametrize("k", [7, 13, 32])
+def test_pcg_wide_zero_columns_and_warm_start(device, k):
+    """Blocks solved one column per lane: zero columns stay 0, a warm start
+    is honoured, and every column matches the oracle's CG."""
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    rows = pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(8, 8), p_move=0.1, seed=11))
+    c = orc.pass1(rows)
+    S = orc.build_explicit(c)
+    rng = np.random.default_rng(100 + k)
+    b = orc.csr_matmat(S, rng.standard_normal((c.L, k)))
+    zero = np.zeros(k, bool)
+    zero[[1, k - 1]] = True
+    x0 = 0.5 * rng.standard_normal((c.L, k))
+    solve = _solvers(S, c.diag, 1e-10)
+    for guess in (None, x0):
+        X_ref, it_ref, ok_ref, _ = orc.pcg(S, orc.jacobi(c.diag), b, zero, guess, 1e-10)
+        X, it, ok, rel = solve(b, zero, guess)
+        assert ok and ok_ref and abs(it - it_ref) <= 1 and rel <= 1e-10
+        assert np.all(X[:, zero] == 0.0)
+        assert np.max(np.abs(X - X_ref)) < 1e-8 * np.max(np.abs(X_ref))
+
+
+def test_pcg_wide_golden_and_deterministic(device):
+    """The golden right-hand sides repeated to 32 columns: each copy solves
+    like the narrow kernel's, and two solves give identical bits."""
+    g = load_golden("akm_small")
+    S = (g["S_indptr"], g["S_indices"], g["S_data"])
+    reps = -(-32 // g["pcg_b"].shape[1])
+    b = np.tile(g["pcg_b"], (1, reps))[:, :32]
+    zero = np.tile(g["pcg_zero"], reps)[:32]
+    solve = _solvers(S, g["diag"], 1e-12)
+    X_ref, it_ref, ok_ref, _ = orc.pcg(S, orc.jacobi(g["diag"]), b, zero, None, 1e-12)
+    X1, it, ok, rel = solve(b, zero)
+    X2, *_ = solve(b, zero)
+    assert ok and abs(it - it_ref) <= 1
+    assert np.array_equal(X1, X2)
+    assert np.max(np.abs(X1 - X_ref)) < 1e-8 * np.max(np.abs(X_ref))
+
+
+def test_pcg_wide_maxiter(device):
+    g = load_golden("akm_small")
+    S = (g["S_indptr"], g["S_indices"], g["S_data"])
+    b = np.tile(g["pcg_b"], (1, 8))[:, :20]
+    X, it, ok, rel = _solvers(S, g["diag"], 1e-12, maxiter=3)(b)
+    X_ref, it_ref, ok_ref, rel_ref = orc.pcg(S, orc.jacobi(g["diag"]), b, None, None, 1e-12,
+                                             maxiter=3)
+    assert it == it_ref == 3 and not ok and not ok_ref
+    assert rel == pytest.approx(rel_ref, rel=1e-6)
     assert np.max(np.abs(X - X_ref)) < 1e-8 * np.max(np.abs(X_ref))
 
 
