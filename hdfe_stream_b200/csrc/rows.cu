@@ -10,17 +10,21 @@
 // `_nb_rademacher`, never stored -- or explicit row vectors (the covariates
 // themselves, for the Schur border).  Rows come grouped by the streamed
 // dimension; a sub-warp of Bp lanes (Bp = the draw count rounded up to 8, 16
-// or 32) takes one group, lane j one draw, so every group mean and scatter is
-// a per-lane loop over the group's rows:
+// or 32) takes one group, lane j one draw.  The group's rows are staged 32 at
+// a time in shared memory (codes, covariates; weights in registers), loaded
+// lane-parallel; the draws' signs of a group's first chunk are kept as bits
+// between its two passes.
 //   center   acc[level, j] += w_i (R_ij - Rbar_gj)  over the group's rows, for
-//            each non-streamed dimension; acc_x[c, j] += X_ic w_i (R_ij -
-//            Rbar_gj); sum w R^2 per draw.  Levels of small dimensions are
+//            each non-streamed dimension, summed over each run of rows with
+//            equal codes and added once per run; acc_x[c, j] += X_ic w_i (R_ij
+//            - Rbar_gj); sum w R^2 per draw.  Levels of small dimensions are
 //            accumulated in shared memory per CTA.
-//   project  h_ij = sum_d U[level_d(i), j] + X_i . C[:, j]; Ubar = weighted
-//            group mean of (R - h); out_ij = h_ij + Ubar (times sqrt(w_i) in
-//            the square-root weight metric), and the JLA sink's five running
-//            sums per row: P = out^2, M = (r - out)^2, P^2, M^2, P M, summed
-//            over the block's draws in draw order.
+//   project  h_ij = sum_d U[level_d(i), j] (read once per run) + X_i . C[:, j];
+//            Ubar = weighted group mean of (R - h); out_ij = h_ij + Ubar
+//            (times sqrt(w_i) in the square-root weight metric), and the JLA
+//            sink's five running sums per row: P = out^2, M = (r - out)^2, P^2,
+//            M^2, P M, summed over the block's draws in draw order (through a
+//            shared-memory transpose: lane t sums row t).
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -70,148 +74,382 @@ struct Args {
     unsigned *status;
 };
 
-__device__ __forceinline__ double row_vec(const Args &a, int64_t i, int j)
+// The sign of `rademacher` from precomputed row and draw terms: the last
+// step of splitmix64 (x ^= x >> 31) leaves bit 63 alone, so the draw is -1
+// exactly when bit 63 is set before it.
+__device__ __forceinline__ bool rad_negative(uint64_t seed, uint64_t rterm, uint64_t dterm)
 {
-    if (a.R) return a.R[i * a.B + j];
-    return rademacher(a.seed, a.ordinal0 + i, a.first_draw + j);
+    uint64_t x = seed ^ rterm ^ dterm;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return (x >> 63) != 0;
 }
 
-// the weight metric: the vectors enter scaled by w^(-1/2) (inverse.py:280-281)
-__device__ __forceinline__ double inv_root(const Args &a, double wi)
+constexpr uint64_t kRowMul = 0x9E3779B97F4A7C15ull, kDrawMul = 0xBF58476D1CE4E5B9ull;
+constexpr int kPassThreads = 128;
+
+// Per sub-warp staging of a chunk of up to BP rows: codes (BP x D) and
+// covariates (BP x c), loaded lane-parallel (lane t: row i0 + t) and read by
+// every lane from shared memory; the weights stay in registers (shuffled).
+template <int BP>
+struct Chunk {
+    static constexpr int kBytes = BP * (HDFE_MAX_DIMS * 4 + kMaxCov * 8);
+    uint32_t *codes;    // [BP][D]
+    double *x;          // [BP][c]
+};
+
+// a sub-warp of BP lanes: lane j holds draw j of the block (on: j < B)
+template <int BP>
+struct Lanes {
+    int lane, j, sub;
+    unsigned mask;
+    bool on;
+    __device__ Lanes(int B)
+    {
+        lane = threadIdx.x & 31;
+        j = lane % BP;
+        sub = lane / BP;
+        mask = BP == 32 ? 0xffffffffu : (((1u << BP) - 1u) << (sub * BP));
+        on = j < B;
+    }
+};
+
+// Load rows [i0, i0 + n) of the group into the chunk (lane t: row i0 + t):
+// codes (checked: an out-of-range code is reported and read as 0) and
+// covariates; returns this lane's row weight (1 without weights).
+template <int BP>
+__device__ __forceinline__ double load_chunk(const Args &a, const Lanes<BP> &ln, Chunk<BP> &ch,
+                                             int64_t i0, int n)
 {
-    if (!a.sqrt_weights) return 1.0;
-    const double r = sqrt(wi);
-    return r > 0.0 ? 1.0 / r : 0.0;
+    double w = 1.0;
+    if (ln.j < n) {
+        const int64_t i = i0 + ln.j;
+        if (a.w) w = a.w[i];
+        for (int d = 0; d < a.D; d++) {
+            uint32_t code = a.codes[i * a.D + d];
+            if ((int64_t)code >= a.nlev[d]) {
+                if (a.status) atomicCAS(a.status, 0u, (unsigned)HDFE_ERR_BAD_CODE);
+                code = 0;
+            }
+            ch.codes[ln.j * a.D + d] = code;
+        }
+        for (int c = 0; c < a.c; c++) ch.x[ln.j * a.c + c] = a.X[i * a.c + c];
+    }
+    __syncwarp(ln.mask);
+    return w;
 }
 
-__global__ void __launch_bounds__(kThreads) k_center(Args a)
+// codes of chunk row q equal to the previous row's (prev)
+__device__ __forceinline__ bool same_codes(const Args &a, const uint32_t *codes, int q,
+                                           const uint32_t (&prev)[HDFE_MAX_DIMS])
 {
-    extern __shared__ double s_acc[];
-    const int lane = threadIdx.x & 31;
-    const int j = lane % a.Bp, sub = lane / a.Bp, per_warp = 32 / a.Bp;
-    const int64_t nsm = a.n_small * a.B;
-    for (int64_t k = threadIdx.x; k < nsm; k += kThreads) s_acc[k] = 0.0;
+    bool same = true;
+#pragma unroll
+    for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+        if (d >= a.D) break;
+        same &= codes[q * a.D + d] == prev[d];
+    }
+    return same;
+}
+
+__device__ __forceinline__ void take_codes(const Args &a, const uint32_t *codes, int q,
+                                           uint32_t (&prev)[HDFE_MAX_DIMS])
+{
+#pragma unroll
+    for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+        if (d >= a.D) break;
+        prev[d] = codes[q * a.D + d];
+    }
+}
+
+__device__ __forceinline__ double inv_root(const Args &a, double w)
+{
+    return a.sqrt_weights ? (w > 0.0 ? 1.0 / sqrt(w) : 0.0) : 1.0;
+}
+
+// `_nb_center_rows` for one sub-warp of BP lanes per group (lane j: draw j).
+// Pass 1 over the group's rows: sum w, sum w r, sum w r^2, with the draws'
+// signs kept as bits for the group's first chunk; pass 2: v = w (r - mean)
+// summed over each run of rows with equal codes and added once per run to
+// every dimension's level (shared-memory copies for small dimensions), and
+// the covariate block per row.
+template <int BP>
+__global__ void __launch_bounds__(kPassThreads) k_center(Args a)
+{
+    extern __shared__ double s_dyn[];
+    constexpr int SUBS = kPassThreads / BP;
+    double *s_acc = s_dyn;                                          // small dimensions
+    char *s_chunks = reinterpret_cast<char *>(s_dyn + a.n_small * a.B);
+    const Lanes<BP> ln(a.B);
+    const int subw = threadIdx.x / BP;
+    Chunk<BP> ch;
+    ch.codes = reinterpret_cast<uint32_t *>(s_chunks + subw * Chunk<BP>::kBytes);
+    ch.x = reinterpret_cast<double *>(s_chunks + subw * Chunk<BP>::kBytes + BP * HDFE_MAX_DIMS * 4);
+    for (int64_t k = threadIdx.x; k < a.n_small * a.B; k += kPassThreads) s_acc[k] = 0.0;
     __syncthreads();
-    const bool on = j < a.B;
+    const uint64_t dterm = (uint64_t)(a.first_draw + ln.j) * kDrawMul;
     double sq = 0.0;
     double ax[kMaxCov];
-    for (int c = 0; c < a.c; c++) ax[c] = 0.0;
-    const int64_t gsub = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / 32 * per_warp + sub;
-    const int64_t nsub = (int64_t)gridDim.x * kThreads / 32 * per_warp;
-    for (int64_t g = gsub; g < a.G; g += nsub) {
+#pragma unroll
+    for (int c = 0; c < kMaxCov; c++) ax[c] = 0.0;
+    auto flush = [&](const uint32_t (&codes)[HDFE_MAX_DIMS], double v) {
+        if (!ln.on) return;
+#pragma unroll
+        for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+            if (d >= a.D) break;
+            if (a.small[d]) atomicAdd(s_acc + (a.soff[d] + codes[d]) * a.B + ln.j, v);
+            else atomicAdd(a.acc + (a.offs[d] + codes[d]) * a.B + ln.j, v);
+        }
+    };
+    const int64_t g0 = (int64_t)blockIdx.x * SUBS + subw, gstep = (int64_t)gridDim.x * SUBS;
+    for (int64_t g = g0; g < a.G; g += gstep) {
         const int64_t s = a.starts[g], e = a.starts[g + 1];
+        const int n = (int)(e - s);
+        // pass 1
         double sw = 0.0, tot = 0.0;
-        for (int64_t i = s; i < e; i++) {
-            const double wi = a.w ? a.w[i] : 1.0;
-            sw += wi;
-            if (on) {
-                const double r = row_vec(a, i, j) * inv_root(a, wi);
-                tot += wi * r;
-                sq += wi * r * r;
+        uint32_t bits = 0;
+        double wl = 1.0, irl = 1.0;
+        for (int c0 = 0; c0 < n; c0 += BP) {
+            const int m = min(BP, n - c0);
+            wl = load_chunk<BP>(a, ln, ch, s + c0, m);
+            irl = inv_root(a, wl);
+            for (int q = 0; q < m; q++) {
+                const double wi = __shfl_sync(ln.mask, wl, q, BP);
+                const double ir = __shfl_sync(ln.mask, irl, q, BP);
+                sw += wi;
+                if (ln.on) {
+                    double r;
+                    const int64_t i = s + c0 + q;
+                    if (a.R) {
+                        r = a.R[i * a.B + ln.j] * ir;
+                    } else {
+                        const bool neg =
+                            rad_negative(a.seed, (uint64_t)(a.ordinal0 + i) * kRowMul, dterm);
+                        if (c0 == 0 && neg) bits |= 1u << q;
+                        r = neg ? -ir : ir;
+                    }
+                    tot += wi * r;
+                    sq += wi * r * r;
+                }
             }
+            if (c0 + BP < n) __syncwarp(ln.mask);     // the next chunk reuses the staging
         }
-        if (!(sw > 0.0) || !on) continue;
+        if (!(sw > 0.0)) continue;
         const double mean = tot / sw;
-        for (int64_t i = s; i < e; i++) {
-            const double wi = a.w ? a.w[i] : 1.0;
-            const double r = row_vec(a, i, j) * inv_root(a, wi);
-            const double v = wi * (r - mean);
-            for (int d = 0; d < a.D; d++) {
-                uint32_t code = a.codes[i * a.D + d];
-                if ((int64_t)code >= a.nlev[d]) { atomicCAS(a.status, 0u, (unsigned)HDFE_ERR_BAD_CODE); code = 0; }
-                if (a.small[d]) atomicAdd(s_acc + (a.soff[d] + code) * a.B + j, v);
-                else atomicAdd(a.acc + (a.offs[d] + code) * a.B + j, v);
+        // pass 2 (a group of one chunk keeps its staged rows and weights)
+        uint32_t prev[HDFE_MAX_DIMS] = {0, 0, 0, 0};
+        double run = 0.0;
+        bool have = false;
+        for (int c0 = 0; c0 < n; c0 += BP) {
+            const int m = min(BP, n - c0);
+            if (n > BP) {
+                __syncwarp(ln.mask);
+                wl = load_chunk<BP>(a, ln, ch, s + c0, m);
+                irl = inv_root(a, wl);
             }
-            for (int c = 0; c < a.c; c++) ax[c] += a.X[i * a.c + c] * v;
+            for (int q = 0; q < m; q++) {
+                const double wi = __shfl_sync(ln.mask, wl, q, BP);
+                const double ir = __shfl_sync(ln.mask, irl, q, BP);
+                if (have && !same_codes(a, ch.codes, q, prev)) {
+                    flush(prev, run);
+                    run = 0.0;
+                }
+                take_codes(a, ch.codes, q, prev);
+                have = true;
+                if (!ln.on) continue;
+                const int64_t i = s + c0 + q;
+                double r;
+                if (a.R) {
+                    r = a.R[i * a.B + ln.j] * ir;
+                } else {
+                    const bool neg =
+                        c0 == 0 ? ((bits >> q) & 1u) != 0
+                                : rad_negative(a.seed, (uint64_t)(a.ordinal0 + i) * kRowMul, dterm);
+                    r = neg ? -ir : ir;
+                }
+                const double v = wi * (r - mean);
+                run += v;
+#pragma unroll
+                for (int c = 0; c < kMaxCov; c++) {
+                    if (c >= a.c) break;
+                    ax[c] += ch.x[q * a.c + c] * v;
+                }
+            }
         }
+        if (have) flush(prev, run);
+        __syncwarp(ln.mask);
     }
     // the covariate block and the sums of squares: per lane, then per CTA
-    if (a.acc_x && j < a.B)
-        for (int c = 0; c < a.c; c++) atomicAdd(a.acc_x + c * a.B + j, ax[c]);
-    if (a.squares && j < a.B) atomicAdd(a.squares + j, sq);
+    if (a.acc_x && ln.on) {
+#pragma unroll
+        for (int c = 0; c < kMaxCov; c++) {
+            if (c >= a.c) break;
+            atomicAdd(a.acc_x + c * a.B + ln.j, ax[c]);
+        }
+    }
+    if (a.squares && ln.on) atomicAdd(a.squares + ln.j, sq);
     __syncthreads();
     for (int d = 0; d < a.D; d++) {
         if (!a.small[d]) continue;
-        for (int64_t q = threadIdx.x; q < a.nlev[d] * a.B; q += kThreads) {
+        for (int64_t q = threadIdx.x; q < a.nlev[d] * a.B; q += kPassThreads) {
             const double v = s_acc[a.soff[d] * a.B + q];
             if (v != 0.0) atomicAdd(a.acc + a.offs[d] * a.B + q, v);
         }
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_project(Args a)
+// `_nb_project_rows` and the JLA sink, one sub-warp of BP lanes per group.
+// h_ij = sum_d U[level_d(i), j] (loaded once per run of equal codes) +
+// X_i . C[:, j]; pass 1: the weighted group mean of r - h; pass 2: the
+// projection o_ij (times sqrt(w_i) in the square-root weight metric), written
+// to out and/or turned into the sink's P = o^2 and M = (r - o)^2.  The five
+// per-row sums over the block's draws go through shared memory: each lane
+// stores its P and M for up to MR rows, then lane t sums row t's values in
+// draw order and adds them to the running moments.
+template <int BP>
+__global__ void __launch_bounds__(kPassThreads) k_project(Args a)
 {
-    const int lane = threadIdx.x & 31;
-    const int j = lane % a.Bp, sub = lane / a.Bp, per_warp = 32 / a.Bp;
-    const bool on = j < a.B;
-    const unsigned smask = a.Bp == 32 ? 0xffffffffu : (((1u << a.Bp) - 1u) << (sub * a.Bp));
-    double Cj[kMaxCov];
-    for (int c = 0; c < a.c; c++) Cj[c] = on ? a.C[c * a.B + j] : 0.0;
-    const int64_t gsub = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / 32 * per_warp + sub;
-    const int64_t nsub = (int64_t)gridDim.x * kThreads / 32 * per_warp;
-    // the sub-warp loops over groups; per_warp sub-warps of a warp run the same
-    // trip count so their shuffles stay converged (idle ones take g = -1)
-    const int64_t rounds = (a.G + nsub - 1) / nsub;
-    for (int64_t t = 0; t < rounds; t++) {
-        const int64_t g = gsub + t * nsub;
-        const bool live = g < a.G;
-        const int64_t s = live ? a.starts[g] : 0, e = live ? a.starts[g + 1] : 0;
-        double sw = 0.0, tot = 0.0;
-        for (int64_t i = s; i < e; i++) {
-            const double wi = a.w ? a.w[i] : 1.0;
-            sw += wi;
-            if (!on) continue;
-            double h = 0.0;
-            for (int d = 0; d < a.D; d++) {
-                uint32_t code = a.codes[i * a.D + d];
-                if ((int64_t)code >= a.nlev[d]) code = 0;
-                h += a.U[(a.offs[d] + code) * a.B + j];
+    constexpr int SUBS = kPassThreads / BP;
+    constexpr int MR = BP < 16 ? BP : 16;                 // rows per moment flush
+    extern __shared__ double s_dyn[];
+    const Lanes<BP> ln(a.B);
+    const int subw = threadIdx.x / BP;
+    double *s_C = s_dyn;                                   // (c, B)
+    double *s_mom = s_dyn + kMaxCov * 32 + subw * (MR * (BP + 1) * 2);   // [2][MR][BP+1]
+    char *s_chunks = reinterpret_cast<char *>(s_dyn + kMaxCov * 32 + SUBS * MR * (BP + 1) * 2);
+    Chunk<BP> ch;
+    ch.codes = reinterpret_cast<uint32_t *>(s_chunks + subw * Chunk<BP>::kBytes);
+    ch.x = reinterpret_cast<double *>(s_chunks + subw * Chunk<BP>::kBytes + BP * HDFE_MAX_DIMS * 4);
+    for (int k = threadIdx.x; k < a.c * a.B; k += kPassThreads) s_C[k] = a.C[k];
+    __syncthreads();
+    const uint64_t dterm = (uint64_t)(a.first_draw + ln.j) * kDrawMul;
+    double *pp_buf = s_mom, *mm_buf = s_mom + MR * (BP + 1);
+    auto hU_of = [&](const uint32_t (&codes)[HDFE_MAX_DIMS]) {
+        double h = 0.0;
+        if (ln.on) {
+#pragma unroll
+            for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+                if (d >= a.D) break;
+                h += a.U[(a.offs[d] + codes[d]) * a.B + ln.j];
             }
-            for (int c = 0; c < a.c; c++) h += a.X[i * a.c + c] * Cj[c];
-            const double r = row_vec(a, i, j) * inv_root(a, wi);
-            tot += wi * (r - h);
+        }
+        return h;
+    };
+    auto h_cov = [&](int q) {
+        double h = 0.0;
+        for (int c = 0; c < a.c; c++) h += ch.x[q * a.c + c] * s_C[c * a.B + ln.j];
+        return h;
+    };
+    // lane t < nrow adds the sums of row i0 + t to the moments
+    auto flush_moments = [&](int64_t i0, int nrow) {
+        __syncwarp(ln.mask);
+        if (ln.j < nrow) {
+            double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
+            const double *pr = pp_buf + ln.j * (BP + 1), *mr = mm_buf + ln.j * (BP + 1);
+            for (int k = 0; k < a.B; k++) {
+                const double P = pr[k], M = mr[k];
+                m0 += P;
+                m1 += M;
+                m2 += P * P;
+                m3 += M * M;
+                m4 += P * M;
+            }
+            const int64_t i = i0 + ln.j;
+            a.moments[0 * a.N + i] += m0;
+            a.moments[1 * a.N + i] += m1;
+            a.moments[2 * a.N + i] += m2;
+            a.moments[3 * a.N + i] += m3;
+            a.moments[4 * a.N + i] += m4;
+        }
+        __syncwarp(ln.mask);
+    };
+    const int64_t g0 = (int64_t)blockIdx.x * SUBS + subw, gstep = (int64_t)gridDim.x * SUBS;
+    for (int64_t g = g0; g < a.G; g += gstep) {
+        const int64_t s = a.starts[g], e = a.starts[g + 1];
+        const int n = (int)(e - s);
+        // pass 1
+        double sw = 0.0, tot = 0.0;
+        uint32_t bits = 0;
+        double wl = 1.0, irl = 1.0;
+        uint32_t prev[HDFE_MAX_DIMS] = {0, 0, 0, 0};
+        bool have = false;
+        double hU = 0.0;
+        for (int c0 = 0; c0 < n; c0 += BP) {
+            const int m = min(BP, n - c0);
+            wl = load_chunk<BP>(a, ln, ch, s + c0, m);
+            irl = inv_root(a, wl);
+            for (int q = 0; q < m; q++) {
+                const double wi = __shfl_sync(ln.mask, wl, q, BP);
+                const double ir = __shfl_sync(ln.mask, irl, q, BP);
+                sw += wi;
+                if (!have || !same_codes(a, ch.codes, q, prev)) {
+                    take_codes(a, ch.codes, q, prev);
+                    hU = hU_of(prev);
+                    have = true;
+                }
+                if (!ln.on) continue;
+                const int64_t i = s + c0 + q;
+                double r;
+                if (a.R) {
+                    r = a.R[i * a.B + ln.j] * ir;
+                } else {
+                    const bool neg = rad_negative(a.seed, (uint64_t)(a.ordinal0 + i) * kRowMul, dterm);
+                    if (c0 == 0 && neg) bits |= 1u << q;
+                    r = neg ? -ir : ir;
+                }
+                tot += wi * (r - (hU + h_cov(q)));
+            }
+            if (c0 + BP < n) __syncwarp(ln.mask);
         }
         const double mean = sw > 0.0 ? tot / sw : 0.0;
-        // the group's rows again: the projection, and the sink
-        const int64_t n = e - s;
-        for (int64_t ii = 0; ii < n; ii++) {
-            const int64_t i = s + ii;
-            const double wi = a.w ? a.w[i] : 1.0;
-            double o = 0.0, pp = 0.0, mm = 0.0;
-            if (on) {
-                double h = 0.0;
-                for (int d = 0; d < a.D; d++) {
-                    uint32_t code = a.codes[i * a.D + d];
-                    if ((int64_t)code >= a.nlev[d]) code = 0;
-                    h += a.U[(a.offs[d] + code) * a.B + j];
-                }
-                for (int c = 0; c < a.c; c++) h += a.X[i * a.c + c] * Cj[c];
-                o = h + mean;
-                if (a.sqrt_weights) o *= sqrt(wi);
-                if (a.out) a.out[i * a.B + j] = o;
-                const double rr = row_vec(a, i, j);     // the sink's unscaled draw
-                pp = o * o;
-                mm = (rr - o) * (rr - o);
+        // pass 2
+        have = false;
+        int nbuf = 0;               // rows in the moment buffer
+        int64_t buf0 = s;           // the first of them
+        for (int c0 = 0; c0 < n; c0 += BP) {
+            const int m = min(BP, n - c0);
+            if (n > BP) {
+                __syncwarp(ln.mask);
+                wl = load_chunk<BP>(a, ln, ch, s + c0, m);
             }
-            if (a.moments) {
-                // the five sums over the block's draws, in draw order
-                double m0 = pp, m1 = mm, m2 = pp * pp, m3 = mm * mm, m4 = pp * mm;
-                for (int q = 1; q < a.Bp; q <<= 1) {
-                    m0 += __shfl_down_sync(smask, m0, q, a.Bp);
-                    m1 += __shfl_down_sync(smask, m1, q, a.Bp);
-                    m2 += __shfl_down_sync(smask, m2, q, a.Bp);
-                    m3 += __shfl_down_sync(smask, m3, q, a.Bp);
-                    m4 += __shfl_down_sync(smask, m4, q, a.Bp);
+            for (int q = 0; q < m; q++) {
+                const double wi = __shfl_sync(ln.mask, wl, q, BP);
+                if (!have || !same_codes(a, ch.codes, q, prev)) {
+                    take_codes(a, ch.codes, q, prev);
+                    hU = hU_of(prev);
+                    have = true;
                 }
-                if (j == 0) {
-                    a.moments[0 * a.N + i] += m0;
-                    a.moments[1 * a.N + i] += m1;
-                    a.moments[2 * a.N + i] += m2;
-                    a.moments[3 * a.N + i] += m3;
-                    a.moments[4 * a.N + i] += m4;
+                const int64_t i = s + c0 + q;
+                double P = 0.0, M = 0.0;
+                if (ln.on) {
+                    double o = hU + h_cov(q) + mean;
+                    if (a.sqrt_weights) o *= sqrt(wi);
+                    if (a.out) a.out[i * a.B + ln.j] = o;
+                    double rr;       // the sink's unscaled draw
+                    if (a.R) {
+                        rr = a.R[i * a.B + ln.j];
+                    } else {
+                        const bool neg =
+                            c0 == 0 ? ((bits >> q) & 1u) != 0
+                                    : rad_negative(a.seed, (uint64_t)(a.ordinal0 + i) * kRowMul, dterm);
+                        rr = neg ? -1.0 : 1.0;
+                    }
+                    P = o * o;
+                    M = (rr - o) * (rr - o);
+                }
+                if (a.moments) {
+                    pp_buf[nbuf * (BP + 1) + ln.j] = P;
+                    mm_buf[nbuf * (BP + 1) + ln.j] = M;
+                    if (++nbuf == MR) {
+                        flush_moments(buf0, nbuf);
+                        nbuf = 0;
+                        buf0 = i + 1;
+                    }
                 }
             }
         }
+        if (a.moments && nbuf > 0) flush_moments(buf0, nbuf);
+        __syncwarp(ln.mask);
     }
 }
 
@@ -324,10 +562,41 @@ int fill_args(Args &a, const int64_t *starts, int64_t G, const uint32_t *codes, 
 
 inline unsigned grid_for(int64_t G, int Bp)
 {
-    const int64_t groups_per_cta = (int64_t)kThreads / 32 * (32 / Bp);
+    const int64_t groups_per_cta = kPassThreads / Bp;
     int64_t b = (G + groups_per_cta - 1) / groups_per_cta;
     if (b > 148 * 16) b = 148 * 16;
     return (unsigned)(b > 0 ? b : 1);
+}
+
+template <int BP>
+constexpr int project_smem()
+{
+    constexpr int subs = kPassThreads / BP, mr = BP < 16 ? BP : 16;
+    return (kMaxCov * 32 + subs * mr * (BP + 1) * 2) * 8 + subs * Chunk<BP>::kBytes;
+}
+
+template <int BP>
+constexpr int center_chunk_smem() { return (kPassThreads / BP) * Chunk<BP>::kBytes; }
+
+constexpr int kSmallBytes = 40 * 1024;    // small dimensions' level x draw sums per CTA
+
+// the dynamic shared memory limits, raised once per device
+bool set_smem_limits()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (done[dev]) return true;
+    const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (cudaFuncSetAttribute(k_center<8>, at, kSmallBytes + center_chunk_smem<8>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_center<16>, at, kSmallBytes + center_chunk_smem<16>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_center<32>, at, kSmallBytes + center_chunk_smem<32>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_project<8>, at, project_smem<8>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_project<16>, at, project_smem<16>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_project<32>, at, project_smem<32>()) != cudaSuccess)
+        return false;
+    done[dev] = true;
+    return true;
 }
 
 }  // namespace rows
@@ -379,7 +648,7 @@ extern "C" int hdfe_rows_center(const int64_t *starts, int64_t n_groups, const u
     // small dimensions in shared memory (up to 40 KB of level x draw sums)
     int64_t slots = 0;
     for (int d = 0; d < D; d++) {
-        if ((slots + n_levels[d]) * B * 8 <= 40 * 1024 && n_levels[d] <= 4096) {
+        if ((slots + n_levels[d]) * B * 8 <= rows::kSmallBytes && n_levels[d] <= 4096) {
             a.small[d] = 1;
             a.soff[d] = slots;
             slots += n_levels[d];
@@ -391,7 +660,14 @@ extern "C" int hdfe_rows_center(const int64_t *starts, int64_t n_groups, const u
     HDFE_CUDA_TRY(cudaMemsetAsync(acc, 0, a.L * B * 8, s));
     if (c > 0) HDFE_CUDA_TRY(cudaMemsetAsync(acc_x, 0, (int64_t)c * B * 8, s));
     if (squares) HDFE_CUDA_TRY(cudaMemsetAsync(squares, 0, B * 8, s));
-    rows::k_center<<<rows::grid_for(n_groups, a.Bp), rows::kThreads, slots * B * 8, s>>>(a);
+    if (!rows::set_smem_limits()) return hdfe_set_cuda_error(cudaGetLastError());
+    const unsigned grid = rows::grid_for(n_groups, a.Bp);
+    if (a.Bp == 8)
+        rows::k_center<8><<<grid, rows::kPassThreads, slots * B * 8 + rows::center_chunk_smem<8>(), s>>>(a);
+    else if (a.Bp == 16)
+        rows::k_center<16><<<grid, rows::kPassThreads, slots * B * 8 + rows::center_chunk_smem<16>(), s>>>(a);
+    else
+        rows::k_center<32><<<grid, rows::kPassThreads, slots * B * 8 + rows::center_chunk_smem<32>(), s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
     return HDFE_OK;
@@ -416,7 +692,14 @@ extern "C" int hdfe_rows_project(const int64_t *starts, int64_t n_groups, const 
     a.moments = moments;
     a.N = n_rows;
     cudaStream_t s = (cudaStream_t)stream;
-    rows::k_project<<<rows::grid_for(n_groups, a.Bp), rows::kThreads, 0, s>>>(a);
+    if (!rows::set_smem_limits()) return hdfe_set_cuda_error(cudaGetLastError());
+    const unsigned grid = rows::grid_for(n_groups, a.Bp);
+    if (a.Bp == 8)
+        rows::k_project<8><<<grid, rows::kPassThreads, rows::project_smem<8>(), s>>>(a);
+    else if (a.Bp == 16)
+        rows::k_project<16><<<grid, rows::kPassThreads, rows::project_smem<16>(), s>>>(a);
+    else
+        rows::k_project<32><<<grid, rows::kPassThreads, rows::project_smem<32>(), s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
     return HDFE_OK;

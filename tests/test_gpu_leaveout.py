@@ -100,3 +100,27 @@ def test_projection_is_idempotent(device):
         out.contiguous().data_ptr(), 4, 0, 0, 0, 0, op.N, out2.data_ptr(), None,
         _lib.stream_handle()))
     assert rel(out2.cpu().numpy(), out.cpu().numpy()) < 1e-8
+
+
+@pytest.mark.parametrize("weights", [False, True])
+def test_long_groups_and_block_widths(device, weights):
+    """Workers with 20-36 rows (many groups longer than one 32-row chunk of
+    the row passes), two non-streamed dimensions (300 firms: level sums in
+    global memory for wide blocks, in shared memory for narrow ones),
+    covariates, and blocks of 1, 5, 13 and 32 vectors: projections and JLA
+    sums against the oracle."""
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    rows = pass0_layout(simulate_panel(600, 300, 40, spell=(20, 36), p_move=0.05,
+                                       weights=weights, seed=5))
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), X=rows.V[:, 1:], tol=1e-12)
+    op = operator(rows, 1e-12, covariates=True)
+    sw = rows.w is not None
+    for B, first in ((1, 0), (5, 2), (13, 7), (32, 40)):
+        ref = des.project_rows(B, 9, first, sqrt_weights=sw)
+        out, _ = op.project(B, seed=9, first_draw=first, sqrt_weights=sw)
+        assert rel(out.cpu().numpy(), ref) < 1e-8, B
+    lev_ref, _, f_ref = des.jla_leverages(45, 16, 4)
+    lev, _, f = op.jla_leverages(45, block=32, seed=4)
+    assert rel(lev.cpu().numpy(), lev_ref) < 1e-8
+    assert rel(f.cpu().numpy(), f_ref) < 1e-8
