@@ -45,7 +45,7 @@ PEAKS = REPO / "MEASURED_PEAKS.json"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default=WORKLOAD)
@@ -79,22 +79,32 @@ class ClockSampler:
         self.proc = None
         self.lines = []
 
-    def start(self):
+    def start(self, wait_s=10.0):
+        """Start sampling and wait (up to wait_s) for the first sample, so that
+        nvidia-smi's own start-up is over before anything is timed."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except FileNotFoundError:
             self.proc = None
+            return
+        t_end = time.monotonic() + wait_s
+        while not self.lines and time.monotonic() < t_end and self.proc.poll() is None:
+            time.sleep(0.02)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
-    def stop(self):
+    def mark(self):
+        """Host time stamps bracketing the timed region (samples outside are dropped)."""
+        return time.monotonic()
+
+    def stop(self, t_begin=None, t_end=None):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -104,7 +114,9 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for t, line in self.lines:
+            if (t_begin is not None and t < t_begin) or (t_end is not None and t > t_end):
+                continue
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -161,28 +173,30 @@ def run_ours(args, rank, world, local_rank):
     rows = prepare(args.workload, seed=rank)
     drows = fit.DeviceRows.from_rows(rows)
     torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()                 # before the warm-up: its start-up is not timed
     for _ in range(max(args.warmup, 0)):
         res = fit.fit(drows, tol=args.tol)
     torch.cuda.synchronize()
     lib = _lib.lib()
     timer = fit.PhaseTimer()
-    sampler = ClockSampler(local_rank)
-    sampler.start()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = lib.hdfe_kernel_launches()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
+    h0 = sampler.mark()
     t0.record()
     for _ in range(args.steps):
         res = fit.fit(drows, tol=args.tol, timer=timer)
     t1.record()
     torch.cuda.synchronize()
+    h1 = sampler.mark()
     if dist:
         dist.barrier()
     launches = lib.hdfe_kernel_launches() - launches0
-    clocks = sampler.stop()
+    clocks = sampler.stop(h0, h1)
     ms = t0.elapsed_time(t1)
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -393,22 +407,26 @@ def run_reference(args, rank):
     import oracle as orc
     orc.set_threads(os.cpu_count() or 1)
     rows = prepare(args.workload, seed=0)
-    for _ in range(max(args.warmup, 0)):
+    # a bounded sample of the workload: one full CPU fit takes seconds, so at
+    # most one warm-up fit and three timed fits, whatever --steps asks
+    warm, steps = min(max(args.warmup, 0), 1), max(1, min(args.steps, 3))
+    for _ in range(warm):
         oracle_fit(rows, args.tol)
     t = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         _, info = oracle_fit(rows, args.tol)
     dt = time.perf_counter() - t
-    value = args.steps / dt
+    value = steps / dt
     return {"metric": METRIC, "value": round(value, 5), "unit": UNIT, "impl": "reference",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(dt / args.steps * 1e3, 1), "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
+            "ms_per_step": round(dt / steps * 1e3, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded generator, 5M-worker AKM panel)",
             "config": config(args, 1, rows),
             "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": orc.num_threads(),
                              "kind": "port",
-                             "sample": "full fits of the panel, each step one fit"},
+                             "sample": f"{steps} full fits of the panel (each step one fit), "
+                                       f"after {warm} warm-up fit"},
             "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "solve": {"iterations": info["iterations"], "converged": info["converged"]}}

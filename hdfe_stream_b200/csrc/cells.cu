@@ -16,12 +16,11 @@
 //   rows_index   per tile: each group's first row and first cell
 //   groups_count per tile of groups: identifying groups and their cells
 //   scan_tiles   offsets of those
-//   groups_work  persistent: one thread per group forms its cells from its
-//                rows, scatters obs/cnt, writes the identifying cells and
-//                adds their diag / rhs contributions.  Levels of small
-//                dimensions (years) accumulate in shared memory per CTA and
-//                are flushed once per CTA, so 40M rows do not all hit 15
-//                addresses.
+//   groups_work  persistent over tiles of groups: each warp walks its groups
+//                in windows of whole groups (one row per lane), forms cells and
+//                group sums by segmented warp scans, writes the identifying
+//                cells and aggregates the level statistics per level before
+//                updating them (years in per-warp shared slots).
 // Integer-valued sums (cnt; obs without weights) are exact in any order;
 // other sums are FP64 in atomic order (well inside the 1e-8 bar).
 #include <cuda_runtime.h>
@@ -36,7 +35,7 @@ constexpr int kRowTile = 4096;          // rows per tile (16 per thread)
 constexpr int kGroupTile = 1024;        // groups per tile (4 per thread)
 constexpr int kMaxDims = HDFE_MAX_DIMS;
 constexpr int kMaxVars = HDFE_MAX_VARS;
-constexpr int kSmemLevelBudget = 40 * 1024;   // bytes of level accumulators per CTA
+constexpr int kSmemLevelBudget = 64 * 1024;   // bytes of level accumulators per CTA (all warps)
 // a shared level slot: obs, cnt, diag, groups (lcount), work, then rhs[m]
 constexpr int kSlotFixed = 5;
 
@@ -408,42 +407,306 @@ __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, i
     }
 }
 
+// ------------------------------------------------- warp-cooperative groups
+//
+// groups_work processes a tile of kGroupTile groups per CTA iteration: the
+// tile's identifying-group and identifying-cell offsets are scanned into
+// shared memory, then each warp takes kGroupsPerWarp consecutive groups and
+// walks them in windows of whole groups of at most 32 rows, one row per lane
+// (coalesced loads of codes, weights and variables).  Within a window:
+//   - group and cell sums are segmented warp scans (lanes = rows);
+//   - identifying cells are written by the lane ending each cell;
+//   - the level statistics (obs, cnt, diag with its -u^2/N_g correction, rhs,
+//     lcount, work) are aggregated first per (group, level) and then per level
+//     with __match_any_sync, so each distinct level of the window is updated
+//     once: small dimensions in this warp's own shared slots (plain adds, no
+//     contention), the others by global atomics.
+// A group longer than 32 rows is processed by one lane with do_group.
+constexpr int kWarpsPerCta = kThreads / 32;
+constexpr int kGroupsPerWarp = kGroupTile / kWarpsPerCta;
+
+// inclusive segmented sums of x over lanes; seg: first lane of this lane's segment
+template <int NV>
+__device__ __forceinline__ void seg_scan(double (&x)[NV], int nv, int seg, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            if (k >= nv) break;
+            const double y = __shfl_up_sync(0xffffffffu, x[k], o);
+            if (lane - o >= seg) x[k] += y;
+        }
+    }
+}
+
+// first lane of the segment holding `lane`, and its last lane (< n)
+__device__ __forceinline__ void segment(unsigned heads, int lane, int n, int &first, int &last)
+{
+    const unsigned upto = (2u << lane) - 1u;        // lanes 0..lane (all 32 when lane = 31)
+    first = 31 - __clz(heads & upto);
+    const unsigned after = heads & ~upto;
+    last = after ? __ffs(after) - 2 : n - 1;
+}
+
 template <int D, int MV>
 __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sums_scratch)
 {
-    extern __shared__ double s_acc[];
+    extern __shared__ double s_dyn[];
+    __shared__ int64_t s_gi[kGroupTile], s_co[kGroupTile];
+    __shared__ int s_nc[kGroupTile];
     __shared__ int s_scr[2][kThreads / 32 + 1];
     const Dims &dm = a.dims;
-    const int m = dm.m;
-    const int64_t nsm = dm.n_small * (kSlotFixed + m);
-    for (int64_t k = threadIdx.x; k < nsm; k += kThreads) s_acc[k] = 0.0;
+    const int m = MV > 0 ? MV : dm.m;
+    constexpr int kV = MV > 0 ? MV : kMaxVars;
+    const int NS = kSlotFixed + m;                  // values per level slot
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *w_slots = s_dyn + (int64_t)warp * dm.n_small * NS;           // this warp's small levels
+    double *w_scr = s_dyn + (int64_t)kWarpsPerCta * dm.n_small * NS + warp * 32 * NS;
+    for (int64_t k = threadIdx.x; k < (int64_t)kWarpsPerCta * dm.n_small * NS; k += kThreads)
+        s_dyn[k] = 0.0;
     __syncthreads();
     const int64_t G = a.totals[0];
     const int64_t tiles = (G + kGroupTile - 1) / kGroupTile;
     double *sums_buf = a.cell_sums ? a.cell_sums : sums_scratch;
     for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         const int64_t t0 = t * kGroupTile, t1 = min(t0 + kGroupTile, G);
-        int64_t gi_run = a.tile_off[t * 2 + 0];
-        int64_t co_run = a.tile_off[t * 2 + 1];
-        for (int64_t base = t0; base < t1; base += kThreads) {
-            const int64_t g = base + threadIdx.x;
-            int64_t nc = 0;
-            if (g < t1) nc = a.gcell[g + 1] - a.gcell[g];
-            const bool keep = nc > 1;
-            int tg, tc;
-            const int eg = block_exclusive(keep ? 1 : 0, s_scr[0], tg);
-            const int ec = block_exclusive(keep ? (int)nc : 0, s_scr[1], tc);
-            if (g < t1) do_group<D, MV>(a, g, keep, gi_run + eg, co_run + ec, s_acc, sums_buf);
-            gi_run += tg;
-            co_run += tc;
+        {
+            int64_t gi_run = a.tile_off[t * 2 + 0];
+            int64_t co_run = a.tile_off[t * 2 + 1];
+            for (int64_t base = t0; base < t1; base += kThreads) {
+                const int64_t g = base + threadIdx.x;
+                int64_t nc = 0;
+                if (g < t1) nc = a.gcell[g + 1] - a.gcell[g];
+                const bool keep = nc > 1;
+                int tg, tc;
+                const int eg = block_exclusive(keep ? 1 : 0, s_scr[0], tg);
+                const int ec = block_exclusive(keep ? (int)nc : 0, s_scr[1], tc);
+                if (g < t1) {
+                    s_gi[g - t0] = keep ? gi_run + eg : -1;
+                    s_co[g - t0] = co_run + ec;
+                    s_nc[g - t0] = (int)nc;
+                }
+                gi_run += tg;
+                co_run += tc;
+            }
         }
+        __syncthreads();
+        const int64_t gb = t0 + (int64_t)warp * kGroupsPerWarp;
+        const int64_t ge = min(gb + kGroupsPerWarp, t1);
+        int64_t g = gb;
+        while (g < ge) {
+            const int64_t r = a.grow[g];
+            const int64_t gl = g + 1 + lane;
+            const int64_t e = gl <= ge ? a.grow[gl] : INT64_MAX;   // end of group g + lane
+            const unsigned fm = __ballot_sync(0xffffffffu, e - r <= 32);
+            const int k = __popc(fm);                              // whole groups in the window
+            if (k == 0) {       // group g has more than 32 rows: one lane takes it
+                if (lane == 0) {
+                    const int64_t gloc = g - t0;
+                    do_group<D, MV>(a, g, s_gi[gloc] >= 0, s_gi[gloc], s_co[gloc], w_slots, sums_buf);
+                }
+                __syncwarp();
+                g++;
+                continue;
+            }
+            const int n = (int)(__shfl_sync(0xffffffffu, e, k - 1) - r);
+            const unsigned heads =
+                __reduce_or_sync(0xffffffffu, lane < k - 1 ? (1u << (int)(e - r)) : 0u) | 1u;
+            const bool act = lane < n;
+            const int64_t i = r + lane;
+            // the lane's row
+            uint32_t c[D];
+#pragma unroll
+            for (int d = 0; d < D; d++) c[d] = 0;
+            double x[1 + kV];                   // w, then w (v - mean) per variable
+#pragma unroll
+            for (int v = 0; v <= kV; v++) x[v] = 0.0;
+            if (act) {
+                load_codes<D>(a.codes, i, c);
+                const double wv = a.w ? a.w[i] : 1.0;
+                x[0] = wv;
+#pragma unroll
+                for (int v = 0; v < kV; v++) {
+                    if (v >= m) break;
+                    const double z = a.V[(int64_t)v * a.N + i] - a.means[v];
+                    x[1 + v] = a.w ? wv * z : z;
+                }
+            }
+            int gf, gla;
+            segment(heads, lane, n, gf, gla);
+            const int grp = __popc(heads & ((2u << lane) - 1u)) - 1;
+            const int64_t gloc = g + grp - t0;
+            const int64_t gi = s_gi[gloc], co = s_co[gloc];
+            const int ncg = s_nc[gloc];
+            const bool keep = gi >= 0;
+            // cells: a new cell at a group start or where the codes change (the
+            // codes as stored, as the cell counts were made); then out-of-range
+            // codes are reported and read as level 0
+            bool cs = lane == gf;
+#pragma unroll
+            for (int d = 0; d < D; d++) cs |= __shfl_up_sync(0xffffffffu, c[d], 1) != c[d];
+            const unsigned cells = __ballot_sync(0xffffffffu, act && cs) | 1u;
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+                if (act && (int64_t)c[d] >= dm.nlev[d]) {
+                    atomicCAS(a.status, 0u, (unsigned)HDFE_ERR_BAD_CODE);
+                    c[d] = 0;
+                }
+            }
+            // group sums
+            double gsum[1 + kV];
+#pragma unroll
+            for (int v = 0; v <= kV; v++) gsum[v] = x[v];
+            seg_scan<1 + kV>(gsum, 1 + m, gf, lane);
+            const double Ng = __shfl_sync(0xffffffffu, gsum[0], gla);
+            double vbar[kV];
+#pragma unroll
+            for (int v = 0; v < kV; v++) {
+                if (v >= m) break;
+                vbar[v] = __shfl_sync(0xffffffffu, gsum[1 + v], gla) / Ng;
+            }
+            // identifying cells and groups
+            if (__any_sync(0xffffffffu, act && keep)) {
+                int cf, cl;
+                segment(cells, lane, n, cf, cl);
+                double csum[1 + kV];
+#pragma unroll
+                for (int v = 0; v <= kV; v++) csum[v] = x[v];
+                const unsigned actmask = n == 32 ? 0xffffffffu : ((1u << n) - 1u);
+                if ((cells & actmask) != actmask) seg_scan<1 + kV>(csum, 1 + m, cf, lane);
+                const int cidx = __popc(cells & ((2u << lane) - 1u) & ~((1u << gf) - 1u)) - 1;
+                if (act && keep && lane == cl && cidx < ncg) {
+                    const int64_t q = co + cidx;
+#pragma unroll
+                    for (int d = 0; d < D; d++) a.cell_codes[q * D + d] = c[d];
+                    a.cell_n[q] = csum[0];
+                    if (a.cell_sums) {
+#pragma unroll
+                        for (int v = 0; v < kV; v++) {
+                            if (v >= m) break;
+                            a.cell_sums[q * m + v] = csum[1 + v];
+                        }
+                    }
+                }
+                if (act && keep && lane == gf) {
+                    a.starts[gi] = co;
+                    a.group_n[gi] = Ng;
+                }
+            }
+            // level statistics: per (group, level), then per level
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+                const unsigned long long key1 =
+                    act ? (((unsigned long long)c[d] << 5) | (unsigned)grp) : (~0ull - lane);
+                const unsigned mk1 = __match_any_sync(0xffffffffu, key1);
+                const bool lead1 = act && lane == __ffs(mk1) - 1;
+                if (act) {
+#pragma unroll
+                    for (int v = 0; v <= kV; v++) {
+                        if (v > m) break;
+                        w_scr[lane * NS + v] = x[v];
+                    }
+                }
+                __syncwarp();
+                double T[kSlotFixed + kV];
+#pragma unroll
+                for (int q = 0; q < kSlotFixed + kV; q++) T[q] = 0.0;
+                if (lead1) {
+                    double u = 0.0, sv[kV];
+#pragma unroll
+                    for (int v = 0; v < kV; v++) sv[v] = 0.0;
+                    for (unsigned b = mk1; b; b &= b - 1) {
+                        const int l = __ffs(b) - 1;
+                        u += w_scr[l * NS];
+#pragma unroll
+                        for (int v = 0; v < kV; v++) {
+                            if (v >= m) break;
+                            sv[v] += w_scr[l * NS + 1 + v];
+                        }
+                    }
+                    T[0] = u;
+                    T[1] = (double)__popc(mk1);
+                    if (keep) {
+                        T[2] = u - u * u / Ng;
+                        T[3] = 1.0;
+                        T[4] = (double)ncg;
+#pragma unroll
+                        for (int v = 0; v < kV; v++) {
+                            if (v >= m) break;
+                            T[kSlotFixed + v] = sv[v] - u * vbar[v];
+                        }
+                    }
+                }
+                __syncwarp();
+                const unsigned long long key2 =
+                    lead1 ? (unsigned long long)c[d] : (0xffffffff00000000ull | (unsigned)lane);
+                const unsigned mk2 = __match_any_sync(0xffffffffu, key2);
+                const bool lead2 = lead1 && lane == __ffs(mk2) - 1;
+                if (lead1) {
+#pragma unroll
+                    for (int q = 0; q < kSlotFixed + kV; q++) {
+                        if (q >= NS) break;
+                        w_scr[lane * NS + q] = T[q];
+                    }
+                }
+                __syncwarp();
+                if (lead2) {
+                    for (unsigned b = mk2 & (mk2 - 1); b; b &= b - 1) {     // the other leaders
+                        const int l = __ffs(b) - 1;
+#pragma unroll
+                        for (int q = 0; q < kSlotFixed + kV; q++) {
+                            if (q >= NS) break;
+                            T[q] += w_scr[l * NS + q];
+                        }
+                    }
+                    if (dm.small[d]) {
+                        double *sl = w_slots + (dm.soff[d] + c[d]) * NS;
+#pragma unroll
+                        for (int q = 0; q < kSlotFixed + kV; q++) {
+                            if (q >= NS) break;
+                            sl[q] += T[q];
+                        }
+                    } else {
+                        const int64_t lv = dm.offs[d] + c[d];
+                        atomicAdd(a.obs + lv, T[0]);
+                        atomicAdd(a.cnt + lv, T[1]);
+                        if (T[3] > 0.0) {
+                            atomicAdd(a.diag + lv, T[2]);
+#pragma unroll
+                            for (int v = 0; v < kV; v++) {
+                                if (v >= m) break;
+                                atomicAdd(a.rhs + lv * m + v, T[kSlotFixed + v]);
+                            }
+                            if (a.lcount) {
+                                atomicAdd(a.lcount + lv, (int)T[3]);
+                                atomicAdd(reinterpret_cast<unsigned long long *>(a.work) + lv,
+                                          (unsigned long long)T[4]);
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            g += k;
+        }
+        __syncthreads();            // the tile's offsets are replaced next
     }
-    __syncthreads();
-    // flush the shared accumulators of the small dimensions
+    // the warps' small-dimension slots: summed in warp order, flushed once per CTA
     for (int d = 0; d < dm.D; d++) {
         if (!dm.small[d]) continue;
         for (int64_t l = threadIdx.x; l < dm.nlev[d]; l += kThreads) {
-            const double *sl = s_acc + (dm.soff[d] + l) * (kSlotFixed + m);
+            double sl[kSlotFixed + kV];
+#pragma unroll
+            for (int q = 0; q < kSlotFixed + kV; q++) sl[q] = 0.0;
+            for (int wv = 0; wv < kWarpsPerCta; wv++) {
+                const double *src = s_dyn + ((int64_t)wv * dm.n_small + dm.soff[d] + l) * NS;
+#pragma unroll
+                for (int q = 0; q < kSlotFixed + kV; q++) {
+                    if (q >= NS) break;
+                    sl[q] += src[q];
+                }
+            }
             const int64_t lv = dm.offs[d] + l;
             if (sl[0] != 0.0) atomicAdd(a.obs + lv, sl[0]);
             if (sl[1] != 0.0) atomicAdd(a.cnt + lv, sl[1]);
@@ -453,8 +716,11 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
                 atomicAdd(reinterpret_cast<unsigned long long *>(a.work) + lv,
                           (unsigned long long)sl[4]);
             }
-            for (int v = 0; v < m; v++)
+#pragma unroll
+            for (int v = 0; v < kV; v++) {
+                if (v >= m) break;
                 if (sl[kSlotFixed + v] != 0.0) atomicAdd(a.rhs + lv * m + v, sl[kSlotFixed + v]);
+            }
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -525,14 +791,14 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
         dm.nlev[d] = n_levels[d];
         L += n_levels[d];
     }
-    // small dimensions: shared-memory accumulators, smallest first
-    const int64_t per_level = (kSlotFixed + m) * 8;
+    // small dimensions: shared-memory accumulators (one copy per warp), smallest first
+    const int64_t per_level = (int64_t)(kSlotFixed + m) * 8 * kWarpsPerCta;
     for (int pass = 0; pass < D; pass++) {
         int best = -1;
         for (int d = 0; d < D; d++)
             if (!dm.small[d] && (best < 0 || n_levels[d] < n_levels[best])) best = d;
         if (best < 0) break;
-        if ((slots + n_levels[best]) * per_level > kSmemLevelBudget || n_levels[best] > 4096) {
+        if ((slots + n_levels[best]) * per_level > kSmemLevelBudget || n_levels[best] > 1024) {
             dm.small[best] = -1;        // tried; stays global
             continue;
         }
@@ -593,10 +859,12 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     int dev = 0, sms = 0, per_sm = 0;
     HDFE_CUDA_TRY(cudaGetDevice(&dev));
     HDFE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const size_t smem = (size_t)(slots * per_level);
+    // the warps' small-level slots, then their 32-lane scratch rows
+    const size_t smem = (size_t)(slots * per_level) + (size_t)kWarpsPerCta * 32 * (kSlotFixed + m) * 8;
     void (*kern)(GroupArgs, double *) = m == 1 ? groups_work<D, 1> : m == 2 ? groups_work<D, 2>
                                        : m == 3 ? groups_work<D, 3> : m == 4 ? groups_work<D, 4>
                                        : groups_work<D, 0>;
+    HDFE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     HDFE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
     int64_t blocks = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
     if (blocks > gtiles) blocks = gtiles > 0 ? gtiles : 1;
