@@ -563,111 +563,152 @@ __global__ void __launch_bounds__(kThreads) k_cell_widx(Args a)
 //     C_g(a, b) - (u_a / N_g) u_b
 // (the reference's per-cell sum  sum_{i has b} (n_i [i has a] - n_i u_a / N_g)
 // regrouped), with u_a = sum of n over g's cells with wide level a and
-// C_g(a, b) = sum of n over its cells having both (C_g(a, a) = u_a).  Each
-// thread forms its group's u and u / N_g in shared memory; each lane of the
-// warp then owns W^2 / 32 entries and adds the 32 groups' outer products in
-// lane order.  Cells with two wide levels (two small dimensions) add their
-// off-diagonal C into its own array.  Warps and CTAs are summed in a fixed
-// order, so the block is deterministic.
-constexpr int kWideThreads = 128;   // static shared memory stays under 48 KB
+// C_g(a, b) = sum of n over its cells having both (C_g(a, a) = u_a).  A warp
+// takes 32 consecutive groups at a time: their cells are read coalesced (one
+// per lane) and summed into the groups' u rows in shared memory (lanes with
+// the same group and level combined by __match_any_sync in lane order); then
+// each lane owns W^2 / 32 entries and adds the 32 groups' (u_a / N_g) u_b in
+// group order, lanes a < W add the diagonal's u_a, and the pattern is the
+// union of the groups' level masks.  Cells with two wide levels (two small
+// dimensions) add their off-diagonal C into its own array.  Warps and CTAs
+// are summed in a fixed order, so the block is deterministic.
+constexpr int kWideThreads = 128;
+constexpr int kWideWarps = kWideThreads / 32;
 
 __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
 {
-    __shared__ double s_u[kWideThreads][kWideWarp + 1];
-    __shared__ double s_w[kWideThreads][kWideWarp + 1];
-    __shared__ double s_acc[kWideThreads / 32][kWideWarp * kWideWarp];
-    __shared__ uint8_t s_pr[kWideThreads / 32][kWideWarp * kWideWarp];
+    __shared__ double s_u[kWideWarps][32][kWideWarp + 1];
+    __shared__ double s_w[kWideWarps][32][kWideWarp + 1];
+    __shared__ int64_t s_gs[kWideWarps][33];
+    __shared__ double s_stage[kWideWarps][32];
+    __shared__ double s_acc[kWideWarps][kWideWarp * kWideWarp];
+    __shared__ unsigned s_pat[kWideWarps][kWideWarp];
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const int W = (int)a.W;
     const int E = W * W;
+    double (*u)[kWideWarp + 1] = s_u[wl];
+    double (*wv)[kWideWarp + 1] = s_w[wl];
+    int64_t *gs = s_gs[wl];
     double acc[kWideEntries];
     int ea[kWideEntries], eb[kWideEntries];
-    unsigned pres = 0, owned = 0;
 #pragma unroll
     for (int t = 0; t < kWideEntries; t++) {
         acc[t] = 0.0;
         const int en = lane + 32 * t;
         ea[t] = en < E ? en / W : 0;
         eb[t] = en < E ? en % W : 0;
-        if (en < E) owned |= 1u << t;
     }
-    double *u = s_u[threadIdx.x];
-    double *wv = s_w[threadIdx.x];
-    const int64_t stride = (int64_t)gridDim.x * kWideThreads;
-    for (int64_t base = (int64_t)blockIdx.x * kWideThreads; base < a.G; base += stride) {
-        const int64_t g = base + threadIdx.x;
-        for (int k = 0; k < W; k++) u[k] = 0.0;
-        if (g < a.G) {
-            const int64_t s = a.starts[g], e = a.starts[g + 1];
-            for (int64_t i = s; i < e; i++) {
-                const double ni = a.n[i];
-                int nw = 0, k0 = -1;
-                for (int d = 0; d < a.D; d++) {
-                    const int32_t k = a.cell_widx[i * a.D + d];
-                    if (k < 0) continue;
-                    u[k] += ni;
-                    if (nw++ == 0) k0 = k;
+    double dsum = 0.0;          // lane a < W: sum of u_a
+    unsigned pat = 0;           // lane a < W: levels sharing a group with a
+    const int64_t chunks = (a.G + 31) / 32;
+    const int64_t wstep = (int64_t)gridDim.x * kWideWarps;
+    for (int64_t ch = (int64_t)blockIdx.x * kWideWarps + wl; ch < chunks; ch += wstep) {
+        const int64_t g0 = ch * 32;
+        const int ng = (int)min((int64_t)32, a.G - g0);
+        gs[lane] = a.starts[g0 + min(lane, ng)];
+        if (lane == 0) gs[32] = a.starts[g0 + ng];
+        for (int q = lane; q < 32 * (kWideWarp + 1); q += 32) (&u[0][0])[q] = 0.0;
+        __syncwarp();
+        const int64_t c0 = gs[0], c1 = gs[ng];
+        for (int64_t i0 = c0; i0 < c1; i0 += 32) {
+            const int64_t i = i0 + lane;
+            const bool valid = i < c1;
+            int gq = 0;
+            double ni = 0.0;
+            if (valid) {
+                int lo = 0, hi = ng;        // last group with start <= i
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (gs[mid] <= i) lo = mid; else hi = mid;
+                }
+                gq = lo;
+                ni = a.n[i];
+            }
+            int k0 = -1;
+            for (int d = 0; d < a.D; d++) {
+                const int32_t k = valid ? a.cell_widx[i * a.D + d] : -1;
+                const int key = k >= 0 ? gq * 32 + k : -1 - lane;
+                const unsigned peers = __match_any_sync(0xffffffffu, key);
+                s_stage[wl][lane] = ni;
+                __syncwarp();
+                if (k >= 0 && lane == __ffs(peers) - 1) {
+                    double sum = 0.0;
+                    for (unsigned p = peers; p; p &= p - 1) sum += s_stage[wl][__ffs(p) - 1];
+                    u[gq][k] += sum;
+                }
+                if (k >= 0) {
+                    if (k0 < 0) k0 = k;
                     else {
                         // a cell with two wide levels: C(k0, k) and C(k, k0)
                         atomicAdd(a.wcross + (int64_t)k0 * W + k, ni);
                         atomicAdd(a.wcross + (int64_t)k * W + k0, ni);
                     }
                 }
+                __syncwarp();
             }
-            const double Ng = a.group_n[g];
-            for (int k = 0; k < W; k++) wv[k] = u[k] / Ng;
-        } else {
-            for (int k = 0; k < W; k++) wv[k] = 0.0;
         }
         __syncwarp();
-        // the warp's 32 groups, in lane order, into the lane-owned entries
-        const int src0 = wl * 32;
-        for (int q = 0; q < 32; q++) {
-            const double *us = s_u[src0 + q];
-            const double *ws = s_w[src0 + q];
-#pragma unroll
-            for (int t = 0; t < kWideEntries; t++) {
-                const double ua = us[ea[t]], ub = us[eb[t]];
-                if (((owned >> t) & 1u) && ua > 0.0 && ub > 0.0) {
-                    const double c = ea[t] == eb[t] ? ua : 0.0;
-                    acc[t] += c - ws[ea[t]] * ub;
-                    pres |= 1u << t;
-                }
+        // each group's u / N_g and level mask
+        unsigned mask = 0;
+        if (lane < ng) {
+            const double inv = 1.0 / a.group_n[g0 + lane];
+            for (int k = 0; k < W; k++) {
+                const double x = u[lane][k];
+                wv[lane][k] = x * inv;
+                if (x > 0.0) mask |= 1u << k;
             }
+        }
+        __syncwarp();
+        for (int q = 0; q < ng; q++) {
+            const unsigned mq = __shfl_sync(0xffffffffu, mask, q);
+            if (lane < W) {
+                if ((mq >> lane) & 1u) pat |= mq;
+                dsum += u[q][lane];
+            }
+#pragma unroll
+            for (int t = 0; t < kWideEntries; t++) acc[t] += wv[q][ea[t]] * u[q][eb[t]];
         }
         __syncwarp();
     }
-    // warps of the CTA summed in order
+    // the warp's entries, then the CTA's warps summed in order
 #pragma unroll
     for (int t = 0; t < kWideEntries; t++) {
         const int en = lane + 32 * t;
-        if (en < E) {
-            s_acc[wl][en] = acc[t];
-            s_pr[wl][en] = (pres >> t) & 1u;
-        }
+        if (en < E) s_acc[wl][en] = -acc[t];
     }
+    if (lane < W) s_pat[wl][lane] = pat;
+    __syncwarp();
+    if (lane < W) s_acc[wl][lane * W + lane] += dsum;
     __syncthreads();
     for (int en = threadIdx.x; en < E; en += kWideThreads) {
         double sum = 0.0;
         uint8_t p = 0;
-        for (int w = 0; w < kWideThreads / 32; w++) { sum += s_acc[w][en]; p |= s_pr[w][en]; }
+        const int ra = en / W, rb = en % W;
+        for (int w = 0; w < kWideWarps; w++) {
+            sum += s_acc[w][en];
+            p |= (uint8_t)((s_pat[w][ra] >> rb) & 1u);
+        }
         a.wpart[(int64_t)blockIdx.x * E + en] = sum;
         a.wpres[(int64_t)blockIdx.x * E + en] = p;
     }
 }
 
+// per entry: the CTAs' partial sums in CTA order (one warp per entry)
 __global__ void __launch_bounds__(kThreads) k_wide_block_reduce(Args a)
 {
+    const int lane = threadIdx.x & 31;
     const int64_t E = a.W * a.W;
-    for (int64_t en = (int64_t)blockIdx.x * kThreads + threadIdx.x; en < E;
-         en += (int64_t)gridDim.x * kThreads) {
+    const int64_t warps = (int64_t)gridDim.x * (kThreads / 32);
+    for (int64_t en = ((int64_t)blockIdx.x * kThreads + threadIdx.x) / 32; en < E; en += warps) {
         double sum = 0.0;
-        uint8_t p = 0;
-        for (int64_t b = 0; b < a.wide_ctas; b++) {
+        unsigned p = 0;
+        for (int64_t b = lane; b < a.wide_ctas; b += 32) {
             sum += a.wpart[b * E + en];
             p |= a.wpres[b * E + en];
         }
-        if (!p) continue;
+        sum = warp_sum(sum);
+        p = __any_sync(0xffffffffu, p != 0);
+        if (!p || lane != 0) continue;
         const int64_t wa = en / a.W, wb = en % a.W;
         const int64_t lb = a.wide_list[wb];
         a.dval[wa * a.L + lb] = sum + a.wcross[en];
@@ -1037,7 +1078,7 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
     if (n_wide > 0) {
         if (n_wide <= kWideWarp) {
             k_wide_block_warp<<<(unsigned)a.wide_ctas, kWideThreads, 0, c.s>>>(a);
-            k_wide_block_reduce<<<grid_for(n_wide * n_wide, kThreads, 64), kThreads, 0, c.s>>>(a);
+            k_wide_block_reduce<<<grid_for(n_wide * n_wide * 32, kThreads, 64), kThreads, 0, c.s>>>(a);
             launched += 2;
         } else {
             k_wide_block_atomic<<<(unsigned)(c.sms * 8), kThreads, 0, c.s>>>(a);
