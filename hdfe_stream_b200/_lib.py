@@ -58,6 +58,14 @@ SIGNATURES = {
     "hdfe_rows_project": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
                                      _i32, _c.c_uint64, _i64, _i64, _i32, _i64, _vp, _vp, _vp]),
     "hdfe_jla_combine": (_c.c_int, [_vp, _i64, _i64, _vp]),
+    "hdfe_rows_reduce": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _vp, _i32,
+                                    _vp, _vp, _vp, _vp, _vp]),
+    "hdfe_rows_project_coef": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _vp,
+                                          _vp, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hdfe_trace_moments_workspace_bytes": (_i64, [_i32]),
+    "hdfe_trace_moments": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _vp, _vp,
+                                      _vp, _i32, _vp, _vp, _i64, _vp, _vp]),
+    "hdfe_rademacher": (_c.c_int, [_vp, _i64, _i64, _i32, _c.c_uint64, _i64, _vp]),
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),

@@ -124,6 +124,152 @@ class InverseOperator:
             self._ptr(res), self._ptr(moments), _lib.stream_handle()))
         return res, info
 
+    # ---- coefficient-space right-hand sides (inverse.py:311-460)
+
+    def null_space(self):
+        """inverse.py:376-428 `_null_space`: an orthonormal basis of S's null
+        space as (streamed (G, k), levels (L, k)) device blocks -- per
+        connected component, +1 on its groups and -1 on its levels of the
+        first non-streamed dimension; per further dimension, +1 across the
+        first and -1 across it.  Built once (host QR of a (G + L) x k matrix
+        of structured columns, as the reference does)."""
+        if getattr(self, "_null", None) is None:
+            torch = _torch()
+            from .fit import components, rank_components
+            cells = self.cells
+            root, _ = components(cells, 0)
+            nl0 = int(self.nlev[0])
+            cnt_first = cells.cnt[:nl0].cpu().numpy()
+            comp, n_comp = rank_components(root.cpu().numpy(), cnt_first)
+            # inverse.py:430-437 `_group_components`: each group's first row
+            first = self.rows.codes.view(-1, len(self.nlev))[self.starts[:-1], 0]
+            gcomp = comp[first.cpu().numpy().astype(np.int64)]
+            offs = np.concatenate(([0], np.cumsum(self.nlev)[:-1]))
+            vecs = []
+            for c in range(n_comp):
+                lv = np.zeros(self.L)
+                lv[offs[0]:offs[0] + nl0] = -(comp == c).astype(float)
+                vecs.append(np.concatenate([(gcomp == c).astype(float), lv]))
+            for d in range(1, len(self.nlev)):
+                lv = np.zeros(self.L)
+                lv[offs[0]:offs[0] + nl0] = 1.0
+                lv[offs[d]:offs[d] + self.nlev[d]] = -1.0
+                vecs.append(np.concatenate([np.zeros(self.G), lv]))
+            q = np.linalg.qr(np.column_stack(vecs))[0] if vecs else np.zeros((self.G + self.L, 0))
+            q = torch.as_tensor(q, device=self.dev)
+            self._null = (q[:self.G].contiguous(), q[self.G:].contiguous())
+        return self._null
+
+    def drop_null(self, levels, streamed):
+        """inverse.py:445-460 `_drop_null_component` (thin GEMMs)."""
+        qs, ql = self.null_space()
+        if ql.shape[1] == 0:
+            return levels, streamed
+        overlap = qs.T @ streamed + ql.T @ levels
+        return (levels - ql @ overlap).contiguous(), (streamed - qs @ overlap).contiguous()
+
+    def _status(self):
+        torch = _torch()
+        if getattr(self, "_st", None) is None:
+            self._st = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        return self._st
+
+    def apply_inverse(self, levels, cov_values, streamed, omega=None, rows=False):
+        """inverse.py:311-374 `apply_inverse`: u = S^- v for v in coefficient
+        space -- levels (L, B), cov_values (c, B), streamed (G, B), device
+        tensors, B <= 32.  Returns (U (L, B), C (c, B), U_streamed (G, B),
+        rows (N, B) or None).  With omega (N), also the Hutchinson trace's
+        collect sink (leaveout.py:423-431), v = A' Omega A u, as a fifth item
+        (v_levels, v_cov, v_groups)."""
+        torch = _torch()
+        lib = _lib.lib()
+        B = int(levels.shape[1])
+        if not 1 <= B <= MAX_BLOCK:
+            raise ValueError(f"apply_inverse: 1 <= B <= {MAX_BLOCK}")
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        Z, schur_inv = self.border()
+        levels, streamed = self.drop_null(levels.to(**f64), streamed.to(**f64).contiguous())
+        scale = torch.sqrt((levels * levels).sum(dim=0) + (streamed * streamed).sum(dim=0))
+        acc = torch.zeros((self.L, B), **f64)
+        acc_x = torch.zeros((max(self.c, 1), B), **f64)
+        st, sh = self._status(), _lib.stream_handle()
+        base = (self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
+                self.nlev.ctypes.data, self._ptr(self.w), self._ptr(self.X), self.c)
+        _lib.check(lib.hdfe_rows_reduce(*base, streamed.data_ptr(), None, B, acc.data_ptr(),
+                                        acc_x.data_ptr(), None, st.data_ptr(), sh))
+        rhs = levels - acc
+        U, info = self.solve_reduced(rhs.contiguous(), scale)
+        if Z is not None:
+            rhs_x = cov_values.to(**f64) - acc_x[:self.c]
+            C = (schur_inv @ (rhs_x - Z.T @ rhs)).contiguous()
+            U = (U - Z @ C).contiguous()
+        else:
+            C = None
+        U_g = torch.empty((self.G, B), **f64)
+        out_rows = torch.empty((self.N, B), **f64) if rows else None
+        v = None
+        if omega is not None:
+            v = (torch.zeros((self.L, B), **f64), torch.zeros((max(self.c, 1), B), **f64),
+                 torch.empty((self.G, B), **f64))
+        _lib.check(lib.hdfe_rows_project_coef(
+            *base, self._ptr(C), U.data_ptr(), streamed.data_ptr(), B, self._ptr(out_rows),
+            U_g.data_ptr(), self._ptr(omega), self._ptr(None if v is None else v[0]),
+            self._ptr(None if v is None else v[1]), self._ptr(None if v is None else v[2]),
+            st.data_ptr(), sh))
+        self.ainv_info = info
+        res = (U, C, U_g, out_rows)
+        if v is not None:
+            res = res + ((v[0], v[1][:self.c], v[2]),)
+        return res
+
+    def hutchinson_trace(self, sigma2, n_draws=250, block=MAX_BLOCK, seed=0, psi_column=0):
+        """leaveout.py:321-391 `hutchinson_trace` and :393-448 `_trace_block`:
+        the bias terms (var(psi), var(alpha), cov(psi, alpha)) from n_draws
+        Rademacher vectors in coefficient space, two applications of the
+        inverse per block; sigma2 (N) per-row variances.  Draws are keyed on
+        (seed, position, draw), so the answer does not depend on blocking."""
+        torch = _torch()
+        lib = _lib.lib()
+        block = int(block)
+        if block < 1 or n_draws < 1:
+            raise ValueError("n_draws and block must be at least 1")
+        block = min(block, MAX_BLOCK)
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        omega = torch.as_tensor(sigma2).to(**f64).contiguous()
+        L, G, c = self.L, self.G, self.c
+        totals = torch.zeros(8, **f64)
+        ws = torch.empty(int(lib.hdfe_trace_moments_workspace_bytes(block)), dtype=torch.uint8,
+                         device=self.dev)
+        mom = torch.empty((block, 8), **f64)
+        drawn, blocks = 0, 0
+        sh = _lib.stream_handle()
+        while drawn < n_draws:
+            size = min(block, n_draws - drawn)
+            Zall = torch.empty((L + G + c, size), **f64)
+            _lib.check(lib.hdfe_rademacher(Zall.data_ptr(), L + G + c, 0, size,
+                                           int(seed) & (2**64 - 1), drawn, sh))
+            Zl, Zg, Zc = Zall[:L], Zall[L:L + G], Zall[L + G:]
+            *_, (vl, vx, vg) = self.apply_inverse(Zl, Zc, Zg, omega=omega)
+            Ul, _, Ug, _ = self.apply_inverse(vl, vx, vg)
+            _lib.check(lib.hdfe_trace_moments(
+                self.starts.data_ptr(), G, self.rows.codes.data_ptr(), len(self.nlev),
+                self.nlev.ctypes.data, psi_column, self._ptr(self.w), Zl.data_ptr(),
+                Zg.data_ptr(), Ul.data_ptr(), Ug.data_ptr(), size, mom.data_ptr(), ws.data_ptr(),
+                ws.numel(), self._status().data_ptr(), sh))
+            totals += mom[:size].sum(dim=0)
+            drawn += size
+            blocks += 1
+        t = (totals / n_draws).cpu().numpy()
+        weight, a1a2, b1b2, cross, a1, a2, b1, b2 = t
+        var_psi = a1a2 / weight - (a1 / weight) * (a2 / weight)
+        var_alpha = b1b2 / weight - (b1 / weight) * (b2 / weight)
+        cov = 0.5 * (cross / weight - (a1 / weight) * (b2 / weight) - (b1 / weight) * (a2 / weight))
+        # leaveout_se.py:202-214 `_moment_divisor`: n - 1 person-years
+        R = float(self.N)
+        scale = weight / (weight * (R - 1.0) / R) if R > 1 else 1.0
+        self.trace_info = {"blocks": blocks, "n_obs": float(weight)}
+        return np.array([scale * var_psi, scale * var_alpha, scale * cov])
+
     def jla_leverages(self, n_draws=250, block=MAX_BLOCK, seed=0):
         """leaveout.py:130-198 `jla_leverages`: (leverage, complement, factor)
         per row (device tensors), in the square-root weight metric when the

@@ -200,6 +200,57 @@ int hdfe_rows_project(const int64_t *starts, int64_t n_groups, const uint32_t *c
 
 int hdfe_jla_combine(double *moments, int64_t n_rows, int64_t n_draws, void *stream);
 
+/* Coefficient-space right-hand sides (inverse.py:311-374 `apply_inverse`) and
+ * the Hutchinson trace's moments (leaveout.py:321-448).  Same row layout and
+ * argument conventions as above; `status` is a DEVICE uint32 that a bad code
+ * sets to HDFE_ERR_BAD_CODE, or NULL.  acc / acc_x are ADDED into (zero them
+ * first); sums over rows are in atomic order (FP64).
+ *
+ * hdfe_rows_reduce: kernels_inverse.py:112-130 `_nb_reduce_rows` (no
+ *   centring) of either explicit rows R (N, B) or, with R NULL, the streamed
+ *   block `streamed` (G, B) spread over each group's rows divided by its
+ *   weight total (kernels_inverse.py:134-152 `_nb_spread_groups`):
+ *   acc[level, j] += w_i R_ij, acc_x[c, j] += X_ic w_i R_ij; with explicit R,
+ *   group_sums (G, B) (or NULL) = sum over the group of w_i R_ij
+ *   (core/kernels_groups.py:17-27 `_nb_group_sums`).
+ * hdfe_rows_project_coef: kernels_inverse.py:157-188 `_nb_project_coef` for
+ *   the solution U (L, B), C (c, B) and the spread streamed block: rows
+ *   (N, B) = (A u)_i and groups (G, B) = the streamed block (either may be
+ *   NULL); with omega (N) given, also the collect sink of the Hutchinson
+ *   trace (leaveout.py:423-431) in the same pass: v_i = omega_i (A u)_i
+ *   reduced as hdfe_rows_reduce does into acc, acc_x and group_sums.
+ * hdfe_trace_moments: kernels_inverse.py:192-231 `_nb_trace_moments`: out
+ *   (B, 8) = per vector the eight weighted sums over rows of the psi
+ *   dimension's values a (from Z_levels, U_levels (L, B)) and the streamed
+ *   values b (Z_groups, U_groups (G, B)); the sums are per CTA in a fixed
+ *   order, then over CTAs in a fixed order.
+ * hdfe_rademacher: core/kernels_groups.py:53-76 `_nb_rademacher`: out
+ *   (n_rows, B) of +-1 from (seed, ordinal0 + row, first_draw + j),
+ *   bit-identical.
+ */
+int hdfe_rows_reduce(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                     const int64_t *n_levels, const double *w, const double *X, int32_t c,
+                     const double *streamed, const double *R, int32_t B, double *acc,
+                     double *acc_x, double *group_sums, void *status, void *stream);
+
+int hdfe_rows_project_coef(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                           int32_t D, const int64_t *n_levels, const double *w, const double *X,
+                           int32_t c, const double *C, const double *U, const double *streamed,
+                           int32_t B, double *rows, double *groups, const double *omega,
+                           double *acc, double *acc_x, double *group_sums, void *status,
+                           void *stream);
+
+int64_t hdfe_trace_moments_workspace_bytes(int32_t B);
+
+int hdfe_trace_moments(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                       const int64_t *n_levels, int32_t psi_column, const double *w,
+                       const double *Z_levels, const double *Z_groups, const double *U_levels,
+                       const double *U_groups, int32_t B, double *out, void *workspace,
+                       int64_t workspace_bytes, void *status, void *stream);
+
+int hdfe_rademacher(double *out, int64_t n_rows, int64_t ordinal0, int32_t B, uint64_t seed,
+                    int64_t first_draw, void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,

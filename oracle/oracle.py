@@ -592,6 +592,103 @@ class Design:
                                   R, U)
         return out * root[:, None] if sqrt_weights else out
 
+    # ---- coefficient-space right-hand sides (inverse.py:311-460)
+
+    def null_space(self):
+        """inverse.py:376-428 `_null_space`: an orthonormal basis of S's null
+        space in (streamed, levels) blocks -- per connected component, +1 on
+        its groups and -1 on its levels of the first non-streamed dimension;
+        per further dimension, +1 across the first and -1 across it."""
+        if getattr(self, "_null", None) is None:
+            cells, starts = self.cells, self.starts
+            G, L = len(starts) - 1, cells.L
+            D = len(cells.n_levels)
+            comp, _ = component_labels(cells)
+            n_comp = int(comp.max()) + 1 if len(comp) else 0
+            # inverse.py:430-437 `_group_components`: the component of each
+            # group's first row's first-dimension level
+            gcomp = comp[self.codes[starts[:-1], 0].astype(np.int64)]
+            off = cells.offs
+            vecs = []
+            for c in range(n_comp):
+                lv = np.zeros(L)
+                lv[off[0]:off[0] + cells.n_levels[0]] = -(comp == c).astype(float)
+                vecs.append(np.concatenate([(gcomp == c).astype(float), lv]))
+            for d in range(1, D):
+                lv = np.zeros(L)
+                lv[off[0]:off[0] + cells.n_levels[0]] = 1.0
+                lv[off[d]:off[d] + cells.n_levels[d]] = -1.0
+                vecs.append(np.concatenate([np.zeros(G), lv]))
+            if vecs:
+                q, _ = np.linalg.qr(np.column_stack(vecs))
+            else:
+                q = np.zeros((G + L, 0))
+            self._null = (q[:G], q[G:])
+        return self._null
+
+    def drop_null(self, levels, streamed):
+        """inverse.py:445-460 `_drop_null_component`."""
+        qs, ql = self.null_space()
+        if ql.shape[1] == 0:
+            return levels, streamed
+        overlap = qs.T @ streamed + ql.T @ levels
+        return levels - ql @ overlap, streamed - qs @ overlap
+
+    def apply_inverse(self, levels, cov_values, streamed, row_weights=None):
+        """inverse.py:311-374 `apply_inverse`: (U_levels, C, U_streamed, rows)
+        for a coefficient-space right-hand side; rows = (A u)_i.  With
+        row_weights, also the collect sink of leaveout.py:423-431: v = A' Omega
+        rows as (v_levels, v_cov, v_groups)."""
+        cells, starts = self.cells, self.starts
+        B = levels.shape[1]
+        Z, schur_inv = self.border()
+        levels, streamed = self.drop_null(np.asarray(levels, float), np.asarray(streamed, float))
+        scale = np.sqrt((levels * levels).sum(axis=0) + (streamed * streamed).sum(axis=0))
+        rho = spread_groups(starts, self.w, streamed)
+        acc, acc_x = reduce_rows(starts, self.codes, cells.offs, self.w, self.X, rho, cells.L,
+                                 self.nt)
+        rhs = levels - acc
+        rhs_x = np.asarray(cov_values, float) - acc_x
+        U = self.solve_reduced(rhs, scale)
+        if Z is not None:
+            C = schur_inv @ (rhs_x - Z.T @ rhs)
+            U = U - Z @ C
+        else:
+            C = np.zeros((0, B))
+        rows, groups = project_coef(starts, self.codes, cells.offs, self.w, self.X, C, rho, U)
+        out = (U, C, groups, rows)
+        if row_weights is not None:
+            weighted = rows * np.asarray(row_weights, float)[:, None]
+            v, v_x = reduce_rows(starts, self.codes, cells.offs, self.w, self.X, weighted,
+                                 cells.L, self.nt)
+            out = out + ((v, v_x, group_sums(starts, self.w, weighted)),)
+        return out
+
+    def hutchinson_trace(self, sigma2, n_draws, block, seed, psi_column=0):
+        """leaveout.py:321-391 `hutchinson_trace` with :393-448
+        `_trace_block`: the bias terms (var(psi), var(alpha), cov)."""
+        cells, starts = self.cells, self.starts
+        G, L, c = len(starts) - 1, cells.L, self.X.shape[1]
+        totals = np.zeros(8)
+        drawn = 0
+        while drawn < n_draws:
+            size = min(block, n_draws - drawn)
+            Zall = rademacher(0, L + G + c, size, seed, drawn)
+            Zl, Zg, Zc = Zall[:L], Zall[L:L + G], Zall[L + G:]
+            *_, (vl, vx, vg) = self.apply_inverse(Zl, Zc, Zg, row_weights=sigma2)
+            Ul, _, Ug, _ = self.apply_inverse(vl, vx, vg)
+            totals += trace_moments(starts, self.codes, psi_column, int(cells.offs[psi_column]),
+                                    self.w, Zl, Zg, Ul, Ug, self.nt).sum(axis=(0, 1))
+            drawn += size
+        weight, a1a2, b1b2, cross, a1, a2, b1, b2 = totals / n_draws
+        var_psi = a1a2 / weight - (a1 / weight) * (a2 / weight)
+        var_alpha = b1b2 / weight - (b1 / weight) * (b2 / weight)
+        cov = 0.5 * (cross / weight - (a1 / weight) * (b2 / weight) - (b1 / weight) * (a2 / weight))
+        # leaveout_se.py:202-214 `_moment_divisor`: n - 1 person-years
+        R = float(self.rows.n_rows)
+        scale = weight / (weight * (R - 1.0) / R) if R > 1 else 1.0
+        return np.array([scale * var_psi, scale * var_alpha, scale * cov])
+
     def jla_leverages(self, n_draws, block, seed):
         """leaveout.py:130-198 `jla_leverages` and :210-282
         `_combine_moments`: (leverage, complement, factor)."""

@@ -124,3 +124,48 @@ def test_long_groups_and_block_widths(device, weights):
     lev, _, f = op.jla_leverages(45, block=32, seed=4)
     assert rel(lev.cpu().numpy(), lev_ref) < 1e-8
     assert rel(f.cpu().numpy(), f_ref) < 1e-8
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_apply_inverse_matches_reference(device, name):
+    """S^- v for a coefficient-space v (inverse.py `apply_inverse`): the
+    solution, its streamed block and the rows' (A u)_i against the
+    reference's outputs, null-space component dropped as there."""
+    import torch
+    g = load_golden(name)
+    rows = golden_rows(g)
+    op = operator(rows, float(g["tol"]))
+    dev = torch.device("cuda")
+    U, C, Ug, R = op.apply_inverse(torch.as_tensor(g["ainv_levels"], device=dev),
+                                   torch.zeros((0, 3), dtype=torch.float64, device=dev),
+                                   torch.as_tensor(g["ainv_groups"], device=dev), rows=True)
+    assert rel(U.cpu().numpy(), g["ainv_U"]) < 1e-8
+    assert rel(Ug.cpu().numpy(), g["ainv_Ug"]) < 1e-8
+    assert rel(R.cpu().numpy(), g["ainv_rows"]) < 1e-8
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_hutchinson_trace_matches_reference(device, name):
+    """leaveout.py `hutchinson_trace`: var(psi), var(alpha), cov for 16
+    draws in blocks of 8, against the reference's numbers."""
+    g = load_golden(name)
+    rows = golden_rows(g)
+    op = operator(rows, float(g["tol"]))
+    tr = op.hutchinson_trace(g["trace_sigma2"], n_draws=16, block=8, seed=4)
+    assert rel(tr, g["trace"]) < 1e-8
+
+
+def test_hutchinson_blocking_and_covariates(device):
+    """With the model's covariates (Schur border) against the oracle, and
+    the same answer whatever the blocking."""
+    g = load_golden("akm_weighted")
+    rows = golden_rows(g)
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), X=rows.V[:, 1:], tol=1e-12)
+    sigma2 = g["trace_sigma2"]
+    ref = des.hutchinson_trace(sigma2, 20, 20, 3)
+    op = operator(rows, 1e-12, covariates=True)
+    a = op.hutchinson_trace(sigma2, n_draws=20, block=20, seed=3)
+    b = op.hutchinson_trace(sigma2, n_draws=20, block=7, seed=3)
+    assert rel(a, ref) < 1e-8
+    assert rel(a, b) < 1e-9

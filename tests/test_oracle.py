@@ -136,3 +136,27 @@ def test_jla_leverages_match_reference(cells):
     lev, comp, factor = des.jla_leverages(24, 8, 2)
     assert rel(lev, g["jla_leverage"]) < 1e-9
     assert rel(factor, g["jla_factor"]) < 1e-9
+
+
+def test_apply_inverse_matches_reference(golden):
+    """inverse.py `apply_inverse` on a coefficient-space right-hand side
+    (levels and groups, null-space component dropped): U, the streamed block
+    and the rows' (A u)_i against the reference's outputs."""
+    _, g = golden
+    rows = golden_rows(g)
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g["tol"]))
+    U, C, Ug, R = des.apply_inverse(g["ainv_levels"], np.zeros((0, 3)), g["ainv_groups"])
+    for got, ref in ((U, g["ainv_U"]), (Ug, g["ainv_Ug"]), (R, g["ainv_rows"])):
+        assert np.max(np.abs(got - ref)) < 1e-10 * np.max(np.abs(ref))
+
+
+def test_hutchinson_trace_matches_reference(golden):
+    """leaveout.py `hutchinson_trace`: the three bias terms for 16 draws in
+    blocks of 8."""
+    _, g = golden
+    rows = golden_rows(g)
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g["tol"]))
+    tr = des.hutchinson_trace(g["trace_sigma2"], 16, 8, 4)
+    assert np.max(np.abs(tr - g["trace"])) < 1e-10 * np.max(np.abs(g["trace"]))
