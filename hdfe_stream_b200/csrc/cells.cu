@@ -462,7 +462,8 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
     const int NS = kSlotFixed + m;                  // values per level slot
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *w_slots = s_dyn + (int64_t)warp * dm.n_small * NS;           // this warp's small levels
-    double *w_scr = s_dyn + (int64_t)kWarpsPerCta * dm.n_small * NS + warp * 32 * NS;
+    const int NSP = NS | 1;                         // scratch row stride: odd, no bank conflicts
+    double *w_scr = s_dyn + (int64_t)kWarpsPerCta * dm.n_small * NS + warp * 32 * NSP;
     for (int64_t k = threadIdx.x; k < (int64_t)kWarpsPerCta * dm.n_small * NS; k += kThreads)
         s_dyn[k] = 0.0;
     __syncthreads();
@@ -605,7 +606,7 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
 #pragma unroll
                     for (int v = 0; v <= kV; v++) {
                         if (v > m) break;
-                        w_scr[lane * NS + v] = x[v];
+                        w_scr[lane * NSP + v] = x[v];
                     }
                 }
                 __syncwarp();
@@ -618,11 +619,11 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
                     for (int v = 0; v < kV; v++) sv[v] = 0.0;
                     for (unsigned b = mk1; b; b &= b - 1) {
                         const int l = __ffs(b) - 1;
-                        u += w_scr[l * NS];
+                        u += w_scr[l * NSP];
 #pragma unroll
                         for (int v = 0; v < kV; v++) {
                             if (v >= m) break;
-                            sv[v] += w_scr[l * NS + 1 + v];
+                            sv[v] += w_scr[l * NSP + 1 + v];
                         }
                     }
                     T[0] = u;
@@ -647,7 +648,7 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
 #pragma unroll
                     for (int q = 0; q < kSlotFixed + kV; q++) {
                         if (q >= NS) break;
-                        w_scr[lane * NS + q] = T[q];
+                        w_scr[lane * NSP + q] = T[q];
                     }
                 }
                 __syncwarp();
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
 #pragma unroll
                         for (int q = 0; q < kSlotFixed + kV; q++) {
                             if (q >= NS) break;
-                            T[q] += w_scr[l * NS + q];
+                            T[q] += w_scr[l * NSP + q];
                         }
                     }
                     if (dm.small[d]) {
@@ -860,7 +861,7 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     HDFE_CUDA_TRY(cudaGetDevice(&dev));
     HDFE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // the warps' small-level slots, then their 32-lane scratch rows
-    const size_t smem = (size_t)(slots * per_level) + (size_t)kWarpsPerCta * 32 * (kSlotFixed + m) * 8;
+    const size_t smem = (size_t)(slots * per_level) + (size_t)kWarpsPerCta * 32 * ((kSlotFixed + m) | 1) * 8;
     void (*kern)(GroupArgs, double *) = m == 1 ? groups_work<D, 1> : m == 2 ? groups_work<D, 2>
                                        : m == 3 ? groups_work<D, 3> : m == 4 ? groups_work<D, 4>
                                        : groups_work<D, 0>;

@@ -62,7 +62,9 @@ struct Params {
     const int64_t *indptr;
     const int32_t *indices;
     const double *data;
-    int64_t L, nnz, chunk;
+    int64_t L, nnz;
+    const int64_t *wlo;     // (warps + 1) first nonzero of each warp's range
+    int64_t nwarps;
     const double *dinv;
     const double *B;
     const uint8_t *zero;
@@ -81,7 +83,7 @@ struct Params {
 // Workspace layout in bytes: R (L*K), P (L*KP), AP (L*K), carry, part,
 // wfirst, cut flags, then the barrier words.
 struct Layout {
-    int64_t r, p, ap, carry, part, wfirst, cut, bar, total;
+    int64_t r, p, ap, carry, part, wfirst, wlo, cut, bar, total;
 };
 
 inline Layout layout(int64_t L, int k, int64_t blocks)
@@ -97,6 +99,7 @@ inline Layout layout(int64_t L, int k, int64_t blocks)
     o.carry = take(warps * 2 * k * 8);
     o.part = take(4 * (int64_t)k * blocks * 8);
     o.wfirst = take(warps * 8);
+    o.wlo = take((warps + 1) * 8);
     o.cut = take(L);
     o.bar = take(64);
     o.total = p;
@@ -111,6 +114,47 @@ __device__ __forceinline__ int64_t upper_bound(const int64_t *a, int64_t n, int6
         if (a[mid] <= x) lo = mid + 1; else hi = mid;
     }
     return lo;
+}
+
+// The warp holding nonzero e: the last warp whose range starts at or before e.
+__device__ __forceinline__ int64_t warp_of(const Params &a, int64_t e)
+{
+    return upper_bound(a.wlo, a.nwarps + 1, e) - 1;
+}
+
+// Warp ranges of S's nonzeros balanced by cost: a row costs its nonzeros plus
+// kRowCost (the per-row work of a short row's setup and write-back), so warps
+// of short rows take fewer nonzeros than warps inside long rows.
+// The lane kernel's nonzeros are heavy (K-wide gathers), so its rows cost
+// their nonzeros alone.
+#ifndef HDFE_PCG_ROW_COST
+#define HDFE_PCG_ROW_COST 32
+#endif
+constexpr int64_t kRowCost = HDFE_PCG_ROW_COST;
+
+__global__ void k_partition(const int64_t *indptr, int64_t L, int64_t nnz, int64_t nwarps,
+                            int64_t row_cost, int64_t *wlo)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > nwarps) return;
+    const int64_t kRowCost = row_cost;
+    const int64_t total = nnz + kRowCost * L;
+    const int64_t T = t * total / nwarps;
+    // the last row r with indptr[r] + kRowCost r <= T
+    int64_t lo = 0, hi = L;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (indptr[mid] + kRowCost * mid <= T) lo = mid; else hi = mid - 1;
+    }
+    const int64_t r = lo;
+    int64_t at;
+    if (r >= L) {
+        at = nnz;
+    } else {
+        const int64_t first = indptr[r] + kRowCost * (r + 1);   // where the row's nonzeros start
+        at = T < first ? indptr[r] : min(indptr[r] + (T - first), indptr[r + 1]);
+    }
+    wlo[t] = t == nwarps ? nnz : at;
 }
 
 // Sum of partial q over all CTAs, in fixed order; lane-parallel within one
@@ -252,8 +296,8 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
 {
     const int lane = threadIdx.x & 31, sub = lane >> 3, sl = lane & 7;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int64_t lo = gw * a.chunk;
-    const int64_t hi = min(lo + a.chunk, a.nnz);
+    const int64_t lo = a.wlo[gw];
+    const int64_t hi = a.wlo[gw + 1];
     if (lo >= hi) return;
     int64_t r0 = a.wfirst[gw];
     for (;;) {
@@ -331,17 +375,18 @@ __device__ bool finish_cut_row(const Params &a, const T *carry, int64_t &row, T 
 {
     const int lane = threadIdx.x & 31;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int64_t lo = gw * a.chunk;
-    const int64_t hi = min(lo + a.chunk, a.nnz);
+    const int64_t lo = a.wlo[gw];
+    const int64_t hi = a.wlo[gw + 1];
     if (lo >= hi) return false;
     const int64_t r = a.wfirst[gw];
     const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
     if (!(rs < lo && re <= hi)) return false;
-    const int64_t w0 = rs / a.chunk;
+    const int64_t w0 = warp_of(a, rs);
     T s[K];
 #pragma unroll
     for (int k = 0; k < K; k++) s[k] = T(0);
     for (int64_t w = w0 + lane; w <= gw; w += 32) {
+        if (a.wlo[w] == a.wlo[w + 1]) continue;         // an empty range wrote no slots
         const T *cs = carry + (w * 2 + (w == w0 ? 1 : 0)) * K;
 #pragma unroll
         for (int k = 0; k < K; k++) s[k] += __ldcg(cs + k);
@@ -401,12 +446,12 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
     // warps / threads later, so no barrier is needed for them)
     {
         const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-        const int64_t lo = gw * a.chunk;
+        const int64_t lo = a.wlo[gw];
         if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
         __syncwarp();
         for (int64_t r = gtid; r < L; r += gstride) {
             const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
-            a.cut[r] = (re > rs && (rs / a.chunk) != ((re - 1) / a.chunk)) ? 1 : 0;
+            a.cut[r] = (re > rs && warp_of(a, rs) != warp_of(a, re - 1)) ? 1 : 0;
         }
     }
     // ---- R = B - S X0 (or B), the zero columns, ||B||, rz
@@ -688,7 +733,7 @@ inline bool use_lanes(int k) { return k >= HDFE_PCG_LANE_FROM || k > 8; }
 inline int lane_width(int k) { return k <= 8 ? 8 : (k <= 16 ? 16 : 32); }
 
 struct LaneLayout {
-    int64_t r, p, ap, x, carry, part, wfirst, cut, bar, total;
+    int64_t r, p, ap, x, carry, part, wfirst, wlo, cut, bar, total;
 };
 
 // R, P, AP (L, K); X (L, K) unless the caller's X has K columns already
@@ -706,6 +751,7 @@ inline LaneLayout lane_layout(int64_t L, int k, int64_t blocks)
     o.carry = take(warps * 2 * kw * 8);
     o.part = take(3 * (int64_t)kw * blocks * 8);
     o.wfirst = take(warps * 8);
+    o.wlo = take((warps + 1) * 8);
     o.cut = take(L);
     o.bar = take(64);
     o.total = p;
@@ -760,8 +806,8 @@ __device__ void lane_spmm(const Params &a, const double *__restrict__ V, double 
     constexpr int H = 32 / K, NS = kLaneStages;
     const int lane = threadIdx.x & 31, col = lane % K, sub = lane / K;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int64_t lo = gw * a.chunk;
-    const int64_t hi = min(lo + a.chunk, a.nnz);
+    const int64_t lo = a.wlo[gw];
+    const int64_t hi = a.wlo[gw + 1];
     if (lo >= hi) return;
     double *vals = stage;                   // [NS][32][K]
     double *wts = stage + NS * 32 * K;      // [NS][32]
@@ -861,15 +907,16 @@ __device__ bool lane_finish_cut(const Params &a, const double *carry, int64_t &r
 {
     const int col = (threadIdx.x & 31) % K;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int64_t lo = gw * a.chunk;
-    const int64_t hi = min(lo + a.chunk, a.nnz);
+    const int64_t lo = a.wlo[gw];
+    const int64_t hi = a.wlo[gw + 1];
     if (lo >= hi) return false;
     const int64_t r = a.wfirst[gw];
     const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
     if (!(rs < lo && re <= hi)) return false;
-    const int64_t w0 = rs / a.chunk;
+    const int64_t w0 = warp_of(a, rs);
     double s = 0.0;
-    for (int64_t w = w0; w <= gw; w++) s += __ldcg(carry + (w * 2 + (w == w0 ? 1 : 0)) * K + col);
+    for (int64_t w = w0; w <= gw; w++)
+        if (a.wlo[w] != a.wlo[w + 1]) s += __ldcg(carry + (w * 2 + (w == w0 ? 1 : 0)) * K + col);
     ap = s;
     row = r;
     return true;
@@ -923,12 +970,12 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
     // ---- set-up: each warp's first row and the cut flags
     {
         const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-        const int64_t lo = gw * a.chunk;
+        const int64_t lo = a.wlo[gw];
         if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
         __syncwarp();
         for (int64_t r = gtid; r < L; r += gstride) {
             const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
-            a.cut[r] = (re > rs && (rs / a.chunk) != ((re - 1) / a.chunk) ? kRowCut : 0) |
+            a.cut[r] = (re > rs && warp_of(a, rs) != warp_of(a, re - 1) ? kRowCut : 0) |
                        (re == rs ? kRowEmpty : 0);
         }
     }
@@ -1156,7 +1203,7 @@ int solve_lanes(const int64_t *indptr, const int32_t *indices, const double *dat
     p.L = L;
     p.nnz = nnz;
     const int64_t warps = (int64_t)blocks * (lane_threads(kw) / 32);
-    p.chunk = nnz > 0 ? (nnz + warps - 1) / warps : 1;
+    p.nwarps = warps;
     p.dinv = dinv;
     p.B = B;
     p.zero = zero;
@@ -1170,6 +1217,7 @@ int solve_lanes(const int64_t *indptr, const int32_t *indices, const double *dat
     p.carry = (double *)(ws + lay.carry);
     p.part = (double *)(ws + lay.part);
     p.wfirst = (int64_t *)(ws + lay.wfirst);
+    p.wlo = (int64_t *)(ws + lay.wlo);
     p.cut = (uint8_t *)(ws + lay.cut);
     p.bar = (unsigned *)(ws + lay.bar);
     p.info = info;
@@ -1177,13 +1225,15 @@ int solve_lanes(const int64_t *indptr, const int32_t *indices, const double *dat
     x.Xw = lay.x < 0 ? X : (double *)(ws + lay.x);
     x.k = k;
     HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
+    pcg::k_partition<<<(unsigned)((p.nwarps + 256) / 256), 256, 0, s>>>(indptr, L, nnz, p.nwarps,
+                                                                      0, (int64_t *)p.wlo);
     cudaError_t e = kw == 8 ? launch_lanes<8>(p, x, blocks, s)
                   : kw == 16 ? launch_lanes<16>(p, x, blocks, s)
                              : launch_lanes<32>(p, x, blocks, s);
     HDFE_CUDA_TRY(e);
     pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);
     HDFE_CUDA_TRY(cudaGetLastError());
-    hdfe_add_launches(2);
+    hdfe_add_launches(3);
     return HDFE_OK;
 }
 
@@ -1233,7 +1283,7 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     p.L = L;
     p.nnz = nnz;
     const int64_t warps = (int64_t)blocks * (pcg::threads_for(k) / 32);
-    p.chunk = nnz > 0 ? (nnz + warps - 1) / warps : 1;
+    p.nwarps = warps;
     p.dinv = dinv;
     p.B = B;
     p.zero = zero;
@@ -1247,10 +1297,13 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     p.carry = (double *)(ws + lay.carry);
     p.part = (double *)(ws + lay.part);
     p.wfirst = (int64_t *)(ws + lay.wfirst);
+    p.wlo = (int64_t *)(ws + lay.wlo);
     p.cut = (uint8_t *)(ws + lay.cut);
     p.bar = (unsigned *)(ws + lay.bar);
     p.info = info;
     HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
+    pcg::k_partition<<<(unsigned)((p.nwarps + 256) / 256), 256, 0, s>>>(indptr, L, nnz, p.nwarps,
+                                                                      pcg::kRowCost, (int64_t *)p.wlo);
     cudaError_t e = cudaErrorInvalidValue;
     switch (k) {
     case 1: e = pcg::launch<1>(p, blocks, s); break;
@@ -1265,7 +1318,7 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     HDFE_CUDA_TRY(e);
     pcg::pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);
     HDFE_CUDA_TRY(cudaGetLastError());
-    hdfe_add_launches(2);
+    hdfe_add_launches(3);
     return HDFE_OK;
 }
 
@@ -1342,7 +1395,7 @@ struct Mixed {
 };
 
 struct MixedLayout {
-    int64_t r, p, ap, d, ax, carry, part, wfirst, cut, bar, total;
+    int64_t r, p, ap, d, ax, carry, part, wfirst, wlo, cut, bar, total;
 };
 
 inline MixedLayout mixed_layout(int64_t L, int k, int64_t blocks)
@@ -1360,6 +1413,7 @@ inline MixedLayout mixed_layout(int64_t L, int k, int64_t blocks)
     o.carry = take(warps * 2 * k * 8);
     o.part = take(4 * (int64_t)k * blocks * 8);
     o.wfirst = take(warps * 8);
+    o.wlo = take((warps + 1) * 8);
     o.cut = take(L);
     o.bar = take(64);
     o.total = p;
@@ -1392,7 +1446,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) mixed_kernel(Params a, Mixe
     // each warp's first row and the cut flags, X = X0 (or 0), ||B||
     {
         const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-        const int64_t lo = gw * a.chunk;
+        const int64_t lo = a.wlo[gw];
         if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
         __syncwarp();
         double sb[K];
@@ -1400,7 +1454,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) mixed_kernel(Params a, Mixe
         for (int k = 0; k < K; k++) sb[k] = 0.0;
         for (int64_t r = gtid; r < L; r += gstride) {
             const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
-            a.cut[r] = (re > rs && (rs / a.chunk) != ((re - 1) / a.chunk)) ? 1 : 0;
+            a.cut[r] = (re > rs && warp_of(a, rs) != warp_of(a, re - 1)) ? 1 : 0;
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 const double b = a.B[r * K + k];
@@ -1702,7 +1756,7 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
     p.L = L;
     p.nnz = nnz;
     const int64_t warps = (int64_t)blocks * (pcg::threads_for(k) / 32);
-    p.chunk = nnz > 0 ? (nnz + warps - 1) / warps : 1;
+    p.nwarps = warps;
     p.dinv = dinv;
     p.B = B;
     p.zero = zero;
@@ -1713,6 +1767,7 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
     p.carry = (double *)(ws + lay.carry);
     p.part = (double *)(ws + lay.part);
     p.wfirst = (int64_t *)(ws + lay.wfirst);
+    p.wlo = (int64_t *)(ws + lay.wlo);
     p.cut = (uint8_t *)(ws + lay.cut);
     p.bar = (unsigned *)(ws + lay.bar);
     p.info = info;
@@ -1725,6 +1780,8 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
     m.AX = (double *)(ws + lay.ax);
     m.inner_tol = inner_tol;
     HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
+    pcg::k_partition<<<(unsigned)((p.nwarps + 256) / 256), 256, 0, s>>>(indptr, L, nnz, p.nwarps,
+                                                                      pcg::kRowCost, (int64_t *)p.wlo);
     cudaError_t e = cudaErrorInvalidValue;
     switch (k) {
     case 1: e = pcg::launch_mixed<1>(p, m, blocks, s); break;
@@ -1739,6 +1796,6 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
     HDFE_CUDA_TRY(e);
     pcg::pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);
     HDFE_CUDA_TRY(cudaGetLastError());
-    hdfe_add_launches(2);
+    hdfe_add_launches(3);
     return HDFE_OK;
 }
