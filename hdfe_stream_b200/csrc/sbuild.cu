@@ -38,6 +38,9 @@ namespace hdfe {
 namespace sbuild {
 
 constexpr int kThreads = 256;
+constexpr int kSmallSlots = 256;                // hash slots per warp (small warp rows)
+constexpr int kSmallListCap = 64;               // groups per small warp row
+constexpr int kSmallWarpsPerCta = 8;
 constexpr int kWarpSlots = 512;                 // max hash slots per warp (warp rows)
 constexpr int kBlockSlots = 8192;               // max hash slots per CTA (block rows)
 constexpr int kWarpListCap = 128;               // groups per warp row
@@ -50,9 +53,6 @@ constexpr int kScanTile = 4096;
 constexpr int64_t kSeg = 16384;                 // columns per wide-row segment
 constexpr int kWarpsPerCta = 4;
 
-// work thresholds: distinct columns <= work * D must stay <= 3/4 of a table
-__host__ __device__ inline int64_t warp_work(int D) { return (kWarpSlots * 3 / 4) / D; }
-__host__ __device__ inline int64_t block_work(int D) { return (kBlockSlots * 3 / 4) / D; }
 
 __host__ __device__ inline int ceil_log2(int64_t x)
 {
@@ -142,17 +142,27 @@ __global__ void __launch_bounds__(kThreads) k_level_stats(Args a)
 
 __global__ void __launch_bounds__(kThreads) k_classify(Args a)
 {
-    const int64_t ww = warp_work(a.D), bw = block_work(a.D);
     for (int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x; r < a.L;
          r += (int64_t)gridDim.x * kThreads) {
         const unsigned long long w = a.work[r];
         const int32_t lc = a.lcount[r];
+        // distinct columns of the row: at most min(items, levels) per dimension
+        int64_t cap = 0;
+        for (int d = 0; d < a.D; d++) cap += (int64_t)w < a.nlev[d] ? (int64_t)w : a.nlev[d];
+        if (cap > a.L) cap = a.L;
         int32_t k;
         if (w == 0) k = kKindEmpty;
-        else if ((int64_t)w <= ww && lc <= kWarpListCap) k = kKindWarp;
-        else if ((int64_t)w <= bw && lc <= kBlockListCap) k = kKindBlock;
+        else if (cap <= kSmallSlots * 3 / 4 && lc <= kSmallListCap) k = kKindWarp;
+        else if (cap <= kWarpSlots * 3 / 4 && lc <= kWarpListCap) k = kKindWarp;
+        else if (cap <= kBlockSlots * 3 / 4 && lc <= kBlockListCap) k = kKindBlock;
         else k = kKindWide;
-        if (k == kKindWarp) a.warp_rows[atomicAdd((unsigned long long *)(a.ctr + 1), 1ull)] = (int32_t)r;
+        if (k == kKindWarp) {
+            if (cap <= kSmallSlots * 3 / 4 && lc <= kSmallListCap)   // small rows from the front
+                a.warp_rows[atomicAdd((unsigned long long *)(a.ctr + 1), 1ull)] = (int32_t)r;
+            else                                                      // the others from the back
+                a.warp_rows[a.L - 1 - (int64_t)atomicAdd((unsigned long long *)(a.ctr + 6), 1ull)] =
+                    (int32_t)r;
+        }
         if (k == kKindBlock) a.block_rows[atomicAdd((unsigned long long *)(a.ctr + 2), 1ull)] = (int32_t)r;
         if (k == kKindWide) {
             const int64_t wi = (int64_t)atomicAdd((unsigned long long *)a.ctr, 1ull);
@@ -162,9 +172,7 @@ __global__ void __launch_bounds__(kThreads) k_classify(Args a)
         a.kind[r] = k;
         const bool narrow = k == kKindWarp || k == kKindBlock;
         a.lptr[r] = narrow ? lc : 0;
-        // capacity of the row in the temp buffer: its distinct columns at most
-        const int64_t cap = (int64_t)w * a.D < a.L ? (int64_t)w * a.D : a.L;
-        a.toff[r] = narrow ? cap : 0;
+        a.toff[r] = narrow ? cap : 0;   // capacity of the row in the temp buffer
     }
 }
 
@@ -486,6 +494,26 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
     __syncwarp();
 }
 
+// small warp rows (the front of warp_rows): 256-slot tables, 8 warps per CTA
+__global__ void __launch_bounds__(kSmallWarpsPerCta * 32) k_small_rows(Args a)
+{
+    __shared__ int32_t s_keys[kSmallWarpsPerCta][kSmallSlots];
+    __shared__ double s_vals[kSmallWarpsPerCta][kSmallSlots];
+    __shared__ int32_t s_list[kSmallWarpsPerCta][kSmallListCap];
+    __shared__ int32_t s_loff[kSmallWarpsPerCta][kSmallListCap + 1];
+    __shared__ int64_t s_gs[kSmallWarpsPerCta][kSmallListCap];
+    __shared__ double s_wv[kSmallWarpsPerCta][kSmallListCap];
+    __shared__ double s_stage[kSmallWarpsPerCta][32];
+    __shared__ int s_cnt[kSmallWarpsPerCta];
+    const int w = threadIdx.x >> 5;
+    RowSmem sm{s_keys[w], s_vals[w], s_list[w], s_loff[w], s_gs[w], s_wv[w], s_stage[w], &s_cnt[w]};
+    const int64_t nrows = a.ctr[1];
+    for (int64_t k = (int64_t)blockIdx.x * kSmallWarpsPerCta + w; k < nrows;
+         k += (int64_t)gridDim.x * kSmallWarpsPerCta)
+        narrow_row(a, a.warp_rows[k], sm, 8);
+}
+
+// the other warp rows (the back of warp_rows): 512-slot tables
 __global__ void __launch_bounds__(kWarpsPerCta * 32) k_warp_rows(Args a)
 {
     __shared__ int32_t s_keys[kWarpsPerCta][kWarpSlots];
@@ -498,10 +526,10 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_warp_rows(Args a)
     __shared__ int s_cnt[kWarpsPerCta];
     const int w = threadIdx.x >> 5;
     RowSmem sm{s_keys[w], s_vals[w], s_list[w], s_loff[w], s_gs[w], s_wv[w], s_stage[w], &s_cnt[w]};
-    const int64_t nrows = a.ctr[1];
+    const int64_t nrows = a.ctr[6];
     for (int64_t k = (int64_t)blockIdx.x * kWarpsPerCta + w; k < nrows;
          k += (int64_t)gridDim.x * kWarpsPerCta)
-        narrow_row(a, a.warp_rows[k], sm, 9);
+        narrow_row(a, a.warp_rows[a.L - 1 - k], sm, 9);
 }
 
 // block rows: one warp per CTA with the large table in dynamic shared memory
@@ -530,9 +558,10 @@ __global__ void __launch_bounds__(kThreads) k_copy_narrow(Args a)
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
-    const int64_t n1 = a.ctr[1], n2 = a.ctr[2];
-    for (int64_t k = gw; k < n1 + n2; k += nw) {
-        const int64_t r = k < n1 ? a.warp_rows[k] : a.block_rows[k - n1];
+    const int64_t n1 = a.ctr[1], n6 = a.ctr[6], n2 = a.ctr[2];
+    for (int64_t k = gw; k < n1 + n6 + n2; k += nw) {
+        const int64_t r = k < n1 ? a.warp_rows[k]
+                        : k < n1 + n6 ? a.warp_rows[a.L - 1 - (k - n1)] : a.block_rows[k - n1 - n6];
         const int64_t src = a.toff[r], dst = a.indptr[r], cnt = a.rnnz[r];
         for (int64_t i = lane; i < cnt; i += 32) {
             a.indices[dst + i] = a.tcol[src + i];
@@ -815,7 +844,7 @@ __global__ void k_write_info(Args a, hdfe_sbuild_info *info)
     if (threadIdx.x != 0) return;
     info->L = a.L;
     info->n_wide = a.ctr[0];
-    info->n_warp_rows = a.ctr[1];
+    info->n_warp_rows = a.ctr[1] + a.ctr[6];
     info->n_block_rows = a.ctr[2];
     info->lgrp_len = a.ctr[3];
     info->nnz = a.ctr[4];
@@ -1070,11 +1099,12 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
         launched++;
     }
     HDFE_CUDA_TRY(cudaMemsetAsync(a.rnnz, 0, (a.L + 1) * 8, c.s));
+    k_small_rows<<<(unsigned)(c.sms * 6), kSmallWarpsPerCta * 32, 0, c.s>>>(a);
     k_warp_rows<<<(unsigned)(c.sms * 8), kWarpsPerCta * 32, 0, c.s>>>(a);
     HDFE_CUDA_TRY(cudaFuncSetAttribute(k_block_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kBlockSmem));
     k_block_rows<<<(unsigned)(c.sms), 32, kBlockSmem, c.s>>>(a);
-    launched += 2;
+    launched += 3;
     if (n_wide > 0) {
         if (n_wide <= kWideWarp) {
             k_wide_block_warp<<<(unsigned)a.wide_ctas, kWideThreads, 0, c.s>>>(a);
