@@ -158,37 +158,46 @@ __global__ void __launch_bounds__(kThreads) rows_count(RowArgs a)
 }
 
 // Exclusive scan of `ncols` int64 columns of (tiles, ncols) in place, fixed
-// order, one CTA; totals to out_totals.  Optionally reduces the moment
-// columns into means and sums of squared deviations.
+// order, one CTA of 1024 threads (each a contiguous run of tiles, combined by
+// warp scans); totals to out_totals.  Optionally reduces the moment columns
+// into means and sums of squared deviations (fixed-order tree sums).
 __global__ void __launch_bounds__(1024) scan_tiles(int64_t *cnt, int64_t tiles, int ncols,
                                                    int64_t *out_totals, const double *mom, int m,
                                                    int64_t N, double *means, double *ss)
 {
-    __shared__ int64_t s_part[1024];
-    __shared__ double s_d[1024];
-    const int T = blockDim.x;
+    __shared__ int64_t s_w[32];
+    __shared__ double s_d[32];
+    const int T = blockDim.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t per = (tiles + T - 1) / T;
     const int64_t b0 = threadIdx.x * per, b1 = min(b0 + per, tiles);
     for (int c = 0; c < ncols; c++) {
         int64_t s = 0;
         for (int64_t b = b0; b < b1; b++) s += cnt[b * ncols + c];
-        s_part[threadIdx.x] = s;
+        // exclusive prefix over threads: warp scans, then the warps' totals
+        int64_t x = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_w[warp] = x;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int64_t run = 0;
-            for (int t = 0; t < T; t++) {
-                int64_t x = s_part[t];
-                s_part[t] = run;
-                run += x;
+        if (warp == 0) {
+            int64_t t = s_w[lane], u = t;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t y = __shfl_up_sync(0xffffffffu, u, o);
+                if (lane >= o) u += y;
             }
-            out_totals[c] = run;
+            s_w[lane] = u - t;
+            if (lane == 31) out_totals[c] = u;
         }
         __syncthreads();
-        int64_t run = s_part[threadIdx.x];
+        int64_t run = s_w[warp] + x - s;
         for (int64_t b = b0; b < b1; b++) {
-            int64_t x = cnt[b * ncols + c];
+            const int64_t v = cnt[b * ncols + c];
             cnt[b * ncols + c] = run;
-            run += x;
+            run += v;
         }
         __syncthreads();
     }
@@ -196,19 +205,17 @@ __global__ void __launch_bounds__(1024) scan_tiles(int64_t *cnt, int64_t tiles, 
     for (int j = 0; j < 2 * m; j++) {
         double s = 0.0;
         for (int64_t b = b0; b < b1; b++) s += mom[b * 2 * m + j];
-        s_d[threadIdx.x] = s;
+        s = warp_sum(s);
+        if (lane == 0) s_d[warp] = s;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (int t = 0; t < T; t++) tot += s_d[t];
-            s_d[0] = tot;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            if (j < m) means[j] = N > 0 ? s_d[0] / (double)N : 0.0;
-            else {
-                const double mu = N > 0 ? means[j - m] : 0.0;
-                ss[j - m] = fmax(s_d[0] - (double)N * mu * mu, 0.0);
+        if (warp == 0) {
+            const double tot = warp_sum(lane < (T >> 5) ? s_d[lane] : 0.0);
+            if (lane == 0) {
+                if (j < m) means[j] = N > 0 ? tot / (double)N : 0.0;
+                else {
+                    const double mu = N > 0 ? means[j - m] : 0.0;
+                    ss[j - m] = fmax(tot - (double)N * mu * mu, 0.0);
+                }
             }
         }
         __syncthreads();

@@ -46,34 +46,53 @@ __global__ void __launch_bounds__(kThreads) k_init(int32_t *parent, int64_t n)
         parent[i] = (int32_t)i;
 }
 
-// union of every level (dimension col) of each group with the group's first
+// link a and b: the larger root under the smaller (bounded retries)
+__device__ __forceinline__ void unite(int32_t *parent, int32_t a, int32_t b, unsigned *status)
+{
+    for (int step = 0;; step++) {
+        if (step >= kMaxSteps) { atomicCAS(status, 0u, (unsigned)HDFE_ERR_SPIN_LIMIT); return; }
+        a = find_root(parent, a);
+        b = find_root(parent, b);
+        if (a == b) return;
+        const int32_t hi = a > b ? a : b, lo = a > b ? b : a;
+        const int32_t old = atomicCAS(parent + hi, hi, lo);
+        if (old == hi) return;
+        a = hi;         // hi gained a parent meanwhile: retry from there
+        b = lo;
+    }
+}
+
+// The levels (dimension col) of each group joined into one component: a
+// warp takes 32 groups, reads their cells coalesced (one per lane, 32 at a
+// time) and joins each cell's level with the previous cell's of the same
+// group where they differ -- a chain over the group, which connects what the
+// reference's star over the group's first level connects (every root is the
+// component's smallest level either way).
 __global__ void __launch_bounds__(kThreads) k_union(const int64_t *starts, int64_t G,
                                                     const uint32_t *codes, int D, int col,
                                                     int64_t nlev, int32_t *parent,
                                                     unsigned *status)
 {
-    for (int64_t g = (int64_t)blockIdx.x * kThreads + threadIdx.x; g < G;
-         g += (int64_t)gridDim.x * kThreads) {
-        const int64_t s = starts[g], e = starts[g + 1];
-        if (e <= s) continue;
-        const uint32_t c0 = codes[s * D + col];
-        if ((int64_t)c0 >= nlev) { atomicCAS(status, 0u, (unsigned)HDFE_ERR_BAD_CODE); continue; }
-        for (int64_t i = s + 1; i < e; i++) {
-            const uint32_t c = codes[i * D + col];
-            if ((int64_t)c >= nlev) { atomicCAS(status, 0u, (unsigned)HDFE_ERR_BAD_CODE); continue; }
-            if (c == c0) continue;
-            int32_t a = (int32_t)c0, b = (int32_t)c;
-            for (int step = 0;; step++) {
-                if (step >= kMaxSteps) { atomicCAS(status, 0u, (unsigned)HDFE_ERR_SPIN_LIMIT); break; }
-                a = find_root(parent, a);
-                b = find_root(parent, b);
-                if (a == b) break;
-                const int32_t hi = a > b ? a : b, lo = a > b ? b : a;
-                const int32_t old = atomicCAS(parent + hi, hi, lo);
-                if (old == hi) break;
-                a = hi;         // hi gained a parent meanwhile: retry from there
-                b = lo;
-            }
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
+    for (int64_t g0 = wid * 32; g0 < G; g0 += nw * 32) {
+        const int ng = (int)min((int64_t)32, G - g0);
+        const int64_t gend = starts[g0 + ng];
+        const int64_t st = lane < ng ? starts[g0 + lane] : gend;   // this lane's group start
+        for (int64_t base = starts[g0]; base < gend; base += 32) {
+            const bool in = lane < ng && st >= base && st < base + 32;
+            const unsigned heads = __reduce_or_sync(0xffffffffu, in ? 1u << (int)(st - base) : 0u);
+            const int64_t i = base + lane;
+            const bool valid = i < gend;
+            uint32_t c = valid ? codes[i * D + col] : 0u;
+            uint32_t prev = __shfl_up_sync(0xffffffffu, c, 1);
+            if (lane == 0 && valid && i > 0) prev = codes[(i - 1) * D + col];
+            const bool head = (heads >> lane) & 1u;
+            if (valid && (int64_t)c >= nlev) atomicCAS(status, 0u, (unsigned)HDFE_ERR_BAD_CODE);
+            if (!valid || head || c == prev || (int64_t)c >= nlev || (int64_t)prev >= nlev)
+                continue;
+            unite(parent, (int32_t)prev, (int32_t)c, status);
         }
     }
 }

@@ -264,16 +264,19 @@ __global__ void __launch_bounds__(kThreads) k_fill_lists(Args a)
          g += (int64_t)gridDim.x * kThreads) {
         const int64_t s = a.starts[g], e = a.starts[g + 1];
         for (int d = 0; d < a.D; d++) {
+            uint32_t prev = 0xffffffffu;
             for (int64_t i = s; i < e; i++) {
                 const uint32_t c = a.codes[i * a.D + d];
-                if ((int64_t)c >= a.nlev[d]) continue;
+                if (c == prev || (int64_t)c >= a.nlev[d]) continue;    // a run of one level
+                prev = c;
+                const int64_t lv = a.offs[d] + c;
+                const int32_t k = a.kind[lv];
+                if (k != kKindWarp && k != kKindBlock) continue;        // no list for wide rows
                 bool first = true;
                 for (int64_t j = s; j < i; j++)
                     if (a.codes[j * a.D + d] == c) { first = false; break; }
                 if (!first) continue;
-                const int64_t lv = a.offs[d] + c;
-                const int32_t k = a.kind[lv];
-                if (k == kKindWarp || k == kKindBlock) {
+                {
                     const int32_t at = atomicAdd(a.fillpos + lv, 1);
                     if (a.lptr[lv] + at < a.lptr[lv + 1]) a.lgrp[a.lptr[lv] + at] = (int32_t)g;
                 }
