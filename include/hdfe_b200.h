@@ -251,6 +251,33 @@ int hdfe_trace_moments(const int64_t *starts, int64_t n_groups, const uint32_t *
 int hdfe_rademacher(double *out, int64_t n_rows, int64_t ordinal0, int32_t B, uint64_t seed,
                     int64_t first_draw, void *stream);
 
+/* ------------------------------------------- connected set (pass 0's side)
+ *
+ * core/connected.py:378-493 `_find_components` for two fixed effects on
+ * coded rows, with the min_degree core (core/kernels_graph.py:188-221
+ * `_nb_peel`), union-find over the distinct pairs (:225-241
+ * `_nb_union_keys`), labels numbered by root (:244-266 `_nb_dense_labels`)
+ * and rows per component (:277-289 `_nb_pair_rows`).
+ *
+ * a, b (n_rows) uint32: the rows' codes of the two dimensions (a < n0,
+ *   b < n1), sorted by a and then b (pass 0's order); rows out of order set
+ *   status HDFE_ERR_ARG in counts[2].
+ * k0, k1: the min_degree thresholds (1, 1: no pruning).
+ * Out (DEVICE): alive (n0 + n1) uint8 (1 = in the core), labels (n0 + n1)
+ *   int32 (component numbered in the order of its smallest vertex, -1 where
+ *   pruned), rows (n0 + n1) int64 (rows per label; the first counts[1]
+ *   used), counts[4] int64 = distinct pairs, components, status, peel rounds.
+ * The peel rounds read a flag back to the host, and the call synchronises
+ * the stream before returning.  Ranking the components by size (the
+ * reference's stable sort) is the caller's.
+ */
+int64_t hdfe_pair_components_workspace_bytes(int64_t n_rows, int64_t n0, int64_t n1);
+
+int hdfe_pair_components(const uint32_t *a, const uint32_t *b, int64_t n_rows, int64_t n0,
+                         int64_t n1, int64_t k0, int64_t k1, uint8_t *alive, int32_t *labels,
+                         int64_t *rows, int64_t *counts, void *workspace,
+                         int64_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,

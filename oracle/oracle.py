@@ -526,7 +526,8 @@ def largest_connected(a, b, n0, n1, min_degree=(1, 1)):
     order = np.argsort(-rows, kind="stable")
     rank = np.empty(nc, np.int64)
     rank[order] = np.arange(nc)
-    labels = np.where(parent >= 0, rank[np.maximum(parent, 0)], -1)
+    # core/kernels_graph.py `_nb_relabel`: negative labels (pruned) stay
+    labels = np.where(parent >= 0, rank[np.maximum(parent, 0)] if nc else -1, -1)
     return labels == 0, labels, rows[order]
 
 

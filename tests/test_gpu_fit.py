@@ -83,3 +83,48 @@ def test_mixed_precision_fit(device, name, rows):
     gamma = res.gamma.cpu().numpy()
     assert res.info["converged"]
     assert np.max(np.abs(gamma - gamma_ref)) / np.max(np.abs(gamma_ref)) < 1e-8
+
+
+@pytest.mark.parametrize("panel", ["sparse", "middle", "dense"])
+@pytest.mark.parametrize("k", [1, 2])
+def test_pair_components_match_reference(device, panel, k):
+    """The connected set on the device (`_find_components`, min_degree core,
+    labels ranked by rows) against the reference's kernels' golden output."""
+    import torch
+    from conftest import load_golden
+    from hdfe_stream_b200.connected import pair_components
+    g = load_golden("connected")
+    n0, n1 = (int(x) for x in g[f"{panel}_n"])
+    a = torch.as_tensor(g[f"{panel}_a"].astype(np.int32), device=device)
+    b = torch.as_tensor(g[f"{panel}_b"].astype(np.int32), device=device)
+    labels, rows, info = pair_components(a, b, n0, n1, (k, k))
+    assert np.array_equal(labels.cpu().numpy(), g[f"{panel}_k{k}_labels"])
+    assert np.array_equal(rows, g[f"{panel}_k{k}_rows"])
+    assert info["pruning_rounds"] == int(g[f"{panel}_k{k}_rounds"][0])
+
+
+def test_pair_components_5m_panel_matches_oracle(device):
+    """The 5M-worker panel's restriction (min_degree 2, largest set) on the
+    device agrees with the oracle's on a 200k-worker panel of the same shape."""
+    import torch
+    from hdfe_stream_b200.connected import pair_components
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    rows = pass0_layout(simulate_panel(200_000, 20_000, 15, spell=(5, 12), p_move=0.08, seed=3))
+    a, b = rows.gcode.astype(np.uint32), rows.codes[:, 0].astype(np.uint32)
+    n0, n1 = int(rows.n_groups), int(rows.n_levels[0])
+    _, ref_labels, ref_rows = orc.largest_connected(a, b, n0, n1, (2, 2))
+    labels, got_rows, _ = pair_components(torch.as_tensor(a.astype(np.int32), device=device),
+                                          torch.as_tensor(b.astype(np.int32), device=device),
+                                          n0, n1, (2, 2))
+    assert np.array_equal(labels.cpu().numpy(), ref_labels)
+    assert np.array_equal(got_rows, ref_rows)
+
+
+def test_pair_components_rejects_unsorted_rows(device):
+    import torch
+    from hdfe_stream_b200 import _lib
+    from hdfe_stream_b200.connected import pair_components
+    a = torch.tensor([0, 1, 0], dtype=torch.int32, device=device)
+    b = torch.tensor([0, 0, 1], dtype=torch.int32, device=device)
+    with pytest.raises(_lib.HDFEError):
+        pair_components(a, b, 2, 2)

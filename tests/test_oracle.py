@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as orc
-from conftest import golden_rows
+from conftest import golden_rows, load_golden
 
 
 def rel(a, b):
@@ -160,3 +160,17 @@ def test_hutchinson_trace_matches_reference(golden):
     des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g["tol"]))
     tr = des.hutchinson_trace(g["trace_sigma2"], 16, 8, 4)
     assert np.max(np.abs(tr - g["trace"])) < 1e-10 * np.max(np.abs(g["trace"]))
+
+
+@pytest.mark.parametrize("panel", ["sparse", "middle", "dense"])
+@pytest.mark.parametrize("k", [1, 2])
+def test_largest_connected_matches_reference(panel, k):
+    """`_find_components` for connected="largest": distinct pairs, the
+    min_degree core, component labels ranked by rows, rows per component --
+    against the reference's own kernels (tests/golden/connected.npz)."""
+    g = load_golden("connected")
+    n0, n1 = (int(x) for x in g[f"{panel}_n"])
+    largest, labels, rows = orc.largest_connected(g[f"{panel}_a"], g[f"{panel}_b"], n0, n1,
+                                                  (k, k))
+    assert np.array_equal(labels, g[f"{panel}_k{k}_labels"])
+    assert np.array_equal(rows, g[f"{panel}_k{k}_rows"])
