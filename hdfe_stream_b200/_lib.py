@@ -66,6 +66,8 @@ SIGNATURES = {
     "hdfe_trace_moments": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _vp, _vp,
                                       _vp, _i32, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_rademacher": (_c.c_int, [_vp, _i64, _i64, _i32, _c.c_uint64, _i64, _vp]),
+    "hdfe_stream_matvec": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _vp, _vp,
+                                      _vp]),
     "hdfe_pair_components_workspace_bytes": (_i64, [_i64, _i64, _i64]),
     "hdfe_pair_components": (_c.c_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp,
                                         _vp, _vp, _i64, _vp]),

@@ -48,7 +48,8 @@ struct Args {
     const double *streamed;     // (G, B): spread over the rows, or null
     const double *R;            // (N, B) explicit rows (reduce), or null
     const double *U, *C;        // (L, B), (c, B)
-    const double *omega;        // (N) or null: the collect sink's row weights
+    const double *omega;        // (N) or null: the collect sink's row weights (ones)
+    bool collect;               // project_coef: run the collect sink
     double *rows;               // (N, B) or null
     double *groups;             // (G, B) or null
     double *acc, *acc_x;        // (L, B), (c, B): added into
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(kThreads) k_project_coef(Args a)
         }
         const double mean = sw > 0.0 ? tot / sw : 0.0;
         if (a.groups && ln.on) a.groups[g * a.B + ln.j] = mean;
-        if (!a.rows && !a.omega) continue;
+        if (!a.rows && !a.collect) continue;
         // pass 2: the rows, and the collect sink
         key.have = false;
         Runs run{};
@@ -257,9 +258,9 @@ __global__ void __launch_bounds__(kThreads) k_project_coef(Args a)
             row_codes(a, i, c);
             const double o = h_of(i, c, hU, key) + mean;
             if (a.rows && ln.on) a.rows[i * a.B + ln.j] = o;
-            if (a.omega) {
+            if (a.collect) {
                 const double wi = a.w ? __ldg(a.w + i) : 1.0;
-                const double v = wi * __ldg(a.omega + i) * o;
+                const double v = wi * (a.omega ? __ldg(a.omega + i) : 1.0) * o;
                 run_add(a, run, c, v, ln.j, ln.on);
                 gs += v;
 #pragma unroll
@@ -269,12 +270,12 @@ __global__ void __launch_bounds__(kThreads) k_project_coef(Args a)
                 }
             }
         }
-        if (a.omega) {
+        if (a.collect) {
             if (run.have && ln.on) run_flush(a, run, ln.j);
             if (a.gsum && ln.on) a.gsum[g * a.B + ln.j] = gs;
         }
     }
-    if (a.omega && a.acc_x && a.c > 0) flush_cov(a, ax, s_ax, ln.j, ln.on);
+    if (a.collect && a.acc_x && a.c > 0) flush_cov(a, ax, s_ax, ln.j, ln.on);
 }
 
 // ---------------------------------------------------------- trace moments
@@ -462,6 +463,7 @@ extern "C" int hdfe_rows_project_coef(const int64_t *starts, int64_t n_groups,
     a.rows = rows;
     a.groups = groups;
     a.omega = omega;
+    a.collect = omega != nullptr;
     a.acc = acc;
     a.acc_x = acc_x;
     a.gsum = group_sums;
@@ -535,6 +537,35 @@ extern "C" int hdfe_rademacher(double *out, int64_t n_rows, int64_t ordinal0, in
     if (blocks > 148 * 32) blocks = 148 * 32;
     coef::k_rademacher<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(out, n_rows, ordinal0,
                                                                           B, seed, first_draw);
+    HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(1);
+    return HDFE_OK;
+}
+
+// (D_o' M_0 D_o) P from the identifying cells, without S: per group the
+// n-weighted mean of h_i = sum_d P[level_d(i)] is taken off, and
+// n_i (h_i - mean) is added to each of cell i's levels -- the projection pass
+// with U = P, no streamed block, weights n and the collect sink's unit weights
+// (core/kernels_base.py:478-507 `_nb_stream_matvec`).
+extern "C" int hdfe_stream_matvec(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                                  int32_t D, const int64_t *n_levels, const double *n,
+                                  const double *P, int32_t k, double *out, void *status,
+                                  void *stream)
+{
+    coef::Args a;
+    int st = coef::fill(a, starts, n_groups, codes, D, n_levels, n, nullptr, 0, k,
+                        (unsigned *)status);
+    if (st != HDFE_OK) return st;
+    if (!n || !P || !out) return hdfe_set_arg_error("hdfe_stream_matvec: bad argument");
+    a.U = P;
+    a.collect = true;
+    a.acc = out;
+    cudaStream_t s = (cudaStream_t)stream;
+    HDFE_CUDA_TRY(cudaMemsetAsync(out, 0, a.L * k * 8, s));
+    const unsigned grid = coef::grid_for(n_groups, a.Bp);
+    if (a.Bp == 8) coef::k_project_coef<8><<<grid, coef::kThreads, 0, s>>>(a);
+    else if (a.Bp == 16) coef::k_project_coef<16><<<grid, coef::kThreads, 0, s>>>(a);
+    else coef::k_project_coef<32><<<grid, coef::kThreads, 0, s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
     return HDFE_OK;

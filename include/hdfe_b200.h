@@ -251,6 +251,14 @@ int hdfe_trace_moments(const int64_t *starts, int64_t n_groups, const uint32_t *
 int hdfe_rademacher(double *out, int64_t n_rows, int64_t ordinal0, int32_t B, uint64_t seed,
                     int64_t first_draw, void *stream);
 
+/* core/kernels_base.py:478-507 `_nb_stream_matvec`: out (L, k) =
+ * (D_o' M_0 D_o) P for P (L, k), k <= 32, straight from the identifying cells
+ * (starts (G'+1), codes (M, D), n (M)) without forming S -- the `stream_cg`
+ * solver's product.  out is overwritten; sums in atomic order. */
+int hdfe_stream_matvec(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                       const int64_t *n_levels, const double *n, const double *P, int32_t k,
+                       double *out, void *status, void *stream);
+
 /* ------------------------------------------- connected set (pass 0's side)
  *
  * core/connected.py:378-493 `_find_components` for two fixed effects on

@@ -195,3 +195,32 @@ def test_mixed_precision_maxiter(device):
                             precision="mixed")
     X, it, ok, rel = solve(g["pcg_b"])
     assert it == 4 and not ok and rel > 1e-12
+
+
+@pytest.mark.parametrize("k", [1, 3, 32])
+def test_stream_matvec_matches_explicit_s(device, k):
+    """`_nb_stream_matvec`: (D_o' M_0 D_o) P from the cells equals S P with
+    the explicit S, on the golden panels and a two-dimension panel."""
+    import torch
+    from hdfe_stream_b200 import _lib, fit
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    panels = [golden_rows(load_golden(n)) for n in GOLDEN_PANELS]
+    panels.append(pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(3, 10), p_move=0.1,
+                                              weights=True, seed=13)))
+    for rows in panels:
+        c = orc.pass1(rows)
+        S = orc.build_explicit(c)
+        P = np.random.default_rng(k).standard_normal((c.L, k))
+        ref = orc.csr_matmat(S, P)
+        cells = fit.pass1(fit.DeviceRows.from_rows(rows))
+        out = torch.empty((cells.L, k), dtype=torch.float64, device=device)
+        nlev = np.asarray(cells.n_levels, dtype=np.int64)
+        st = torch.zeros(1, dtype=torch.int32, device=device)
+        _lib.check(_lib.lib().hdfe_stream_matvec(
+            cells.starts.data_ptr(), int(cells.starts.shape[0]) - 1, cells.codes.data_ptr(),
+            len(nlev), nlev.ctypes.data, cells.n.data_ptr(),
+            torch.as_tensor(P, device=device).data_ptr(), k, out.data_ptr(), st.data_ptr(),
+            _lib.stream_handle()))
+        got = out.cpu().numpy()
+        assert int(st.item()) == 0
+        assert np.max(np.abs(got - ref)) < 1e-12 * np.max(np.abs(ref))
