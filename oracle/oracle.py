@@ -532,6 +532,39 @@ def largest_connected(a, b, n0, n1, min_degree=(1, 1)):
 
 
 
+# ------------------------------------------------ steps 3-4 of a fit
+
+def residual_moments(starts, codes, offs, w, V, Gamma):
+    """core/kernels_base.py:114-146 `_nb_residualize_rows` then
+    core/inference.py:109-135 `_assemble` (row assembly): V' W V of the
+    variables less their fixed-effect projections and weighted group means."""
+    V = np.array(V, dtype=np.float64)
+    codes = np.asarray(codes, dtype=np.int64)
+    for d in range(codes.shape[1]):
+        V -= Gamma[offs[d] + codes[:, d]]
+    sizes = np.diff(starts)
+    Wg = np.add.reduceat(w, starts[:-1])
+    q = np.add.reduceat(w[:, None] * V, starts[:-1], axis=0) / Wg[:, None]
+    V -= np.repeat(q, sizes, axis=0)
+    Vs = V * np.sqrt(w)[:, None]
+    return Vs.T @ Vs
+
+
+def row_effects(starts, codes, offs, w, V, Gamma, beta):
+    """core/inference.py:454-456 and core/kernels_base.py:544-615 `_nb_pass2`
+    for y = V[:, 0], X = V[:, 1:]: (residual per row, the streamed effect per
+    group, the first non-streamed effect per row, gam_y)."""
+    codes = np.asarray(codes, dtype=np.int64)
+    gam_y = Gamma[:, 0] - Gamma[:, 1:] @ beta
+    u = V[:, 0] - V[:, 1:] @ beta
+    for d in range(codes.shape[1]):
+        u = u - gam_y[offs[d] + codes[:, d]]
+    Wg = np.add.reduceat(w, starts[:-1])
+    alpha = np.add.reduceat(w * u, starts[:-1]) / Wg
+    e = u - np.repeat(alpha, np.diff(starts))
+    return e, alpha, gam_y[offs[0] + codes[:, 0]], gam_y
+
+
 # ------------------------------------------------- inverse operator, JLA
 
 class Design:
@@ -689,6 +722,34 @@ class Design:
         R = float(self.rows.n_rows)
         scale = weight / (weight * (R - 1.0) / R) if R > 1 else 1.0
         return np.array([scale * var_psi, scale * var_alpha, scale * cov])
+
+    def leave_out_components(self, Gamma, n_draws, block, seed):
+        """leaveout.py:634-805 `leave_out_components` (point estimates;
+        stayers "own", weighted centring): the plug-in var(psi), var(alpha),
+        cov(psi, alpha) (:807-833), sigma2 from the leverages and residuals
+        (:949-1016), the Hutchinson bias (seed + 1_000_003) and their
+        difference.  psi = the first non-streamed dimension."""
+        rows, cells, starts = self.rows, self.cells, self.starts
+        w = self.w
+        A = residual_moments(starts, self.codes, cells.offs, w, rows.V, Gamma)
+        beta = np.linalg.solve(A[1:, 1:], A[1:, 0])
+        e, alpha_g, psi_row, _ = row_effects(starts, self.codes, cells.offs, w, rows.V, Gamma,
+                                             beta)
+        alpha_row = np.repeat(alpha_g, np.diff(starts))
+        T = w.sum()
+        R = float(rows.n_rows)
+        scale = T / (T * (R - 1.0) / R) if R > 1 else 1.0
+        ma, mb = (w @ psi_row) / T, (w @ alpha_row) / T
+        plug_in = np.array([scale * ((w @ (psi_row * psi_row)) / T - ma * ma),
+                            scale * ((w @ (alpha_row * alpha_row)) / T - mb * mb),
+                            scale * ((w @ (psi_row * alpha_row)) / T - ma * mb)])
+        lev, comp, factor = self.jla_leverages(n_draws, block, seed)
+        y = rows.V[:, 0]
+        ybar = float(w @ y / T)
+        sigma2 = w * (y - ybar) * e / comp * factor
+        bias = self.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003)
+        return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "beta": beta,
+                "sigma2": sigma2, "max_leverage": float(lev.max())}
 
     def jla_leverages(self, n_draws, block, seed):
         """leaveout.py:130-198 `jla_leverages` and :210-282

@@ -174,3 +174,23 @@ def test_largest_connected_matches_reference(panel, k):
                                                   (k, k))
     assert np.array_equal(labels, g[f"{panel}_k{k}_labels"])
     assert np.array_equal(rows, g[f"{panel}_k{k}_rows"])
+
+
+def test_steps_3_4_match_reference(golden):
+    """V' W V (`_nb_residualize_rows` + `_assemble`), beta, and the row pass
+    (`_nb_pass2`): residuals, the streamed effect and the first non-streamed
+    effect per row, against the reference's kernels on its own Gamma."""
+    name, g = golden
+    a = load_golden("assemble")
+    rows = golden_rows(g)
+    starts = orc.row_starts(rows.gcode)
+    offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1])).astype(np.int64)
+    w = rows.w if rows.w is not None else np.ones(rows.n_rows)
+    A = orc.residual_moments(starts, rows.codes, offs, w, rows.V, g["gamma"])
+    assert rel(A, a[f"{name}_A"]) < 1e-12
+    beta = np.linalg.solve(A[1:, 1:], A[1:, 0])
+    assert rel(beta, a[f"{name}_beta"]) < 1e-10
+    e, alpha, psi, gam_y = orc.row_effects(starts, rows.codes, offs, w, rows.V, g["gamma"], beta)
+    assert rel(e, a[f"{name}_resid"]) < 1e-10
+    assert rel(alpha, a[f"{name}_alpha"]) < 1e-10
+    assert rel(psi, a[f"{name}_psi"]) < 1e-10
