@@ -288,52 +288,57 @@ def run_ours(args, rank, world, local_rank):
 
 
 def run_jla(args, rank, world, dist):
-    """KSS on the 1M-worker panel with the model's covariates: JLA leverages
-    for p = 256 probes and the Hutchinson bias term for 256 draws (two
-    applications of the inverse per draw), blocks of 32.  RHS solves per
-    second = p (1 + 2) / wall time of both."""
+    """KSS `leave_out_components` on the 1M-worker panel with the model's
+    covariates, from the device fit's Gamma: beta and the residuals (steps
+    3-4), JLA leverages for p = 256 probes, sigma2, and the Hutchinson bias
+    term for 256 draws (two applications of the inverse per draw), blocks of
+    32.  RHS solves per second = p (1 + 2) / device time of the whole call."""
     import torch
     from hdfe_stream_b200 import fit, leaveout
     from hdfe_stream_b200.simulate import prepare
 
     rows = prepare("kss_1m", seed=100 + rank)
     drows = fit.DeviceRows.from_rows(rows)
-    cells = fit.pass1(drows)
-    S = fit.build_s(cells)
+    res = fit.fit(drows, tol=args.tol)
+    S = res.S
     X = drows.V[1:].T.contiguous()
-    op = leaveout.InverseOperator(drows, cells, S, X, tol=args.tol)
+    op = leaveout.InverseOperator(drows, res.cells, S, X, tol=args.tol)
     p = 256
-    # per-row variances for the bias term: seeded, positive (the cost does not
-    # depend on the values)
-    sigma2 = torch.as_tensor(np.abs(np.random.default_rng(9 + rank).standard_normal(rows.n_rows))
-                             + 0.1, device="cuda")
-    op.jla_leverages(p, block=32, seed=1)          # warm-up (the border, the null space)
-    op.hutchinson_trace(sigma2, n_draws=32, block=32, seed=2)
+    op.leave_out_components(res.gamma, 32, block=32, seed=1)   # warm-up (border, null space)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    timer = fit.PhaseTimer()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ev[0].record()
-    lev, comp, factor = op.jla_leverages(p, block=32, seed=1)
+    kss = op.leave_out_components(res.gamma, p, block=32, seed=1, timer=timer)
     ev[1].record()
-    trace = op.hutchinson_trace(sigma2, n_draws=p, block=32, seed=2)
-    ev[2].record()
     torch.cuda.synchronize()
-    ms_jla, ms_tr = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
-    ms = ms_jla + ms_tr
+    phases = {k: v[0] for k, v in timer.totals().items()}
+    ms = ev[0].elapsed_time(ev[1])
+    ms_jla, ms_tr = phases["leverages"], phases["trace"]
     if dist:
         t = torch.tensor([ms, ms_jla, ms_tr], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_jla, ms_tr = (float(x) for x in t.tolist())
+    sigma2 = kss["sigma2"]
+    bad = int((~torch.isfinite(sigma2)).sum().item())
+
+    def finite(x):
+        return [float(v) if np.isfinite(v) else None for v in x]
     out = {"workload": "kss_1m: 1M workers, 100k firms, 10 years, largest connected set; "
                        "log_earn ~ age_squared + age_cubed | worker_id + firm_id",
            "rows": rows.n_rows, "levels": int(sum(rows.n_levels)), "S_nnz": S.nnz, "draws": p,
            "block": 32, "ms": round(ms, 3), "ms_leverages": round(ms_jla, 3),
-           "ms_trace": round(ms_tr, 3),
+           "ms_trace": round(ms_tr, 3), "ms_steps34": round(phases["steps34"], 3),
+           "ms_sigma2": round(phases["sigma2"], 3),
            "value": round(world * 3 * p / (ms / 1e3), 2), "unit": "RHS solves/s",
            "note": "p (1 + 2 Hutchinson) RHS solves: the leverages' one application of "
-                   "the inverse per probe and the bias term's two per draw",
-           "max_leverage": float(lev.max()), "bias_terms": [float(x) for x in trace],
+                   "the inverse per probe and the bias term's two per draw; the timed call "
+                   "is the whole leave_out_components (steps 3-4, leverages, sigma2, trace)",
+           "max_leverage": kss["max_leverage"], "plug_in": finite(kss["plug_in"]),
+           "bias_terms": finite(kss["bias"]), "leave_out": finite(kss["leave_out"]),
+           "rows_without_sigma2": bad,
            "iterations_last_block": op.jla_info["iterations"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, str(REPO / "oracle"))
@@ -346,7 +351,7 @@ def run_jla(args, rank, world, dist):
         t0 = time.perf_counter()
         des.jla_leverages(32, 32, 1)
         t1 = time.perf_counter()
-        des.hutchinson_trace(sigma2.cpu().numpy(), 32, 32, 2)
+        des.hutchinson_trace(np.nan_to_num(sigma2.cpu().numpy()), 32, 32, 2)
         t2 = time.perf_counter()
         out["cpu_baseline"] = {"value": round(3 * 32 / (t2 - t0), 3), "unit": "RHS solves/s",
                                "cores": orc.num_threads(), "kind": "port",

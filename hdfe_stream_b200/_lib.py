@@ -71,6 +71,12 @@ SIGNATURES = {
     "hdfe_pair_components_workspace_bytes": (_i64, [_i64, _i64, _i64]),
     "hdfe_pair_components": (_c.c_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp,
                                         _vp, _vp, _i64, _vp]),
+    "hdfe_assemble_workspace_bytes": (_i64, [_i32]),
+    "hdfe_resid_moments": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _i64, _vp,
+                                      _vp, _vp, _i64, _vp, _vp]),
+    "hdfe_row_effects": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _i32, _i64, _vp,
+                                    _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
+    "hdfe_kss_sigma2": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _f64, _i64, _vp, _vp]),
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),

@@ -270,6 +270,92 @@ class InverseOperator:
         self.trace_info = {"blocks": blocks, "n_obs": float(weight)}
         return np.array([scale * var_psi, scale * var_alpha, scale * cov])
 
+    # ---- steps 3-4 and the KSS components (core/inference.py, leaveout.py:634-1016)
+
+    def _assemble_ws(self, m):
+        torch = _torch()
+        return torch.empty(int(_lib.lib().hdfe_assemble_workspace_bytes(m)), dtype=torch.uint8,
+                           device=self.dev)
+
+    def residual_moments(self, gamma):
+        """V' W V of the rows' variables less Gamma's projections and their
+        weighted group means (`_nb_residualize_rows` + `_assemble`), (m, m)
+        on the device."""
+        torch = _torch()
+        m = self.rows.m
+        gamma = gamma.to(self.dev, torch.float64).contiguous()
+        out = torch.empty((m, m), dtype=torch.float64, device=self.dev)
+        ws = self._assemble_ws(m)
+        _lib.check(_lib.lib().hdfe_resid_moments(
+            self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
+            self.nlev.ctypes.data, self._ptr(self.w), self.rows.V.data_ptr(), m, self.N,
+            gamma.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(),
+            self._status().data_ptr(), _lib.stream_handle()))
+        return out
+
+    def row_effects(self, gamma, beta, psi_column=0):
+        """`_nb_pass2` for y = V[0], X = V[1:]: (residual (N), streamed effect
+        per group (G), gam_y (L), sums (7): w, w y, w a, w b, w a^2, w b^2,
+        w a b with a the psi dimension's effect and b the streamed one)."""
+        torch = _torch()
+        m = self.rows.m
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        gamma = gamma.to(**f64)
+        beta = torch.as_tensor(np.asarray(beta, dtype=np.float64)).to(**f64).reshape(-1)
+        gam_y = (gamma[:, 0] - gamma[:, 1:] @ beta).contiguous() if m > 1 else \
+            gamma[:, 0].contiguous()
+        resid = torch.empty(self.N, **f64)
+        alpha = torch.empty(max(self.G, 1), **f64)
+        sums = torch.empty(7, **f64)
+        ws = self._assemble_ws(m)
+        _lib.check(_lib.lib().hdfe_row_effects(
+            self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
+            self.nlev.ctypes.data, int(psi_column), self._ptr(self.w), self.rows.V.data_ptr(), m,
+            self.N, beta.contiguous().data_ptr() if m > 1 else None, gam_y.data_ptr(),
+            resid.data_ptr(), alpha.data_ptr(), sums.data_ptr(), ws.data_ptr(), ws.numel(),
+            self._status().data_ptr(), _lib.stream_handle()))
+        return resid, alpha[:self.G], gam_y, sums
+
+    def leave_out_components(self, gamma, n_draws=250, block=MAX_BLOCK, seed=0, psi_column=0,
+                             timer=None):
+        """leaveout.py:634-805 `leave_out_components` (point estimates;
+        stayers "own", weighted centring): beta from the residual moments,
+        the plug-in var(psi), var(alpha), cov(psi, alpha) (:807-833) with the
+        n - 1 divisor, sigma2 from the JLA leverages and the residuals
+        (:949-1016), the Hutchinson bias with seed + 1_000_003, and
+        leave_out = plug_in - bias.  gamma (L, m) the fit's normalised
+        effects for V's variables (y first).  timer: a `fit.PhaseTimer` for
+        the phases "steps34", "leverages", "sigma2" and "trace"."""
+        import contextlib
+        torch = _torch()
+        phase = timer or (lambda name: contextlib.nullcontext())
+        with phase("steps34"):
+            A = self.residual_moments(gamma).cpu().numpy()
+            m = A.shape[0]
+            beta = np.linalg.solve(A[1:, 1:], A[1:, 0]) if m > 1 else np.zeros(0)
+            resid, _, _, sums = self.row_effects(gamma, beta, psi_column)
+            s = sums.cpu().numpy()
+        if int(self._status().item()) != _lib.HDFE_OK:
+            raise _lib.HDFEError(int(self._status().item()), "a level code is out of range")
+        T = s[0]
+        R = float(self.N)
+        scale = T / (T * (R - 1.0) / R) if R > 1 else 1.0
+        ma, mb = s[2] / T, s[3] / T
+        plug_in = np.array([scale * (s[4] / T - ma * ma), scale * (s[5] / T - mb * mb),
+                            scale * (s[6] / T - ma * mb)])
+        with phase("leverages"):
+            lev, comp, factor = self.jla_leverages(n_draws, block, seed)
+        with phase("sigma2"):
+            sigma2 = torch.empty(self.N, dtype=torch.float64, device=self.dev)
+            _lib.check(_lib.lib().hdfe_kss_sigma2(
+                self.rows.V.data_ptr(), self._ptr(self.w), resid.data_ptr(), comp.data_ptr(),
+                factor.data_ptr(), float(s[1] / T), self.N, sigma2.data_ptr(),
+                _lib.stream_handle()))
+        with phase("trace"):
+            bias = self.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003, psi_column)
+        return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "beta": beta,
+                "sigma2": sigma2, "max_leverage": float(lev.max().item())}
+
     def jla_leverages(self, n_draws=250, block=MAX_BLOCK, seed=0):
         """leaveout.py:130-198 `jla_leverages`: (leverage, complement, factor)
         per row (device tensors), in the square-root weight metric when the

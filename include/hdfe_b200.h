@@ -286,6 +286,46 @@ int hdfe_pair_components(const uint32_t *a, const uint32_t *b, int64_t n_rows, i
                          int64_t *rows, int64_t *counts, void *workspace,
                          int64_t workspace_bytes, void *stream);
 
+/* ------------------------------------------------- steps 3-4, KSS components
+ *
+ * The row passes after step 2 that the leave-out components read, on pass
+ * 0's rows (row groups starts (G+1), codes (N, D), V (m, N) one row per
+ * variable, y first, w (N) or NULL) and the normalised Gamma (L, m):
+ *
+ * hdfe_resid_moments: out (m, m) = V' W V of the variables less their
+ *   fixed-effect projections Gamma and their weighted group means --
+ *   core/kernels_base.py:114-146 `_nb_residualize_rows` with the row
+ *   assembly of core/inference.py:109-135 `_assemble`.  Per-CTA partials,
+ *   summed in a fixed order: deterministic.
+ * hdfe_row_effects: for beta (m-1) and gam_y (L) = Gamma_y - Gamma_x beta
+ *   (core/inference.py:454-456), the residual per row resid (N) and the
+ *   streamed effect per group alpha (G) (core/kernels_base.py:544-615
+ *   `_nb_pass2`; either may be NULL), and sums[7] = (w, w y, w a, w b, w a^2,
+ *   w b^2, w a b) over rows, a = the effect of dimension psi_column and b =
+ *   the streamed effect: the plug-in moments' sums (leaveout.py:807-833).
+ * hdfe_kss_sigma2: out_i = w_i (y_i - ybar) resid_i / complement_i * factor_i,
+ *   the KSS per-row variance of leaveout.py:949-1016 `_leave_one_out_sigma2`
+ *   (stayers "own", weighted centring); w may be NULL.
+ * status: a device uint32 that an out-of-range code sets to
+ *   HDFE_ERR_BAD_CODE, or NULL.  m <= 8.
+ */
+int64_t hdfe_assemble_workspace_bytes(int32_t m);
+
+int hdfe_resid_moments(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                       const int64_t *n_levels, const double *w, const double *V, int32_t m,
+                       int64_t n_rows, const double *Gamma, double *out, void *workspace,
+                       int64_t workspace_bytes, void *status, void *stream);
+
+int hdfe_row_effects(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                     const int64_t *n_levels, int32_t psi_column, const double *w,
+                     const double *V, int32_t m, int64_t n_rows, const double *beta,
+                     const double *gam_y, double *resid, double *alpha, double *sums,
+                     void *workspace, int64_t workspace_bytes, void *status, void *stream);
+
+int hdfe_kss_sigma2(const double *y, const double *w, const double *resid,
+                    const double *complement, const double *factor, double ybar,
+                    int64_t n_rows, double *out, void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,

@@ -169,3 +169,90 @@ def test_hutchinson_blocking_and_covariates(device):
     b = op.hutchinson_trace(sigma2, n_draws=20, block=7, seed=3)
     assert rel(a, ref) < 1e-8
     assert rel(a, b) < 1e-9
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_steps_3_4_match_reference(device, name):
+    """V' W V of the residualised variables, beta and the pass-2 residuals
+    and effects on the reference's own Gamma, against the reference's
+    `_nb_residualize_rows` / `_assemble` / `_nb_pass2` outputs."""
+    import torch
+    g = load_golden(name)
+    a = load_golden("assemble")
+    rows = golden_rows(g)
+    op = operator(rows, float(g["tol"]))
+    gamma = torch.as_tensor(g["gamma"], device=device)
+    A = op.residual_moments(gamma).cpu().numpy()
+    assert rel(A, a[f"{name}_A"]) < 1e-11
+    assert np.array_equal(A, op.residual_moments(gamma).cpu().numpy())
+    beta = np.linalg.solve(A[1:, 1:], A[1:, 0])
+    assert rel(beta, a[f"{name}_beta"]) < 1e-9
+    e, alpha, gam_y, sums = op.row_effects(gamma, beta)
+    assert rel(e.cpu().numpy(), a[f"{name}_resid"]) < 1e-9
+    assert rel(alpha.cpu().numpy(), a[f"{name}_alpha"]) < 1e-9
+    psi = gam_y.cpu().numpy()[rows.codes[:, 0].astype(np.int64)]
+    assert rel(psi, a[f"{name}_psi"]) < 1e-9
+    w = rows.w if rows.w is not None else np.ones(rows.n_rows)
+    s = sums.cpu().numpy()
+    assert rel(s[:2], [w.sum(), w @ rows.V[:, 0]]) < 1e-12
+    assert rel(s[4], w @ (psi * psi)) < 1e-10
+
+
+def without_singletons(rows):
+    """The rows of groups seen at least twice: a single-row group has
+    leverage 1 and no leave-one-out residual (the reference asks for the
+    leave-one-out connected set before the KSS components)."""
+    from hdfe_stream_b200.simulate import Rows
+    sizes = np.bincount(rows.gcode)
+    keep = sizes[rows.gcode] >= 2
+    number = np.cumsum(sizes >= 2) - 1
+    return Rows(gcode=number[rows.gcode[keep]].astype(rows.gcode.dtype), codes=rows.codes[keep],
+                V=rows.V[keep], w=None if rows.w is None else rows.w[keep],
+                n_levels=rows.n_levels, n_groups=int((sizes >= 2).sum()), names=rows.names)
+
+
+@pytest.mark.parametrize("name", ["akm_small", "akm_weighted"])
+def test_leave_out_components_match_oracle(device, name):
+    """leaveout.py `leave_out_components` (plug-in, sigma2, bias, leave-out)
+    with the model's covariates, against the oracle on the same Gamma.  (The
+    many-component panel has rows of leverage 1 -- its small components --
+    whose sigma2 is not defined.)"""
+    import torch
+    rows = without_singletons(golden_rows(load_golden(name)))
+    c = orc.pass1(rows)
+    S = orc.build_explicit(c)
+    gamma, _ = orc.solve(c, S, tol=1e-12)
+    des = orc.Design(rows, c, S, X=rows.V[:, 1:], tol=1e-12)
+    ref = des.leave_out_components(gamma, 16, 8, 5)
+    assert np.all(np.isfinite(ref["sigma2"]))
+    op = operator(rows, 1e-12, covariates=True)
+    got = op.leave_out_components(torch.as_tensor(gamma, device=device), 16, 8, 5)
+    assert rel(got["beta"], ref["beta"]) < 1e-10
+    assert rel(got["plug_in"], ref["plug_in"]) < 1e-10
+    assert rel(got["sigma2"].cpu().numpy(), ref["sigma2"]) < 1e-8
+    assert rel(got["bias"], ref["bias"]) < 1e-8
+    assert rel(got["leave_out"], ref["leave_out"]) < 1e-8
+    assert abs(got["max_leverage"] - ref["max_leverage"]) < 1e-8
+
+
+def test_steps_3_4_on_a_device_fit(device):
+    """On a 200k-row panel fitted on the device: the residuals have zero
+    weighted mean in every group and their weighted sum of squares is
+    A_yy - A_yx beta (the normal equations), to the solver's tolerance."""
+    import torch
+    from hdfe_stream_b200 import fit, simulate
+    panel = simulate.simulate_panel(25_000, 1_500, 10, spell=(5, 10), weights=True, seed=7)
+    rows = simulate.pass0_layout(panel, simulate.restrict_connected(panel, (1, 1)))
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    from hdfe_stream_b200 import leaveout
+    op = leaveout.InverseOperator(drows, res.cells, res.S, tol=1e-12)
+    A = op.residual_moments(res.gamma).cpu().numpy()
+    beta = np.linalg.solve(A[1:, 1:], A[1:, 0])
+    e, alpha, _, _ = op.row_effects(res.gamma, beta)
+    e = e.cpu().numpy()
+    w = rows.w
+    starts = op.starts.cpu().numpy()
+    gsum = np.add.reduceat(w * e, starts[:-1])
+    assert np.max(np.abs(gsum)) < 1e-8 * np.sqrt(w @ (e * e))
+    assert rel(w @ (e * e), A[0, 0] - A[0, 1:] @ beta) < 1e-7
