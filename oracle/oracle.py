@@ -531,6 +531,67 @@ def largest_connected(a, b, n0, n1, min_degree=(1, 1)):
     return labels == 0, labels, rows[order]
 
 
+def leave_one_out(a, b, n0, n1, min_degree=(1, 1)):
+    """core/connected.py:503-557 `_leave_one_out` (after `_nb_peel` when
+    min_degree is given, as `_find_components` does at :429-447): the largest
+    component by rows, workers (first dimension) seen once removed, then
+    every worker that is an articulation point removed, the largest piece
+    kept, until none is left.  Returns (alive (n0 + n1) bool, rows alive,
+    counts dict)."""
+    lib_ = lib()
+    keys, counts = distinct_pairs(a, b, n1)
+    n1u = ctypes.c_uint64(max(n1, 1))
+    nv = n0 + n1
+    alive = np.ones(nv, np.uint8)
+    if tuple(min_degree) != (1, 1):
+        a0, a1 = np.ones(n0, np.uint8), np.ones(n1, np.uint8)
+        peel(keys, n1, min_degree[0], min_degree[1], a0, a1)
+        alive[:n0], alive[n0:] = a0, a1
+    indptr = np.zeros(nv + 1, np.int64)
+    lib_.orc_pairs_csr(_p(keys), _i(len(keys)), n1u, _i(n0), _p(alive), _i(nv), _p(indptr), None)
+    indices = np.empty(max(int(indptr[-1]), 1), np.int64)
+    lib_.orc_pairs_csr(_p(keys), _i(len(keys)), n1u, _i(n0), _p(alive), _i(nv), _p(indptr),
+                       _p(indices))
+    label = np.empty(nv, np.int64)
+
+    def keep_largest():
+        nc = int(lib_.orc_bfs_components(_p(indptr), _p(indices), _i(nv), _p(alive), _p(label)))
+        if nc == 0:
+            return 0
+        size = np.zeros(nc, np.int64)
+        lib_.orc_pair_rows(_p(keys), _p(counts), _i(len(keys)), n1u, _p(label), _i(nv),
+                           _p(size))
+        alive[:] = alive & (label == int(np.argmax(size)))
+        return nc
+
+    out = {"components_before": keep_largest()}
+    rows0 = np.zeros(n0, np.int64)
+    lib_.orc_level_rows(_p(keys), _p(counts), _i(len(keys)), n1u, _p(alive), _i(n0), _p(rows0))
+    single = (rows0 == 1) & (alive[:n0] != 0)
+    out["single_observation"] = int(single.sum())
+    if out["single_observation"]:
+        alive[:n0] &= ~single
+        keep_largest()
+    cut_total, rounds = 0, 0
+    is_cut = np.zeros(nv, np.uint8)
+    while True:
+        is_cut[:] = 0
+        lib_.orc_articulation_points(_p(indptr), _p(indices), _i(nv), _p(is_cut), _p(alive))
+        cut = (is_cut[:n0] != 0) & (alive[:n0] != 0)
+        n_cut = int(cut.sum())
+        if not n_cut:
+            break
+        cut_total += n_cut
+        rounds += 1
+        alive[:n0] &= ~cut
+        keep_largest()
+    out.update(cut=cut_total, rounds=rounds)
+    lab = np.where(alive != 0, 0, -1).astype(np.int64)
+    rows = np.zeros(1, np.int64)
+    lib_.orc_pair_rows(_p(keys), _p(counts), _i(len(keys)), n1u, _p(lab), _i(nv), _p(rows))
+    return alive != 0, int(rows[0]), out
+
+
 
 # ------------------------------------------------ steps 3-4 of a fit
 

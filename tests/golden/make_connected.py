@@ -10,7 +10,9 @@ core/connected.py:656-687 `_DistinctPairs` does (sorted keys a * n1 + b and
 their row counts), then runs the reference's core/kernels_graph.py kernels
 the way `_find_components` (core/connected.py:378-493) does for
 `connected="largest"`: `_nb_peel` for min_degree, `_nb_union_keys`,
-`_nb_dense_labels`, `_nb_pair_rows`, and the stable ranking by rows.
+`_nb_dense_labels`, `_nb_pair_rows`, and the stable ranking by rows; and
+the leave-one-out connected set, core/connected.py:503-557 `_leave_one_out`
+(after `_nb_peel` for min_degree (2, 2), as `_find_components` does).
 Inputs and outputs go to tests/golden/connected.npz.  Nothing at test time
 reads the reference.
 """
@@ -36,11 +38,16 @@ PANELS = {
     "middle": dict(n_workers=3_000, n_firms=600, n_years=8, spell=(2, 8), p_move=0.04, seed=23),
     # one large component with a fringe
     "dense": dict(n_workers=4_000, n_firms=300, n_years=10, spell=(2, 10), p_move=0.1, seed=22),
+    # one large component of small firms: single observations and many
+    # articulation-point movers, removed over several rounds
+    "fringe": dict(n_workers=5_000, n_firms=1_500, n_years=8, spell=(1, 8), p_move=0.15,
+                   seed=24),
 }
 
 
 def main(root):
-    kg = import_reference(root)["core.kernels_graph"]
+    mods = import_reference(root)
+    kg, cn = mods["core.kernels_graph"], mods["core.connected"]
     out = {}
     for name, spec in PANELS.items():
         rows = pass0_layout(simulate_panel(**spec))
@@ -72,6 +79,17 @@ def main(root):
             out[f"{name}_k{k}_rows"] = comp_rows[order]
             out[f"{name}_k{k}_rounds"] = np.array([rounds])
             print(name, k, "components", nc, "largest rows", comp_rows[order][:3], "rounds", rounds)
+            # the leave-one-out connected set, after the (k, k) core
+            alive = np.ones(n0 + n1, bool)
+            if k > 1:
+                kg._nb_peel(keys, n1u, k, k, alive[:n0], alive[n0:])
+            lo = cn._leave_one_out(keys, counts, n1u, n0, n1, alive, None)
+            kept = cn._rows_alive(keys, counts, n1u, n0, alive)
+            out[f"{name}_k{k}_loo_alive"] = alive
+            out[f"{name}_k{k}_loo_counts"] = np.array([lo["components_before"],
+                                                       lo["single_observation"], lo["cut"],
+                                                       lo["rounds"], kept])
+            print("  leave-one-out", lo, "rows", kept)
     np.savez_compressed(Path(__file__).resolve().parent / "connected.npz", **out)
 
 

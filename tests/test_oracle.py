@@ -194,3 +194,18 @@ def test_steps_3_4_match_reference(golden):
     assert rel(e, a[f"{name}_resid"]) < 1e-10
     assert rel(alpha, a[f"{name}_alpha"]) < 1e-10
     assert rel(psi, a[f"{name}_psi"]) < 1e-10
+
+
+@pytest.mark.parametrize("panel", ["sparse", "middle", "dense", "fringe"])
+@pytest.mark.parametrize("k", [1, 2])
+def test_leave_one_out_matches_reference(panel, k):
+    """`_leave_one_out` (the leave-one-out connected set, after the (k, k)
+    core): levels kept, components before, single observations, workers cut
+    and rounds, rows kept -- against the reference's own function."""
+    g = load_golden("connected")
+    n0, n1 = (int(x) for x in g[f"{panel}_n"])
+    alive, rows, info = orc.leave_one_out(g[f"{panel}_a"], g[f"{panel}_b"], n0, n1, (k, k))
+    assert np.array_equal(alive, g[f"{panel}_k{k}_loo_alive"])
+    got = [info["components_before"], info["single_observation"], info["cut"], info["rounds"],
+           rows]
+    assert got == [int(x) for x in g[f"{panel}_k{k}_loo_counts"]]
