@@ -326,7 +326,7 @@ def run_jla(args, rank, world, dist):
 
     def finite(x):
         return [float(v) if np.isfinite(v) else None for v in x]
-    out = {"workload": "kss_1m: 1M workers, 100k firms, 10 years, largest connected set; "
+    out = {"workload": "kss_1m: 1M workers, 100k firms, 10 years, leave-one-out connected set; "
                        "log_earn ~ age_squared + age_cubed | worker_id + firm_id",
            "rows": rows.n_rows, "levels": int(sum(rows.n_levels)), "S_nnz": S.nnz, "draws": p,
            "block": 32, "ms": round(ms, 3), "ms_leverages": round(ms_jla, 3),

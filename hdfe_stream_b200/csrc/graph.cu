@@ -39,6 +39,16 @@ __device__ __forceinline__ int32_t find_root(int32_t *parent, int32_t x)
     return x;
 }
 
+// The root of x without writing: for the flattening passes, where each thread
+// writes only its own vertex's entry (a compressing find could overwrite a
+// vertex another thread has just set to its root with a non-root ancestor).
+__device__ __forceinline__ int32_t root_of(const int32_t *parent, int32_t x)
+{
+    int steps = 0;
+    for (int32_t p = parent[x]; p != x && steps < kMaxSteps; p = parent[x], steps++) x = p;
+    return x;
+}
+
 __global__ void __launch_bounds__(kThreads) k_init(int32_t *parent, int64_t n)
 {
     for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
@@ -103,7 +113,7 @@ __global__ void __launch_bounds__(kThreads) k_flatten(int32_t *parent, int64_t n
     unsigned long long roots = 0;
     for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * kThreads) {
-        const int32_t r = find_root(parent, (int32_t)i);
+        const int32_t r = root_of(parent, (int32_t)i);
         parent[i] = r;
         roots += (r == (int32_t)i);
     }

@@ -227,6 +227,29 @@ def restrict_connected(panel: Panel, min_degree=(1, 1)) -> np.ndarray:
     return ok0[a] & ok1[b]
 
 
+def restrict_leave_one_out(panel: Panel, keep: np.ndarray | None = None) -> np.ndarray:
+    """Rows of the leave-one-out connected set of the (worker, firm) network
+    (core/connected.py:503-557 `_leave_one_out`, which the reference's
+    `leave_out_kss` applies), among the rows where `keep`: found on the
+    device by `connected.leave_one_out` from the rows' codes in (worker,
+    firm) order."""
+    import torch
+    from .connected import leave_one_out
+    sel = np.ones(panel.n_rows, bool) if keep is None else np.asarray(keep, bool)
+    idx = np.flatnonzero(sel)
+    a, _ = _rank_codes(panel.worker[idx])
+    b, flev = _rank_codes(panel.firm[idx])
+    n0, n1 = int(a.max()) + 1, len(flev)
+    order = np.lexsort((b, a))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    alive, _ = leave_one_out(torch.as_tensor(a[order].astype(np.int32), device=dev),
+                             torch.as_tensor(b[order].astype(np.int32), device=dev), n0, n1)
+    alive = alive.cpu().numpy()
+    out = np.zeros(panel.n_rows, bool)
+    out[idx] = alive[a] & alive[n0 + b.astype(np.int64)]
+    return out
+
+
 # The panels the solve path is measured on, by what they are.
 PANELS = {
     # 20k workers, 2k firms, 10 years, 8 consecutive years each (160k rows)
@@ -247,14 +270,13 @@ PANELS = {
 def prepare(name: str, seed: int = 0):
     """The named panel's rows in pass 0's layout, restricted as its
     specification says: akm_5m the largest connected set after min_degree 2;
-    kss_1m the largest connected set (the leave-one-out pruning's removal of
-    single-observation and articulation-point workers is not applied), with
-    worker and firm effects only (log_earn ~ age_squared + age_cubed |
-    worker_id + firm_id)."""
+    kss_1m the leave-one-out connected set (found on the device: kss_1m
+    needs a GPU), with worker and firm effects only (log_earn ~ age_squared +
+    age_cubed | worker_id + firm_id)."""
     spec = dict(PANELS[name])
     panel = simulate_panel(seed=seed, **spec)
     if name == "akm_5m":
         return pass0_layout(panel, restrict_connected(panel, (2, 2)))
     if name == "kss_1m":
-        return pass0_layout(panel, restrict_connected(panel, (1, 1)), year_fe=False)
+        return pass0_layout(panel, restrict_leave_one_out(panel), year_fe=False)
     return pass0_layout(panel)

@@ -286,6 +286,24 @@ int hdfe_pair_components(const uint32_t *a, const uint32_t *b, int64_t n_rows, i
                          int64_t *rows, int64_t *counts, void *workspace,
                          int64_t workspace_bytes, void *stream);
 
+/* The leave-one-out connected set: core/connected.py:503-557 `_leave_one_out`
+ * as `_find_components` (:429-447) runs it, after the (k0, k1)-core -- the
+ * largest component by rows, workers (the first dimension) seen in a single
+ * row removed, then every worker that is an articulation point of what is
+ * left removed and the largest piece kept, until no worker is one.  Same
+ * inputs as hdfe_pair_components.  Out (DEVICE): alive (n0 + n1) uint8,
+ * counts[8] int64 = distinct pairs, components before, single-observation
+ * workers, workers cut, cut rounds, rows kept, status, largest BFS depth.
+ * The articulation points come from a breadth-first spanning tree with the
+ * Tarjan-Vishkin rules instead of the reference's depth-first search; the
+ * set is the same.  Reads sizes back to the host between rounds and
+ * synchronises the stream before returning. */
+int64_t hdfe_leave_one_out_workspace_bytes(int64_t n_rows, int64_t n0, int64_t n1);
+
+int hdfe_leave_one_out(const uint32_t *a, const uint32_t *b, int64_t n_rows, int64_t n0,
+                       int64_t n1, int64_t k0, int64_t k1, uint8_t *alive, int64_t *counts,
+                       void *workspace, int64_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------- steps 3-4, KSS components
  *
  * The row passes after step 2 that the leave-out components read, on pass
