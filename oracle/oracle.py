@@ -626,6 +626,102 @@ def row_effects(starts, codes, offs, w, V, Gamma, beta):
     return e, alpha, gam_y[offs[0] + codes[:, 0]], gam_y
 
 
+# ------------------------------------------------ KSS standard-error pieces
+
+def readout(starts, codes, offs, X, U_l, U_c, U_g):
+    """kernels_se.py:19-43 `_nb_readout`: (A u)_i = u_g(i) + sum_d
+    u_levels[level_d(i)] + x_i' u_cov, rows (N, m)."""
+    codes = np.asarray(codes, np.int64)
+    out = np.repeat(np.asarray(U_g, float), np.diff(starts), axis=0)
+    for d in range(codes.shape[1]):
+        out = out + U_l[offs[d] + codes[:, d]]
+    for c in range(X.shape[1]):
+        out = out + X[:, c:c + 1] * U_c[c][None, :]
+    return out
+
+
+def cov_cross(starts, codes, psi_column, psi_offset, w, U_l, U_g, L):
+    """kernels_se.py:46-77 `_nb_cov_cross`: (acc (L, m): per psi level the sum
+    of w_i u_streamed[g(i)]; out_groups (G, m): per group the sum of w_i
+    u_levels[psi(i)])."""
+    lev = psi_offset + np.asarray(codes, np.int64)[:, psi_column]
+    ug = np.repeat(np.asarray(U_g, float), np.diff(starts), axis=0)
+    m = ug.shape[1]
+    acc = np.zeros((L, m))
+    for j in range(m):
+        acc[:, j] = np.bincount(lev, weights=w * ug[:, j], minlength=L)
+    return acc, np.add.reduceat(w[:, None] * U_l[lev], starts[:-1], axis=0)
+
+
+SMOOTH_QUANTILE_SAMPLE = 2_000_000
+
+
+def _smooth_bins(n, dims):
+    """leaveout_se.py:955-964 `_auto_bins`: n^(1/6) bins per axis in two
+    dimensions (n^(1/3) in one), clipped to 2..500."""
+    power = 1.0 / 6.0 if dims == 2 else 1.0 / 3.0
+    return int(np.clip(round(n ** power), 2, 500))
+
+
+def _smooth_knots(values, n_bins, take):
+    """leaveout_se.py:967-973 `_knots`: strictly increasing quantile knots."""
+    q = np.quantile(np.asarray(values[take], dtype=np.float64),
+                    np.linspace(0.0, 1.0, n_bins + 1))
+    q = np.maximum.accumulate(q)
+    span = max(float(q[-1] - q[0]), 1e-300)
+    return q + np.arange(len(q)) * span * 1e-12
+
+
+def _smooth_rank(knots, values):
+    """leaveout_se.py:976-979 `_rank`: piecewise-linear map to [0, 1]."""
+    return np.interp(np.asarray(values, dtype=np.float64), knots,
+                     np.linspace(0.0, 1.0, len(knots)))
+
+
+def fit_smoother(sigma2, leverage, b_ii=None, n_bins=None):
+    """leaveout_se.py:982-1035 `fit_smoother`: sigma2 averaged over a grid of
+    cells in the empirical quantiles of (P_ii, B_ii); (knots, means, bins)."""
+    n = len(sigma2)
+    dims = 1 if b_ii is None else 2
+    n_bins = _smooth_bins(n, dims) if n_bins is None else int(n_bins)
+    if n_bins < 1:
+        return None
+    rng = np.random.default_rng(0)
+    take = (np.arange(n) if n <= SMOOTH_QUANTILE_SAMPLE
+            else np.sort(rng.choice(n, SMOOTH_QUANTILE_SAMPLE, replace=False)))
+    knots = (_smooth_knots(leverage, n_bins, take),
+             None if b_ii is None else _smooth_knots(b_ii, n_bins, take))
+    shape = (n_bins,) * dims
+    cells = [np.minimum((_smooth_rank(knots[0], leverage) * n_bins).astype(np.int64),
+                        n_bins - 1)]
+    if b_ii is not None:
+        cells.append(np.minimum((_smooth_rank(knots[1], b_ii) * n_bins).astype(np.int64),
+                                n_bins - 1))
+    flat = np.ravel_multi_index(cells, shape)
+    totals = np.bincount(flat, weights=np.asarray(sigma2, float),
+                         minlength=int(np.prod(shape))).reshape(shape)
+    counts = np.bincount(flat, minlength=int(np.prod(shape))).reshape(shape)
+    overall = float(totals.sum() / max(counts.sum(), 1.0))
+    means = np.where(counts > 0, totals / np.maximum(counts, 1.0), overall)
+    return knots, means, n_bins
+
+
+def smooth_eval(table, leverage, b_ii=None):
+    """leaveout_se.py:1038-1054 `smooth_eval`: bilinear between cell centres."""
+    knots, means, n_bins = table
+
+    def weights(values, k):
+        f = _smooth_rank(knots[k], values) * n_bins - 0.5
+        j0 = np.clip(np.floor(f).astype(np.int64), 0, n_bins - 2)
+        return j0, np.clip(f - j0, 0.0, 1.0)
+    i0, a = weights(leverage, 0)
+    if knots[1] is None:
+        return (1.0 - a) * means[i0] + a * means[i0 + 1]
+    j0, b = weights(b_ii, 1)
+    return ((1.0 - a) * (1.0 - b) * means[i0, j0] + a * (1.0 - b) * means[i0 + 1, j0]
+            + (1.0 - a) * b * means[i0, j0 + 1] + a * b * means[i0 + 1, j0 + 1])
+
+
 # ------------------------------------------------- inverse operator, JLA
 
 class Design:
@@ -811,6 +907,164 @@ class Design:
         bias = self.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003)
         return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "beta": beta,
                 "sigma2": sigma2, "max_leverage": float(lev.max())}
+
+    # ---- KSS standard errors (leaveout_se.py), weighted centring
+
+    def se_layout(self):
+        """leaveout_se.py:135-180 `_level_weight_totals` / `_se_layout`:
+        (per-level weight totals, per-group totals, total, the n - 1 divisor
+        `_moment_divisor`, the psi dimension's slice of the levels)."""
+        cells, starts = self.cells, self.starts
+        L = cells.L
+        codes = np.asarray(self.codes, np.int64)
+        lw = np.zeros(L)
+        for d in range(codes.shape[1]):
+            lw += np.bincount(cells.offs[d] + codes[:, d], weights=self.w, minlength=L)
+        gw = np.add.reduceat(self.w, starts[:-1])
+        total = float(gw.sum())
+        R = float(self.rows.n_rows)
+        norm = total * (R - 1.0) / R if R > 1 else total
+        psi = slice(int(cells.offs[0]), int(cells.offs[0]) + int(cells.n_levels[0]))
+        return lw, gw, total, norm, psi
+
+    def _roots(self):
+        root = np.sqrt(self.w)
+        return root, np.divide(1.0, root, out=np.zeros_like(root), where=root > 0)
+
+    def _to_coef(self, R):
+        """A' W R as (levels, covariates, groups): `_nb_reduce_rows` and
+        `_nb_group_sums` on explicit rows."""
+        cells, starts = self.cells, self.starts
+        acc, acc_x = reduce_rows(starts, self.codes, cells.offs, self.w, self.X, R, cells.L,
+                                 self.nt)
+        return acc, acc_x, group_sums(starts, self.w, R)
+
+    def bii_rows(self, n_draws, block, seed):
+        """leaveout_se.py:228-327 `bii_rows`: B_ii of var(psi), var(alpha)
+        and cov per row, (3, N), by random projection (one pair of solves per
+        draw)."""
+        lw, gw, total, norm, psi = self.se_layout()
+        N, L, G, c = self.rows.n_rows, self.cells.L, len(self.starts) - 1, self.X.shape[1]
+        root, inv = self._roots()
+        root_total = np.sqrt(norm)
+        out = np.zeros((3, N))
+        drawn = 0
+        while drawn < n_draws:
+            size = min(block, n_draws - drawn)
+            q = rademacher(0, N, size, seed, drawn) * inv[:, None]
+            levels, _, gsum = self._to_coef(q)
+            grand = levels[psi].sum(axis=0) / total
+            rhs_l = np.zeros((L, 2 * size))
+            rhs_l[psi, :size] = (levels[psi] - np.outer(lw[psi], grand)) / root_total
+            rhs_g = np.zeros((G, 2 * size))
+            rhs_g[:, size:] = (gsum - np.outer(gw, grand)) / root_total
+            U_l, U_c, U_g, _ = self.apply_inverse(rhs_l, np.zeros((c, 2 * size)), rhs_g)
+            rows = readout(self.starts, self.codes, self.cells.offs, self.X, U_l, U_c, U_g)
+            x, y = root[:, None] * rows[:, :size], root[:, None] * rows[:, size:]
+            out[0] += (x * x).sum(axis=1)
+            out[1] += (y * y).sum(axis=1)
+            out[2] += (x * y).sum(axis=1)
+            drawn += size
+        return out / n_draws
+
+    def apply_q(self, k, U_l, U_g, layout):
+        """leaveout_se.py:339-385 `_apply_q`: Q_k u in coefficient space
+        (k = 0 var(psi), 1 var(alpha), 2 cov, the last with a row sweep)."""
+        lw, gw, total, norm, psi = layout
+        L, G = self.cells.L, len(self.starts) - 1
+        m = U_l.shape[1]
+        out_l, out_g = np.zeros((L, m)), np.zeros((G, m))
+        level_w, base = lw[psi], U_l[psi]
+        psi_mean = (level_w @ base) / total
+        alpha_mean = (gw @ U_g) / total
+        if k == 0:
+            out_l[psi] = level_w[:, None] * (base - psi_mean) / norm
+        elif k == 1:
+            out_g[:] = gw[:, None] * (U_g - alpha_mean) / norm
+        else:
+            cross_l, cross_g = cov_cross(self.starts, self.codes, 0, int(self.cells.offs[0]),
+                                         self.w, U_l, U_g, L)
+            out_l[psi] = (cross_l[psi] - level_w[:, None] * alpha_mean) / (2 * norm)
+            out_g[:] = (cross_g - gw[:, None] * psi_mean) / (2 * norm)
+        return out_l, out_g
+
+    def apply_c(self, v, b, per_component, layout):
+        """leaveout_se.py:426-597 `_apply_c` (no deflation, no rank-two
+        term): C v = B v - (b .* M v + M (b .* v)) / 2 for each component,
+        v (N, size) shared or (N, 3, size) one per component; (N, 3, size)."""
+        N, L, G, c = self.rows.n_rows, self.cells.L, len(self.starts) - 1, self.X.shape[1]
+        n_in = 3 if per_component else 1
+        size = v.shape[-1]
+        root, inv = self._roots()
+
+        def part(k):
+            return v[:, k, :] if per_component else v
+
+        def in_cols(k):
+            j = k if per_component else 0
+            return slice(j * size, (j + 1) * size)
+
+        def b_cols(k):
+            return slice((n_in + k) * size, (n_in + k + 1) * size)
+        stack = np.empty((N, (n_in + 3) * size))
+        for k in range(n_in):
+            stack[:, k * size:(k + 1) * size] = part(k)
+        for k in range(3):
+            stack[:, b_cols(k)] = part(k) * b[k][:, None]
+        levels, cov_block, gsum = self._to_coef(stack * inv[:, None])
+        U0_l, U0_c, U0_g, _ = self.apply_inverse(levels, cov_block, gsum)
+        q_l, q_g = np.zeros((L, 3 * size)), np.zeros((G, 3 * size))
+        for k in range(3):
+            cols = slice(k * size, (k + 1) * size)
+            q_l[:, cols], q_g[:, cols] = self.apply_q(k, U0_l[:, in_cols(k)],
+                                                      U0_g[:, in_cols(k)], layout)
+        U1_l, U1_c, U1_g, _ = self.apply_inverse(q_l, np.zeros((c, 3 * size)), q_g)
+        offs = self.cells.offs
+        base = readout(self.starts, self.codes, offs, self.X, U0_l, U0_c, U0_g)
+        through_q = readout(self.starts, self.codes, offs, self.X, U1_l, U1_c, U1_g)
+        cv = np.empty((N, 3, size))
+        for k in range(3):
+            vk = part(k)
+            Mv = vk - root[:, None] * base[:, in_cols(k)]
+            Bv = root[:, None] * through_q[:, k * size:(k + 1) * size]
+            M_bv = vk * b[k][:, None] - root[:, None] * base[:, b_cols(k)]
+            cv[:, k, :] = Bv - 0.5 * (b[k][:, None] * Mv + M_bv)
+        return cv
+
+    def component_variances(self, sigma2, leverage, complement, factor, b_ii, n_draws,
+                            block, seed, smooth_bins=None):
+        """leaveout_se.py:599-784 `component_variances` (weighted centring,
+        trace included, no weak-identification pieces): per component the
+        first term 4 sum s~ (C y~)^2, the trace term 2 tr(C Om~ C Om~) by
+        Hutchinson draws (seed + 7_700_017), theta = y~' C y~, and
+        variance = first - trace term; s~ the smoothed sigma2."""
+        layout = self.se_layout()
+        b = b_ii * (factor / complement)[None, :]
+        tables = [fit_smoother(sigma2, leverage, b_ii[k], smooth_bins) for k in range(3)]
+        sig = [smooth_eval(t, leverage, b_ii[k]) if t is not None else np.asarray(sigma2)
+               for k, t in enumerate(tables)]
+        y = self.rows.V[:, 0]
+        w = self.w
+        y_bar = float(w @ y / w.sum())
+        shifted = np.sqrt(w) * (y - y_bar)
+        cv = self.apply_c(shifted[:, None], b, False, layout)
+        first = np.array([4.0 * float(sig[k] @ (cv[:, k, 0] ** 2)) for k in range(3)])
+        theta = np.array([float(shifted @ cv[:, k, 0]) for k in range(3)])
+        trace = np.zeros(3)
+        N = self.rows.n_rows
+        drawn = 0
+        while drawn < n_draws:
+            size = min(block, n_draws - drawn)
+            z = rademacher(0, N, size, seed + 7_700_017, drawn)
+            v = np.stack([z * np.sqrt(np.maximum(sig[k], 0.0))[:, None] for k in range(3)],
+                         axis=1)
+            cvt = self.apply_c(v, b, True, layout)
+            for k in range(3):
+                trace[k] += float(sig[k] @ (cvt[:, k, :] ** 2).sum(axis=1))
+            drawn += size
+        trace /= n_draws
+        return {"variance": first - 2.0 * trace, "first_term": first,
+                "trace_term": 2.0 * trace, "theta": theta}
 
     def jla_leverages(self, n_draws, block, seed):
         """leaveout.py:130-198 `jla_leverages` and :210-282

@@ -209,3 +209,30 @@ def test_leave_one_out_matches_reference(panel, k):
     got = [info["components_before"], info["single_observation"], info["cut"], info["rounds"],
            rows]
     assert got == [int(x) for x in g[f"{panel}_k{k}_loo_counts"]]
+
+
+def se_rows(g, name):
+    """The standard-error golden panel's rows (its leave-one-out set)."""
+    from hdfe_stream_b200.simulate import Rows
+    w = g[f"{name}_w"] if len(g[f"{name}_w"]) else None
+    return Rows(gcode=g[f"{name}_gcode"], codes=g[f"{name}_codes_rows"], V=g[f"{name}_V"], w=w,
+                n_levels=[int(x) for x in g[f"{name}_n_levels"]],
+                n_groups=int(g[f"{name}_n_groups"][0]),
+                names=["log_earn", "age_squared", "age_cubed"])
+
+
+@pytest.mark.parametrize("name", ["akm_small", "akm_weighted"])
+def test_standard_errors_match_reference(name):
+    """leaveout_se.py `bii_rows` and `component_variances` (B_ii per row,
+    the first and trace terms, theta, the variance) against the reference's
+    own outputs for the same draws."""
+    g = load_golden("se")
+    rows = se_rows(g, name)
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g[f"{name}_tol"][0]))
+    b_ii = des.bii_rows(16, 8, 6)
+    assert rel(b_ii, g[f"{name}_bii"]) < 1e-9
+    out = des.component_variances(g[f"{name}_sigma2"], g[f"{name}_leverage"],
+                                  g[f"{name}_complement"], g[f"{name}_factor"], b_ii, 16, 8, 6)
+    for key in ("first_term", "trace_term", "theta", "variance"):
+        assert rel(out[key], g[f"{name}_{key}"]) < 1e-8, key
