@@ -80,6 +80,16 @@ SIGNATURES = {
     "hdfe_leave_one_out_workspace_bytes": (_i64, [_i64, _i64, _i64]),
     "hdfe_leave_one_out": (_c.c_int, [_vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp, _vp, _vp,
                                       _i64, _vp]),
+    "hdfe_rows_readout": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i32, _vp, _vp, _vp,
+                                     _i32, _vp, _vp, _vp, _vp]),
+    "hdfe_cov_cross": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _vp, _i32, _vp,
+                                  _vp, _vp, _vp]),
+    "hdfe_bii_moments": (_c.c_int, [_vp, _i32, _vp, _i64, _vp, _vp]),
+    "hdfe_c_sums_workspace_bytes": (_i64, []),
+    "hdfe_c_sums": (_c.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _i64,
+                               _vp]),
+    "hdfe_smooth_cells": (_c.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
+    "hdfe_smooth_eval": (_c.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),

@@ -302,6 +302,7 @@ class InverseOperator:
         f64 = dict(dtype=torch.float64, device=self.dev)
         gamma = gamma.to(**f64)
         beta = torch.as_tensor(np.asarray(beta, dtype=np.float64)).to(**f64).reshape(-1)
+        beta = beta.contiguous()
         gam_y = (gamma[:, 0] - gamma[:, 1:] @ beta).contiguous() if m > 1 else \
             gamma[:, 0].contiguous()
         resid = torch.empty(self.N, **f64)
@@ -311,7 +312,7 @@ class InverseOperator:
         _lib.check(_lib.lib().hdfe_row_effects(
             self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
             self.nlev.ctypes.data, int(psi_column), self._ptr(self.w), self.rows.V.data_ptr(), m,
-            self.N, beta.contiguous().data_ptr() if m > 1 else None, gam_y.data_ptr(),
+            self.N, beta.data_ptr() if m > 1 else None, gam_y.data_ptr(),
             resid.data_ptr(), alpha.data_ptr(), sums.data_ptr(), ws.data_ptr(), ws.numel(),
             self._status().data_ptr(), _lib.stream_handle()))
         return resid, alpha[:self.G], gam_y, sums

@@ -344,6 +344,61 @@ int hdfe_kss_sigma2(const double *y, const double *w, const double *resid,
                     const double *complement, const double *factor, double ybar,
                     int64_t n_rows, double *out, void *stream);
 
+/* ------------------------------------------------- KSS standard errors
+ *
+ * The row passes of leaveout_se.py's standard errors, in the layouts above:
+ * hdfe_rows_readout: kernels_se.py:19-43 `_nb_readout`, out (N, B) =
+ *   (A u)_i = U_groups[g(i)] + sum_d U_levels[level_d(i)] + x_i' U_cov,
+ *   times sqrt(w_i) when w is given (NULL: not scaled).
+ * hdfe_cov_cross: kernels_se.py:46-77 `_nb_cov_cross`: acc (L, B) is ADDED
+ *   per psi level the sum of w_i U_groups[g(i)] (atomic order), out_groups
+ *   (G, B) = per group the sum of w_i U_levels[psi(i)]; B <= 32.
+ * hdfe_bii_moments: kernels_se.py:80-98 `_nb_bii_moments`: out (3, N) +=
+ *   per row the sums over j < size of (root r1_j)^2, (root r2_j)^2 and
+ *   root^2 r1_j r2_j, rows (N, 2 size) = [r1 | r2], root = sqrt(w) (1 if w
+ *   is NULL).
+ * hdfe_c_sums: leaveout_se.py:579-596 (C v per component, from v, b (3, N)
+ *   and the root-scaled readouts base (N, (n_in + 3) size) of S^- X'[v | b.*v]
+ *   and through_q (N, 3 size) of S^- Q S^- X'v) with the sums the first
+ *   term, theta and the trace term take (:718-726, :918-925): sums[6] =
+ *   per component sum_i s_k,i sum_j cv_kij^2, then sum_i y_i cv_ki0 (y NULL:
+ *   0).  per_component: v is the draws z (N, size) and component k's input is
+ *   z sqrt(max(s_k, 0)); else v (N, size) is shared.  Deterministic.
+ * hdfe_smooth_cells / hdfe_smooth_eval: leaveout_se.py:982-1054: each row's
+ *   cell in the grid of the quantile knots (knots0 of the leverage, knots1 of
+ *   B_ii or NULL for one axis; fp the rank of each knot, n_bins + 1 values
+ *   each), totals / counts (n_bins^dims) ADDED per cell; and the bilinear
+ *   evaluation of the cell means between cell centres.
+ */
+int hdfe_rows_readout(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                      const int64_t *n_levels, const double *X, int32_t c,
+                      const double *U_levels, const double *U_cov, const double *U_groups,
+                      int32_t B, const double *w, double *out, void *status, void *stream);
+
+int hdfe_cov_cross(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                   const int64_t *n_levels, int32_t psi_column, const double *w,
+                   const double *U_levels, const double *U_groups, int32_t B, double *acc,
+                   double *out_groups, void *status, void *stream);
+
+int hdfe_bii_moments(const double *rows, int32_t size, const double *w, int64_t n_rows,
+                     double *out, void *stream);
+
+int64_t hdfe_c_sums_workspace_bytes(void);
+
+int hdfe_c_sums(const double *v, int32_t size, int32_t per_component, const double *b,
+                const double *s, const double *base, const double *through_q, const double *y,
+                int64_t n_rows, double *sums, void *workspace, int64_t workspace_bytes,
+                void *stream);
+
+int hdfe_smooth_cells(const double *knots0, const double *knots1, const double *fp,
+                      int32_t n_bins, const double *leverage, const double *b_ii,
+                      const double *sigma2, int64_t n_rows, double *totals, double *counts,
+                      void *stream);
+
+int hdfe_smooth_eval(const double *knots0, const double *knots1, const double *fp,
+                     int32_t n_bins, const double *means, const double *leverage,
+                     const double *b_ii, int64_t n_rows, double *out, void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,

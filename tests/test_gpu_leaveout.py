@@ -94,11 +94,11 @@ def test_projection_is_idempotent(device):
     U, _ = op.solve_reduced(rhs, torch.sqrt(sq))
     out2 = torch.empty_like(out)
     from hdfe_stream_b200 import _lib
+    U, out = U.contiguous(), out.contiguous()
     _lib.check(_lib.lib().hdfe_rows_project(
         op.starts.data_ptr(), op.G, op.rows.codes.data_ptr(), len(op.nlev),
-        op.nlev.ctypes.data, None, None, 0, None, U.contiguous().data_ptr(),
-        out.contiguous().data_ptr(), 4, 0, 0, 0, 0, op.N, out2.data_ptr(), None,
-        _lib.stream_handle()))
+        op.nlev.ctypes.data, None, None, 0, None, U.data_ptr(), out.data_ptr(), 4, 0, 0, 0, 0,
+        op.N, out2.data_ptr(), None, _lib.stream_handle()))
     assert rel(out2.cpu().numpy(), out.cpu().numpy()) < 1e-8
 
 

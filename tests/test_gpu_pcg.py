@@ -216,11 +216,11 @@ def test_stream_matvec_matches_explicit_s(device, k):
         out = torch.empty((cells.L, k), dtype=torch.float64, device=device)
         nlev = np.asarray(cells.n_levels, dtype=np.int64)
         st = torch.zeros(1, dtype=torch.int32, device=device)
+        Pd = torch.as_tensor(P, device=device)
         _lib.check(_lib.lib().hdfe_stream_matvec(
             cells.starts.data_ptr(), int(cells.starts.shape[0]) - 1, cells.codes.data_ptr(),
-            len(nlev), nlev.ctypes.data, cells.n.data_ptr(),
-            torch.as_tensor(P, device=device).data_ptr(), k, out.data_ptr(), st.data_ptr(),
-            _lib.stream_handle()))
+            len(nlev), nlev.ctypes.data, cells.n.data_ptr(), Pd.data_ptr(), k, out.data_ptr(),
+            st.data_ptr(), _lib.stream_handle()))
         got = out.cpu().numpy()
         assert int(st.item()) == 0
         assert np.max(np.abs(got - ref)) < 1e-12 * np.max(np.abs(ref))
