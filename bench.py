@@ -323,6 +323,17 @@ def run_jla(args, rank, world, dist):
         ms, ms_jla, ms_tr = (float(x) for x in t.tolist())
     sigma2 = kss["sigma2"]
     bad = int((~torch.isfinite(sigma2)).sum().item())
+    # KSS standard errors (leaveout_se.py `component_variances`): B_ii by p
+    # draws, C y, and the trace term by p draws
+    from hdfe_stream_b200.leaveout_se import StandardErrors
+    se_op = StandardErrors(op)
+    se_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    se_ev[0].record()
+    ses = se_op.component_variances(sigma2, kss["leverage"], kss["complement"], kss["factor"],
+                                    None, n_draws=p, block=8, seed=1)
+    se_ev[1].record()
+    torch.cuda.synchronize()
+    ms_se = se_ev[0].elapsed_time(se_ev[1])
 
     def finite(x):
         return [float(v) if np.isfinite(v) else None for v in x]
@@ -339,6 +350,13 @@ def run_jla(args, rank, world, dist):
            "max_leverage": kss["max_leverage"], "plug_in": finite(kss["plug_in"]),
            "bias_terms": finite(kss["bias"]), "leave_out": finite(kss["leave_out"]),
            "rows_without_sigma2": bad,
+           "standard_errors": {"se": dict(zip(ses["se"], finite(ses["se"].values()))),
+                               "se_conservative": dict(zip(ses["se_conservative"], finite(
+                                   ses["se_conservative"].values()))),
+                               "ms": round(ms_se, 3), "draws": p,
+                               "rhs_solves": 2 * p + 7 + 9 * p,
+                               "note": "B_ii: 2 solves per draw; C y: 7; trace term: 9 "
+                                       "per draw (6 then 3)"},
            "iterations_last_block": op.jla_info["iterations"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, str(REPO / "oracle"))

@@ -355,7 +355,8 @@ class InverseOperator:
         with phase("trace"):
             bias = self.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003, psi_column)
         return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "beta": beta,
-                "sigma2": sigma2, "max_leverage": float(lev.max().item())}
+                "sigma2": sigma2, "max_leverage": float(lev.max().item()), "leverage": lev,
+                "complement": comp, "factor": factor}
 
     def jla_leverages(self, n_draws=250, block=MAX_BLOCK, seed=0):
         """leaveout.py:130-198 `jla_leverages`: (leverage, complement, factor)
