@@ -256,3 +256,24 @@ def test_steps_3_4_on_a_device_fit(device):
     gsum = np.add.reduceat(w * e, starts[:-1])
     assert np.max(np.abs(gsum)) < 1e-8 * np.sqrt(w @ (e * e))
     assert rel(w @ (e * e), A[0, 0] - A[0, 1:] @ beta) < 1e-7
+
+
+def test_leave_out_components_against_exact_prototype(device):
+    """On the device, the same check as the oracle's against the reference's
+    dense exact KSS (prototypes/kss_exact.py on a 1,500-worker leave-one-out
+    panel, worker and firm effects only): the plug-in exactly, the leave-out
+    components within 5% of the bias term at 1,024 probes and draws."""
+    import torch
+    from hdfe_stream_b200 import fit, leaveout
+    from hdfe_stream_b200.simulate import Rows
+    g = load_golden("exact")
+    rows = Rows(gcode=g["gcode"], codes=g["codes_rows"], V=g["V"][:, :1], w=None,
+                n_levels=[int(x) for x in g["n_levels"]], n_groups=int(g["n_groups"][0]),
+                names=["log_earn"])
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    op = leaveout.InverseOperator(drows, res.cells, res.S, None, tol=1e-12)
+    out = op.leave_out_components(res.gamma, 1024, 32, 3)
+    assert rel(out["plug_in"], g["plug_in"]) < 1e-9
+    assert np.all(np.abs(out["leave_out"] - g["kss"]) <= 0.05 * np.abs(g["bias"]))
+    assert float(torch.mean(torch.abs(out["leverage"].cpu() - torch.as_tensor(g["P_ii"])))) < 0.02

@@ -236,3 +236,28 @@ def test_standard_errors_match_reference(name):
                                   g[f"{name}_complement"], g[f"{name}_factor"], b_ii, 16, 8, 6)
     for key in ("first_term", "trace_term", "theta", "variance"):
         assert rel(out[key], g[f"{name}_{key}"]) < 1e-8, key
+
+
+def exact_rows(g):
+    from hdfe_stream_b200.simulate import Rows
+    return Rows(gcode=g["gcode"], codes=g["codes_rows"], V=g["V"][:, :1], w=None,
+                n_levels=[int(x) for x in g["n_levels"]], n_groups=int(g["n_groups"][0]),
+                names=["log_earn"])
+
+
+def test_jla_components_against_exact_prototype():
+    """The leave-out components by JLA (1,024 probes and draws) against the
+    reference's dense exact prototype (prototypes/kss_exact.py `kss`,
+    tests/golden/exact.npz): the plug-in exactly, the leave-out estimates
+    within 5% of the bias term, the leverages within 0.02 on average."""
+    g = load_golden("exact")
+    rows = exact_rows(g)
+    c = orc.pass1(rows)
+    S = orc.build_explicit(c)
+    gamma, _ = orc.solve(c, S, tol=1e-12)
+    des = orc.Design(rows, c, S, tol=1e-12)
+    out = des.leave_out_components(gamma, 1024, 32, 3)
+    assert rel(out["plug_in"], g["plug_in"]) < 1e-9
+    assert np.all(np.abs(out["leave_out"] - g["kss"]) <= 0.05 * np.abs(g["bias"]))
+    lev, _, _ = des.jla_leverages(1024, 32, 3)
+    assert np.mean(np.abs(lev - g["P_ii"])) < 0.02
