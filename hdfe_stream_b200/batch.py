@@ -1,0 +1,300 @@
+"""Many independent fixed-effects regressions fitted together.
+
+The systems' rows are laid end to end with disjoint codes (each system's
+groups and levels shifted past the previous systems'), so ONE pass 1 and ONE
+S build serve them all and the reduced matrix comes out block-diagonal.  Its
+levels are renumbered so each system's are contiguous, and one persistent
+launch (`hdfe_batch_pcg_solve`, csrc/batch.cu) runs the Jacobi block PCG of
+every system with its own scalars -- the same algorithm, iteration rule and
+tolerance as a single fit (core/solve.py:66-140) -- over warps that the host
+assigns to the systems in proportion to their cost.  The lanes per row of the
+SpMV are tuned on the batch itself (`BatchSolver.tune`).  The normalisation
+is the reference's per system (core/solve.py:383-399: the first non-streamed
+dimension per connected component, the others per system).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .fit import RHS_ZERO_TOL, DeviceRows, build_s, components, jacobi, pass1
+from .simulate import Rows
+
+LANE_CHOICES = (4, 8, 16, 32)
+ROW_COST = 32           # a row's fixed cost in the warp split, in nonzeros
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@dataclass
+class Batch:
+    """Systems laid end to end: `rows` and per system its rows, groups and,
+    per dimension, level ranges (start, count) in the combined numbering."""
+
+    rows: Rows
+    row_ranges: list
+    group_ranges: list
+    level_ranges: list          # [system][dim] = (start within the dim, count)
+
+
+def concat(systems) -> Batch:
+    """Lay systems (pass 0's `Rows`, the same dimensions and variables) end
+    to end with disjoint codes."""
+    D = systems[0].codes.shape[1]
+    m = systems[0].V.shape[1]
+    weighted = systems[0].w is not None
+    for r in systems:
+        if r.codes.shape[1] != D or r.V.shape[1] != m or (r.w is not None) != weighted:
+            raise ValueError("systems must share dimensions, variables and weighting")
+    gcodes, codes, V, w = [], [], [], []
+    row_ranges, group_ranges, level_ranges = [], [], []
+    g0, r0 = 0, 0
+    l0 = [0] * D
+    for r in systems:
+        gcodes.append(r.gcode.astype(np.int64) + g0)
+        c = r.codes.astype(np.int64).copy()
+        lv = []
+        for d in range(D):
+            c[:, d] += l0[d]
+            lv.append((l0[d], int(r.n_levels[d])))
+            l0[d] += int(r.n_levels[d])
+        codes.append(c)
+        V.append(r.V)
+        if weighted:
+            w.append(r.w)
+        row_ranges.append((r0, r.n_rows))
+        group_ranges.append((g0, r.n_groups))
+        level_ranges.append(lv)
+        g0 += r.n_groups
+        r0 += r.n_rows
+    rows = Rows(gcode=np.concatenate(gcodes).astype(np.uint32),
+                codes=np.ascontiguousarray(np.concatenate(codes).astype(np.uint32)),
+                V=np.ascontiguousarray(np.concatenate(V)),
+                w=np.concatenate(w) if weighted else None, n_levels=list(l0), n_groups=g0,
+                names=list(systems[0].names))
+    return Batch(rows, row_ranges, group_ranges, level_ranges)
+
+
+def split_rows(S, level_perm, sys_of_new, n_systems, blocks_warps):
+    """Warp ranges: (warp_rows (W+1), warp_system (W), system_warps (n+1)).
+    Each system gets one warp and then warps in proportion to its cost
+    (nonzeros + ROW_COST per row, largest remainders); its rows are split
+    over them by cumulative cost."""
+    indptr = S.indptr.cpu().numpy()
+    rowlen = np.diff(indptr)[level_perm]
+    cost = rowlen + ROW_COST
+    W = int(blocks_warps)
+    if n_systems > W:
+        raise ValueError(f"{n_systems} systems need more than the grid's {W} warps")
+    bounds = np.searchsorted(sys_of_new, np.arange(n_systems + 1))     # row range per system
+    sys_cost = np.bincount(sys_of_new, weights=cost, minlength=n_systems)
+    share = sys_cost / max(sys_cost.sum(), 1) * (W - n_systems)
+    nw = 1 + np.floor(share).astype(np.int64)
+    spare = W - int(nw.sum())
+    order = np.argsort(-(share - np.floor(share)), kind="stable")
+    for i in order[:spare]:
+        nw[i] += 1
+    warp_rows = np.empty(W + 1, np.int64)
+    warp_sys = np.empty(W, np.int32)
+    system_warps = np.zeros(n_systems + 1, np.int32)
+    w = 0
+    for i in range(n_systems):
+        a, b = int(bounds[i]), int(bounds[i + 1])
+        c = np.concatenate(([0], np.cumsum(cost[a:b])))
+        targets = c[-1] * np.arange(nw[i]) / nw[i]
+        starts = a + np.searchsorted(c, targets, side="left")
+        starts = np.minimum(np.maximum.accumulate(starts), b)
+        system_warps[i] = w
+        for j in range(nw[i]):
+            warp_rows[w] = starts[j]
+            warp_sys[w] = i
+            w += 1
+    system_warps[n_systems] = w
+    end = int(bounds[-1])
+    while w < W:                  # any warps left over own no rows
+        warp_rows[w] = end
+        warp_sys[w] = n_systems - 1
+        w += 1
+    warp_rows[W] = end
+    return warp_rows, warp_sys, system_warps
+
+
+class BatchSolver:
+    """The block-diagonal system of a `Batch` after pass 1 and the S build,
+    renumbered system by system, with its warp split for the batched PCG."""
+
+    def __init__(self, batch: Batch, tol=1e-10, maxiter=5000, lanes=None):
+        torch = _torch()
+        self.batch = batch
+        self.tol, self.maxiter = float(tol), int(maxiter)
+        rows = batch.rows
+        self.drows = DeviceRows.from_rows(rows)
+        self.cells = pass1(self.drows)
+        self.S = build_s(self.cells)
+        dev = self.S.indptr.device
+        D = rows.codes.shape[1]
+        offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1])).astype(np.int64)
+        n = len(batch.level_ranges)
+        perm, sys_of = [], []
+        for i, lv in enumerate(batch.level_ranges):
+            start = len(perm)
+            for d in range(D):
+                s0, cnt = lv[d]
+                perm.extend(range(int(offs[d]) + s0, int(offs[d]) + s0 + cnt))
+            sys_of.extend([i] * (len(perm) - start))
+        self.perm = np.asarray(perm, np.int64)
+        self.sys_of = np.asarray(sys_of, np.int64)
+        L = len(self.perm)
+        inv = np.empty(L, np.int64)
+        inv[self.perm] = np.arange(L)
+        self.perm_t = torch.as_tensor(self.perm, device=dev)
+        self.inv_t = torch.as_tensor(inv, device=dev)
+        # CSR of the renumbered matrix: row r of it is row perm[r] of S,
+        # columns mapped through inv (entries keep their order)
+        S = self.S
+        rowlen = (S.indptr[1:] - S.indptr[:-1])[self.perm_t]
+        indptr = torch.zeros(L + 1, dtype=torch.int64, device=dev)
+        indptr[1:] = torch.cumsum(rowlen, 0)
+        nnz = int(indptr[-1].item())
+        src = torch.repeat_interleave(S.indptr[:-1][self.perm_t], rowlen) + (
+            torch.arange(nnz, device=dev) - torch.repeat_interleave(indptr[:-1], rowlen))
+        self.indptr = indptr
+        self.indices = self.inv_t[S.indices[src].to(torch.int64)].to(torch.int32).contiguous()
+        self.data = S.data[src].contiguous()
+        self.dinv = jacobi(self.cells.diag)[self.perm_t].contiguous()
+        self.m = int(self.cells.rhs.shape[1])
+        self.B = self.cells.rhs[self.perm_t].contiguous()
+        # per system zero right-hand sides (core/solve.py:44): ||b|| <= 1e-11 sqrt(raw ss)
+        zero = np.zeros((n, self.m), np.uint8)
+        bn = torch.zeros((n, self.m), dtype=torch.float64, device=dev).index_add_(
+            0, torch.as_tensor(self.sys_of, device=dev), self.B * self.B).cpu().numpy()
+        for i, (r0, cnt) in enumerate(batch.row_ranges):
+            Vi = rows.V[r0:r0 + cnt]
+            raw = ((Vi - Vi.mean(axis=0)) ** 2).sum(axis=0) if cnt else np.zeros(self.m)
+            zero[i] = np.sqrt(bn[i]) <= RHS_ZERO_TOL * np.sqrt(np.maximum(raw, 0.0))
+        self.zero = torch.as_tensor(zero.reshape(-1), device=dev)
+        self.n = n
+        self.lanes = lanes
+        self._plans = {}
+        self.root, _ = components(self.cells, 0)
+
+    def plan(self, lanes):
+        """Grid and warp split for a lanes-per-row choice."""
+        torch = _torch()
+        if lanes not in self._plans:
+            lib = _lib.lib()
+            blocks = _lib._c.c_int32()
+            wpb = _lib._c.c_int32()
+            _lib.check(lib.hdfe_batch_pcg_grid(self.m, lanes, _lib._c.byref(blocks),
+                                               _lib._c.byref(wpb)))
+            W = blocks.value * wpb.value
+            wr, ws, sw = split_rows(self.S, self.perm, self.sys_of, self.n, W)
+            dev = self.indptr.device
+            ws_bytes = int(lib.hdfe_batch_pcg_workspace_bytes(len(self.perm), self.m, W))
+            self._plans[lanes] = dict(
+                blocks=blocks.value, warp_rows=torch.as_tensor(wr, device=dev),
+                warp_sys=torch.as_tensor(ws, device=dev),
+                sys_warps=torch.as_tensor(sw, device=dev),
+                ws=torch.empty(ws_bytes, dtype=torch.uint8, device=dev))
+        return self._plans[lanes]
+
+    def solve(self, lanes=None):
+        """X (L, m) in the renumbered order and per-system info."""
+        torch = _torch()
+        lanes = lanes or self.lanes or 8
+        p = self.plan(lanes)
+        dev = self.indptr.device
+        L = len(self.perm)
+        X = torch.empty((L, self.m), dtype=torch.float64, device=dev)
+        its = torch.empty(self.n, dtype=torch.int64, device=dev)
+        rel = torch.empty(self.n, dtype=torch.float64, device=dev)
+        conv = torch.empty(self.n, dtype=torch.int32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        _lib.check(_lib.lib().hdfe_batch_pcg_solve(
+            self.indptr.data_ptr(), self.indices.data_ptr(), self.data.data_ptr(), L,
+            self.dinv.data_ptr(), self.B.data_ptr(), self.m, self.zero.data_ptr(), self.n,
+            p["warp_rows"].data_ptr(), p["warp_sys"].data_ptr(), p["sys_warps"].data_ptr(),
+            p["blocks"], lanes, self.tol, self.maxiter, X.data_ptr(), its.data_ptr(),
+            rel.data_ptr(), conv.data_ptr(), status.data_ptr(), p["ws"].data_ptr(),
+            p["ws"].numel(), _lib.stream_handle()))
+        st = int(status.item())
+        if st != _lib.HDFE_OK:
+            raise _lib.HDFEError(st, "batched PCG stopped early")
+        return X, {"iterations": its.cpu().numpy(), "max_rel_residual": rel.cpu().numpy(),
+                   "converged": conv.cpu().numpy().astype(bool), "lanes": lanes}
+
+    def tune(self):
+        """Lanes per row for this batch: each choice timed once with CUDA
+        events after one untimed solve, the fastest kept."""
+        torch = _torch()
+        best, best_ms = None, None
+        for lanes in LANE_CHOICES:
+            self.solve(lanes)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            self.solve(lanes)
+            b.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b)
+            if best_ms is None or ms < best_ms:
+                best, best_ms = lanes, ms
+        self.lanes = best
+        return best
+
+    def normalize(self, X):
+        """Gamma (L, m) in the combined numbering, normalised per system
+        (core/solve.py:383-399)."""
+        torch = _torch()
+        rows = self.batch.rows
+        dev = X.device
+        G = torch.empty_like(X)
+        G[self.perm_t] = X
+        offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1])).astype(np.int64)
+        obs = self.cells.obs
+        nl0 = int(rows.n_levels[0])
+        w0 = obs[:nl0]
+        root = self.root.to(torch.int64)
+        cw = torch.zeros(nl0, dtype=torch.float64, device=dev).index_add_(0, root, w0)
+        cw = torch.where(cw == 0, torch.ones_like(cw), cw)
+        cs = torch.zeros((nl0, self.m), dtype=torch.float64, device=dev).index_add_(
+            0, root, w0[:, None] * G[:nl0])
+        G[:nl0] -= (cs / cw[:, None])[root]
+        for d in range(1, rows.codes.shape[1]):
+            o, nl = int(offs[d]), int(rows.n_levels[d])
+            sys_d = torch.as_tensor(np.repeat(np.arange(self.n), [lv[d][1] for lv in
+                                                                   self.batch.level_ranges]),
+                                    device=dev)
+            wd = obs[o:o + nl]
+            sw = torch.zeros(self.n, dtype=torch.float64, device=dev).index_add_(0, sys_d, wd)
+            ss = torch.zeros((self.n, self.m), dtype=torch.float64, device=dev).index_add_(
+                0, sys_d, wd[:, None] * G[o:o + nl])
+            G[o:o + nl] -= (ss / torch.clamp(sw, min=1.0)[:, None])[sys_d]
+        return G
+
+    def gammas(self, G):
+        """Per system its effects (L_i, m), dimension by dimension."""
+        torch = _torch()
+        rows = self.batch.rows
+        offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1])).astype(np.int64)
+        out = []
+        for lv in self.batch.level_ranges:
+            out.append(torch.cat([G[int(offs[d]) + s0:int(offs[d]) + s0 + cnt]
+                                  for d, (s0, cnt) in enumerate(lv)], 0))
+        return out
+
+
+def fit_batch(systems, tol=1e-10, maxiter=5000, lanes=None, tune=False):
+    """Fit every system of `systems` (pass 0's `Rows`): one pass 1, one S
+    build, one batched PCG launch.  Returns (per-system gamma (L_i, m) on
+    the device, info)."""
+    solver = BatchSolver(concat(systems), tol, maxiter, lanes)
+    if tune:
+        solver.tune()
+    X, info = solver.solve()
+    return solver.gammas(solver.normalize(X)), info

@@ -1,0 +1,391 @@
+// Many independent fixed-effects systems in one persistent launch.
+//
+// The systems' reduced matrices sit on the diagonal of one CSR matrix, each
+// system's levels a contiguous range of rows.  Every warp of the cooperative
+// grid owns a contiguous range of rows inside ONE system (the host splits the
+// systems' rows over the warps by cost, at least one warp per system), so the
+// Jacobi block PCG of core/solve.py:66-140 runs per system with its own
+// scalars: per (system, column) alpha, beta, the active flag and the relative
+// residual, exactly the algorithm of the single-system kernel (pcg.cu).  The
+// dot products are per-warp partials; after a grid barrier each warp sums its
+// system's partials (lanes over the system's warps, then a warp sum: a fixed
+// order, so every warp of a system holds the same scalars and the result does
+// not depend on scheduling).  The loop ends when no system has an active
+// column: a flag per iteration parity, set by the warps whose system is still
+// active and cleared two phases before its next use.
+//
+// The SpMV gives each row LPR lanes (4, 8, 16 or 32: the caller's tuner picks
+// it for the batch), LPR nonzeros in flight per row, reduced by shuffles.
+#include <climits>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace hdfe {
+namespace batch {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxK = 8;
+
+struct Args {
+    const int64_t *indptr;
+    const int32_t *indices;
+    const double *data;
+    int64_t L;
+    const double *dinv;
+    const double *B;            // (L, K)
+    const uint8_t *zero;        // (systems, K) or null
+    double tol;
+    int64_t maxiter;
+    double *X, *R, *P, *AP;     // (L, K)
+    const int64_t *wrow;        // (warps + 1) first row of each warp
+    const int32_t *wsys;        // (warps) system of each warp
+    const int32_t *swarp;       // (systems + 1) first warp of each system
+    double *part;               // (warps, 3, K)
+    unsigned *flag;             // [2]
+    unsigned *bar;
+    int64_t *iterations;        // (systems)
+    double *max_rel;            // (systems)
+    int32_t *converged;         // (systems)
+};
+
+// sum of part[w][q] over the system's warps [w0, w1), fixed order
+__device__ __forceinline__ double system_sum(const double *part, int stride, int q, int w0, int w1)
+{
+    double t = 0.0;
+    for (int w = w0 + (int)(threadIdx.x & 31); w < w1; w += 32) t += part[(int64_t)w * stride + q];
+    return warp_sum(t);
+}
+
+template <int K, int LPR>
+__global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
+{
+    GridBarrier gb{a.bar};
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
+    const int64_t r0 = a.wrow[gw], r1 = a.wrow[gw + 1];
+    const int sys = a.wsys[gw];
+    const int w0 = a.swarp[sys], w1 = a.swarp[sys + 1];
+    constexpr int S3 = 3 * K;
+    double *mine = a.part + gw * S3;
+
+    bool zero[K], active[K];
+    double bnorm[K], rz[K], rel[K];
+    // ---- set-up: R = B, P = dinv R, ||B||^2, R'dinv R
+    double sb[K], sz[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        zero[k] = a.zero != nullptr && a.zero[sys * K + k] != 0;
+        sb[k] = sz[k] = 0.0;
+        rel[k] = 0.0;
+    }
+    for (int64_t r = r0 + lane; r < r1; r += 32) {
+        const double di = a.dinv[r];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double b = a.B[r * K + k];
+            const double res = zero[k] ? 0.0 : b;
+            a.X[r * K + k] = 0.0;
+            a.R[r * K + k] = res;
+            a.P[r * K + k] = res * di;
+            sb[k] += b * b;
+            sz[k] += res * res * di;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const double t1 = warp_sum(sb[k]), t2 = warp_sum(sz[k]);
+        if (lane == 0) { mine[k] = t1; mine[K + k] = t2; }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { a.flag[0] = 0; a.flag[1] = 0; }
+    if (!gb.sync()) return;
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const double bn = sqrt(system_sum(a.part, S3, k, w0, w1));
+        bnorm[k] = bn == 0.0 ? 1.0 : bn;
+        rz[k] = system_sum(a.part, S3, K + k, w0, w1);
+        active[k] = !zero[k];
+        any |= active[k];
+    }
+    int64_t done_at = any ? -1 : 0;
+    if (!gb.sync()) return;          // the set-up partials are read before phase A reuses them
+    int64_t it;
+    for (it = 1; it <= a.maxiter; it++) {
+        // ---- A: AP = S P for the warp's rows, p'Ap
+        double dot[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) dot[k] = 0.0;
+        {
+            constexpr int RPW = 32 / LPR;           // rows per warp step
+            const int sub = lane / LPR, sl = lane % LPR;
+            for (int64_t base = r0; base < r1; base += RPW) {
+                const int64_t r = base + sub;
+                double acc[K];
+#pragma unroll
+                for (int k = 0; k < K; k++) acc[k] = 0.0;
+                if (r < r1) {
+                    const int64_t e = a.indptr[r + 1];
+                    for (int64_t j = a.indptr[r] + sl; j < e; j += LPR) {
+                        const int32_t c = a.indices[j];
+                        const double v = a.data[j];
+                        if (c < 0 || c >= a.L) { gb.fail(HDFE_ERR_BAD_CODE); continue; }
+#pragma unroll
+                        for (int k = 0; k < K; k++) acc[k] += v * a.P[(int64_t)c * K + k];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < K; k++)
+#pragma unroll
+                    for (int o = LPR / 2; o > 0; o >>= 1)
+                        acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+                if (sl == 0 && r < r1) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        a.AP[r * K + k] = acc[k];
+                        dot[k] += acc[k] * a.P[r * K + k];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double t = warp_sum(dot[k]);
+            if (lane == 0) mine[k] = t;
+        }
+        if (!gb.sync()) return;
+        // the parity-(it + 1) flag was read by everyone before this barrier
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.flag[(it + 1) & 1] = 0;
+        double alpha[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double pap = system_sum(a.part, S3, k, w0, w1);
+            alpha[k] = (active[k] && pap > 0.0) ? rz[k] / pap : 0.0;
+        }
+        // ---- B: X += alpha P, R -= alpha AP; ||R||^2, R'dinv R
+        double sr[K], s2[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) sr[k] = s2[k] = 0.0;
+        for (int64_t r = r0 + lane; r < r1; r += 32) {
+            const double di = a.dinv[r];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                a.X[r * K + k] += alpha[k] * a.P[r * K + k];
+                const double res = a.R[r * K + k] - alpha[k] * a.AP[r * K + k];
+                a.R[r * K + k] = res;
+                sr[k] += res * res;
+                s2[k] += res * res * di;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double t1 = warp_sum(sr[k]), t2 = warp_sum(s2[k]);
+            if (lane == 0) { mine[K + k] = t1; mine[2 * K + k] = t2; }
+        }
+        if (!gb.sync()) return;
+        // ---- C: convergence, beta, P = dinv R + beta P
+        bool sys_active = false;
+        double beta[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double rr = system_sum(a.part, S3, K + k, w0, w1);
+            const double rzn = system_sum(a.part, S3, 2 * K + k, w0, w1);
+            rel[k] = sqrt(rr) / bnorm[k];
+            active[k] = rel[k] > a.tol;
+            sys_active |= active[k];
+            beta[k] = active[k] ? rzn / (rz[k] != 0.0 ? rz[k] : 1.0) : 0.0;
+            rz[k] = rzn;
+        }
+        if (!sys_active && done_at < 0) done_at = it;
+        if (sys_active) {
+            for (int64_t r = r0 + lane; r < r1; r += 32) {
+                const double di = a.dinv[r];
+#pragma unroll
+                for (int k = 0; k < K; k++)
+                    a.P[r * K + k] = a.R[r * K + k] * di + beta[k] * a.P[r * K + k];
+            }
+            if (lane == 0) atomicOr(a.flag + (it & 1), 1u);
+        }
+        if (!gb.sync()) return;
+        if (*(volatile unsigned *)(a.flag + (it & 1)) == 0) break;
+    }
+    if (gw == w0 && lane == 0) {
+        double mx = 0.0;
+        bool conv = true;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (zero[k]) continue;
+            mx = fmax(mx, rel[k]);
+            conv &= !active[k];
+        }
+        a.iterations[sys] = done_at >= 0 ? done_at : (it > a.maxiter ? a.maxiter : it);
+        a.converged[sys] = conv ? 1 : 0;
+        a.max_rel[sys] = mx;
+    }
+}
+
+template <int K, int LPR>
+int blocks_per_sm()
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_pcg<K, LPR>, kThreads, 0) !=
+        cudaSuccess)
+        return -1;
+    return per_sm;
+}
+
+template <int K>
+int per_sm_for(int lpr)
+{
+    switch (lpr) {
+    case 4: return blocks_per_sm<K, 4>();
+    case 8: return blocks_per_sm<K, 8>();
+    case 16: return blocks_per_sm<K, 16>();
+    case 32: return blocks_per_sm<K, 32>();
+    }
+    return -1;
+}
+
+int per_sm(int k, int lpr)
+{
+    switch (k) {
+    case 1: return per_sm_for<1>(lpr);
+    case 2: return per_sm_for<2>(lpr);
+    case 3: return per_sm_for<3>(lpr);
+    case 4: return per_sm_for<4>(lpr);
+    case 5: return per_sm_for<5>(lpr);
+    case 6: return per_sm_for<6>(lpr);
+    case 7: return per_sm_for<7>(lpr);
+    case 8: return per_sm_for<8>(lpr);
+    }
+    return -1;
+}
+
+template <int K, int LPR>
+cudaError_t launch(Args a, int blocks, cudaStream_t s)
+{
+    void *args[] = {&a};
+    return cudaLaunchCooperativeKernel((const void *)k_batch_pcg<K, LPR>, dim3(blocks),
+                                       dim3(kThreads), args, 0, s);
+}
+
+template <int K>
+cudaError_t launch_k(Args a, int lpr, int blocks, cudaStream_t s)
+{
+    switch (lpr) {
+    case 4: return launch<K, 4>(a, blocks, s);
+    case 8: return launch<K, 8>(a, blocks, s);
+    case 16: return launch<K, 16>(a, blocks, s);
+    default: return launch<K, 32>(a, blocks, s);
+    }
+}
+
+cudaError_t launch_any(Args a, int k, int lpr, int blocks, cudaStream_t s)
+{
+    switch (k) {
+    case 1: return launch_k<1>(a, lpr, blocks, s);
+    case 2: return launch_k<2>(a, lpr, blocks, s);
+    case 3: return launch_k<3>(a, lpr, blocks, s);
+    case 4: return launch_k<4>(a, lpr, blocks, s);
+    case 5: return launch_k<5>(a, lpr, blocks, s);
+    case 6: return launch_k<6>(a, lpr, blocks, s);
+    case 7: return launch_k<7>(a, lpr, blocks, s);
+    default: return launch_k<8>(a, lpr, blocks, s);
+    }
+}
+
+__global__ void k_status(const unsigned *bar, int32_t *status)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *status = (int32_t)bar[2];
+}
+
+}  // namespace batch
+}  // namespace hdfe
+
+using namespace hdfe;
+
+extern "C" int hdfe_batch_pcg_grid(int32_t k, int32_t lanes_per_row, int32_t *blocks,
+                                   int32_t *warps_per_block)
+{
+    if (k < 1 || k > batch::kMaxK || !(lanes_per_row == 4 || lanes_per_row == 8 ||
+                                       lanes_per_row == 16 || lanes_per_row == 32) ||
+        !blocks || !warps_per_block)
+        return hdfe_set_arg_error("hdfe_batch_pcg_grid: bad argument (k <= 8, lanes 4/8/16/32)");
+    int dev = 0, sms = 0;
+    HDFE_CUDA_TRY(cudaGetDevice(&dev));
+    HDFE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int per = batch::per_sm(k, lanes_per_row);
+    if (per < 1) return hdfe_set_error(HDFE_ERR_CUDA, "hdfe_batch_pcg_grid: no occupancy");
+    *blocks = sms * per;
+    *warps_per_block = batch::kWarps;
+    return HDFE_OK;
+}
+
+extern "C" int64_t hdfe_batch_pcg_workspace_bytes(int64_t L, int32_t k, int64_t warps)
+{
+    if (L < 1 || k < 1 || k > batch::kMaxK || warps < 1) return -1;
+    auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
+    return 3 * up(L * k * 8) + up(warps * 3 * k * 8) + 256;
+}
+
+extern "C" int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indices,
+                                    const double *data, int64_t L, const double *dinv,
+                                    const double *B, int32_t k, const uint8_t *zero,
+                                    int64_t n_systems, const int64_t *warp_rows,
+                                    const int32_t *warp_system, const int32_t *system_warps,
+                                    int32_t blocks, int32_t lanes_per_row, double tol,
+                                    int64_t maxiter, double *X, int64_t *iterations,
+                                    double *max_rel, int32_t *converged, int32_t *status,
+                                    void *workspace, int64_t workspace_bytes, void *stream)
+{
+    if (!indptr || !indices || !data || L < 1 || !dinv || !B || k < 1 || k > batch::kMaxK ||
+        n_systems < 1 || !warp_rows || !warp_system || !system_warps || blocks < 1 ||
+        !(lanes_per_row == 4 || lanes_per_row == 8 || lanes_per_row == 16 ||
+          lanes_per_row == 32) ||
+        !(tol > 0.0) || maxiter < 1 || !X || !iterations || !max_rel || !converged || !status ||
+        !workspace)
+        return hdfe_set_arg_error("hdfe_batch_pcg_solve: bad argument");
+    const int64_t warps = (int64_t)blocks * batch::kWarps;
+    if (workspace_bytes < hdfe_batch_pcg_workspace_bytes(L, k, warps))
+        return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_batch_pcg_solve: workspace too small");
+    int dev = 0, sms = 0;
+    HDFE_CUDA_TRY(cudaGetDevice(&dev));
+    HDFE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int per = batch::per_sm(k, lanes_per_row);
+    if (per < 1 || blocks > sms * per)
+        return hdfe_set_arg_error("hdfe_batch_pcg_solve: more blocks than can be resident");
+    cudaStream_t s = (cudaStream_t)stream;
+    auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
+    char *ws = (char *)workspace;
+    batch::Args a{};
+    a.indptr = indptr;
+    a.indices = indices;
+    a.data = data;
+    a.L = L;
+    a.dinv = dinv;
+    a.B = B;
+    a.zero = zero;
+    a.tol = tol;
+    a.maxiter = maxiter;
+    a.X = X;
+    a.R = (double *)ws;
+    a.P = (double *)(ws + up(L * k * 8));
+    a.AP = (double *)(ws + 2 * up(L * k * 8));
+    a.part = (double *)(ws + 3 * up(L * k * 8));
+    unsigned *words = (unsigned *)(ws + 3 * up(L * k * 8) + up(warps * 3 * k * 8));
+    a.bar = words;          // [0..2] barrier
+    a.flag = words + 4;     // [2]
+    a.wrow = warp_rows;
+    a.wsys = warp_system;
+    a.swarp = system_warps;
+    a.iterations = iterations;
+    a.max_rel = max_rel;
+    a.converged = converged;
+    HDFE_CUDA_TRY(cudaMemsetAsync(words, 0, 64, s));
+    HDFE_CUDA_TRY(batch::launch_any(a, k, lanes_per_row, blocks, s));
+    batch::k_status<<<1, 32, 0, s>>>(a.bar, status);
+    HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(2);
+    return HDFE_OK;
+}

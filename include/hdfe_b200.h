@@ -399,6 +399,36 @@ int hdfe_smooth_eval(const double *knots0, const double *knots1, const double *f
                      int32_t n_bins, const double *means, const double *leverage,
                      const double *b_ii, int64_t n_rows, double *out, void *stream);
 
+/* ------------------------------------------- many systems in one launch
+ *
+ * The Jacobi block PCG of core/solve.py:66-140 for many independent systems
+ * at once: their reduced matrices on the diagonal of one CSR matrix (L rows,
+ * each system's a contiguous range), B (L, k) and X (L, k) row-major, the
+ * zero flags (n_systems, k) uint8 or NULL.  The caller splits the rows over
+ * the grid's warps (hdfe_batch_pcg_grid gives blocks x warps_per_block):
+ * warp_rows (W + 1) int64 each warp's first row (a warp's rows inside one
+ * system), warp_system (W) int32, system_warps (n_systems + 1) int32 each
+ * system's first warp.  Per system: its own alpha / beta / active flags and
+ * relative residuals; iterations (n_systems) int64, max_rel (n_systems),
+ * converged (n_systems) int32 out; status (int32, DEVICE) HDFE_OK or
+ * HDFE_ERR_SPIN_LIMIT / HDFE_ERR_BAD_CODE.  lanes_per_row 4, 8, 16 or 32:
+ * the SpMV's lanes per matrix row.  One cooperative launch; no host reads.
+ * No reference counterpart: the reference fits one system at a time.
+ */
+int hdfe_batch_pcg_grid(int32_t k, int32_t lanes_per_row, int32_t *blocks,
+                        int32_t *warps_per_block);
+
+int64_t hdfe_batch_pcg_workspace_bytes(int64_t L, int32_t k, int64_t warps);
+
+int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *data,
+                         int64_t L, const double *dinv, const double *B, int32_t k,
+                         const uint8_t *zero, int64_t n_systems, const int64_t *warp_rows,
+                         const int32_t *warp_system, const int32_t *system_warps, int32_t blocks,
+                         int32_t lanes_per_row, double tol, int64_t maxiter, double *X,
+                         int64_t *iterations, double *max_rel, int32_t *converged,
+                         int32_t *status, void *workspace, int64_t workspace_bytes,
+                         void *stream);
+
 /* ------------------------------------------------------------ step 2: PCG
  *
  * Jacobi-preconditioned block conjugate gradients on the reduced matrix S,

@@ -1,0 +1,65 @@
+"""Many regressions in one launch (hdfe_stream_b200.batch): every system's
+fixed effects and iteration count against its own single fit, for each
+lanes-per-row choice, weighted and unweighted, with a zero right-hand side."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def systems(sizes, weights=False, seed=0):
+    from hdfe_stream_b200.simulate import pass0_layout, restrict_connected, simulate_panel
+    out = []
+    for i, n in enumerate(sizes):
+        p = simulate_panel(n, max(n // 10, 5), 10, spell=(4, 10), p_move=0.1, weights=weights,
+                           seed=seed + i)
+        out.append(pass0_layout(p, restrict_connected(p, (1, 1))))
+    return out
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("weights", [False, True])
+def test_batch_matches_single_fits(device, weights):
+    from hdfe_stream_b200 import batch, fit
+    sys_rows = systems([2_000, 500, 8_000, 1_200, 300, 20_000], weights, seed=11)
+    solver = batch.BatchSolver(batch.concat(sys_rows), tol=1e-12)
+    ref = []
+    for r in sys_rows:
+        res = fit.fit(fit.DeviceRows.from_rows(r), tol=1e-12)
+        ref.append((res.gamma.cpu().numpy(), int(np.max(np.atleast_1d(res.info["iterations"])))))
+    for lanes in batch.LANE_CHOICES:
+        X, info = solver.solve(lanes)
+        gammas = solver.gammas(solver.normalize(X))
+        assert info["converged"].all()
+        for i, (g, it) in enumerate(ref):
+            assert rel(gammas[i].cpu().numpy(), g) < 1e-9, (lanes, i)
+            assert abs(int(info["iterations"][i]) - it) <= 1, (lanes, i)
+
+
+def test_batch_tune_and_zero_column(device):
+    """The tuner picks one of the choices; a system whose outcome is
+    constant (a right-hand side of rounding noise) comes out with effects of
+    rounding size, as alone, and the others as alone."""
+    from hdfe_stream_b200 import batch, fit
+    sys_rows = systems([3_000, 900, 5_000], seed=21)
+    sys_rows[1].V[:, 0] = 1.5                 # y constant: spanned by the effects
+    gammas, info = batch.fit_batch(sys_rows, tol=1e-12, tune=True)
+    assert info["lanes"] in batch.LANE_CHOICES
+    for i, r in enumerate(sys_rows):
+        res = fit.fit(fit.DeviceRows.from_rows(r), tol=1e-12)
+        g = res.gamma.cpu().numpy()
+        assert rel(gammas[i].cpu().numpy(), g) < 1e-9
+    assert np.max(np.abs(gammas[1].cpu().numpy()[:, 0])) < 1e-9
