@@ -41,6 +41,7 @@ class Batch:
     row_ranges: list
     group_ranges: list
     level_ranges: list          # [system][dim] = (start within the dim, count)
+    raw_ss: np.ndarray          # (systems, m) sums of squared deviations of V
 
 
 def concat(systems) -> Batch:
@@ -53,7 +54,7 @@ def concat(systems) -> Batch:
         if r.codes.shape[1] != D or r.V.shape[1] != m or (r.w is not None) != weighted:
             raise ValueError("systems must share dimensions, variables and weighting")
     gcodes, codes, V, w = [], [], [], []
-    row_ranges, group_ranges, level_ranges = [], [], []
+    row_ranges, group_ranges, level_ranges, raw_ss = [], [], [], []
     g0, r0 = 0, 0
     l0 = [0] * D
     for r in systems:
@@ -66,6 +67,8 @@ def concat(systems) -> Batch:
             l0[d] += int(r.n_levels[d])
         codes.append(c)
         V.append(r.V)
+        raw_ss.append(((r.V - r.V.mean(axis=0)) ** 2).sum(axis=0) if r.n_rows
+                      else np.zeros(m))
         if weighted:
             w.append(r.w)
         row_ranges.append((r0, r.n_rows))
@@ -78,7 +81,7 @@ def concat(systems) -> Batch:
                 V=np.ascontiguousarray(np.concatenate(V)),
                 w=np.concatenate(w) if weighted else None, n_levels=list(l0), n_groups=g0,
                 names=list(systems[0].names))
-    return Batch(rows, row_ranges, group_ranges, level_ranges)
+    return Batch(rows, row_ranges, group_ranges, level_ranges, np.asarray(raw_ss))
 
 
 def split_rows(S, level_perm, sys_of_new, n_systems, blocks_warps):
@@ -129,27 +132,24 @@ class BatchSolver:
     """The block-diagonal system of a `Batch` after pass 1 and the S build,
     renumbered system by system, with its warp split for the batched PCG."""
 
-    def __init__(self, batch: Batch, tol=1e-10, maxiter=5000, lanes=None):
+    def __init__(self, batch: Batch, tol=1e-10, maxiter=5000, lanes=None, drows=None):
+        """drows: the batch's rows already on the device (`DeviceRows`), or
+        None to upload them here."""
         torch = _torch()
         self.batch = batch
         self.tol, self.maxiter = float(tol), int(maxiter)
         rows = batch.rows
-        self.drows = DeviceRows.from_rows(rows)
+        self.drows = DeviceRows.from_rows(rows) if drows is None else drows
         self.cells = pass1(self.drows)
         self.S = build_s(self.cells)
         dev = self.S.indptr.device
-        D = rows.codes.shape[1]
         offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1])).astype(np.int64)
         n = len(batch.level_ranges)
-        perm, sys_of = [], []
-        for i, lv in enumerate(batch.level_ranges):
-            start = len(perm)
-            for d in range(D):
-                s0, cnt = lv[d]
-                perm.extend(range(int(offs[d]) + s0, int(offs[d]) + s0 + cnt))
-            sys_of.extend([i] * (len(perm) - start))
-        self.perm = np.asarray(perm, np.int64)
-        self.sys_of = np.asarray(sys_of, np.int64)
+        perm = [np.arange(int(offs[d]) + s0, int(offs[d]) + s0 + cnt, dtype=np.int64)
+                for lv in batch.level_ranges for d, (s0, cnt) in enumerate(lv)]
+        self.perm = np.concatenate(perm) if perm else np.zeros(0, np.int64)
+        self.sys_of = np.repeat(np.arange(n, dtype=np.int64),
+                                [sum(cnt for _, cnt in lv) for lv in batch.level_ranges])
         L = len(self.perm)
         inv = np.empty(L, np.int64)
         inv[self.perm] = np.arange(L)
@@ -174,10 +174,8 @@ class BatchSolver:
         zero = np.zeros((n, self.m), np.uint8)
         bn = torch.zeros((n, self.m), dtype=torch.float64, device=dev).index_add_(
             0, torch.as_tensor(self.sys_of, device=dev), self.B * self.B).cpu().numpy()
-        for i, (r0, cnt) in enumerate(batch.row_ranges):
-            Vi = rows.V[r0:r0 + cnt]
-            raw = ((Vi - Vi.mean(axis=0)) ** 2).sum(axis=0) if cnt else np.zeros(self.m)
-            zero[i] = np.sqrt(bn[i]) <= RHS_ZERO_TOL * np.sqrt(np.maximum(raw, 0.0))
+        for i in range(n):
+            zero[i] = np.sqrt(bn[i]) <= RHS_ZERO_TOL * np.sqrt(np.maximum(batch.raw_ss[i], 0.0))
         self.zero = torch.as_tensor(zero.reshape(-1), device=dev)
         self.n = n
         self.lanes = lanes
