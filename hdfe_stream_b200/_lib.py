@@ -91,10 +91,10 @@ SIGNATURES = {
     "hdfe_smooth_cells": (_c.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
     "hdfe_smooth_eval": (_c.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_batch_pcg_grid": (_c.c_int, [_i32, _i32, _vp, _vp]),
-    "hdfe_batch_pcg_workspace_bytes": (_i64, [_i64, _i32, _i64]),
+    "hdfe_batch_pcg_workspace_bytes": (_i64, [_i64, _i32, _i64, _i64]),
     "hdfe_batch_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i32, _vp, _i64, _vp,
-                                        _vp, _vp, _i32, _i32, _f64, _i64, _vp, _vp, _vp, _vp,
-                                        _vp, _vp, _i64, _vp]),
+                                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i32, _i32,
+                                        _f64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_pcg_workspace_bytes": (_i64, [_i64, _i64, _i32]),
     "hdfe_pcg_solve": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _vp, _i32, _vp, _vp, _f64,
                                   _i64, _vp, _vp, _i64, _vp, _vp]),

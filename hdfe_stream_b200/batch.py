@@ -25,6 +25,7 @@ from .simulate import Rows
 
 LANE_CHOICES = (4, 8, 16, 32)
 ROW_COST = 32           # a row's fixed cost in the warp split, in nonzeros
+LONG_ROW = 1024         # rows with more nonzeros are cut into chunks of this size
 
 
 def _torch():
@@ -84,48 +85,69 @@ def concat(systems) -> Batch:
     return Batch(rows, row_ranges, group_ranges, level_ranges, np.asarray(raw_ss))
 
 
-def split_rows(S, level_perm, sys_of_new, n_systems, blocks_warps):
-    """Warp ranges: (warp_rows (W+1), warp_system (W), system_warps (n+1)).
-    Each system gets one warp and then warps in proportion to its cost
-    (nonzeros + ROW_COST per row, largest remainders); its rows are split
-    over them by cumulative cost."""
-    indptr = S.indptr.cpu().numpy()
-    rowlen = np.diff(indptr)[level_perm]
-    cost = rowlen + ROW_COST
-    W = int(blocks_warps)
+def split_work(indptr, sys_of_new, n_systems, W):
+    """The warps' work for the batched PCG, from the renumbered CSR's indptr
+    (host array): rows longer than LONG_ROW nonzeros are cut into chunks of
+    LONG_ROW; each system gets one warp and then warps in proportion to its
+    cost (largest remainders); the system's rows, then its chunks, are split
+    over its warps by cumulative cost (nonzeros + ROW_COST per row or chunk,
+    a long row counting ROW_COST for its vector work).  Returns a dict of the
+    arrays `hdfe_batch_pcg_solve` takes."""
+    indptr = np.asarray(indptr, np.int64)
+    L = len(indptr) - 1
+    rowlen = np.diff(indptr)
+    long_ = rowlen > LONG_ROW
+    nch = np.where(long_, (rowlen + LONG_ROW - 1) // LONG_ROW, 0)
+    C = int(nch.sum())
+    first = np.concatenate(([0], np.cumsum(nch)[:-1])).astype(np.int64)
+    chunk_row = np.repeat(np.arange(L, dtype=np.int64), nch)
+    j = np.arange(C, dtype=np.int64) - np.repeat(first, nch)
+    chunk_lo = indptr[chunk_row] + j * LONG_ROW
+    chunk_hi = np.minimum(chunk_lo + LONG_ROW, indptr[chunk_row + 1])
+    row_chunk = np.where(long_, first, -1).astype(np.int32)
+    row_cost = np.where(long_, 0, rowlen) + ROW_COST
+    chunk_cost = (chunk_hi - chunk_lo) + ROW_COST
     if n_systems > W:
         raise ValueError(f"{n_systems} systems need more than the grid's {W} warps")
-    bounds = np.searchsorted(sys_of_new, np.arange(n_systems + 1))     # row range per system
-    sys_cost = np.bincount(sys_of_new, weights=cost, minlength=n_systems)
+    rb = np.searchsorted(sys_of_new, np.arange(n_systems + 1))          # rows per system
+    cb = np.searchsorted(chunk_row, rb)                                  # chunks per system
+    sys_cost = (np.bincount(sys_of_new, weights=row_cost, minlength=n_systems)
+                + np.bincount(sys_of_new[chunk_row], weights=chunk_cost, minlength=n_systems))
     share = sys_cost / max(sys_cost.sum(), 1) * (W - n_systems)
     nw = 1 + np.floor(share).astype(np.int64)
-    spare = W - int(nw.sum())
     order = np.argsort(-(share - np.floor(share)), kind="stable")
-    for i in order[:spare]:
+    for i in order[:W - int(nw.sum())]:
         nw[i] += 1
     warp_rows = np.empty(W + 1, np.int64)
+    warp_chunks = np.empty(W + 1, np.int32)
     warp_sys = np.empty(W, np.int32)
     system_warps = np.zeros(n_systems + 1, np.int32)
     w = 0
     for i in range(n_systems):
-        a, b = int(bounds[i]), int(bounds[i + 1])
-        c = np.concatenate(([0], np.cumsum(cost[a:b])))
+        a, b, ca, cbb = int(rb[i]), int(rb[i + 1]), int(cb[i]), int(cb[i + 1])
+        cost = np.concatenate((row_cost[a:b], chunk_cost[ca:cbb]))
+        c = np.concatenate(([0], np.cumsum(cost)))
         targets = c[-1] * np.arange(nw[i]) / nw[i]
-        starts = a + np.searchsorted(c, targets, side="left")
-        starts = np.minimum(np.maximum.accumulate(starts), b)
+        t = np.searchsorted(c, targets, side="left")
+        t = np.minimum(np.maximum.accumulate(t), len(cost))
+        nrows = b - a
         system_warps[i] = w
-        for j in range(nw[i]):
-            warp_rows[w] = starts[j]
+        for k in range(nw[i]):
+            warp_rows[w] = a + min(int(t[k]), nrows)
+            warp_chunks[w] = ca + max(int(t[k]) - nrows, 0)
             warp_sys[w] = i
             w += 1
     system_warps[n_systems] = w
-    end = int(bounds[-1])
-    while w < W:                  # any warps left over own no rows
-        warp_rows[w] = end
+    while w < W:                  # any warps left over own no work
+        warp_rows[w] = L
+        warp_chunks[w] = C
         warp_sys[w] = n_systems - 1
         w += 1
-    warp_rows[W] = end
-    return warp_rows, warp_sys, system_warps
+    warp_rows[W] = L
+    warp_chunks[W] = C
+    return dict(warp_rows=warp_rows, warp_sys=warp_sys, system_warps=system_warps,
+                warp_chunks=warp_chunks, chunk_row=chunk_row.astype(np.int32),
+                chunk_lo=chunk_lo, chunk_hi=chunk_hi, row_chunk=row_chunk, n_chunks=C)
 
 
 class BatchSolver:
@@ -183,7 +205,7 @@ class BatchSolver:
         self.root, _ = components(self.cells, 0)
 
     def plan(self, lanes):
-        """Grid and warp split for a lanes-per-row choice."""
+        """Grid and work split for a lanes-per-row choice."""
         torch = _torch()
         if lanes not in self._plans:
             lib = _lib.lib()
@@ -192,14 +214,15 @@ class BatchSolver:
             _lib.check(lib.hdfe_batch_pcg_grid(self.m, lanes, _lib._c.byref(blocks),
                                                _lib._c.byref(wpb)))
             W = blocks.value * wpb.value
-            wr, ws, sw = split_rows(self.S, self.perm, self.sys_of, self.n, W)
+            work = split_work(self.indptr.cpu().numpy(), self.sys_of, self.n, W)
             dev = self.indptr.device
-            ws_bytes = int(lib.hdfe_batch_pcg_workspace_bytes(len(self.perm), self.m, W))
-            self._plans[lanes] = dict(
-                blocks=blocks.value, warp_rows=torch.as_tensor(wr, device=dev),
-                warp_sys=torch.as_tensor(ws, device=dev),
-                sys_warps=torch.as_tensor(sw, device=dev),
-                ws=torch.empty(ws_bytes, dtype=torch.uint8, device=dev))
+            ws_bytes = int(lib.hdfe_batch_pcg_workspace_bytes(len(self.perm), self.m, W,
+                                                              work["n_chunks"]))
+            plan = {k: torch.as_tensor(v, device=dev) for k, v in work.items()
+                    if k != "n_chunks"}
+            plan.update(blocks=blocks.value, n_chunks=work["n_chunks"],
+                        ws=torch.empty(ws_bytes, dtype=torch.uint8, device=dev))
+            self._plans[lanes] = plan
         return self._plans[lanes]
 
     def solve(self, lanes=None):
@@ -217,8 +240,10 @@ class BatchSolver:
         _lib.check(_lib.lib().hdfe_batch_pcg_solve(
             self.indptr.data_ptr(), self.indices.data_ptr(), self.data.data_ptr(), L,
             self.dinv.data_ptr(), self.B.data_ptr(), self.m, self.zero.data_ptr(), self.n,
-            p["warp_rows"].data_ptr(), p["warp_sys"].data_ptr(), p["sys_warps"].data_ptr(),
-            p["blocks"], lanes, self.tol, self.maxiter, X.data_ptr(), its.data_ptr(),
+            p["warp_rows"].data_ptr(), p["warp_sys"].data_ptr(), p["system_warps"].data_ptr(),
+            p["warp_chunks"].data_ptr(), p["chunk_row"].data_ptr(), p["chunk_lo"].data_ptr(),
+            p["chunk_hi"].data_ptr(), p["row_chunk"].data_ptr(), p["n_chunks"], p["blocks"],
+            lanes, self.tol, self.maxiter, X.data_ptr(), its.data_ptr(),
             rel.data_ptr(), conv.data_ptr(), status.data_ptr(), p["ws"].data_ptr(),
             p["ws"].numel(), _lib.stream_handle()))
         st = int(status.item())

@@ -7,15 +7,24 @@
 // Jacobi block PCG of core/solve.py:66-140 runs per system with its own
 // scalars: per (system, column) alpha, beta, the active flag and the relative
 // residual, exactly the algorithm of the single-system kernel (pcg.cu).  The
-// dot products are per-warp partials; after a grid barrier each warp sums its
-// system's partials (lanes over the system's warps, then a warp sum: a fixed
-// order, so every warp of a system holds the same scalars and the result does
-// not depend on scheduling).  The loop ends when no system has an active
+// dot products are summed per warp, then per CTA and system (a CTA's warps
+// cover at most kWarps systems) into a global slot; after a grid barrier one
+// warp per (CTA, system) sums that system's CTA slots (lanes over the CTAs,
+// then a warp sum) and shares the totals through shared memory.  The order is
+// fixed, so every warp of a system holds the same scalars and the result does
+// not depend on scheduling; each phase has its own slots, so a phase's
+// writes never meet the previous phase's reads.  The loop ends when no system has an active
 // column: a flag per iteration parity, set by the warps whose system is still
 // active and cleared two phases before its next use.
 //
 // The SpMV gives each row LPR lanes (4, 8, 16 or 32: the caller's tuner picks
 // it for the batch), LPR nonzeros in flight per row, reduced by shuffles.
+// Long rows (the small dimensions' levels, whose rows hold a nonzero per
+// level they meet) are cut by the host into chunks that any warps of the
+// system take, a whole warp per chunk: each chunk's partial sums go to its
+// own slot and its share of p'Ap is taken there, and the row's owner adds
+// the slots in chunk order when it needs the row of AP, so no row holds one
+// warp for long and the sums keep a fixed order.
 #include <climits>
 #include <cuda_runtime.h>
 
@@ -42,33 +51,80 @@ struct Args {
     const int64_t *wrow;        // (warps + 1) first row of each warp
     const int32_t *wsys;        // (warps) system of each warp
     const int32_t *swarp;       // (systems + 1) first warp of each system
-    double *part;               // (warps, 3, K)
+    const int32_t *wchunk;      // (warps + 1) first chunk of each warp
+    const int32_t *chunk_row;   // (chunks) row of each chunk
+    const int64_t *chunk_lo;    // (chunks) first nonzero of each chunk
+    const int64_t *chunk_hi;    // (chunks) one past its last
+    const int32_t *row_chunk;   // (L) a long row's first chunk, -1 for the others
+    double *cp;                 // (chunks, K) chunk partial sums
+    double *cpart;              // (blocks, kWarps, 5 K): per CTA and local system
     unsigned *flag;             // [2]
     unsigned *bar;
     int64_t *iterations;        // (systems)
     double *max_rel;            // (systems)
     int32_t *converged;         // (systems)
+    int64_t nwarps;
 };
 
-// sum of part[w][q] over the system's warps [w0, w1), fixed order
-__device__ __forceinline__ double system_sum(const double *part, int stride, int q, int w0, int w1)
+// Totals over each warp's system of N per-warp values v (already summed over
+// the warp, the same in every lane), through slots [q0, q0 + N) of cpart;
+// S the slots per entry.  One grid barrier.  Returns false when the kernel
+// must stop.
+template <int N, int S>
+__device__ __forceinline__ bool system_totals(const Args &a, const GridBarrier &gb, double (&v)[N],
+                                              int q0, double *s_w, double *s_sys, int first,
+                                              int nsys, int local)
 {
-    double t = 0.0;
-    for (int w = w0 + (int)(threadIdx.x & 31); w < w1; w += 32) t += part[(int64_t)w * stride + q];
-    return warp_sum(t);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < N; q++) s_w[warp * N + q] = v[q];
+    }
+    __syncthreads();
+    if (warp < nsys) {
+        for (int q = lane; q < N; q += 32) {
+            double t = 0.0;
+            for (int w = 0; w < kWarps; w++)
+                if (a.wsys[blockIdx.x * kWarps + w] == first + warp) t += s_w[w * N + q];
+            a.cpart[((int64_t)blockIdx.x * kWarps + warp) * S + q0 + q] = t;
+        }
+    }
+    if (!gb.sync()) return false;
+    if (warp < nsys) {
+        const int sys = first + warp;
+        const int bf = a.swarp[sys] / kWarps, bl = (a.swarp[sys + 1] - 1) / kWarps;
+#pragma unroll
+        for (int q = 0; q < N; q++) {
+            double t = 0.0;
+            for (int b = bf + lane; b <= bl; b += 32) {
+                const int j = sys - a.wsys[b * kWarps];
+                t += a.cpart[((int64_t)b * kWarps + j) * S + q0 + q];
+            }
+            t = warp_sum(t);
+            if (lane == 0) s_sys[warp * N + q] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < N; q++) v[q] = s_sys[local * N + q];
+    __syncthreads();
+    return true;
 }
 
 template <int K, int LPR>
 __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
 {
+    __shared__ double s_w[kWarps * 2 * K], s_sys[kWarps * 2 * K];
     GridBarrier gb{a.bar};
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
     const int64_t r0 = a.wrow[gw], r1 = a.wrow[gw + 1];
     const int sys = a.wsys[gw];
-    const int w0 = a.swarp[sys], w1 = a.swarp[sys + 1];
-    constexpr int S3 = 3 * K;
-    double *mine = a.part + gw * S3;
+    const int w0 = a.swarp[sys];
+    const int first = a.wsys[blockIdx.x * kWarps];
+    const int nsys = a.wsys[blockIdx.x * kWarps + kWarps - 1] - first + 1;
+    const int local = sys - first;
+    constexpr int S5 = 5 * K;       // slots: set-up 2K, phase A K, phase B 2K
 
     bool zero[K], active[K];
     double bnorm[K], rz[K], rel[K];
@@ -93,24 +149,25 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
             sz[k] += res * res * di;
         }
     }
+    {
+        double v[2 * K];
 #pragma unroll
-    for (int k = 0; k < K; k++) {
-        const double t1 = warp_sum(sb[k]), t2 = warp_sum(sz[k]);
-        if (lane == 0) { mine[k] = t1; mine[K + k] = t2; }
+        for (int k = 0; k < K; k++) { v[k] = warp_sum(sb[k]); v[K + k] = warp_sum(sz[k]); }
+        if (blockIdx.x == 0 && threadIdx.x == 0) { a.flag[0] = 0; a.flag[1] = 0; }
+        if (!system_totals<2 * K, S5>(a, gb, v, 0, s_w, s_sys, first, nsys, local)) return;
+#pragma unroll
+        for (int k = 0; k < K; k++) { sb[k] = v[k]; sz[k] = v[K + k]; }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) { a.flag[0] = 0; a.flag[1] = 0; }
-    if (!gb.sync()) return;
     bool any = false;
 #pragma unroll
     for (int k = 0; k < K; k++) {
-        const double bn = sqrt(system_sum(a.part, S3, k, w0, w1));
+        const double bn = sqrt(sb[k]);
         bnorm[k] = bn == 0.0 ? 1.0 : bn;
-        rz[k] = system_sum(a.part, S3, K + k, w0, w1);
+        rz[k] = sz[k];
         active[k] = !zero[k];
         any |= active[k];
     }
     int64_t done_at = any ? -1 : 0;
-    if (!gb.sync()) return;          // the set-up partials are read before phase A reuses them
     int64_t it;
     for (it = 1; it <= a.maxiter; it++) {
         // ---- A: AP = S P for the warp's rows, p'Ap
@@ -125,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
                 double acc[K];
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = 0.0;
-                if (r < r1) {
+                if (r < r1 && a.row_chunk[r] < 0) {
                     const int64_t e = a.indptr[r + 1];
                     for (int64_t j = a.indptr[r] + sl; j < e; j += LPR) {
                         const int32_t c = a.indices[j];
@@ -140,7 +197,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
 #pragma unroll
                     for (int o = LPR / 2; o > 0; o >>= 1)
                         acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-                if (sl == 0 && r < r1) {
+                if (sl == 0 && r < r1 && a.row_chunk[r] < 0) {
 #pragma unroll
                     for (int k = 0; k < K; k++) {
                         a.AP[r * K + k] = acc[k];
@@ -148,19 +205,40 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
                     }
                 }
             }
+            // the warp's chunks of long rows: partial sums and their p'Ap
+            const int c1 = a.wchunk[gw + 1];
+            for (int c = a.wchunk[gw]; c < c1; c++) {
+                const int64_t r = a.chunk_row[c];
+                const int64_t e = a.chunk_hi[c];
+                double acc[K];
+#pragma unroll
+                for (int k = 0; k < K; k++) acc[k] = 0.0;
+                for (int64_t j = a.chunk_lo[c] + lane; j < e; j += 32) {
+                    const int32_t col = a.indices[j];
+                    const double v = a.data[j];
+                    if (col < 0 || col >= a.L) { gb.fail(HDFE_ERR_BAD_CODE); continue; }
+#pragma unroll
+                    for (int k = 0; k < K; k++) acc[k] += v * a.P[(int64_t)col * K + k];
+                }
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const double t = warp_sum(acc[k]);
+                    if (lane == 0) {
+                        a.cp[(int64_t)c * K + k] = t;
+                        dot[k] += t * a.P[r * K + k];
+                    }
+                }
+            }
         }
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            const double t = warp_sum(dot[k]);
-            if (lane == 0) mine[k] = t;
-        }
-        if (!gb.sync()) return;
-        // the parity-(it + 1) flag was read by everyone before this barrier
+        for (int k = 0; k < K; k++) dot[k] = warp_sum(dot[k]);
+        if (!system_totals<K, S5>(a, gb, dot, 2 * K, s_w, s_sys, first, nsys, local)) return;
+        // the parity-(it + 1) flag was read by everyone before that barrier
         if (blockIdx.x == 0 && threadIdx.x == 0) a.flag[(it + 1) & 1] = 0;
         double alpha[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            const double pap = system_sum(a.part, S3, k, w0, w1);
+            const double pap = dot[k];
             alpha[k] = (active[k] && pap > 0.0) ? rz[k] / pap : 0.0;
         }
         // ---- B: X += alpha P, R -= alpha AP; ||R||^2, R'dinv R
@@ -169,28 +247,40 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
         for (int k = 0; k < K; k++) sr[k] = s2[k] = 0.0;
         for (int64_t r = r0 + lane; r < r1; r += 32) {
             const double di = a.dinv[r];
+            double ap[K];
+            const int32_t c0 = a.row_chunk[r];
+            if (c0 < 0) {
+#pragma unroll
+                for (int k = 0; k < K; k++) ap[k] = a.AP[r * K + k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < K; k++) ap[k] = 0.0;
+                for (int c = c0; a.chunk_row[c] == (int32_t)r; c++) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) ap[k] += a.cp[(int64_t)c * K + k];
+                    if (c + 1 >= a.wchunk[a.nwarps]) break;
+                }
+            }
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 a.X[r * K + k] += alpha[k] * a.P[r * K + k];
-                const double res = a.R[r * K + k] - alpha[k] * a.AP[r * K + k];
+                const double res = a.R[r * K + k] - alpha[k] * ap[k];
                 a.R[r * K + k] = res;
                 sr[k] += res * res;
                 s2[k] += res * res * di;
             }
         }
+        double v[2 * K];
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            const double t1 = warp_sum(sr[k]), t2 = warp_sum(s2[k]);
-            if (lane == 0) { mine[K + k] = t1; mine[2 * K + k] = t2; }
-        }
-        if (!gb.sync()) return;
+        for (int k = 0; k < K; k++) { v[k] = warp_sum(sr[k]); v[K + k] = warp_sum(s2[k]); }
+        if (!system_totals<2 * K, S5>(a, gb, v, 3 * K, s_w, s_sys, first, nsys, local)) return;
         // ---- C: convergence, beta, P = dinv R + beta P
         bool sys_active = false;
         double beta[K];
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            const double rr = system_sum(a.part, S3, K + k, w0, w1);
-            const double rzn = system_sum(a.part, S3, 2 * K + k, w0, w1);
+            const double rr = v[k];
+            const double rzn = v[K + k];
             rel[k] = sqrt(rr) / bnorm[k];
             active[k] = rel[k] > a.tol;
             sys_active |= active[k];
@@ -322,11 +412,12 @@ extern "C" int hdfe_batch_pcg_grid(int32_t k, int32_t lanes_per_row, int32_t *bl
     return HDFE_OK;
 }
 
-extern "C" int64_t hdfe_batch_pcg_workspace_bytes(int64_t L, int32_t k, int64_t warps)
+extern "C" int64_t hdfe_batch_pcg_workspace_bytes(int64_t L, int32_t k, int64_t warps,
+                                                  int64_t n_chunks)
 {
-    if (L < 1 || k < 1 || k > batch::kMaxK || warps < 1) return -1;
+    if (L < 1 || k < 1 || k > batch::kMaxK || warps < 1 || n_chunks < 0) return -1;
     auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
-    return 3 * up(L * k * 8) + up(warps * 3 * k * 8) + 256;
+    return 3 * up(L * k * 8) + up(warps * 5 * k * 8) + up((n_chunks + 1) * k * 8) + 256;
 }
 
 extern "C" int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indices,
@@ -334,20 +425,26 @@ extern "C" int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indice
                                     const double *B, int32_t k, const uint8_t *zero,
                                     int64_t n_systems, const int64_t *warp_rows,
                                     const int32_t *warp_system, const int32_t *system_warps,
-                                    int32_t blocks, int32_t lanes_per_row, double tol,
+                                    const int32_t *warp_chunks, const int32_t *chunk_row,
+                                    const int64_t *chunk_lo, const int64_t *chunk_hi,
+                                    const int32_t *row_chunk,
+                                    int64_t n_chunks, int32_t blocks, int32_t lanes_per_row,
+                                    double tol,
                                     int64_t maxiter, double *X, int64_t *iterations,
                                     double *max_rel, int32_t *converged, int32_t *status,
                                     void *workspace, int64_t workspace_bytes, void *stream)
 {
     if (!indptr || !indices || !data || L < 1 || !dinv || !B || k < 1 || k > batch::kMaxK ||
-        n_systems < 1 || !warp_rows || !warp_system || !system_warps || blocks < 1 ||
+        n_systems < 1 || !warp_rows || !warp_system || !system_warps || !warp_chunks ||
+        !row_chunk || n_chunks < 0 || (n_chunks > 0 && (!chunk_row || !chunk_lo || !chunk_hi)) ||
+        blocks < 1 ||
         !(lanes_per_row == 4 || lanes_per_row == 8 || lanes_per_row == 16 ||
           lanes_per_row == 32) ||
         !(tol > 0.0) || maxiter < 1 || !X || !iterations || !max_rel || !converged || !status ||
         !workspace)
         return hdfe_set_arg_error("hdfe_batch_pcg_solve: bad argument");
     const int64_t warps = (int64_t)blocks * batch::kWarps;
-    if (workspace_bytes < hdfe_batch_pcg_workspace_bytes(L, k, warps))
+    if (workspace_bytes < hdfe_batch_pcg_workspace_bytes(L, k, warps, n_chunks))
         return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_batch_pcg_solve: workspace too small");
     int dev = 0, sms = 0;
     HDFE_CUDA_TRY(cudaGetDevice(&dev));
@@ -372,13 +469,21 @@ extern "C" int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indice
     a.R = (double *)ws;
     a.P = (double *)(ws + up(L * k * 8));
     a.AP = (double *)(ws + 2 * up(L * k * 8));
-    a.part = (double *)(ws + 3 * up(L * k * 8));
-    unsigned *words = (unsigned *)(ws + 3 * up(L * k * 8) + up(warps * 3 * k * 8));
+    a.cpart = (double *)(ws + 3 * up(L * k * 8));
+    a.cp = (double *)(ws + 3 * up(L * k * 8) + up(warps * 5 * k * 8));
+    unsigned *words = (unsigned *)(ws + 3 * up(L * k * 8) + up(warps * 5 * k * 8) +
+                                   up((n_chunks + 1) * k * 8));
     a.bar = words;          // [0..2] barrier
     a.flag = words + 4;     // [2]
     a.wrow = warp_rows;
     a.wsys = warp_system;
     a.swarp = system_warps;
+    a.wchunk = warp_chunks;
+    a.chunk_row = chunk_row;
+    a.chunk_lo = chunk_lo;
+    a.chunk_hi = chunk_hi;
+    a.row_chunk = row_chunk;
+    a.nwarps = warps;
     a.iterations = iterations;
     a.max_rel = max_rel;
     a.converged = converged;

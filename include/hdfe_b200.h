@@ -408,7 +408,11 @@ int hdfe_smooth_eval(const double *knots0, const double *knots1, const double *f
  * the grid's warps (hdfe_batch_pcg_grid gives blocks x warps_per_block):
  * warp_rows (W + 1) int64 each warp's first row (a warp's rows inside one
  * system), warp_system (W) int32, system_warps (n_systems + 1) int32 each
- * system's first warp.  Per system: its own alpha / beta / active flags and
+ * system's first warp.  Long rows are cut into n_chunks chunks of nonzeros
+ * (chunk_row (n_chunks) int32, chunk_lo / chunk_hi (n_chunks) int64, in row
+ * order; row_chunk (L) int32 a long row's first chunk, -1 for the others)
+ * taken by warps of their system: warp_chunks (W + 1) int32 each warp's
+ * first chunk, warp_chunks[W] = n_chunks.  Per system: its own alpha / beta / active flags and
  * relative residuals; iterations (n_systems) int64, max_rel (n_systems),
  * converged (n_systems) int32 out; status (int32, DEVICE) HDFE_OK or
  * HDFE_ERR_SPIN_LIMIT / HDFE_ERR_BAD_CODE.  lanes_per_row 4, 8, 16 or 32:
@@ -418,12 +422,15 @@ int hdfe_smooth_eval(const double *knots0, const double *knots1, const double *f
 int hdfe_batch_pcg_grid(int32_t k, int32_t lanes_per_row, int32_t *blocks,
                         int32_t *warps_per_block);
 
-int64_t hdfe_batch_pcg_workspace_bytes(int64_t L, int32_t k, int64_t warps);
+int64_t hdfe_batch_pcg_workspace_bytes(int64_t L, int32_t k, int64_t warps, int64_t n_chunks);
 
 int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *data,
                          int64_t L, const double *dinv, const double *B, int32_t k,
                          const uint8_t *zero, int64_t n_systems, const int64_t *warp_rows,
-                         const int32_t *warp_system, const int32_t *system_warps, int32_t blocks,
+                         const int32_t *warp_system, const int32_t *system_warps,
+                         const int32_t *warp_chunks, const int32_t *chunk_row,
+                         const int64_t *chunk_lo, const int64_t *chunk_hi,
+                         const int32_t *row_chunk, int64_t n_chunks, int32_t blocks,
                          int32_t lanes_per_row, double tol, int64_t maxiter, double *X,
                          int64_t *iterations, double *max_rel, int32_t *converged,
                          int32_t *status, void *workspace, int64_t workspace_bytes,
