@@ -460,8 +460,9 @@ def run_batched(args, rank):
     solver, gammas, info = batched_fit()
     ev[1].record()
     torch.cuda.synchronize()
-    for r in singles[:2]:                           # warm-up
+    for r in singles:                               # warm-up (allocator, occupancy)
         fit.fit(r, tol=args.tol)
+    torch.cuda.synchronize()
     ev[2].record()
     ref = [fit.fit(r, tol=args.tol).gamma for r in singles]
     ev[3].record()
