@@ -127,6 +127,10 @@ __device__ __forceinline__ int64_t warp_of(const Params &a, int64_t e)
 // of short rows take fewer nonzeros than warps inside long rows.
 // The lane kernel's nonzeros are heavy (K-wide gathers), so its rows cost
 // their nonzeros alone.
+#ifndef HDFE_PCG_UNROLL
+#define HDFE_PCG_UNROLL 6               // nonzeros per lane in flight (k = 3, 4)
+#endif
+
 #ifndef HDFE_PCG_ROW_COST
 #define HDFE_PCG_ROW_COST 32
 #endif
@@ -238,7 +242,7 @@ template <int K, int VS, int VW, int STEP, typename T>
 __device__ __forceinline__ void row_products(const Params &a, const T *vals, const T *V,
                                              int64_t e0, int64_t re, T (&acc)[K])
 {
-    constexpr int U = K <= 4 ? 4 : 2;
+    constexpr int U = K <= 2 ? 4 : (K <= 4 ? HDFE_PCG_UNROLL : 2);
     for (; e0 < re; e0 += STEP * U) {
         int64_t c[U];
         T d[U];
