@@ -154,6 +154,90 @@ __global__ void __launch_bounds__(kThreads) k_effects(Args a, int psi, const dou
     cta_sums(acc, 7, s_part, part);
 }
 
+// The sums of the variances of beta (core/inference.py:566-578, OLS with
+// analytic weights): with h the residualised covariates (x less Gamma_x's
+// projection and its weighted group mean) and e the residuals (the y
+// equation's, as k_effects), per CTA: the bread sum w h h', the meat sum
+// (w e)^2 h h', the streamed groups' meat sum_g s_g s_g' (s_g the group's
+// sum of w e h) -- each as its upper triangle, row by row -- and sum w e^2.
+template <int M>
+__global__ void __launch_bounds__(kThreads) k_variance(Args a, const double *Gamma,
+                                                       const double *beta, double *part)
+{
+    constexpr int KX = M - 1;
+    constexpr int T = KX * (KX + 1) / 2;
+    constexpr int NQ = 3 * T + 1;
+    __shared__ double s_part[(kThreads / 32) * NQ];
+    double acc[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) acc[q] = 0.0;
+    double b[KX];
+#pragma unroll
+    for (int j = 0; j < KX; j++) b[j] = beta[j];
+    for (int64_t g = (int64_t)blockIdx.x * kThreads + threadIdx.x; g < a.G;
+         g += (int64_t)gridDim.x * kThreads) {
+        const int64_t s = a.starts[g], e = a.starts[g + 1];
+        // row i's y and covariates less their fixed-effect projections
+        auto raw = [&](int64_t i, double &yr, double (&hr)[KX]) {
+            yr = a.V[i];
+#pragma unroll
+            for (int j = 0; j < KX; j++) hr[j] = a.V[(int64_t)(j + 1) * a.N + i];
+            for (int d = 0; d < a.D; d++) {
+                const int64_t l = level(a, i, d);
+                yr -= Gamma[l * M];
+#pragma unroll
+                for (int j = 0; j < KX; j++) hr[j] -= Gamma[l * M + j + 1];
+            }
+        };
+        double Wg = 0.0, mu = 0.0, mh[KX];
+#pragma unroll
+        for (int j = 0; j < KX; j++) mh[j] = 0.0;
+        for (int64_t i = s; i < e; i++) {
+            const double wi = a.w ? a.w[i] : 1.0;
+            double yr, hr[KX];
+            raw(i, yr, hr);
+            double u = yr;
+#pragma unroll
+            for (int j = 0; j < KX; j++) { u -= b[j] * hr[j]; mh[j] += wi * hr[j]; }
+            Wg += wi;
+            mu += wi * u;
+        }
+        const double inv = Wg > 0.0 ? 1.0 / Wg : 0.0;
+        mu *= inv;
+#pragma unroll
+        for (int j = 0; j < KX; j++) mh[j] *= inv;
+        double sg[KX];
+#pragma unroll
+        for (int j = 0; j < KX; j++) sg[j] = 0.0;
+        for (int64_t i = s; i < e; i++) {
+            const double wi = a.w ? a.w[i] : 1.0;
+            double yr, h[KX];
+            raw(i, yr, h);
+            double u = yr;
+#pragma unroll
+            for (int j = 0; j < KX; j++) { u -= b[j] * h[j]; h[j] -= mh[j]; }
+            const double ei = u - mu, we = wi * ei;
+            int t = 0;
+#pragma unroll
+            for (int j1 = 0; j1 < KX; j1++)
+#pragma unroll
+                for (int j2 = j1; j2 < KX; j2++, t++) {
+                    acc[t] += wi * h[j1] * h[j2];
+                    acc[T + t] += we * we * h[j1] * h[j2];
+                }
+#pragma unroll
+            for (int j = 0; j < KX; j++) sg[j] += we * h[j];
+            acc[3 * T] += wi * ei * ei;
+        }
+        int t = 0;
+#pragma unroll
+        for (int j1 = 0; j1 < KX; j1++)
+#pragma unroll
+            for (int j2 = j1; j2 < KX; j2++, t++) acc[2 * T + t] += sg[j1] * sg[j2];
+    }
+    cta_sums(acc, NQ, s_part, part);
+}
+
 // out[q] = sum over CTAs of part[., q], one warp per entry, fixed order
 __global__ void __launch_bounds__(kThreads) k_sum_parts(const double *part, int blocks, int n,
                                                         double *out)
@@ -306,5 +390,49 @@ extern "C" int hdfe_kss_sigma2(const double *y, const double *w, const double *r
         y, w, resid, complement, factor, ybar, n_rows, out);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
+    return HDFE_OK;
+}
+
+extern "C" int64_t hdfe_variance_sums_workspace_bytes(int32_t m)
+{
+    if (m < 2 || m > assemble::kMaxM) return -1;
+    const int kx = m - 1, nq = 3 * kx * (kx + 1) / 2 + 1;
+    return (int64_t)assemble::kGrid * nq * 8;
+}
+
+extern "C" int hdfe_variance_sums(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                                  int32_t D, const int64_t *n_levels, const double *w,
+                                  const double *V, int32_t m, int64_t n_rows,
+                                  const double *Gamma, const double *beta, double *out,
+                                  void *workspace, int64_t workspace_bytes, void *status,
+                                  void *stream)
+{
+    assemble::Args a;
+    int st = assemble::fill(a, starts, n_groups, codes, D, n_levels, w, V, m, n_rows,
+                            (unsigned *)status);
+    if (st != HDFE_OK) return st;
+    if (m < 2 || !Gamma || !beta || !out || !workspace ||
+        workspace_bytes < hdfe_variance_sums_workspace_bytes(m))
+        return hdfe_set_arg_error("hdfe_variance_sums: bad argument (2 <= m <= 8)");
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned grid = assemble::grid_for(n_groups);
+    double *part = (double *)workspace;
+    const int kx = m - 1, nq = 3 * kx * (kx + 1) / 2 + 1;
+#define HDFE_VARIANCE(M) assemble::k_variance<M><<<grid, assemble::kThreads, 0, s>>>( \
+        a, Gamma, beta, part)
+    switch (m) {
+    case 2: HDFE_VARIANCE(2); break;
+    case 3: HDFE_VARIANCE(3); break;
+    case 4: HDFE_VARIANCE(4); break;
+    case 5: HDFE_VARIANCE(5); break;
+    case 6: HDFE_VARIANCE(6); break;
+    case 7: HDFE_VARIANCE(7); break;
+    default: HDFE_VARIANCE(8); break;
+    }
+#undef HDFE_VARIANCE
+    assemble::k_sum_parts<<<(unsigned)((nq * 32 + assemble::kThreads - 1) / assemble::kThreads),
+                            assemble::kThreads, 0, s>>>(part, (int)grid, nq, out);
+    HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(2);
     return HDFE_OK;
 }

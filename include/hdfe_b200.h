@@ -340,6 +340,20 @@ int hdfe_row_effects(const int64_t *starts, int64_t n_groups, const uint32_t *co
                      const double *gam_y, double *resid, double *alpha, double *sums,
                      void *workspace, int64_t workspace_bytes, void *status, void *stream);
 
+/* hdfe_variance_sums: the row pass's sums for the variances of beta,
+ * core/kernels_base.py:544-615 `_nb_pass2` with core/inference.py:566-578
+ * (OLS, analytic weights): for h the covariates V[1:] less their Gamma
+ * projections and weighted group means and e the y equation's residuals,
+ * out[3 T + 1] (T = k (k + 1) / 2, k = m - 1; upper triangles row by row) =
+ * sum w h h', sum (w e)^2 h h', sum over the streamed groups of s s' with s
+ * the group's sum of w e h, then sum w e^2.  Deterministic.  2 <= m <= 8. */
+int64_t hdfe_variance_sums_workspace_bytes(int32_t m);
+
+int hdfe_variance_sums(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                       const int64_t *n_levels, const double *w, const double *V, int32_t m,
+                       int64_t n_rows, const double *Gamma, const double *beta, double *out,
+                       void *workspace, int64_t workspace_bytes, void *status, void *stream);
+
 int hdfe_kss_sigma2(const double *y, const double *w, const double *resid,
                     const double *complement, const double *factor, double ybar,
                     int64_t n_rows, double *out, void *stream);

@@ -626,6 +626,47 @@ def row_effects(starts, codes, offs, w, V, Gamma, beta):
     return e, alpha, gam_y[offs[0] + codes[:, 0]], gam_y
 
 
+def variance_sums(starts, codes, offs, w, V, Gamma, beta):
+    """core/kernels_base.py:544-615 `_nb_pass2` with the sums
+    core/inference.py:566-578 takes of its output (OLS, analytic weights):
+    (bread sum w h h', meat sum (w e)^2 h h', meat of the streamed groups'
+    scores sum_g s_g s_g' with s_g the group's sum of w e h, rss), h the
+    residualised covariates."""
+    codes = np.asarray(codes, dtype=np.int64)
+    X = np.asarray(V[:, 1:], dtype=np.float64)
+    H = X.copy()
+    for d in range(codes.shape[1]):
+        H -= Gamma[offs[d] + codes[:, d], 1:]
+    Wg = np.add.reduceat(w, starts[:-1])
+    mh = np.add.reduceat(w[:, None] * H, starts[:-1], axis=0) / Wg[:, None]
+    H -= np.repeat(mh, np.diff(starts), axis=0)
+    e, _, _, _ = row_effects(starts, codes, offs, w, V, Gamma, beta)
+    sw = np.sqrt(w)
+    B = (H * sw[:, None]).T @ (H * sw[:, None])
+    he = H * (w * e)[:, None]
+    sg = np.add.reduceat(he, starts[:-1], axis=0)
+    return B, he.T @ he, sg.T @ sg, float(w @ (e * e))
+
+
+def variances(B, meat_hc, meat_g, rss, n_obs, n_groups, n_levels, pair_components):
+    """The iid, HC1 and CRV1 (clustered on the streamed dimension) variances
+    of beta: core/inference.py:886-912 (pyfixest's small-sample factors) with
+    core/estimator.py:446-464 `_k_fe` (fe_dof "exact": the fixed-effect
+    parameters less the largest pair's components and one per further
+    dimension; the streamed dimension's levels nested in its own clusters,
+    so CRV1 counts one parameter for them)."""
+    k = B.shape[0]
+    G, N = int(n_groups), float(n_obs)
+    k_fe = G + int(sum(n_levels)) - (max(pair_components) + len(n_levels) - 1)
+    K = k + k_fe
+    Binv = np.linalg.inv(B)
+    Kc = k + k_fe - G + 1
+    adj = G / (G - 1) * (N - 1) / (N - Kc)
+    return {"iid": rss / (N - K) * Binv, "hetero": N / (N - K) * Binv @ meat_hc @ Binv,
+            "CRV1": adj * Binv @ meat_g @ Binv, "k_fe": k_fe, "df_resid": N - K,
+            "df_cluster": G - 1}
+
+
 # ------------------------------------------------ KSS standard-error pieces
 
 def readout(starts, codes, offs, X, U_l, U_c, U_g):

@@ -11,8 +11,15 @@ reference's normalised Gamma), it runs core/kernels_base.py
 `_assemble` does, solves for beta as :874 does (A[xk, xk] \\ A[xk, y]), and
 runs `_nb_pass2` (:544) with gam_y = Gamma_y - Gamma_x beta (:454-456) for the
 residuals and the streamed effect; the non-streamed effect per row is
-gam_y[level] (:615).  Outputs go to tests/golden/assemble.npz.  Nothing at
-test time reads the reference.
+gam_y[level] (:615).  With the kernel's group scores (sum over a group of
+w e z~) it forms the pass's sums as core/inference.py:566-578 does -- the
+bread sum w h h', the heteroskedastic meat sum (w e)^2 h h', the meat of
+scores clustered on the streamed dimension, the residual sum of squares --
+and the iid, HC1 and CRV1(streamed dimension) variances with the small-sample
+factors of :886-912 and the fixed-effect parameter count of
+core/estimator.py:446-464 (fe_dof "exact"; the streamed dimension's levels
+nested in its own clusters).  Outputs go to tests/golden/assemble.npz.
+Nothing at test time reads the reference.
 """
 
 from __future__ import annotations
@@ -62,9 +69,38 @@ def main(root):
         zt = np.empty((N, len(xk)))
         g_eff = np.empty(G)
         acc_s = np.zeros((4, 4))
+        k = len(xk)
+        sg = np.empty((G, k))
         kb._nb_pass2(starts, codes, offs, w, y, X, beta, gam_y, gam_y0, X,
                      np.ascontiguousarray(gam_x), float(g["means"][yj]), True, g_eff, e, zt,
-                     np.empty((0, len(xk))), acc_s)
+                     sg, acc_s)
+        # inference.py:566-578 (analytic weights, OLS: h = z~)
+        sw = np.sqrt(w)
+        B = (zt * sw[:, None]).T @ (zt * sw[:, None])
+        he = zt * (w * e)[:, None]
+        meat_hc = he.T @ he
+        meat_g = sg.T @ sg
+        rss = float(acc_s[:, 0].sum())
+        # estimator.py:446-464: fixed-effect parameters net of the redundant
+        n_o = len(nlev)
+        fe_params = [G] + [int(x) for x in nlev]
+        comps = max(int(x) for x in g["pair_components"])
+        k_fe = sum(fe_params) - (comps + n_o - 1)
+        K = k + k_fe
+        Binv = np.linalg.inv(B)
+        V_iid = rss / (N - K) * Binv
+        V_hc1 = N / (N - K) * Binv @ meat_hc @ Binv
+        Kc = k + k_fe - G + 1
+        adj = G / (G - 1) * (N - 1) / (N - Kc)
+        V_crv1 = adj * Binv @ meat_g @ Binv
+        out[f"{name}_B"] = B
+        out[f"{name}_meat_hc"] = meat_hc
+        out[f"{name}_meat_g"] = meat_g
+        out[f"{name}_rss"] = np.array([rss])
+        out[f"{name}_k_fe"] = np.array([k_fe])
+        out[f"{name}_V_iid"] = V_iid
+        out[f"{name}_V_hc1"] = V_hc1
+        out[f"{name}_V_crv1"] = V_crv1
         out[f"{name}_A"] = A
         out[f"{name}_beta"] = beta
         out[f"{name}_gam_y"] = gam_y

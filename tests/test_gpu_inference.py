@@ -1,0 +1,69 @@
+"""beta and its variances on the device (hdfe_stream_b200.inference): the
+iid, HC1 and CRV1 (streamed dimension) variances, the fixed-effect parameter
+count and the pairs' components against the reference's `_nb_pass2` sums and
+`_estimate` formulas (tests/golden/assemble.npz) and against the oracle on a
+device fit."""
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from conftest import GOLDEN_PANELS, golden_rows, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_variances_match_reference(device, name):
+    import torch
+    from hdfe_stream_b200 import fit, inference
+    g = load_golden(name)
+    a = load_golden("assemble")
+    drows = fit.DeviceRows.from_rows(golden_rows(g))
+    cells = fit.pass1(drows)
+    out = inference.estimate(drows, cells, torch.as_tensor(g["gamma"]))
+    assert rel(out["beta"], a[f"{name}_beta"]) < 1e-10
+    assert sorted(out["pair_components"]) == sorted(int(x) for x in g["pair_components"])
+    assert out["k_fe"] == int(a[f"{name}_k_fe"][0])
+    for key, ref in (("iid", "V_iid"), ("hetero", "V_hc1"), ("CRV1", "V_crv1")):
+        assert rel(out["vcov"][key], a[f"{name}_{ref}"]) < 1e-9, key
+
+
+def test_variances_on_a_device_fit(device):
+    """A 60k-worker weighted panel fitted on the device: the variances from
+    its own Gamma against the oracle's on the same Gamma."""
+    from hdfe_stream_b200 import fit, inference
+    from hdfe_stream_b200.simulate import pass0_layout, restrict_connected, simulate_panel
+    panel = simulate_panel(60_000, 6_000, 10, spell=(3, 10), p_move=0.1, weights=True, seed=4)
+    rows = pass0_layout(panel, restrict_connected(panel, (1, 1)))
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    out = inference.estimate(drows, res.cells, res.gamma)
+    gamma = res.gamma.cpu().numpy()
+    starts = orc.row_starts(rows.gcode)
+    offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1])).astype(np.int64)
+    A = orc.residual_moments(starts, rows.codes, offs, rows.w, rows.V, gamma)
+    beta = np.linalg.solve(A[1:, 1:], A[1:, 0])
+    assert rel(out["beta"], beta) < 1e-10
+    c = orc.pass1(rows)
+    pcs = [c.pair_components[(0, 1)], orc.component_labels(c)[1],
+           int(np.count_nonzero(orc.components(c, 1) == np.arange(rows.n_levels[1])))]
+    assert sorted(out["pair_components"]) == sorted(pcs)
+    v = orc.variances(*orc.variance_sums(starts, rows.codes, offs, rows.w, rows.V, gamma, beta),
+                      rows.n_rows, rows.n_groups, rows.n_levels, pcs)
+    assert out["k_fe"] == v["k_fe"]
+    for key in ("iid", "hetero", "CRV1"):
+        assert rel(out["vcov"][key], v[key]) < 1e-9, key

@@ -261,3 +261,24 @@ def test_jla_components_against_exact_prototype():
     assert np.all(np.abs(out["leave_out"] - g["kss"]) <= 0.05 * np.abs(g["bias"]))
     lev, _, _ = des.jla_leverages(1024, 32, 3)
     assert np.mean(np.abs(lev - g["P_ii"])) < 0.02
+
+
+def test_variances_match_reference(golden):
+    """The pass-2 sums (bread, heteroskedastic meat, the streamed groups'
+    clustered meat, rss) against the reference's `_nb_pass2` and
+    core/inference.py's sums, and the iid / HC1 / CRV1 variances."""
+    name, g = golden
+    a = load_golden("assemble")
+    rows = golden_rows(g)
+    starts = orc.row_starts(rows.gcode)
+    offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1])).astype(np.int64)
+    w = rows.w if rows.w is not None else np.ones(rows.n_rows)
+    B, mhc, mg, rss = orc.variance_sums(starts, rows.codes, offs, w, rows.V, g["gamma"],
+                                        a[f"{name}_beta"])
+    for got, key in ((B, "B"), (mhc, "meat_hc"), (mg, "meat_g"), (rss, "rss")):
+        assert rel(got, a[f"{name}_{key}"]) < 1e-10, key
+    v = orc.variances(B, mhc, mg, rss, rows.n_rows, rows.n_groups, rows.n_levels,
+                      [int(x) for x in g["pair_components"]])
+    assert v["k_fe"] == int(a[f"{name}_k_fe"][0])
+    for key, ref in (("iid", "V_iid"), ("hetero", "V_hc1"), ("CRV1", "V_crv1")):
+        assert rel(v[key], a[f"{name}_{ref}"]) < 1e-9, key
