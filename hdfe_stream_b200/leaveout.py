@@ -222,7 +222,8 @@ class InverseOperator:
             res = res + ((v[0], v[1][:self.c], v[2]),)
         return res
 
-    def hutchinson_trace(self, sigma2, n_draws=250, block=MAX_BLOCK, seed=0, psi_column=0):
+    def hutchinson_trace(self, sigma2, n_draws=250, block=MAX_BLOCK, seed=0, psi_column=0,
+                         person_years=None):
         """leaveout.py:321-391 `hutchinson_trace` and :393-448 `_trace_block`:
         the bias terms (var(psi), var(alpha), cov(psi, alpha)) from n_draws
         Rademacher vectors in coefficient space, two applications of the
@@ -265,7 +266,7 @@ class InverseOperator:
         var_alpha = b1b2 / weight - (b1 / weight) * (b2 / weight)
         cov = 0.5 * (cross / weight - (a1 / weight) * (b2 / weight) - (b1 / weight) * (a2 / weight))
         # leaveout_se.py:202-214 `_moment_divisor`: n - 1 person-years
-        R = float(self.N)
+        R = float(self.N if person_years is None else person_years)
         scale = weight / (weight * (R - 1.0) / R) if R > 1 else 1.0
         self.trace_info = {"blocks": blocks, "n_obs": float(weight)}
         return np.array([scale * var_psi, scale * var_alpha, scale * cov])

@@ -667,6 +667,71 @@ def variances(B, meat_hc, meat_g, rss, n_obs, n_groups, n_levels, pair_component
             "df_cluster": G - 1}
 
 
+def leave_out_match(rows, n_draws, block, seed, tol=1e-12):
+    """leaveout_match.py:156-214 `leave_out_match`, point estimates: the
+    row-level fit's partialled outcome y~ = fe_alpha + fe_psi + resid
+    (:76-77), collapsed to one row per (streamed level, psi level) match with
+    its weighted mean and total weight (:63-88), the weighted match-level fit
+    y~ ~ 1 | alpha + psi, and leaveout.py:634-805 on it with centering
+    "reference" (:949-1016: (sqrt(w) ybar - its mean over matches) sqrt(w) e
+    / M times the JLA factor), the stayers' matches given
+    `sigma_for_stayers` (:91-132) and the n - 1 divisor counting
+    person-years.  psi = the first non-streamed dimension."""
+    c = pass1(rows)
+    S = build_explicit(c)
+    Gamma, _ = solve(c, S, tol=tol)
+    starts = row_starts(rows.gcode)
+    codes = np.asarray(rows.codes, np.int64)
+    N = rows.n_rows
+    w = rows.w if rows.w is not None else np.ones(N)
+    A = residual_moments(starts, codes, c.offs, w, rows.V, Gamma)
+    beta = np.linalg.solve(A[1:, 1:], A[1:, 0]) if A.shape[0] > 1 else np.zeros(0)
+    e, alpha_g, psi_row, _ = row_effects(starts, codes, c.offs, w, rows.V, Gamma, beta)
+    y_t = np.repeat(alpha_g, np.diff(starts)) + psi_row + e
+    g, f = rows.gcode.astype(np.int64), codes[:, 0]
+    head = np.concatenate(([True], (g[1:] != g[:-1]) | (f[1:] != f[:-1])))
+    match = np.cumsum(head) - 1
+    W_m = np.bincount(match, weights=w)
+    Y_m = np.bincount(match, weights=w * y_t) / W_m
+    first = np.flatnonzero(head)
+    mrows = type(rows)(gcode=rows.gcode[first], codes=np.ascontiguousarray(rows.codes[first, :1]),
+                       V=Y_m[:, None], w=W_m, n_levels=[int(rows.n_levels[0])],
+                       n_groups=rows.n_groups, names=[rows.names[0]])
+    cm = pass1(mrows)
+    Sm = build_explicit(cm)
+    gm, _ = solve(cm, Sm, tol=tol)
+    des = Design(mrows, cm, Sm, tol=tol)
+    sm_ = des.starts
+    cm_codes = np.asarray(mrows.codes, np.int64)
+    e_m, alpha_m, psi_m, _ = row_effects(sm_, cm_codes, cm.offs, W_m, mrows.V, gm, np.zeros(0))
+    a_m = np.repeat(alpha_m, np.diff(sm_))
+    T = W_m.sum()
+    R = float(N)
+    scale = T / (T * (R - 1.0) / R) if R > 1 else 1.0
+    ma, mb = (W_m @ psi_m) / T, (W_m @ a_m) / T
+    plug_in = np.array([scale * ((W_m @ (psi_m * psi_m)) / T - ma * ma),
+                        scale * ((W_m @ (a_m * a_m)) / T - mb * mb),
+                        scale * ((W_m @ (psi_m * a_m)) / T - ma * mb)])
+    lev, comp, factor = des.jla_leverages(n_draws, block, seed)
+    root = np.sqrt(W_m)
+    yt = root * Y_m
+    with np.errstate(divide="ignore", invalid="ignore"):     # stayers: replaced below
+        sigma2 = (yt - yt.mean()) * root * e_m / comp * factor
+    # the stayers' matches: leaveout_match.py:91-132 `stayer_sigma2`
+    gm_codes = mrows.gcode.astype(np.int64)
+    stayer = np.bincount(gm_codes)[gm_codes] == 1
+    fitted = Y_m - e_m
+    worker_w = np.bincount(g, weights=w)
+    y_mean = (w @ y_t) / w.sum()
+    r = (y_t - y_mean) * (y_t - fitted[match]) / (1.0 - w / worker_w[g])
+    stay = np.bincount(match, weights=w * w * r) / W_m
+    sigma2 = np.where(stayer, stay, sigma2)
+    bias = des.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003, person_years=R)
+    return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "sigma2": sigma2,
+            "n_matches": len(W_m), "stayer_matches": int(stayer.sum()), "person_years": N,
+            "max_leverage": float(lev[~stayer].max()) if (~stayer).any() else 0.0}
+
+
 # ------------------------------------------------ KSS standard-error pieces
 
 def readout(starts, codes, offs, X, U_l, U_c, U_g):
@@ -896,9 +961,11 @@ class Design:
             out = out + ((v, v_x, group_sums(starts, self.w, weighted)),)
         return out
 
-    def hutchinson_trace(self, sigma2, n_draws, block, seed, psi_column=0):
+    def hutchinson_trace(self, sigma2, n_draws, block, seed, psi_column=0, person_years=None):
         """leaveout.py:321-391 `hutchinson_trace` with :393-448
-        `_trace_block`: the bias terms (var(psi), var(alpha), cov)."""
+        `_trace_block`: the bias terms (var(psi), var(alpha), cov);
+        person_years the divisor's count when the rows are matches
+        (leaveout_se.py:216-220 `_person_years`)."""
         cells, starts = self.cells, self.starts
         G, L, c = len(starts) - 1, cells.L, self.X.shape[1]
         totals = np.zeros(8)
@@ -917,7 +984,7 @@ class Design:
         var_alpha = b1b2 / weight - (b1 / weight) * (b2 / weight)
         cov = 0.5 * (cross / weight - (a1 / weight) * (b2 / weight) - (b1 / weight) * (a2 / weight))
         # leaveout_se.py:202-214 `_moment_divisor`: n - 1 person-years
-        R = float(self.rows.n_rows)
+        R = float(self.rows.n_rows if person_years is None else person_years)
         scale = weight / (weight * (R - 1.0) / R) if R > 1 else 1.0
         return np.array([scale * var_psi, scale * var_alpha, scale * cov])
 

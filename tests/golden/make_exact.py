@@ -8,7 +8,9 @@ Run once, in a container where the reference tree is readable:
 The panel (worker and firm effects only, unweighted) is restricted to its
 leave-one-out connected set by the reference's own core/connected.py:503-557
 `_leave_one_out`; the rows, the exact leverages and the exact plug-in, bias
-and leave-out components go to tests/golden/exact.npz.  The prototype divides
+and leave-out components -- leaving out an observation (`kss`) and a match
+(`kss_match`, centering "reference", with its per-match sigma2 and stayer
+flags) -- go to tests/golden/exact.npz.  The prototype divides
 the components by n; hdfe-stream by n - 1.  Nothing at test time reads the
 reference.
 """
@@ -50,7 +52,16 @@ def main(root):
                keys=np.array(keys), plug_in=np.array([res.plug_in[k] for k in keys]),
                bias=np.array([res.bias[k] for k in keys]),
                kss=np.array([res.kss[k] for k in keys]), P_ii=np.asarray(P_ii))
+    mres = ke.kss_match(kp)
+    out.update(match_plug_in=np.array([mres.plug_in[k] for k in keys]),
+               match_bias=np.array([mres.bias[k] for k in keys]),
+               match_kss=np.array([mres.kss[k] for k in keys]),
+               match_sigma2=np.asarray(mres.diagnostics["sigma2"]),
+               match_stayer=np.asarray(mres.diagnostics["stayer"]),
+               match_worker=np.asarray(mres.diagnostics["worker"]),
+               match_firm=np.asarray(mres.diagnostics["firm"]))
     print(res.summary())
+    print(mres.summary())
     np.savez_compressed(Path(__file__).resolve().parent / "exact.npz", **out)
 
 

@@ -277,3 +277,39 @@ def test_leave_out_components_against_exact_prototype(device):
     assert rel(out["plug_in"], g["plug_in"]) < 1e-9
     assert np.all(np.abs(out["leave_out"] - g["kss"]) <= 0.05 * np.abs(g["bias"]))
     assert float(torch.mean(torch.abs(out["leverage"].cpu() - torch.as_tensor(g["P_ii"])))) < 0.02
+
+
+def test_leave_out_match_matches_oracle(device):
+    """Leaving out a match on the device against the oracle's restatement with
+    the same draws, on a leave-one-out panel with year effects and the
+    model's covariates (partialled out before the collapse), and against the
+    exact prototype's stayer variances and plug-in on the exact panel."""
+    from hdfe_stream_b200 import fit
+    from hdfe_stream_b200.leaveout_match import leave_out_match
+    from hdfe_stream_b200.simulate import Rows, pass0_layout, simulate_panel, _rank_codes
+    panel = simulate_panel(3_000, 300, 8, spell=(2, 8), p_move=0.15, seed=31)
+    a, _ = _rank_codes(panel.worker)
+    b, flev = _rank_codes(panel.firm)
+    n0, n1 = int(a.max()) + 1, len(flev)
+    order = np.lexsort((b, a))
+    alive, _, _ = orc.leave_one_out(a[order], b[order], n0, n1)
+    keep = alive[a] & alive[n0 + b.astype(np.int64)]
+    rows = pass0_layout(panel, keep)
+    ref = orc.leave_out_match(rows, 64, 32, 5)
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    got = leave_out_match(drows, res, n_draws=64, block=32, seed=5, tol=1e-12)
+    assert got["n_matches"] == ref["n_matches"]
+    assert got["stayer_matches"] == ref["stayer_matches"]
+    assert rel(got["plug_in"], ref["plug_in"]) < 1e-9
+    assert rel(got["sigma2"].cpu().numpy(), ref["sigma2"]) < 1e-7
+    assert rel(got["bias"], ref["bias"]) < 1e-7
+    g = load_golden("exact")
+    erows = Rows(gcode=g["gcode"], codes=g["codes_rows"], V=g["V"][:, :1], w=None,
+                 n_levels=[int(x) for x in g["n_levels"]], n_groups=int(g["n_groups"][0]),
+                 names=["log_earn"])
+    d2 = fit.DeviceRows.from_rows(erows)
+    out = leave_out_match(d2, fit.fit(d2, tol=1e-12), n_draws=256, block=32, seed=3, tol=1e-12)
+    st = g["match_stayer"]
+    assert rel(out["plug_in"], g["match_plug_in"]) < 1e-9
+    assert rel(out["sigma2"].cpu().numpy()[st], g["match_sigma2"][st]) < 1e-8

@@ -282,3 +282,20 @@ def test_variances_match_reference(golden):
     assert v["k_fe"] == int(a[f"{name}_k_fe"][0])
     for key, ref in (("iid", "V_iid"), ("hetero", "V_hc1"), ("CRV1", "V_crv1")):
         assert rel(v[key], a[f"{name}_{ref}"]) < 1e-9, key
+
+
+def test_leave_out_match_against_exact_prototype():
+    """Leaving out a match (leaveout_match.py `leave_out_match`) against the
+    reference's dense exact `kss_match` on the same leave-one-out panel: the
+    plug-in exactly, the stayers' matches' sigma2 (`sigma_for_stayers`, no
+    leverage involved) to 1e-8, and the leave-out components within 15% of
+    the bias term at 1,024 draws (the movers' leverages come from JLA, which
+    at match level -- leverages up to 0.9 -- converges slowly)."""
+    g = load_golden("exact")
+    rows = exact_rows(g)
+    out = orc.leave_out_match(rows, 1024, 32, 3)
+    assert rel(out["plug_in"], g["match_plug_in"]) < 1e-9
+    st = g["match_stayer"]
+    assert out["n_matches"] == len(st) and out["stayer_matches"] == int(st.sum())
+    assert rel(out["sigma2"][st], g["match_sigma2"][st]) < 1e-8
+    assert np.all(np.abs(out["leave_out"] - g["match_kss"]) <= 0.15 * np.abs(g["match_bias"]))
