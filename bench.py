@@ -166,17 +166,12 @@ def measured_peak():
 
 def run_ours(args, rank, world, local_rank):
     import torch
-    from hdfe_stream_b200 import _lib, fit
+    from hdfe_stream_b200 import _lib, fit, replicas
     from hdfe_stream_b200.simulate import prepare
 
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local_rank))
-    rows = prepare(args.workload, seed=rank)
+    dist = replicas.init(world, "nccl", device=torch.device("cuda", local_rank))
+    rows = prepare(args.workload, seed=replicas.rank_seed(rank))
     drows = fit.DeviceRows.from_rows(rows)
     torch.cuda.synchronize()
     sampler = ClockSampler(local_rank)
@@ -203,11 +198,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     launches = lib.hdfe_kernel_launches() - launches0
     clocks = sampler.stop(h0, h1)
-    ms = t0.elapsed_time(t1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
     phases = timer.totals()
     info = res.info
     its = int(np.max(np.atleast_1d(info["iterations"])))
@@ -247,7 +238,7 @@ def run_ours(args, rank, world, local_rank):
 
     out = None
     if rank == 0:
-        value = world * args.steps / (ms / 1e3)
+        value = replicas.job_rate(args.steps, ms, world)
         by = phase_bytes(rows, res.cells.counts, res.S, its)
         peak, peak_kind = measured_peak()
         roof = {}
@@ -519,14 +510,10 @@ def run_e2e(args, rows, dist):
         step()
     b.record()
     torch.cuda.synchronize()
-    ms = a.elapsed_time(b)
-    world = 1
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        world = dist.get_world_size()
-    return {"value": round(world * args.steps / (ms / 1e3), 4), "unit": UNIT,
+    from hdfe_stream_b200 import replicas
+    ms = replicas.max_over_ranks(a.elapsed_time(b), dist, "cuda")
+    world = dist.get_world_size() if dist else 1
+    return {"value": round(replicas.job_rate(args.steps, ms, world), 4), "unit": UNIT,
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
 
