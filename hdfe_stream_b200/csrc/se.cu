@@ -130,10 +130,14 @@ __global__ void __launch_bounds__(kThreads) k_bii_moments(const double *rows, in
 //   A U1 (both already scaled by the root);
 //   part[blockIdx][k][0] = sum_i s_k,i sum_j cv_kij^2,
 //   part[blockIdx][k][1] = sum_i y_i cv_ki0  (y NULL: 0).
+// u (3, N) and coef (3, 2, size), when given, add the rank-two term of the
+// reference-centred kernel: cv_kij += coef[k][0][j] + u_ki coef[k][1][j]
+// (leaveout_se.py:591-595, the two scalars u_k'v and 1'v scaled by 1/(2R)).
 __global__ void __launch_bounds__(kThreads) k_c_sums(const double *v, int size, int per_component,
                                                      const double *b, const double *s,
                                                      const double *base, const double *thq,
-                                                     const double *y, int64_t N, double *part)
+                                                     const double *y, const double *u,
+                                                     const double *coef, int64_t N, double *part)
 {
     __shared__ double s_red[kWarps][6];
     const int n_in = per_component ? 3 : 1;
@@ -149,13 +153,15 @@ __global__ void __launch_bounds__(kThreads) k_c_sums(const double *v, int size, 
             const double scale = per_component ? sqrt(fmax(sk, 0.0)) : 1.0;
             const int in0 = (per_component ? k : 0) * size;
             const int bc0 = (n_in + k) * size;
+            const double uk = u ? u[k * N + i] : 0.0;
             double sq = 0.0;
             for (int j = 0; j < size; j++) {
                 const double vk = v[i * size + j] * scale;
                 const double Mv = vk - bs[in0 + j];
                 const double Bv = tq[k * size + j];
                 const double M_bv = vk * bk - bs[bc0 + j];
-                const double cv = Bv - 0.5 * (bk * Mv + M_bv);
+                double cv = Bv - 0.5 * (bk * Mv + M_bv);
+                if (u) cv += coef[(2 * k) * size + j] + uk * coef[(2 * k + 1) * size + j];
                 sq += cv * cv;
                 if (j == 0 && y) acc[3 + k] += y[i] * cv;
             }
@@ -371,23 +377,33 @@ extern "C" int64_t hdfe_c_sums_workspace_bytes(void)
     return (int64_t)se::kSumGrid * 6 * 8;
 }
 
-extern "C" int hdfe_c_sums(const double *v, int32_t size, int32_t per_component, const double *b,
-                           const double *s, const double *base, const double *through_q,
-                           const double *y, int64_t n_rows, double *sums, void *workspace,
-                           int64_t workspace_bytes, void *stream)
+extern "C" int hdfe_c_sums_rank_two(const double *v, int32_t size, int32_t per_component,
+                                    const double *b, const double *s, const double *base,
+                                    const double *through_q, const double *y, const double *u,
+                                    const double *coef, int64_t n_rows, double *sums,
+                                    void *workspace, int64_t workspace_bytes, void *stream)
 {
     if (!v || size < 1 || !b || !s || !base || !through_q || n_rows < 1 || !sums || !workspace ||
-        workspace_bytes < hdfe_c_sums_workspace_bytes())
+        workspace_bytes < hdfe_c_sums_workspace_bytes() || (u && !coef))
         return hdfe_set_arg_error("hdfe_c_sums: bad argument");
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned grid = se::grid_for(n_rows, se::kThreads, se::kSumGrid);
     double *part = (double *)workspace;
     se::k_c_sums<<<grid, se::kThreads, 0, st>>>(v, size, per_component, b, s, base, through_q, y,
-                                                n_rows, part);
+                                                u, u ? coef : nullptr, n_rows, part);
     se::k_sum_parts<<<1, se::kThreads, 0, st>>>(part, (int)grid, 6, sums);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(2);
     return HDFE_OK;
+}
+
+extern "C" int hdfe_c_sums(const double *v, int32_t size, int32_t per_component, const double *b,
+                           const double *s, const double *base, const double *through_q,
+                           const double *y, int64_t n_rows, double *sums, void *workspace,
+                           int64_t workspace_bytes, void *stream)
+{
+    return hdfe_c_sums_rank_two(v, size, per_component, b, s, base, through_q, y, nullptr,
+                                nullptr, n_rows, sums, workspace, workspace_bytes, stream);
 }
 
 extern "C" int hdfe_smooth_cells(const double *knots0, const double *knots1, const double *fp,

@@ -14,6 +14,15 @@ stayers' matches, whose leverage is one, given `sigma_for_stayers`
 by person-years - 1 (leaveout_se.py:216-220).  Everything runs on the device
 (the collapse and the stayer sums as tensor segment sums; the fits, leverages
 and trace through the library's kernels).
+
+With `se`, the standard errors of var(psi) and cov(psi, alpha)
+(leaveout.py:760-772, :848-894 `_match_se_sigma2`): each match's variance
+is, by `se_variance`, "person_year" -- the within-match variance
+(leaveout_match.py:135-153) plus, for movers, the weighted-centred
+leave-match-out sigma2 over T -- or "match" -- that sigma2 alone, stayers'
+from `sigma_for_stayers`; then `StandardErrors.component_variances` on the
+match rows with the stayers' b zeroed, the reference-centred kernel, the
+person-year divisor and seed + 5_500_011.
 """
 
 from __future__ import annotations
@@ -22,6 +31,9 @@ import numpy as np
 
 from . import fit as _fit
 from .leaveout import MAX_BLOCK, InverseOperator
+from .leaveout_se import StandardErrors
+
+SE_SEED_OFFSET = 5_500_011          # leaveout.py:770
 
 
 def _torch():
@@ -30,12 +42,20 @@ def _torch():
 
 
 def leave_out_match(rows: _fit.DeviceRows, res: _fit.FitResult, covariates=None,
-                    n_draws=250, block=MAX_BLOCK, seed=0, tol=1e-10):
+                    n_draws=250, block=MAX_BLOCK, seed=0, tol=1e-10, se=False,
+                    se_variance="person_year", se_draws=None, se_trace=True, smooth_bins=None):
     """The match-level KSS components for a row-level fit `res` of `rows`
     (pass 0's layout; psi = the first non-streamed dimension; covariates
     (N, c) the model's, or None): {"plug_in", "bias", "leave_out", "sigma2"
     (per match), "n_matches", "stayer_matches", "person_years",
-    "max_leverage" (movers' matches)}."""
+    "max_leverage" (movers' matches)}; with `se` also "se" (the
+    `component_variances` dict, var(alpha) NaN) and "sigma2_se"."""
+    if se_variance not in ("match", "person_year"):
+        raise ValueError("se_variance must be 'match' or 'person_year'")
+    if se and se_variance == "person_year" and rows.w is not None:
+        # leaveout_match.py:168-171
+        raise ValueError("se_variance='person_year' is LeaveOutTwoWay's, which has no user "
+                         "weights; use se_variance='match' with a weighted fit")
     torch = _torch()
     dev = rows.gcode.device
     f64 = dict(dtype=torch.float64, device=dev)
@@ -86,6 +106,28 @@ def leave_out_match(rows: _fit.DeviceRows, res: _fit.FitResult, covariates=None,
     sigma2 = torch.where(stayer, stay, sigma2).contiguous()
     bias = mop.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003, person_years=R)
     movers = ~stayer
-    return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "sigma2": sigma2,
-            "n_matches": n_m, "stayer_matches": int(stayer.sum().item()), "person_years": N,
-            "max_leverage": float(lev[movers].max().item()) if bool(movers.any()) else 0.0}
+    out = {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "sigma2": sigma2,
+           "n_matches": n_m, "stayer_matches": int(stayer.sum().item()), "person_years": N,
+           "max_leverage": float(lev[movers].max().item()) if bool(movers.any()) else 0.0}
+    if not se:
+        return out
+    # the movers' weighted-centred leave-match-out sigma2 (leaveout.py:949-1016)
+    y_bar = (W_m @ Y_m) / W_m.sum()
+    block_s2 = W_m * (Y_m - y_bar) * e_m / comp * factor
+    if se_variance == "match":
+        sigma2_se = torch.where(stayer, stay, block_s2)
+    else:
+        # leaveout_match.py:135-153: the mean over the match of (y~ - its mean)^2
+        dev2 = (y_t - Y_m[match]) ** 2
+        within = torch.zeros(n_m, **f64).index_add_(0, match, dev2) / \
+            torch.bincount(match, minlength=n_m).to(torch.float64)
+        sigma2_se = torch.where(stayer, within, within + block_s2 / W_m)
+    sigma2_se = sigma2_se.contiguous()
+    ses = StandardErrors(mop, 0, person_years=N)
+    draws = n_draws if se_draws is None else int(se_draws)
+    out["se"] = ses.component_variances(sigma2_se, lev, comp, factor, None, draws, block,
+                                        seed + SE_SEED_OFFSET, se_trace, smooth_bins,
+                                        stayer_rows=stayer, centering="reference",
+                                        reported=(0, 2))
+    out["sigma2_se"] = sigma2_se
+    return out

@@ -1,5 +1,6 @@
 """KSS standard errors on the device: leaveout_se.py's `bii_rows` and
-`component_variances` (weighted centring, trace term included).
+`component_variances` (trace term included), leaving out an observation or
+a match.
 
 In the square-root-weight metric the leave-out estimate of each component is
 theta = y~' C y~ with the zero-diagonal kernel
@@ -19,6 +20,12 @@ covariance), S^- again, then the readouts (`hdfe_rows_readout`) assembled into
 C v and summed (`hdfe_c_sums`).  The smoother's knots come from the
 reference's own quantile rule on a sample gathered to the host; the cell sums
 and the evaluation run on the device (`hdfe_smooth_cells`, `hdfe_smooth_eval`).
+
+Leaving out a match (leaveout_se.py:616-636), the rows are matches: b is zero
+on the stayers' matches, the divisor counts person-years, and the
+reference-centred estimator is the uncentred sqrt(w) y through
+K = C + (1 u' + u 1') / (2 R), u = M b (`m_times`, one more solve), whose
+two scalars per column ride into `hdfe_c_sums_rank_two`.
 """
 
 from __future__ import annotations
@@ -55,9 +62,11 @@ def smoother_knots(values: np.ndarray, n_bins: int) -> np.ndarray:
 
 class StandardErrors:
     """The KSS standard errors of one design (`InverseOperator`): psi is the
-    non-streamed dimension `psi_column`, alpha the streamed one."""
+    non-streamed dimension `psi_column`, alpha the streamed one;
+    `person_years` the observations behind the rows when they are matches
+    (leaveout_se.py:216-220 `_person_years`; None: the rows)."""
 
-    def __init__(self, op: InverseOperator, psi_column: int = 0):
+    def __init__(self, op: InverseOperator, psi_column: int = 0, person_years=None):
         torch = _torch()
         self.op = op
         self.psi_column = int(psi_column)
@@ -76,7 +85,7 @@ class StandardErrors:
         lw, _, gw = self._to_coef(torch.ones((self.N, 1), **self.f64))
         self.level_w, self.group_w = lw[:, 0], gw[:, 0]
         self.total = float(self.group_w.sum().item())
-        R = float(self.N)
+        R = float(self.N if person_years is None else person_years)
         # leaveout_se.py:202-214 `_moment_divisor`
         self.norm = self.total * (R - 1.0) / R if R > 1 else self.total
         self._ws = torch.empty(int(_lib.lib().hdfe_c_sums_workspace_bytes()), dtype=torch.uint8,
@@ -220,11 +229,23 @@ class StandardErrors:
             out_g[:] = (cross_g - self.group_w[:, None] * psi_mean) / (2 * norm)
         return out_l, out_g
 
-    def c_sums(self, v, b, s, per_component, y=None):
+    def m_times(self, b):
+        """leaveout_se.py:387-424 `_m_times`: u_k = M b_k for the three rows
+        of b (3, N), one solve for all three."""
+        rhs = b.t().contiguous()
+        if self.inv_root is not None:
+            rhs = rhs * self.inv_root[:, None]
+        levels, cov, gsum = self._to_coef(rhs)
+        U_l, U_c, U_g = self._apply_inverse(levels, cov, gsum)
+        return (b - self._readout(U_l, U_c, U_g, root=True).t()).contiguous()
+
+    def c_sums(self, v, b, s, per_component, y=None, u=None):
         """leaveout_se.py:426-597 `_apply_c` with its sinks: C v for the three
         components (v (N, size) shared, or the draws z scaled per component by
         sqrt(max(s_k, 0)) when per_component), returned as sums[6]: per k the
-        sum of s_k (C v)_k^2 over rows and draws, then of y (C v)_k."""
+        sum of s_k (C v)_k^2 over rows and draws, then of y (C v)_k.  With
+        u = M b (3, N), the kernel is the reference-centred K = C +
+        (1 u' + u 1') / (2 N) (:536-543, :591-595)."""
         torch = _torch()
         size = int(v.shape[1])
         n_in = 3 if per_component else 1
@@ -233,6 +254,12 @@ class StandardErrors:
             ins = [v * scale[k][:, None] for k in range(3)]
         else:
             ins = [v]
+        coef = None
+        if u is not None:
+            half = 0.5 / self.N
+            coef = torch.stack([torch.stack([(u[k] @ ins[k if per_component else 0]) * half,
+                                             ins[k if per_component else 0].sum(0) * half])
+                                for k in range(3)]).contiguous()
         stack = torch.cat(ins + [ins[k if per_component else 0] * b[k][:, None]
                                  for k in range(3)], 1)
         if self.inv_root is not None:
@@ -255,10 +282,13 @@ class StandardErrors:
         assert n_in * size + 3 * size == base.shape[1]
         v, b, s = v.contiguous(), b.contiguous(), s.contiguous()
         y = None if y is None else y.contiguous()
-        _lib.check(_lib.lib().hdfe_c_sums(
+        u = None if u is None else u.contiguous()
+        _lib.check(_lib.lib().hdfe_c_sums_rank_two(
             v.data_ptr(), size, int(bool(per_component)), b.data_ptr(), s.data_ptr(),
-            base.data_ptr(), thq.data_ptr(), None if y is None else y.data_ptr(), self.N,
-            sums.data_ptr(), self._ws.data_ptr(), self._ws.numel(), _lib.stream_handle()))
+            base.data_ptr(), thq.data_ptr(), None if y is None else y.data_ptr(),
+            None if u is None else u.data_ptr(), None if coef is None else coef.data_ptr(),
+            self.N, sums.data_ptr(), self._ws.data_ptr(), self._ws.numel(),
+            _lib.stream_handle()))
         return sums
 
     # ---- the smoother of sigma2 (leaveout_se.py:982-1054)
@@ -302,12 +332,16 @@ class StandardErrors:
     # ---- V
 
     def component_variances(self, sigma2, leverage, complement, factor, b_ii=None,
-                            n_draws=250, block=8, seed=0, trace=True, smooth_bins=None):
-        """leaveout_se.py:599-784 `component_variances` (weighted centring):
-        {"se", "variance", "first_term", "trace_term", "theta",
-        "se_conservative"} per component.  sigma2, leverage, complement and
-        factor come from `leave_out_components` / `jla_leverages`; b_ii from
-        `bii_rows` (computed here with the same draws when None)."""
+                            n_draws=250, block=8, seed=0, trace=True, smooth_bins=None,
+                            stayer_rows=None, centering="weighted", reported=(0, 1, 2)):
+        """leaveout_se.py:599-784 `component_variances`: {"se", "variance",
+        "first_term", "trace_term", "theta", "se_conservative"} per
+        component.  sigma2, leverage, complement and factor come from
+        `leave_out_components` / `jla_leverages`; b_ii from `bii_rows`
+        (computed here with the same draws when None).  Leaving out a match:
+        `stayer_rows` (bool, N) zeroes b on the stayers' matches,
+        centering "reference" applies the rank-two kernel to the uncentred
+        outcome, and components outside `reported` are NaN."""
         torch = _torch()
         f64 = self.f64
         sigma2 = torch.as_tensor(sigma2).to(**f64)
@@ -317,15 +351,23 @@ class StandardErrors:
         if b_ii is None:
             b_ii = self.bii_rows(n_draws, min(int(block), MAX_BLOCK // 2), seed)
         b_ii = torch.as_tensor(b_ii).to(**f64)
-        b = (b_ii * (factor / complement)[None, :]).contiguous()
+        if centering not in ("weighted", "reference"):
+            raise ValueError("centering must be 'reference' or 'weighted'")
+        b = b_ii * (factor / complement)[None, :]
+        if stayer_rows is not None:
+            keep = ~torch.as_tensor(stayer_rows, device=self.dev).to(torch.bool)
+            b = torch.where(keep[None, :], b, torch.zeros_like(b))
+        b = b.contiguous()
+        u = self.m_times(b) if centering == "reference" else None
         s = torch.stack([self.smooth(sigma2, leverage, b_ii[k], smooth_bins)
                          for k in range(3)]).contiguous()
         op = self.op
         y = op.rows.V[0]
         w = op.w if op.w is not None else torch.ones(self.N, **f64)
-        y_bar = float((w @ y).item() / w.sum().item())
+        y_bar = float((w @ y).item() / w.sum().item()) if centering == "weighted" else 0.0
         shifted = (torch.sqrt(w) * (y - y_bar)).contiguous()
-        sums = self.c_sums(shifted[:, None].contiguous(), b, s, False, y=shifted).cpu().numpy()
+        sums = self.c_sums(shifted[:, None].contiguous(), b, s, False, y=shifted,
+                           u=u).cpu().numpy()
         first = 4.0 * sums[:3]
         theta = sums[3:]
         tr = np.zeros(3)
@@ -336,11 +378,14 @@ class StandardErrors:
             while drawn < n_draws:
                 size = min(block, n_draws - drawn)
                 z = self._draws(size, int(seed) + TRACE_SEED_OFFSET, drawn)
-                tr += self.c_sums(z, b, s, True).cpu().numpy()[:3]
+                tr += self.c_sums(z, b, s, True, u=u).cpu().numpy()[:3]
                 drawn += size
                 blocks += 1
             tr /= n_draws
         variance = first - 2.0 * tr
+        for k in range(3):
+            if k not in reported:
+                variance[k] = first[k] = tr[k] = theta[k] = np.nan
         names = list(COMPONENTS)
         return {"se": {n: float(np.sqrt(v)) if v > 0 else float("nan")
                        for n, v in zip(names, variance)},

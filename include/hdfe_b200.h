@@ -378,6 +378,12 @@ int hdfe_kss_sigma2(const double *y, const double *w, const double *resid,
  *   per component sum_i s_k,i sum_j cv_kij^2, then sum_i y_i cv_ki0 (y NULL:
  *   0).  per_component: v is the draws z (N, size) and component k's input is
  *   z sqrt(max(s_k, 0)); else v (N, size) is shared.  Deterministic.
+ * hdfe_c_sums_rank_two: hdfe_c_sums for the reference-centred kernel of the
+ *   match level (leaveout_se.py:616-636, :536-543, :591-595):
+ *   K = C + (1 u' + u 1') / (2 R), u (3, N) = M b per component; coef
+ *   (3, 2, size) holds per component and column u_k'v / (2R), then
+ *   1'v / (2R), so that cv_kij gains coef[k][0][j] + u_ki coef[k][1][j].
+ *   u NULL: exactly hdfe_c_sums.
  * hdfe_smooth_cells / hdfe_smooth_eval: leaveout_se.py:982-1054: each row's
  *   cell in the grid of the quantile knots (knots0 of the leverage, knots1 of
  *   B_ii or NULL for one axis; fp the rank of each knot, n_bins + 1 values
@@ -403,6 +409,11 @@ int hdfe_c_sums(const double *v, int32_t size, int32_t per_component, const doub
                 const double *s, const double *base, const double *through_q, const double *y,
                 int64_t n_rows, double *sums, void *workspace, int64_t workspace_bytes,
                 void *stream);
+
+int hdfe_c_sums_rank_two(const double *v, int32_t size, int32_t per_component, const double *b,
+                         const double *s, const double *base, const double *through_q,
+                         const double *y, const double *u, const double *coef, int64_t n_rows,
+                         double *sums, void *workspace, int64_t workspace_bytes, void *stream);
 
 int hdfe_smooth_cells(const double *knots0, const double *knots1, const double *fp,
                       int32_t n_bins, const double *leverage, const double *b_ii,

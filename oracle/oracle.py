@@ -667,7 +667,8 @@ def variances(B, meat_hc, meat_g, rss, n_obs, n_groups, n_levels, pair_component
             "df_cluster": G - 1}
 
 
-def leave_out_match(rows, n_draws, block, seed, tol=1e-12):
+def leave_out_match(rows, n_draws, block, seed, tol=1e-12, se=False, se_variance="person_year",
+                    se_draws=None, smooth_bins=None):
     """leaveout_match.py:156-214 `leave_out_match`, point estimates: the
     row-level fit's partialled outcome y~ = fe_alpha + fe_psi + resid
     (:76-77), collapsed to one row per (streamed level, psi level) match with
@@ -727,9 +728,39 @@ def leave_out_match(rows, n_draws, block, seed, tol=1e-12):
     stay = np.bincount(match, weights=w * w * r) / W_m
     sigma2 = np.where(stayer, stay, sigma2)
     bias = des.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003, person_years=R)
-    return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "sigma2": sigma2,
-            "n_matches": len(W_m), "stayer_matches": int(stayer.sum()), "person_years": N,
-            "max_leverage": float(lev[~stayer].max()) if (~stayer).any() else 0.0}
+    out = {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "sigma2": sigma2,
+           "n_matches": len(W_m), "stayer_matches": int(stayer.sum()), "person_years": N,
+           "max_leverage": float(lev[~stayer].max()) if (~stayer).any() else 0.0}
+    if not se:
+        return out
+    # leaveout.py:848-894 `_match_se_sigma2`: the weighted-centred
+    # leave-match-out sigma2 of the movers' matches (:949-1016)
+    movers = ~stayer
+    y_bar = (W_m @ Y_m) / W_m.sum()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        block_s2 = np.where(movers, W_m * (Y_m - y_bar) * e_m / comp * factor, np.nan)
+    if se_variance == "match":
+        sigma2_se = np.where(stayer, stay, block_s2)
+    elif se_variance == "person_year":
+        if rows.w is not None:
+            raise ValueError("se_variance='person_year' has no user weights; use 'match'")
+        # leaveout_match.py:135-153 `within_match_variance`
+        within = np.bincount(match, weights=(y_t - Y_m[match]) ** 2) / np.bincount(match)
+        sigma2_se = np.where(movers, within + block_s2 / W_m, within)
+    else:
+        raise ValueError("se_variance must be 'match' or 'person_year'")
+    # leaveout.py:760-772: component_variances on the match rows, seed +
+    # 5_500_011, stayers' b zeroed, reference centring, var(alpha) unreported
+    des.person_years = R
+    se_seed = seed + 5_500_011
+    draws = n_draws if se_draws is None else int(se_draws)
+    b_ii = des.bii_rows(draws, block, se_seed)
+    out["se"] = des.component_variances(sigma2_se, lev, comp, factor, b_ii, draws, block,
+                                        se_seed, smooth_bins, stayer_rows=stayer,
+                                        centering="reference", reported=(0, 2))
+    out["sigma2_se"] = sigma2_se
+    out["b_ii"] = b_ii
+    return out
 
 
 # ------------------------------------------------ KSS standard-error pieces
@@ -843,6 +874,9 @@ class Design:
         self.X = np.zeros((rows.n_rows, 0)) if X is None else np.ascontiguousarray(X, np.float64)
         self.dinv = jacobi(cells.diag)
         self._border = None
+        # leaveout_se.py:216-220 `_person_years`: the rows behind the fit when
+        # each row is a match (None: the rows themselves)
+        self.person_years = None
 
     def solve_reduced(self, rhs, scale):
         """inverse.py:86-103 `_solve_reduced`: zero columns, then the PCG."""
@@ -1030,7 +1064,7 @@ class Design:
             lw += np.bincount(cells.offs[d] + codes[:, d], weights=self.w, minlength=L)
         gw = np.add.reduceat(self.w, starts[:-1])
         total = float(gw.sum())
-        R = float(self.rows.n_rows)
+        R = float(self.rows.n_rows if self.person_years is None else self.person_years)
         norm = total * (R - 1.0) / R if R > 1 else total
         psi = slice(int(cells.offs[0]), int(cells.offs[0]) + int(cells.n_levels[0]))
         return lw, gw, total, norm, psi
@@ -1096,10 +1130,20 @@ class Design:
             out_g[:] = (cross_g - gw[:, None] * psi_mean) / (2 * norm)
         return out_l, out_g
 
-    def apply_c(self, v, b, per_component, layout):
-        """leaveout_se.py:426-597 `_apply_c` (no deflation, no rank-two
-        term): C v = B v - (b .* M v + M (b .* v)) / 2 for each component,
-        v (N, size) shared or (N, 3, size) one per component; (N, 3, size)."""
+    def m_times(self, b):
+        """leaveout_se.py:387-424 `_m_times`: u_k = M b_k for the three
+        rows of b (3, N), one solve for all three."""
+        root, inv = self._roots()
+        levels, cov_block, gsum = self._to_coef(np.ascontiguousarray(b.T) * inv[:, None])
+        U_l, U_c, U_g, _ = self.apply_inverse(levels, cov_block, gsum)
+        base = readout(self.starts, self.codes, self.cells.offs, self.X, U_l, U_c, U_g)
+        return b - (root[:, None] * base).T
+
+    def apply_c(self, v, b, per_component, layout, rank_two=None):
+        """leaveout_se.py:426-597 `_apply_c` (no deflation): C v = B v -
+        (b .* M v + M (b .* v)) / 2 for each component, v (N, size) shared or
+        (N, 3, size) one per component; (N, 3, size).  rank_two = (u (3, N),
+        scale) adds scale (1 u_k' + u_k 1') v (:536-543, :591-595)."""
         N, L, G, c = self.rows.n_rows, self.cells.L, len(self.starts) - 1, self.X.shape[1]
         n_in = 3 if per_component else 1
         size = v.shape[-1]
@@ -1137,25 +1181,40 @@ class Design:
             Bv = root[:, None] * through_q[:, k * size:(k + 1) * size]
             M_bv = vk * b[k][:, None] - root[:, None] * base[:, b_cols(k)]
             cv[:, k, :] = Bv - 0.5 * (b[k][:, None] * Mv + M_bv)
+            if rank_two is not None:
+                u, scale = rank_two
+                cv[:, k, :] += scale * ((u[k] @ vk)[None, :] + np.outer(u[k], vk.sum(axis=0)))
         return cv
 
     def component_variances(self, sigma2, leverage, complement, factor, b_ii, n_draws,
-                            block, seed, smooth_bins=None):
-        """leaveout_se.py:599-784 `component_variances` (weighted centring,
-        trace included, no weak-identification pieces): per component the
-        first term 4 sum s~ (C y~)^2, the trace term 2 tr(C Om~ C Om~) by
-        Hutchinson draws (seed + 7_700_017), theta = y~' C y~, and
-        variance = first - trace term; s~ the smoothed sigma2."""
+                            block, seed, smooth_bins=None, stayer_rows=None,
+                            centering="weighted", reported=(0, 1, 2)):
+        """leaveout_se.py:599-784 `component_variances` (trace included, no
+        weak-identification pieces): per component the first term
+        4 sum s~ (C y~)^2, the trace term 2 tr(C Om~ C Om~) by Hutchinson
+        draws (seed + 7_700_017), theta = y~' C y~, and variance = first -
+        trace term; s~ the smoothed sigma2.  Leaving out matches (:616-636):
+        b is zero on `stayer_rows`; centering "reference" applies
+        K = C + (1 u' + u 1') / (2 R), u = M b, R the rows, to the uncentred
+        sqrt(w) y; components not in `reported` are NaN."""
         layout = self.se_layout()
-        b = b_ii * (factor / complement)[None, :]
+        with np.errstate(divide="ignore", invalid="ignore"):   # stayers' M_ii = 0
+            b = b_ii * (factor / complement)[None, :]
+        if stayer_rows is not None:
+            b[:, np.asarray(stayer_rows, bool)] = 0.0
+        rank_two = None
+        if centering == "reference":
+            rank_two = (self.m_times(b), 0.5 / self.rows.n_rows)
+        elif centering != "weighted":
+            raise ValueError("centering must be 'reference' or 'weighted'")
         tables = [fit_smoother(sigma2, leverage, b_ii[k], smooth_bins) for k in range(3)]
         sig = [smooth_eval(t, leverage, b_ii[k]) if t is not None else np.asarray(sigma2)
                for k, t in enumerate(tables)]
         y = self.rows.V[:, 0]
         w = self.w
-        y_bar = float(w @ y / w.sum())
+        y_bar = float(w @ y / w.sum()) if centering == "weighted" else 0.0
         shifted = np.sqrt(w) * (y - y_bar)
-        cv = self.apply_c(shifted[:, None], b, False, layout)
+        cv = self.apply_c(shifted[:, None], b, False, layout, rank_two)
         first = np.array([4.0 * float(sig[k] @ (cv[:, k, 0] ** 2)) for k in range(3)])
         theta = np.array([float(shifted @ cv[:, k, 0]) for k in range(3)])
         trace = np.zeros(3)
@@ -1166,12 +1225,16 @@ class Design:
             z = rademacher(0, N, size, seed + 7_700_017, drawn)
             v = np.stack([z * np.sqrt(np.maximum(sig[k], 0.0))[:, None] for k in range(3)],
                          axis=1)
-            cvt = self.apply_c(v, b, True, layout)
+            cvt = self.apply_c(v, b, True, layout, rank_two)
             for k in range(3):
                 trace[k] += float(sig[k] @ (cvt[:, k, :] ** 2).sum(axis=1))
             drawn += size
         trace /= n_draws
-        return {"variance": first - 2.0 * trace, "first_term": first,
+        variance = first - 2.0 * trace
+        for k in range(3):
+            if k not in reported:
+                variance[k] = first[k] = trace[k] = theta[k] = np.nan
+        return {"variance": variance, "first_term": first,
                 "trace_term": 2.0 * trace, "theta": theta}
 
     def jla_leverages(self, n_draws, block, seed):

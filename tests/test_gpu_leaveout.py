@@ -313,3 +313,37 @@ def test_leave_out_match_matches_oracle(device):
     st = g["match_stayer"]
     assert rel(out["plug_in"], g["match_plug_in"]) < 1e-9
     assert rel(out["sigma2"].cpu().numpy()[st], g["match_sigma2"][st]) < 1e-8
+
+
+@pytest.mark.parametrize("rule,weights", [("person_year", False), ("match", True)])
+def test_leave_out_match_standard_errors_match_oracle(device, rule, weights):
+    """Match-level standard errors on the device against the oracle with the
+    same draws: the per-match variances and theta, the first and trace
+    terms and V of var(psi) and cov(psi, alpha), on a leave-one-out panel
+    with year effects (weighted for the "match" rule, which takes weights)."""
+    from hdfe_stream_b200 import fit
+    from hdfe_stream_b200.leaveout_match import leave_out_match
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel, _rank_codes
+    panel = simulate_panel(2_000, 200, 8, spell=(2, 8), p_move=0.15, weights=weights, seed=37)
+    a, _ = _rank_codes(panel.worker)
+    b, flev = _rank_codes(panel.firm)
+    n0, n1 = int(a.max()) + 1, len(flev)
+    order = np.lexsort((b, a))
+    alive, _, _ = orc.leave_one_out(a[order], b[order], n0, n1)
+    keep = alive[a] & alive[n0 + b.astype(np.int64)]
+    rows = pass0_layout(panel, keep)
+    ref = orc.leave_out_match(rows, 64, 32, 5, se=True, se_variance=rule, se_draws=24)
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    got = leave_out_match(drows, res, n_draws=64, block=32, seed=5, tol=1e-12, se=True,
+                          se_variance=rule, se_draws=24)
+    assert rel(got["sigma2_se"].cpu().numpy(), ref["sigma2_se"]) < 1e-7
+    names = ("var(psi)", "cov(psi, alpha)")
+    for key in ("theta", "first_term", "trace_term", "variance"):
+        assert rel([got["se"][key][n] for n in names], ref["se"][key][[0, 2]]) < 1e-6, key
+    assert np.isnan(got["se"]["variance"]["var(alpha)"])
+    if rule == "person_year":
+        with pytest.raises(ValueError):
+            wrows = fit.DeviceRows.from_rows(pass0_layout(
+                simulate_panel(300, 30, 6, spell=(2, 6), weights=True, seed=3)))
+            leave_out_match(wrows, fit.fit(wrows), se=True, se_variance="person_year")

@@ -81,3 +81,22 @@ def test_smoother_matches_oracle(device):
                         torch.as_tensor(b, device=device), bins).cpu().numpy()
         ref = orc.smooth_eval(orc.fit_smoother(s2, lev, b, bins), lev, b)
         assert rel(got, ref) < 1e-12
+
+
+def test_match_level_kernel_matches_reference(device):
+    """The match level's options (stayers' b zeroed, the reference-centred
+    kernel with the rank-two term, var(alpha) unreported) against the
+    reference's `component_variances` for the same sigma2, leverages and
+    draws (tests/golden/match_se.npz)."""
+    g = load_golden("match_se")
+    ref = {f"r_{k[4:]}": v for k, v in g.items() if k.startswith("ref_")}
+    ref["r_w"] = np.zeros(0)
+    se = standard_errors(se_rows(ref, "r"), float(ref["r_tol"][0]))
+    out = se.component_variances(ref["r_sigma2"], ref["r_leverage"], ref["r_complement"],
+                                 ref["r_factor"], None, n_draws=16, block=8, seed=6,
+                                 stayer_rows=ref["r_stayer"], centering="reference",
+                                 reported=(0, 2))
+    for key in ("first_term", "trace_term", "theta", "variance"):
+        got = [out[key][n] for n in ("var(psi)", "cov(psi, alpha)")]
+        assert rel(got, ref[f"r_{key}"][[0, 2]]) < 1e-7, key
+        assert np.isnan(out[key]["var(alpha)"])

@@ -299,3 +299,46 @@ def test_leave_out_match_against_exact_prototype():
     assert out["n_matches"] == len(st) and out["stayer_matches"] == int(st.sum())
     assert rel(out["sigma2"][st], g["match_sigma2"][st]) < 1e-8
     assert np.all(np.abs(out["leave_out"] - g["match_kss"]) <= 0.15 * np.abs(g["match_bias"]))
+
+
+def test_match_level_kernel_matches_reference():
+    """The match level's options of leaveout_se.py `component_variances`
+    (stayers' b zeroed, the reference-centred kernel with its rank-two term
+    through `_m_times`, var(alpha) unreported) against the reference's own
+    outputs for the same sigma2, leverages and draws (tests/golden/
+    match_se.npz, made by tests/golden/make_match_se.py)."""
+    g = load_golden("match_se")
+    ref = {f"r_{k[4:]}": v for k, v in g.items() if k.startswith("ref_")}
+    ref["r_w"] = np.zeros(0)
+    rows = se_rows(ref, "r")
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(ref["r_tol"][0]))
+    b_ii = des.bii_rows(16, 8, 6)
+    assert rel(b_ii, ref["r_bii"]) < 1e-9
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out = des.component_variances(ref["r_sigma2"], ref["r_leverage"], ref["r_complement"],
+                                      ref["r_factor"], b_ii, 16, 8, 6,
+                                      stayer_rows=ref["r_stayer"], centering="reference",
+                                      reported=(0, 2))
+    for key in ("first_term", "trace_term", "theta", "variance"):
+        assert np.isnan(out[key][1]) and np.isnan(ref[f"r_{key}"][1])
+        assert rel(out[key][[0, 2]], ref[f"r_{key}"][[0, 2]]) < 1e-8, key
+
+
+@pytest.mark.parametrize("rule", ["person_year", "match"])
+def test_match_standard_errors_against_exact_prototype(rule):
+    """Match-level standard errors of var(psi) and cov(psi, alpha) with 512
+    JLA and trace draws against the reference's dense exact `kss_match_se`
+    (prototypes/kss_exact.py:636-716, exact leverages and B_ii) on the
+    exact panel: theta within 1%, the variance and its first term within
+    10%, the trace term within 25% (the JLA leverages and B_ii move the
+    smoother's cells)."""
+    g = load_golden("match_se")
+    rows = exact_rows(load_golden("exact"))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        se = orc.leave_out_match(rows, 512, 32, 3, se=True, se_variance=rule)["se"]
+    for key, ek, tol in (("theta", "theta", 0.01), ("variance", "V", 0.1),
+                         ("first_term", "first", 0.1), ("trace_term", "trace", 0.25)):
+        want = g[f"exact_{rule}_{ek}"]
+        assert np.all(np.abs(se[key][[0, 2]] - want) <= tol * np.abs(want)), key
+    assert np.isnan(se["variance"][1])
