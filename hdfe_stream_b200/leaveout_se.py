@@ -152,11 +152,17 @@ class StandardErrors:
         return out
 
     def _draws(self, size, seed, first_draw):
+        return self._draws_at(self.N, 0, size, seed, first_draw)
+
+    def _draws_at(self, n, ordinal0, size, seed, first_draw):
+        """Rademacher draws (n, size) for the ordinals ordinal0 .. ordinal0 + n
+        (core/kernels_groups.py:53-76 `_nb_rademacher`)."""
         torch = _torch()
-        z = torch.empty((self.N, size), **self.f64)
-        _lib.check(_lib.lib().hdfe_rademacher(z.data_ptr(), self.N, 0, size,
-                                              int(seed) & (2**64 - 1), int(first_draw),
-                                              _lib.stream_handle()))
+        z = torch.empty((n, size), **self.f64)
+        if n:
+            _lib.check(_lib.lib().hdfe_rademacher(z.data_ptr(), n, int(ordinal0), size,
+                                                  int(seed) & (2**64 - 1), int(first_draw),
+                                                  _lib.stream_handle()))
         return z
 
     # ---- B_ii
@@ -294,11 +300,13 @@ class StandardErrors:
     # ---- the smoother of sigma2 (leaveout_se.py:982-1054)
 
     def smooth(self, sigma2, leverage, b_ii, n_bins=None):
-        """sigma2 smoothed on (P_ii, B_ii), one value per row (device)."""
+        """sigma2 smoothed on (P_ii, B_ii), or on P_ii alone when b_ii is
+        None, one value per row (device)."""
         torch = _torch()
         lib = _lib.lib()
         N = self.N
-        n_bins = smoother_bins(N, 2) if n_bins is None else int(n_bins)
+        dims = 1 if b_ii is None else 2
+        n_bins = smoother_bins(N, dims) if n_bins is None else int(n_bins)
         if n_bins < 1:
             return sigma2
         if N <= QUANTILE_SAMPLE:
@@ -311,22 +319,25 @@ class StandardErrors:
         def sample(x):
             return (x if take is None else x[take]).cpu().numpy()
         k0 = torch.as_tensor(smoother_knots(sample(leverage), n_bins), **self.f64)
-        k1 = torch.as_tensor(smoother_knots(sample(b_ii), n_bins), **self.f64)
+        k1 = None if b_ii is None else \
+            torch.as_tensor(smoother_knots(sample(b_ii), n_bins), **self.f64)
         fp = torch.as_tensor(np.linspace(0.0, 1.0, n_bins + 1), **self.f64)
-        totals = torch.zeros(n_bins * n_bins, **self.f64)
-        counts = torch.zeros(n_bins * n_bins, **self.f64)
+        totals = torch.zeros(n_bins ** dims, **self.f64)
+        counts = torch.zeros(n_bins ** dims, **self.f64)
         sh = _lib.stream_handle()
-        leverage, b_ii, sigma2 = leverage.contiguous(), b_ii.contiguous(), sigma2.contiguous()
-        _lib.check(lib.hdfe_smooth_cells(k0.data_ptr(), k1.data_ptr(), fp.data_ptr(), n_bins,
-                                         leverage.data_ptr(), b_ii.data_ptr(),
-                                         sigma2.data_ptr(), N, totals.data_ptr(),
-                                         counts.data_ptr(), sh))
+        leverage, sigma2 = leverage.contiguous(), sigma2.contiguous()
+        b_ii = None if b_ii is None else b_ii.contiguous()
+        k1_ptr = None if k1 is None else k1.data_ptr()
+        b_ptr = None if b_ii is None else b_ii.data_ptr()
+        _lib.check(lib.hdfe_smooth_cells(k0.data_ptr(), k1_ptr, fp.data_ptr(), n_bins,
+                                         leverage.data_ptr(), b_ptr, sigma2.data_ptr(), N,
+                                         totals.data_ptr(), counts.data_ptr(), sh))
         overall = totals.sum() / torch.clamp(counts.sum(), min=1.0)
         means = torch.where(counts > 0, totals / torch.clamp(counts, min=1.0), overall)
         out = torch.empty(N, **self.f64)
-        _lib.check(lib.hdfe_smooth_eval(k0.data_ptr(), k1.data_ptr(), fp.data_ptr(), n_bins,
-                                        means.data_ptr(), leverage.data_ptr(), b_ii.data_ptr(),
-                                        N, out.data_ptr(), sh))
+        _lib.check(lib.hdfe_smooth_eval(k0.data_ptr(), k1_ptr, fp.data_ptr(), n_bins,
+                                        means.data_ptr(), leverage.data_ptr(), b_ptr, N,
+                                        out.data_ptr(), sh))
         return out
 
     # ---- V

@@ -1268,3 +1268,309 @@ class Design:
         factor = np.where(usable, 1.0 - factor + np.divide(B, M_bar, out=np.zeros_like(B),
                                                              where=usable), 1.0)
         return P_bar, M_bar, factor
+
+
+# ------------------------------------------- the weak-identification diagnostic
+
+WEAK_ID_THRESHOLD = 0.1             # leaveout_weakid.py:64 (KSS Section 6.2)
+
+
+def ritz_top(alpha, beta, top):
+    """leaveout_weakid.py:386-434 `_ritz_top`: the leading genuine Ritz values
+    of the tridiagonal (alpha, beta[:-1]), their error bounds |beta[-1] s_m|
+    and vectors; copies within 1e-8 of the largest merge (the one with the
+    smaller bound kept), and a lone value that is also an eigenvalue of the
+    tridiagonal without its first row and column (to 1e-11) is spurious
+    (Cullum-Willoughby)."""
+    from scipy.linalg import eigh_tridiagonal, eigvalsh_tridiagonal
+    m = len(alpha)
+    if m == 0:
+        return np.array([]), np.array([]), np.zeros((0, 0))
+    off = np.asarray(beta[:m - 1], float)
+    theta, S = eigh_tridiagonal(np.asarray(alpha, float), off)
+    bounds = np.abs(beta[m - 1] * S[-1, :])
+    scale = max(float(np.abs(theta).max()), 1e-300)
+    order = np.argsort(theta)
+    kept = []
+    for i in order:
+        if kept and abs(theta[i] - theta[kept[-1]]) <= 1e-8 * scale:
+            if bounds[i] < bounds[kept[-1]]:
+                kept[-1] = i
+            continue
+        kept.append(i)
+    copies = {}
+    for i in order:
+        head = min(kept, key=lambda h: abs(theta[h] - theta[i]))
+        copies[head] = copies.get(head, 0) + 1
+    if m > 1:
+        hat = eigvalsh_tridiagonal(alpha[1:], off[1:]) if m > 2 else np.asarray(alpha[1:])
+        kept = [h for h in kept
+                if copies[h] > 1 or np.min(np.abs(hat - theta[h])) > 1e-11 * scale]
+    kept = sorted(kept, key=lambda h: -abs(theta[h]))[:top]
+    return theta[kept], bounds[kept], S[:, kept]
+
+
+def weak_id_diagnostics(des, sigma2, leverage, n_draws=64, block=32, seed=0, max_iter=150,
+                        tol=1e-4, top=3, smooth_bins=None, scratch_mb=32):
+    """leaveout_weakid.py:565-713 `weak_id_diagnostics`: per component the
+    leading eigenvalues of S^- Q by Lanczos in the S^- inner product (three
+    components in lockstep, one solve of three columns a step; :217-383),
+    sum lambda^2 by deflated Hutchinson (:467-555, seed + 3_300_007), the
+    ratios, q, and the first-stage F of the leading direction (:715-744).
+    No covariates in the design."""
+    layout = des.se_layout()
+    lw, gw, total, norm, psi = layout
+    L, G, c = des.cells.L, len(des.starts) - 1, des.X.shape[1]
+    n_psi = psi.stop - psi.start
+    if n_draws < 2:
+        raise ValueError("n_draws must be at least 2")
+
+    def q_block(comps, U_l, U_g):
+        out_l, out_g = np.zeros_like(U_l), np.zeros_like(U_g)
+        comps = np.asarray(comps)
+        for k in range(3):
+            cols = np.flatnonzero(comps == k)
+            if len(cols):
+                ql, qg = des.apply_q(k, U_l[:, cols], U_g[:, cols], layout)
+                out_l[:, cols], out_g[:, cols] = ql, qg
+        return out_l, out_g
+
+    def solve(t):
+        U_l, U_c, U_g, _ = des.apply_inverse(t[0], t[1], t[2])
+        return [U_l, U_c, U_g]
+
+    def dot(a, b):
+        return sum((x * y).sum(axis=0) for x, y in zip(a, b))
+
+    # :185-215 `_krylov_plan`
+    dims = [max(n_psi - 1, 0), max(L + c + 1, 1), max(2 * (n_psi - 1), 0)]
+    support_rows = [n_psi, G, n_psi + G]
+    budget = int(scratch_mb) << 20
+    caps = [min(max_iter, d) for d in dims]
+    reorth = [cap * 2 * r * 8 <= budget for cap, r in zip(caps, support_rows)]
+
+    def support(k, t):
+        parts = []
+        if k in (0, 2):
+            parts.append(t[0][psi, k])
+        if k in (1, 2):
+            parts.append(t[2][:, k])
+        return np.concatenate(parts) if len(parts) > 1 else parts[0].copy()
+
+    def scatter(k, flat, t):
+        at = 0
+        if k in (0, 2):
+            t[0][psi, k] -= flat[:n_psi]
+            at = n_psi
+        if k in (1, 2):
+            t[2][:, k] -= flat[at:]
+
+    def project(t):
+        for k in (0, 2):
+            t[0][psi, k] -= t[0][psi, k].mean()
+        for k in (1, 2):
+            t[2][:, k] -= t[2][:, k].mean()
+
+    shapes = [(L, 3), (c, 3), (G, 3)]
+
+    def lanczos(n_iter, ritz=None, check=None, every=20):
+        r = [rademacher(pos, s[0], 3, seed, 0) for pos, s in zip((0, L, L + c), shapes)]
+        ql, qg = q_block([0, 1, 2], r[0], r[2])
+        x = [ql, np.zeros(shapes[1]), qg]
+        project(x)
+        y = solve(x)
+        nrm = np.sqrt(np.maximum(dot(x, y), 0.0))
+        live = (nrm > 0) & (np.array(caps) > 0)
+        for t in (*x, *y):
+            t[:, live] /= nrm[live]
+            t[:, ~live] = 0.0
+        x_prev = [np.zeros(s) for s in shapes]
+        beta_prev = np.zeros(3)
+        basis = [([], []) for _ in range(3)]
+        alphas, betas = [[], [], []], [[], [], []]
+        lengths = np.zeros(3, dtype=int)
+        acc = None
+        if ritz is not None:
+            kk = ritz[0].shape[1]
+            acc = ([np.zeros((s[0], 3 * kk)) for s in shapes],
+                   [np.zeros((s[0], 3 * kk)) for s in shapes])
+        beta_max = np.zeros(3)
+        steps = 0
+        for j in range(n_iter):
+            if not live.any():
+                break
+            if (check is not None and j > 0 and j % every == 0
+                    and check([np.array(a) for a in alphas], [np.array(b) for b in betas],
+                              lengths, j)):
+                break
+            steps = j + 1
+            if acc is not None:
+                for k in np.flatnonzero(live):
+                    if j < len(ritz[k]):
+                        cols = slice(k * kk, (k + 1) * kk)
+                        for ax, ay, xb, yb in zip(acc[0], acc[1], x, y):
+                            ax[:, cols] += np.outer(xb[:, k], ritz[k][j])
+                            ay[:, cols] += np.outer(yb[:, k], ritz[k][j])
+            for k in np.flatnonzero(live):
+                if reorth[k]:
+                    basis[k][0].append(support(k, x))
+                    basis[k][1].append(support(k, y))
+            ql, qg = q_block([0, 1, 2], y[0], y[2])
+            w = [ql, np.zeros(shapes[1]), qg]
+            for wb, xp in zip(w, x_prev):
+                wb -= beta_prev * xp
+            alpha = dot(w, y)
+            for wb, xb in zip(w, x):
+                wb -= alpha * xb
+            fix = dot(w, y)
+            for wb, xb in zip(w, x):
+                wb -= fix * xb
+            alpha = alpha + fix
+            project(w)
+            for k in np.flatnonzero(live):
+                if not reorth[k] or not basis[k][0]:
+                    continue
+                for _ in range(2):
+                    wk = support(k, w)
+                    Xs, Ys = np.column_stack(basis[k][0]), np.column_stack(basis[k][1])
+                    scatter(k, Xs @ (Ys.T @ wk), w)
+            project(w)
+            z = solve(w)
+            beta = np.sqrt(np.maximum(dot(w, z), 0.0))
+            beta_max = np.maximum(beta_max, beta)
+            for k in np.flatnonzero(live):
+                alphas[k].append(float(alpha[k]))
+                betas[k].append(float(beta[k]))
+                lengths[k] = j + 1
+            live = (live & (beta > 1e-8 * np.maximum(beta_max, 1e-300))
+                    & (lengths < np.array(caps)))
+            x_prev = x
+            x = [wb.copy() for wb in w]
+            y = z
+            for t in (*x, *y):
+                t[:, live] /= beta[live]
+                t[:, ~live] = 0.0
+            beta_prev = np.where(live, beta, 0.0)
+        if acc is not None:
+            return acc
+        return [np.array(a) for a in alphas], [np.array(b) for b in betas], lengths, steps
+
+    def converged_all(alphas, betas, lengths, steps):
+        for k in range(3):
+            if lengths[k] < steps:
+                continue
+            theta, bounds, _ = ritz_top(alphas[k], betas[k], top)
+            lead = float(np.abs(theta[0])) if len(theta) else 0.0
+            if np.any(bounds[:2] > tol * max(lead, 1e-300)):
+                return False
+        return True
+
+    alphas, betas, lengths, n_iter = lanczos(max_iter, check=converged_all, every=10)
+    checked = [ritz_top(alphas[k], betas[k], top) for k in range(3)]
+    n_coef = L + c + G
+    kk = top if 2 * 3 * top * n_coef * 8 <= budget else 1
+    ritz = []
+    for _, _, S in checked:
+        coef = np.zeros((S.shape[0], kk))
+        coef[:, :min(kk, S.shape[1])] = S[:, :kk]
+        ritz.append(coef)
+    X, Y = lanczos(n_iter, ritz=ritz)
+    # :436-465 `_s_orthonormalize`: modified Gram-Schmidt in <x, y> = x' S^- y
+    for k in range(3):
+        base = k * kk
+        for a in range(kk):
+            ca = base + a
+            for p in range(a):
+                cp = base + p
+                co = sum(xb[:, ca] @ yb[:, cp] for xb, yb in zip(X, Y))
+                for xb, yb in zip(X, Y):
+                    xb[:, ca] -= co * xb[:, cp]
+                    yb[:, ca] -= co * yb[:, cp]
+            n2 = sum(xb[:, ca] @ yb[:, ca] for xb, yb in zip(X, Y))
+            lead = sum(xb[:, base] @ yb[:, base] for xb, yb in zip(X, Y))
+            if n2 <= 1e-20 * max(lead, 1e-300) or n2 <= 0:
+                for t in (*X, *Y):
+                    t[:, ca] = 0.0
+                continue
+            for t in (*X, *Y):
+                t[:, ca] *= 1.0 / np.sqrt(n2)
+    u = [t[:, ::kk].copy() for t in Y]
+    leading = [theta for theta, _, _ in checked]
+
+    # :467-555 `_sum_sq_eigenvalues`
+    comps = [k for k in range(3) for _ in range(kk)]
+    ql, qg = q_block(comps, Y[0], Y[2])
+    zq = solve([ql, np.zeros((c, 3 * kk)), qg])
+    exact = ((ql * zq[0]).sum(0) + (qg * zq[2]).sum(0)).reshape(3, kk).sum(axis=1)
+    N = des.rows.n_rows
+    _, inv = des._roots()
+    draws, drawn = [], 0
+    size = max(1, block // 3)
+
+    def summarize(values):
+        n = values.shape[1]
+        se = values.std(axis=1, ddof=1) / np.sqrt(n) if n > 1 else np.full(3, np.nan)
+        return exact + values.mean(axis=1), se
+
+    def settled(est, se):
+        for k in range(3):
+            if not est[k] > 0 or not np.isfinite(se[k]):
+                return False
+            r = leading[k] ** 2 / est[k]
+            if np.any(np.abs(r - WEAK_ID_THRESHOLD) < 2.0 * (se[k] / est[k]) * r):
+                return False
+        return True
+
+    while drawn < n_draws:
+        m = min(size, n_draws - drawn)
+        xi = rademacher(0, N, m, seed + 3_300_007, drawn) * inv[:, None]
+        zeta = list(des._to_coef(xi))
+        yv = solve(zeta)
+        y_def = [np.empty((t.shape[0], 3 * m)) for t in yv]
+        for k in range(3):
+            cols = slice(k * kk, (k + 1) * kk)
+            proj = sum(zb.T @ Yb[:, cols] for zb, Yb in zip(zeta, Y))
+            for yd, yb, Yb in zip(y_def, yv, Y):
+                yd[:, k * m:(k + 1) * m] = yb - Yb[:, cols] @ proj.T
+        ql, qg = q_block([k for k in range(3) for _ in range(m)], y_def[0], y_def[2])
+        bq = solve([ql, np.zeros((c, 3 * m)), qg])
+        draws.append(((ql * bq[0]).sum(axis=0) + (qg * bq[2]).sum(axis=0)).reshape(3, m))
+        drawn += m
+        if drawn >= 16 and drawn < n_draws and settled(*summarize(np.hstack(draws))):
+            break
+    sum_sq, sum_sq_se = summarize(np.hstack(draws))
+
+    # :715-744 `_first_stage_f`, sigma2 smoothed on the leverage alone
+    table = fit_smoother(sigma2, leverage, None, smooth_bins)
+    smooth = smooth_eval(table, leverage, None) if table is not None else np.asarray(sigma2)
+    rows_u = readout(des.starts, des.codes, des.cells.offs, des.X, u[0], u[1], u[2])
+    root = np.sqrt(des.w)
+    x1 = rows_u * root[:, None]
+    y = des.rows.V[:, 0]
+    y_t = root * (y - float(des.w @ y / des.w.sum()))
+    num, den = x1.T @ y_t, (x1 ** 2).T @ smooth
+    f_stat = np.where(den > 0, num ** 2 / np.where(den > 0, den, 1.0), np.nan)
+
+    out = {"eigenvalues": [], "bounds": [], "ratios": [], "q": [], "q_capped": [],
+           "q_borderline": [], "converged": [], "sum_sq": sum_sq, "sum_sq_se": sum_sq_se,
+           "f_stat": f_stat, "steps": n_iter, "lengths": lengths, "n_draws": drawn,
+           "deflated": kk, "caps": caps, "reorth": reorth, "lead_vectors": u}
+    for k in range(3):
+        theta, bnd, _ = checked[k]
+        lead = float(np.abs(theta[0])) if len(theta) else 0.0
+        r = theta ** 2 / sum_sq[k] if sum_sq[k] > 0 else np.zeros_like(theta)
+        q = 0
+        for v in r:
+            if v < WEAK_ID_THRESHOLD:
+                break
+            q += 1
+        rel_se = sum_sq_se[k] / sum_sq[k] if sum_sq[k] > 0 else np.inf
+        out["eigenvalues"].append(theta)
+        out["bounds"].append(bnd)
+        out["ratios"].append(r)
+        out["q"].append(q)
+        out["q_capped"].append(bool(q == len(r) and q > 0))
+        out["q_borderline"].append(bool(np.any(np.abs(r - WEAK_ID_THRESHOLD) < 2.0 * rel_se * r)))
+        out["converged"].append(bool(lengths[k] < n_iter or lengths[k] >= caps[k]
+                                     or np.all(bnd[:2] <= tol * max(lead, 1e-300))))
+    return out

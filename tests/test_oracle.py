@@ -342,3 +342,29 @@ def test_match_standard_errors_against_exact_prototype(rule):
         want = g[f"exact_{rule}_{ek}"]
         assert np.all(np.abs(se[key][[0, 2]] - want) <= tol * np.abs(want)), key
     assert np.isnan(se["variance"][1])
+
+
+@pytest.mark.parametrize("name", ["akm_small", "low_mobility"])
+def test_weak_id_diagnostics_match_reference(name):
+    """leaveout_weakid.py `weak_id_diagnostics` (Lanczos on Q S^-, the
+    deflated Hutchinson sum of squared eigenvalues, q, the first-stage F)
+    against the reference's own outputs on a well-connected panel (q = 0)
+    and a low-mobility one (q = 1) (tests/golden/weakid.npz, made by
+    tests/golden/make_weakid.py)."""
+    g = load_golden("weakid")
+    rows = se_rows(g, name)
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g[f"{name}_tol"][0]))
+    out = orc.weak_id_diagnostics(des, g[f"{name}_sigma2"], g[f"{name}_leverage"], n_draws=48,
+                                  block=12, seed=9)
+    assert out["steps"] == int(g[f"{name}_steps"][0])
+    assert list(out["lengths"]) == list(g[f"{name}_lengths"])
+    assert out["n_draws"] == int(g[f"{name}_n_draws"][0])
+    assert out["deflated"] == int(g[f"{name}_deflated"][0])
+    for k in range(3):
+        assert rel(out["eigenvalues"][k], g[f"{name}_eig{k}"]) < 1e-10
+        assert rel(out["ratios"][k], g[f"{name}_ratio{k}"]) < 1e-10
+    assert rel(out["sum_sq"], g[f"{name}_sum_sq"]) < 1e-10
+    assert rel(out["sum_sq_se"], g[f"{name}_sum_sq_se"]) < 1e-8
+    assert list(out["q"]) == list(g[f"{name}_q"])
+    assert rel(out["f_stat"], g[f"{name}_f_stat"]) < 1e-10
