@@ -91,8 +91,8 @@ SIGNATURES = {
     "hdfe_c_sums_workspace_bytes": (_i64, []),
     "hdfe_c_sums": (_c.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _i64,
                                _vp]),
-    "hdfe_c_sums_rank_two": (_c.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                        _i64, _vp, _vp, _i64, _vp]),
+    "hdfe_c_sums_ext": (_c.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _vp, _vp,
+                                   _vp, _i64, _vp, _vp, _i64, _vp]),
     "hdfe_smooth_cells": (_c.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
     "hdfe_smooth_eval": (_c.c_int, [_vp, _vp, _vp, _i32, _vp, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_batch_pcg_grid": (_c.c_int, [_i32, _i32, _vp, _vp]),

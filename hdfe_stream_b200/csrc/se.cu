@@ -128,21 +128,27 @@ __global__ void __launch_bounds__(kThreads) k_bii_moments(const double *rows, in
 //   per component by scale_k = sqrt(max(s_k, 0)) (per_component);
 //   base (N, (n_in + 3) size) = sqrt(w) A U0, through_q (N, 3 size) = sqrt(w)
 //   A U1 (both already scaled by the root);
-//   part[blockIdx][k][0] = sum_i s_k,i sum_j cv_kij^2,
-//   part[blockIdx][k][1] = sum_i y_i cv_ki0  (y NULL: 0).
-// u (3, N) and coef (3, 2, size), when given, add the rank-two term of the
-// reference-centred kernel: cv_kij += coef[k][0][j] + u_ki coef[k][1][j]
-// (leaveout_se.py:591-595, the two scalars u_k'v and 1'v scaled by 1/(2R)).
+//   part[blockIdx][q] (kSums values): q = k: sum_i s_k,i sum_j cv_kij^2;
+//   q = 3 + k: sum_i y_i cv_ki0 (y NULL: 0); q = 6 + k: see g below.
+// n_vec row vectors u (n_vec, 3, N) with coef (3, 1 + n_vec, size), when
+// given, add low-rank terms: cv_kij += coef[k][0][j] + sum_r u_rki
+// coef[k][1 + r][j] -- the rank-two term of the reference-centred kernel
+// (leaveout_se.py:591-595) and the deflation of C2 (:580-582).  g (3, N), when
+// given, adds sums[6 + k] = sum_i g_ki cv_ki0 (the covariance of b1 and theta1).
+constexpr int kMaxVec = 4;
+constexpr int kSums = 9;
+
 __global__ void __launch_bounds__(kThreads) k_c_sums(const double *v, int size, int per_component,
                                                      const double *b, const double *s,
                                                      const double *base, const double *thq,
-                                                     const double *y, const double *u,
-                                                     const double *coef, int64_t N, double *part)
+                                                     const double *y, int n_vec, const double *u,
+                                                     const double *coef, const double *g,
+                                                     int64_t N, double *part)
 {
-    __shared__ double s_red[kWarps][6];
+    __shared__ double s_red[kWarps][kSums];
     const int n_in = per_component ? 3 : 1;
     const int wide = (n_in + 3) * size;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    double acc[kSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < N;
          i += (int64_t)gridDim.x * kThreads) {
         const double *bs = base + i * wide;
@@ -153,7 +159,9 @@ __global__ void __launch_bounds__(kThreads) k_c_sums(const double *v, int size, 
             const double scale = per_component ? sqrt(fmax(sk, 0.0)) : 1.0;
             const int in0 = (per_component ? k : 0) * size;
             const int bc0 = (n_in + k) * size;
-            const double uk = u ? u[k * N + i] : 0.0;
+            double uk[kMaxVec];
+            for (int r = 0; r < n_vec; r++) uk[r] = u[((int64_t)r * 3 + k) * N + i];
+            const double *ck = coef ? coef + (int64_t)k * (1 + n_vec) * size : nullptr;
             double sq = 0.0;
             for (int j = 0; j < size; j++) {
                 const double vk = v[i * size + j] * scale;
@@ -161,34 +169,43 @@ __global__ void __launch_bounds__(kThreads) k_c_sums(const double *v, int size, 
                 const double Bv = tq[k * size + j];
                 const double M_bv = vk * bk - bs[bc0 + j];
                 double cv = Bv - 0.5 * (bk * Mv + M_bv);
-                if (u) cv += coef[(2 * k) * size + j] + uk * coef[(2 * k + 1) * size + j];
+                if (ck) {
+                    double low = ck[j];
+                    for (int r = 0; r < n_vec; r++) low += uk[r] * ck[(1 + r) * size + j];
+                    cv += low;
+                }
                 sq += cv * cv;
-                if (j == 0 && y) acc[3 + k] += y[i] * cv;
+                if (j == 0) {
+                    if (y) acc[3 + k] += y[i] * cv;
+                    if (g) acc[6 + k] += g[k * N + i] * cv;
+                }
             }
             acc[k] += sk * sq;
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int q = 0; q < 6; q++) {
+    for (int q = 0; q < kSums; q++) {
         const double t = warp_sum(acc[q]);
         if (lane == 0) s_red[warp][q] = t;
     }
     __syncthreads();
-    if (threadIdx.x < 6) {
+    if (threadIdx.x < kSums) {
         double t = 0.0;
         for (int wv = 0; wv < kWarps; wv++) t += s_red[wv][threadIdx.x];
-        part[(int64_t)blockIdx.x * 6 + threadIdx.x] = t;
+        part[(int64_t)blockIdx.x * kSums + threadIdx.x] = t;
     }
 }
 
+// out[q] for q < n = the sum over blocks of part[block * stride + q], one warp
+// per q, in a fixed order
 __global__ void __launch_bounds__(kThreads) k_sum_parts(const double *part, int blocks, int n,
-                                                        double *out)
+                                                        int stride, double *out)
 {
     const int lane = threadIdx.x & 31;
     const int q = (int)(((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5);
     if (q >= n) return;
     double t = 0.0;
-    for (int bl = lane; bl < blocks; bl += 32) t += part[(int64_t)bl * n + q];
+    for (int bl = lane; bl < blocks; bl += 32) t += part[(int64_t)bl * stride + q];
     t = warp_sum(t);
     if (lane == 0) out[q] = t;
 }
@@ -374,24 +391,28 @@ extern "C" int hdfe_bii_moments(const double *rows, int32_t size, const double *
 
 extern "C" int64_t hdfe_c_sums_workspace_bytes(void)
 {
-    return (int64_t)se::kSumGrid * 6 * 8;
+    return (int64_t)se::kSumGrid * se::kSums * 8;
 }
 
-extern "C" int hdfe_c_sums_rank_two(const double *v, int32_t size, int32_t per_component,
-                                    const double *b, const double *s, const double *base,
-                                    const double *through_q, const double *y, const double *u,
-                                    const double *coef, int64_t n_rows, double *sums,
-                                    void *workspace, int64_t workspace_bytes, void *stream)
+extern "C" int hdfe_c_sums_ext(const double *v, int32_t size, int32_t per_component,
+                               const double *b, const double *s, const double *base,
+                               const double *through_q, const double *y, int32_t n_vec,
+                               const double *u, const double *coef, const double *g,
+                               int64_t n_rows, double *sums, void *workspace,
+                               int64_t workspace_bytes, void *stream)
 {
     if (!v || size < 1 || !b || !s || !base || !through_q || n_rows < 1 || !sums || !workspace ||
-        workspace_bytes < hdfe_c_sums_workspace_bytes() || (u && !coef))
-        return hdfe_set_arg_error("hdfe_c_sums: bad argument");
+        workspace_bytes < hdfe_c_sums_workspace_bytes() || n_vec < 0 || n_vec > se::kMaxVec ||
+        (n_vec > 0 && !u))
+        return hdfe_set_arg_error("hdfe_c_sums: bad argument (0 <= n_vec <= 4)");
     cudaStream_t st = (cudaStream_t)stream;
     const unsigned grid = se::grid_for(n_rows, se::kThreads, se::kSumGrid);
     double *part = (double *)workspace;
     se::k_c_sums<<<grid, se::kThreads, 0, st>>>(v, size, per_component, b, s, base, through_q, y,
-                                                u, u ? coef : nullptr, n_rows, part);
-    se::k_sum_parts<<<1, se::kThreads, 0, st>>>(part, (int)grid, 6, sums);
+                                                coef ? n_vec : 0, u, coef, g, n_rows, part);
+    const int n_sums = g ? se::kSums : 6;
+    se::k_sum_parts<<<(n_sums + se::kWarps - 1) / se::kWarps, se::kThreads, 0, st>>>(
+        part, (int)grid, n_sums, se::kSums, sums);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(2);
     return HDFE_OK;
@@ -402,8 +423,8 @@ extern "C" int hdfe_c_sums(const double *v, int32_t size, int32_t per_component,
                            const double *y, int64_t n_rows, double *sums, void *workspace,
                            int64_t workspace_bytes, void *stream)
 {
-    return hdfe_c_sums_rank_two(v, size, per_component, b, s, base, through_q, y, nullptr,
-                                nullptr, n_rows, sums, workspace, workspace_bytes, stream);
+    return hdfe_c_sums_ext(v, size, per_component, b, s, base, through_q, y, 0, nullptr, nullptr,
+                           nullptr, n_rows, sums, workspace, workspace_bytes, stream);
 }
 
 extern "C" int hdfe_smooth_cells(const double *knots0, const double *knots1, const double *fp,

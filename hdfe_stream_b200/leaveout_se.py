@@ -25,7 +25,7 @@ Leaving out a match (leaveout_se.py:616-636), the rows are matches: b is zero
 on the stayers' matches, the divisor counts person-years, and the
 reference-centred estimator is the uncentred sqrt(w) y through
 K = C + (1 u' + u 1') / (2 R), u = M b (`m_times`, one more solve), whose
-two scalars per column ride into `hdfe_c_sums_rank_two`.
+two scalars per column ride into `hdfe_c_sums_ext`.
 """
 
 from __future__ import annotations
@@ -38,6 +38,7 @@ from .leaveout import MAX_BLOCK, InverseOperator
 COMPONENTS = ("var(psi)", "var(alpha)", "cov(psi, alpha)")
 QUANTILE_SAMPLE = 2_000_000         # rows sampled for the smoother's knots
 TRACE_SEED_OFFSET = 7_700_017       # leaveout_se.py:731
+WEAK_SEED_OFFSET = 8_800_021        # leaveout_se.py:757
 
 
 def _torch():
@@ -245,13 +246,15 @@ class StandardErrors:
         U_l, U_c, U_g = self._apply_inverse(levels, cov, gsum)
         return (b - self._readout(U_l, U_c, U_g, root=True).t()).contiguous()
 
-    def c_sums(self, v, b, s, per_component, y=None, u=None):
+    def c_sums(self, v, b, s, per_component, y=None, u=None, deflate=None, g=None):
         """leaveout_se.py:426-597 `_apply_c` with its sinks: C v for the three
         components (v (N, size) shared, or the draws z scaled per component by
         sqrt(max(s_k, 0)) when per_component), returned as sums[6]: per k the
         sum of s_k (C v)_k^2 over rows and draws, then of y (C v)_k.  With
         u = M b (3, N), the kernel is the reference-centred K = C +
-        (1 u' + u 1') / (2 N) (:536-543, :591-595)."""
+        (1 u' + u 1') / (2 N) (:536-543, :591-595); with deflate = (lambda (3,),
+        x1 (3, N)) B loses lambda_k x1_k x1_k' (:580-582); with g (3, N) sums
+        has 9 entries, the last three sum_i g_ki (C v)_ki0."""
         torch = _torch()
         size = int(v.shape[1])
         n_in = 3 if per_component else 1
@@ -260,12 +263,24 @@ class StandardErrors:
             ins = [v * scale[k][:, None] for k in range(3)]
         else:
             ins = [v]
-        coef = None
+        # the low-rank terms: per component a constant row and one row per vector
+        vecs, rows_c = [], [[torch.zeros(size, **self.f64)] for _ in range(3)]
         if u is not None:
             half = 0.5 / self.N
-            coef = torch.stack([torch.stack([(u[k] @ ins[k if per_component else 0]) * half,
-                                             ins[k if per_component else 0].sum(0) * half])
-                                for k in range(3)]).contiguous()
+            vecs.append(u)
+            for k in range(3):
+                vk = ins[k if per_component else 0]
+                rows_c[k][0] = (u[k] @ vk) * half
+                rows_c[k].append(vk.sum(0) * half)
+        if deflate is not None:
+            lams, x1 = deflate
+            vecs.append(x1)
+            for k in range(3):
+                vk = ins[k if per_component else 0]
+                rows_c[k].append(-float(lams[k]) * (x1[k] @ vk))
+        coef = None
+        if vecs:
+            coef = torch.stack([torch.stack(r) for r in rows_c]).contiguous()
         stack = torch.cat(ins + [ins[k if per_component else 0] * b[k][:, None]
                                  for k in range(3)], 1)
         if self.inv_root is not None:
@@ -284,17 +299,18 @@ class StandardErrors:
                                                q_g)
         base = self._readout(U0_l, U0_c, U0_g, root=True)
         thq = self._readout(U1_l, U1_c, U1_g, root=True)
-        sums = torch.empty(6, **self.f64)
+        sums = torch.empty(9 if g is not None else 6, **self.f64)
         assert n_in * size + 3 * size == base.shape[1]
         v, b, s = v.contiguous(), b.contiguous(), s.contiguous()
         y = None if y is None else y.contiguous()
-        u = None if u is None else u.contiguous()
-        _lib.check(_lib.lib().hdfe_c_sums_rank_two(
+        g = None if g is None else g.contiguous()
+        uv = torch.stack(vecs).contiguous() if vecs else None
+        _lib.check(_lib.lib().hdfe_c_sums_ext(
             v.data_ptr(), size, int(bool(per_component)), b.data_ptr(), s.data_ptr(),
-            base.data_ptr(), thq.data_ptr(), None if y is None else y.data_ptr(),
-            None if u is None else u.data_ptr(), None if coef is None else coef.data_ptr(),
-            self.N, sums.data_ptr(), self._ws.data_ptr(), self._ws.numel(),
-            _lib.stream_handle()))
+            base.data_ptr(), thq.data_ptr(), None if y is None else y.data_ptr(), len(vecs),
+            None if uv is None else uv.data_ptr(), None if coef is None else coef.data_ptr(),
+            None if g is None else g.data_ptr(), self.N, sums.data_ptr(), self._ws.data_ptr(),
+            self._ws.numel(), _lib.stream_handle()))
         return sums
 
     # ---- the smoother of sigma2 (leaveout_se.py:982-1054)
@@ -344,15 +360,20 @@ class StandardErrors:
 
     def component_variances(self, sigma2, leverage, complement, factor, b_ii=None,
                             n_draws=250, block=8, seed=0, trace=True, smooth_bins=None,
-                            stayer_rows=None, centering="weighted", reported=(0, 1, 2)):
+                            stayer_rows=None, centering="weighted", reported=(0, 1, 2),
+                            weak_id=None, weak_components=None, sigma2_point=None):
         """leaveout_se.py:599-784 `component_variances`: {"se", "variance",
-        "first_term", "trace_term", "theta", "se_conservative"} per
+        "first_term", "trace_term", "theta", "se_conservative", "weak"} per
         component.  sigma2, leverage, complement and factor come from
         `leave_out_components` / `jla_leverages`; b_ii from `bii_rows`
         (computed here with the same draws when None).  Leaving out a match:
         `stayer_rows` (bool, N) zeroes b on the stayers' matches,
         centering "reference" applies the rank-two kernel to the uncentred
-        outcome, and components outside `reported` are NaN."""
+        outcome, and components outside `reported` are NaN.  With `weak_id`
+        (`weakid.weak_id_diagnostics`), "weak" holds the q = 1 moments
+        (`weak_moments`, seed + 8_800_021) of the flagged components (by
+        default those with q >= 1; at match level var(psi) alone), sigma2_point
+        the point estimate's sigma2 when `sigma2` is another (:737-759)."""
         torch = _torch()
         f64 = self.f64
         sigma2 = torch.as_tensor(sigma2).to(**f64)
@@ -393,11 +414,24 @@ class StandardErrors:
                 drawn += size
                 blocks += 1
             tr /= n_draws
+        names = list(COMPONENTS)
+        weak = None
+        if weak_id is not None:
+            if weak_components is None:
+                weak_components = [k for k in range(3) if weak_id["q"][k] >= 1]
+            weak_components = [k for k in weak_components
+                               if k in reported and (stayer_rows is None or k == 0)]
+            if weak_components:
+                point = sigma2 if sigma2_point is None else \
+                    torch.as_tensor(sigma2_point).to(**f64)
+                weak = self.weak_moments(point, s, b_ii, complement, factor, weak_id,
+                                         weak_components, n_draws, block,
+                                         int(seed) + WEAK_SEED_OFFSET, stayer_rows, centering)
+                weak = {names[k]: v for k, v in weak.items()}
         variance = first - 2.0 * tr
         for k in range(3):
             if k not in reported:
                 variance[k] = first[k] = tr[k] = theta[k] = np.nan
-        names = list(COMPONENTS)
         return {"se": {n: float(np.sqrt(v)) if v > 0 else float("nan")
                        for n, v in zip(names, variance)},
                 "variance": dict(zip(names, variance.tolist())),
@@ -406,4 +440,85 @@ class StandardErrors:
                 "theta": dict(zip(names, theta.tolist())),
                 "se_conservative": {n: float(np.sqrt(f)) if f > 0 else float("nan")
                                     for n, f in zip(names, first)},
-                "n_draws": n_draws if trace else 0, "blocks": blocks}
+                "n_draws": n_draws if trace else 0, "blocks": blocks, "weak": weak}
+
+    def weak_moments(self, sigma2, s, b_ii, complement, factor, weak_id, components, n_draws,
+                     block, seed, stayer_rows=None, centering="weighted"):
+        """leaveout_se.py:786-888 `_weak_moments`: per flagged component k
+        {"lambda_1", "b1", "v_raw", "sigma" (2x2), "conservative", "trace",
+        "quadratic"}: b1 = x1' y~ with x1 = sqrt(w) A u1 (u1 the leading
+        direction), v_raw = sum x1^2 sigma2, and the covariance of (b1,
+        theta1) from the deflated kernel C2 (B2 = B - lambda_1 x1 x1', b2 from
+        diag(B2), the low-rank terms of `c_sums`), s the smoothed sigma2
+        floored at zero; the first term alone where subtracting the trace
+        leaves the matrix indefinite."""
+        torch = _torch()
+        f64 = self.f64
+        lams = np.array([float(e[0]) if len(e) else 0.0 for e in weak_id["eigenvalues"]])
+        U = weak_id["lead_vectors"]
+        x1 = self._readout(U[0], U[1], U[2], root=True).t().contiguous()       # (3, N)
+        op = self.op
+        y = op.rows.V[0]
+        w = op.w if op.w is not None else torch.ones(self.N, **f64)
+        root = torch.sqrt(w)
+        y_bar = float((w @ y).item() / w.sum().item())
+        yt = root * (y - y_bar)
+        flo = torch.clamp(s, min=0.0).contiguous()
+        b1 = (x1 @ yt).cpu().numpy()
+        v_raw = ((x1 * x1) @ sigma2).cpu().numpy()
+        s11 = (x1 * x1 * flo).sum(dim=1).cpu().numpy()
+        lam_d = torch.as_tensor(lams, **f64)
+        b2 = (b_ii - lam_d[:, None] * x1 * x1) * (factor / complement)[None, :]
+        if stayer_rows is not None:
+            keep = ~torch.as_tensor(stayer_rows, device=self.dev).to(torch.bool)
+            b2 = torch.where(keep[None, :], b2, torch.zeros_like(b2))
+        b2 = b2.contiguous()
+        u2 = self.m_times(b2) if centering == "reference" else None
+        shift = y_bar if centering == "weighted" else 0.0
+        y_c = (root * (y - shift)).contiguous()
+        deflate = (lams, x1)
+        sums = self.c_sums(y_c[:, None].contiguous(), b2, flo, False, y=y_c, u=u2,
+                           deflate=deflate, g=(x1 * flo)).cpu().numpy()
+        first, quad, s12 = 4.0 * sums[:3], sums[3:6], 2.0 * sums[6:9]
+        # the trace with only the flagged components drawn (leaveout_se.py:890-930
+        # `_cc_trace`, clamp=True): the others get a zero input and weight
+        mask = torch.zeros(3, **f64)
+        mask[list(components)] = 1.0
+        flo_m = (flo * mask[:, None]).contiguous()
+        trace = np.zeros(3)
+        block = int(min(max(int(block), 1), MAX_BLOCK))
+        drawn = 0
+        while drawn < n_draws:
+            size = min(block, n_draws - drawn)
+            z = self._draws(size, int(seed), drawn)
+            trace += self.c_sums(z, b2, flo_m, True, u=u2, deflate=deflate).cpu().numpy()[:3]
+            drawn += size
+        trace /= n_draws
+        out = {}
+        for k in components:
+            s22 = first[k] - 2.0 * trace[k]
+            conservative = not (s22 > 0 and s12[k] ** 2 < s11[k] * s22)
+            if conservative:
+                s22 = first[k]
+            out[k] = {"lambda_1": float(lams[k]), "b1": float(b1[k]), "v_raw": float(v_raw[k]),
+                      "sigma": np.array([[s11[k], s12[k]], [s12[k], s22]]),
+                      "conservative": bool(conservative), "trace": float(trace[k]),
+                      "quadratic": float(quad[k])}
+        return out
+
+
+def weak_intervals(leave_out, weak, confidence=0.95):
+    """leaveout.py:774-791: for each flagged component, theta1 = the
+    leave-out estimate less lambda_1 (b1^2 - v_raw), and the q = 1 interval
+    (`am_interval.am_interval`) around it; `leave_out` maps the component
+    names (or indexes 0..2) to the estimates.  Adds "theta1", "interval",
+    "confidence", "kappa", "z", "rho" to each piece of `weak` and returns it."""
+    from .am_interval import am_interval
+    for name, piece in (weak or {}).items():
+        k = COMPONENTS.index(name)
+        est = leave_out[name] if isinstance(leave_out, dict) else leave_out[k]
+        theta1 = float(est) - piece["lambda_1"] * (piece["b1"] ** 2 - piece["v_raw"])
+        lo, hi, info = am_interval(piece["lambda_1"], piece["b1"], theta1, piece["sigma"],
+                                   1.0 - confidence)
+        piece.update(theta1=theta1, interval=(lo, hi), confidence=confidence, **info)
+    return weak

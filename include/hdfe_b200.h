@@ -378,12 +378,15 @@ int hdfe_kss_sigma2(const double *y, const double *w, const double *resid,
  *   per component sum_i s_k,i sum_j cv_kij^2, then sum_i y_i cv_ki0 (y NULL:
  *   0).  per_component: v is the draws z (N, size) and component k's input is
  *   z sqrt(max(s_k, 0)); else v (N, size) is shared.  Deterministic.
- * hdfe_c_sums_rank_two: hdfe_c_sums for the reference-centred kernel of the
- *   match level (leaveout_se.py:616-636, :536-543, :591-595):
- *   K = C + (1 u' + u 1') / (2 R), u (3, N) = M b per component; coef
- *   (3, 2, size) holds per component and column u_k'v / (2R), then
- *   1'v / (2R), so that cv_kij gains coef[k][0][j] + u_ki coef[k][1][j].
- *   u NULL: exactly hdfe_c_sums.
+ * hdfe_c_sums_ext: hdfe_c_sums with low-rank terms added to C v and one
+ *   more sum.  n_vec (<= 4) row vectors u (n_vec, 3, N) and coef
+ *   (3, 1 + n_vec, size): cv_kij += coef[k][0][j] + sum_r u_rki
+ *   coef[k][1 + r][j] -- the reference-centred kernel of the match level,
+ *   K = C + (1 u' + u 1') / (2R) with u = M b (leaveout_se.py:616-636,
+ *   :536-543, :591-595), and the deflated kernel C2 = C - lambda_1 x1 x1' +
+ *   ... of the q = 1 interval (:580-582, :786-876).  g (3, N) non-NULL: sums
+ *   has 9 entries, sums[6 + k] = sum_i g_ki cv_ki0.  coef NULL: exactly
+ *   hdfe_c_sums.
  * hdfe_smooth_cells / hdfe_smooth_eval: leaveout_se.py:982-1054: each row's
  *   cell in the grid of the quantile knots (knots0 of the leverage, knots1 of
  *   B_ii or NULL for one axis; fp the rank of each knot, n_bins + 1 values
@@ -410,10 +413,11 @@ int hdfe_c_sums(const double *v, int32_t size, int32_t per_component, const doub
                 int64_t n_rows, double *sums, void *workspace, int64_t workspace_bytes,
                 void *stream);
 
-int hdfe_c_sums_rank_two(const double *v, int32_t size, int32_t per_component, const double *b,
-                         const double *s, const double *base, const double *through_q,
-                         const double *y, const double *u, const double *coef, int64_t n_rows,
-                         double *sums, void *workspace, int64_t workspace_bytes, void *stream);
+int hdfe_c_sums_ext(const double *v, int32_t size, int32_t per_component, const double *b,
+                    const double *s, const double *base, const double *through_q,
+                    const double *y, int32_t n_vec, const double *u, const double *coef,
+                    const double *g, int64_t n_rows, double *sums, void *workspace,
+                    int64_t workspace_bytes, void *stream);
 
 int hdfe_smooth_cells(const double *knots0, const double *knots1, const double *fp,
                       int32_t n_bins, const double *leverage, const double *b_ii,

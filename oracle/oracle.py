@@ -1139,11 +1139,12 @@ class Design:
         base = readout(self.starts, self.codes, self.cells.offs, self.X, U_l, U_c, U_g)
         return b - (root[:, None] * base).T
 
-    def apply_c(self, v, b, per_component, layout, rank_two=None):
-        """leaveout_se.py:426-597 `_apply_c` (no deflation): C v = B v -
-        (b .* M v + M (b .* v)) / 2 for each component, v (N, size) shared or
-        (N, 3, size) one per component; (N, 3, size).  rank_two = (u (3, N),
-        scale) adds scale (1 u_k' + u_k 1') v (:536-543, :591-595)."""
+    def apply_c(self, v, b, per_component, layout, rank_two=None, deflate=None):
+        """leaveout_se.py:426-597 `_apply_c`: C v = B v - (b .* M v +
+        M (b .* v)) / 2 for each component, v (N, size) shared or (N, 3, size)
+        one per component; (N, 3, size).  rank_two = (u (3, N), scale) adds
+        scale (1 u_k' + u_k 1') v (:536-543, :591-595); deflate = (lambda (3,),
+        x1 (N, 3)) takes lambda_k x1_k x1_k' v off B v (:532-535, :580-582)."""
         N, L, G, c = self.rows.n_rows, self.cells.L, len(self.starts) - 1, self.X.shape[1]
         n_in = 3 if per_component else 1
         size = v.shape[-1]
@@ -1179,6 +1180,9 @@ class Design:
             vk = part(k)
             Mv = vk - root[:, None] * base[:, in_cols(k)]
             Bv = root[:, None] * through_q[:, k * size:(k + 1) * size]
+            if deflate is not None:
+                lams, x1 = deflate
+                Bv = Bv - lams[k] * np.outer(x1[:, k], x1[:, k] @ vk)
             M_bv = vk * b[k][:, None] - root[:, None] * base[:, b_cols(k)]
             cv[:, k, :] = Bv - 0.5 * (b[k][:, None] * Mv + M_bv)
             if rank_two is not None:
@@ -1188,7 +1192,8 @@ class Design:
 
     def component_variances(self, sigma2, leverage, complement, factor, b_ii, n_draws,
                             block, seed, smooth_bins=None, stayer_rows=None,
-                            centering="weighted", reported=(0, 1, 2)):
+                            centering="weighted", reported=(0, 1, 2), weak_id=None,
+                            weak_components=None, sigma2_point=None):
         """leaveout_se.py:599-784 `component_variances` (trace included, no
         weak-identification pieces): per component the first term
         4 sum s~ (C y~)^2, the trace term 2 tr(C Om~ C Om~) by Hutchinson
@@ -1230,12 +1235,84 @@ class Design:
                 trace[k] += float(sig[k] @ (cvt[:, k, :] ** 2).sum(axis=1))
             drawn += size
         trace /= n_draws
+        # :737-759: the q = 1 pieces for the components the diagnostic flags
+        weak = None
+        if weak_id is not None:
+            if weak_components is None:
+                weak_components = [k for k in range(3) if weak_id["q"][k] >= 1]
+            weak_components = [k for k in weak_components
+                               if k in reported and (stayer_rows is None or k == 0)]
+            if weak_components:
+                weak = self.weak_moments(sigma2 if sigma2_point is None else sigma2_point,
+                                         sig, b_ii, complement, factor, weak_id,
+                                         weak_components, n_draws, block, seed + 8_800_021,
+                                         layout, stayer_rows, centering)
         variance = first - 2.0 * trace
         for k in range(3):
             if k not in reported:
                 variance[k] = first[k] = trace[k] = theta[k] = np.nan
         return {"variance": variance, "first_term": first,
-                "trace_term": 2.0 * trace, "theta": theta}
+                "trace_term": 2.0 * trace, "theta": theta, "weak": weak}
+
+    def weak_moments(self, sigma2, sig, b_ii, complement, factor, weak_id, components, n_draws,
+                     block, seed, layout, stayer_rows=None, centering="weighted"):
+        """leaveout_se.py:786-888 `_weak_moments`: per flagged component the
+        leading direction's estimate b1 = x1' y~ (x1 = sqrt(w) A u1), its raw
+        variance sum x1^2 sigma2, and the 2x2 covariance of (b1, theta1) from
+        the deflated kernel C2 (B2 = B - lambda_1 x1 x1', b2 from diag(B2)),
+        sigma2 smoothed and floored at zero; the first term alone when the
+        trace leaves it indefinite."""
+        N = self.rows.n_rows
+        lams = np.array([float(e[0]) if len(e) else 0.0 for e in weak_id["eigenvalues"]])
+        U = weak_id["lead_vectors"]
+        root = np.sqrt(self.w)
+        x1 = root[:, None] * readout(self.starts, self.codes, self.cells.offs, self.X, U[0],
+                                     U[1], U[2])
+        y = self.rows.V[:, 0]
+        y_bar = float(self.w @ y / self.w.sum())
+        yt = root * (y - y_bar)
+        flo = [np.maximum(sk, 0.0) for sk in sig]
+        b1 = x1.T @ yt
+        v_raw = (x1 ** 2).T @ np.asarray(sigma2, float)
+        s11 = np.array([(x1[:, k] ** 2) @ flo[k] for k in range(3)])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv_m = factor / complement
+        b2 = np.stack([(b_ii[k] - lams[k] * x1[:, k] ** 2) * inv_m for k in range(3)])
+        if stayer_rows is not None:
+            b2[:, np.asarray(stayer_rows, bool)] = 0.0
+        rank_two = (self.m_times(b2), 0.5 / N) if centering == "reference" else None
+        shift = y_bar if centering == "weighted" else 0.0
+        y_c = root * (y - shift)
+        deflate = (lams, x1)
+        cv = self.apply_c(y_c[:, None], b2, False, layout, rank_two, deflate)
+        s12 = np.array([2.0 * float((x1[:, k] * flo[k]) @ cv[:, k, 0]) for k in range(3)])
+        first = np.array([4.0 * float(flo[k] @ (cv[:, k, 0] ** 2)) for k in range(3)])
+        quad = np.array([float(y_c @ cv[:, k, 0]) for k in range(3)])
+        # :890-930 `_cc_trace` with clamp and only the flagged components drawn
+        trace = np.zeros(3)
+        drawn = 0
+        while drawn < n_draws:
+            size = min(block, n_draws - drawn)
+            z = rademacher(0, N, size, seed, drawn)
+            v = np.zeros((N, 3, size))
+            for k in components:
+                v[:, k, :] = z * np.sqrt(flo[k])[:, None]
+            cvt = self.apply_c(v, b2, True, layout, rank_two, deflate)
+            for k in components:
+                trace[k] += float(flo[k] @ (cvt[:, k, :] ** 2).sum(axis=1))
+            drawn += size
+        trace /= n_draws
+        out = {}
+        for k in components:
+            s22 = first[k] - 2.0 * trace[k]
+            conservative = not (s22 > 0 and s12[k] ** 2 < s11[k] * s22)
+            if conservative:
+                s22 = first[k]
+            out[k] = {"lambda_1": float(lams[k]), "b1": float(b1[k]), "v_raw": float(v_raw[k]),
+                      "sigma": np.array([[s11[k], s12[k]], [s12[k], s22]]),
+                      "conservative": bool(conservative), "trace": float(trace[k]),
+                      "quadratic": float(quad[k])}
+        return out
 
     def jla_leverages(self, n_draws, block, seed):
         """leaveout.py:130-198 `jla_leverages` and :210-282

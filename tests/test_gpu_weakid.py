@@ -89,3 +89,34 @@ def test_weak_id_on_a_weighted_panel_matches_oracle(device):
     assert rel(out["sum_sq"], ref["sum_sq"]) < 1e-6
     assert list(out["q"]) == list(ref["q"])
     assert rel(out["f_stat"], ref["f_stat"]) < 1e-6
+
+
+def test_weak_moments_and_interval_match_reference(device):
+    """The q = 1 pieces on the device (`component_variances` with the
+    diagnostic: b1, its raw variance, the 2x2 covariance of (b1, theta1)
+    from the deflated kernel C2) and the interval formed from them against
+    the reference on the low-mobility panel, where all three components are
+    flagged."""
+    from hdfe_stream_b200.leaveout_se import COMPONENTS, weak_intervals
+    from hdfe_stream_b200.weakid import weak_id_diagnostics
+    g = load_golden("weakid")
+    name = "low_mobility"
+    _, se = golden_se(g, name)
+    wid = weak_id_diagnostics(se, g[f"{name}_sigma2"], g[f"{name}_leverage"], n_draws=48,
+                              block=12, seed=9)
+    out = se.component_variances(g[f"{name}_sigma2"], g[f"{name}_leverage"],
+                                 g[f"{name}_complement"], g[f"{name}_factor"], None, n_draws=16,
+                                 block=8, seed=6, weak_id=wid)
+    for f in ("variance", "first_term", "trace_term", "theta"):
+        assert rel([out[f][n] for n in COMPONENTS], g[f"{name}_se_{f}"]) < 1e-7, f
+    flagged = [int(k) for k in g[f"{name}_weak_components"]]
+    assert sorted(COMPONENTS.index(n) for n in out["weak"]) == flagged
+    leave_out = g[f"{name}_weak_leave_out"]
+    weak = weak_intervals(leave_out, out["weak"], 0.95)
+    for k in flagged:
+        piece = weak[COMPONENTS[k]]
+        for f in ("lambda_1", "b1", "v_raw", "trace", "quadratic"):
+            assert rel(piece[f], g[f"{name}_weak{k}_{f}"]) < 1e-6, f
+        assert rel(piece["sigma"], g[f"{name}_weak{k}_sigma"]) < 1e-6
+        want = g[f"{name}_weak{k}_interval"]
+        assert rel([*piece["interval"], piece["kappa"], piece["z"]], want[:4]) < 1e-6

@@ -368,3 +368,50 @@ def test_weak_id_diagnostics_match_reference(name):
     assert rel(out["sum_sq_se"], g[f"{name}_sum_sq_se"]) < 1e-8
     assert list(out["q"]) == list(g[f"{name}_q"])
     assert rel(out["f_stat"], g[f"{name}_f_stat"]) < 1e-10
+
+
+def test_weak_moments_match_reference():
+    """leaveout_se.py `_weak_moments` (b1, its raw variance, the 2x2
+    covariance of (b1, theta1) from the deflated kernel C2) for the
+    components the diagnostic flags on the low-mobility panel, and the
+    standard errors beside them, against the reference's own outputs."""
+    g = load_golden("weakid")
+    name = "low_mobility"
+    rows = se_rows(g, name)
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), tol=float(g[f"{name}_tol"][0]))
+    wid = orc.weak_id_diagnostics(des, g[f"{name}_sigma2"], g[f"{name}_leverage"], n_draws=48,
+                                  block=12, seed=9)
+    b_ii = des.bii_rows(16, 8, 6)
+    out = des.component_variances(g[f"{name}_sigma2"], g[f"{name}_leverage"],
+                                  g[f"{name}_complement"], g[f"{name}_factor"], b_ii, 16, 8, 6,
+                                  weak_id=wid)
+    for f in ("variance", "first_term", "trace_term", "theta"):
+        assert rel(out[f], g[f"{name}_se_{f}"]) < 1e-10, f
+    flagged = list(g[f"{name}_weak_components"])
+    assert sorted(out["weak"]) == flagged and flagged
+    for k in flagged:
+        piece = out["weak"][k]
+        for f in ("lambda_1", "b1", "v_raw", "trace", "quadratic"):
+            assert rel(piece[f], g[f"{name}_weak{k}_{f}"]) < 1e-10, f
+        assert rel(piece["sigma"], g[f"{name}_weak{k}_sigma"]) < 1e-10
+        assert piece["conservative"] == bool(g[f"{name}_weak{k}_conservative"][0])
+
+
+def test_am_interval_matches_reference():
+    """The q = 1 interval (am_interval.py `am_interval`: the Andrews-
+    Mikusheva critical value for KSS's curvature and the range of
+    lambda_1 b^2 + t over the ellipse) against the reference on fixed inputs
+    across curvatures and on the low-mobility panel's moments."""
+    from hdfe_stream_b200.am_interval import am_interval
+    g = load_golden("weakid")
+    for lam, b1, th, s00, s01, s11, alpha, lo, hi, kap, z in g["am_cases"]:
+        l2, h2, info = am_interval(lam, b1, th, [[s00, s01], [s01, s11]], alpha)
+        assert rel([l2, h2, info["kappa"], info["z"]], [lo, hi, kap, z]) < 1e-12
+    name = "low_mobility"
+    for k in g[f"{name}_weak_components"]:
+        lam, b1 = g[f"{name}_weak{k}_lambda_1"][0], g[f"{name}_weak{k}_b1"][0]
+        theta1 = g[f"{name}_weak_leave_out"][k] - lam * (b1 ** 2 - g[f"{name}_weak{k}_v_raw"][0])
+        lo, hi, info = am_interval(lam, b1, theta1, g[f"{name}_weak{k}_sigma"], 0.05)
+        want = g[f"{name}_weak{k}_interval"]
+        assert rel([lo, hi, info["kappa"], info["z"], info["rho"]], want) < 1e-12
