@@ -475,8 +475,9 @@ def run_batched(args, rank):
 
 
 def run_e2e(args, rows, dist):
-    """Same metric through fit.fit_rows-style calls with pinned host buffers:
-    every step copies the rows host->device and the fixed effects back."""
+    """Same metric through `fit.fit_host` with pinned host buffers: every
+    step copies the rows host->device (the outcome's upload overlapped with
+    the structure-only pass 1 and the S build) and the fixed effects back."""
     import torch
     from hdfe_stream_b200 import fit
 
@@ -485,15 +486,16 @@ def run_e2e(args, rows, dist):
         "codes": torch.from_numpy(np.ascontiguousarray(rows.codes).view(np.int32)).pin_memory(),
         "V": torch.from_numpy(np.ascontiguousarray(rows.V.T)).pin_memory(),
     }
+    if rows.w is not None:
+        pinned["w"] = torch.from_numpy(np.ascontiguousarray(rows.w, dtype=np.float64)).pin_memory()
     h2d = sum(t.numel() * t.element_size() for t in pinned.values())
     out_host = None
     d2h = 0
 
     def step():
         nonlocal out_host, d2h
-        dev = {k: v.to("cuda", non_blocking=True) for k, v in pinned.items()}
-        drows = fit.DeviceRows(dev["gcode"], dev["codes"], dev["V"], None, list(rows.n_levels))
-        res = fit.fit(drows, tol=args.tol)
+        res = fit.fit_host(pinned["gcode"], pinned["codes"], pinned["V"], rows.n_levels,
+                           w=pinned.get("w"), tol=args.tol)
         if out_host is None:
             out_host = torch.empty(res.gamma.shape, dtype=res.gamma.dtype, pin_memory=True)
         out_host.copy_(res.gamma, non_blocking=True)

@@ -821,7 +821,7 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     HDFE_CUDA_TRY(cudaMemsetAsync(obs, 0, L * 8, s));
     HDFE_CUDA_TRY(cudaMemsetAsync(cnt, 0, L * 8, s));
     HDFE_CUDA_TRY(cudaMemsetAsync(diag, 0, L * 8, s));
-    HDFE_CUDA_TRY(cudaMemsetAsync(rhs, 0, L * m * 8, s));
+    if (m > 0) HDFE_CUDA_TRY(cudaMemsetAsync(rhs, 0, L * m * 8, s));
     if (lcount) {
         HDFE_CUDA_TRY(cudaMemsetAsync(lcount, 0, L * 4, s));
         HDFE_CUDA_TRY(cudaMemsetAsync(work, 0, L * 8, s));

@@ -114,7 +114,9 @@ def pass1(rows: DeviceRows, keep_sums: bool = False, stream=None) -> DeviceCells
     nlev = np.asarray(rows.n_levels, dtype=np.int64)
     ws_bytes = lib.hdfe_pass1_workspace_bytes(N, m, int(keep_sums))
     ws = torch.empty(int(ws_bytes), dtype=torch.uint8, device=dev)
-    means, raw_ss = torch.empty(m, **f64), torch.empty(m, **f64)
+    # one slot at least: a structure-only pass (m = 0) still passes valid pointers
+    means_buf, ss_buf = torch.empty(max(m, 1), **f64), torch.empty(max(m, 1), **f64)
+    means, raw_ss = means_buf[:m], ss_buf[:m]
     starts = torch.empty(N + 1, dtype=torch.int64, device=dev)
     ccodes = torch.empty((N, D), dtype=torch.int32, device=dev)
     cn = torch.empty(N, **f64)
@@ -127,8 +129,8 @@ def pass1(rows: DeviceRows, keep_sums: bool = False, stream=None) -> DeviceCells
     counts = torch.zeros(6, dtype=torch.int64, device=dev)
     _lib.check(lib.hdfe_pass1(
         rows.gcode.data_ptr(), rows.codes.data_ptr(), D, rows.V.data_ptr(), m,
-        None if rows.w is None else rows.w.data_ptr(), N, nlev.ctypes.data, means.data_ptr(),
-        raw_ss.data_ptr(), starts.data_ptr(), ccodes.data_ptr(), cn.data_ptr(),
+        None if rows.w is None else rows.w.data_ptr(), N, nlev.ctypes.data, means_buf.data_ptr(),
+        ss_buf.data_ptr(), starts.data_ptr(), ccodes.data_ptr(), cn.data_ptr(),
         None if csums is None else csums.data_ptr(), gn.data_ptr(), obs.data_ptr(),
         cnt.data_ptr(), diag.data_ptr(), rhs.data_ptr(), lcount.data_ptr(), work.data_ptr(),
         counts.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream_handle(stream)))
@@ -337,6 +339,63 @@ def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None,
         cells = pass1(rows)
     with timer("sbuild"):
         S = build_s(cells)
+    with timer("solve"):
+        return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision)
+
+
+_COPY_STREAMS = {}
+
+
+def _copy_stream(dev):
+    torch = _torch()
+    key = dev.index
+    if key not in _COPY_STREAMS:
+        _COPY_STREAMS[key] = torch.cuda.Stream(device=dev)
+    return _COPY_STREAMS[key]
+
+
+def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_block=8,
+             timer=None, precision="fp64") -> FitResult:
+    """The fit from host tensors in pass 0's layout -- gcode (N,) int32,
+    codes (N, D) int32, V (m, N) float64, w (N,) float64 or None, pinned for
+    the copies to overlap -- with the upload overlapped with the work that
+    needs no outcome: the group and level structure (and the weights) are
+    copied first; while V follows on a copy stream, pass 1 runs on the
+    structure alone (m = 0: cells, counts, diag) and S is built from it; then
+    pass 1 runs again with V for the right-hand sides and the solve follows.
+    S depends on the structure only and comes out identical to `fit`'s; the
+    right-hand sides are pass 1's own (its level sums are atomic, so their
+    last bits vary from run to run exactly as they do in `fit`)."""
+    torch = _torch()
+    timer = timer or _NoTimer()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    compute = torch.cuda.current_stream(dev)
+    copy = _copy_stream(dev)
+    copy.wait_stream(compute)       # the buffers it writes may be freed memory of compute's
+    with torch.cuda.stream(copy):
+        g_d = gcode.to(dev, non_blocking=True)
+        c_d = codes.to(dev, non_blocking=True)
+        w_d = None if w is None else w.to(dev, non_blocking=True)
+        structure = torch.cuda.Event()
+        structure.record(copy)
+        V_d = V.to(dev, non_blocking=True)
+        values = torch.cuda.Event()
+        values.record(copy)
+    compute.wait_event(structure)
+    for t in (g_d, c_d, w_d):
+        if t is not None:
+            t.record_stream(compute)
+    n_levels = list(n_levels)
+    empty = torch.empty((0, int(g_d.shape[0])), dtype=torch.float64, device=dev)
+    with timer("pass1"):
+        shape = pass1(DeviceRows(g_d, c_d, empty, w_d, n_levels))
+    with timer("sbuild"):
+        S = build_s(shape)
+    del shape
+    compute.wait_event(values)
+    V_d.record_stream(compute)
+    with timer("pass1"):
+        cells = pass1(DeviceRows(g_d, c_d, V_d, w_d, n_levels))
     with timer("solve"):
         return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision)
 

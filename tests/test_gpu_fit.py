@@ -204,3 +204,31 @@ def test_pair_components_rejects_unsorted_rows(device):
     b = torch.tensor([0, 0, 1], dtype=torch.int32, device=device)
     with pytest.raises(_lib.HDFEError):
         pair_components(a, b, 2, 2)
+
+
+@pytest.mark.parametrize("name,rows", PANELS, ids=[p[0] for p in PANELS])
+def test_fit_from_host_equals_device_fit(device, name, rows):
+    """`fit.fit_host` (the upload overlapped with the structure-only pass 1
+    and the S build) gives the same S, bit for bit, as `fit.fit` on rows
+    already on the device, and the same right-hand sides and fixed effects up
+    to the rounding of pass 1's atomic level sums."""
+    import torch
+    from hdfe_stream_b200 import fit
+    pin = {"gcode": torch.from_numpy(rows.gcode.astype(np.uint32).view(np.int32)).pin_memory(),
+           "codes": torch.from_numpy(np.ascontiguousarray(rows.codes.astype(np.uint32))
+                                     .view(np.int32)).pin_memory(),
+           "V": torch.from_numpy(np.ascontiguousarray(rows.V.T)).pin_memory()}
+    w = None if rows.w is None else torch.from_numpy(rows.w.astype(np.float64)).pin_memory()
+    got = fit.fit_host(pin["gcode"], pin["codes"], pin["V"], rows.n_levels, w=w, tol=1e-12)
+    want = fit.fit(fit.DeviceRows.from_rows(rows), tol=1e-12)
+    assert torch.equal(got.S.indptr, want.S.indptr)
+    assert torch.equal(got.S.indices, want.S.indices)
+    assert torch.equal(got.S.data, want.S.data)
+    def rel(a, b):
+        return float((a - b).abs().max() / b.abs().max())
+    assert rel(got.cells.rhs, want.cells.rhs) < 1e-13
+    assert torch.equal(got.cells.diag, want.cells.diag) or rel(got.cells.diag,
+                                                               want.cells.diag) < 1e-13
+    assert rel(got.gamma, want.gamma) < 1e-9
+    its = np.atleast_1d(got.info["iterations"]) - np.atleast_1d(want.info["iterations"])
+    assert np.all(np.abs(its) <= 1)
