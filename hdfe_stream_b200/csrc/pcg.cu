@@ -252,8 +252,10 @@ __device__ __forceinline__ void row_products(const Params &a, const T *vals, con
             c[u] = 0;
             d[u] = T(0);
             if (e < re) {
-                c[u] = __ldg(a.indices + e);
-                d[u] = __ldg(vals + e);
+                // S streams through once per iteration: evict-first loads, so
+                // that it does not push the vectors (P, X, R, AP) out of L2
+                c[u] = __ldcs(a.indices + e);
+                d[u] = __ldcs(vals + e);
             }
         }
 #pragma unroll
