@@ -216,6 +216,31 @@ def components(cells: DeviceCells, col: int = 0, stream=None):
     return root, out
 
 
+_SIDE_STREAMS = {}
+
+
+def components_async(cells: DeviceCells, col: int = 0):
+    """`components` on a side stream, so that it runs beside the S build (it
+    reads only pass 1's groups and codes).  Returns (root, out, event); wait
+    on the event before reading root or out."""
+    torch = _torch()
+    dev = cells.starts.device
+    main = torch.cuda.current_stream(dev)
+    if dev.index not in _SIDE_STREAMS:
+        _SIDE_STREAMS[dev.index] = torch.cuda.Stream(device=dev)
+    side = _SIDE_STREAMS[dev.index]
+    side.wait_stream(main)                  # pass 1's output is written
+    for t in (cells.starts, cells.codes):
+        t.record_stream(side)
+    with torch.cuda.stream(side):
+        root, out = components(cells, col, stream=side)
+        done = torch.cuda.Event()
+        done.record(side)
+    for t in (root, out):
+        t.record_stream(main)
+    return root, out, done
+
+
 def rank_components(root, cnt_first):
     """Labels 0, 1, ... by rows, ties to the smallest root (a stable sort):
     core/passes.py:933-950 `_rank_components`, on host arrays."""
@@ -256,10 +281,12 @@ class FitResult:
 
 
 def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
-          x0=None, normalize_fe=True, timer=None, precision="fp64") -> FitResult:
+          x0=None, normalize_fe=True, timer=None, precision="fp64", comps=None) -> FitResult:
     """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
     right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
-    zero, block PCG per `rhs_block` columns, then `_normalize`."""
+    zero, block PCG per `rhs_block` columns, then `_normalize`.  `comps`:
+    the first dimension's components from `components_async`, else computed
+    here."""
     torch = _torch()
     timer = timer or _NoTimer()
     m = int(cells.rhs.shape[1])
@@ -268,7 +295,11 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     solver.timer = timer
     scale = torch.sqrt(torch.clamp(cells.raw_ss, min=0.0))
     zero_all = (torch.linalg.vector_norm(cells.rhs, dim=0) <= RHS_ZERO_TOL * scale).cpu().numpy()
-    root, ncomp = components(cells, 0)
+    if comps is None:
+        root, ncomp = components(cells, 0)
+    else:
+        root, ncomp, done = comps
+        torch.cuda.current_stream(root.device).wait_event(done)
     gamma = torch.empty_like(cells.rhs)
     its, conv, rel = [], True, 0.0
     for j0 in range(0, m, rhs_block):
@@ -337,10 +368,12 @@ def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None,
     timer = timer or _NoTimer()
     with timer("pass1"):
         cells = pass1(rows)
+    comps = components_async(cells)         # beside the S build
     with timer("sbuild"):
         S = build_s(cells)
     with timer("solve"):
-        return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision)
+        return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
+                     comps=comps)
 
 
 _COPY_STREAMS = {}
@@ -389,6 +422,7 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
     empty = torch.empty((0, int(g_d.shape[0])), dtype=torch.float64, device=dev)
     with timer("pass1"):
         shape = pass1(DeviceRows(g_d, c_d, empty, w_d, n_levels))
+    comps = components_async(shape)         # the structure is all it reads
     with timer("sbuild"):
         S = build_s(shape)
     del shape
@@ -397,7 +431,8 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
     with timer("pass1"):
         cells = pass1(DeviceRows(g_d, c_d, V_d, w_d, n_levels))
     with timer("solve"):
-        return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision)
+        return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
+                     comps=comps)
 
 
 def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):
