@@ -206,13 +206,24 @@ __device__ __forceinline__ void reduce_range(const double *part, int q0, int q1,
 }
 
 // Row c of V (stride VS) into g[0..K), with vector loads of VW elements
-// (2 doubles, or 2 or 4 floats: 8- or 16-byte aligned rows) or scalars.
+// (4 doubles: one 32-byte load; 2 doubles; 2 or 4 floats: 8-, 16- or 32-byte
+// aligned rows) or scalars.  A gather of a random row costs the L1 one
+// wavefront per load instruction, so the widest load that holds the row wins.
 // Plain loads: V may be written by this kernel between grid barriers.
 template <int K, int VS, int VW, typename T>
 __device__ __forceinline__ void gather(const T *V, int64_t c, T (&g)[K])
 {
     const T *p = V + c * VS;
-    if constexpr (VW == 4) {
+    if constexpr (VW == 4 && sizeof(T) == 8) {
+        static_assert(VS % 4 == 0 && K <= 4, "32-byte rows");
+        double t0, t1, t2, t3;
+        asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                     : "=d"(t0), "=d"(t1), "=d"(t2), "=d"(t3) : "l"(p));
+        g[0] = t0;
+        if constexpr (K > 1) g[1] = t1;
+        if constexpr (K > 2) g[2] = t2;
+        if constexpr (K > 3) g[3] = t3;
+    } else if constexpr (VW == 4) {
 #pragma unroll
         for (int k = 0; k < K; k += 4) {
             const float4 t = *reinterpret_cast<const float4 *>(p + k);
@@ -540,7 +551,10 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
             // ---- A: AP = S P, p'Ap
 #pragma unroll
             for (int k = 0; k < K; k++) dot[k] = 0.0;
-            spmm_range<K, KP, (KP % 2 == 0) ? 2 : 1, double>(a, a.data, a.P, a.AP, a.carry, dot, true);
+            // P's rows are KP wide from a 256-byte aligned workspace: 32-byte
+            // rows for k = 3, 4
+            spmm_range<K, KP, (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1), double>(
+                a, a.data, a.P, a.AP, a.carry, dot, true);
             block_partials<K>(dot, s_scratch, a.part, 0, nb);
             if (!gb.sync()) return;
             if (warp == 0) {
