@@ -37,6 +37,29 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxK = 8;
 
+// P's row stride: 3 columns padded to 4, so that a row is one aligned
+// 32-byte load (a random gather costs the L1 a wavefront per load instruction)
+__host__ __device__ constexpr int p_stride(int k) { return k == 3 ? 4 : k; }
+
+// Row c of P (stride PS) into g[0..K)
+template <int K, int PS>
+__device__ __forceinline__ void gather_p(const double *P, int64_t c, double (&g)[K])
+{
+    const double *p = P + c * PS;
+    if constexpr (PS == 4) {
+        double t0, t1, t2, t3;
+        asm volatile("ld.global.v4.f64 {%0, %1, %2, %3}, [%4];"
+                     : "=d"(t0), "=d"(t1), "=d"(t2), "=d"(t3) : "l"(p));
+        g[0] = t0;
+        if constexpr (K > 1) g[1] = t1;
+        if constexpr (K > 2) g[2] = t2;
+        if constexpr (K > 3) g[3] = t3;
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; k++) g[k] = p[k];
+    }
+}
+
 struct Args {
     const int64_t *indptr;
     const int32_t *indices;
@@ -125,6 +148,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
     const int nsys = a.wsys[blockIdx.x * kWarps + kWarps - 1] - first + 1;
     const int local = sys - first;
     constexpr int S5 = 5 * K;       // slots: set-up 2K, phase A K, phase B 2K
+    constexpr int PS = p_stride(K);
 
     bool zero[K], active[K];
     double bnorm[K], rz[K], rel[K];
@@ -144,7 +168,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
             const double res = zero[k] ? 0.0 : b;
             a.X[r * K + k] = 0.0;
             a.R[r * K + k] = res;
-            a.P[r * K + k] = res * di;
+            a.P[r * PS + k] = res * di;
             sb[k] += b * b;
             sz[k] += res * res * di;
         }
@@ -188,8 +212,10 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
                         const int32_t c = a.indices[j];
                         const double v = a.data[j];
                         if (c < 0 || c >= a.L) { gb.fail(HDFE_ERR_BAD_CODE); continue; }
+                        double g[K];
+                        gather_p<K, PS>(a.P, c, g);
 #pragma unroll
-                        for (int k = 0; k < K; k++) acc[k] += v * a.P[(int64_t)c * K + k];
+                        for (int k = 0; k < K; k++) acc[k] += v * g[k];
                     }
                 }
 #pragma unroll
@@ -201,7 +227,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
 #pragma unroll
                     for (int k = 0; k < K; k++) {
                         a.AP[r * K + k] = acc[k];
-                        dot[k] += acc[k] * a.P[r * K + k];
+                        dot[k] += acc[k] * a.P[r * PS + k];
                     }
                 }
             }
@@ -217,15 +243,17 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
                     const int32_t col = a.indices[j];
                     const double v = a.data[j];
                     if (col < 0 || col >= a.L) { gb.fail(HDFE_ERR_BAD_CODE); continue; }
+                    double g[K];
+                    gather_p<K, PS>(a.P, col, g);
 #pragma unroll
-                    for (int k = 0; k < K; k++) acc[k] += v * a.P[(int64_t)col * K + k];
+                    for (int k = 0; k < K; k++) acc[k] += v * g[k];
                 }
 #pragma unroll
                 for (int k = 0; k < K; k++) {
                     const double t = warp_sum(acc[k]);
                     if (lane == 0) {
                         a.cp[(int64_t)c * K + k] = t;
-                        dot[k] += t * a.P[r * K + k];
+                        dot[k] += t * a.P[r * PS + k];
                     }
                 }
             }
@@ -263,7 +291,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
             }
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                a.X[r * K + k] += alpha[k] * a.P[r * K + k];
+                a.X[r * K + k] += alpha[k] * a.P[r * PS + k];
                 const double res = a.R[r * K + k] - alpha[k] * ap[k];
                 a.R[r * K + k] = res;
                 sr[k] += res * res;
@@ -293,7 +321,7 @@ __global__ void __launch_bounds__(kThreads) k_batch_pcg(Args a)
                 const double di = a.dinv[r];
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    a.P[r * K + k] = a.R[r * K + k] * di + beta[k] * a.P[r * K + k];
+                    a.P[r * PS + k] = a.R[r * K + k] * di + beta[k] * a.P[r * PS + k];
             }
             if (lane == 0) atomicOr(a.flag + (it & 1), 1u);
         }
@@ -417,7 +445,8 @@ extern "C" int64_t hdfe_batch_pcg_workspace_bytes(int64_t L, int32_t k, int64_t 
 {
     if (L < 1 || k < 1 || k > batch::kMaxK || warps < 1 || n_chunks < 0) return -1;
     auto up = [](int64_t b) { return (b + 255) / 256 * 256; };
-    return 3 * up(L * k * 8) + up(warps * 5 * k * 8) + up((n_chunks + 1) * k * 8) + 256;
+    return 2 * up(L * k * 8) + up(L * batch::p_stride(k) * 8) + up(warps * 5 * k * 8) +
+           up((n_chunks + 1) * k * 8) + 256;
 }
 
 extern "C" int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indices,
@@ -443,6 +472,8 @@ extern "C" int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indice
         !(tol > 0.0) || maxiter < 1 || !X || !iterations || !max_rel || !converged || !status ||
         !workspace)
         return hdfe_set_arg_error("hdfe_batch_pcg_solve: bad argument");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return hdfe_set_arg_error("hdfe_batch_pcg_solve: workspace must be 256-byte aligned");
     const int64_t warps = (int64_t)blocks * batch::kWarps;
     if (workspace_bytes < hdfe_batch_pcg_workspace_bytes(L, k, warps, n_chunks))
         return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_batch_pcg_solve: workspace too small");
@@ -466,12 +497,13 @@ extern "C" int hdfe_batch_pcg_solve(const int64_t *indptr, const int32_t *indice
     a.tol = tol;
     a.maxiter = maxiter;
     a.X = X;
+    const int64_t vec = up(L * k * 8), pvec = up(L * batch::p_stride(k) * 8);
     a.R = (double *)ws;
-    a.P = (double *)(ws + up(L * k * 8));
-    a.AP = (double *)(ws + 2 * up(L * k * 8));
-    a.cpart = (double *)(ws + 3 * up(L * k * 8));
-    a.cp = (double *)(ws + 3 * up(L * k * 8) + up(warps * 5 * k * 8));
-    unsigned *words = (unsigned *)(ws + 3 * up(L * k * 8) + up(warps * 5 * k * 8) +
+    a.P = (double *)(ws + vec);
+    a.AP = (double *)(ws + vec + pvec);
+    a.cpart = (double *)(ws + 2 * vec + pvec);
+    a.cp = (double *)(ws + 2 * vec + pvec + up(warps * 5 * k * 8));
+    unsigned *words = (unsigned *)(ws + 2 * vec + pvec + up(warps * 5 * k * 8) +
                                    up((n_chunks + 1) * k * 8));
     a.bar = words;          // [0..2] barrier
     a.flag = words + 4;     // [2]
