@@ -56,9 +56,22 @@ def parse():
     return ap.parse_args()
 
 
+def describe(name):
+    """The panel preset in words (simulate.PANELS) and its restriction."""
+    from hdfe_stream_b200.simulate import PANELS
+    p = PANELS[name]
+    lo, hi = p["spell"]
+    text = (f"{name}: {p['n_workers']:,} workers, {p['n_firms']:,} firms, {p['n_years']} years, "
+            f"spells of {lo}-{hi} years, p_move {p['p_move']}")
+    if p.get("weights"):
+        text += ", weights U[0.5, 2]"
+    restriction = {"akm_5m": "largest connected set with min_degree=2",
+                   "kss_1m": "leave-one-out connected set"}.get(name)
+    return text + (f", {restriction}" if restriction else "")
+
+
 def config(args, n, rows):
-    return {"workload": f"{args.workload}: 5M workers, 500k firms, 15 years, ~8.5 rows/worker, "
-                        "p_move 0.08, largest connected set with min_degree=2",
+    return {"workload": describe(args.workload),
             "rows": rows.n_rows, "workers": rows.n_groups, "levels": int(sum(rows.n_levels)),
             "model": "log_earn ~ age_squared + age_cubed | worker_id + firm_id + year",
             "tol": args.tol, "parallelism": f"replicas{n}" if n > 1 else "single",
