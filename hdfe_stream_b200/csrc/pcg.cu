@@ -51,6 +51,9 @@ __host__ __device__ constexpr int threads_for(int k) { return k >= HDFE_PCG_WIDE
 constexpr int kMaxWarps = 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kLong = 64;           // nonzeros in a warp's range that make a row "long"
+// rows per thread per trip in the vector phases (their loads all issued
+// before the updates), as many as fit the registers without spills
+__host__ __device__ constexpr int row_batch(int k) { return k <= 3 ? 2 : 1; }
 
 // P's row stride: even, so a row's pairs of values are 16-byte aligned
 template <int K>
@@ -468,7 +471,9 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
         __syncwarp();
         for (int64_t r = gtid; r < L; r += gstride) {
             const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
-            a.cut[r] = (re > rs && warp_of(a, rs) != warp_of(a, re - 1)) ? 1 : 0;
+            // bit 0: the row is cut across warps; bit 1: it has no nonzeros
+            a.cut[r] = ((re > rs && warp_of(a, rs) != warp_of(a, re - 1)) ? 1 : 0) |
+                       (re == rs ? 2 : 0);
         }
     }
     // ---- R = B - S X0 (or B), the zero columns, ||B||, rz
@@ -503,8 +508,8 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
         };
         for (int64_t r = gtid; r < L; r += gstride) {
             double ap[K];
-            if (a.X0 != nullptr && a.cut[r]) continue;
-            const bool empty = a.indptr[r + 1] == a.indptr[r];
+            if (a.X0 != nullptr && (a.cut[r] & 1)) continue;
+            const bool empty = (a.cut[r] & 2) != 0;
 #pragma unroll
             for (int k = 0; k < K; k++) ap[k] = (a.X0 != nullptr && !empty) ? a.AP[r * K + k] : 0.0;
             setup_row(r, ap);
@@ -587,13 +592,41 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                     sz[k] += res * res * di;
                 }
             };
-            for (int64_t r = gtid; r < L; r += gstride) {
-                if (a.cut[r]) continue;
-                double ap[K];
-                const bool empty = a.indptr[r + 1] == a.indptr[r];
+            // kRowBatch rows per thread per trip, every load issued before the
+            // updates; the rows are summed in the same order as one at a time
+            constexpr int kRowBatch = row_batch(K);
+            for (int64_t r0 = gtid; r0 < L; r0 += kRowBatch * gstride) {
+                uint8_t f[kRowBatch];
+                double di[kRowBatch], p[kRowBatch][K], ap[kRowBatch][K], x[kRowBatch][K],
+                    rr[kRowBatch][K];
 #pragma unroll
-                for (int k = 0; k < K; k++) ap[k] = empty ? 0.0 : a.AP[r * K + k];
-                step_row(r, ap);
+                for (int u = 0; u < kRowBatch; u++) {
+                    const int64_t r = r0 + u * gstride;
+                    f[u] = r < L ? a.cut[r] : 1;
+                    const bool use = (f[u] & 1) == 0;
+                    const bool empty = (f[u] & 2) != 0;
+                    di[u] = use ? a.dinv[r] : 0.0;
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        p[u][k] = use ? a.P[r * KP + k] : 0.0;
+                        ap[u][k] = (use && !empty) ? a.AP[r * K + k] : 0.0;
+                        x[u][k] = use ? a.X[r * K + k] : 0.0;
+                        rr[u][k] = use ? a.R[r * K + k] : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kRowBatch; u++) {
+                    if (f[u] & 1) continue;
+                    const int64_t r = r0 + u * gstride;
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        a.X[r * K + k] = x[u][k] + alpha[k] * p[u][k];
+                        const double res = rr[u][k] - alpha[k] * ap[u][k];
+                        a.R[r * K + k] = res;
+                        sr[k] += res * res;
+                        sz[k] += res * res * di[u];
+                    }
+                }
             }
             {
                 int64_t r;
@@ -631,11 +664,27 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                 rz[k] = rzn;
             }
             __syncthreads();
-            for (int64_t r = gtid; r < L; r += gstride) {
-                const double di = a.dinv[r];
+            for (int64_t r0 = gtid; r0 < L; r0 += row_batch(K) * gstride) {
+                constexpr int kRowBatch = row_batch(K);
+                double di[kRowBatch], rr[kRowBatch][K], p[kRowBatch][K];
 #pragma unroll
-                for (int k = 0; k < K; k++)
-                    a.P[r * KP + k] = a.R[r * K + k] * di + beta[k] * a.P[r * KP + k];
+                for (int u = 0; u < kRowBatch; u++) {
+                    const int64_t r = r0 + u * gstride;
+                    const bool in = r < L;
+                    di[u] = in ? a.dinv[r] : 0.0;
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        rr[u][k] = in ? a.R[r * K + k] : 0.0;
+                        p[u][k] = in ? a.P[r * KP + k] : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kRowBatch; u++) {
+                    const int64_t r = r0 + u * gstride;
+                    if (r >= L) continue;
+#pragma unroll
+                    for (int k = 0; k < K; k++) a.P[r * KP + k] = rr[u][k] * di[u] + beta[k] * p[u][k];
+                }
             }
             if (!gb.sync()) return;
         }
