@@ -1,0 +1,122 @@
+"""The path at the benchmark's full sizes, through properties that do not
+depend on size (the oracle would take minutes there):
+
+* the 5M-worker panel (20.5M rows after pruning, L = 499,862): the solve's
+  residual recomputed independently, the normalisation's zero means, the
+  fit repeated (S bit for bit) and the overlapped host-input fit;
+* the 1M-worker panel's leave-one-out set (8.5M rows): the KSS leave-out
+  components recover the variances and covariance of the generator's true
+  effects over the same rows, which they estimate without bias;
+* the weighted 400k-worker panel: residual and weighted normalisation.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.filterwarnings("ignore:Sparse:UserWarning")]
+
+
+@pytest.fixture(scope="module")
+def device():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def residual(res):
+    """max over columns of ||rhs - S gamma|| / ||rhs||, in float64 with a
+    sparse product outside the library."""
+    import torch
+    S = res.S
+    A = torch.sparse_csr_tensor(S.indptr, S.indices.to(torch.int64), S.data,
+                                size=(S.L, S.L))
+    r = res.cells.rhs - A @ res.gamma
+    num = torch.linalg.vector_norm(r, dim=0)
+    den = torch.linalg.vector_norm(res.cells.rhs, dim=0).clamp(min=1e-300)
+    return float((num / den).max())
+
+
+def normalisation(res):
+    """The largest obs-weighted mean of the first dimension's effects within a
+    component and of a further dimension's effects, relative to the effects'
+    scale (core/solve.py:383-399 `_normalize` makes them zero)."""
+    import torch
+    from hdfe_stream_b200 import fit
+    cells, gamma = res.cells, res.gamma
+    offs = np.concatenate(([0], np.cumsum(cells.n_levels)[:-1]))
+    root, _ = fit.components(cells, 0)
+    nl0 = int(cells.n_levels[0])
+    w = cells.obs[:nl0]
+    comp = root.to(torch.int64)
+    tot = torch.zeros((nl0, gamma.shape[1]), dtype=torch.float64, device=gamma.device)
+    tot.index_add_(0, comp, w[:, None] * gamma[:nl0])
+    cw = torch.zeros(nl0, dtype=torch.float64, device=gamma.device).index_add_(0, comp, w)
+    worst = float((tot[cw > 0] / cw[cw > 0][:, None]).abs().max())
+    for d in range(1, len(cells.n_levels)):
+        o, n = int(offs[d]), int(cells.n_levels[d])
+        wd = cells.obs[o:o + n]
+        worst = max(worst, float(((wd @ gamma[o:o + n]) / wd.sum()).abs().max()))
+    return worst / float(gamma.abs().max())
+
+
+def test_akm_5m_fit_properties(device):
+    import torch
+    from hdfe_stream_b200 import fit
+    from hdfe_stream_b200.simulate import prepare
+    rows = prepare("akm_5m", seed=0)
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-10)
+    assert res.info["converged"] and res.info["max_rel_residual"] <= 1e-10
+    assert residual(res) < 1e-8
+    assert normalisation(res) < 1e-10
+    again = fit.fit(drows, tol=1e-10)
+    assert torch.equal(again.S.indptr, res.S.indptr)
+    assert torch.equal(again.S.indices, res.S.indices)
+    assert torch.equal(again.S.data, res.S.data)
+    assert float((again.gamma - res.gamma).abs().max() / res.gamma.abs().max()) < 1e-9
+    pin = {"g": torch.from_numpy(rows.gcode.view(np.int32)).pin_memory(),
+           "c": torch.from_numpy(np.ascontiguousarray(rows.codes).view(np.int32)).pin_memory(),
+           "V": torch.from_numpy(np.ascontiguousarray(rows.V.T)).pin_memory()}
+    host = fit.fit_host(pin["g"], pin["c"], pin["V"], rows.n_levels, tol=1e-10)
+    assert torch.equal(host.S.data, res.S.data)
+    assert float((host.gamma - res.gamma).abs().max() / res.gamma.abs().max()) < 1e-9
+
+
+def test_kss_1m_recovers_the_true_components(device):
+    """KSS leave-out components (256 JLA probes and Hutchinson draws) against
+    the variances and covariance of the generator's own worker and firm
+    effects over the rows of the leave-one-out set, with the n - 1 divisor
+    the estimator uses; the plug-in components, biased upward for the
+    variances, are further away."""
+    from hdfe_stream_b200 import fit, leaveout
+    from hdfe_stream_b200.simulate import (PANELS, pass0_layout, restrict_leave_one_out,
+                                           simulate_panel)
+    panel = simulate_panel(seed=100, **PANELS["kss_1m"])
+    keep = restrict_leave_one_out(panel)
+    rows = pass0_layout(panel, keep, year_fe=False)
+    psi = panel.truth["psi"][panel.firm[keep]]
+    alpha = panel.truth["alpha"][panel.worker[keep]]
+    n = len(psi)
+    truth = np.array([np.var(psi) * n / (n - 1), np.var(alpha) * n / (n - 1),
+                      np.cov(psi, alpha)[0, 1]])
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-10)
+    op = leaveout.InverseOperator(drows, res.cells, res.S, drows.V[1:].T.contiguous(),
+                                  tol=1e-10)
+    kss = op.leave_out_components(res.gamma, 256, block=32, seed=1)
+    est = np.asarray(kss["leave_out"])
+    assert np.all(np.abs(est - truth) <= 0.03 * np.abs(truth)), (est, truth)
+    plug = np.asarray(kss["plug_in"])
+    assert np.all(np.abs(est - truth)[:2] < np.abs(plug - truth)[:2])
+
+
+def test_akm_400k_weighted_fit_properties(device):
+    from hdfe_stream_b200 import fit
+    from hdfe_stream_b200.simulate import prepare
+    rows = prepare("akm_400k_w", seed=300)
+    res = fit.fit(fit.DeviceRows.from_rows(rows), tol=1e-10)
+    assert res.info["converged"]
+    assert residual(res) < 1e-8
+    assert normalisation(res) < 1e-10
