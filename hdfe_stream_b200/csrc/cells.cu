@@ -296,14 +296,15 @@ struct GroupArgs {
 
 // One group: cells from its rows, level scatter, identifying-cell output.
 // MV > 0 fixes the number of variables at compile time (registers, unrolled
-// loops); MV == 0 takes it from the arguments.
+// loops); MV == 0 takes it from the arguments; MV < 0 is the structure-only
+// pass (no variables: cells, counts and diag alone).
 template <int D, int MV>
 __device__ void do_group(const GroupArgs &a, int64_t g, bool keep, int64_t gi, int64_t co,
                          double *s_acc, double *sums_buf)
 {
     const Dims &dm = a.dims;
-    const int m = MV > 0 ? MV : dm.m;
-    constexpr int kV = MV > 0 ? MV : kMaxVars;
+    const int m = MV > 0 ? MV : (MV < 0 ? 0 : dm.m);
+    constexpr int kV = MV > 0 ? MV : (MV < 0 ? 1 : kMaxVars);
     const int64_t r0 = a.grow[g], r1 = a.grow[g + 1];
     double Ng = 0.0, vsum[kV];
     for (int j = 0; j < m; j++) vsum[j] = 0.0;
@@ -464,8 +465,8 @@ __global__ void __launch_bounds__(kThreads) groups_work(GroupArgs a, double *sum
     __shared__ int s_nc[kGroupTile];
     __shared__ int s_scr[2][kThreads / 32 + 1];
     const Dims &dm = a.dims;
-    const int m = MV > 0 ? MV : dm.m;
-    constexpr int kV = MV > 0 ? MV : kMaxVars;
+    const int m = MV > 0 ? MV : (MV < 0 ? 0 : dm.m);
+    constexpr int kV = MV > 0 ? MV : (MV < 0 ? 1 : kMaxVars);
     const int NS = kSlotFixed + m;                  // values per level slot
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *w_slots = s_dyn + (int64_t)warp * dm.n_small * NS;           // this warp's small levels
@@ -869,7 +870,8 @@ int run(const uint32_t *gcode, const uint32_t *codes, const double *V, int m, co
     HDFE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // the warps' small-level slots, then their 32-lane scratch rows
     const size_t smem = (size_t)(slots * per_level) + (size_t)kWarpsPerCta * 32 * ((kSlotFixed + m) | 1) * 8;
-    void (*kern)(GroupArgs, double *) = m == 1 ? groups_work<D, 1> : m == 2 ? groups_work<D, 2>
+    void (*kern)(GroupArgs, double *) = m == 0 ? groups_work<D, -1>
+                                       : m == 1 ? groups_work<D, 1> : m == 2 ? groups_work<D, 2>
                                        : m == 3 ? groups_work<D, 3> : m == 4 ? groups_work<D, 4>
                                        : groups_work<D, 0>;
     HDFE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
