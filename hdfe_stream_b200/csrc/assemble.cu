@@ -238,6 +238,62 @@ __global__ void __launch_bounds__(kThreads) k_variance(Args a, const double *Gam
     cta_sums(acc, NQ, s_part, part);
 }
 
+// The per-row scores w e h (out (N, m - 1) row-major) from the same row pass
+// as k_variance: core/inference.py:594-603, the rows that pass 2 scatters
+// into the clusters of a CRV1 term that is not the streamed dimension.
+template <int M>
+__global__ void __launch_bounds__(kThreads) k_scores(Args a, const double *Gamma,
+                                                     const double *beta, double *out)
+{
+    constexpr int KX = M - 1;
+    double b[KX];
+#pragma unroll
+    for (int j = 0; j < KX; j++) b[j] = beta[j];
+    for (int64_t g = (int64_t)blockIdx.x * kThreads + threadIdx.x; g < a.G;
+         g += (int64_t)gridDim.x * kThreads) {
+        const int64_t s = a.starts[g], e = a.starts[g + 1];
+        auto raw = [&](int64_t i, double &yr, double (&hr)[KX]) {
+            yr = a.V[i];
+#pragma unroll
+            for (int j = 0; j < KX; j++) hr[j] = a.V[(int64_t)(j + 1) * a.N + i];
+            for (int d = 0; d < a.D; d++) {
+                const int64_t l = level(a, i, d);
+                yr -= Gamma[l * M];
+#pragma unroll
+                for (int j = 0; j < KX; j++) hr[j] -= Gamma[l * M + j + 1];
+            }
+        };
+        double Wg = 0.0, mu = 0.0, mh[KX];
+#pragma unroll
+        for (int j = 0; j < KX; j++) mh[j] = 0.0;
+        for (int64_t i = s; i < e; i++) {
+            const double wi = a.w ? a.w[i] : 1.0;
+            double yr, hr[KX];
+            raw(i, yr, hr);
+            double u = yr;
+#pragma unroll
+            for (int j = 0; j < KX; j++) { u -= b[j] * hr[j]; mh[j] += wi * hr[j]; }
+            Wg += wi;
+            mu += wi * u;
+        }
+        const double inv = Wg > 0.0 ? 1.0 / Wg : 0.0;
+        mu *= inv;
+#pragma unroll
+        for (int j = 0; j < KX; j++) mh[j] *= inv;
+        for (int64_t i = s; i < e; i++) {
+            const double wi = a.w ? a.w[i] : 1.0;
+            double yr, h[KX];
+            raw(i, yr, h);
+            double u = yr;
+#pragma unroll
+            for (int j = 0; j < KX; j++) { u -= b[j] * h[j]; h[j] -= mh[j]; }
+            const double we = wi * (u - mu);
+#pragma unroll
+            for (int j = 0; j < KX; j++) out[i * KX + j] = we * h[j];
+        }
+    }
+}
+
 // out[q] = sum over CTAs of part[., q], one warp per entry, fixed order
 __global__ void __launch_bounds__(kThreads) k_sum_parts(const double *part, int blocks, int n,
                                                         double *out)
@@ -434,5 +490,34 @@ extern "C" int hdfe_variance_sums(const int64_t *starts, int64_t n_groups, const
                             assemble::kThreads, 0, s>>>(part, (int)grid, nq, out);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(2);
+    return HDFE_OK;
+}
+
+extern "C" int hdfe_row_scores(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                               int32_t D, const int64_t *n_levels, const double *w,
+                               const double *V, int32_t m, int64_t n_rows, const double *Gamma,
+                               const double *beta, double *out, void *status, void *stream)
+{
+    assemble::Args a;
+    int st = assemble::fill(a, starts, n_groups, codes, D, n_levels, w, V, m, n_rows,
+                            (unsigned *)status);
+    if (st != HDFE_OK) return st;
+    if (m < 2 || !Gamma || !beta || !out)
+        return hdfe_set_arg_error("hdfe_row_scores: bad argument (2 <= m <= 8)");
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned grid = assemble::grid_for(n_groups);
+#define HDFE_SCORES(M) assemble::k_scores<M><<<grid, assemble::kThreads, 0, s>>>(a, Gamma, beta, out)
+    switch (m) {
+    case 2: HDFE_SCORES(2); break;
+    case 3: HDFE_SCORES(3); break;
+    case 4: HDFE_SCORES(4); break;
+    case 5: HDFE_SCORES(5); break;
+    case 6: HDFE_SCORES(6); break;
+    case 7: HDFE_SCORES(7); break;
+    default: HDFE_SCORES(8); break;
+    }
+#undef HDFE_SCORES
+    HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(1);
     return HDFE_OK;
 }

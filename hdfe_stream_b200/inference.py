@@ -68,12 +68,135 @@ def fe_pair_components(rows: DeviceRows, cells: DeviceCells):
     return counts
 
 
-def estimate(rows: DeviceRows, cells: DeviceCells, gamma):
+def row_scores(rows: DeviceRows, cells: DeviceCells, gamma, beta):
+    """The per-row scores w e h (N, m - 1) of pass 2 (`hdfe_row_scores`)."""
+    torch = _torch()
+    lib = _lib.lib()
+    dev = rows.gcode.device
+    starts, G = row_groups(rows)
+    nlev = np.asarray(rows.n_levels, dtype=np.int64)
+    gamma = gamma.to(dev, torch.float64).contiguous()
+    beta_d = torch.as_tensor(np.asarray(beta, np.float64), device=dev)
+    out = torch.empty((rows.n_rows, rows.m - 1), dtype=torch.float64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    w = rows.w
+    _lib.check(lib.hdfe_row_scores(starts.data_ptr(), G, rows.codes.data_ptr(), len(nlev),
+                                   nlev.ctypes.data, None if w is None else w.data_ptr(),
+                                   rows.V.data_ptr(), rows.m, rows.n_rows, gamma.data_ptr(),
+                                   beta_d.data_ptr(), out.data_ptr(), status.data_ptr(),
+                                   _lib.stream_handle()))
+    if int(status.item()) != _lib.HDFE_OK:
+        raise _lib.HDFEError(int(status.item()), "row_scores: a level code is out of range")
+    return out
+
+
+def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_components,
+                 group_meat=None, extra=None):
+    """CRV1 variances for cluster requests (core/inference.py:176-240
+    `_resolve_clusters`, :242-269 `_nested_dims`, :886-906): a request "a",
+    "a^b" (one cluster per distinct combination) or "a+b" (two-way,
+    inclusion-exclusion over a, b and a^b); the names are `fe_names` (the
+    streamed dimension first, then the others in column order) or keys of
+    `extra` (per-row integer codes).  Each term's meat sums the scores per
+    cluster (a device index_add over the cluster codes found by a sort of the
+    combined keys) and takes S'S; a fixed-effect dimension is nested in a
+    term when its columns are among the term's or (except for a refinement of
+    the streamed groups) every level lies within one cluster; K drops the
+    nested dimensions' levels (core/estimator.py:446-464 `_k_fe` with the
+    pairs whose both dimensions are nested left out); G is the smallest
+    one-way count.  Returns {request: (V, {"G", "adj", "nested"})}."""
+    torch = _torch()
+    from itertools import combinations
+    dev = rows.gcode.device
+    N = rows.n_rows
+    D = rows.D
+    g0 = fe_names[0]
+    col = {g0: rows.gcode.to(torch.int64)}
+    for d in range(D):
+        col[fe_names[d + 1]] = rows.codes[:, d].to(torch.int64)
+    for name, c in (extra or {}).items():
+        col[name] = torch.as_tensor(c, device=dev).to(torch.int64)
+    card = {name: int(c.max().item()) + 1 if N else 0 for name, c in col.items()}
+    G_groups = int(rows.gcode[-1].item()) + 1 if N else 0
+    fe_params = {g0: G_groups}
+    for d in range(D):
+        fe_params[fe_names[d + 1]] = int(rows.n_levels[d])
+    fe_dims = list(fe_params)
+    cache = {}
+
+    def term(cols):
+        key_name = "^".join(cols)
+        if key_name in cache:
+            return cache[key_name]
+        cs = set(cols)
+        if cs == {g0}:
+            kind, code, G = "seg", col[g0], G_groups
+        elif len(cols) == 1 and cols[0] in fe_params:
+            kind, code, G = "fe", col[cols[0]], card[cols[0]]
+        else:
+            key = torch.zeros(N, dtype=torch.int64, device=dev)
+            for c in cols:
+                key = key * card[c] + col[c]
+            _, code = torch.unique(key, sorted=True, return_inverse=True)
+            G = int(code.max().item()) + 1 if N else 0
+            kind = "segsub" if g0 in cs else ("fe" if len(cols) == 1 else "extra")
+        if kind == "seg" and group_meat is not None:
+            meat = group_meat
+        else:
+            S = torch.zeros((G, k), dtype=torch.float64, device=dev).index_add_(0, code, scores)
+            meat = (S.T @ S).cpu().numpy()
+        nested = []
+        for d in fe_dims:
+            if cs <= {d}:
+                nested.append(d)
+                continue
+            if kind == "segsub":
+                continue
+            nl = fe_params[d]
+            lo = torch.full((nl,), N, dtype=torch.int64, device=dev).scatter_reduce_(
+                0, col[d], code, "amin")
+            hi = torch.full((nl,), -1, dtype=torch.int64, device=dev).scatter_reduce_(
+                0, col[d], code, "amax")
+            if bool((lo == hi).all().item()):
+                nested.append(d)
+        cache[key_name] = (G, meat, nested)
+        return cache[key_name]
+
+    def k_fe(nest):
+        total = sum(fe_params.values())
+        if len(fe_params) < 2:
+            return total
+        comps = max((c for (a, b), c in pair_components.items()
+                     if a not in nest or b not in nest), default=1)
+        return total - (comps + len(fe_params) - 2)
+
+    out = {}
+    for req in requests:
+        parts = [[c.strip() for c in p.split("^")] for p in req.split("+")]
+        terms = []
+        for r in range(1, len(parts) + 1):
+            for combo in combinations(range(len(parts)), r):
+                cols = list(dict.fromkeys(c for i in combo for c in parts[i]))
+                terms.append((term(cols), (-1) ** (r + 1), r == 1))
+        Gs = [t[0] for t, _, single in terms if single]
+        Gm = min(Gs)
+        nest = list(dict.fromkeys(d for t, _, _ in terms for d in t[2]))
+        Kc = k + k_fe(nest) - sum(fe_params[d] for d in nest) + len(nest)
+        adj = Gm / (Gm - 1) * (N - 1) / (N - Kc)
+        V = sum(sign * adj * (Binv @ t[1] @ Binv) for t, sign, _ in terms)
+        out[req] = (V, {"G": Gs, "adj": adj, "nested": nest, "df": Gm - 1})
+    return out
+
+
+def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=None,
+             extra=None):
     """beta (k,) and its variances for y = V[0] on X = V[1:] with the fit's
     normalised effects gamma (L, m): {"beta", "vcov": {"iid", "hetero",
-    "CRV1"}, "se": {...}, "k_fe", "df_resid", "df_cluster", "rss",
-    "pair_components", "n_obs", "n_groups"}; CRV1 clusters on the streamed
-    dimension."""
+    "CRV1", "CRV1:<request>" ...}, "se": {...}, "k_fe", "df_resid",
+    "df_cluster", "rss", "pair_components", "n_obs", "n_groups"}; "CRV1"
+    clusters on the streamed dimension; `clusters` adds the requests of
+    `cluster_vcov` (names from `fe_names`, default "fe0" for the streamed
+    dimension and "fe1", "fe2", ... for the others, or from `extra`)."""
     torch = _torch()
     lib = _lib.lib()
     m = rows.m
@@ -121,7 +244,24 @@ def estimate(rows: DeviceRows, cells: DeviceCells, gamma):
     adj = G / (G - 1) * (N - 1) / (N - Kc)
     vcov = {"iid": rss / (N - K) * Binv, "hetero": N / (N - K) * Binv @ meat_hc @ Binv,
             "CRV1": adj * Binv @ meat_g @ Binv}
+    cluster_info = {}
+    if clusters:
+        names = list(fe_names) if fe_names else [f"fe{d}" for d in range(len(nlev) + 1)]
+        D = len(nlev)
+        pair = {}
+        for d in range(D):
+            pair[(names[0], names[d + 1])] = pcs[d]
+        j = D
+        for d1 in range(D):
+            for d2 in range(d1 + 1, D):
+                pair[(names[d1 + 1], names[d2 + 1])] = pcs[j]
+                j += 1
+        scores = row_scores(rows, cells, gamma, beta)
+        for req, (V, info) in cluster_vcov(rows, scores, Binv, k, clusters, names, pair,
+                                           group_meat=meat_g, extra=extra).items():
+            vcov[f"CRV1:{req}"] = V
+            cluster_info[req] = info
     return {"beta": beta, "vcov": vcov,
             "se": {key: np.sqrt(np.diag(v)) for key, v in vcov.items()},
             "k_fe": k_fe, "df_resid": N - K, "df_cluster": G - 1, "rss": rss,
-            "pair_components": pcs, "n_obs": int(N), "n_groups": G}
+            "pair_components": pcs, "n_obs": int(N), "n_groups": G, "clusters": cluster_info}

@@ -648,6 +648,94 @@ def variance_sums(starts, codes, offs, w, V, Gamma, beta):
     return B, he.T @ he, sg.T @ sg, float(w @ (e * e))
 
 
+def row_scores(starts, codes, offs, w, V, Gamma, beta):
+    """The per-row scores w e h of core/inference.py:594-603 (`he`), the
+    rows pass 2 sums per cluster."""
+    codes = np.asarray(codes, dtype=np.int64)
+    H = np.asarray(V[:, 1:], dtype=np.float64).copy()
+    for d in range(codes.shape[1]):
+        H -= Gamma[offs[d] + codes[:, d], 1:]
+    Wg = np.add.reduceat(w, starts[:-1])
+    H -= np.repeat(np.add.reduceat(w[:, None] * H, starts[:-1], axis=0) / Wg[:, None],
+                   np.diff(starts), axis=0)
+    e, _, _, _ = row_effects(starts, codes, offs, w, V, Gamma, beta)
+    return H * (w * e)[:, None]
+
+
+def cluster_variances(he, gcode, codes, n_levels, Binv, requests, names, pair_components,
+                      extra=None):
+    """CRV1 variances of beta for cluster requests (core/inference.py:176-240
+    `_resolve_clusters`: "a" one term, "a^b" one term of the combinations,
+    "a+b" the terms a, b, a^b with signs + + -; :242-269 `_nested_dims`;
+    :886-906 the variance with G the smallest one-way count, K less the
+    nested dimensions' levels plus one each, core/estimator.py:446-464
+    `_k_fe` "exact" skipping pairs of two nested dimensions).  names: the
+    streamed dimension first, then the others; pair_components keyed by
+    (name, name); extra: name -> per-row integer codes.  Returns
+    {request: (V, G list, adj, nested)}."""
+    from itertools import combinations
+    N, k = he.shape
+    codes = np.asarray(codes, np.int64)
+    g0 = names[0]
+    col = {g0: np.asarray(gcode, np.int64)}
+    for d in range(codes.shape[1]):
+        col[names[d + 1]] = codes[:, d]
+    for name, c in (extra or {}).items():
+        col[name] = np.asarray(c, np.int64)
+    params = {g0: int(col[g0].max()) + 1}
+    for d in range(codes.shape[1]):
+        params[names[d + 1]] = int(n_levels[d])
+
+    def term(cols):
+        cs = set(cols)
+        if len(cols) == 1 and cols[0] in params:
+            code = col[cols[0]]
+            G = params[cols[0]]
+            kind = "seg" if cols[0] == g0 else "fe"
+        else:
+            key = np.zeros(N, np.int64)
+            for c in cols:
+                key = key * (int(col[c].max()) + 1) + col[c]
+            _, code = np.unique(key, return_inverse=True)
+            G = int(code.max()) + 1
+            kind = "segsub" if g0 in cs else "extra"
+        sums = np.zeros((G, k))
+        np.add.at(sums, code, he)
+        nested = []
+        for d in params:
+            if cs <= {d}:
+                nested.append(d)
+            elif kind != "segsub":
+                lo = np.full(params[d], np.iinfo(np.int64).max)
+                hi = np.full(params[d], -1)
+                np.minimum.at(lo, col[d], code)
+                np.maximum.at(hi, col[d], code)
+                if np.all(lo == hi):
+                    nested.append(d)
+        return G, sums.T @ sums, nested
+
+    def k_fe(nest):
+        comps = max((c for (a, b), c in pair_components.items()
+                     if a not in nest or b not in nest), default=1)
+        return sum(params.values()) - (comps + len(params) - 2)
+
+    out = {}
+    for req in requests:
+        parts = [[c.strip() for c in p_.split("^")] for p_ in req.split("+")]
+        terms = []
+        for r in range(1, len(parts) + 1):
+            for combo in combinations(range(len(parts)), r):
+                cols = list(dict.fromkeys(c for i in combo for c in parts[i]))
+                terms.append((term(cols), (-1) ** (r + 1), r == 1))
+        Gs = [t[0] for t, _, single in terms if single]
+        nest = list(dict.fromkeys(d for t, _, _ in terms for d in t[2]))
+        Kc = k + k_fe(nest) - sum(params[d] for d in nest) + len(nest)
+        adj = min(Gs) / (min(Gs) - 1) * (N - 1) / (N - Kc)
+        V = sum(sign * adj * (Binv @ t[1] @ Binv) for t, sign, _ in terms)
+        out[req] = (V, Gs, adj, nest)
+    return out
+
+
 def variances(B, meat_hc, meat_g, rss, n_obs, n_groups, n_levels, pair_components):
     """The iid, HC1 and CRV1 (clustered on the streamed dimension) variances
     of beta: core/inference.py:886-912 (pyfixest's small-sample factors) with

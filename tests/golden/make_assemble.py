@@ -18,7 +18,12 @@ scores clustered on the streamed dimension, the residual sum of squares --
 and the iid, HC1 and CRV1(streamed dimension) variances with the small-sample
 factors of :886-912 and the fixed-effect parameter count of
 core/estimator.py:446-464 (fe_dof "exact"; the streamed dimension's levels
-nested in its own clusters).  Outputs go to tests/golden/assemble.npz.
+nested in its own clusters).  It also keeps the per-row scores w e z~ and,
+for the CRV1 requests in REQUESTS (another dimension, two-way, a refinement
+of the streamed groups, two-way over the non-streamed dimensions), the
+variances of :886-906 with each term's meat from the reference's own scatter
+(core/utils.py `_scatter`) and its nested dimensions (:242-269).  Outputs go
+to tests/golden/assemble.npz.
 Nothing at test time reads the reference.
 """
 
@@ -35,10 +40,85 @@ sys.path.insert(0, str(HERE))
 from make_golden import import_reference  # noqa: E402
 
 PANELS = ("akm_small", "akm_weighted", "akm_components")
+# CRV1 requests beyond the streamed dimension: one-way on another dimension,
+# two-way with inclusion-exclusion, a refinement of the streamed groups
+# ("segsub") and two-way over the non-streamed dimensions (their intersection
+# an "extra" cluster)
+REQUESTS = ("firm", "worker+firm", "worker^firm", "firm+year")
+DIMS = ("worker", "firm", "year")
+
+
+def cluster_variances(utils, gcode, codes, nlev, G, he, meat_g, Binv, k, N, pc):
+    """core/inference.py:176-240 `_resolve_clusters`, :242-269
+    `_nested_dims`, :597-606 and :656-658 (the meats), :886-906 (the CRV1
+    variances) and core/estimator.py:446-464 `_k_fe` (fe_dof "exact") for
+    REQUESTS, on the reference's own pass-2 scores `he` and group scores."""
+    from itertools import combinations
+    col = {"worker": gcode.astype(np.int64), "firm": codes[:, 0], "year": codes[:, 1]}
+    card = {"worker": G, "firm": int(nlev[0]), "year": int(nlev[1])}
+    fe_params = {"worker": G, "firm": int(nlev[0]), "year": int(nlev[1])}
+
+    def term(cols):
+        cs = set(cols)
+        if cs == {"worker"}:
+            return {"kind": "seg", "code": col["worker"], "G": G, "meat": meat_g}
+        key = np.zeros(N, np.int64)
+        for c in cols:
+            key = key * card[c] + col[c]
+        if len(cols) == 1:
+            code, Gt = col[cols[0]], card[cols[0]]
+            kind = "fe"
+        else:
+            _, code = np.unique(key, return_inverse=True)
+            Gt = int(code.max()) + 1
+            kind = "segsub" if "worker" in cs else "extra"
+        S = utils._scatter(code.astype(np.int64), he, Gt)
+        return {"kind": kind, "code": code, "G": Gt, "meat": S.T @ S}
+
+    def nested(t, cols):
+        out = []
+        for d in DIMS:
+            if set(cols) <= {d}:
+                out.append(d)
+                continue
+            if t["kind"] == "segsub":
+                continue
+            lo = np.full(card[d], np.iinfo(np.int64).max)
+            hi = np.full(card[d], -1)
+            np.minimum.at(lo, col[d], t["code"])
+            np.maximum.at(hi, col[d], t["code"])
+            if np.all(lo == hi):
+                out.append(d)
+        return out
+
+    def k_fe(nest):
+        comps = max((c for (a, b), c in pc.items() if a not in nest or b not in nest),
+                    default=1)
+        return sum(fe_params.values()) - (comps + len(DIMS) - 2)
+
+    out = {}
+    for req in REQUESTS:
+        parts = [[c.strip() for c in p_.split("^")] for p_ in req.split("+")]
+        terms = []
+        for r in range(1, len(parts) + 1):
+            for combo in combinations(range(len(parts)), r):
+                cols = list(dict.fromkeys(c for i in combo for c in parts[i]))
+                t = term(cols)
+                terms.append((t, (-1) ** (r + 1), r == 1, nested(t, cols)))
+        Gm = min(t["G"] for t, _, single, _ in terms if single)
+        nest = list(dict.fromkeys(d for *_, nd in terms for d in nd))
+        Kc = k + k_fe(nest) - sum(fe_params[d] for d in nest) + len(nest)
+        adj = Gm / (Gm - 1) * (N - 1) / (N - Kc)
+        out[req] = {"V": sum(sign * adj * (Binv @ t["meat"] @ Binv) for t, sign, _, _ in terms),
+                    "G": [t["G"] for t, _, single, _ in terms if single], "adj": adj,
+                    "nested": nest}
+    return out
 
 
 def main(root):
     kb = import_reference(root)["core.kernels_base"]
+    import importlib
+    utils = importlib.import_module("hdfe_stream.core.utils")
     out = {}
     for name in PANELS:
         g = np.load(HERE / f"{name}.npz")
@@ -107,6 +187,15 @@ def main(root):
         out[f"{name}_resid"] = e
         out[f"{name}_alpha"] = g_eff
         out[f"{name}_psi"] = gam_y[offs[0] + codes[:, 0]]
+        out[f"{name}_scores"] = he
+        pcs = [int(x) for x in g["pair_components"]]      # sorted keys of the pairs
+        pc = {("firm", "year"): pcs[0], ("worker", "firm"): pcs[1], ("worker", "year"): pcs[2]}
+        for req, res in cluster_variances(utils, gcode, codes, nlev, G, he, meat_g, Binv, k, N,
+                                          pc).items():
+            out[f"{name}_crv1_{req}_V"] = res["V"]
+            out[f"{name}_crv1_{req}_G"] = np.array(res["G"])
+            out[f"{name}_crv1_{req}_adj"] = np.array([res["adj"]])
+            print(name, req, "G", res["G"], "nested", res["nested"], "adj", res["adj"])
         print(name, "beta", beta, "rss", float(w @ (e * e)))
     np.savez_compressed(HERE / "assemble.npz", **out)
 

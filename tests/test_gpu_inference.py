@@ -67,3 +67,63 @@ def test_variances_on_a_device_fit(device):
     assert out["k_fe"] == v["k_fe"]
     for key in ("iid", "hetero", "CRV1"):
         assert rel(out["vcov"][key], v[key]) < 1e-9, key
+
+
+REQUESTS = ("firm", "worker+firm", "worker^firm", "firm+year")
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_cluster_requests_match_reference(device, name):
+    """CRV1 for cluster requests beyond the streamed dimension (another
+    dimension, two-way, a refinement of the streamed groups, two-way over the
+    non-streamed dimensions): the device's per-row scores against pass 2's
+    and the variances against the reference's formulas on its own Gamma."""
+    import torch
+    from hdfe_stream_b200 import fit, inference
+    g = load_golden(name)
+    a = load_golden("assemble")
+    drows = fit.DeviceRows.from_rows(golden_rows(g))
+    cells = fit.pass1(drows)
+    gamma = torch.as_tensor(g["gamma"])
+    scores = inference.row_scores(drows, cells, gamma, a[f"{name}_beta"]).cpu().numpy()
+    assert rel(scores, a[f"{name}_scores"]) < 1e-10
+    out = inference.estimate(drows, cells, gamma, clusters=REQUESTS,
+                             fe_names=("worker", "firm", "year"))
+    for req in REQUESTS:
+        assert out["clusters"][req]["G"] == [int(x) for x in a[f"{name}_crv1_{req}_G"]], req
+        assert abs(out["clusters"][req]["adj"] - a[f"{name}_crv1_{req}_adj"][0]) < 1e-12, req
+        assert rel(out["vcov"][f"CRV1:{req}"], a[f"{name}_crv1_{req}_V"]) < 1e-9, req
+
+
+def test_cluster_requests_with_an_extra_column_match_oracle(device):
+    """A request on a column that is not a fixed effect (a region of the
+    firms, given per row) and its two-way with the workers, on a weighted
+    device fit, against the oracle on the same Gamma."""
+    from hdfe_stream_b200 import fit, inference
+    from hdfe_stream_b200.simulate import pass0_layout, restrict_connected, simulate_panel
+    panel = simulate_panel(30_000, 3_000, 8, spell=(3, 8), p_move=0.1, weights=True, seed=9)
+    rows = pass0_layout(panel, restrict_connected(panel, (1, 1)))
+    region = (rows.codes[:, 0].astype(np.int64) * 7919) % 37
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    reqs = ("region", "worker+region", "firm^region")
+    out = inference.estimate(drows, res.cells, res.gamma, clusters=reqs,
+                             fe_names=("worker", "firm", "year"), extra={"region": region})
+    gamma = res.gamma.cpu().numpy()
+    starts = orc.row_starts(rows.gcode)
+    codes = np.asarray(rows.codes, np.int64)
+    nlev = np.asarray(rows.n_levels, np.int64)
+    offs = np.concatenate(([0], np.cumsum(nlev)[:-1]))
+    he = orc.row_scores(starts, codes, offs, rows.w, rows.V, gamma, out["beta"])
+    pcs = out["pair_components"]
+    pc = {("worker", "firm"): pcs[0], ("worker", "year"): pcs[1], ("firm", "year"): pcs[2]}
+    B = orc.variance_sums(starts, codes, offs, rows.w, rows.V, gamma, out["beta"])[0]
+    ref = orc.cluster_variances(he, rows.gcode, codes, nlev, np.linalg.inv(B), reqs,
+                                ("worker", "firm", "year"), pc, extra={"region": region})
+    for req in reqs:
+        V, Gs, adj, nest = ref[req]
+        assert out["clusters"][req]["G"] == list(Gs), req
+        assert out["clusters"][req]["nested"] == nest, req
+        assert abs(out["clusters"][req]["adj"] - adj) < 1e-12, req
+        assert rel(out["vcov"][f"CRV1:{req}"], V) < 1e-8, req
+    assert out["clusters"]["region"]["nested"] == ["firm"]

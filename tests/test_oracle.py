@@ -415,3 +415,37 @@ def test_am_interval_matches_reference():
         lo, hi, info = am_interval(lam, b1, theta1, g[f"{name}_weak{k}_sigma"], 0.05)
         want = g[f"{name}_weak{k}_interval"]
         assert rel([lo, hi, info["kappa"], info["z"], info["rho"]], want) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["akm_small", "akm_weighted", "akm_components"])
+def test_cluster_variances_match_reference(name):
+    """Pass 2's per-row scores and the CRV1 variances for cluster requests
+    beyond the streamed dimension -- another dimension, two-way
+    (inclusion-exclusion), a refinement of the streamed groups, two-way over
+    the non-streamed dimensions -- against the reference's own kernel outputs
+    and formulas (tests/golden/assemble.npz)."""
+    ga = load_golden("assemble")
+    g = load_golden(name)
+    rows = golden_rows(g)
+    starts = orc.row_starts(rows.gcode)
+    codes = np.asarray(rows.codes, np.int64)
+    nlev = np.asarray(rows.n_levels, np.int64)
+    offs = np.concatenate(([0], np.cumsum(nlev)[:-1]))
+    w = rows.w if rows.w is not None else np.ones(rows.n_rows)
+    he = orc.row_scores(starts, codes, offs, w, rows.V, g["gamma"], ga[f"{name}_beta"])
+    assert rel(he, ga[f"{name}_scores"]) < 1e-10
+    pcs = [int(x) for x in g["pair_components"]]
+    pc = {("firm", "year"): pcs[0], ("worker", "firm"): pcs[1], ("worker", "year"): pcs[2]}
+    Binv = np.linalg.inv(ga[f"{name}_B"])
+    reqs = ("firm", "worker+firm", "worker^firm", "firm+year")
+    out = orc.cluster_variances(he, rows.gcode, codes, nlev, Binv, reqs,
+                                ("worker", "firm", "year"), pc)
+    for req in reqs:
+        V, Gs, adj, _ = out[req]
+        assert list(Gs) == [int(x) for x in ga[f"{name}_crv1_{req}_G"]], req
+        assert abs(adj - ga[f"{name}_crv1_{req}_adj"][0]) < 1e-12, req
+        assert rel(V, ga[f"{name}_crv1_{req}_V"]) < 1e-9, req
+    # the one-way request on the streamed dimension is the kernel's own CRV1
+    V, Gs, adj, nest = orc.cluster_variances(he, rows.gcode, codes, nlev, Binv, ("worker",),
+                                             ("worker", "firm", "year"), pc)["worker"]
+    assert nest == ["worker"] and rel(V, ga[f"{name}_V_crv1"]) < 1e-9
