@@ -7,7 +7,9 @@ depend on size (the oracle would take minutes there):
 * the 1M-worker panel's leave-one-out set (8.5M rows): the KSS leave-out
   components recover the variances and covariance of the generator's true
   effects over the same rows, which they estimate without bias;
-* the weighted 400k-worker panel: residual and weighted normalisation.
+* the weighted 400k-worker panel: residual and weighted normalisation, and
+  the gradients through the fit against central finite differences on 1,000
+  random coordinates.
 """
 
 import numpy as np
@@ -120,3 +122,48 @@ def test_akm_400k_weighted_fit_properties(device):
     assert res.info["converged"]
     assert residual(res) < 1e-8
     assert normalisation(res) < 1e-10
+
+
+def test_adjoint_400k_matches_finite_differences(device):
+    """Gradients through the fit on the weighted 400k-worker panel (3.4M
+    rows) -- the age_squared coefficient and the plug-in var(psi) with
+    respect to y and the weights -- against central finite differences along
+    random directions on 1,000 random coordinates: in y with a unit step (the
+    objectives are linear and quadratic in y, so the difference is exact up to
+    the solves' tolerance), in the weights with a step of 1e-3."""
+    import torch
+    from hdfe_stream_b200.adjoint import FixedEffectsSolve, plug_in_components
+    from hdfe_stream_b200.simulate import prepare
+    rows = prepare("akm_400k_w", seed=300)
+    dev = device
+    t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), device=dev).to(dt)
+    gcode, codes = t(rows.gcode.view(np.int32), torch.int32), t(rows.codes.view(np.int32),
+                                                                  torch.int32)
+    X = t(rows.V[:, 1:], torch.float64)
+    nl = rows.n_levels
+
+    def objectives(y, w):
+        beta, gam, alpha, _ = FixedEffectsSolve.apply(y, w, gcode, codes, X, nl, 1e-13)
+        return beta[0], plug_in_components(gam, alpha, w, gcode, codes, nl)[0]
+
+    y = t(rows.V[:, 0], torch.float64).requires_grad_(True)
+    w = t(rows.w, torch.float64).requires_grad_(True)
+    b0, vpsi = objectives(y, w)
+    grads = [torch.autograd.grad(f, (y, w), retain_graph=True) for f in (b0, vpsi)]
+    rng = np.random.default_rng(17)
+    idx = torch.as_tensor(rng.choice(rows.n_rows, 1_000, replace=False), device=dev)
+    v = torch.zeros(rows.n_rows, dtype=torch.float64, device=dev)
+    v[idx] = torch.as_tensor(rng.choice([-1.0, 1.0], 1_000), device=dev)
+    y0, w0 = y.detach(), w.detach()
+
+    def values(yy, ww):
+        with torch.no_grad():
+            bb, vv = objectives(yy, ww)
+        return np.array([bb.item(), vv.item()])
+    fd_y = (values(y0 + v, w0) - values(y0 - v, w0)) / 2.0
+    h = 1e-3
+    fd_w = (values(y0, w0 + h * v) - values(y0, w0 - h * v)) / (2 * h)
+    for j, (gy, gw) in enumerate(grads):
+        an_y, an_w = float((gy * v).sum()), float((gw * v).sum())
+        assert abs(fd_y[j] - an_y) <= 1e-6 * abs(an_y) + 1e-14, (j, fd_y[j], an_y)
+        assert abs(fd_w[j] - an_w) <= 1e-4 * abs(an_w) + 1e-12, (j, fd_w[j], an_w)
