@@ -120,3 +120,27 @@ def test_weak_moments_and_interval_match_reference(device):
         assert rel(piece["sigma"], g[f"{name}_weak{k}_sigma"]) < 1e-6
         want = g[f"{name}_weak{k}_interval"]
         assert rel([*piece["interval"], piece["kappa"], piece["z"]], want[:4]) < 1e-6
+
+
+def test_weak_id_against_exact_prototype(device):
+    """The device's Lanczos eigenvalues of S^- Q against the reference's dense
+    exact prototype (prototypes/kss_exact.py `weak_id`, tests/golden/
+    exact_se.npz) to 1e-6, with q equal and sum lambda^2 within 10% at 64
+    draws."""
+    from hdfe_stream_b200 import fit, leaveout, leaveout_se
+    from hdfe_stream_b200.simulate import Rows
+    from hdfe_stream_b200.weakid import weak_id_diagnostics
+    g, ge = load_golden("exact"), load_golden("exact_se")
+    rows = Rows(gcode=g["gcode"], codes=g["codes_rows"], V=g["V"][:, :1], w=None,
+                n_levels=[int(x) for x in g["n_levels"]], n_groups=int(g["n_groups"][0]),
+                names=["log_earn"])
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    op = leaveout.InverseOperator(drows, res.cells, res.S, None, tol=1e-12)
+    kss = op.leave_out_components(res.gamma, 256, block=32, seed=3)
+    out = weak_id_diagnostics(leaveout_se.StandardErrors(op), kss["sigma2"], kss["leverage"],
+                              n_draws=64, block=32, seed=9)
+    for k in range(3):
+        assert rel(out["eigenvalues"][k], ge[f"weak_eig{k}"]) < 1e-6
+    assert list(out["q"]) == [int(x) for x in ge["weak_q"]]
+    assert np.all(np.abs(out["sum_sq"] - ge["weak_sum_sq"]) <= 0.1 * ge["weak_sum_sq"])

@@ -449,3 +449,33 @@ def test_cluster_variances_match_reference(name):
     V, Gs, adj, nest = orc.cluster_variances(he, rows.gcode, codes, nlev, Binv, ("worker",),
                                              ("worker", "firm", "year"), pc)["worker"]
     assert nest == ["worker"] and rel(V, ga[f"{name}_V_crv1"]) < 1e-9
+
+
+def test_standard_errors_and_weak_id_against_exact_prototype():
+    """The observation-level standard errors (512 JLA probes, B_ii and trace
+    draws) and the weak-identification diagnostic against the reference's
+    dense exact prototype on the exact panel (prototypes/kss_exact.py
+    `kss_se` with the smoothed sigma2 and `weak_id`; tests/golden/
+    exact_se.npz): theta within 0.5%, V and its first term within 3%, the
+    trace term within 10%; the Lanczos eigenvalues to 1e-6 (no Monte Carlo
+    in them), sum lambda^2 within 10% at 64 draws, q equal, F within 10%."""
+    g, ge = load_golden("exact"), load_golden("exact_se")
+    rows = exact_rows(g)
+    c = orc.pass1(rows)
+    S = orc.build_explicit(c)
+    gamma, _ = orc.solve(c, S, tol=1e-12)
+    des = orc.Design(rows, c, S, tol=1e-12)
+    out = des.leave_out_components(gamma, 512, 32, 3)
+    lev, comp, factor = des.jla_leverages(512, 32, 3)
+    se = des.component_variances(out["sigma2"], lev, comp, factor, des.bii_rows(512, 32, 8), 512,
+                                 32, 8)
+    for key, ek, tol in (("theta", "se_theta", 0.005), ("variance", "se_V", 0.03),
+                         ("first_term", "se_V_first_term", 0.03),
+                         ("trace_term", "se_V_trace_term", 0.1)):
+        assert np.all(np.abs(se[key] - ge[ek]) <= tol * np.abs(ge[ek])), key
+    wid = orc.weak_id_diagnostics(des, out["sigma2"], lev, n_draws=64, block=32, seed=9)
+    for k in range(3):
+        assert rel(wid["eigenvalues"][k], ge[f"weak_eig{k}"]) < 1e-6
+    assert np.all(np.abs(wid["sum_sq"] - ge["weak_sum_sq"]) <= 0.1 * ge["weak_sum_sq"])
+    assert list(wid["q"]) == [int(x) for x in ge["weak_q"]]
+    assert np.all(np.abs(wid["f_stat"] - ge["weak_f_stat"]) <= 0.1 * ge["weak_f_stat"])
