@@ -281,7 +281,8 @@ class FitResult:
 
 
 def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
-          x0=None, normalize_fe=True, timer=None, precision="fp64", comps=None) -> FitResult:
+          x0=None, normalize_fe=True, timer=None, precision="fp64", comps=None,
+          solver="explicit") -> FitResult:
     """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
     right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
     zero, block PCG per `rhs_block` columns, then `_normalize`.  `comps`:
@@ -291,8 +292,14 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     timer = timer or _NoTimer()
     m = int(cells.rhs.shape[1])
     dinv = jacobi(cells.diag)
-    solver = BlockSolver(S, dinv, tol, maxiter, precision=precision)
-    solver.timer = timer
+    if solver == "stream_cg":
+        from .gpu import StreamSolver
+        solver = StreamSolver(cells, dinv, tol, maxiter)
+    elif solver == "explicit":
+        solver = BlockSolver(S, dinv, tol, maxiter, precision=precision)
+        solver.timer = timer
+    else:
+        raise ValueError("solver must be 'explicit' or 'stream_cg'")
     scale = torch.sqrt(torch.clamp(cells.raw_ss, min=0.0))
     zero_all = (torch.linalg.vector_norm(cells.rhs, dim=0) <= RHS_ZERO_TOL * scale).cpu().numpy()
     if comps is None:
@@ -315,10 +322,13 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     n_comp = ncomp.cpu().numpy()
     if int(n_comp[1]) != _lib.HDFE_OK:
         raise _lib.HDFEError(int(n_comp[1]), "components: union-find failed")
-    info = {"solver": "explicit", "device": "cuda", "iterations": its if len(its) > 1 else its[0],
-            "converged": conv, "max_rel_residual": rel, "S_nnz": S.nnz,
-            "S_mb": round(S.nbytes / 1e6, 1), "n_components": int(n_comp[0]),
-            "fe_spanned": [j for j in range(m) if zero_all[j]]}
+    explicit = S is not None and not hasattr(solver, "matvec")
+    info = {"solver": "explicit" if explicit else "stream_cg", "device": "cuda",
+            "iterations": its if len(its) > 1 else its[0],
+            "converged": conv, "max_rel_residual": rel,
+            "S_nnz": S.nnz if explicit else None,
+            "S_mb": round(S.nbytes / 1e6, 1) if explicit else None,
+            "n_components": int(n_comp[0]), "fe_spanned": [j for j in range(m) if zero_all[j]]}
     return FitResult(gamma=gamma, info=info, cells=cells, S=S, root=root)
 
 

@@ -181,6 +181,114 @@ class BlockSolver:
         return X.cpu().numpy(), it, conv, rel
 
 
+class StreamSolver:
+    """The `stream_cg` solver (core/solve.py:251-266): the same Jacobi block
+    PCG (core/solve.py:66-140, step for step: per-column alpha and beta, the
+    active mask, `zero` columns, warm start, rel = ||R|| / ||B||) with S P
+    computed from pass 1's identifying cells every iteration
+    (`hdfe_stream_matvec`) instead of from an explicit S.  The reference
+    falls back to it when S does not fit its memory budget; here it serves the
+    same role for a caller that would rather not hold S.  The iteration is
+    driven from the host (one read of the active mask per iteration), the
+    product and the vector updates run on the device."""
+
+    def __init__(self, cells, dinv, tol: float, maxiter: int, debug=None):
+        import torch
+        self.cells = cells
+        self.dev = cells.starts.device
+        self.dinv = dinv.to(self.dev, torch.float64).contiguous() if torch.is_tensor(dinv) \
+            else torch.as_tensor(np.asarray(dinv, np.float64), device=self.dev)
+        self.tol, self.maxiter, self.debug = float(tol), int(maxiter), debug
+        self._nlev = np.asarray(cells.n_levels, dtype=np.int64)
+        self._status = torch.zeros(1, dtype=torch.int32, device=self.dev)
+
+    def matvec(self, P):
+        """S P (P (L, k), k <= 32) from the cells."""
+        import torch
+        P = P.contiguous()
+        out = torch.empty_like(P)
+        c = self.cells
+        _lib.check(_lib.lib().hdfe_stream_matvec(
+            c.starts.data_ptr(), int(c.starts.shape[0]) - 1, c.codes.data_ptr(),
+            len(self._nlev), self._nlev.ctypes.data, c.n.data_ptr(), P.data_ptr(), P.shape[1],
+            out.data_ptr(), self._status.data_ptr(), _lib.stream_handle()))
+        return out
+
+    def _solve_block(self, B, zero, X0):
+        import torch
+        L, k = B.shape
+        bnorm = torch.linalg.vector_norm(B, dim=0)
+        bnorm = torch.where(bnorm == 0, torch.ones_like(bnorm), bnorm)
+        if X0 is None:
+            X = torch.zeros_like(B)
+            R = B.clone()
+        else:
+            X = X0.clone()
+            R = B - self.matvec(X)
+        zero_t = torch.zeros(k, dtype=torch.bool, device=self.dev) if zero is None else \
+            torch.as_tensor(np.asarray(zero, bool), device=self.dev)
+        if bool(zero_t.any()):
+            X[:, zero_t] = 0.0
+            R[:, zero_t] = 0.0
+            if bool(zero_t.all()):
+                return X, 0, True, 0.0
+        active = ~zero_t
+        rel = torch.zeros(k, dtype=torch.float64, device=self.dev)
+        if X0 is not None:
+            rel = torch.linalg.vector_norm(R, dim=0) / bnorm
+            active &= rel > self.tol
+            if not bool(active.any()):
+                return X, 0, True, float(rel.max())
+        d = self.dinv[:, None]
+        P = R * d
+        rz = (R * P).sum(0)
+        it = 0
+        for it in range(1, self.maxiter + 1):
+            AP = self.matvec(P)
+            pAp = (P * AP).sum(0)
+            alpha = torch.where(active & (pAp > 0), rz / torch.where(pAp > 0, pAp, 1.0),
+                                torch.zeros_like(pAp))
+            X += alpha * P
+            R -= alpha * AP
+            rel = torch.sqrt((R * R).sum(0)) / bnorm
+            rz_new = (R * R * d).sum(0)
+            active = rel > self.tol
+            if not bool(active.any()):
+                break
+            beta = torch.where(active, rz_new / torch.where(rz != 0, rz, 1.0),
+                               torch.zeros_like(rz))
+            P = R * d + beta * P
+            rz = rz_new
+        if int(self._status.item()) != _lib.HDFE_OK:
+            raise _lib.HDFEError(int(self._status.item()), "stream_cg: a level code is out of range")
+        return X, it, not bool(active.any()), float(rel.max())
+
+    def solve_device(self, B, zero=None, X0=None):
+        import torch
+        B = B.to(self.dev, torch.float64).contiguous()
+        L, k = B.shape
+        X = torch.empty_like(B)
+        its, conv, rel = 0, True, 0.0
+        zero = None if zero is None else np.asarray(zero, bool)
+        for j0 in range(0, k, 32):
+            j1 = min(k, j0 + 32)
+            X0j = None if X0 is None else X0[:, j0:j1].to(self.dev, torch.float64)
+            Xj, it, c, r = self._solve_block(B[:, j0:j1], None if zero is None else zero[j0:j1],
+                                             X0j)
+            X[:, j0:j1] = Xj
+            its, conv, rel = max(its, it), conv and c, max(rel, r)
+        if self.debug is not None:
+            self.debug(f"  CG iter {its}: max rel. residual {rel:.2e}")
+        return X, its, conv, rel
+
+    def __call__(self, b, zero=None, x0=None):
+        import torch
+        B = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float64)).to(self.dev)
+        X0 = None if x0 is None else torch.as_tensor(np.ascontiguousarray(x0, np.float64)).to(self.dev)
+        X, it, conv, rel = self.solve_device(B, zero, X0)
+        return X.cpu().numpy(), it, conv, rel
+
+
 def explicit_solver(S, dinv, tol, maxiter, debug=None):
     """(solve(b, zero, x0) -> (X, iterations, converged, rel), device name):
     S (scipy CSR) and the preconditioner are copied to the device here, once

@@ -224,3 +224,24 @@ def test_stream_matvec_matches_explicit_s(device, k):
         got = out.cpu().numpy()
         assert int(st.item()) == 0
         assert np.max(np.abs(got - ref)) < 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("name", list(GOLDEN_PANELS) + ["weighted"])
+def test_stream_cg_matches_explicit(device, name):
+    """The `stream_cg` solver (S P from the cells every iteration) gives the
+    explicit solve's fixed effects (1e-9) with iterations within one, and
+    the oracle's PCG on the explicit S."""
+    from hdfe_stream_b200 import fit
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    rows = (golden_rows(load_golden(name)) if name != "weighted" else
+            pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(3, 10), p_move=0.1,
+                                        weights=True, seed=13)))
+    drows = fit.DeviceRows.from_rows(rows)
+    cells = fit.pass1(drows)
+    want = fit.solve(cells, fit.build_s(cells), tol=1e-12)
+    got = fit.solve(cells, None, tol=1e-12, solver="stream_cg")
+    assert got.info["solver"] == "stream_cg" and got.info["converged"]
+    g, w = got.gamma.cpu().numpy(), want.gamma.cpu().numpy()
+    assert np.max(np.abs(g - w)) <= 1e-9 * np.max(np.abs(w))
+    its = np.atleast_1d(got.info["iterations"]) - np.atleast_1d(want.info["iterations"])
+    assert np.all(np.abs(its) <= 1)
