@@ -243,7 +243,8 @@ __global__ void __launch_bounds__(kThreads) k_variance(Args a, const double *Gam
 // into the clusters of a CRV1 term that is not the streamed dimension.
 template <int M>
 __global__ void __launch_bounds__(kThreads) k_scores(Args a, const double *Gamma,
-                                                     const double *beta, double *out)
+                                                     const double *beta, double *out,
+                                                     double *h_out)
 {
     constexpr int KX = M - 1;
     double b[KX];
@@ -290,6 +291,10 @@ __global__ void __launch_bounds__(kThreads) k_scores(Args a, const double *Gamma
             const double we = wi * (u - mu);
 #pragma unroll
             for (int j = 0; j < KX; j++) out[i * KX + j] = we * h[j];
+            if (h_out) {
+#pragma unroll
+                for (int j = 0; j < KX; j++) h_out[i * KX + j] = h[j];
+            }
         }
     }
 }
@@ -496,7 +501,8 @@ extern "C" int hdfe_variance_sums(const int64_t *starts, int64_t n_groups, const
 extern "C" int hdfe_row_scores(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
                                int32_t D, const int64_t *n_levels, const double *w,
                                const double *V, int32_t m, int64_t n_rows, const double *Gamma,
-                               const double *beta, double *out, void *status, void *stream)
+                               const double *beta, double *out, double *h_out, void *status,
+                               void *stream)
 {
     assemble::Args a;
     int st = assemble::fill(a, starts, n_groups, codes, D, n_levels, w, V, m, n_rows,
@@ -506,7 +512,8 @@ extern "C" int hdfe_row_scores(const int64_t *starts, int64_t n_groups, const ui
         return hdfe_set_arg_error("hdfe_row_scores: bad argument (2 <= m <= 8)");
     cudaStream_t s = (cudaStream_t)stream;
     const unsigned grid = assemble::grid_for(n_groups);
-#define HDFE_SCORES(M) assemble::k_scores<M><<<grid, assemble::kThreads, 0, s>>>(a, Gamma, beta, out)
+#define HDFE_SCORES(M) assemble::k_scores<M><<<grid, assemble::kThreads, 0, s>>>(a, Gamma, beta, out, \
+                                                                                h_out)
     switch (m) {
     case 2: HDFE_SCORES(2); break;
     case 3: HDFE_SCORES(3); break;

@@ -68,8 +68,9 @@ def fe_pair_components(rows: DeviceRows, cells: DeviceCells):
     return counts
 
 
-def row_scores(rows: DeviceRows, cells: DeviceCells, gamma, beta):
-    """The per-row scores w e h (N, m - 1) of pass 2 (`hdfe_row_scores`)."""
+def row_scores(rows: DeviceRows, cells: DeviceCells, gamma, beta, with_h=False):
+    """The per-row scores w e h (N, m - 1) of pass 2 (`hdfe_row_scores`);
+    with_h: also the residualised covariates h, as (scores, h)."""
     torch = _torch()
     lib = _lib.lib()
     dev = rows.gcode.device
@@ -78,20 +79,22 @@ def row_scores(rows: DeviceRows, cells: DeviceCells, gamma, beta):
     gamma = gamma.to(dev, torch.float64).contiguous()
     beta_d = torch.as_tensor(np.asarray(beta, np.float64), device=dev)
     out = torch.empty((rows.n_rows, rows.m - 1), dtype=torch.float64, device=dev)
+    h = torch.empty_like(out) if with_h else None
     status = torch.zeros(1, dtype=torch.int32, device=dev)
     w = rows.w
     _lib.check(lib.hdfe_row_scores(starts.data_ptr(), G, rows.codes.data_ptr(), len(nlev),
                                    nlev.ctypes.data, None if w is None else w.data_ptr(),
                                    rows.V.data_ptr(), rows.m, rows.n_rows, gamma.data_ptr(),
-                                   beta_d.data_ptr(), out.data_ptr(), status.data_ptr(),
+                                   beta_d.data_ptr(), out.data_ptr(),
+                                   None if h is None else h.data_ptr(), status.data_ptr(),
                                    _lib.stream_handle()))
     if int(status.item()) != _lib.HDFE_OK:
         raise _lib.HDFEError(int(status.item()), "row_scores: a level code is out of range")
-    return out
+    return (out, h) if with_h else out
 
 
 def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_components,
-                 group_meat=None, extra=None):
+                 group_meat=None, extra=None, crv3=(), h=None, B=None):
     """CRV1 variances for cluster requests (core/inference.py:176-240
     `_resolve_clusters`, :242-269 `_nested_dims`, :886-906): a request "a",
     "a^b" (one cluster per distinct combination) or "a+b" (two-way,
@@ -104,7 +107,15 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
     the streamed groups) every level lies within one cluster; K drops the
     nested dimensions' levels (core/estimator.py:446-464 `_k_fe` with the
     pairs whose both dimensions are nested left out); G is the smallest
-    one-way count.  Returns {request: (V, {"G", "adj", "nested"})}."""
+    one-way count.  Returns {request: (V, {"G", "adj", "nested"})}.
+
+    `crv3` lists one-way requests that also get the cluster jackknife
+    (core/inference.py:270-298, core/kernels_base.py:620-680): leaving
+    cluster g out moves beta by -(B - A_g)^+ s_g, with A_g the cluster's sum
+    of w h h' and s_g its sum of w e h, so CRV3 = adj sum_g d_g d_g' (the
+    CRV1 factor), from h (N, k) and the bread B; every fixed-effect dimension
+    must be nested in the clusters (else ValueError).  Its entries come back
+    under "CRV3:<request>"."""
     torch = _torch()
     from itertools import combinations
     dev = rows.gcode.device
@@ -140,7 +151,8 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
             _, code = torch.unique(key, sorted=True, return_inverse=True)
             G = int(code.max().item()) + 1 if N else 0
             kind = "segsub" if g0 in cs else ("fe" if len(cols) == 1 else "extra")
-        if kind == "seg" and group_meat is not None:
+        S = None
+        if kind == "seg" and group_meat is not None and key_name not in crv3_terms:
             meat = group_meat
         else:
             S = torch.zeros((G, k), dtype=torch.float64, device=dev).index_add_(0, code, scores)
@@ -159,7 +171,7 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
                 0, col[d], code, "amax")
             if bool((lo == hi).all().item()):
                 nested.append(d)
-        cache[key_name] = (G, meat, nested)
+        cache[key_name] = (G, meat, nested, code, S)
         return cache[key_name]
 
     def k_fe(nest):
@@ -170,8 +182,13 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
                      if a not in nest or b not in nest), default=1)
         return total - (comps + len(fe_params) - 2)
 
+    crv3_terms = set()
+    for req in crv3:
+        if "+" in req:
+            raise ValueError(f"CRV3 takes a one-way cluster request, not {req!r}")
+        crv3_terms.add("^".join(dict.fromkeys(c.strip() for c in req.split("^"))))
     out = {}
-    for req in requests:
+    for req in list(dict.fromkeys(list(requests) + list(crv3))):
         parts = [[c.strip() for c in p.split("^")] for p in req.split("+")]
         terms = []
         for r in range(1, len(parts) + 1):
@@ -185,18 +202,52 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
         adj = Gm / (Gm - 1) * (N - 1) / (N - Kc)
         V = sum(sign * adj * (Binv @ t[1] @ Binv) for t, sign, _ in terms)
         out[req] = (V, {"G": Gs, "adj": adj, "nested": nest, "df": Gm - 1})
+        if req in crv3:
+            (t, _, _), = terms
+            loose = [d for d in fe_dims if d not in t[2]]
+            if loose:
+                raise ValueError(
+                    f"CRV3 standard errors need every fixed effect to be nested within the "
+                    f"clusters, and {', '.join(map(repr, loose))} "
+                    f"{'is' if len(loose) == 1 else 'are'} not nested within {req!r}; "
+                    "only CRV1 is supported there")
+            if h is None or B is None:
+                raise ValueError("CRV3 needs the residualised covariates h and the bread B")
+            G, _, _, code, S = t
+            jack = crv3_jack(code, G, rows.w, h, S, B)
+            out["CRV3:" + req] = (adj * jack, {"G": Gs, "adj": adj, "nested": nest,
+                                               "df": Gm - 1})
     return out
 
 
+def crv3_jack(code, G, w, h, S, B):
+    """sum over clusters of d_g d_g', d_g = (B - A_g)^+ s_g (core/kernels_base.py:
+    658-680 `_nb_crv3_scatter` / `_nb_crv3_finish`): code (N,) cluster ids, w
+    (N,) or None, h (N, k) the residualised covariates, S (G, k) the clusters'
+    sums of w e h, B the bread; A_g by a device index-add of w h h', the
+    pseudo-inverses batched on the device."""
+    torch = _torch()
+    N, k = h.shape
+    dev = h.device
+    w = w if w is not None else torch.ones(N, dtype=torch.float64, device=dev)
+    outer = (w[:, None, None] * h[:, :, None] * h[:, None, :]).reshape(N, k * k)
+    AG = torch.zeros((G, k * k), dtype=torch.float64, device=dev).index_add_(
+        0, code, outer).reshape(G, k, k)
+    Bd = torch.as_tensor(np.asarray(B, np.float64), device=dev)
+    d = (torch.linalg.pinv(Bd[None] - AG) @ S[:, :, None])[:, :, 0]
+    return (d.T @ d).cpu().numpy()
+
+
 def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=None,
-             extra=None):
+             extra=None, crv3=()):
     """beta (k,) and its variances for y = V[0] on X = V[1:] with the fit's
     normalised effects gamma (L, m): {"beta", "vcov": {"iid", "hetero",
     "CRV1", "CRV1:<request>" ...}, "se": {...}, "k_fe", "df_resid",
     "df_cluster", "rss", "pair_components", "n_obs", "n_groups"}; "CRV1"
     clusters on the streamed dimension; `clusters` adds the requests of
     `cluster_vcov` (names from `fe_names`, default "fe0" for the streamed
-    dimension and "fe1", "fe2", ... for the others, or from `extra`)."""
+    dimension and "fe1", "fe2", ... for the others, or from `extra`); `crv3`
+    one-way requests that also get the cluster jackknife ("CRV3:<request>")."""
     torch = _torch()
     lib = _lib.lib()
     m = rows.m
@@ -245,7 +296,7 @@ def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=
     vcov = {"iid": rss / (N - K) * Binv, "hetero": N / (N - K) * Binv @ meat_hc @ Binv,
             "CRV1": adj * Binv @ meat_g @ Binv}
     cluster_info = {}
-    if clusters:
+    if clusters or crv3:
         names = list(fe_names) if fe_names else [f"fe{d}" for d in range(len(nlev) + 1)]
         D = len(nlev)
         pair = {}
@@ -256,10 +307,15 @@ def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=
             for d2 in range(d1 + 1, D):
                 pair[(names[d1 + 1], names[d2 + 1])] = pcs[j]
                 j += 1
-        scores = row_scores(rows, cells, gamma, beta)
+        if crv3:
+            scores, h = row_scores(rows, cells, gamma, beta, with_h=True)
+        else:
+            scores, h = row_scores(rows, cells, gamma, beta), None
         for req, (V, info) in cluster_vcov(rows, scores, Binv, k, clusters, names, pair,
-                                           group_meat=meat_g, extra=extra).items():
-            vcov[f"CRV1:{req}"] = V
+                                           group_meat=meat_g, extra=extra, crv3=crv3, h=h,
+                                           B=B).items():
+            key = req if req.startswith("CRV3:") else f"CRV1:{req}"
+            vcov[key] = V
             cluster_info[req] = info
     return {"beta": beta, "vcov": vcov,
             "se": {key: np.sqrt(np.diag(v)) for key, v in vcov.items()},

@@ -357,11 +357,13 @@ int hdfe_variance_sums(const int64_t *starts, int64_t n_groups, const uint32_t *
 /* hdfe_row_scores: the same row pass's per-row scores w e h, out (N, m - 1)
  * row-major (core/inference.py:594-603 `he`), which pass 2 sums per cluster
  * for a CRV1 term other than the streamed dimension (core/inference.py:
- * 509-510, 597-606, 656-658).  2 <= m <= 8. */
+ * 509-510, 597-606, 656-658); h_out (N, m - 1) or NULL: the residualised
+ * covariates h themselves (the per-cluster sums w h h' of the CRV3
+ * jackknife, core/kernels_base.py:658-670).  2 <= m <= 8. */
 int hdfe_row_scores(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
                     const int64_t *n_levels, const double *w, const double *V, int32_t m,
                     int64_t n_rows, const double *Gamma, const double *beta, double *out,
-                    void *status, void *stream);
+                    double *h_out, void *status, void *stream);
 
 int hdfe_kss_sigma2(const double *y, const double *w, const double *resid,
                     const double *complement, const double *factor, double ybar,

@@ -648,9 +648,9 @@ def variance_sums(starts, codes, offs, w, V, Gamma, beta):
     return B, he.T @ he, sg.T @ sg, float(w @ (e * e))
 
 
-def row_scores(starts, codes, offs, w, V, Gamma, beta):
+def row_scores(starts, codes, offs, w, V, Gamma, beta, with_h=False):
     """The per-row scores w e h of core/inference.py:594-603 (`he`), the
-    rows pass 2 sums per cluster."""
+    rows pass 2 sums per cluster; with_h: (he, h)."""
     codes = np.asarray(codes, dtype=np.int64)
     H = np.asarray(V[:, 1:], dtype=np.float64).copy()
     for d in range(codes.shape[1]):
@@ -659,7 +659,25 @@ def row_scores(starts, codes, offs, w, V, Gamma, beta):
     H -= np.repeat(np.add.reduceat(w[:, None] * H, starts[:-1], axis=0) / Wg[:, None],
                    np.diff(starts), axis=0)
     e, _, _, _ = row_effects(starts, codes, offs, w, V, Gamma, beta)
-    return H * (w * e)[:, None]
+    he = H * (w * e)[:, None]
+    return (he, H) if with_h else he
+
+
+def crv3_jack(code, w, H, he, B):
+    """core/kernels_base.py:658-680 `_nb_crv3_scatter` and `_nb_crv3_finish`:
+    the sum over clusters of d_g d_g', d_g = pinv(B - A_g) s_g with A_g the
+    cluster's sum of w h h' and s_g its sum of w e h."""
+    code = np.asarray(code, np.int64)
+    G, k = int(code.max()) + 1, H.shape[1]
+    AG = np.zeros((G, k, k))
+    np.add.at(AG, code, w[:, None, None] * H[:, :, None] * H[:, None, :])
+    sG = np.zeros((G, k))
+    np.add.at(sG, code, he)
+    acc = np.zeros((k, k))
+    for g in range(G):
+        d = np.linalg.pinv(B - AG[g]) @ sG[g]
+        acc += np.outer(d, d)
+    return acc
 
 
 def cluster_variances(he, gcode, codes, n_levels, Binv, requests, names, pair_components,

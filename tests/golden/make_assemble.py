@@ -188,6 +188,18 @@ def main(root):
         out[f"{name}_alpha"] = g_eff
         out[f"{name}_psi"] = gam_y[offs[0] + codes[:, 0]]
         out[f"{name}_scores"] = he
+        # the CRV3 jackknife sums of core/kernels_base.py:620-680 (the kernels
+        # alone: whether the request is valid is the caller's check)
+        nt = 4
+        acc = np.zeros((nt, k, k))
+        kb._nb_crv3_groups(starts, w, e, np.ascontiguousarray(zt), B, acc)
+        out[f"{name}_crv3_worker_jack"] = acc.sum(axis=0)
+        nf = int(nlev[0])
+        AG, sG = np.zeros((nf, k, k)), np.zeros((nf, k))
+        kb._nb_crv3_scatter(codes[:, 0].astype(np.int64), w, e, np.ascontiguousarray(zt), AG, sG)
+        acc = np.zeros((nt, k, k))
+        kb._nb_crv3_finish(B, AG, sG, acc)
+        out[f"{name}_crv3_firm_jack"] = acc.sum(axis=0)
         pcs = [int(x) for x in g["pair_components"]]      # sorted keys of the pairs
         pc = {("firm", "year"): pcs[0], ("worker", "firm"): pcs[1], ("worker", "year"): pcs[2]}
         for req, res in cluster_variances(utils, gcode, codes, nlev, G, he, meat_g, Binv, k, N,

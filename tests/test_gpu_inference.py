@@ -127,3 +127,74 @@ def test_cluster_requests_with_an_extra_column_match_oracle(device):
         assert abs(out["clusters"][req]["adj"] - adj) < 1e-12, req
         assert rel(out["vcov"][f"CRV1:{req}"], V) < 1e-8, req
     assert out["clusters"]["region"]["nested"] == ["firm"]
+
+
+@pytest.mark.parametrize("name", GOLDEN_PANELS)
+def test_crv3_jackknife_matches_reference(device, name):
+    """The device's CRV3 jackknife sums by worker and by firm against the
+    reference's `_nb_crv3_*` kernels on its own Gamma."""
+    import torch
+    from hdfe_stream_b200 import fit, inference
+    g = load_golden(name)
+    a = load_golden("assemble")
+    rows = golden_rows(g)
+    drows = fit.DeviceRows.from_rows(rows)
+    cells = fit.pass1(drows)
+    he, h = inference.row_scores(drows, cells, torch.as_tensor(g["gamma"]), a[f"{name}_beta"],
+                                 with_h=True)
+    for key, code in (("worker", drows.gcode.to(torch.int64)),
+                      ("firm", drows.codes[:, 0].to(torch.int64))):
+        G = int(code.max().item()) + 1
+        S = torch.zeros((G, he.shape[1]), dtype=torch.float64, device=he.device)
+        S.index_add_(0, code, he)
+        jack = inference.crv3_jack(code, G, drows.w, h, S, a[f"{name}_B"])
+        assert rel(jack, a[f"{name}_crv3_{key}_jack"]) < 1e-9, key
+
+
+def regions_panel(n_regions=30, seed=0):
+    """Regions with their own workers and firms (no one moves between
+    regions), so that both fixed effects are nested in the region clusters."""
+    from hdfe_stream_b200.simulate import Panel, pass0_layout, simulate_panel
+    parts = [simulate_panel(300, 30, 6, spell=(3, 6), p_move=0.2, weights=True, seed=seed + r)
+             for r in range(n_regions)]
+    cat = lambda f: np.concatenate([getattr(p, f) for p in parts])
+    panel = Panel(worker=np.concatenate([p.worker + 300 * r for r, p in enumerate(parts)]),
+                  firm=np.concatenate([p.firm + 30 * r for r, p in enumerate(parts)]),
+                  year=cat("year"), log_earn=cat("log_earn"), age_squared=cat("age_squared"),
+                  age_cubed=cat("age_cubed"), weight=cat("weight"))
+    rows = pass0_layout(panel, year_fe=False)      # year effects would span the regions
+    firms = np.unique(panel.firm)
+    return rows, firms[rows.codes[:, 0]] // 30
+
+
+def test_crv3_on_nested_regions_matches_oracle(device):
+    """CRV3 by region (worker and firm effects, both nested in the regions)
+    and CRV1 by region on a device fit of 30 separate regions, against the
+    oracle on the same Gamma; CRV3 on a request whose fixed effects are not
+    nested is refused (firm clusters: the workers move between firms)."""
+    from hdfe_stream_b200 import fit, inference
+    rows, region = regions_panel()
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    names = ("worker", "firm")
+    out = inference.estimate(drows, res.cells, res.gamma, clusters=("region",), fe_names=names,
+                             extra={"region": region}, crv3=("region",))
+    assert sorted(out["clusters"]["region"]["nested"]) == ["firm", "worker"]
+    gamma = res.gamma.cpu().numpy()
+    starts = orc.row_starts(rows.gcode)
+    codes = np.asarray(rows.codes, np.int64)
+    nlev = np.asarray(rows.n_levels, np.int64)
+    offs = np.concatenate(([0], np.cumsum(nlev)[:-1]))
+    he, H = orc.row_scores(starts, codes, offs, rows.w, rows.V, gamma, out["beta"], with_h=True)
+    B = orc.variance_sums(starts, codes, offs, rows.w, rows.V, gamma, out["beta"])[0]
+    pc = {("worker", "firm"): out["pair_components"][0]}
+    assert pc[("worker", "firm")] == 30
+    V1, Gs, adj, nest = orc.cluster_variances(he, rows.gcode, codes, nlev, np.linalg.inv(B),
+                                              ("region",), names, pc,
+                                              extra={"region": region})["region"]
+    assert Gs == [30] and sorted(nest) == ["firm", "worker"]
+    assert rel(out["vcov"]["CRV1:region"], V1) < 1e-8
+    V3 = adj * orc.crv3_jack(region, rows.w, H, he, B)
+    assert rel(out["vcov"]["CRV3:region"], V3) < 1e-8
+    with pytest.raises(ValueError):
+        inference.estimate(drows, res.cells, res.gamma, fe_names=names, crv3=("firm",))

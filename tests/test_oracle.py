@@ -479,3 +479,24 @@ def test_standard_errors_and_weak_id_against_exact_prototype():
     assert np.all(np.abs(wid["sum_sq"] - ge["weak_sum_sq"]) <= 0.1 * ge["weak_sum_sq"])
     assert list(wid["q"]) == [int(x) for x in ge["weak_q"]]
     assert np.all(np.abs(wid["f_stat"] - ge["weak_f_stat"]) <= 0.1 * ge["weak_f_stat"])
+
+
+@pytest.mark.parametrize("name", ["akm_small", "akm_weighted", "akm_components"])
+def test_crv3_jackknife_matches_reference(name):
+    """The CRV3 jackknife sums (core/kernels_base.py `_nb_crv3_groups`,
+    `_nb_crv3_scatter`, `_nb_crv3_finish`: sum over clusters of d_g d_g',
+    d_g = pinv(B - A_g) s_g) by worker and by firm against the reference's
+    kernels on its own pass-2 outputs (tests/golden/assemble.npz)."""
+    ga = load_golden("assemble")
+    g = load_golden(name)
+    rows = golden_rows(g)
+    starts = orc.row_starts(rows.gcode)
+    codes = np.asarray(rows.codes, np.int64)
+    nlev = np.asarray(rows.n_levels, np.int64)
+    offs = np.concatenate(([0], np.cumsum(nlev)[:-1]))
+    w = rows.w if rows.w is not None else np.ones(rows.n_rows)
+    he, H = orc.row_scores(starts, codes, offs, w, rows.V, g["gamma"], ga[f"{name}_beta"],
+                           with_h=True)
+    B = ga[f"{name}_B"]
+    for key, code in (("worker", rows.gcode), ("firm", codes[:, 0])):
+        assert rel(orc.crv3_jack(code, w, H, he, B), ga[f"{name}_crv3_{key}_jack"]) < 1e-9, key
