@@ -162,9 +162,9 @@ def phase_bytes(rows, counts, S, iterations, m=3):
 
 
 # DRAM bytes (read + write) of one PCG iteration on the 5M-worker panel, from
-# an ncu capture of pcg_kernel<3> in this bench's own command: 6.79 GB over
+# an ncu capture of pcg_kernel<3> in this bench's own command: 5.34 GB over
 # 19 iterations and the set-up
-PCG_DRAM_BYTES_PER_ITER = 6.785702912e9 / 19
+PCG_DRAM_BYTES_PER_ITER = (5241279232 + 95878656) / 19
 
 
 def measured_peak():
