@@ -77,6 +77,9 @@ SIGNATURES = {
     "hdfe_row_effects": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _i32, _i64, _vp,
                                     _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_kss_sigma2": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _f64, _i64, _vp, _vp]),
+    "hdfe_solver_create": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _f64, _i64, _i32, _vp]),
+    "hdfe_solver_solve": (_c.c_int, [_vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "hdfe_solver_destroy": (_c.c_int, [_vp]),
     "hdfe_row_scores": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _vp, _i32, _i64, _vp, _vp,
                                    _vp, _vp, _vp, _vp]),
     "hdfe_variance_sums_workspace_bytes": (_i64, [_i32]),

@@ -563,6 +563,34 @@ int hdfe_pcg_solve_noalloc(const int64_t *indptr, const int32_t *indices, const 
                            int32_t k, const uint8_t *zero, const double *X0, double tol,
                            int64_t maxiter, double *X, hdfe_pcg_info *info, void *stream);
 
+/* ------------------------------------------- the solver handle
+ *
+ * core/gpu.py:186-197 `explicit_solver(S, dinv, tol, maxiter)` returns a
+ * `solve(b, zero, x0) -> (X, iterations, converged, max_rel)` closure that
+ * keeps S and the preconditioner on the device; these three calls are that
+ * closure for hosts binding the C ABI (cgo, JNI, N-API).  The handle keeps the
+ * caller's device pointers to S (CSR, as for hdfe_pcg_solve) and dinv, which
+ * must stay alive until hdfe_solver_destroy, and owns the one piece of device
+ * memory this library allocates: the PCG workspace for up to max_k columns
+ * (<= HDFE_PCG_MAX_K), the info record and the zero flags, allocated on the
+ * current device by hdfe_solver_create.  hdfe_solver_solve: B (L, k), X0 (L,
+ * k) or NULL and X (L, k) out are DEVICE pointers; zero (k) uint8 is a HOST
+ * array or NULL; info is HOST memory, filled before the call returns (the
+ * call synchronises its stream, as the reference's solve returns host
+ * values).  It returns info->status (HDFE_OK unless the kernel stopped early;
+ * non-convergence is info->converged = 0, not an error).  One solve at a time
+ * per handle, on the device the handle was created on. */
+typedef struct hdfe_solver hdfe_solver;
+
+int hdfe_solver_create(const int64_t *indptr, const int32_t *indices, const double *data,
+                       int64_t L, int64_t nnz, const double *dinv, double tol, int64_t maxiter,
+                       int32_t max_k, hdfe_solver **out);
+
+int hdfe_solver_solve(hdfe_solver *solver, const double *B, int32_t k, const uint8_t *zero,
+                      const double *X0, double *X, hdfe_pcg_info *info, void *stream);
+
+int hdfe_solver_destroy(hdfe_solver *solver);
+
 #ifdef __cplusplus
 }
 #endif

@@ -245,3 +245,44 @@ def test_stream_cg_matches_explicit(device, name):
     assert np.max(np.abs(g - w)) <= 1e-9 * np.max(np.abs(w))
     its = np.atleast_1d(got.info["iterations"]) - np.atleast_1d(want.info["iterations"])
     assert np.all(np.abs(its) <= 1)
+
+
+def test_solver_handle_matches_block_solver(device):
+    """The opaque solver handle of the C ABI (`hdfe_solver_create` /
+    `_solve` / `_destroy`, the `explicit_solver` closure for FFI hosts): the
+    same X bit for bit as BlockSolver on the same S, host info filled, host
+    zero flags honoured, k above max_k refused."""
+    import ctypes
+    import torch
+    from hdfe_stream_b200 import _lib, fit
+    rows = golden_rows(load_golden(GOLDEN_PANELS[0]))
+    drows = fit.DeviceRows.from_rows(rows)
+    cells = fit.pass1(drows)
+    S = fit.build_s(cells)
+    dinv = fit.jacobi(cells.diag).contiguous()
+    lib = _lib.lib()
+    handle = ctypes.c_void_p()
+    _lib.check(lib.hdfe_solver_create(S.indptr.data_ptr(), S.indices.data_ptr(),
+                                      S.data.data_ptr(), S.L, S.nnz, dinv.data_ptr(), 1e-12,
+                                      5000, 4, ctypes.byref(handle)))
+    try:
+        B = cells.rhs.contiguous()
+        k = int(B.shape[1])
+        X = torch.empty_like(B)
+        info = _lib.PcgInfo()
+        zero = (ctypes.c_uint8 * k)(*([0] * (k - 1) + [1]))
+        _lib.check(lib.hdfe_solver_solve(handle, B.data_ptr(), k, zero, None, X.data_ptr(),
+                                         ctypes.byref(info), _lib.stream_handle()))
+        from hdfe_stream_b200.gpu import BlockSolver
+        want, its, conv, rel = BlockSolver(S, dinv, 1e-12, 5000).solve_device(
+            B, np.array([False] * (k - 1) + [True]))
+        assert torch.equal(X, want)
+        assert (info.iterations, bool(info.converged)) == (its, conv)
+        assert abs(info.max_rel - rel) <= 1e-15
+        assert float(X[:, -1].abs().max()) == 0.0
+        X5 = torch.empty((S.L, 5), dtype=torch.float64, device=device)
+        B5 = torch.zeros_like(X5)
+        assert lib.hdfe_solver_solve(handle, B5.data_ptr(), 5, None, None, X5.data_ptr(),
+                                     ctypes.byref(info), _lib.stream_handle()) != _lib.HDFE_OK
+    finally:
+        assert lib.hdfe_solver_destroy(handle) == _lib.HDFE_OK
