@@ -94,7 +94,7 @@ def row_scores(rows: DeviceRows, cells: DeviceCells, gamma, beta, with_h=False):
 
 
 def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_components,
-                 group_meat=None, extra=None, crv3=(), h=None, B=None):
+                 group_meat=None, extra=None, crv3=(), h=None, B=None, boot=None):
     """CRV1 variances for cluster requests (core/inference.py:176-240
     `_resolve_clusters`, :242-269 `_nested_dims`, :886-906): a request "a",
     "a^b" (one cluster per distinct combination) or "a+b" (two-way,
@@ -115,7 +115,10 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
     of w h h' and s_g its sum of w e h, so CRV3 = adj sum_g d_g d_g' (the
     CRV1 factor), from h (N, k) and the bread B; every fixed-effect dimension
     must be nested in the clusters (else ValueError).  Its entries come back
-    under "CRV3:<request>"."""
+    under "CRV3:<request>".  `boot`, a one-way request with the same nesting
+    and not a refinement of the streamed groups (core/inference.py:312-330),
+    keeps its clusters' sums for the wild bootstrap under "BOOT:<request>":
+    ({"AG", "sG", "adj", "cluster"}, info)."""
     torch = _torch()
     from itertools import combinations
     dev = rows.gcode.device
@@ -183,12 +186,12 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
         return total - (comps + len(fe_params) - 2)
 
     crv3_terms = set()
-    for req in crv3:
+    for req in list(crv3) + ([boot] if boot else []):
         if "+" in req:
             raise ValueError(f"CRV3 takes a one-way cluster request, not {req!r}")
         crv3_terms.add("^".join(dict.fromkeys(c.strip() for c in req.split("^"))))
     out = {}
-    for req in list(dict.fromkeys(list(requests) + list(crv3))):
+    for req in list(dict.fromkeys(list(requests) + list(crv3) + ([boot] if boot else []))):
         parts = [[c.strip() for c in p.split("^")] for p in req.split("+")]
         terms = []
         for r in range(1, len(parts) + 1):
@@ -202,6 +205,19 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
         adj = Gm / (Gm - 1) * (N - 1) / (N - Kc)
         V = sum(sign * adj * (Binv @ t[1] @ Binv) for t, sign, _ in terms)
         out[req] = (V, {"G": Gs, "adj": adj, "nested": nest, "df": Gm - 1})
+        if req == boot:
+            (t, _, _), = terms
+            loose = [d for d in fe_dims if d not in t[2]]
+            if loose or g0 in [c for part in parts for c in part] and len(parts[0]) > 1:
+                raise ValueError(
+                    f"the wild cluster bootstrap by {req!r} needs every fixed effect nested "
+                    "within clusters that are not a refinement of the streamed groups")
+            if h is None:
+                raise ValueError("the bootstrap sums need the residualised covariates h")
+            G, _, _, code, S = t
+            out["BOOT:" + req] = ({"AG": cluster_sums(code, G, rows.w, h), "sG": S, "adj": adj,
+                                   "cluster": req}, {"G": Gs, "adj": adj, "nested": nest,
+                                                     "df": Gm - 1})
         if req in crv3:
             (t, _, _), = terms
             loose = [d for d in fe_dims if d not in t[2]]
@@ -220,6 +236,18 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
     return out
 
 
+def cluster_sums(code, G, w, h):
+    """A_g = sum over the cluster's rows of w h h' (G, k, k), by a device
+    index-add (core/kernels_base.py:658-670 `_nb_crv3_scatter`)."""
+    torch = _torch()
+    N, k = h.shape
+    dev = h.device
+    w = w if w is not None else torch.ones(N, dtype=torch.float64, device=dev)
+    outer = (w[:, None, None] * h[:, :, None] * h[:, None, :]).reshape(N, k * k)
+    return torch.zeros((G, k * k), dtype=torch.float64, device=dev).index_add_(
+        0, code, outer).reshape(G, k, k)
+
+
 def crv3_jack(code, G, w, h, S, B):
     """sum over clusters of d_g d_g', d_g = (B - A_g)^+ s_g (core/kernels_base.py:
     658-680 `_nb_crv3_scatter` / `_nb_crv3_finish`): code (N,) cluster ids, w
@@ -227,19 +255,14 @@ def crv3_jack(code, G, w, h, S, B):
     sums of w e h, B the bread; A_g by a device index-add of w h h', the
     pseudo-inverses batched on the device."""
     torch = _torch()
-    N, k = h.shape
-    dev = h.device
-    w = w if w is not None else torch.ones(N, dtype=torch.float64, device=dev)
-    outer = (w[:, None, None] * h[:, :, None] * h[:, None, :]).reshape(N, k * k)
-    AG = torch.zeros((G, k * k), dtype=torch.float64, device=dev).index_add_(
-        0, code, outer).reshape(G, k, k)
-    Bd = torch.as_tensor(np.asarray(B, np.float64), device=dev)
+    AG = cluster_sums(code, G, w, h)
+    Bd = torch.as_tensor(np.asarray(B, np.float64), device=h.device)
     d = (torch.linalg.pinv(Bd[None] - AG) @ S[:, :, None])[:, :, 0]
     return (d.T @ d).cpu().numpy()
 
 
 def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=None,
-             extra=None, crv3=()):
+             extra=None, crv3=(), bootcluster=None):
     """beta (k,) and its variances for y = V[0] on X = V[1:] with the fit's
     normalised effects gamma (L, m): {"beta", "vcov": {"iid", "hetero",
     "CRV1", "CRV1:<request>" ...}, "se": {...}, "k_fe", "df_resid",
@@ -247,7 +270,9 @@ def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=
     clusters on the streamed dimension; `clusters` adds the requests of
     `cluster_vcov` (names from `fe_names`, default "fe0" for the streamed
     dimension and "fe1", "fe2", ... for the others, or from `extra`); `crv3`
-    one-way requests that also get the cluster jackknife ("CRV3:<request>")."""
+    one-way requests that also get the cluster jackknife ("CRV3:<request>");
+    `bootcluster` a one-way request whose clusters' sums are kept as
+    "boot" for `wildboot.wildboottest`."""
     torch = _torch()
     lib = _lib.lib()
     m = rows.m
@@ -296,7 +321,8 @@ def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=
     vcov = {"iid": rss / (N - K) * Binv, "hetero": N / (N - K) * Binv @ meat_hc @ Binv,
             "CRV1": adj * Binv @ meat_g @ Binv}
     cluster_info = {}
-    if clusters or crv3:
+    boot = None
+    if clusters or crv3 or bootcluster:
         names = list(fe_names) if fe_names else [f"fe{d}" for d in range(len(nlev) + 1)]
         D = len(nlev)
         pair = {}
@@ -307,17 +333,21 @@ def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=
             for d2 in range(d1 + 1, D):
                 pair[(names[d1 + 1], names[d2 + 1])] = pcs[j]
                 j += 1
-        if crv3:
+        if crv3 or bootcluster:
             scores, h = row_scores(rows, cells, gamma, beta, with_h=True)
         else:
             scores, h = row_scores(rows, cells, gamma, beta), None
         for req, (V, info) in cluster_vcov(rows, scores, Binv, k, clusters, names, pair,
                                            group_meat=meat_g, extra=extra, crv3=crv3, h=h,
-                                           B=B).items():
+                                           B=B, boot=bootcluster).items():
+            if req.startswith("BOOT:"):
+                boot = V
+                continue
             key = req if req.startswith("CRV3:") else f"CRV1:{req}"
             vcov[key] = V
             cluster_info[req] = info
     return {"beta": beta, "vcov": vcov,
             "se": {key: np.sqrt(np.diag(v)) for key, v in vcov.items()},
             "k_fe": k_fe, "df_resid": N - K, "df_cluster": G - 1, "rss": rss,
-            "pair_components": pcs, "n_obs": int(N), "n_groups": G, "clusters": cluster_info}
+            "pair_components": pcs, "n_obs": int(N), "n_groups": G, "clusters": cluster_info,
+            "boot": boot}

@@ -1757,3 +1757,44 @@ def weak_id_diagnostics(des, sigma2, leverage, n_draws=64, block=32, seed=0, max
         out["converged"].append(bool(lengths[k] < n_iter or lengths[k] >= caps[k]
                                      or np.all(bnd[:2] <= tol * max(lead, 1e-300))))
     return out
+
+
+# ------------------------------------------------ the wild cluster bootstrap
+
+def wild_bootstrap(AG, sG, beta, j, adj, reps, weights_type, impose_null, seed):
+    """core/wildboot.py:65-102 (`_draws`, `_Test`) and core/results.py:
+    296-307, 863-867: (t, t*, p-value) of the restricted (or unrestricted)
+    wild cluster bootstrap of beta_j = 0 from the clusters' sums."""
+    from itertools import product
+    G = AG.shape[0]
+    A = np.linalg.inv(AG.sum(axis=0))
+    Aj = A[:, j]
+    S = sG + np.einsum("gab,b->ga", AG, Aj * (beta[j] / A[j, j])) if impose_null else sG
+    a, C = S @ Aj, np.einsum("gab,b->ga", AG, Aj) @ A
+    t = beta[j] / np.sqrt(adj * np.sum((sG @ Aj) ** 2))
+    if weights_type == "rademacher" and 2 ** G < reps:
+        blocks = [np.array(list(product([-1, 1], repeat=G)), dtype=float).T]
+    else:
+        rng = np.random.default_rng(seed)
+        r5 = np.sqrt(5)
+        gen = {"rademacher": lambda n: rng.choice([-1, 1], size=n, replace=True),
+               "mammen": lambda n: rng.choice(np.array([-1, 1]) * (r5 + np.array([-1, 1])) / 2,
+                                              size=n, replace=True,
+                                              p=(r5 + np.array([1, -1])) / (2 * r5)),
+               "webb": lambda n: rng.choice(np.concatenate([-np.sqrt(np.array([3, 2, 1]) / 2),
+                                                            np.sqrt(np.array([1, 2, 3]) / 2)]),
+                                            replace=True, size=n),
+               "norm": lambda n: rng.normal(size=n)}[weights_type]
+        per = reps if G * reps <= (1 << 25) else max(1, (1 << 25) // G)
+        blocks, left = [], reps
+        while left:
+            b = min(per, left)
+            blocks.append(np.asarray(gen(G * b), dtype=float).reshape(G, b))
+            left -= b
+    tstar = []
+    for V in blocks:
+        Vt = V.T
+        U = Vt * a - (Vt @ S) @ C.T
+        tstar.append((Vt @ a) / np.sqrt(adj * np.einsum("bg,bg->b", U, U)))
+    tstar = np.concatenate(tstar)
+    return t, tstar, float(np.mean(np.abs(tstar) >= np.abs(t) * (1 - 1e-9)))

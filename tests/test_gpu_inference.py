@@ -198,3 +198,39 @@ def test_crv3_on_nested_regions_matches_oracle(device):
     assert rel(out["vcov"]["CRV3:region"], V3) < 1e-8
     with pytest.raises(ValueError):
         inference.estimate(drows, res.cells, res.gamma, fe_names=names, crv3=("firm",))
+
+
+def test_wild_bootstrap_on_nested_regions_matches_oracle(device):
+    """The wild cluster bootstrap by region on a device fit of 30 separate
+    regions (worker and firm effects nested in them): the clusters' sums from
+    the device against the oracle's, and the t statistic, every t* and the
+    p-value against the oracle's bootstrap on the same draws; a bootstrap
+    clustering that does not nest the effects is refused."""
+    from hdfe_stream_b200 import fit, inference, wildboot
+    rows, region = regions_panel()
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-12)
+    names = ("worker", "firm")
+    est = inference.estimate(drows, res.cells, res.gamma, clusters=("region",),
+                             fe_names=names, extra={"region": region}, bootcluster="region")
+    boot = est["boot"]
+    assert abs(boot["adj"] - est["clusters"]["region"]["adj"]) < 1e-15
+    gamma = res.gamma.cpu().numpy()
+    starts = orc.row_starts(rows.gcode)
+    codes = np.asarray(rows.codes, np.int64)
+    offs = np.concatenate(([0], np.cumsum(rows.n_levels)[:-1]))
+    he, H = orc.row_scores(starts, codes, offs, rows.w, rows.V, gamma, est["beta"], with_h=True)
+    AG = np.zeros((30, 2, 2))
+    np.add.at(AG, region, rows.w[:, None, None] * H[:, :, None] * H[:, None, :])
+    sG = np.zeros((30, 2))
+    np.add.at(sG, region, he)
+    assert rel(boot["AG"].cpu().numpy(), AG) < 1e-10
+    assert rel(boot["sG"].cpu().numpy(), sG) < 1e-10
+    for kind, null in (("rademacher", True), ("webb", False)):
+        got = wildboot.wildboottest(est, 0, reps=999, weights_type=kind, impose_null=null,
+                                    seed=5)
+        t, tstar, p = orc.wild_bootstrap(AG, sG, est["beta"], 0, boot["adj"], 999, kind, null, 5)
+        assert abs(got["t value"] - t) <= 1e-8 * abs(t)
+        assert got["Pr(>|t|)"] == p and got["reps"] == 999
+    with pytest.raises(ValueError):
+        inference.estimate(drows, res.cells, res.gamma, fe_names=names, bootcluster="firm")

@@ -500,3 +500,28 @@ def test_crv3_jackknife_matches_reference(name):
     B = ga[f"{name}_B"]
     for key, code in (("worker", rows.gcode), ("firm", codes[:, 0])):
         assert rel(orc.crv3_jack(code, w, H, he, B), ga[f"{name}_crv3_{key}_jack"]) < 1e-9, key
+
+
+CASES_WB = [("rademacher", True, 999, 11), ("rademacher", False, 999, 12),
+            ("mammen", True, 499, 13), ("webb", True, 499, 14), ("norm", False, 499, 15),
+            ("rademacher", True, 999, 16)]
+
+
+@pytest.mark.parametrize("c", range(6))
+def test_wild_bootstrap_matches_reference(c):
+    """The wild cluster bootstrap (the oracle and the library's host draws
+    with its arithmetic in torch on the CPU) against the reference's
+    core/wildboot.py `_draws` / `_Test` for every weight distribution,
+    restricted and not, and the Rademacher enumeration (tests/golden/
+    wildboot.npz): t and every t* to 1e-10."""
+    import torch
+    from hdfe_stream_b200.wildboot import bootstrap_t
+    g = load_golden("wildboot")
+    kind, null, reps, seed = CASES_WB[c]
+    args = (g[f"c{c}_AG"], g[f"c{c}_sG"], g[f"c{c}_beta"], 1, float(g[f"c{c}_adj"][0]))
+    t, tstar, _ = orc.wild_bootstrap(*args, reps, kind, null, seed)
+    assert abs(t - g[f"c{c}_t"][0]) <= 1e-10 * abs(g[f"c{c}_t"][0])
+    assert rel(tstar, g[f"c{c}_tstar"]) < 1e-10
+    t2, tstar2, _ = bootstrap_t(*args, reps, kind, null, seed, device=torch.device("cpu"))
+    assert abs(t2 - g[f"c{c}_t"][0]) <= 1e-10 * abs(g[f"c{c}_t"][0])
+    assert rel(tstar2, g[f"c{c}_tstar"]) < 1e-10
