@@ -1102,8 +1102,17 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
         launched++;
     }
     HDFE_CUDA_TRY(cudaMemsetAsync(a.rnnz, 0, (a.L + 1) * 8, c.s));
-    k_small_rows<<<(unsigned)(c.sms * 6), kSmallWarpsPerCta * 32, 0, c.s>>>(a);
-    k_warp_rows<<<(unsigned)(c.sms * 8), kWarpsPerCta * 32, 0, c.s>>>(a);
+    // one wave: as many CTAs as stay resident (the rows are grid-strided, so a
+    // second partial wave would run its share of rows after the first)
+    int per_small = 0, per_warp = 0;
+    HDFE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_small, k_small_rows,
+                                                              kSmallWarpsPerCta * 32, 0));
+    HDFE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_warp, k_warp_rows,
+                                                              kWarpsPerCta * 32, 0));
+    k_small_rows<<<(unsigned)(c.sms * (per_small > 0 ? per_small : 1)), kSmallWarpsPerCta * 32, 0,
+                   c.s>>>(a);
+    k_warp_rows<<<(unsigned)(c.sms * (per_warp > 0 ? per_warp : 1)), kWarpsPerCta * 32, 0,
+                  c.s>>>(a);
     HDFE_CUDA_TRY(cudaFuncSetAttribute(k_block_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kBlockSmem));
     k_block_rows<<<(unsigned)(c.sms), 32, kBlockSmem, c.s>>>(a);
