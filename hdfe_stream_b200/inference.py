@@ -25,6 +25,13 @@ from .connected import pair_components
 from .fit import DeviceCells, DeviceRows, components
 
 
+def ratio(num, den):
+    """num / den, or nan when den is zero (core/inference.py:83-87 `_ratio`):
+    a saturated model or a request with a single cluster has no degrees of
+    freedom left, so its variances are undefined rather than an error."""
+    return num / den if den else np.nan
+
+
 def _torch():
     import torch
     return torch
@@ -148,11 +155,16 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
         elif len(cols) == 1 and cols[0] in fe_params:
             kind, code, G = "fe", col[cols[0]], card[cols[0]]
         else:
-            key = torch.zeros(N, dtype=torch.int64, device=dev)
+            # compose the clusters column by column, re-coding densely after
+            # each step, so the packed key never exceeds (distinct so far) x
+            # card[c] < 2^63 whatever the columns' cardinalities
+            code, G = None, 1
             for c in cols:
-                key = key * card[c] + col[c]
-            _, code = torch.unique(key, sorted=True, return_inverse=True)
-            G = int(code.max().item()) + 1 if N else 0
+                if G * max(card[c], 1) >= 2 ** 63:
+                    raise ValueError(f"cluster request {'^'.join(cols)!r}: too many clusters")
+                key = col[c] if code is None else code * card[c] + col[c]
+                _, code = torch.unique(key, sorted=True, return_inverse=True)
+                G = int(code.max().item()) + 1 if N else 0
             kind = "segsub" if g0 in cs else ("fe" if len(cols) == 1 else "extra")
         S = None
         if kind == "seg" and group_meat is not None and key_name not in crv3_terms:
@@ -202,7 +214,7 @@ def cluster_vcov(rows: DeviceRows, scores, Binv, k, requests, fe_names, pair_com
         Gm = min(Gs)
         nest = list(dict.fromkeys(d for t, _, _ in terms for d in t[2]))
         Kc = k + k_fe(nest) - sum(fe_params[d] for d in nest) + len(nest)
-        adj = Gm / (Gm - 1) * (N - 1) / (N - Kc)
+        adj = ratio(Gm, Gm - 1) * ratio(N - 1, N - Kc)
         V = sum(sign * adj * (Binv @ t[1] @ Binv) for t, sign, _ in terms)
         out[req] = (V, {"G": Gs, "adj": adj, "nested": nest, "df": Gm - 1})
         if req == boot:
@@ -317,8 +329,8 @@ def estimate(rows: DeviceRows, cells: DeviceCells, gamma, clusters=(), fe_names=
     K = k + k_fe
     Binv = np.linalg.inv(B)
     Kc = k + k_fe - G + 1
-    adj = G / (G - 1) * (N - 1) / (N - Kc)
-    vcov = {"iid": rss / (N - K) * Binv, "hetero": N / (N - K) * Binv @ meat_hc @ Binv,
+    adj = ratio(G, G - 1) * ratio(N - 1, N - Kc)
+    vcov = {"iid": ratio(rss, N - K) * Binv, "hetero": ratio(N, N - K) * Binv @ meat_hc @ Binv,
             "CRV1": adj * Binv @ meat_g @ Binv}
     cluster_info = {}
     boot = None

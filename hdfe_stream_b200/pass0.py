@@ -15,6 +15,8 @@ The sorts and uniques are torch's (CUB radix sorts).
 
 from __future__ import annotations
 
+import numpy as np
+
 from .fit import DeviceRows
 
 
@@ -42,12 +44,26 @@ def pass0(streamed, fixed_effects, V, w=None, sort_only=()):
     extra = [factorize(c) for c in sort_only]
     cols = [g] + [c for c, _ in fe] + [c for c, _ in extra]
     sizes = [len(glev)] + [len(l) for _, l in fe] + [len(l) for _, l in extra]
-    key = torch.zeros_like(g)
-    for c, n in zip(cols, sizes):
-        key = key * n + c
-    order = torch.argsort(key, stable=True)
-    sk = key[order]
-    if sk.numel() > 1 and bool((sk[1:] == sk[:-1]).any()):
+    if np.prod([float(max(n, 1)) for n in sizes]) < 2.0 ** 62:
+        key = torch.zeros_like(g)
+        for c, n in zip(cols, sizes):
+            key = key * n + c
+        order = torch.argsort(key, stable=True)
+        sk = key[order]
+        tie = sk.numel() > 1 and bool((sk[1:] == sk[:-1]).any())
+    else:
+        # the packed key would overflow int64: sort column by column instead
+        # (least significant first, each sort stable) and find ties by
+        # comparing every column of neighbouring rows
+        order = torch.arange(g.numel(), device=g.device)
+        for c in cols[::-1]:
+            order = order[torch.argsort(c[order], stable=True)]
+        same = torch.ones(max(g.numel() - 1, 0), dtype=torch.bool, device=g.device)
+        for c in cols:
+            sc = c[order]
+            same &= sc[1:] == sc[:-1]
+        tie = bool(same.any())
+    if tie:
         # rows sharing every code: the variables break the tie (least
         # significant key sorted first, each sort stable)
         order = torch.arange(key.numel(), device=key.device)

@@ -234,3 +234,28 @@ def test_wild_bootstrap_on_nested_regions_matches_oracle(device):
         assert got["Pr(>|t|)"] == p and got["reps"] == 999
     with pytest.raises(ValueError):
         inference.estimate(drows, res.cells, res.gamma, fe_names=names, bootcluster="firm")
+
+
+def test_saturated_model_and_single_cluster_give_nan(device):
+    """core/inference.py:83-87 `_ratio`: a model with no residual degrees of
+    freedom (N = K) has undefined iid and HC1 variances, and a cluster
+    request with a single cluster an undefined CRV1 -- NaN, not an error."""
+    from hdfe_stream_b200 import fit, inference
+    from hdfe_stream_b200.simulate import Rows
+    rng = np.random.default_rng(3)
+    # two workers, two firms: w0 at f0, f0, f1; w1 at f0, f1.  N = 5 rows,
+    # K = 2 covariates + (2 workers + 2 firms - 1) effects = 5
+    gcode = np.array([0, 0, 0, 1, 1], np.uint32)
+    firm = np.array([[0], [0], [1], [0], [1]], np.uint32)
+    V = rng.standard_normal((5, 3))
+    rows = Rows(gcode=gcode, codes=firm, V=V, w=None, n_levels=[2], n_groups=2,
+                names=["y", "x1", "x2"])
+    drows = fit.DeviceRows.from_rows(rows)
+    res = fit.fit(drows, tol=1e-13)
+    out = inference.estimate(drows, res.cells, res.gamma, clusters=("one",),
+                             extra={"one": np.zeros(5, np.int64)})
+    assert out["df_resid"] == 0
+    assert np.isnan(out["vcov"]["iid"]).all()
+    assert np.isnan(out["vcov"]["hetero"]).all()
+    assert np.isfinite(out["vcov"]["CRV1"]).all()
+    assert np.isnan(out["vcov"]["CRV1:one"]).all()
