@@ -34,39 +34,56 @@ def _torch():
     return torch
 
 
+GHOST_TOL = 1e-8        # leaveout_weakid.py:403: copies of one converged eigenvalue
+SPURIOUS_TOL = 1e-11    # leaveout_weakid.py:422: the Cullum-Willoughby match
+
+
 def ritz_top(alpha, beta, top):
-    """The leading genuine Ritz values of the tridiagonal (alpha, beta[:-1]),
-    their error bounds |beta[-1] s_m| and vectors (leaveout_weakid.py:
-    386-434): copies within 1e-8 of the largest are one eigenvalue (the copy
-    with the smaller bound kept), and a lone value that is also an eigenvalue
-    of the tridiagonal without its first row and column (to 1e-11) is a ghost."""
+    """The `top` leading genuine Ritz values of the Lanczos tridiagonal
+    T = tridiag(beta[:-1], alpha, beta[:-1]), with their error bounds
+    |beta[-1] s_m| (s_m the eigenvector's last entry) and eigenvectors, as
+    the reference's `_ritz_top` (leaveout_weakid.py:386-434) selects them:
+
+    * ghosts -- in floating point a converged eigenvalue reappears as
+      further Ritz values that agree with it to the convergence level, far
+      closer than two genuine eigenvalues: sorted Ritz values chained by gaps
+      of at most 1e-8 max|theta| are one eigenvalue, represented by the
+      member with the smallest error bound;
+    * spurious values (Cullum and Willoughby, 1985) -- a value seen once
+      that is also an eigenvalue of T without its first row and column (to
+      1e-11 max|theta|) is not an eigenvalue of the operator.
+
+    The survivors are ranked by |theta|."""
     from scipy.linalg import eigh_tridiagonal, eigvalsh_tridiagonal
-    m = len(alpha)
+    diag = np.asarray(alpha, float)
+    m = len(diag)
     if m == 0:
         return np.array([]), np.array([]), np.zeros((0, 0))
-    alpha = np.asarray(alpha, float)
-    off = np.asarray(beta[:m - 1], float)
-    theta, S = eigh_tridiagonal(alpha, off)
-    bounds = np.abs(beta[m - 1] * S[-1, :])
-    scale = max(float(np.abs(theta).max()), 1e-300)
-    order = np.argsort(theta)
-    kept = []
-    for i in order:
-        if kept and abs(theta[i] - theta[kept[-1]]) <= 1e-8 * scale:
-            if bounds[i] < bounds[kept[-1]]:
-                kept[-1] = i
-            continue
-        kept.append(i)
-    copies = {}
-    for i in order:
-        head = min(kept, key=lambda h: abs(theta[h] - theta[i]))
-        copies[head] = copies.get(head, 0) + 1
+    sub = np.asarray(beta, float)[:m - 1]
+    theta, vecs = eigh_tridiagonal(diag, sub)          # ascending
+    err = np.abs(float(beta[m - 1]) * vecs[m - 1])
+    scale = max(float(np.max(np.abs(theta))), 1e-300)
+    # runs of the sorted values: a new run starts where the gap to the run's
+    # current representative exceeds the ghost tolerance
+    run_of = np.empty(m, np.int64)
+    reps, sizes = [], []
+    for i in np.argsort(theta):
+        if reps and theta[i] - theta[reps[-1]] <= GHOST_TOL * scale:
+            sizes[-1] += 1
+            if err[i] < err[reps[-1]]:
+                reps[-1] = i
+        else:
+            reps.append(i)
+            sizes.append(1)
+        run_of[i] = len(reps) - 1
+    reps, sizes = np.array(reps, np.int64), np.array(sizes, np.int64)
     if m > 1:
-        hat = eigvalsh_tridiagonal(alpha[1:], off[1:]) if m > 2 else alpha[1:]
-        kept = [h for h in kept
-                if copies[h] > 1 or np.min(np.abs(hat - theta[h])) > 1e-11 * scale]
-    kept = sorted(kept, key=lambda h: -abs(theta[h]))[:top]
-    return theta[kept], bounds[kept], S[:, kept]
+        deleted = eigvalsh_tridiagonal(diag[1:], sub[1:]) if m > 2 else diag[1:]
+        near = np.min(np.abs(deleted[None, :] - theta[reps][:, None]), axis=1)
+        genuine = (sizes > 1) | (near > SPURIOUS_TOL * scale)
+        reps = reps[genuine]
+    ranked = reps[np.argsort(-np.abs(theta[reps]), kind="stable")][:top]
+    return theta[ranked], err[ranked], vecs[:, ranked]
 
 
 class _Lanczos:

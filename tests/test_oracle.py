@@ -417,6 +417,53 @@ def test_am_interval_matches_reference():
         assert rel([lo, hi, info["kappa"], info["z"], info["rho"]], want) < 1e-12
 
 
+def test_am_critical_value_at_small_curvature():
+    """Where kappa is tiny the drop of the integrand over b is ~1/(2 kappa^-1)
+    wide; the critical value must still exceed the chi-squared(1) bound
+    (P(rho <= z1) < 1 - alpha for every kappa > 0).  Checked against the
+    distribution function integrated over b on a split interval."""
+    import math
+    from scipy import integrate, special
+    from hdfe_stream_b200.am_interval import am_cdf, am_critical_value
+    for kappa in (1e-6, 1.5e-4, 1e-2, 1.0, 50.0):
+        c = 1.0 / kappa
+        z1 = math.sqrt(special.chdtri(1, 0.05))
+        z = am_critical_value(kappa, 0.05)
+        assert z > z1
+
+        def f(b, zz=z):
+            r = math.sqrt(max((zz - b) * (zz + b + 2.0 * c), 0.0))
+            return 2.0 * math.exp(-0.5 * b * b) / math.sqrt(2.0 * math.pi) * (
+                2.0 * special.ndtr(r) - 1.0)
+        cuts = sorted({0.0, max(z - 50.0 / c, 0.0), max(z - 5.0 / c, 0.0), z})
+        F = sum(integrate.quad(f, a, b, epsabs=1e-15, epsrel=1e-13, limit=500)[0]
+                for a, b in zip(cuts[:-1], cuts[1:]))
+        assert abs(F - 0.95) < 1e-11, (kappa, F)
+        assert abs(am_cdf(z, kappa) - 0.95) < 1e-13
+
+
+def test_ritz_selection_matches_oracle():
+    """weakid.ritz_top (ghost runs, the Cullum-Willoughby test, ranking)
+    against the oracle's restatement of the reference's `_ritz_top` on
+    random tridiagonals and on ones with exact and near copies of an
+    eigenvalue (two identical blocks joined by a zero or tiny coupling)."""
+    from hdfe_stream_b200.weakid import ritz_top
+    rng = np.random.default_rng(8)
+    cases = []
+    for m in (1, 2, 3, 7, 20):
+        cases.append((rng.normal(size=m), np.abs(rng.normal(size=m))))
+    for couple in (0.0, 1e-14, 1e-3):
+        a = rng.normal(size=6)
+        b = np.abs(rng.normal(size=6))
+        cases.append((np.concatenate([a, a]), np.concatenate([b[:5], [couple], b[:5], [b[5]]])))
+    for alpha, beta in cases:
+        for top in (1, 3):
+            got = ritz_top(alpha, beta, top)
+            ref = orc.ritz_top(alpha, beta, top)
+            for x, y in zip(got, ref):
+                assert np.array_equal(np.asarray(x), np.asarray(y))
+
+
 @pytest.mark.parametrize("name", ["akm_small", "akm_weighted", "akm_components"])
 def test_cluster_variances_match_reference(name):
     """Pass 2's per-row scores and the CRV1 variances for cluster requests
