@@ -282,12 +282,16 @@ class FitResult:
 
 def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
           x0=None, normalize_fe=True, timer=None, precision="fp64", comps=None,
-          solver="explicit") -> FitResult:
+          solver="explicit", names=None) -> FitResult:
     """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
     right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
     zero, block PCG per `rhs_block` columns, then `_normalize`.  `comps`:
     the first dimension's components from `components_async`, else computed
-    here."""
+    here.  `names`: the variables' names, for info["fe_spanned"].  The info
+    dict has the keys of core/solve.py:370-381 `_solve_info` (iterations,
+    converged, blocks; max_rel_residual unless NaN; fe_spanned, the names
+    of the variables the fixed effects span, only when there are any) and
+    the device's own (solver, device, S_nnz, S_mb, n_components)."""
     torch = _torch()
     timer = timer or _NoTimer()
     m = int(cells.rhs.shape[1])
@@ -325,10 +329,16 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     explicit = S is not None and not hasattr(solver, "matvec")
     info = {"solver": "explicit" if explicit else "stream_cg", "device": "cuda",
             "iterations": its if len(its) > 1 else its[0],
-            "converged": conv, "max_rel_residual": rel,
+            "converged": conv, "blocks": len(its),
             "S_nnz": S.nnz if explicit else None,
             "S_mb": round(S.nbytes / 1e6, 1) if explicit else None,
-            "n_components": int(n_comp[0]), "fe_spanned": [j for j in range(m) if zero_all[j]]}
+            "n_components": int(n_comp[0])}
+    if not np.isnan(rel):
+        info["max_rel_residual"] = rel
+    names = list(names) if names else [f"v{j}" for j in range(m)]
+    spanned = [names[j] for j in range(m) if zero_all[j]]
+    if spanned:
+        info["fe_spanned"] = spanned
     return FitResult(gamma=gamma, info=info, cells=cells, S=S, root=root)
 
 
@@ -383,7 +393,7 @@ def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None,
         S = build_s(cells)
     with timer("solve"):
         return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
-                     comps=comps)
+                     comps=comps, names=rows.names)
 
 
 _COPY_STREAMS = {}

@@ -99,6 +99,7 @@ class BlockSolver:
         self._ws = {}
         self._info = torch.zeros(3, dtype=torch.float64, device=self.dev)   # 24 bytes
         self._zero = torch.zeros(_lib.PCG_MAX_K, dtype=torch.uint8, device=self.dev)
+        self.stats = {"launches": 0, "iterations": 0}     # solves so far (for the roofline)
 
     def _workspace(self, k):
         import torch
@@ -143,6 +144,8 @@ class BlockSolver:
                    _lib.HDFE_ERR_BAD_CODE: "a column index of S is out of range"}
             raise _lib.HDFEError(info.status, "the PCG kernel stopped early: "
                                  + why.get(info.status, "device error"))
+        self.stats["launches"] += 1
+        self.stats["iterations"] += max(int(info.iterations), 0)
         return int(info.iterations), bool(info.converged), float(info.max_rel)
 
     def solve_device(self, B, zero=None, X0=None):

@@ -11,6 +11,8 @@ depend on how the draws are blocked, exactly as in the reference.
 
 from __future__ import annotations
 
+from dataclasses import dataclass, field
+
 import numpy as np
 
 from . import _lib
@@ -18,6 +20,10 @@ from .fit import DeviceCells, DeviceRows, RHS_ZERO_TOL, jacobi
 from .gpu import BlockSolver, DeviceCSR
 
 MAX_BLOCK = 32      # vectors per row pass (one lane each)
+COMPONENTS = ("var(psi)", "var(alpha)", "cov(psi, alpha)")
+TRACE_SEED_OFFSET = 1_000_003       # leaveout.py:733 (the bias term's draws)
+SE_SEED_OFFSET = 5_500_011          # leaveout.py:770
+WEAK_ID_SEED_OFFSET = 9_900_019     # leaveout.py:751
 
 
 def _torch():
@@ -25,14 +31,148 @@ def _torch():
     return torch
 
 
+@dataclass
+class JLALeverages:
+    """Per-row leverage estimates in the rows' order (leaveout.py:65-86
+    `JLALeverages`), as device tensors (N,): the leverage P_ii in [0, 1],
+    its complement M_ii = 1 - P_ii and the non-linearity correction factor
+    for sigma^2; n_draws Rademacher draws; diagnostics: blocks, covariates,
+    the last block's PCG iterations."""
+
+    leverage: object
+    complement: object
+    factor: object
+    n_draws: int
+    diagnostics: dict = field(default_factory=dict)
+
+    @property
+    def n_rows(self) -> int:
+        return int(self.leverage.shape[0])
+
+    def summary(self) -> str:
+        d = self.diagnostics
+        lev, f = self.leverage, self.factor
+        return (f"JLA leverages: {self.n_rows:,} rows, {self.n_draws} draws in "
+                f"{d.get('blocks', '?')} block(s)\n"
+                f"  leverage   min {float(lev.min()):.6f}  max {float(lev.max()):.6f}  "
+                f"mean {float(lev.mean()):.6f}\n"
+                f"  correction min {float(f.min()):.6f}  max {float(f.max()):.6f}  "
+                f"mean {float(f.mean()):.6f}")
+
+
+@dataclass
+class TraceEstimate:
+    """The bias terms of the three AKM variance components (leaveout.py:
+    290-313 `TraceEstimate`)."""
+
+    var_psi: float
+    var_alpha: float
+    cov: float
+    n_draws: int
+    diagnostics: dict = field(default_factory=dict)
+
+    def as_dict(self) -> dict:
+        return {"var(psi)": self.var_psi, "var(alpha)": self.var_alpha,
+                "cov(psi, alpha)": self.cov}
+
+    def as_array(self) -> np.ndarray:
+        return np.array([self.var_psi, self.var_alpha, self.cov])
+
+    def summary(self) -> str:
+        d = self.diagnostics
+        return (f"bias terms from {self.n_draws} Hutchinson draws in "
+                f"{d.get('blocks', '?')} block(s)\n"
+                f"  var(psi)        {self.var_psi:+.6f}\n"
+                f"  var(alpha)      {self.var_alpha:+.6f}\n"
+                f"  cov(psi, alpha) {self.cov:+.6f}")
+
+
+@dataclass
+class LeaveOutComponents:
+    """KSS leave-out variance components with the plug-in ones beside them
+    (leaveout.py:456-630 `LeaveOutComponents`).  plug_in, bias and
+    leave_out are dicts keyed "var(psi)", "var(alpha)", "cov(psi, alpha)";
+    n_obs the observations (person-years); n_movers the movers'
+    observations (movers' matches when leaving out a match); leverages a
+    `JLALeverages`; trace a `TraceEstimate`; se a
+    `leaveout_se.ComponentSE` with se=True; weak_id the weak-identification
+    diagnostic's dict when it ran; diagnostics settings and summary
+    statistics (maximum leverage, mean sigma2, ...); fit the regression the
+    components are from; match_fit the collapsed match-level regression
+    when leaving out a match.  The per-row sigma2 is in diagnostics
+    ["sigma2"] (a device tensor)."""
+
+    plug_in: dict
+    bias: dict
+    leave_out: dict
+    n_obs: int
+    n_movers: int
+    leverages: object
+    trace: object
+    se: object = None
+    weak_id: object = None
+    diagnostics: dict = field(default_factory=dict)
+    pruning: dict | None = None
+    fit: object = None
+    match_fit: object = None
+
+    def tidy(self):
+        """The three components as a table (pandas DataFrame)."""
+        import pandas as pd
+        keys = list(self.plug_in)
+        return pd.DataFrame({"component": keys,
+                             "plug_in": [self.plug_in[k] for k in keys],
+                             "bias": [self.bias[k] for k in keys],
+                             "leave_out": [self.leave_out[k] for k in keys]})
+
+    def summary(self) -> str:
+        d = self.diagnostics
+        lines = [f"leave-out variance components ({d.get('psi')} and {d.get('alpha')})",
+                 f"  {self.n_obs:,} observations, {self.n_movers:,} of them movers'; "
+                 f"{self.leverages.n_draws} draws",
+                 f"  max leverage {d.get('max_leverage', float('nan')):.6f}   "
+                 f"mean sigma2 {d.get('sigma2_mean', float('nan')):.6f}", "",
+                 f"{'component':<20}{'plug-in':>12}{'bias':>12}{'leave-out':>12}"
+                 + (f"{'se':>11}" if self.se is not None else ""),
+                 "-" * (67 if self.se is not None else 56)]
+        for key in self.plug_in:
+            row = (f"{key:<20}{self.plug_in[key]:>12.6f}{self.bias[key]:>12.6f}"
+                   f"{self.leave_out[key]:>12.6f}")
+            if self.se is not None:
+                row += f"{self.se.se[key]:>11.6f}"
+            lines.append(row)
+        return "\n".join(lines)
+
+
+def trace_components(mean, person_years):
+    """The three bias terms from the eight Hutchinson moments averaged over
+    the draws (leaveout.py:380-391): var = E[a1 a2]/w - (E[a1]/w)(E[a2]/w)
+    per component and the covariance's symmetrised form, times the n - 1
+    divisor's correction (leaveout_se.py:202-214 `_moment_divisor`)."""
+    weight, a1a2, b1b2, cross, a1, a2, b1, b2 = (float(x) for x in mean)
+    var_psi = a1a2 / weight - (a1 / weight) * (a2 / weight)
+    var_alpha = b1b2 / weight - (b1 / weight) * (b2 / weight)
+    cov = 0.5 * (cross / weight - (a1 / weight) * (b2 / weight) - (b1 / weight) * (a2 / weight))
+    R = float(person_years)
+    scale = weight / (weight * (R - 1.0) / R) if R > 1 else 1.0
+    return np.array([scale * var_psi, scale * var_alpha, scale * cov])
+
+
 class InverseOperator:
     """A S^- A' for one fit's design: its rows (device), identifying cells
     and reduced matrix S, and optional covariates (N, c) joining the fixed
-    effects in the design (leaveout.py:91-110 `_model_covariates`)."""
+    effects in the design (leaveout.py:91-110 `_model_covariates`).
+    `fe_names`: the fixed effects' names, the streamed dimension (alpha)
+    first, then the non-streamed ones in the codes' column order (default
+    "fe0", "fe1", ...); `psi` arguments name one of the latter."""
 
     def __init__(self, rows: DeviceRows, cells: DeviceCells, S: DeviceCSR, covariates=None,
-                 tol=1e-10, maxiter=5000, precision="fp64"):
+                 tol=1e-10, maxiter=5000, precision="fp64", fe_names=None):
         torch = _torch()
+        names = list(fe_names) if fe_names else [f"fe{d}" for d in range(len(cells.n_levels) + 1)]
+        if len(names) != len(cells.n_levels) + 1:
+            raise ValueError("fe_names: the streamed dimension and one name per column of codes")
+        self.g_fe, self.o_fe = names[0], names[1:]
         self.rows, self.cells, self.S = rows, cells, S
         self.dev = rows.gcode.device
         self.N = rows.n_rows
@@ -46,6 +186,15 @@ class InverseOperator:
         self.starts, self.G = self._row_groups()
         self._border = None
         self._ws = torch.empty(256, dtype=torch.uint8, device=self.dev)
+        self.timer = None       # a fit.PhaseTimer: CUDA events around each kernel launch
+
+    def _phase(self, name):
+        """The timer's phase `name`, or nothing when no timer is set."""
+        import contextlib
+        if self.timer is None:
+            return contextlib.nullcontext()
+        self.solver.timer = self.timer
+        return self.timer(name)
 
     def _row_groups(self):
         torch = _torch()
@@ -70,12 +219,13 @@ class InverseOperator:
         acc = torch.empty((self.L, B), **f64)
         acc_x = torch.empty((max(self.c, 1), B), **f64)
         sq = torch.empty(B, **f64)
-        _lib.check(_lib.lib().hdfe_rows_center(
-            self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
-            self.nlev.ctypes.data, self._ptr(self.w), self._ptr(self.X), self.c, self._ptr(R), B,
-            int(seed) & (2**64 - 1), int(first_draw), 0, int(bool(sqrt_weights)), acc.data_ptr(),
-            acc_x.data_ptr(), sq.data_ptr(), self._ws.data_ptr(), self._ws.numel(),
-            _lib.stream_handle()))
+        with self._phase("k_center"):
+            _lib.check(_lib.lib().hdfe_rows_center(
+                self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
+                self.nlev.ctypes.data, self._ptr(self.w), self._ptr(self.X), self.c,
+                self._ptr(R), B, int(seed) & (2**64 - 1), int(first_draw), 0,
+                int(bool(sqrt_weights)), acc.data_ptr(), acc_x.data_ptr(), sq.data_ptr(),
+                self._ws.data_ptr(), self._ws.numel(), _lib.stream_handle()))
         return acc, acc_x[:self.c], sq
 
     def solve_reduced(self, rhs, scale):
@@ -116,12 +266,13 @@ class InverseOperator:
         else:
             C = None
         res = torch.empty((self.N, B), dtype=torch.float64, device=self.dev) if out else None
-        _lib.check(_lib.lib().hdfe_rows_project(
-            self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
-            self.nlev.ctypes.data, self._ptr(self.w), self._ptr(self.X), self.c,
-            self._ptr(None if C is None else C.contiguous()), U.data_ptr(), None, B,
-            int(seed) & (2**64 - 1), int(first_draw), 0, int(bool(sqrt_weights)), self.N,
-            self._ptr(res), self._ptr(moments), _lib.stream_handle()))
+        with self._phase("k_project"):
+            _lib.check(_lib.lib().hdfe_rows_project(
+                self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
+                self.nlev.ctypes.data, self._ptr(self.w), self._ptr(self.X), self.c,
+                self._ptr(None if C is None else C.contiguous()), U.data_ptr(), None, B,
+                int(seed) & (2**64 - 1), int(first_draw), 0, int(bool(sqrt_weights)), self.N,
+                self._ptr(res), self._ptr(moments), _lib.stream_handle()))
         return res, info
 
     # ---- coefficient-space right-hand sides (inverse.py:311-460)
@@ -195,8 +346,9 @@ class InverseOperator:
         st, sh = self._status(), _lib.stream_handle()
         base = (self.starts.data_ptr(), self.G, self.rows.codes.data_ptr(), len(self.nlev),
                 self.nlev.ctypes.data, self._ptr(self.w), self._ptr(self.X), self.c)
-        _lib.check(lib.hdfe_rows_reduce(*base, streamed.data_ptr(), None, B, acc.data_ptr(),
-                                        acc_x.data_ptr(), None, st.data_ptr(), sh))
+        with self._phase("k_reduce"):
+            _lib.check(lib.hdfe_rows_reduce(*base, streamed.data_ptr(), None, B, acc.data_ptr(),
+                                                acc_x.data_ptr(), None, st.data_ptr(), sh))
         rhs = levels - acc
         U, info = self.solve_reduced(rhs.contiguous(), scale)
         if Z is not None:
@@ -211,29 +363,53 @@ class InverseOperator:
         if omega is not None:
             v = (torch.zeros((self.L, B), **f64), torch.zeros((max(self.c, 1), B), **f64),
                  torch.empty((self.G, B), **f64))
-        _lib.check(lib.hdfe_rows_project_coef(
-            *base, self._ptr(C), U.data_ptr(), streamed.data_ptr(), B, self._ptr(out_rows),
-            U_g.data_ptr(), self._ptr(omega), self._ptr(None if v is None else v[0]),
-            self._ptr(None if v is None else v[1]), self._ptr(None if v is None else v[2]),
-            st.data_ptr(), sh))
+        with self._phase("k_project_coef"):
+            _lib.check(lib.hdfe_rows_project_coef(
+                *base, self._ptr(C), U.data_ptr(), streamed.data_ptr(), B, self._ptr(out_rows),
+                U_g.data_ptr(), self._ptr(omega), self._ptr(None if v is None else v[0]),
+                self._ptr(None if v is None else v[1]), self._ptr(None if v is None else v[2]),
+                st.data_ptr(), sh))
         self.ainv_info = info
         res = (U, C, U_g, out_rows)
         if v is not None:
             res = res + ((v[0], v[1][:self.c], v[2]),)
         return res
 
-    def hutchinson_trace(self, sigma2, n_draws=250, block=MAX_BLOCK, seed=0, psi_column=0,
-                         person_years=None):
-        """leaveout.py:321-391 `hutchinson_trace` and :393-448 `_trace_block`:
-        the bias terms (var(psi), var(alpha), cov(psi, alpha)) from n_draws
-        Rademacher vectors in coefficient space, two applications of the
-        inverse per block; sigma2 (N) per-row variances.  Draws are keyed on
-        (seed, position, draw), so the answer does not depend on blocking."""
+    def _psi_column(self, psi):
+        """The codes' column of `psi` (a name of `o_fe`, a column index, or
+        None for the first)."""
+        if psi is None:
+            return 0
+        if isinstance(psi, (int, np.integer)):
+            if not 0 <= int(psi) < len(self.o_fe):
+                raise ValueError(f"psi column {psi} out of range")
+            return int(psi)
+        if psi not in self.o_fe:
+            raise ValueError(f"psi must be a non-streamed dimension, one of {self.o_fe}; "
+                             f"got {psi!r}")
+        return self.o_fe.index(psi)
+
+    def _check_covariates(self, covariates):
+        """The design is fixed when the operator is built: covariates=None
+        (the operator's own) or the same number of columns passes."""
+        if covariates is None:
+            return
+        if len(tuple(covariates)) != self.c:
+            raise ValueError(f"this operator's design has {self.c} covariate(s); build an "
+                             "InverseOperator with the covariates wanted")
+
+    def trace_totals(self, sigma2, first, last, block=None, seed=0, psi=None):
+        """The eight Hutchinson moment sums (w, a1 a2, b1 b2, cross, a1, a2,
+        b1, b2; leaveout.py:393-448 `_trace_block`) over the draws
+        [first, last), a device tensor (8,), and the blocks run.  Draw j is
+        keyed on (seed, position, j) whoever computes it, so sums over
+        disjoint draw ranges add up to the sum over their union."""
         torch = _torch()
         lib = _lib.lib()
-        block = int(block)
-        if block < 1 or n_draws < 1:
-            raise ValueError("n_draws and block must be at least 1")
+        psi_column = self._psi_column(psi)
+        block = MAX_BLOCK if block is None else int(block)
+        if block < 1:
+            raise ValueError("block must be at least 1")
         block = min(block, MAX_BLOCK)
         f64 = dict(dtype=torch.float64, device=self.dev)
         omega = torch.as_tensor(sigma2).to(**f64).contiguous()
@@ -242,34 +418,57 @@ class InverseOperator:
         ws = torch.empty(int(lib.hdfe_trace_moments_workspace_bytes(block)), dtype=torch.uint8,
                          device=self.dev)
         mom = torch.empty((block, 8), **f64)
-        drawn, blocks = 0, 0
+        drawn, blocks = int(first), 0
         sh = _lib.stream_handle()
-        while drawn < n_draws:
-            size = min(block, n_draws - drawn)
+        while drawn < last:
+            size = min(block, last - drawn)
             Zall = torch.empty((L + G + c, size), **f64)
             _lib.check(lib.hdfe_rademacher(Zall.data_ptr(), L + G + c, 0, size,
                                            int(seed) & (2**64 - 1), drawn, sh))
             Zl, Zg, Zc = Zall[:L], Zall[L:L + G], Zall[L + G:]
             *_, (vl, vx, vg) = self.apply_inverse(Zl, Zc, Zg, omega=omega)
             Ul, _, Ug, _ = self.apply_inverse(vl, vx, vg)
-            _lib.check(lib.hdfe_trace_moments(
-                self.starts.data_ptr(), G, self.rows.codes.data_ptr(), len(self.nlev),
-                self.nlev.ctypes.data, psi_column, self._ptr(self.w), Zl.data_ptr(),
-                Zg.data_ptr(), Ul.data_ptr(), Ug.data_ptr(), size, mom.data_ptr(), ws.data_ptr(),
-                ws.numel(), self._status().data_ptr(), sh))
+            with self._phase("k_trace"):
+                _lib.check(lib.hdfe_trace_moments(
+                    self.starts.data_ptr(), G, self.rows.codes.data_ptr(), len(self.nlev),
+                    self.nlev.ctypes.data, psi_column, self._ptr(self.w), Zl.data_ptr(),
+                    Zg.data_ptr(), Ul.data_ptr(), Ug.data_ptr(), size, mom.data_ptr(),
+                    ws.data_ptr(), ws.numel(), self._status().data_ptr(), sh))
             totals += mom[:size].sum(dim=0)
             drawn += size
             blocks += 1
-        t = (totals / n_draws).cpu().numpy()
-        weight, a1a2, b1b2, cross, a1, a2, b1, b2 = t
-        var_psi = a1a2 / weight - (a1 / weight) * (a2 / weight)
-        var_alpha = b1b2 / weight - (b1 / weight) * (b2 / weight)
-        cov = 0.5 * (cross / weight - (a1 / weight) * (b2 / weight) - (b1 / weight) * (a2 / weight))
-        # leaveout_se.py:202-214 `_moment_divisor`: n - 1 person-years
-        R = float(self.N if person_years is None else person_years)
-        scale = weight / (weight * (R - 1.0) / R) if R > 1 else 1.0
-        self.trace_info = {"blocks": blocks, "n_obs": float(weight)}
-        return np.array([scale * var_psi, scale * var_alpha, scale * cov])
+        return totals, blocks
+
+    def hutchinson_trace(self, sigma2, n_draws=250, block=None, seed=0, covariates=None,
+                         psi=None, person_years=None) -> TraceEstimate:
+        """leaveout.py:321-391 `hutchinson_trace` and :393-448 `_trace_block`:
+        the bias terms of var(psi), var(alpha) and cov(psi, alpha) from
+        n_draws Rademacher vectors in coefficient space, two applications of
+        the inverse per block; sigma2 (N) per-row variances (w Var(e)).
+        Draws are keyed on (seed, position, draw), so the answer does not
+        depend on blocking.  person_years: the divisor's count when the rows
+        are matches (leaveout_se.py:216-220)."""
+        return self._hutchinson(sigma2, n_draws, block, seed, covariates, psi, person_years)
+
+    def _hutchinson(self, sigma2, n_draws, block, seed, covariates, psi, person_years,
+                    draws=None, reduce=None):
+        self._check_covariates(covariates)
+        psi_column = self._psi_column(psi)
+        if n_draws < 1:
+            raise ValueError("n_draws must be at least 1")
+        first, last = (0, int(n_draws)) if draws is None else draws
+        totals, blocks = self.trace_totals(sigma2, first, last, block, seed, psi_column)
+        if reduce is not None:
+            reduce(totals)
+        bias = trace_components(totals.cpu().numpy() / n_draws,
+                                self.N if person_years is None else person_years)
+        self.trace_info = {"blocks": blocks, "n_obs": float(totals[0].item() / n_draws)}
+        return TraceEstimate(var_psi=float(bias[0]), var_alpha=float(bias[1]),
+                             cov=float(bias[2]), n_draws=int(n_draws),
+                             diagnostics={"blocks": blocks,
+                                          "block": MAX_BLOCK if block is None else int(block),
+                                          "psi": self.o_fe[psi_column], "covariates": self.c,
+                                          "draws": (first, last)})
 
     # ---- steps 3-4 and the KSS components (core/inference.py, leaveout.py:634-1016)
 
@@ -318,65 +517,240 @@ class InverseOperator:
             self._status().data_ptr(), _lib.stream_handle()))
         return resid, alpha[:self.G], gam_y, sums
 
-    def leave_out_components(self, gamma, n_draws=250, block=MAX_BLOCK, seed=0, psi_column=0,
-                             timer=None):
-        """leaveout.py:634-805 `leave_out_components` (point estimates;
-        stayers "own", weighted centring): beta from the residual moments,
-        the plug-in var(psi), var(alpha), cov(psi, alpha) (:807-833) with the
-        n - 1 divisor, sigma2 from the JLA leverages and the residuals
-        (:949-1016), the Hutchinson bias with seed + 1_000_003, and
-        leave_out = plug_in - bias.  gamma (L, m) the fit's normalised
-        effects for V's variables (y first).  timer: a `fit.PhaseTimer` for
-        the phases "steps34", "leverages", "sigma2" and "trace"."""
-        import contextlib
+    def movers(self, psi=None):
+        """(movers (N) bool, psi codes (N) int64) on the device
+        (leaveout.py:928-947 `_mover_mask`): a row is a mover's when its
+        group is seen at more than one level of psi."""
         torch = _torch()
-        phase = timer or (lambda name: contextlib.nullcontext())
-        with phase("steps34"):
-            A = self.residual_moments(gamma).cpu().numpy()
-            m = A.shape[0]
-            beta = np.linalg.solve(A[1:, 1:], A[1:, 0]) if m > 1 else np.zeros(0)
-            resid, _, _, sums = self.row_effects(gamma, beta, psi_column)
-            s = sums.cpu().numpy()
+        col = self._psi_column(psi)
+        code = self.rows.codes[:, col].to(torch.int64)
+        g = self.rows.gcode.to(torch.int64)
+        n_g = int(g.max().item()) + 1 if self.N else 0
+        lo = torch.full((n_g,), 2 ** 62, dtype=torch.int64, device=self.dev)
+        hi = torch.full((n_g,), -1, dtype=torch.int64, device=self.dev)
+        lo.scatter_reduce_(0, g, code, "amin")
+        hi.scatter_reduce_(0, g, code, "amax")
+        return (lo != hi)[g], code
+
+    def leave_out_sigma2(self, y, residual, leverages: JLALeverages, movers, psi_code,
+                         stayers="own", centering="weighted", stayer_sigma2=None, ybar=None):
+        """leaveout.py:949-1016 `_leave_one_out_sigma2` on the device:
+        sigma2_i = w_i (y_i - ybar) e_i / M_ii times the JLA factor (the
+        weighted centring's fused kernel `hdfe_kss_sigma2`), or
+        (sqrt(w) y - its mean) sqrt(w) e / M times the factor with
+        centering "reference"; stayers "own" keep theirs, "drop" get zero,
+        "firm_mean" the w-weighted mean of sigma2 / w over the movers at
+        their psi level (times w), "within_match" the caller's
+        `stayer_sigma2` (N).  ybar: the weighted mean of y when known."""
+        torch = _torch()
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        w = self.w if self.w is not None else torch.ones(self.N, **f64)
+        comp, factor = leverages.complement, leverages.factor
+        if centering == "weighted":
+            sigma2 = torch.empty(self.N, **f64)
+            if ybar is None:
+                ybar = float((w @ y).item() / w.sum().item())
+            y, residual = y.contiguous(), residual.contiguous()
+            _lib.check(_lib.lib().hdfe_kss_sigma2(
+                y.data_ptr(), self._ptr(self.w), residual.data_ptr(), comp.data_ptr(),
+                factor.data_ptr(), ybar, self.N, sigma2.data_ptr(), _lib.stream_handle()))
+        elif centering == "reference":
+            root = torch.sqrt(w)
+            yt = root * y
+            sigma2 = (yt - yt.mean()) * root * residual / comp * factor
+        else:
+            raise ValueError("centering must be 'weighted' or 'reference'")
+        if stayers == "own":
+            return sigma2
+        stay = ~movers
+        if stayers == "drop":
+            return torch.where(stay, torch.zeros_like(sigma2), sigma2)
+        if stayers == "within_match":
+            return torch.where(stay, torch.as_tensor(stayer_sigma2).to(**f64), sigma2)
+        n_lev = int(psi_code.max().item()) + 1 if self.N else 0
+        tot = torch.zeros(n_lev, **f64).index_add_(0, psi_code[movers], (sigma2 * w)[movers])
+        cnt = torch.zeros(n_lev, **f64).index_add_(0, psi_code[movers], (w * w)[movers])
+        mean = torch.where(cnt > 0, tot / torch.where(cnt > 0, cnt, 1.0),
+                           torch.full_like(cnt, float("nan")))
+        sigma2 = torch.where(stay, mean[psi_code] * w, sigma2)
+        orphaned = int((~torch.isfinite(sigma2)).sum().item())
+        if orphaned:
+            raise ValueError(f"{orphaned:,} observations sit at a level of the chosen dimension "
+                             "with no movers, so there is nothing to impute their variance "
+                             "from; prune to the leave-one-out connected set first")
+        return sigma2
+
+    def plug_in_moments(self, gamma, psi=None):
+        """(plug-in dict, beta, residuals (N), sums (7)): beta from the
+        residual moments (steps 3-4), the rows' residuals and the weighted
+        plug-in var(psi), var(alpha), cov(psi, alpha) with the n - 1 divisor
+        (leaveout.py:807-833 `_plug_in_moments`)."""
+        A = self.residual_moments(gamma).cpu().numpy()
+        m = A.shape[0]
+        beta = np.linalg.solve(A[1:, 1:], A[1:, 0]) if m > 1 else np.zeros(0)
+        resid, _, _, sums = self.row_effects(gamma, beta, self._psi_column(psi))
+        s = sums.cpu().numpy()
         if int(self._status().item()) != _lib.HDFE_OK:
             raise _lib.HDFEError(int(self._status().item()), "a level code is out of range")
         T = s[0]
         R = float(self.N)
         scale = T / (T * (R - 1.0) / R) if R > 1 else 1.0
         ma, mb = s[2] / T, s[3] / T
-        plug_in = np.array([scale * (s[4] / T - ma * ma), scale * (s[5] / T - mb * mb),
-                            scale * (s[6] / T - ma * mb)])
-        with phase("leverages"):
-            lev, comp, factor = self.jla_leverages(n_draws, block, seed)
-        with phase("sigma2"):
-            sigma2 = torch.empty(self.N, dtype=torch.float64, device=self.dev)
-            _lib.check(_lib.lib().hdfe_kss_sigma2(
-                self.rows.V.data_ptr(), self._ptr(self.w), resid.data_ptr(), comp.data_ptr(),
-                factor.data_ptr(), float(s[1] / T), self.N, sigma2.data_ptr(),
-                _lib.stream_handle()))
-        with phase("trace"):
-            bias = self.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003, psi_column)
-        return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "beta": beta,
-                "sigma2": sigma2, "max_leverage": float(lev.max().item()), "leverage": lev,
-                "complement": comp, "factor": factor}
+        plug_in = {COMPONENTS[0]: float(scale * (s[4] / T - ma * ma)),
+                   COMPONENTS[1]: float(scale * (s[5] / T - mb * mb)),
+                   COMPONENTS[2]: float(scale * (s[6] / T - ma * mb))}
+        return plug_in, beta, resid, s
 
-    def jla_leverages(self, n_draws=250, block=MAX_BLOCK, seed=0):
-        """leaveout.py:130-198 `jla_leverages`: (leverage, complement, factor)
-        per row (device tensors), in the square-root weight metric when the
-        fit is weighted."""
+    def leave_out_components(self, result, n_draws=250, block=None, seed=0, psi=None,
+                             covariates=None, stayers="own", se=False, se_draws=None,
+                             se_trace=True, smooth_bins=None, diagnose=None, diagnose_draws=64,
+                             weak_interval=True, confidence=0.95, stayer_sigma2=None,
+                             centering="weighted", timer=None, split=None) -> LeaveOutComponents:
+        """leaveout.py:634-805 `leave_out_components`, on the device:
+        `result` the fit (a `fit.FitResult`, or its normalised effects
+        Gamma (L, m) for V's variables, outcome first).  JLA leverages for
+        n_draws probes (seed), the maximum-leverage check, the weighted
+        plug-in components, beta and the residuals (steps 3-4), sigma2 by
+        the `stayers` and `centering` rules, the Hutchinson bias
+        (seed + 1_000_003) and leave_out = plug_in - bias; with `diagnose`
+        (default: `se`) the weak-identification diagnostic (diagnose_draws,
+        seed + 9_900_019); with `se` the standard errors
+        (`component_variances`, se_draws, seed + 5_500_011) and, for the
+        components the diagnostic flags, the q = 1 intervals at
+        `confidence`.  `timer`: a `fit.PhaseTimer` for the phases
+        "steps34", "leverages", "sigma2" and "trace".  `split`: a
+        `shard.DrawSplit` when the job's probes and draws are shared among
+        ranks (each rank runs this call on its own replica of the design)."""
+        import contextlib
         torch = _torch()
-        block = int(block)
-        if block < 1 or n_draws < 1:
-            raise ValueError("n_draws and block must be at least 1")
+        if stayers not in ("own", "firm_mean", "drop", "within_match"):
+            raise ValueError("stayers must be 'own', 'firm_mean', 'drop' or 'within_match'")
+        if (stayers == "within_match") != (stayer_sigma2 is not None):
+            raise ValueError("stayers='within_match' needs stayer_sigma2, the per-match values "
+                             "from leave_out_match")
+        self._check_covariates(covariates)
+        col = self._psi_column(psi)
+        psi_name = self.o_fe[col]
+        gamma = result.gamma if hasattr(result, "gamma") else result
+        phase = timer or (lambda name: contextlib.nullcontext())
+        with phase("leverages"):
+            if split is None:
+                lev = self.jla_leverages(n_draws, block, seed)
+            else:
+                lev = self._jla(n_draws, block, seed, None, split.draws(n_draws), split.sum)
+        movers, psi_code = self.movers(col)
+        match_level = stayers == "within_match"
+        checked = movers if match_level else torch.ones_like(movers)
+        worst = float(lev.leverage[checked].max().item()) if bool(checked.any()) else 0.0
+        if worst >= 1.0 - 1e-9:
+            unit = "match" if match_level else "observation"
+            raise ValueError(
+                f"maximum leverage is {worst:.6f}: the panel is not leave-one-out connected "
+                f"(leaving out one {unit} at a time), so the leave-out residual is undefined "
+                f"for at least one {unit}; restrict the rows to the leave-one-out connected "
+                "set first (connected.leave_one_out)")
+        with phase("steps34"):
+            plug_in, beta, resid, sums = self.plug_in_moments(gamma, col)
+        with phase("sigma2"):
+            sigma2 = self.leave_out_sigma2(self.rows.V[0], resid, lev, movers, psi_code,
+                                           stayers, centering, stayer_sigma2,
+                                           ybar=float(sums[1] / sums[0]))
+        with phase("trace"):
+            if split is None:
+                trace = self.hutchinson_trace(sigma2, n_draws, block, seed + TRACE_SEED_OFFSET,
+                                              psi=col)
+            else:
+                trace = self._hutchinson(sigma2, n_draws, block, seed + TRACE_SEED_OFFSET, None,
+                                         col, None, split.draws(n_draws), split.sum)
+        bias = trace.as_dict()
+        leave_out = {k: plug_in[k] - bias[k] for k in plug_in}
+        if diagnose is None:
+            diagnose = bool(se)
+        weak_id = None
+        errors = None
+        if (diagnose or se) and split is not None:
+            raise ValueError("the standard errors and the diagnostic run on one rank: "
+                             "call without split for se=True or diagnose=True")
+        if diagnose or se:
+            from .leaveout_se import StandardErrors
+            ses = StandardErrors(self, col)
+        if diagnose:
+            from .weakid import weak_id_diagnostics
+            weak_id = weak_id_diagnostics(ses, sigma2, lev.leverage, n_draws=int(diagnose_draws),
+                                          block=MAX_BLOCK if block is None else int(block),
+                                          seed=seed + WEAK_ID_SEED_OFFSET)
+        if se:
+            from .leaveout_se import ComponentSE, weak_intervals
+            draws = n_draws if se_draws is None else int(se_draws)
+            raw = ses.component_variances(
+                sigma2, lev.leverage, lev.complement, lev.factor, None, draws,
+                8 if block is None else int(block), seed + SE_SEED_OFFSET, se_trace,
+                smooth_bins, weak_id=weak_id if weak_interval else None)
+            if raw["weak"]:
+                weak_intervals(leave_out, raw["weak"], confidence)
+            errors = ComponentSE.from_dict(raw, trace=se_trace)
+        w = self.w
+        s2_mean = float((sigma2 / w).mean().item()) if w is not None else \
+            float(sigma2.mean().item())
+        return LeaveOutComponents(
+            plug_in=plug_in, bias=bias, leave_out=leave_out, n_obs=self.N,
+            n_movers=int(movers.sum().item()), leverages=lev, trace=trace, se=errors,
+            weak_id=weak_id, fit=result if hasattr(result, "gamma") else None,
+            diagnostics={"psi": psi_name, "alpha": self.g_fe, "stayers": stayers,
+                         "confidence": confidence, "max_leverage": worst,
+                         "leave_out": "match" if match_level else "observation",
+                         "sigma2_mean": s2_mean, "covariates": self.c, "beta": beta,
+                         "sigma2": sigma2, "centering": centering,
+                         "n_levels": {psi_name: int(self.nlev[col]), self.g_fe: self.G}})
+
+    def jla_moments(self, first, last, block=None, seed=0, moments=None):
+        """The JLA sink's five running sums per row (leaveout.py:181-190:
+        P, M, P^2, M^2, P M over the draws) for the draws [first, last),
+        added into `moments` (5, N) (zeros when None); returns (moments,
+        blocks, the last block's solve info)."""
+        torch = _torch()
+        block = MAX_BLOCK if block is None else int(block)
+        if block < 1:
+            raise ValueError("block must be at least 1")
         block = min(block, MAX_BLOCK)
-        moments = torch.zeros((5, self.N), dtype=torch.float64, device=self.dev)
-        drawn, blocks, info = 0, 0, {}
-        while drawn < n_draws:
-            size = min(block, n_draws - drawn)
+        if moments is None:
+            moments = torch.zeros((5, self.N), dtype=torch.float64, device=self.dev)
+        drawn, blocks, info = int(first), 0, {}
+        while drawn < last:
+            size = min(block, last - drawn)
             _, info = self.project(size, seed, drawn, sqrt_weights=self.w is not None,
                                    out=False, moments=moments)
             drawn += size
             blocks += 1
+        return moments, blocks, info
+
+    def combine_moments(self, moments, n_draws):
+        """leaveout.py:210-282 `_combine_moments` in place (`hdfe_jla_combine`):
+        slot 0 <- the leverage, 1 <- its complement, 2 <- the factor."""
         _lib.check(_lib.lib().hdfe_jla_combine(moments.data_ptr(), self.N, n_draws,
                                                _lib.stream_handle()))
+        return moments
+
+    def jla_leverages(self, n_draws=250, block=None, seed=0, covariates=None) -> JLALeverages:
+        """leaveout.py:130-198 `jla_leverages`: every row's leverage, its
+        complement and the correction factor (device tensors), in the
+        square-root weight metric when the fit is weighted; `block` draws
+        per projection pass (at most 32; None: 32)."""
+        return self._jla(n_draws, block, seed, covariates)
+
+    def _jla(self, n_draws, block, seed, covariates, draws=None, reduce=None):
+        self._check_covariates(covariates)
+        if n_draws < 1:
+            raise ValueError("n_draws must be at least 1")
+        first, last = (0, int(n_draws)) if draws is None else draws
+        moments, blocks, info = self.jla_moments(first, last, block, seed)
+        if reduce is not None:
+            reduce(moments)
+        self.combine_moments(moments, n_draws)
         self.jla_info = {**info, "blocks": blocks}
-        return moments[0], moments[1], moments[2]
+        return JLALeverages(leverage=moments[0], complement=moments[1], factor=moments[2],
+                            n_draws=int(n_draws),
+                            diagnostics={"blocks": blocks,
+                                         "block": MAX_BLOCK if block is None else int(block),
+                                         "covariates": self.c, "draws": (first, last),
+                                         "iterations": info.get("iterations")})

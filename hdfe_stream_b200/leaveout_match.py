@@ -30,10 +30,9 @@ from __future__ import annotations
 import numpy as np
 
 from . import fit as _fit
-from .leaveout import MAX_BLOCK, InverseOperator
-from .leaveout_se import StandardErrors
-
-SE_SEED_OFFSET = 5_500_011          # leaveout.py:770
+from .leaveout import (COMPONENTS, MAX_BLOCK, SE_SEED_OFFSET, TRACE_SEED_OFFSET,
+                       InverseOperator, LeaveOutComponents)
+from .leaveout_se import ComponentSE, StandardErrors
 
 
 def _torch():
@@ -46,10 +45,14 @@ def leave_out_match(rows: _fit.DeviceRows, res: _fit.FitResult, covariates=None,
                     se_variance="person_year", se_draws=None, se_trace=True, smooth_bins=None):
     """The match-level KSS components for a row-level fit `res` of `rows`
     (pass 0's layout; psi = the first non-streamed dimension; covariates
-    (N, c) the model's, or None): {"plug_in", "bias", "leave_out", "sigma2"
-    (per match), "n_matches", "stayer_matches", "person_years",
-    "max_leverage" (movers' matches)}; with `se` also "se" (the
-    `component_variances` dict, var(alpha) NaN) and "sigma2_se"."""
+    (N, c) the model's, or None), as the reference's `leave_out_match`
+    returns them: a `LeaveOutComponents` (plug_in, bias, leave_out keyed by
+    component; n_obs the person-years, n_movers the movers' matches;
+    leverages and trace of the match-level fit; se a `ComponentSE` with
+    var(alpha) NaN when `se`; fit = `res`, match_fit the match-level
+    `FitResult`), its diagnostics holding "sigma2" (per match),
+    "n_matches", "stayer_matches", "person_years", "max_leverage" (movers'
+    matches) and, with `se`, "sigma2_se"."""
     if se_variance not in ("match", "person_year"):
         raise ValueError("se_variance must be 'match' or 'person_year'")
     if se and se_variance == "person_year" and rows.w is not None:
@@ -90,7 +93,8 @@ def leave_out_match(rows: _fit.DeviceRows, res: _fit.FitResult, covariates=None,
     ma, mb = s[2] / T, s[3] / T
     plug_in = np.array([scale * (s[4] / T - ma * ma), scale * (s[5] / T - mb * mb),
                         scale * (s[6] / T - ma * mb)])
-    lev, comp, factor = mop.jla_leverages(n_draws, block, seed)
+    jla = mop.jla_leverages(n_draws, block, seed)
+    lev, comp, factor = jla.leverage, jla.complement, jla.factor
     root = torch.sqrt(W_m)
     yt = root * Y_m
     sigma2 = (yt - yt.mean()) * root * e_m / comp * factor
@@ -104,11 +108,20 @@ def leave_out_match(rows: _fit.DeviceRows, res: _fit.FitResult, covariates=None,
     r = (y_t - y_mean) * (y_t - fitted[match]) / (1.0 - w / worker_w[g])
     stay = torch.zeros(n_m, **f64).index_add_(0, match, w * w * r) / W_m
     sigma2 = torch.where(stayer, stay, sigma2).contiguous()
-    bias = mop.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003, person_years=R)
+    trace = mop.hutchinson_trace(sigma2, n_draws, block, seed + TRACE_SEED_OFFSET,
+                                 person_years=R)
+    bias = trace.as_array()
     movers = ~stayer
-    out = {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "sigma2": sigma2,
-           "n_matches": n_m, "stayer_matches": int(stayer.sum().item()), "person_years": N,
-           "max_leverage": float(lev[movers].max().item()) if bool(movers.any()) else 0.0}
+    diag = {"sigma2": sigma2, "n_matches": n_m, "stayer_matches": int(stayer.sum().item()),
+            "person_years": N, "leave_out": "match", "stayers": "within_match",
+            "centering": "reference", "psi": mop.o_fe[0], "alpha": mop.g_fe,
+            "max_leverage": float(lev[movers].max().item()) if bool(movers.any()) else 0.0,
+            "sigma2_mean": float((sigma2 / W_m).mean().item())}
+    out = LeaveOutComponents(
+        plug_in=dict(zip(COMPONENTS, plug_in.tolist())), bias=trace.as_dict(),
+        leave_out=dict(zip(COMPONENTS, (plug_in - bias).tolist())), n_obs=N,
+        n_movers=int(movers.sum().item()), leverages=jla, trace=trace, diagnostics=diag,
+        fit=res, match_fit=mres)
     if not se:
         return out
     # the movers' weighted-centred leave-match-out sigma2 (leaveout.py:949-1016)
@@ -125,9 +138,9 @@ def leave_out_match(rows: _fit.DeviceRows, res: _fit.FitResult, covariates=None,
     sigma2_se = sigma2_se.contiguous()
     ses = StandardErrors(mop, 0, person_years=N)
     draws = n_draws if se_draws is None else int(se_draws)
-    out["se"] = ses.component_variances(sigma2_se, lev, comp, factor, None, draws, block,
-                                        seed + SE_SEED_OFFSET, se_trace, smooth_bins,
-                                        stayer_rows=stayer, centering="reference",
-                                        reported=(0, 2))
-    out["sigma2_se"] = sigma2_se
+    raw = ses.component_variances(sigma2_se, lev, comp, factor, None, draws, block,
+                                  seed + SE_SEED_OFFSET, se_trace, smooth_bins,
+                                  stayer_rows=stayer, centering="reference", reported=(0, 2))
+    out.se = ComponentSE.from_dict(raw, trace=se_trace)
+    diag["sigma2_se"] = sigma2_se
     return out

@@ -30,12 +30,12 @@ two scalars per column ride into `hdfe_c_sums_ext`.
 
 from __future__ import annotations
 
+from dataclasses import dataclass, field
+
 import numpy as np
 
 from . import _lib
-from .leaveout import MAX_BLOCK, InverseOperator
-
-COMPONENTS = ("var(psi)", "var(alpha)", "cov(psi, alpha)")
+from .leaveout import COMPONENTS, MAX_BLOCK, InverseOperator
 QUANTILE_SAMPLE = 2_000_000         # rows sampled for the smoother's knots
 TRACE_SEED_OFFSET = 7_700_017       # leaveout_se.py:731
 WEAK_SEED_OFFSET = 8_800_021        # leaveout_se.py:757
@@ -59,6 +59,48 @@ def smoother_knots(values: np.ndarray, n_bins: int) -> np.ndarray:
     q = np.maximum.accumulate(q)
     span = max(float(q[-1] - q[0]), 1e-300)
     return q + np.arange(len(q)) * span * 1e-12
+
+
+@dataclass
+class ComponentSE:
+    """Standard errors of the three components and the parts they came from
+    (leaveout_se.py:74-111 `ComponentSE`), each a dict keyed "var(psi)",
+    "var(alpha)", "cov(psi, alpha)": se (NaN where none is reported), the
+    estimator's variance, its first term 4 sum_i sigma2_i (C mu)_i^2, the
+    trace term 2 tr(C Omega C Omega), the conservative se from the first
+    term alone, and theta = y'Cy (the estimand recomputed); n_draws the
+    trace's draws; weak, per weakly identified component, the q = 1
+    interval ("interval") and its pieces."""
+
+    se: dict
+    variance: dict
+    first_term: dict
+    trace_term: dict
+    se_conservative: dict
+    theta: dict
+    n_draws: int
+    diagnostics: dict = field(default_factory=dict)
+    weak: dict = None
+
+    @classmethod
+    def from_dict(cls, raw: dict, trace: bool = True) -> "ComponentSE":
+        """From `StandardErrors.component_variances`' dict."""
+        return cls(se=raw["se"], variance=raw["variance"], first_term=raw["first_term"],
+                   trace_term=raw["trace_term"], se_conservative=raw["se_conservative"],
+                   theta=raw["theta"], n_draws=int(raw["n_draws"]),
+                   diagnostics={"trace_included": bool(trace), "blocks": raw.get("blocks")},
+                   weak=raw.get("weak"))
+
+    def summary(self) -> str:
+        lines = [f"leave-out standard errors ({self.n_draws} draws)",
+                 f"{'component':<20}{'estimate':>12}{'se':>11}{'se (cons.)':>12}"
+                 f"{'trace share':>13}", "-" * 68]
+        for key in COMPONENTS:
+            share = (self.trace_term[key] / self.first_term[key]
+                     if self.first_term[key] else float("nan"))
+            lines.append(f"{key:<20}{self.theta[key]:>12.6f}{self.se[key]:>11.6f}"
+                         f"{self.se_conservative[key]:>12.6f}{share:>12.2%}")
+        return "\n".join(lines)
 
 
 class StandardErrors:

@@ -1154,7 +1154,8 @@ class Design:
         sigma2 = w * (y - ybar) * e / comp * factor
         bias = self.hutchinson_trace(sigma2, n_draws, block, seed + 1_000_003)
         return {"plug_in": plug_in, "bias": bias, "leave_out": plug_in - bias, "beta": beta,
-                "sigma2": sigma2, "max_leverage": float(lev.max())}
+                "sigma2": sigma2, "max_leverage": float(lev.max()), "leverage": lev,
+                "complement": comp, "factor": factor}
 
     # ---- KSS standard errors (leaveout_se.py), weighted centring
 

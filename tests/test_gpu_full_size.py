@@ -107,10 +107,10 @@ def test_kss_1m_recovers_the_true_components(device):
     res = fit.fit(drows, tol=1e-10)
     op = leaveout.InverseOperator(drows, res.cells, res.S, drows.V[1:].T.contiguous(),
                                   tol=1e-10)
-    kss = op.leave_out_components(res.gamma, 256, block=32, seed=1)
-    est = np.asarray(kss["leave_out"])
+    kss = op.leave_out_components(res, 256, block=32, seed=1)
+    est = np.array(list(kss.leave_out.values()))
     assert np.all(np.abs(est - truth) <= 0.03 * np.abs(truth)), (est, truth)
-    plug = np.asarray(kss["plug_in"])
+    plug = np.array(list(kss.plug_in.values()))
     assert np.all(np.abs(est - truth)[:2] < np.abs(plug - truth)[:2])
 
 

@@ -24,6 +24,14 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
+COMPONENTS = ("var(psi)", "var(alpha)", "cov(psi, alpha)")
+
+
+def vals(d):
+    """A component dict as an array in the reference's key order."""
+    return np.array([d[k] for k in COMPONENTS])
+
+
 def operator(rows, tol, covariates=False, precision="fp64"):
     from hdfe_stream_b200 import fit, leaveout
     drows = fit.DeviceRows.from_rows(rows)
@@ -48,7 +56,9 @@ def test_jla_leverages_match_reference(device, name):
     g = load_golden(name)
     rows = golden_rows(g)
     op = operator(rows, float(g["tol"]))
-    lev, comp, factor = op.jla_leverages(24, block=8, seed=2)
+    j = op.jla_leverages(24, block=8, seed=2)
+    lev, comp, factor = j.leverage, j.complement, j.factor
+    assert j.n_draws == 24 and j.diagnostics["blocks"] == 3 and j.n_rows == rows.n_rows
     assert rel(lev.cpu().numpy(), g["jla_leverage"]) < 1e-8
     assert rel(factor.cpu().numpy(), g["jla_factor"]) < 1e-8
     assert np.allclose(lev.cpu().numpy() + comp.cpu().numpy(), 1.0)
@@ -57,9 +67,9 @@ def test_jla_leverages_match_reference(device, name):
 def test_jla_blocking_does_not_change_the_answer(device):
     g = load_golden("akm_small")
     op = operator(golden_rows(g), 1e-12)
-    a = op.jla_leverages(24, block=8, seed=2)[0].cpu().numpy().copy()
-    b = op.jla_leverages(24, block=24, seed=2)[0].cpu().numpy().copy()
-    c = op.jla_leverages(24, block=5, seed=2)[0].cpu().numpy().copy()
+    a = op.jla_leverages(24, block=8, seed=2).leverage.cpu().numpy().copy()
+    b = op.jla_leverages(24, block=24, seed=2).leverage.cpu().numpy().copy()
+    c = op.jla_leverages(24, block=5, seed=2).leverage.cpu().numpy().copy()
     assert rel(a, b) < 1e-9 and rel(a, c) < 1e-9
 
 
@@ -76,7 +86,8 @@ def test_projection_with_covariates_matches_oracle(device, name):
     out, _ = op.project(20, seed=5, first_draw=3, sqrt_weights=rows.w is not None)
     assert rel(out.cpu().numpy(), ref) < 1e-8
     lev_ref, _, f_ref = des.jla_leverages(40, 16, 7)
-    lev, _, f = op.jla_leverages(40, block=32, seed=7)
+    j = op.jla_leverages(40, block=32, seed=7)
+    lev, f = j.leverage, j.factor
     assert rel(lev.cpu().numpy(), lev_ref) < 1e-8
     assert rel(f.cpu().numpy(), f_ref) < 1e-8
 
@@ -121,9 +132,31 @@ def test_long_groups_and_block_widths(device, weights):
         out, _ = op.project(B, seed=9, first_draw=first, sqrt_weights=sw)
         assert rel(out.cpu().numpy(), ref) < 1e-8, B
     lev_ref, _, f_ref = des.jla_leverages(45, 16, 4)
-    lev, _, f = op.jla_leverages(45, block=32, seed=4)
+    j = op.jla_leverages(45, block=32, seed=4)
+    lev, f = j.leverage, j.factor
     assert rel(lev.cpu().numpy(), lev_ref) < 1e-8
     assert rel(f.cpu().numpy(), f_ref) < 1e-8
+
+
+@pytest.mark.parametrize("weights", [False, True])
+def test_mixed_precision_leverages_match_oracle(device, weights):
+    """The JLA leverages with the block solves in mixed precision (FP32 inner
+    CG on 32 columns, FP64 refinement to the same residual tolerance) and
+    the Hutchinson bias terms, against the FP64 oracle with the same draws."""
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    rows = pass0_layout(simulate_panel(3_000, 300, 10, spell=(3, 10), p_move=0.15,
+                                       weights=weights, seed=23))
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), X=rows.V[:, 1:], tol=1e-12)
+    lev_ref, _, f_ref = des.jla_leverages(64, 32, 5)
+    op = operator(rows, 1e-12, covariates=True, precision="mixed")
+    j = op.jla_leverages(64, block=32, seed=5)
+    assert rel(j.leverage.cpu().numpy(), lev_ref) < 1e-8
+    assert rel(j.factor.cpu().numpy(), f_ref) < 1e-8
+    sigma2 = np.abs(rows.V[:, 0] - rows.V[:, 0].mean()) * 0.1 + 0.05
+    tr_ref = des.hutchinson_trace(sigma2, 32, 32, 7)
+    tr = op.hutchinson_trace(sigma2, 32, block=32, seed=7).as_array()
+    assert rel(tr, tr_ref) < 1e-8
 
 
 @pytest.mark.parametrize("name", GOLDEN_PANELS)
@@ -152,7 +185,9 @@ def test_hutchinson_trace_matches_reference(device, name):
     rows = golden_rows(g)
     op = operator(rows, float(g["tol"]))
     tr = op.hutchinson_trace(g["trace_sigma2"], n_draws=16, block=8, seed=4)
-    assert rel(tr, g["trace"]) < 1e-8
+    assert tr.n_draws == 16 and tr.diagnostics["blocks"] == 2
+    assert rel(tr.as_array(), g["trace"]) < 1e-8
+    assert rel(vals(tr.as_dict()), g["trace"]) < 1e-8
 
 
 def test_hutchinson_blocking_and_covariates(device):
@@ -165,8 +200,8 @@ def test_hutchinson_blocking_and_covariates(device):
     sigma2 = g["trace_sigma2"]
     ref = des.hutchinson_trace(sigma2, 20, 20, 3)
     op = operator(rows, 1e-12, covariates=True)
-    a = op.hutchinson_trace(sigma2, n_draws=20, block=20, seed=3)
-    b = op.hutchinson_trace(sigma2, n_draws=20, block=7, seed=3)
+    a = op.hutchinson_trace(sigma2, n_draws=20, block=20, seed=3).as_array()
+    b = op.hutchinson_trace(sigma2, n_draws=20, block=7, seed=3).as_array()
     assert rel(a, ref) < 1e-8
     assert rel(a, b) < 1e-9
 
@@ -226,13 +261,29 @@ def test_leave_out_components_match_oracle(device, name):
     ref = des.leave_out_components(gamma, 16, 8, 5)
     assert np.all(np.isfinite(ref["sigma2"]))
     op = operator(rows, 1e-12, covariates=True)
+    from hdfe_stream_b200.leaveout import JLALeverages, LeaveOutComponents, TraceEstimate
     got = op.leave_out_components(torch.as_tensor(gamma, device=device), 16, 8, 5)
-    assert rel(got["beta"], ref["beta"]) < 1e-10
-    assert rel(got["plug_in"], ref["plug_in"]) < 1e-10
-    assert rel(got["sigma2"].cpu().numpy(), ref["sigma2"]) < 1e-8
-    assert rel(got["bias"], ref["bias"]) < 1e-8
-    assert rel(got["leave_out"], ref["leave_out"]) < 1e-8
-    assert abs(got["max_leverage"] - ref["max_leverage"]) < 1e-8
+    assert isinstance(got, LeaveOutComponents)
+    assert isinstance(got.leverages, JLALeverages) and isinstance(got.trace, TraceEstimate)
+    assert list(got.plug_in) == list(got.bias) == list(got.leave_out) == list(COMPONENTS)
+    assert got.n_obs == rows.n_rows and got.leverages.n_draws == 16 and got.trace.n_draws == 16
+    d = got.diagnostics
+    assert rel(d["beta"], ref["beta"]) < 1e-10
+    assert rel(vals(got.plug_in), ref["plug_in"]) < 1e-10
+    assert rel(d["sigma2"].cpu().numpy(), ref["sigma2"]) < 1e-8
+    assert rel(vals(got.bias), ref["bias"]) < 1e-8
+    assert rel(vals(got.leave_out), ref["leave_out"]) < 1e-8
+    assert rel(got.leverages.leverage.cpu().numpy(), ref["leverage"]) < 1e-8
+    assert rel(got.leverages.factor.cpu().numpy(), ref["factor"]) < 1e-8
+    assert abs(d["max_leverage"] - ref["max_leverage"]) < 1e-8
+    # movers: rows of workers seen at more than one firm
+    firm = rows.codes[:, 0]
+    lo = np.full(rows.n_groups, np.iinfo(np.int64).max)
+    hi = np.full(rows.n_groups, -1)
+    np.minimum.at(lo, rows.gcode, firm)
+    np.maximum.at(hi, rows.gcode, firm)
+    assert got.n_movers == int((lo != hi)[rows.gcode].sum())
+    assert len(got.tidy()) == 3 and "leave-out" in got.summary()
 
 
 def test_steps_3_4_on_a_device_fit(device):
@@ -273,10 +324,11 @@ def test_leave_out_components_against_exact_prototype(device):
     drows = fit.DeviceRows.from_rows(rows)
     res = fit.fit(drows, tol=1e-12)
     op = leaveout.InverseOperator(drows, res.cells, res.S, None, tol=1e-12)
-    out = op.leave_out_components(res.gamma, 1024, 32, 3)
-    assert rel(out["plug_in"], g["plug_in"]) < 1e-9
-    assert np.all(np.abs(out["leave_out"] - g["kss"]) <= 0.05 * np.abs(g["bias"]))
-    assert float(torch.mean(torch.abs(out["leverage"].cpu() - torch.as_tensor(g["P_ii"])))) < 0.02
+    out = op.leave_out_components(res, 1024, 32, 3)
+    assert rel(vals(out.plug_in), g["plug_in"]) < 1e-9
+    assert np.all(np.abs(vals(out.leave_out) - g["kss"]) <= 0.05 * np.abs(g["bias"]))
+    lev = out.leverages.leverage.cpu()
+    assert float(torch.mean(torch.abs(lev - torch.as_tensor(g["P_ii"])))) < 0.02
 
 
 def test_leave_out_match_matches_oracle(device):
@@ -299,11 +351,13 @@ def test_leave_out_match_matches_oracle(device):
     drows = fit.DeviceRows.from_rows(rows)
     res = fit.fit(drows, tol=1e-12)
     got = leave_out_match(drows, res, n_draws=64, block=32, seed=5, tol=1e-12)
-    assert got["n_matches"] == ref["n_matches"]
-    assert got["stayer_matches"] == ref["stayer_matches"]
-    assert rel(got["plug_in"], ref["plug_in"]) < 1e-9
-    assert rel(got["sigma2"].cpu().numpy(), ref["sigma2"]) < 1e-7
-    assert rel(got["bias"], ref["bias"]) < 1e-7
+    d = got.diagnostics
+    assert d["n_matches"] == ref["n_matches"]
+    assert d["stayer_matches"] == ref["stayer_matches"]
+    assert got.n_obs == rows.n_rows and d["leave_out"] == "match"
+    assert rel(vals(got.plug_in), ref["plug_in"]) < 1e-9
+    assert rel(d["sigma2"].cpu().numpy(), ref["sigma2"]) < 1e-7
+    assert rel(vals(got.bias), ref["bias"]) < 1e-7
     g = load_golden("exact")
     erows = Rows(gcode=g["gcode"], codes=g["codes_rows"], V=g["V"][:, :1], w=None,
                  n_levels=[int(x) for x in g["n_levels"]], n_groups=int(g["n_groups"][0]),
@@ -311,8 +365,8 @@ def test_leave_out_match_matches_oracle(device):
     d2 = fit.DeviceRows.from_rows(erows)
     out = leave_out_match(d2, fit.fit(d2, tol=1e-12), n_draws=256, block=32, seed=3, tol=1e-12)
     st = g["match_stayer"]
-    assert rel(out["plug_in"], g["match_plug_in"]) < 1e-9
-    assert rel(out["sigma2"].cpu().numpy()[st], g["match_sigma2"][st]) < 1e-8
+    assert rel(vals(out.plug_in), g["match_plug_in"]) < 1e-9
+    assert rel(out.diagnostics["sigma2"].cpu().numpy()[st], g["match_sigma2"][st]) < 1e-8
 
 
 @pytest.mark.parametrize("rule,weights", [("person_year", False), ("match", True)])
@@ -337,11 +391,12 @@ def test_leave_out_match_standard_errors_match_oracle(device, rule, weights):
     res = fit.fit(drows, tol=1e-12)
     got = leave_out_match(drows, res, n_draws=64, block=32, seed=5, tol=1e-12, se=True,
                           se_variance=rule, se_draws=24)
-    assert rel(got["sigma2_se"].cpu().numpy(), ref["sigma2_se"]) < 1e-7
+    assert rel(got.diagnostics["sigma2_se"].cpu().numpy(), ref["sigma2_se"]) < 1e-7
     names = ("var(psi)", "cov(psi, alpha)")
     for key in ("theta", "first_term", "trace_term", "variance"):
-        assert rel([got["se"][key][n] for n in names], ref["se"][key][[0, 2]]) < 1e-6, key
-    assert np.isnan(got["se"]["variance"]["var(alpha)"])
+        part = getattr(got.se, key)
+        assert rel([part[n] for n in names], ref["se"][key][[0, 2]]) < 1e-6, key
+    assert np.isnan(got.se.variance["var(alpha)"])
     if rule == "person_year":
         with pytest.raises(ValueError):
             wrows = fit.DeviceRows.from_rows(pass0_layout(

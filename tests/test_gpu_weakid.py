@@ -137,9 +137,9 @@ def test_weak_id_against_exact_prototype(device):
     drows = fit.DeviceRows.from_rows(rows)
     res = fit.fit(drows, tol=1e-12)
     op = leaveout.InverseOperator(drows, res.cells, res.S, None, tol=1e-12)
-    kss = op.leave_out_components(res.gamma, 256, block=32, seed=3)
-    out = weak_id_diagnostics(leaveout_se.StandardErrors(op), kss["sigma2"], kss["leverage"],
-                              n_draws=64, block=32, seed=9)
+    kss = op.leave_out_components(res, 256, block=32, seed=3)
+    out = weak_id_diagnostics(leaveout_se.StandardErrors(op), kss.diagnostics["sigma2"],
+                              kss.leverages.leverage, n_draws=64, block=32, seed=9)
     for k in range(3):
         assert rel(out["eigenvalues"][k], ge[f"weak_eig{k}"]) < 1e-6
     assert list(out["q"]) == [int(x) for x in ge["weak_q"]]
