@@ -217,30 +217,11 @@ def run_ours(args, rank, world, local_rank):
     its = int(np.max(np.atleast_1d(info["iterations"])))
 
     # accuracy: FP64 and the mixed-precision solve (FP32 inner CG, FP64
-    # refinement) at tol 1e-12, each against an FP64 solve at 1e-13; the
-    # solves (components, PCG, normalisation) are timed on the same cells and S
-    cells, S = res.cells, res.S
-    ref = fit.solve(cells, S, tol=1e-13)
-    accuracy = {"tol": 1e-12, "oracle": "FP64 PCG at 1e-13"}
-    for prec in ("fp64", "mixed"):
-        for _ in range(2):
-            r = fit.solve(cells, S, tol=1e-12, precision=prec)
-        torch.cuda.synchronize()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        reps = max(args.steps, 3)
-        a0.record()
-        for _ in range(reps):
-            r = fit.solve(cells, S, tol=1e-12, precision=prec)
-        a1.record()
-        torch.cuda.synchronize()
-        err = float((r.gamma - ref.gamma).abs().max() / ref.gamma.abs().max())
-        accuracy[prec] = {"solve_ms": round(a0.elapsed_time(a1) / reps, 3),
-                          "iterations": r.info["iterations"],
-                          "max_rel_residual": r.info["max_rel_residual"],
-                          "rel_fe_err": err}
-    accuracy["mixed_speedup"] = round(accuracy["fp64"]["solve_ms"] / accuracy["mixed"]["solve_ms"], 3)
-
+    # refinement) compared at equal error -- for each, the loosest residual
+    # tolerance whose fixed effects are within 1e-8 (relative, max norm) of an
+    # FP64 solve at 1e-13, and the solve's time at that tolerance (components,
+    # PCG, normalisation on the same cells and S)
+    accuracy = equal_error_solves(res.cells, res.S, max(args.steps, 3))
     # KSS-JLA: p = 256 Rademacher probes through A S^- A' on the 1M-worker panel
     jla = run_jla(args, rank, world, dist) if args.jla else None
     adjoint = run_adjoint(args, rank) if args.jla else None
@@ -282,7 +263,7 @@ def run_ours(args, rank, world, local_rank):
                                            "x this run's iterations",
                          "peak_source": f"{peak_kind} hbm_gbs", "phases": roof},
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
-            "accuracy_1e-8": accuracy, "kss_jla": jla, "adjoint": adjoint,
+            "equal_error_1e-8": accuracy, "kss_jla": jla, "adjoint": adjoint,
             "batched": batched,
             "solve": {"iterations": info["iterations"], "converged": info["converged"],
                       "max_rel_residual": info["max_rel_residual"], "S_nnz": info["S_nnz"],
@@ -294,6 +275,45 @@ def run_ours(args, rank, world, local_rank):
     return out, rows
 
 
+TOL_LADDER = (1e-7, 3e-8, 1e-8, 3e-9, 1e-9, 3e-10, 1e-10, 3e-11, 1e-11, 3e-12, 1e-12)
+
+
+def equal_error_solves(cells, S, reps, target=1e-8):
+    """For FP64 and mixed precision: the loosest tolerance of TOL_LADDER
+    whose fixed effects are within `target` of an FP64 solve at 1e-13, with
+    its iterations and its solve time (CUDA events, `reps` solves)."""
+    import torch
+    from hdfe_stream_b200 import fit
+    ref = fit.solve(cells, S, tol=1e-13)
+    scale = float(ref.gamma.abs().max())
+    out = {"target_rel_fe_err": target, "oracle": "FP64 PCG at 1e-13", "norm": "max |dFE| / max |FE|"}
+    for prec in ("fp64", "mixed"):
+        chosen = None
+        for tol in TOL_LADDER:
+            r = fit.solve(cells, S, tol=tol, precision=prec)
+            err = float((r.gamma - ref.gamma).abs().max()) / scale
+            if err <= target:
+                chosen = (tol, err, r)
+                break
+        if chosen is None:
+            out[prec] = {"reached": False}
+            continue
+        tol, err, r = chosen
+        fit.solve(cells, S, tol=tol, precision=prec)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(reps):
+            fit.solve(cells, S, tol=tol, precision=prec)
+        a1.record()
+        torch.cuda.synchronize()
+        out[prec] = {"tol": tol, "rel_fe_err": err, "iterations": r.info["iterations"],
+                     "solve_ms": round(a0.elapsed_time(a1) / reps, 3)}
+    if out["fp64"].get("solve_ms") and out["mixed"].get("solve_ms"):
+        out["mixed_speedup"] = round(out["fp64"]["solve_ms"] / out["mixed"]["solve_ms"], 3)
+    return out
+
+
 def run_jla(args, rank, world, dist):
     """KSS `leave_out_components` on the 1M-worker panel with the model's
     covariates, from the device fit's Gamma: beta and the residuals (steps
@@ -301,34 +321,72 @@ def run_jla(args, rank, world, dist):
     term for 256 draws (two applications of the inverse per draw), blocks of
     32.  RHS solves per second = p (1 + 2) / device time of the whole call."""
     import torch
-    from hdfe_stream_b200 import fit, leaveout
+    from hdfe_stream_b200 import fit, leaveout, replicas, shard
     from hdfe_stream_b200.simulate import prepare
 
-    rows = prepare("kss_1m", seed=100 + rank)
+    # under torchrun the ranks share ONE job: the same panel, the probes and
+    # draws split over the ranks (one all-reduce of the moment sums each)
+    rows = prepare("kss_1m", seed=100)
     drows = fit.DeviceRows.from_rows(rows)
     res = fit.fit(drows, tol=args.tol)
     S = res.S
     X = drows.V[1:].T.contiguous()
     op = leaveout.InverseOperator(drows, res.cells, S, X, tol=args.tol)
     p = 256
-    op.leave_out_components(res.gamma, 32, block=32, seed=1)   # warm-up (border, null space)
+    split = shard.DrawSplit(rank, world, None) if dist else None
+
+    def kss_call(operator, timer=None):
+        if split is None:
+            return operator.leave_out_components(res, p, block=32, seed=1, timer=timer)
+        return shard.leave_out_components(operator, res, p, block=32, seed=1, timer=timer,
+                                          split=split)
+    op.leave_out_components(res, 32, block=32, seed=1)   # warm-up (border, null space)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     timer = fit.PhaseTimer()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ev[0].record()
-    kss = op.leave_out_components(res.gamma, p, block=32, seed=1, timer=timer)
+    kss = kss_call(op, timer)
     ev[1].record()
     torch.cuda.synchronize()
     phases = {k: v[0] for k, v in timer.totals().items()}
     ms = ev[0].elapsed_time(ev[1])
+    # the kernels one by one: the same call again with an event pair around
+    # every launch (kept apart from the timed call above, whose events are
+    # per phase only)
+    ktimer = fit.PhaseTimer()
+    op.timer = ktimer
+    it0 = dict(op.solver.stats)
+    kss_call(op)
+    op.timer = None
+    op.solver.timer = None
+    kern = {k: v for k, v in ktimer.totals().items()}
+    pcg_its = op.solver.stats["iterations"] - it0["iterations"]
+    roofline = kss_roofline(rows, S, kern, pcg_its, c=X.shape[1], B=32)
+    # the same call with the block solves in mixed precision (FP32 inner CG on
+    # 32 columns, FP64 refinement to the same residual tolerance)
+    op_m = leaveout.InverseOperator(drows, res.cells, S, X, tol=args.tol, precision="mixed")
+    kss_call(op_m)
+    torch.cuda.synchronize()
+    evm = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    evm[0].record()
+    kss_m = kss_call(op_m)
+    evm[1].record()
+    torch.cuda.synchronize()
+    ms_m = replicas.max_over_ranks(evm[0].elapsed_time(evm[1]), dist, "cuda")
+    comp = np.array([*kss.leave_out.values()])
+    comp_m = np.array([*kss_m.leave_out.values()])
+    mixed_block = {"ms": round(ms_m, 3), "value": round(3 * p / (ms_m / 1e3), 2),
+                   "unit": "RHS solves/s", "speedup_vs_fp64": round(ms / ms_m, 3),
+                   "max_rel_diff_leave_out": float(np.max(np.abs(comp_m - comp) / np.abs(comp)))}
+    block_cmp = equal_error_block(op, S, res.cells, max(args.steps, 3))
     ms_jla, ms_tr = phases["leverages"], phases["trace"]
     if dist:
         t = torch.tensor([ms, ms_jla, ms_tr], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_jla, ms_tr = (float(x) for x in t.tolist())
-    sigma2 = kss["sigma2"]
+    sigma2 = kss.diagnostics["sigma2"]
     bad = int((~torch.isfinite(sigma2)).sum().item())
     # KSS standard errors (leaveout_se.py `component_variances`): B_ii by p
     # draws, C y, and the trace term by p draws
@@ -336,7 +394,8 @@ def run_jla(args, rank, world, dist):
     se_op = StandardErrors(op)
     se_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     se_ev[0].record()
-    ses = se_op.component_variances(sigma2, kss["leverage"], kss["complement"], kss["factor"],
+    lev = kss.leverages
+    ses = se_op.component_variances(sigma2, lev.leverage, lev.complement, lev.factor,
                                     None, n_draws=p, block=8, seed=1)
     se_ev[1].record()
     torch.cuda.synchronize()
@@ -350,12 +409,13 @@ def run_jla(args, rank, world, dist):
            "block": 32, "ms": round(ms, 3), "ms_leverages": round(ms_jla, 3),
            "ms_trace": round(ms_tr, 3), "ms_steps34": round(phases["steps34"], 3),
            "ms_sigma2": round(phases["sigma2"], 3),
-           "value": round(world * 3 * p / (ms / 1e3), 2), "unit": "RHS solves/s",
+           "value": round(3 * p / (ms / 1e3), 2), "unit": "RHS solves/s",
            "note": "p (1 + 2 Hutchinson) RHS solves: the leverages' one application of "
                    "the inverse per probe and the bias term's two per draw; the timed call "
                    "is the whole leave_out_components (steps 3-4, leverages, sigma2, trace)",
-           "max_leverage": kss["max_leverage"], "plug_in": finite(kss["plug_in"]),
-           "bias_terms": finite(kss["bias"]), "leave_out": finite(kss["leave_out"]),
+           "max_leverage": kss.diagnostics["max_leverage"],
+           "plug_in": finite(kss.plug_in.values()), "bias_terms": finite(kss.bias.values()),
+           "leave_out": finite(kss.leave_out.values()),
            "rows_without_sigma2": bad,
            "standard_errors": {"se": dict(zip(ses["se"], finite(ses["se"].values()))),
                                "se_conservative": dict(zip(ses["se_conservative"], finite(
@@ -364,7 +424,10 @@ def run_jla(args, rank, world, dist):
                                "rhs_solves": 2 * p + 7 + 9 * p,
                                "note": "B_ii: 2 solves per draw; C y: 7; trace term: 9 "
                                        "per draw (6 then 3)"},
-           "iterations_last_block": op.jla_info["iterations"]}
+           "iterations_last_block": op.jla_info["iterations"], "roofline": roofline,
+           "mixed": mixed_block, "equal_error_1e-8_block": block_cmp,
+           "scaling": "strong (one job: probes and draws split over the ranks)" if dist
+                      else "single"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, str(REPO / "oracle"))
         import oracle as orc
@@ -382,6 +445,100 @@ def run_jla(args, rank, world, dist):
                                "cores": orc.num_threads(), "kind": "port",
                                "sample": "one block of 32 probes and one of 32 Hutchinson draws "
                                          "on the same panel"}
+    return out
+
+
+def equal_error_block(op, S, cells, reps, target=1e-8):
+    """One JLA block of 32 probes (the KSS path's solve): for FP64 and for
+    mixed precision, the loosest tolerance of TOL_LADDER whose projected rows
+    A S^- A' r are within `target` (relative, max norm) of an FP64 solve at
+    1e-13, and the block solve's time at that tolerance (CUDA events), with
+    its roofline: per iteration 12 nnz + 8 (L + 1) + 72 L k bytes in FP64,
+    8 nnz + 4 (L + 1) + 36 L k in the FP32 inner iterations."""
+    import torch
+    from hdfe_stream_b200 import fit
+    from hdfe_stream_b200.gpu import BlockSolver
+    dinv = fit.jacobi(cells.diag)
+    keep = op.solver
+    op.solver = BlockSolver(S, dinv, 1e-13, 5000)
+    ref, _ = op.project(32, seed=1)
+    rhs, _, sq = op.center(32, seed=1)
+    zero = (torch.linalg.vector_norm(rhs, dim=0) <= 1e-11 * torch.sqrt(sq)).cpu().numpy()
+    scale = float(ref.abs().max())
+    peak, _ = measured_peak()
+    L, k = S.L, 32
+    out = {"target_rel_err": target, "quantity": "projected rows of one 32-probe block",
+           "oracle": "FP64 PCG at 1e-13"}
+    for prec in ("fp64", "mixed"):
+        chosen = None
+        for tol in TOL_LADDER:
+            op.solver = BlockSolver(S, dinv, tol, 5000, precision=prec)
+            got, _ = op.project(32, seed=1)
+            err = float((got - ref).abs().max()) / scale
+            if err <= target:
+                chosen = (tol, err)
+                break
+        if chosen is None:
+            out[prec] = {"reached": False}
+            continue
+        tol, err = chosen
+        solver = op.solver
+        solver.solve_device(rhs, zero)
+        torch.cuda.synchronize()
+        its0 = solver.stats["iterations"]
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(reps):
+            solver.solve_device(rhs, zero)
+        a1.record()
+        torch.cuda.synchronize()
+        its = (solver.stats["iterations"] - its0) / reps
+        ms = a0.elapsed_time(a1) / reps
+        per_it = (12 * S.nnz + 8 * (L + 1) + 72 * L * k) if prec == "fp64" else \
+            (8 * S.nnz + 4 * (L + 1) + 36 * L * k)
+        gbs = per_it * its / (ms / 1e3) / 1e9
+        out[prec] = {"tol": tol, "rel_err": err, "iterations": its, "solve_ms": round(ms, 3),
+                     "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    op.solver = keep
+    if out["fp64"].get("solve_ms") and out["mixed"].get("solve_ms"):
+        out["mixed_speedup"] = round(out["fp64"]["solve_ms"] / out["mixed"]["solve_ms"], 3)
+    return out
+
+
+def kss_roofline(rows, S, kern, pcg_its, c, B):
+    """Per-kernel roofline of one leave_out_components call: each kernel's
+    compulsory DRAM bytes (N rows, D non-streamed codes, c covariates, L
+    levels, G groups, B vectors per launch; written out in the design
+    notes) over its CUDA-event time, against the measured HBM peak."""
+    N, D, L, G = rows.n_rows, rows.codes.shape[1], int(sum(rows.n_levels)), rows.n_groups
+    w = 0 if rows.w is None else 8
+    row = N * (4 * D + 8 * c + w)              # codes, covariates, weights: one read
+    per_launch = {
+        "k_center": row + L * B * 8,
+        "k_project": row + L * B * 8 + 80 * N,            # U gathers, the 5 JLA sums r/w
+        "k_reduce": row + G * B * 8 + L * B * 8,
+        "k_project_coef": row + L * B * 8 + 2 * G * B * 8,
+        "k_trace": N * 4 * D + 2 * (L + G) * B * 8,
+    }
+    peak, kind = measured_peak()
+    out = {"bound": "hbm", "peak": peak, "peak_source": f"{kind} hbm_gbs", "unit": "GB/s",
+           "kernels": {}}
+    for name, (tot_ms, launches) in kern.items():
+        if name == "pcg_kernel":
+            nbytes = pcg_its * (12 * S.nnz + 8 * (L + 1) + 72 * L * B)
+        elif name in per_launch:
+            nbytes = launches * per_launch[name]
+        else:
+            continue
+        gbs = nbytes / (tot_ms / 1e3) / 1e9
+        out["kernels"][name] = {"launches": launches, "ms": round(tot_ms, 3),
+                                "bytes": int(nbytes), "achieved_gbs": round(gbs, 1),
+                                "frac": round(gbs / peak, 4)}
+    if "pcg_kernel" in out["kernels"]:
+        out["kernels"]["pcg_kernel"]["iterations"] = int(pcg_its)
+    dom = max(out["kernels"], key=lambda k: out["kernels"][k]["ms"])
+    out.update(kernel=dom, achieved=out["kernels"][dom]["achieved_gbs"],
+               frac=out["kernels"][dom]["frac"])
     return out
 
 
