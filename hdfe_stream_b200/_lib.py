@@ -19,7 +19,7 @@ HDFE_ERR_WORKSPACE = 4
 HDFE_ERR_BAD_CODE = 5
 HDFE_ERR_CAPACITY = 6
 PCG_MAX_K = 32          # HDFE_PCG_MAX_K
-PCG_MIXED_MAX_K = 8     # HDFE_PCG_MIXED_MAX_K
+PCG_MIXED_MAX_K = 32    # HDFE_PCG_MIXED_MAX_K
 
 _c = ctypes
 _vp = _c.c_void_p

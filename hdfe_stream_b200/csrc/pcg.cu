@@ -832,18 +832,17 @@ struct LaneArgs {
     int32_t k;      // the caller's columns (B, X0, X have stride k)
 };
 
-// vr = V[r, lane] (lanes < K), loaded when row r began
-template <int K>
+// vr = V[r, lane] (lanes < K), loaded when row r began; p'Ap in FP64
+template <int K, typename T>
 __device__ __forceinline__ void lane_flush(int64_t r, int64_t st, int64_t en, int64_t lo,
-                                           int64_t hi, int64_t gw, double acc, double vr,
-                                           double *out, double *carry, double &dot,
-                                           bool want_dot)
+                                           int64_t hi, int64_t gw, T acc, T vr, T *out, T *carry,
+                                           double &dot, bool want_dot)
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int o = K; o < 32; o <<= 1) acc += __shfl_xor_sync(kFull, acc, o);
     if (lane < K) {
-        if (want_dot) dot += vr * acc;
+        if (want_dot) dot += (double)vr * (double)acc;
         if (st >= lo && en <= hi)
             out[r * K + lane] = acc;
         else    // cut row: slot 1 in the warp where it starts, 0 elsewhere
@@ -856,21 +855,36 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+// one element of T (8-byte double or 4-byte float) from global to shared memory
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem)
+{
+    if constexpr (sizeof(T) == 8) cp_async8(smem, gmem);
+    else cp_async4(smem, gmem);
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // out = S V over this warp's range of nonzeros (rows inside the range); cut
-// rows to the carry slots; dot += V[r, col] (S V)[r, col] in lanes < K.
+// rows to the carry slots; dot += V[r, col] (S V)[r, col] in lanes < K.  T is
+// the arithmetic of the product: FP64 (S's values `mvals`, V, out, carry and
+// the accumulators in double) or FP32 (S's values as floats and FP32
+// vectors, the accumulators in float); dot is FP64 either way.
 // The gathers go through shared memory: for each window of 32 nonzeros the
 // warp issues asynchronous copies (cp.async) of the 32 rows of V it needs,
 // lane (sub, col) copying column col of the rows it will itself multiply,
 // plus the window's matrix values, and keeps kLaneStages windows in flight,
 // so the bytes in flight per SM do not depend on registers.  Row walk and
 // flushes as described above; V[r] for p'Ap is loaded as row r begins.
-template <int K>
-__device__ void lane_spmm(const Params &a, const double *__restrict__ V, double *__restrict__ out,
-                          double *carry, double &dot, bool want_dot, double *stage)
+template <int K, typename T>
+__device__ void lane_spmm(const Params &a, const T *__restrict__ mvals, const T *__restrict__ V,
+                          T *__restrict__ out, T *carry, double &dot, bool want_dot, T *stage)
 {
     constexpr int H = 32 / K, NS = kLaneStages;
     const int lane = threadIdx.x & 31, col = lane % K, sub = lane / K;
@@ -878,8 +892,8 @@ __device__ void lane_spmm(const Params &a, const double *__restrict__ V, double 
     const int64_t lo = a.wlo[gw];
     const int64_t hi = a.wlo[gw + 1];
     if (lo >= hi) return;
-    double *vals = stage;                   // [NS][32][K]
-    double *wts = stage + NS * 32 * K;      // [NS][32]
+    T *vals = stage;                        // [NS][32][K]
+    T *wts = stage + NS * 32 * K;           // [NS][32]
     const int64_t nwin = (hi - lo + 31) / 32;
     auto load_idx = [&](int64_t w) -> int32_t {
         const int64_t e = lo + w * 32 + lane;
@@ -895,14 +909,14 @@ __device__ void lane_spmm(const Params &a, const double *__restrict__ V, double 
             const int sgi = (int)(w % NS);
             const int64_t base = lo + w * 32;
             const int n = (int)min((int64_t)32, hi - base);
-            double *vs = vals + sgi * 32 * K;
+            T *vs = vals + sgi * 32 * K;
 #pragma unroll
             for (int u = 0; u < K; u++) {
                 const int t = u * H + sub;
                 const int cc = __shfl_sync(kFull, c, t);
-                if (t < n) cp_async8(vs + t * K + col, V + (int64_t)cc * K + col);
+                if (t < n) cp_async_elem<T>(vs + t * K + col, V + (int64_t)cc * K + col);
             }
-            if (lane < n) cp_async8(wts + sgi * 32 + lane, a.data + base + lane);
+            if (lane < n) cp_async_elem<T>(wts + sgi * 32 + lane, mvals + base + lane);
         }
         cp_async_commit();                      // one group per window, empty past the end
     };
@@ -918,8 +932,8 @@ __device__ void lane_spmm(const Params &a, const double *__restrict__ V, double 
     int64_t rw = r;     // row-end window: lane i holds indptr[rw + 1 + i]
     int64_t rend = rw + 1 + lane <= a.L ? a.indptr[rw + 1 + lane] : INT64_MAX;
     int64_t en = __shfl_sync(kFull, rend, 0);
-    double vr = want_dot ? V[r * K + col] : 0.0;
-    double acc = 0.0;
+    T vr = want_dot ? V[r * K + col] : T(0);
+    T acc = T(0);
     for (int64_t w = 0; w < nwin; w++) {
         {
             const int32_t c = cnext;
@@ -930,16 +944,16 @@ __device__ void lane_spmm(const Params &a, const double *__restrict__ V, double 
         __syncwarp();                   // ... and every lane's (the values)
         const int sgi = (int)(w % NS);
         const int64_t base = lo + w * 32;
-        const double *vs = vals + sgi * 32 * K;
-        const double *ws = wts + sgi * 32;
+        const T *vs = vals + sgi * 32 * K;
+        const T *ws = wts + sgi * 32;
 #pragma unroll 8
         for (int u = 0; u < K; u++) {
             const int64_t sb = base + u * H;             // this step's first nonzero
             if (sb >= hi) break;
             const int t = u * H + sub;
             const bool valid = sb + sub < hi;
-            const double g = valid ? vs[t * K + col] : 0.0;
-            const double wv = valid ? ws[t] : 0.0;
+            const T g = valid ? vs[t * K + col] : T(0);
+            const T wv = valid ? ws[t] : T(0);
             if (sb + H <= en) {                          // the whole step in row r
                 acc += wv * g;
                 continue;
@@ -948,8 +962,8 @@ __device__ void lane_spmm(const Params &a, const double *__restrict__ V, double 
                 const int64_t el = sb + h;
                 if (el >= hi) break;
                 while (el >= en) {                       // rows ending before el (empty ones too)
-                    lane_flush<K>(r, st, en, lo, hi, gw, acc, vr, out, carry, dot, want_dot);
-                    acc = 0.0;
+                    lane_flush<K, T>(r, st, en, lo, hi, gw, acc, vr, out, carry, dot, want_dot);
+                    acc = T(0);
                     r++;
                     st = en;
                     if (want_dot) vr = V[r * K + col];
@@ -965,14 +979,14 @@ __device__ void lane_spmm(const Params &a, const double *__restrict__ V, double 
         __syncwarp();                   // every lane is done with this stage before it is refilled
     }
     cp_async_wait<0>();
-    lane_flush<K>(r, st, en, lo, hi, gw, acc, vr, out, carry, dot, want_dot);
+    lane_flush<K, T>(r, st, en, lo, hi, gw, acc, vr, out, carry, dot, want_dot);
 }
 
 // The cut row this warp finishes (its first row, when that row started in an
 // earlier warp and ends in this one): the carry slots of the warps it spans
 // summed in warp order, lane col holding column col.
-template <int K>
-__device__ bool lane_finish_cut(const Params &a, const double *carry, int64_t &row, double &ap)
+template <int K, typename T = double>
+__device__ bool lane_finish_cut(const Params &a, const T *carry, int64_t &row, T &ap)
 {
     const int col = (threadIdx.x & 31) % K;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -983,7 +997,7 @@ __device__ bool lane_finish_cut(const Params &a, const double *carry, int64_t &r
     const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
     if (!(rs < lo && re <= hi)) return false;
     const int64_t w0 = warp_of(a, rs);
-    double s = 0.0;
+    T s = T(0);
     for (int64_t w = w0; w <= gw; w++)
         if (a.wlo[w] != a.wlo[w + 1]) s += __ldcg(carry + (w * 2 + (w == w0 ? 1 : 0)) * K + col);
     ap = s;
@@ -1054,7 +1068,7 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
         for (int64_t t = gtid; t < LK; t += gstride)
             Xw[t] = zero_c ? 0.0 : a.X0[(t / K) * kc + col];
         if (!gb.sync()) return;
-        lane_spmm<K>(a, Xw, a.AP, a.carry, dot, false, stage);
+        lane_spmm<K, double>(a, a.data, Xw, a.AP, a.carry, dot, false, stage);
         if (!gb.sync()) return;
     }
     double rel_c = 0.0, rz_c, bnorm_c;
@@ -1110,7 +1124,7 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
         for (it = 1; it <= a.maxiter; it++) {
             // ---- A: AP = S P, p'Ap
             dot = 0.0;
-            lane_spmm<K>(a, a.P, a.AP, a.carry, dot, true, stage);
+            lane_spmm<K, double>(a, a.data, a.P, a.AP, a.carry, dot, true, stage);
             {
                 double v[1] = {dot};
                 column_partials<K, 1>(v, s_scratch, a.part, 0, nb);
@@ -1231,7 +1245,9 @@ int lane_grid()
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel<K>, lane_threads(K),
                                                       lane_smem_bytes(K)) != cudaSuccess)
         return -1;
-    return per_sm < 1 ? -1 : sms;
+    // one CTA per SM, at most as many as reduce_range sums (32 lanes x
+    // kRedLoads partials each): a larger part runs fewer CTAs than SMs
+    return per_sm < 1 ? -1 : (sms < 32 * kRedLoads ? sms : 32 * kRedLoads);
 }
 
 int lane_grid_for(int kw)
@@ -1744,6 +1760,305 @@ __global__ void __launch_bounds__(threads_for(K), 1) mixed_kernel(Params a, Mixe
     }
 }
 
+// ------------------------------------------- mixed precision, wide blocks
+//
+// The refined solve for blocks of 5 to 32 columns (the JLA's probe blocks),
+// one column per lane as in lane_kernel: the FP64 residual B - S X uses S's
+// FP64 values and the FP64 iterate; the inner PCG runs on S's FP32 values and
+// FP32 vectors R, P, AP, D with FP32 products and updates (p'Ap, the norms and
+// r'z accumulated in FP64); X += D in FP64.  Per inner iteration the bytes are
+// S's 8 per nonzero and 4 per vector element instead of 12 and 8.
+struct MixedLane {
+    const float *data32;
+    float *R, *P, *AP, *D;
+    double *AX;                 // S X, then the FP64 residual
+    double inner_tol;
+};
+
+struct MixedLaneLayout {
+    int64_t r, p, ap, d, ax, x, carry, part, wfirst, wlo, cut, bar, total;
+};
+
+inline MixedLaneLayout mixed_lane_layout(int64_t L, int k, int64_t blocks)
+{
+    MixedLaneLayout o;
+    const int kw = lane_width(k);
+    const int64_t warps = blocks * (lane_threads(kw) / 32);
+    int64_t p = 0;
+    auto take = [&](int64_t bytes) { int64_t at = p; p += (bytes + 255) / 256 * 256; return at; };
+    o.r = take(L * kw * 4);
+    o.p = take(L * kw * 4);
+    o.ap = take(L * kw * 4);
+    o.d = take(L * kw * 4);
+    o.ax = take(L * kw * 8);
+    o.x = k == kw ? -1 : take(L * kw * 8);
+    o.carry = take(warps * 2 * kw * 8);
+    o.part = take(3 * (int64_t)kw * blocks * 8);
+    o.wfirst = take(warps * 8);
+    o.wlo = take((warps + 1) * 8);
+    o.cut = take(L);
+    o.bar = take(64);
+    o.total = p;
+    return o;
+}
+
+template <int K>
+__global__ void __launch_bounds__(lane_threads(K), 1) mixed_lane_kernel(Params a, LaneArgs x,
+                                                                        MixedLane f)
+{
+    constexpr int RU = lane_ru(K);
+    extern __shared__ double s_stage[];
+    __shared__ double s_red[3 * K];
+    __shared__ double s_scratch[(lane_threads(K) / 32) * 3 * K];
+    __shared__ double s_rel[K];
+    __shared__ int s_active[K];
+    GridBarrier gb{a.bar};
+    const int lane = threadIdx.x & 31, col = lane % K;
+    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t L = a.L, LK = a.L * K;
+    const int nb = gridDim.x;
+    const int kc = x.k;
+    double *Xw = x.Xw;
+    const bool zero_c = col >= kc || (a.zero != nullptr && a.zero[col] != 0);
+    double *stage = s_stage + (threadIdx.x >> 5) * kLaneStages * 32 * (K + 1);
+    float *stage32 = reinterpret_cast<float *>(stage);
+    float *carry32 = reinterpret_cast<float *>(a.carry);
+
+    // ---- set-up: each warp's first row, the cut flags, X = X0 (or 0), ||B||
+    {
+        const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        const int64_t lo = a.wlo[gw];
+        if (lane == 0 && lo < a.nnz) a.wfirst[gw] = upper_bound(a.indptr, L + 1, lo) - 1;
+        __syncwarp();
+        for (int64_t r = gtid; r < L; r += gstride) {
+            const int64_t rs = a.indptr[r], re = a.indptr[r + 1];
+            a.cut[r] = (re > rs && warp_of(a, rs) != warp_of(a, re - 1) ? kRowCut : 0) |
+                       (re == rs ? kRowEmpty : 0);
+        }
+    }
+    double bnorm_c;
+    {
+        double v[1] = {0.0};
+        for (int64_t t = gtid; t < LK; t += gstride) {
+            const int64_t r = t / K;
+            const double b = col < kc ? a.B[r * kc + col] : 0.0;
+            v[0] += b * b;
+            Xw[t] = (a.X0 != nullptr && !zero_c) ? a.X0[r * kc + col] : 0.0;
+        }
+        column_partials<K, 1>(v, s_scratch, a.part, 0, nb);
+        if (!gb.sync()) return;
+        reduce_range(a.part, 0, K, s_red);
+        const double bn = sqrt(s_red[col]);
+        bnorm_c = bn == 0.0 ? 1.0 : bn;
+    }
+    int64_t total = 0;
+    double rel_c = 0.0;
+    bool active_c = false;
+    for (int64_t outer = 0;; outer++) {
+        // ---- the FP64 residual B - S X (into AX), its norm
+        const bool have_x = outer > 0 || a.X0 != nullptr;
+        double dot = 0.0;
+        if (have_x) {
+            lane_spmm<K, double>(a, a.data, Xw, f.AX, a.carry, dot, false, stage);
+            if (!gb.sync()) return;
+        }
+        double v1[1] = {0.0};
+        auto resid = [&](int64_t r, double ax) {
+            const int64_t t = r * K + col;
+            const double res = zero_c ? 0.0 : a.B[r * kc + col] - ax;
+            f.AX[t] = res;
+            v1[0] += res * res;
+        };
+        for (int64_t t = gtid; t < LK; t += gstride) {
+            const int64_t r = t / K;
+            const uint8_t fl = a.cut[r];
+            if (have_x && (fl & kRowCut)) continue;
+            resid(r, (have_x && !(fl & kRowEmpty)) ? f.AX[t] : 0.0);
+        }
+        if (have_x) {
+            int64_t r;
+            double ap;
+            if (lane_finish_cut<K, double>(a, a.carry, r, ap) && lane < K) resid(r, ap);
+        }
+        column_partials<K, 1>(v1, s_scratch, a.part, 1, nb);
+        if (!gb.sync()) return;
+        reduce_range(a.part, K, 2 * K, s_red);
+        const double rnorm_c = sqrt(s_red[K + col]);
+        rel_c = rnorm_c / bnorm_c;
+        active_c = !zero_c && rel_c > a.tol;
+        if (threadIdx.x < K) {
+            s_rel[col] = zero_c ? 0.0 : rel_c;
+            s_active[col] = active_c ? 1 : 0;
+        }
+        if (!__syncthreads_or(active_c) || total >= a.maxiter) break;
+        // ---- inner FP32 PCG on S D = R: R, D = 0, P = dinv R, r'z
+        double rz_c;
+        {
+            double v[1] = {0.0};
+            for (int64_t t = gtid; t < LK; t += gstride) {
+                const float di = (float)a.dinv[t / K];
+                const float res = active_c ? (float)f.AX[t] : 0.0f;
+                f.R[t] = res;
+                f.D[t] = 0.0f;
+                const float z = res * di;
+                f.P[t] = z;
+                v[0] += (double)res * (double)z;
+            }
+            column_partials<K, 1>(v, s_scratch, a.part, 2, nb);
+            if (!gb.sync()) return;
+            reduce_range(a.part, 2 * K, 3 * K, s_red);
+            rz_c = s_red[2 * K + col];
+        }
+        bool inner_c = active_c;
+        while (total < a.maxiter) {
+            total++;
+            // A: AP = S P in FP32, p'Ap in FP64
+            dot = 0.0;
+            lane_spmm<K, float>(a, f.data32, f.P, f.AP, carry32, dot, true, stage32);
+            {
+                double v[1] = {dot};
+                column_partials<K, 1>(v, s_scratch, a.part, 0, nb);
+            }
+            if (!gb.sync()) return;
+            reduce_range(a.part, 0, K, s_red);
+            const double pap = s_red[col];
+            const float alpha = (inner_c && pap > 0.0) ? (float)(rz_c / pap) : 0.0f;
+            // B: D += alpha P, R -= alpha AP; sums of R^2 and R^2 dinv in FP64
+            double v[2] = {0.0, 0.0};
+            auto step = [&](int64_t r, float ap) {
+                const double di = a.dinv[r];
+                const int64_t t = r * K + col;
+                f.D[t] += alpha * f.P[t];
+                const float res = f.R[t] - alpha * ap;
+                f.R[t] = res;
+                const double rd = (double)res;
+                v[0] += rd * rd;
+                v[1] += rd * rd * di;
+            };
+            for (int64_t t0 = gtid; t0 < LK; t0 += RU * gstride) {
+                uint8_t fl[RU];
+                float ap[RU], pv[RU], dv[RU], rv[RU];
+                double di[RU];
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    const int64_t t = t0 + u * gstride;
+                    fl[u] = kRowCut;
+                    if (t < LK) {
+                        const int64_t r = t / K;
+                        fl[u] = a.cut[r];
+                        ap[u] = f.AP[t];
+                        pv[u] = f.P[t];
+                        dv[u] = f.D[t];
+                        rv[u] = f.R[t];
+                        di[u] = a.dinv[r];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    if (fl[u] & kRowCut) continue;      // also the slots past the end
+                    const int64_t t = t0 + u * gstride;
+                    f.D[t] = dv[u] + alpha * pv[u];
+                    const float res = rv[u] - alpha * ((fl[u] & kRowEmpty) ? 0.0f : ap[u]);
+                    f.R[t] = res;
+                    const double rd = (double)res;
+                    v[0] += rd * rd;
+                    v[1] += rd * rd * di[u];
+                }
+            }
+            {
+                int64_t r;
+                float ap;
+                if (lane_finish_cut<K, float>(a, carry32, r, ap) && lane < K) step(r, ap);
+            }
+            column_partials<K, 2>(v, s_scratch, a.part, 1, nb);
+            if (!gb.sync()) return;
+            reduce_range(a.part, K, 3 * K, s_red);
+            // C: inner convergence, beta, P = dinv R + beta P
+            inner_c = inner_c && sqrt(s_red[K + col]) > f.inner_tol * rnorm_c;
+            if (!__syncthreads_or(inner_c)) break;
+            const double rzn = s_red[2 * K + col];
+            const float beta = inner_c ? (float)(rzn / (rz_c != 0.0 ? rz_c : 1.0)) : 0.0f;
+            rz_c = rzn;
+            for (int64_t t0 = gtid; t0 < LK; t0 += RU * gstride) {
+                float rv[RU], pv[RU], di[RU];
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    const int64_t t = t0 + u * gstride;
+                    if (t < LK) {
+                        rv[u] = f.R[t];
+                        pv[u] = f.P[t];
+                        di[u] = (float)a.dinv[t / K];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < RU; u++) {
+                    const int64_t t = t0 + u * gstride;
+                    if (t < LK) f.P[t] = rv[u] * di[u] + beta * pv[u];
+                }
+            }
+            if (!gb.sync()) return;
+        }
+        // ---- X += D in FP64, then a barrier before the next product reads X
+        for (int64_t t = gtid; t < LK; t += gstride)
+            if (active_c) Xw[t] += (double)f.D[t];
+        if (!gb.sync()) return;
+    }
+    // ---- the iterate to the caller's X (stride k)
+    if (Xw != a.X) {
+        for (int64_t t = gtid; t < LK; t += gstride)
+            if (col < kc) a.X[(t / K) * kc + col] = Xw[t];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double mx = 0.0;
+        bool conv = true;
+        for (int c = 0; c < kc; c++) {
+            mx = fmax(mx, s_rel[c]);
+            conv &= s_active[c] == 0;
+        }
+        a.info->iterations = total;
+        a.info->converged = conv ? 1 : 0;
+        a.info->status = HDFE_OK;
+        a.info->max_rel = mx;
+    }
+}
+
+template <int K>
+int mixed_lane_grid()
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+    if (cudaFuncSetAttribute(mixed_lane_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             lane_smem_bytes(K)) != cudaSuccess)
+        return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_lane_kernel<K>,
+                                                      lane_threads(K), lane_smem_bytes(K)) !=
+        cudaSuccess)
+        return -1;
+    return per_sm < 1 ? -1 : (sms < 32 * kRedLoads ? sms : 32 * kRedLoads);
+}
+
+int mixed_lane_grid_for(int kw)
+{
+    static int cache[64][3] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    const int i = kw == 8 ? 0 : (kw == 16 ? 1 : 2);
+    if (cache[dev][i] == 0)
+        cache[dev][i] = kw == 8 ? mixed_lane_grid<8>()
+                                : (kw == 16 ? mixed_lane_grid<16>() : mixed_lane_grid<32>());
+    return cache[dev][i];
+}
+
+template <int K>
+cudaError_t launch_mixed_lanes(Params p, LaneArgs x, MixedLane m, int blocks, cudaStream_t s)
+{
+    void *args[] = {&p, &x, &m};
+    return cudaLaunchCooperativeKernel((const void *)mixed_lane_kernel<K>, dim3(blocks),
+                                       dim3(lane_threads(K)), args, lane_smem_bytes(K), s);
+}
+
 template <int K>
 int mixed_grid()
 {
@@ -1758,8 +2073,9 @@ int mixed_grid()
 
 int mixed_grid_for(int k)
 {
-    static int cache[64][HDFE_PCG_MIXED_MAX_K + 1] = {};
+    static int cache[64][5] = {};
     int dev = 0;
+    if (k < 1 || k > 4) return -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
     if (cache[dev][k] == 0) {
         switch (k) {
@@ -1767,10 +2083,6 @@ int mixed_grid_for(int k)
         case 2: cache[dev][k] = mixed_grid<2>(); break;
         case 3: cache[dev][k] = mixed_grid<3>(); break;
         case 4: cache[dev][k] = mixed_grid<4>(); break;
-        case 5: cache[dev][k] = mixed_grid<5>(); break;
-        case 6: cache[dev][k] = mixed_grid<6>(); break;
-        case 7: cache[dev][k] = mixed_grid<7>(); break;
-        case 8: cache[dev][k] = mixed_grid<8>(); break;
         default: return -1;
         }
     }
@@ -1792,10 +2104,78 @@ extern "C" int64_t hdfe_pcg_mixed_workspace_bytes(int64_t L, int64_t nnz, int32_
 {
     (void)nnz;
     if (k < 1 || k > HDFE_PCG_MIXED_MAX_K || L < 0) return -1;
+    if (pcg::use_lanes(k)) {
+        const int blocks = pcg::mixed_lane_grid_for(pcg::lane_width(k));
+        return blocks < 1 ? -1 : pcg::mixed_lane_layout(L, k, blocks).total;
+    }
     const int blocks = pcg::mixed_grid_for(k);
     if (blocks < 1) return -1;
     return pcg::mixed_layout(L, k, blocks).total;
 }
+
+namespace hdfe {
+namespace pcg {
+
+int solve_mixed_lanes(const int64_t *indptr, const int32_t *indices, const double *data,
+                      const float *data32, int64_t L, int64_t nnz, const double *dinv,
+                      const double *B, int32_t k, const uint8_t *zero, const double *X0,
+                      double tol, double inner_tol, int64_t maxiter, double *X, void *workspace,
+                      int64_t workspace_bytes, hdfe_pcg_info *info, cudaStream_t s)
+{
+    const int kw = lane_width(k);
+    const int blocks = mixed_lane_grid_for(kw);
+    if (blocks < 1) return hdfe_set_cuda_error(cudaGetLastError());
+    const MixedLaneLayout lay = mixed_lane_layout(L, k, blocks);
+    if (workspace_bytes < lay.total)
+        return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_pcg_solve_mixed: workspace too small");
+    char *ws = (char *)workspace;
+    Params p{};
+    p.indptr = indptr;
+    p.indices = indices;
+    p.data = data;
+    p.L = L;
+    p.nnz = nnz;
+    p.nwarps = (int64_t)blocks * (lane_threads(kw) / 32);
+    p.dinv = dinv;
+    p.B = B;
+    p.zero = zero;
+    p.X0 = X0;
+    p.tol = tol;
+    p.maxiter = maxiter;
+    p.X = X;
+    p.carry = (double *)(ws + lay.carry);
+    p.part = (double *)(ws + lay.part);
+    p.wfirst = (int64_t *)(ws + lay.wfirst);
+    p.wlo = (int64_t *)(ws + lay.wlo);
+    p.cut = (uint8_t *)(ws + lay.cut);
+    p.bar = (unsigned *)(ws + lay.bar);
+    p.info = info;
+    LaneArgs x;
+    x.Xw = lay.x < 0 ? X : (double *)(ws + lay.x);
+    x.k = k;
+    MixedLane m;
+    m.data32 = data32;
+    m.R = (float *)(ws + lay.r);
+    m.P = (float *)(ws + lay.p);
+    m.AP = (float *)(ws + lay.ap);
+    m.D = (float *)(ws + lay.d);
+    m.AX = (double *)(ws + lay.ax);
+    m.inner_tol = inner_tol;
+    HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
+    k_partition<<<(unsigned)((p.nwarps + 256) / 256), 256, 0, s>>>(indptr, L, nnz, p.nwarps, 0,
+                                                                   (int64_t *)p.wlo);
+    cudaError_t e = kw == 8 ? launch_mixed_lanes<8>(p, x, m, blocks, s)
+                  : kw == 16 ? launch_mixed_lanes<16>(p, x, m, blocks, s)
+                             : launch_mixed_lanes<32>(p, x, m, blocks, s);
+    HDFE_CUDA_TRY(e);
+    pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);
+    HDFE_CUDA_TRY(cudaGetLastError());
+    hdfe_add_launches(3);
+    return HDFE_OK;
+}
+
+}  // namespace pcg
+}  // namespace hdfe
 
 extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indices,
                                     const double *data, const float *data32, int64_t L,
@@ -1812,6 +2192,10 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
     if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
         return hdfe_set_arg_error("hdfe_pcg_solve_mixed: workspace must be 256-byte aligned");
     cudaStream_t s = (cudaStream_t)stream;
+    if (pcg::use_lanes(k))
+        return pcg::solve_mixed_lanes(indptr, indices, data, data32, L, nnz, dinv, B, k, zero, X0,
+                                      tol, inner_tol, maxiter, X, workspace, workspace_bytes, info,
+                                      s);
     const int blocks = pcg::mixed_grid_for(k);
     if (blocks < 1) return hdfe_set_cuda_error(cudaGetLastError());
     const pcg::MixedLayout lay = pcg::mixed_layout(L, k, blocks);
@@ -1857,10 +2241,6 @@ extern "C" int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indice
     case 2: e = pcg::launch_mixed<2>(p, m, blocks, s); break;
     case 3: e = pcg::launch_mixed<3>(p, m, blocks, s); break;
     case 4: e = pcg::launch_mixed<4>(p, m, blocks, s); break;
-    case 5: e = pcg::launch_mixed<5>(p, m, blocks, s); break;
-    case 6: e = pcg::launch_mixed<6>(p, m, blocks, s); break;
-    case 7: e = pcg::launch_mixed<7>(p, m, blocks, s); break;
-    case 8: e = pcg::launch_mixed<8>(p, m, blocks, s); break;
     }
     HDFE_CUDA_TRY(e);
     pcg::pcg_status_kernel<<<1, 32, 0, s>>>(p.bar, info);

@@ -504,8 +504,10 @@ typedef struct hdfe_pcg_info {
  * pass over S per iteration. */
 #define HDFE_PCG_MAX_K 32
 
-/* Largest k hdfe_pcg_solve_mixed accepts. */
-#define HDFE_PCG_MIXED_MAX_K 8
+/* Largest k hdfe_pcg_solve_mixed accepts: blocks of up to 4 columns keep a
+ * row's k values in one thread's registers, wider ones run one column per
+ * lane (padded to 8, 16 or 32), as hdfe_pcg_solve does. */
+#define HDFE_PCG_MIXED_MAX_K 32
 
 /* Device workspace bytes hdfe_pcg_solve needs (for the current device). */
 int64_t hdfe_pcg_workspace_bytes(int64_t L, int64_t nnz, int32_t k);
@@ -551,7 +553,9 @@ int hdfe_pcg_solve_mixed(const int64_t *indptr, const int32_t *indices, const do
  * (hdfe_pcg_workspace_bytes(L, nnz, k) > HDFE_PCG_NOALLOC_BYTES; about
  * L * k <= 600,000 values) are rejected with HDFE_ERR_WORKSPACE.  The first
  * call on a device looks up the array's device address (cudaGetSymbolAddress)
- * with that device current, so make it before any stream capture.  Every
+ * with that device current, so make it before any stream capture.  That
+ * address is cached for the library's lifetime: do not reset the device
+ * (cudaDeviceReset) or re-create its primary context between calls.  Every
  * call shares the one array: calls that overlap on the GPU (other streams,
  * other host threads) race and corrupt each other; serialise them.  Nothing
  * in the array needs clearing between calls: each solve rewrites what it

@@ -170,8 +170,11 @@ def test_mixed_precision_matches_fp64(device, name):
         assert np.max(np.abs(dSX)) < 1e-8 * np.max(np.abs(g["pcg_b"]))
 
 
-@pytest.mark.parametrize("k", [1, 3, 8])
+@pytest.mark.parametrize("k", [1, 3, 8, 13, 32])
 def test_mixed_precision_widths(device, k):
+    """The refined solve at register widths (1, 3) and one column per lane
+    (8, 13 padded to 16, 32), with a zero column and a warm start for the
+    wide ones, against the FP64 oracle at 1e-13."""
     from hdfe_stream_b200 import gpu
     from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
     rows = pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(8, 8), p_move=0.1, seed=9))
@@ -179,12 +182,22 @@ def test_mixed_precision_widths(device, k):
     S = orc.build_explicit(c)
     rng = np.random.default_rng(k)
     b = orc.csr_matmat(S, rng.standard_normal((c.L, k)))
-    X_ref, *_ = orc.pcg(S, orc.jacobi(c.diag), b, None, None, 1e-13)
-    solve = gpu.BlockSolver(gpu.DeviceCSR.from_host(*S), orc.jacobi(c.diag), 1e-10, 5000,
-                            precision="mixed")
-    X, it, ok, rel = solve(b)
+    zero = np.zeros(k, bool)
+    if k > 4:
+        b[:, 2] = 0.0
+        zero[2] = True
+    dinv = orc.jacobi(c.diag)
+    X_ref, *_ = orc.pcg(S, dinv, b, zero, None, 1e-13)
+    solve = gpu.BlockSolver(gpu.DeviceCSR.from_host(*S), dinv, 1e-10, 5000, precision="mixed")
+    X, it, ok, rel = solve(b, zero)
     assert ok and rel <= 1e-10
     assert np.max(np.abs(orc.csr_matmat(S, X - X_ref))) < 1e-8 * np.max(np.abs(b))
+    if k > 4:
+        assert np.all(X[:, 2] == 0.0)
+        x0 = X_ref + 1e-3 * rng.standard_normal(X_ref.shape)
+        X2, it2, ok2, rel2 = solve(b, zero, x0)
+        assert ok2 and rel2 <= 1e-10 and it2 < it
+        assert np.max(np.abs(orc.csr_matmat(S, X2 - X_ref))) < 1e-8 * np.max(np.abs(b))
 
 
 def test_mixed_precision_maxiter(device):
