@@ -20,6 +20,7 @@ HDFE_ERR_BAD_CODE = 5
 HDFE_ERR_CAPACITY = 6
 PCG_MAX_K = 32          # HDFE_PCG_MAX_K
 PCG_MIXED_MAX_K = 32    # HDFE_PCG_MIXED_MAX_K
+GRAM_MAX_COLS = 128     # HDFE_GRAM_MAX_COLS
 
 _c = ctypes
 _vp = _c.c_void_p
@@ -77,6 +78,8 @@ SIGNATURES = {
     "hdfe_row_effects": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _i32, _i64, _vp,
                                     _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_kss_sigma2": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _f64, _i64, _vp, _vp]),
+    "hdfe_gram_workspace_bytes": (_i64, [_i64, _i32]),
+    "hdfe_gram_bf16x3": (_c.c_int, [_vp, _i64, _i32, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_solver_create": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _f64, _i64, _i32, _vp]),
     "hdfe_solver_solve": (_c.c_int, [_vp, _vp, _i32, _vp, _vp, _vp, _vp, _vp]),
     "hdfe_solver_destroy": (_c.c_int, [_vp]),

@@ -567,6 +567,25 @@ int hdfe_pcg_solve_noalloc(const int64_t *indptr, const int32_t *indices, const 
                            int32_t k, const uint8_t *zero, const double *X0, double tol,
                            int64_t maxiter, double *X, hdfe_pcg_info *info, void *stream);
 
+/* ------------------------------------------- X' W X of a wide design
+ *
+ * core/inference.py:109-137 `_assemble` forms the design's cross-products
+ * V' W V with a BLAS product in FP64.  For wide designs this computes X' W X on
+ * the tensor cores: X (n_rows, c) row-major FP64, w (n_rows) or NULL, out
+ * (c, c) FP64.  Every value is split as x = hi + lo, hi = bf16(x), lo =
+ * bf16(x - hi) (rows scaled by sqrt(w)), and hi hi' + hi lo' + lo hi' is
+ * accumulated in FP32 by tcgen05.mma per CTA over chunks of 64 rows, the CTAs'
+ * partials summed in FP64: about 1e-5 relative accuracy per entry.  c <=
+ * HDFE_GRAM_MAX_COLS.  The first 16 bytes of the workspace hold a status word
+ * (HDFE_OK, or HDFE_ERR_SPIN_LIMIT if a wait on the tensor core timed out),
+ * readable once the stream has run the call.  An addition of this library. */
+#define HDFE_GRAM_MAX_COLS 128
+
+int64_t hdfe_gram_workspace_bytes(int64_t n_rows, int32_t c);
+
+int hdfe_gram_bf16x3(const double *X, int64_t n_rows, int32_t c, const double *w, double *out,
+                     void *workspace, int64_t workspace_bytes, void *stream);
+
 /* ------------------------------------------- the solver handle
  *
  * core/gpu.py:186-197 `explicit_solver(S, dinv, tol, maxiter)` returns a
