@@ -39,15 +39,13 @@
 namespace hdfe {
 namespace pcg {
 
-// One CTA per SM (fewer arrivals at each grid barrier).  Narrow blocks could
-// run 1024 threads (64 registers a thread); from HDFE_PCG_WIDE_K columns on, a
-// thread's K-wide accumulators, gathered rows and the S ring's state no longer
-// fit in 64 registers, so those blocks run 512 threads with up to 128
-// registers each instead of spilling to local memory.  With S streamed by the
-// ring the warps' loads of S no longer need the extra warps, so every width
-// runs 512 threads.
+// One CTA per SM (fewer arrivals at each grid barrier).  Narrow blocks run
+// 1024 threads (64 registers a thread: the most warps in flight); from
+// HDFE_PCG_WIDE_K columns on, a thread's K-wide accumulators and gathered
+// rows no longer fit in 64 registers, so those blocks run 512 threads with up
+// to 128 registers each instead of spilling to local memory.
 #ifndef HDFE_PCG_WIDE_K
-#define HDFE_PCG_WIDE_K 1
+#define HDFE_PCG_WIDE_K 3
 #endif
 __host__ __device__ constexpr int threads_for(int k) { return k >= HDFE_PCG_WIDE_K ? 512 : 1024; }
 constexpr int kMaxWarps = 32;
@@ -83,7 +81,6 @@ struct Params {
     uint8_t *cut;       // (L) row spans two or more warps
     unsigned *bar;
     hdfe_pcg_info *info;
-    int ring;           // stream S through the warps' shared-memory rings (pcg_kernel)
 };
 
 // Workspace layout in bytes: R (L*K), P (L*KP), AP (L*K), carry, part,
@@ -390,292 +387,6 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
     }
 }
 
-// ------------------------------------------------ S streamed by bulk copies
-//
-// The iteration's product reads S once, in order, warp by warp; its gathers of
-// P read L2.  When each lane loads its own indices and values, a round of
-// nonzeros costs two dependent round trips (the index from DRAM, then the
-// gather), and too few bytes of S are in flight to keep HBM busy.  Here each
-// warp streams its range of S through a ring of kRingStages chunks of shared
-// memory, CH nonzeros each (indices and values), filled by 1-D bulk copies
-// (cp.async.bulk, this GPU's own memory, no multicast) that complete on one
-// mbarrier per stage; the copies for the chunks ahead are in flight while the
-// lanes gather and multiply, so the lanes only wait on L2.
-//   A chunk starts at a multiple of 4 nonzeros (16-byte aligned indices,
-// 32-byte aligned values) and holds a multiple of 4; the ring covers
-// [lo & ~3, min(round_up(hi, 4), nnz & ~3)).  Elements outside it (the last
-// few of S when nnz is not a multiple of 4) are read from global memory.
-// Every wait on an mbarrier is bounded (kSpinLimitNs); a timeout records
-// HDFE_ERR_SPIN_LIMIT, waits (bounded again) for the warp's copies still in
-// flight and leaves the product; the next grid barrier then stops the kernel.
-constexpr int kRingStages = 3;
-
-__device__ __forceinline__ unsigned smem_u32(const void *p)
-{
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-
-template <int CH>
-struct Ring {
-    int32_t *sidx;          // [kRingStages][CH]
-    double *sval;           // [kRingStages][CH]
-    uint64_t *bars;         // [kRingStages]
-    const int32_t *gidx;
-    const double *gval;
-    int64_t base, cov_end, nch;     // ring elements [base, cov_end) in nch chunks
-    int64_t oldest, issued, landed; // chunk counters
-    unsigned *phase;                // per-stage wait parity bits (kept across calls)
-    uint64_t policy;
-    bool ok;
-
-    __device__ void issue(int64_t j)    // lane 0: chunk j into stage j % kRingStages
-    {
-        const int st = (int)(j % kRingStages);
-        const int64_t cs = base + j * CH;
-        const int64_t ce = min(cs + (int64_t)CH, cov_end);
-        const unsigned ni = (unsigned)(ce - cs) * 4u, nv = (unsigned)(ce - cs) * 8u;
-        const unsigned bar = smem_u32(bars + st);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                     :: "r"(bar), "r"(ni + nv) : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
-                     " [%0], [%1], %2, [%3], %4;"
-                     :: "r"(smem_u32(sidx + st * CH)), "l"(gidx + cs), "r"(ni), "r"(bar),
-                        "l"(policy) : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
-                     " [%0], [%1], %2, [%3], %4;"
-                     :: "r"(smem_u32(sval + st * CH)), "l"(gval + cs), "r"(nv), "r"(bar),
-                        "l"(policy) : "memory");
-    }
-
-    // every lane: wait for chunk `landed` (bounded), then count it
-    __device__ bool wait_next()
-    {
-        const int st = (int)(landed % kRingStages);
-        const unsigned parity = (*phase >> st) & 1u;
-        const unsigned bar = smem_u32(bars + st);
-        const unsigned long long t0 = global_ns();
-        for (;;) {
-            unsigned done;
-            asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;"
-                         " selp.u32 %0, 1, 0, p; }"
-                         : "=r"(done) : "r"(bar), "r"(parity) : "memory");
-            if (done) break;
-            if (global_ns() - t0 > kSpinLimitNs) return false;
-        }
-        *phase ^= 1u << st;
-        landed++;
-        return true;
-    }
-
-    __device__ void start(const Params &a, int64_t lo, int64_t hi, int32_t *si, double *sv,
-                          uint64_t *b, unsigned *ph)
-    {
-        sidx = si;
-        sval = sv;
-        bars = b;
-        phase = ph;
-        gidx = a.indices;
-        gval = a.data;
-        base = lo & ~int64_t(3);
-        cov_end = min((hi + 3) & ~int64_t(3), a.nnz & ~int64_t(3));
-        nch = cov_end > base ? (cov_end - base + CH - 1) / CH : 0;
-        oldest = issued = landed = 0;
-        ok = true;
-        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
-        if ((threadIdx.x & 31) == 0)
-            for (int64_t j = 0; j < nch && j < kRingStages; j++) issue(j);
-        issued = min(nch, (int64_t)kRingStages);
-        __syncwarp();
-    }
-
-    // the chunks holding elements up to e (clamped to the ring) have landed
-    __device__ void ensure(int64_t e)
-    {
-        e = min(e, cov_end - 1);
-        if (!ok || e < base) return;
-        const int64_t j = (e - base) / CH;
-        while (landed <= j) {
-            if (!wait_next()) { ok = false; return; }
-        }
-    }
-
-    // chunks wholly below e are done (every lane is past them): refill
-    __device__ void release(int64_t e)
-    {
-        if (!ok) return;
-        __syncwarp();
-        bool any = false;
-        while (oldest < landed && base + (oldest + 1) * CH <= e) {
-            if (issued < nch) {
-                if (!any) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                any = true;
-                if ((threadIdx.x & 31) == 0) issue(issued);
-                issued++;
-            }
-            oldest++;
-        }
-        __syncwarp();
-    }
-
-    // every chunk issued has landed (the ring's exit; bounded as well)
-    __device__ void drain()
-    {
-        while (landed < issued) {
-            if (!wait_next()) {
-                ok = false;
-                return;
-            }
-        }
-    }
-
-    __device__ __forceinline__ int32_t idx(int64_t e) const
-    {
-        if (e >= base && e < cov_end) {
-            const int64_t off = e - base;
-            return sidx[(int)((off / CH) % kRingStages) * CH + (int)(off % CH)];
-        }
-        return __ldcs(gidx + e);
-    }
-    __device__ __forceinline__ double val(int64_t e) const
-    {
-        if (e >= base && e < cov_end) {
-            const int64_t off = e - base;
-            return sval[(int)((off / CH) % kRingStages) * CH + (int)(off % CH)];
-        }
-        return __ldcs(gval + e);
-    }
-};
-
-// row_products with S's indices and values from the ring
-template <int K, int VS, int VW, int STEP, int CH>
-__device__ __forceinline__ void ring_products(const Params &a, const Ring<CH> &ring,
-                                              const double *V, int64_t e0, int64_t re,
-                                              double (&acc)[K])
-{
-    constexpr int U = K <= 2 ? 4 : (K <= 4 ? HDFE_PCG_UNROLL : 2);
-    for (; e0 < re; e0 += STEP * U) {
-        int64_t c[U];
-        double d[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const int64_t e = e0 + STEP * u;
-            c[u] = 0;
-            d[u] = 0.0;
-            if (e < re) {
-                c[u] = ring.idx(e);
-                d[u] = ring.val(e);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++)
-            if (c[u] < 0 || c[u] >= a.L) { GridBarrier{a.bar}.fail(HDFE_ERR_BAD_CODE); c[u] = 0; }
-        double g[U][K];
-#pragma unroll
-        for (int u = 0; u < U; u++) gather<K, VS, VW, double>(V, c[u], g[u]);
-#pragma unroll
-        for (int u = 0; u < U; u++)
-#pragma unroll
-            for (int k = 0; k < K; k++) acc[k] += d[u] * g[u][k];
-    }
-}
-
-// spmm_range (FP64, p'Ap accumulated) with S streamed through the ring;
-// `sidx`/`sval` are this warp's ring (kRingStages x CH), `bars` its
-// mbarriers, `phase` their parities across calls.  A long row's rounds go in
-// the ring's steps, a batch of short rows spans fewer than 4 kLong nonzeros.
-template <int K, int VS, int VW, int CH>
-__device__ void spmm_range_ring(const Params &a, const double *__restrict__ V,
-                                double *__restrict__ out, double *carry, double (&dot)[K],
-                                int32_t *sidx, double *sval, uint64_t *bars, unsigned *phase)
-{
-    // a step's span (a batch of 4 short rows, or a long row's round) must lie
-    // within the chunks the ring can hold beside the one it starts in
-    static_assert(4 * kLong <= (kRingStages - 1) * CH &&
-                  32 * HDFE_PCG_UNROLL <= (kRingStages - 1) * CH, "a step must fit the ring");
-    const int lane = threadIdx.x & 31, sub = lane >> 3, sl = lane & 7;
-    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int64_t lo = a.wlo[gw];
-    const int64_t hi = a.wlo[gw + 1];
-    if (lo >= hi) return;
-    Ring<CH> ring;
-    ring.start(a, lo, hi, sidx, sval, bars, phase);
-    int64_t r0 = a.wfirst[gw];
-    for (;;) {
-        const int64_t q = r0 + lane;
-        const int64_t st = q < a.L ? __ldg(a.indptr + q) : INT64_MAX;
-        const int64_t en = q < a.L ? __ldg(a.indptr + q + 1) : INT64_MAX;
-        const bool inr = st < hi;
-        const unsigned inmask = __ballot_sync(kFull, inr);
-        const int nrows = __popc(inmask);
-        if (nrows == 0) break;
-        const int64_t cs = max(st, lo), ce = min(en, hi);
-        const int len = inr ? (int)(ce - cs) : 0;
-        const unsigned longmask = __ballot_sync(kFull, inr && len >= kLong);
-        int j = 0;
-        while (j < nrows) {
-            if ((longmask >> j) & 1u) {
-                const int64_t rs = __shfl_sync(kFull, cs, j), re = __shfl_sync(kFull, ce, j);
-                double vrow[K];
-#pragma unroll
-                for (int k = 0; k < K; k++) vrow[k] = (lane == 0) ? V[(r0 + j) * VS + k] : 0.0;
-                double acc[K];
-#pragma unroll
-                for (int k = 0; k < K; k++) acc[k] = 0.0;
-                constexpr int U = K <= 2 ? 4 : (K <= 4 ? HDFE_PCG_UNROLL : 2);
-                for (int64_t e0 = rs; e0 < re; e0 += 32 * U) {
-                    ring.release(e0);
-                    ring.ensure(min(e0 + 32 * U, re) - 1);
-                    ring_products<K, VS, VW, 32, CH>(a, ring, V, e0 + lane, min(e0 + 32 * U, re),
-                                                     acc);
-                }
-#pragma unroll
-                for (int k = 0; k < K; k++) acc[k] = warp_sum(acc[k]);
-                const int64_t row_st = __shfl_sync(kFull, st, j), row_en = __shfl_sync(kFull, en, j);
-                if (lane == 0)
-                    finish_row<K, double>(r0 + j, acc, row_st, row_en, lo, hi, gw, vrow, out,
-                                          carry, dot, true);
-                j++;
-            } else {
-                const unsigned ahead = longmask & (0xffffffffu << j);
-                int batch = ahead ? (__ffs(ahead) - 1 - j) : 4;
-                batch = min(min(batch, 4), nrows - j);
-                const int src = min(j + sub, 31);
-                const bool mine = sub < batch;
-                const int64_t rs = __shfl_sync(kFull, cs, src), re = __shfl_sync(kFull, ce, src);
-                const int64_t row_st = __shfl_sync(kFull, st, src);
-                const int64_t row_en = __shfl_sync(kFull, en, src);
-                const int64_t b_lo = __shfl_sync(kFull, cs, j);
-                const int64_t b_hi = __shfl_sync(kFull, ce, j + batch - 1);
-                ring.release(b_lo);
-                ring.ensure(b_hi - 1);
-                double vrow[K];
-#pragma unroll
-                for (int k = 0; k < K; k++)
-                    vrow[k] = (mine && sl == 0) ? V[(r0 + j + sub) * VS + k] : 0.0;
-                double acc[K];
-#pragma unroll
-                for (int k = 0; k < K; k++) acc[k] = 0.0;
-                if (mine) ring_products<K, VS, VW, 8, CH>(a, ring, V, rs + sl, re, acc);
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    acc[k] += __shfl_xor_sync(kFull, acc[k], 4);
-                    acc[k] += __shfl_xor_sync(kFull, acc[k], 2);
-                    acc[k] += __shfl_xor_sync(kFull, acc[k], 1);
-                }
-                if (mine && sl == 0 && re > rs)
-                    finish_row<K, double>(r0 + j + sub, acc, row_st, row_en, lo, hi, gw, vrow, out,
-                                          carry, dot, true);
-                j += batch;
-            }
-        }
-        if (nrows < 32) break;
-        r0 += 32;
-    }
-    __syncwarp();
-    ring.drain();
-    if (!ring.ok) GridBarrier{a.bar}.fail(HDFE_ERR_SPIN_LIMIT);
-}
-
 // AP[r] for a row whose nonzeros span several warps: summed from their carry
 // slots in a fixed order by the warp holding the row's last nonzero.  Returns
 // true (in all lanes) when this warp finishes such a row, with its AP in ap[].
@@ -729,40 +440,14 @@ __device__ __forceinline__ void block_partials(double (&v)[N], double *scratch, 
     __syncthreads();
 }
 
-// the ring's chunk: 1024-thread CTAs take half the nonzeros per chunk
-__host__ __device__ constexpr int ring_chunk(int k) { return threads_for(k) >= 1024 ? 128 : 256; }
-__host__ __device__ constexpr int ring_smem_bytes(int k)
-{
-    return (threads_for(k) / 32) * kRingStages * (ring_chunk(k) * 12 + 8);
-}
-
 template <int K>
 __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 {
     constexpr int KP = Stride<K>::P;
-    constexpr int CH = ring_chunk(K);
-    constexpr int NW = threads_for(K) / 32;
     __shared__ double s_red[4 * K];
     __shared__ double s_scratch[kMaxWarps * 3 * K];
-    extern __shared__ __align__(16) unsigned char s_ring[];
     GridBarrier gb{a.bar};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // this warp's ring: values, indices, one mbarrier per stage
-    double *ring_val = reinterpret_cast<double *>(s_ring) + warp * kRingStages * CH;
-    int32_t *ring_idx = reinterpret_cast<int32_t *>(s_ring + NW * kRingStages * CH * 8) +
-                        warp * kRingStages * CH;
-    uint64_t *ring_bar = reinterpret_cast<uint64_t *>(s_ring + NW * kRingStages * CH * 12) +
-                         warp * kRingStages;
-    unsigned ring_phase = 0;
-    if (a.ring) {
-        if (lane == 0) {
-            for (int st = 0; st < kRingStages; st++)
-                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(ring_bar + st))
-                             : "memory");
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncwarp();
-    }
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
     const int64_t L = a.L;
@@ -873,12 +558,8 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
             for (int k = 0; k < K; k++) dot[k] = 0.0;
             // P's rows are KP wide from a 256-byte aligned workspace: 32-byte
             // rows for k = 3, 4
-            constexpr int VW = (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1);
-            if (a.ring)
-                spmm_range_ring<K, KP, VW, CH>(a, a.P, a.AP, a.carry, dot, ring_idx, ring_val,
-                                               ring_bar, &ring_phase);
-            else
-                spmm_range<K, KP, VW, double>(a, a.data, a.P, a.AP, a.carry, dot, true);
+            spmm_range<K, KP, (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1), double>(
+                a, a.data, a.P, a.AP, a.carry, dot, true);
             block_partials<K>(dot, s_scratch, a.part, 0, nb);
             if (!gb.sync()) return;
             if (warp == 0) {
@@ -1043,11 +724,8 @@ int grid_blocks()
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-    if (cudaFuncSetAttribute(pcg_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             ring_smem_bytes(K)) != cudaSuccess)
-        return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<K>, threads_for(K),
-                                                      ring_smem_bytes(K)) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel<K>, threads_for(K), 0) !=
+        cudaSuccess)
         return -1;
     if (per_sm < 1) return -1;
     return sms * (per_sm < 1 ? per_sm : 1);
@@ -1084,7 +762,7 @@ cudaError_t launch(Params p, int blocks, cudaStream_t s)
 {
     void *args[] = {&p};
     return cudaLaunchCooperativeKernel((const void *)pcg_kernel<K>, dim3(blocks), dim3(threads_for(K)),
-                                       args, ring_smem_bytes(K), s);
+                                       args, 0, s);
 }
 
 // ------------------------------------------------ one column per lane
@@ -1708,10 +1386,6 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     p.cut = (uint8_t *)(ws + lay.cut);
     p.bar = (unsigned *)(ws + lay.bar);
     p.info = info;
-    // bulk copies of S need 16-byte aligned sources: S's arrays as allocated
-    // (chunks start at multiples of 4 nonzeros)
-    p.ring = (reinterpret_cast<uintptr_t>(indices) % 16 == 0 &&
-              reinterpret_cast<uintptr_t>(data) % 16 == 0) ? 1 : 0;
     HDFE_CUDA_TRY(cudaMemsetAsync(p.bar, 0, 16, s));
     pcg::k_partition<<<(unsigned)((p.nwarps + 256) / 256), 256, 0, s>>>(indptr, L, nnz, p.nwarps,
                                                                       pcg::kRowCost, (int64_t *)p.wlo);
