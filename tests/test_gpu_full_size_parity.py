@@ -86,8 +86,11 @@ def test_akm_5m_fit_matches_oracle(akm_5m):
     assert np.array_equal(cells.codes.cpu().numpy().view(np.uint32), ref.codes)
     assert np.array_equal(cells.cnt.cpu().numpy(), ref.cnt)
     assert np.array_equal(cells.n.cpu().numpy(), ref.n)
-    assert rel(cells.diag.cpu().numpy(), ref.diag) < 1e-12
-    assert rel(cells.rhs.cpu().numpy(), ref.rhs) < 1e-12
+    # the level sums run over up to 1.4M cells per level, on the device in
+    # another order than the oracle's sequential loop, with cancellation in
+    # diag = sum n - sum u^2 / N_g: 1e-10 at this size (1e-12 on small panels)
+    assert rel(cells.diag.cpu().numpy(), ref.diag) < 1e-10
+    assert rel(cells.rhs.cpu().numpy(), ref.rhs) < 1e-10
     S = res.S
     assert S.nnz == len(dt)
     assert np.array_equal(S.indptr.cpu().numpy(), ip)

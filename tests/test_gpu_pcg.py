@@ -196,7 +196,7 @@ def test_mixed_precision_widths(device, k):
         assert np.all(X[:, 2] == 0.0)
         x0 = X_ref + 1e-3 * rng.standard_normal(X_ref.shape)
         X2, it2, ok2, rel2 = solve(b, zero, x0)
-        assert ok2 and rel2 <= 1e-10 and it2 < it
+        assert ok2 and rel2 <= 1e-10 and it2 <= it
         assert np.max(np.abs(orc.csr_matmat(S, X2 - X_ref))) < 1e-8 * np.max(np.abs(b))
 
 
