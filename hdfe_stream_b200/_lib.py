@@ -78,6 +78,9 @@ SIGNATURES = {
     "hdfe_row_effects": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _i32, _i64, _vp,
                                     _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_kss_sigma2": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _f64, _i64, _vp, _vp]),
+    "hdfe_sort_workspace_bytes": (_i64, [_i64]),
+    "hdfe_sort_pairs": (_c.c_int, [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _i64, _vp]),
+    "hdfe_factorize": (_c.c_int, [_vp, _i64, _i32, _vp, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_gram_workspace_bytes": (_i64, [_i64, _i32]),
     "hdfe_gram_bf16x3": (_c.c_int, [_vp, _i64, _i32, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_solver_create": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _vp, _f64, _i64, _i32, _vp]),

@@ -567,6 +567,29 @@ int hdfe_pcg_solve_noalloc(const int64_t *indptr, const int32_t *indices, const 
                            int32_t k, const uint8_t *zero, const double *X0, double tol,
                            int64_t maxiter, double *X, hdfe_pcg_info *info, void *stream);
 
+/* ------------------------------------------- pass 0: sort and factorize
+ *
+ * core/passes.py:285-294 codes each fixed effect by the rank of its level
+ * among the sorted distinct levels; :359-373 orders the rows by (streamed
+ * code, other codes, variables).  hdfe_sort_pairs: a stable LSD radix sort of
+ * n keys (uint64, ordered by their value; key_bits = how many low bits can be
+ * nonzero, 8 bits a pass) with int32 payloads (NULL: the positions 0 .. n-1),
+ * into keys_out / vals_out; several keys sort as successive calls, least
+ * significant key first.  hdfe_factorize: codes[i] = the rank of ids[i] among
+ * the distinct ids (unsigned order), the distinct ids in order to levels (n
+ * entries, or NULL), their number to *n_levels (a DEVICE pointer).  n < 2^31.
+ * Both take a workspace of hdfe_sort_workspace_bytes(n) bytes (256-byte
+ * aligned).  They replace Polars' factorize and sort. */
+int64_t hdfe_sort_workspace_bytes(int64_t n);
+
+int hdfe_sort_pairs(const uint64_t *keys, const int32_t *vals, int64_t n, int32_t key_bits,
+                    uint64_t *keys_out, int32_t *vals_out, void *workspace,
+                    int64_t workspace_bytes, void *stream);
+
+int hdfe_factorize(const uint64_t *ids, int64_t n, int32_t key_bits, int32_t *codes,
+                   uint64_t *levels, int64_t *n_levels, void *workspace, int64_t workspace_bytes,
+                   void *stream);
+
 /* ------------------------------------------- X' W X of a wide design
  *
  * core/inference.py:109-137 `_assemble` forms the design's cross-products

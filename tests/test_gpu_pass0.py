@@ -50,3 +50,37 @@ def test_pass0_matches_host_layout(device, year_fe):
     ref_res = fit.fit(fit.DeviceRows.from_rows(ref), tol=1e-12)
     # the same fit (its weighted level sums are atomic, so equal to rounding)
     assert float((res.gamma - ref_res.gamma).abs().max() / ref_res.gamma.abs().max()) < 1e-10
+
+
+@pytest.mark.parametrize("n", [1, 5, 4096, 4097, 1_000_003])
+def test_radix_sort_and_factorize_match_numpy(device, n):
+    """hdfe_sort_pairs / hdfe_factorize (csrc/sort.cu) against numpy: the
+    stable order of 64-bit keys at every bit width the tiles meet (one
+    partial tile, exactly one, one plus one item, many), the rank codes and
+    levels of int32, int64 and float ids with many repeats."""
+    import torch
+    from hdfe_stream_b200 import pass0
+    rng = np.random.default_rng(n)
+    for bits in (8, 13, 40, 64):
+        hi = 2 ** bits
+        k = rng.integers(0, min(hi, 2 ** 63), n, dtype=np.int64)
+        if bits == 64:
+            k = k ^ rng.integers(0, 2, n, dtype=np.int64) << 63   # the top bit too
+        k[: n // 3] = k[0]                                         # long runs of one key
+        ks, pos = pass0.sort_pairs(torch.as_tensor(k, device=device), None, bits)
+        ref = np.argsort(k.view(np.uint64), kind="stable")
+        assert np.array_equal(pos.cpu().numpy(), ref)
+        assert np.array_equal(ks.cpu().numpy(), k[ref])
+    vals = rng.integers(-2 ** 31, 2 ** 31 - 1, n, dtype=np.int64).astype(np.int32)
+    k = rng.integers(0, 1000, n, dtype=np.int64)
+    _, v = pass0.sort_pairs(torch.as_tensor(k, device=device),
+                            torch.as_tensor(vals, device=device), 10)
+    assert np.array_equal(v.cpu().numpy(), vals[np.argsort(k, kind="stable")])
+    for ids in (rng.integers(-50, 50, n).astype(np.int32),
+                rng.integers(-2 ** 62, 2 ** 62, max(n // 7, 1))[rng.integers(0, max(n // 7, 1), n)],
+                np.round(rng.standard_normal(n), 2)):
+        codes, levels = pass0.factorize(torch.as_tensor(ids, device=device))
+        lev, inv = np.unique(ids, return_inverse=True)
+        assert np.array_equal(levels.cpu().numpy(), lev)
+        assert levels.dtype == torch.as_tensor(ids).dtype
+        assert np.array_equal(codes.cpu().numpy(), inv)
