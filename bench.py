@@ -608,11 +608,12 @@ def run_batched(args, rank):
 
     def batched_fit():
         solver = batch.BatchSolver(b, tol=args.tol, drows=drows, lanes=lanes)
+        solver.shape = dict(shape)
         X, info = solver.solve()
         return solver, solver.gammas(solver.normalize(X)), info
-    lanes = None
     tuner = batch.BatchSolver(b, tol=args.tol, drows=drows)
     lanes = tuner.tune()
+    shape = dict(tuner.shape)
     del tuner
     batched_fit()                                   # warm-up
     torch.cuda.synchronize()
@@ -636,7 +637,8 @@ def run_batched(args, rank):
             "ms_batched": round(ms_b, 3), "ms_sequential": round(ms_s, 3),
             "fits_per_s_batched": round(64 / (ms_b / 1e3), 2),
             "fits_per_s_sequential": round(64 / (ms_s / 1e3), 2),
-            "lanes_per_row": lanes, "max_iterations": int(info["iterations"].max()),
+            "launch_shape": {"lanes_per_row": lanes, **shape},
+            "max_iterations": int(info["iterations"].max()),
             "all_converged": bool(info["converged"].all()), "tol": args.tol,
             "max_rel_diff_vs_sequential": diff,
             "note": "FP64 batched PCG (per-system scalars, one cooperative launch); the "

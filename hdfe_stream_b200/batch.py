@@ -7,8 +7,10 @@ levels are renumbered so each system's are contiguous, and one persistent
 launch (`hdfe_batch_pcg_solve`, csrc/batch.cu) runs the Jacobi block PCG of
 every system with its own scalars -- the same algorithm, iteration rule and
 tolerance as a single fit (core/solve.py:66-140) -- over warps that the host
-assigns to the systems in proportion to their cost.  The lanes per row of the
-SpMV are tuned on the batch itself (`BatchSolver.tune`).  The normalisation
+assigns to the systems in proportion to their cost.  The launch shape (lanes
+per row of the SpMV, the length at which long rows are cut into chunks, a
+row's fixed cost in the warp split) is tuned on the batch itself
+(`BatchSolver.tune`).  The normalisation
 is the reference's per system (core/solve.py:383-399: the first non-streamed
 dimension per connected component, the others per system).
 """
@@ -26,6 +28,8 @@ from .simulate import Rows
 LANE_CHOICES = (4, 8, 16, 32)
 ROW_COST = 32           # a row's fixed cost in the warp split, in nonzeros
 LONG_ROW = 1024         # rows with more nonzeros are cut into chunks of this size
+LONG_ROW_CHOICES = (512, 1024, 4096)
+ROW_COST_CHOICES = (16, 32, 64)
 
 
 def _torch():
@@ -85,28 +89,31 @@ def concat(systems) -> Batch:
     return Batch(rows, row_ranges, group_ranges, level_ranges, np.asarray(raw_ss))
 
 
-def split_work(indptr, sys_of_new, n_systems, W):
+def split_work(indptr, sys_of_new, n_systems, W, long_row=LONG_ROW, fixed_cost=ROW_COST):
     """The warps' work for the batched PCG, from the renumbered CSR's indptr
-    (host array): rows longer than LONG_ROW nonzeros are cut into chunks of
-    LONG_ROW; each system gets one warp and then warps in proportion to its
-    cost (largest remainders); the system's rows, then its chunks, are split
-    over its warps by cumulative cost (nonzeros + ROW_COST per row or chunk,
-    a long row counting ROW_COST for its vector work).  Returns a dict of the
-    arrays `hdfe_batch_pcg_solve` takes."""
+    (host array): rows longer than `long_row` nonzeros are cut into chunks
+    of `long_row`; each system gets one warp and then warps in proportion to
+    its cost (largest remainders); the system's rows, then its chunks, are
+    split over its warps by cumulative cost (nonzeros + `fixed_cost` per row
+    or chunk, a long row counting `fixed_cost` for its vector work).  Returns
+    a dict of the arrays `hdfe_batch_pcg_solve` takes."""
+    long_row, fixed_cost = int(long_row), int(fixed_cost)
+    if long_row < 1 or fixed_cost < 0:
+        raise ValueError("split_work: long_row >= 1 and fixed_cost >= 0")
     indptr = np.asarray(indptr, np.int64)
     L = len(indptr) - 1
     rowlen = np.diff(indptr)
-    long_ = rowlen > LONG_ROW
-    nch = np.where(long_, (rowlen + LONG_ROW - 1) // LONG_ROW, 0)
+    long_ = rowlen > long_row
+    nch = np.where(long_, (rowlen + long_row - 1) // long_row, 0)
     C = int(nch.sum())
     first = np.concatenate(([0], np.cumsum(nch)[:-1])).astype(np.int64)
     chunk_row = np.repeat(np.arange(L, dtype=np.int64), nch)
     j = np.arange(C, dtype=np.int64) - np.repeat(first, nch)
-    chunk_lo = indptr[chunk_row] + j * LONG_ROW
-    chunk_hi = np.minimum(chunk_lo + LONG_ROW, indptr[chunk_row + 1])
+    chunk_lo = indptr[chunk_row] + j * long_row
+    chunk_hi = np.minimum(chunk_lo + long_row, indptr[chunk_row + 1])
     row_chunk = np.where(long_, first, -1).astype(np.int32)
-    row_cost = np.where(long_, 0, rowlen) + ROW_COST
-    chunk_cost = (chunk_hi - chunk_lo) + ROW_COST
+    row_cost = np.where(long_, 0, rowlen) + fixed_cost
+    chunk_cost = (chunk_hi - chunk_lo) + fixed_cost
     if n_systems > W:
         raise ValueError(f"{n_systems} systems need more than the grid's {W} warps")
     rb = np.searchsorted(sys_of_new, np.arange(n_systems + 1))          # rows per system
@@ -201,20 +208,28 @@ class BatchSolver:
         self.zero = torch.as_tensor(zero.reshape(-1), device=dev)
         self.n = n
         self.lanes = lanes
+        self.shape = {}             # tuned long_row / row_cost (empty: the defaults)
+        self.tuning = {}            # (lanes, long_row, row_cost) -> ms of the timed solves
         self._plans = {}
         self.root, _ = components(self.cells, 0)
 
-    def plan(self, lanes):
-        """Grid and work split for a lanes-per-row choice."""
+    def plan(self, lanes, long_row=None, row_cost=None):
+        """Grid and work split for a launch shape: lanes per row, the chunk
+        length of long rows and a row's fixed cost in the split."""
         torch = _torch()
-        if lanes not in self._plans:
+        long_row = int(long_row or self.shape.get("long_row", LONG_ROW))
+        row_cost = int(self.shape.get("row_cost", ROW_COST) if row_cost is None else row_cost)
+        key = (lanes, long_row, row_cost)
+        if key not in self._plans:
             lib = _lib.lib()
             blocks = _lib._c.c_int32()
             wpb = _lib._c.c_int32()
             _lib.check(lib.hdfe_batch_pcg_grid(self.m, lanes, _lib._c.byref(blocks),
                                                _lib._c.byref(wpb)))
             W = blocks.value * wpb.value
-            work = split_work(self.indptr.cpu().numpy(), self.sys_of, self.n, W)
+            if not hasattr(self, "_indptr_host"):
+                self._indptr_host = self.indptr.cpu().numpy()
+            work = split_work(self._indptr_host, self.sys_of, self.n, W, long_row, row_cost)
             dev = self.indptr.device
             ws_bytes = int(lib.hdfe_batch_pcg_workspace_bytes(len(self.perm), self.m, W,
                                                               work["n_chunks"]))
@@ -222,14 +237,15 @@ class BatchSolver:
                     if k != "n_chunks"}
             plan.update(blocks=blocks.value, n_chunks=work["n_chunks"],
                         ws=torch.empty(ws_bytes, dtype=torch.uint8, device=dev))
-            self._plans[lanes] = plan
-        return self._plans[lanes]
+            self._plans[key] = plan
+        return self._plans[key]
 
-    def solve(self, lanes=None):
-        """X (L, m) in the renumbered order and per-system info."""
+    def solve(self, lanes=None, long_row=None, row_cost=None):
+        """X (L, m) in the renumbered order and per-system info; the launch
+        shape defaults to the tuned one."""
         torch = _torch()
         lanes = lanes or self.lanes or 8
-        p = self.plan(lanes)
+        p = self.plan(lanes, long_row, row_cost)
         dev = self.indptr.device
         L = len(self.perm)
         X = torch.empty((L, self.m), dtype=torch.float64, device=dev)
@@ -250,25 +266,38 @@ class BatchSolver:
         if st != _lib.HDFE_OK:
             raise _lib.HDFEError(st, "batched PCG stopped early")
         return X, {"iterations": its.cpu().numpy(), "max_rel_residual": rel.cpu().numpy(),
-                   "converged": conv.cpu().numpy().astype(bool), "lanes": lanes}
+                   "converged": conv.cpu().numpy().astype(bool), "lanes": lanes,
+                   "long_row": int(long_row or self.shape.get("long_row", LONG_ROW)),
+                   "row_cost": int(self.shape.get("row_cost", ROW_COST) if row_cost is None
+                                   else row_cost)}
 
-    def tune(self):
-        """Lanes per row for this batch: each choice timed once with CUDA
-        events after one untimed solve, the fastest kept."""
+    def _time(self, lanes, long_row, row_cost):
+        """ms of one solve with this shape (CUDA events, after an untimed one)."""
         torch = _torch()
-        best, best_ms = None, None
-        for lanes in LANE_CHOICES:
-            self.solve(lanes)
+        key = (lanes, long_row, row_cost)
+        if key not in self.tuning:
+            self.solve(lanes, long_row, row_cost)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
-            self.solve(lanes)
+            self.solve(lanes, long_row, row_cost)
             b.record()
             torch.cuda.synchronize()
-            ms = a.elapsed_time(b)
-            if best_ms is None or ms < best_ms:
-                best, best_ms = lanes, ms
-        self.lanes = best
-        return best
+            self.tuning[key] = a.elapsed_time(b)
+        return self.tuning[key]
+
+    def tune(self):
+        """The launch shape for this batch, one coordinate at a time: lanes
+        per row (LANE_CHOICES) at the default split, then the long-row chunk
+        length (LONG_ROW_CHOICES), then the row cost (ROW_COST_CHOICES), each
+        choice timed once after an untimed solve and the fastest kept.
+        Returns the lanes; the split is kept in `shape`."""
+        long_row, row_cost = LONG_ROW, ROW_COST
+        lanes = min(LANE_CHOICES, key=lambda v: self._time(v, long_row, row_cost))
+        long_row = min(LONG_ROW_CHOICES, key=lambda v: self._time(lanes, v, row_cost))
+        row_cost = min(ROW_COST_CHOICES, key=lambda v: self._time(lanes, long_row, v))
+        self.lanes = lanes
+        self.shape = {"long_row": long_row, "row_cost": row_cost}
+        return lanes
 
     def normalize(self, X):
         """Gamma (L, m) in the combined numbering, normalised per system

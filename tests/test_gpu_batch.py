@@ -57,11 +57,39 @@ def test_batch_tune_and_zero_column(device):
     from hdfe_stream_b200 import batch, fit
     sys_rows = systems([3_000, 900, 5_000], seed=21)
     sys_rows[1].V[:, 0] = 0.0                 # y zero: a zero right-hand side
-    gammas, info = batch.fit_batch(sys_rows, tol=1e-12, tune=True)
-    assert info["lanes"] in batch.LANE_CHOICES
+    solver = batch.BatchSolver(batch.concat(sys_rows), tol=1e-12)
+    lanes = solver.tune()
+    # lanes, then chunk length, then row cost, each shape timed once
+    assert len(solver.tuning) == 8
+    assert lanes in batch.LANE_CHOICES
+    assert solver.shape["long_row"] in batch.LONG_ROW_CHOICES
+    assert solver.shape["row_cost"] in batch.ROW_COST_CHOICES
+    X, info = solver.solve()
+    assert (info["lanes"], info["long_row"], info["row_cost"]) == \
+        (lanes, solver.shape["long_row"], solver.shape["row_cost"])
+    gammas = solver.gammas(solver.normalize(X))
     for i, r in enumerate(sys_rows):
         res = fit.fit(fit.DeviceRows.from_rows(r), tol=1e-12)
         g = res.gamma.cpu().numpy()
         cols = slice(1, None) if i == 1 else slice(None)
         assert rel(gammas[i].cpu().numpy()[:, cols], g[:, cols]) < 1e-9
     assert np.max(np.abs(gammas[1].cpu().numpy()[:, 0])) < 1e-6
+
+
+def test_batch_matches_oracle(device):
+    """Each system of a weighted batch against the oracle's own FP64 solve of
+    that system alone (oracle/hdfe_oracle.c: pass 1, explicit S, Jacobi PCG,
+    normalisation), with long rows cut into short chunks and a small row
+    cost, so the chunked path carries most of the work."""
+    import oracle as orc
+    from hdfe_stream_b200 import batch
+    sys_rows = systems([1_500, 4_000, 700, 9_000], weights=True, seed=31)
+    solver = batch.BatchSolver(batch.concat(sys_rows), tol=1e-12)
+    X, info = solver.solve(16, long_row=512, row_cost=16)
+    assert info["converged"].all() and info["long_row"] == 512
+    gammas = solver.gammas(solver.normalize(X))
+    for i, r in enumerate(sys_rows):
+        c = orc.pass1(r)
+        g_ref, info_ref = orc.solve(c, orc.build_explicit(c), tol=1e-12)
+        assert rel(gammas[i].cpu().numpy(), g_ref) < 1e-8, i
+        assert abs(int(info["iterations"][i]) - int(info_ref["iterations"])) <= 1, i
