@@ -455,6 +455,129 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
                      comps=comps)
 
 
+BATCH_ROWS = 4_000_000      # rows per streamed batch (core/passes.py batch_rows)
+
+
+def group_batches(rows, batch_rows=BATCH_ROWS):
+    """Host rows (pass 0's layout, `simulate.Rows`) cut into batches of at
+    most about `batch_rows` rows at group boundaries -- every group whole in
+    one batch (core/passes.py:397-589 streams pass 1 the same way) -- as
+    pinned tuples (gcode (n,) int32, codes (n, D) int32, V (m, n) float64, w
+    (n,) float64 or None).  A group longer than `batch_rows` is a batch of
+    its own."""
+    import torch
+    g = np.asarray(rows.gcode)
+    N = len(g)
+    heads = np.flatnonzero(np.concatenate(([True], g[1:] != g[:-1]))) if N else np.zeros(0, int)
+    cuts, at = [0], 0
+    while at < N:
+        # the last group start at or below at + batch_rows, past `at`
+        k = int(np.searchsorted(heads, at + int(batch_rows), side="right")) - 1
+        nxt = int(heads[k]) if k >= 0 and heads[k] > at else None
+        if at + int(batch_rows) >= N:
+            nxt = N
+        elif nxt is None:                       # one group longer than a batch
+            j = int(np.searchsorted(heads, at, side="right"))
+            nxt = int(heads[j]) if j < len(heads) else N
+        cuts.append(nxt)
+        at = nxt
+
+    def pin(a, dtype):
+        return torch.from_numpy(np.ascontiguousarray(a).view(dtype)).pin_memory()
+    out = []
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        out.append((pin(rows.gcode[a:b].astype(np.uint32), np.int32),
+                    pin(rows.codes[a:b].astype(np.uint32), np.int32),
+                    pin(np.ascontiguousarray(rows.V[a:b].T, dtype=np.float64), np.float64),
+                    None if rows.w is None else pin(rows.w[a:b].astype(np.float64),
+                                                    np.float64)))
+    return out
+
+
+def fit_stream(batches, n_levels, tol=1e-10, maxiter=5000, rhs_block=8, names=None,
+               precision="fp64", timer=None) -> FitResult:
+    """The fit from row batches streamed through the device (the reference's
+    pass 1 over `batch_rows` batches, core/passes.py:397-589): the batches
+    (`group_batches`' pinned tuples, every group whole in one batch) are
+    uploaded on a copy stream one ahead of pass 1, so batch b + 1 crosses
+    PCIe while pass 1 runs on batch b, and only one or two batches are on the
+    device at a time.  Each batch's level arrays (obs, cnt, diag, rhs,
+    identifying groups and their cells per level) are sums over its groups
+    and add up across batches; its identifying cells append to the cell list
+    (their starts shifted by the cells before them); the variables' raw sums
+    of squares combine by the parallel-variance rule.  The S build and the
+    solve then run on the whole cell list, as in `fit`."""
+    torch = _torch()
+    timer = timer or _NoTimer()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    compute = torch.cuda.current_stream(dev)
+    copy = _copy_stream(dev)
+    n_levels = list(n_levels)
+
+    def upload(b):
+        copy.wait_stream(compute)
+        with torch.cuda.stream(copy):
+            ts = tuple(None if t is None else t.to(dev, non_blocking=True) for t in b)
+            ev = torch.cuda.Event()
+            ev.record(copy)
+        return ts, ev
+
+    if not batches:
+        raise ValueError("fit_stream: no batches")
+    level = None                            # obs, cnt, diag, rhs, lcount, work
+    parts = []                              # per batch: starts, codes, n, group_n
+    counts = {}
+    n_tot, mean, m2 = 0, None, None
+    ahead = upload(batches[0])
+    with timer("pass1"):
+        for i in range(len(batches)):
+            (g, c, V, w), ev = ahead
+            compute.wait_event(ev)
+            for t in (g, c, V, w):
+                if t is not None:
+                    t.record_stream(compute)
+            if i + 1 < len(batches):
+                ahead = upload(batches[i + 1])
+            cells = pass1(DeviceRows(g, c, V, w, n_levels))
+            arrays = (cells.obs, cells.cnt, cells.diag, cells.rhs, cells.lcount, cells.work)
+            level = list(arrays) if level is None else [a + b for a, b in zip(level, arrays)]
+            parts.append((cells.starts.clone(), cells.codes.clone(), cells.n.clone(),
+                          cells.group_n.clone()))
+            for k, v in cells.counts.items():
+                counts[k] = counts.get(k, 0) + v
+            nb = int(g.shape[0])
+            if mean is None:
+                n_tot, mean, m2 = nb, cells.means.clone(), cells.raw_ss.clone()
+            else:                           # Chan, Golub and LeVeque's pairwise update
+                delta = cells.means - mean
+                n_new = n_tot + nb
+                m2 = m2 + cells.raw_ss + delta * delta * (n_tot * nb / n_new)
+                mean = mean + delta * (nb / n_new)
+                n_tot = n_new
+            del cells, g, c, V, w
+        starts, shift = [], 0
+        for s, *_ in parts:
+            starts.append(s[:-1] + shift)
+            shift += int(s[-1].item())          # the batch's identifying cells
+        starts.append(torch.tensor([shift], dtype=torch.int64, device=dev))
+        cells = DeviceCells(starts=torch.cat(starts),
+                            codes=torch.cat([p[1] for p in parts]),
+                            n=torch.cat([p[2] for p in parts]),
+                            sums=None, group_n=torch.cat([p[3] for p in parts]),
+                            lcount=level[4].to(torch.int32), work=level[5], obs=level[0],
+                            cnt=level[1], diag=level[2], rhs=level[3], means=mean,
+                            raw_ss=m2, n_levels=n_levels, counts=counts)
+        del parts
+    comps = components_async(cells)
+    with timer("sbuild"):
+        S = build_s(cells)
+    with timer("solve"):
+        res = solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
+                    comps=comps, names=names)
+    res.info["batches"] = len(batches)
+    return res
+
+
 def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):
     """The fit from host rows (pass 0's layout, `simulate.Rows`): upload,
     solve on the device, and the normalised fixed effects back on the host.

@@ -232,3 +232,39 @@ def test_fit_from_host_equals_device_fit(device, name, rows):
     assert rel(got.gamma, want.gamma) < 1e-9
     its = np.atleast_1d(got.info["iterations"]) - np.atleast_1d(want.info["iterations"])
     assert np.all(np.abs(its) <= 1)
+
+
+@pytest.mark.parametrize("name", ["akm_20k", "weighted"])
+@pytest.mark.parametrize("batch_rows", [20_000, 57_311])
+def test_fit_stream_matches_one_pass(device, name, batch_rows):
+    """`fit.fit_stream` over row batches cut at group boundaries against the
+    one-pass `fit.fit` of the same rows: the identifying cells and S's
+    pattern identical, the level sums and S's values to rounding, the fixed
+    effects within 1e-10 of the one-pass fit and 1e-8 of the oracle."""
+    from hdfe_stream_b200 import fit
+    rows = dict(PANELS)[name]
+    batches = fit.group_batches(rows, batch_rows)
+    assert sum(int(b[0].shape[0]) for b in batches) == rows.n_rows
+    assert len(batches) >= rows.n_rows // batch_rows
+    for a, b in zip(batches[:-1], batches[1:]):       # no group is cut
+        assert int(a[0][-1]) != int(b[0][0])
+    res = fit.fit_stream(batches, rows.n_levels, tol=1e-12, names=rows.names)
+    one = fit.fit(fit.DeviceRows.from_rows(rows), tol=1e-12)
+    assert res.info["batches"] == len(batches)
+    for k in ("starts", "codes", "lcount", "work"):
+        assert np.array_equal(getattr(res.cells, k).cpu().numpy(),
+                              getattr(one.cells, k).cpu().numpy()), k
+    assert res.cells.counts == one.cells.counts
+    # weighted level sums are atomic adds: equal to rounding, not bit for bit
+    for k in ("n", "group_n", "obs", "cnt", "diag", "rhs", "raw_ss"):
+        a, b = getattr(res.cells, k).cpu().numpy(), getattr(one.cells, k).cpu().numpy()
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b)), k
+    assert np.array_equal(res.S.indptr.cpu().numpy(), one.S.indptr.cpu().numpy())
+    assert np.array_equal(res.S.indices.cpu().numpy(), one.S.indices.cpu().numpy())
+    d, d1 = res.S.data.cpu().numpy(), one.S.data.cpu().numpy()
+    assert np.max(np.abs(d - d1)) <= 1e-12 * np.max(np.abs(d1))
+    g, g1 = res.gamma.cpu().numpy(), one.gamma.cpu().numpy()
+    assert np.max(np.abs(g - g1)) / np.max(np.abs(g1)) < 1e-10
+    ref = orc.pass1(rows)
+    g_ref, _ = orc.solve(ref, orc.build_explicit(ref), tol=1e-12)
+    assert np.max(np.abs(g - g_ref)) / np.max(np.abs(g_ref)) < 1e-8
