@@ -127,3 +127,40 @@ def test_gradients_match_finite_differences(device):
             fd = (value(y0, w0 + h * v) - value(y0, w0 - h * v)) / (2 * h)
             an = float((gw * v).sum().item())
             assert abs(fd - an) <= 1e-5 * abs(an) + 1e-12, f_index
+
+
+def test_y_gradient_is_the_references_influence_output(device):
+    """The reference's influence output (normal_equations.py:69-73 `predict`
+    with :115-231 `solve_normal_equations`): for a right-hand side v over
+    the rows, u = (Z'WZ)^- Z'v and w_i z_i'u is the derivative of the sum of
+    predictions sum_i v_i yhat_i with respect to y_i.  The autograd
+    y-gradient of that sum through `FixedEffectsSolve` against the oracle's
+    `Design.apply_inverse` (inverse.py:311-374) of the same Z'v -- its level
+    sums D_d'v, covariate sums X'v and group sums -- read out on the rows."""
+    import torch
+    import oracle as orc
+    from hdfe_stream_b200.adjoint import FixedEffectsSolve
+    rows = panel_rows(1_500, 150, 41)
+    gcode, codes, y, X, w = device_inputs(rows, device)
+    y.requires_grad_(True)
+    nl = rows.n_levels
+    beta, gam, alpha, _ = FixedEffectsSolve.apply(y, w, gcode, codes, X, nl, 1e-13)
+    offs = np.concatenate(([0], np.cumsum(nl)[:-1])).astype(np.int64)
+    c64 = codes.to(torch.int64)
+    yhat = X @ beta + alpha[gcode.to(torch.int64)]
+    for d in range(len(nl)):
+        yhat = yhat + gam[int(offs[d]) + c64[:, d]]
+    rng = np.random.default_rng(8)
+    v = rng.standard_normal(rows.n_rows)
+    (grad_y,) = torch.autograd.grad((torch.as_tensor(v, device=device) * yhat).sum(), y)
+
+    c = orc.pass1(rows)
+    des = orc.Design(rows, c, orc.build_explicit(c), X=rows.V[:, 1:], tol=1e-13)
+    levels = np.concatenate([np.bincount(rows.codes[:, d].astype(np.int64), weights=v,
+                                         minlength=nl[d]) for d in range(len(nl))])
+    cov = rows.V[:, 1:].T @ v
+    streamed = np.bincount(rows.gcode.astype(np.int64), weights=v, minlength=rows.n_groups)
+    *_, zu = des.apply_inverse(levels[:, None], cov[:, None], streamed[:, None])
+    influence = rows.w * zu[:, 0]
+    got = grad_y.cpu().numpy()
+    assert np.max(np.abs(got - influence)) <= 1e-8 * np.max(np.abs(influence))
