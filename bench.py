@@ -147,17 +147,23 @@ class ClockSampler:
 
 # ----------------------------------------------------------- algorithmic bytes
 
-def phase_bytes(rows, counts, S, iterations, m=3):
+def phase_bytes(rows, counts, S, iterations, m=3, small=None):
     """Compulsory DRAM bytes per launch of each phase (written out in the
     design notes): pass 1 reads each row once and writes the identifying
     cells and level arrays; the S build reads the cells and writes S; one
-    PCG iteration reads S and streams the L x k vectors."""
+    PCG iteration reads S and streams the L x k vectors.  small: the fit's
+    info["small_block"] when the PCG ran on the split S -- the big block's
+    CSR, the dense cross block (first x 16 doubles) read once, and the big
+    rows' products with the small levels written and read back (16 L m)."""
     N, D, L = rows.n_rows, rows.codes.shape[1], int(sum(rows.n_levels))
     M, G = counts["n_ident_cells"], counts["n_ident_groups"]
     w = 0 if rows.w is None else 8
     p1 = N * (4 + 4 * D + 8 * m + w) + M * (4 * D + 8) + G * 16 + L * 8 * (3 + m)
     sb = M * (4 * D + 8) + G * 16 + S.nnz * 12 + (L + 1) * 8
     per_it = 12 * S.nnz + 8 * (L + 1) + 8 * L * m * 9
+    if small:
+        per_it = (12 * small["big_nnz"] + 8 * (L + 1) + 8 * 16 * small["first"]
+                  + 8 * L * m * 9 + 16 * small["first"] * m)
     return {"pass1": p1, "sbuild": sb, "pcg_kernel": per_it * max(iterations, 1)}
 
 
@@ -235,7 +241,7 @@ def run_ours(args, rank, world, local_rank):
     out = None
     if rank == 0:
         value = replicas.job_rate(args.steps, ms, world)
-        by = phase_bytes(rows, res.cells.counts, res.S, its)
+        by = phase_bytes(rows, res.cells.counts, res.S, its, small=info.get("small_block"))
         peak, peak_kind = measured_peak()
         roof = {}
         for name in ("pass1", "sbuild", "pcg_kernel"):

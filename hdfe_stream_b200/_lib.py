@@ -21,6 +21,8 @@ HDFE_ERR_CAPACITY = 6
 PCG_MAX_K = 32          # HDFE_PCG_MAX_K
 PCG_MIXED_MAX_K = 32    # HDFE_PCG_MIXED_MAX_K
 GRAM_MAX_COLS = 128     # HDFE_GRAM_MAX_COLS
+SMALL_MAX_LEVELS = 16   # HDFE_SMALL_MAX_LEVELS
+PCG_SMALL_MAX_K = 4     # HDFE_PCG_SMALL_MAX_K
 
 _c = ctypes
 _vp = _c.c_void_p
@@ -78,6 +80,12 @@ SIGNATURES = {
     "hdfe_row_effects": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _i32, _vp, _vp, _i32, _i64, _vp,
                                     _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
     "hdfe_kss_sigma2": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _f64, _i64, _vp, _vp]),
+    "hdfe_small_split_workspace_bytes": (_i64, [_i64]),
+    "hdfe_small_split": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _vp,
+                                    _vp, _vp, _vp, _i64, _vp]),
+    "hdfe_pcg_solve_small": (_c.c_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i32, _vp, _vp, _vp,
+                                        _vp, _i32, _vp, _vp, _f64, _i64, _vp, _vp, _i64, _vp,
+                                        _vp]),
     "hdfe_sort_workspace_bytes": (_i64, [_i64]),
     "hdfe_sort_pairs": (_c.c_int, [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_factorize": (_c.c_int, [_vp, _i64, _i32, _vp, _vp, _vp, _vp, _i64, _vp]),

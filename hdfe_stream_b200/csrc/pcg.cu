@@ -61,11 +61,28 @@ struct Stride {
     static constexpr int P = K == 1 ? 1 : ((K + 1) / 2) * 2;
 };
 
+// A dimension with few levels (years) meets almost every level of the others:
+// its rows and columns of S are nearly dense.  When its levels are the last
+// ns <= kSmall of S ("small levels" [Lb, L)), S's CSR holds only the block of
+// the other ("big") levels, and the rest is dense: cross (Lb x kSmall,
+// row-major, zero-padded) = S[r, Lb + j] and small (ns x ns) = S[Lb + i, Lb + j].
+// A big row's product with the small levels is then a coalesced 128-byte row
+// of cross against ns values held in shared memory, and the small rows'
+// products are the columns of cross summed against P's big rows, reduced
+// with the p'Ap partials: no index round trips, and cross is read once for
+// both halves of the symmetric block.
+constexpr int kSmall = HDFE_SMALL_MAX_LEVELS;
+
 struct Params {
     const int64_t *indptr;
     const int32_t *indices;
     const double *data;
     int64_t L, nnz;
+    int64_t Lb;                 // first small level (L when there is no dense block)
+    int ns;                     // small levels, 0 .. kSmall
+    const double *cross;        // (Lb, kSmall) S[r, Lb + j]
+    const double *small;        // (ns, ns) S[Lb + i, Lb + j]
+    double *AP2;                // (L, K) the big rows' products with the small levels
     const int64_t *wlo;     // (warps + 1) first nonzero of each warp's range
     int64_t nwarps;
     const double *dinv;
@@ -86,7 +103,7 @@ struct Params {
 // Workspace layout in bytes: R (L*K), P (L*KP), AP (L*K), carry, part,
 // wfirst, cut flags, then the barrier words.
 struct Layout {
-    int64_t r, p, ap, carry, part, wfirst, wlo, cut, bar, total;
+    int64_t r, p, ap, ap2, carry, part, wfirst, wlo, cut, bar, total;
 };
 
 inline Layout layout(int64_t L, int k, int64_t blocks)
@@ -98,9 +115,12 @@ inline Layout layout(int64_t L, int k, int64_t blocks)
     o.r = take(L * k * 8);
     o.p = take(L * kp * 8);
     o.ap = take(L * k * 8);
+    o.ap2 = take(L * k * 8);
     const int64_t warps = blocks * (threads_for(k) / 32);
     o.carry = take(warps * 2 * k * 8);
-    o.part = take(4 * (int64_t)k * blocks * 8);
+    // partials: p'Ap, ||R||^2, R'dinv R, ||B||^2 per column, then the dense
+    // block's column sums (kSmall x k)
+    o.part = take((4 + kSmall) * (int64_t)k * blocks * 8);
     o.wfirst = take(warps * 8);
     o.wlo = take((warps + 1) * 8);
     o.cut = take(L);
@@ -440,12 +460,134 @@ __device__ __forceinline__ void block_partials(double (&v)[N], double *scratch, 
     __syncthreads();
 }
 
+// ---- the dense small block (see kSmall)
+//
+// s_ps[j * K + k] = V[Lb + j, k]: the small levels' entries of the vector
+// being multiplied, one copy per CTA.
+template <int K, int VS>
+__device__ __forceinline__ void load_small(const Params &a, const double *V, double *s_ps)
+{
+    if ((int)threadIdx.x < a.ns * K) {
+        const int j = threadIdx.x / K, k = threadIdx.x % K;
+        s_ps[threadIdx.x] = V[(a.Lb + j) * VS + k];
+    }
+    __syncthreads();
+}
+
+// The big rows against the small levels, grid-strided two rows a warp, a lane
+// per small level (j = lane % 16): AP2[r] = cross[r] . ps (a 16-lane sum) and,
+// per lane, col[k] += cross[r, j] V[r, k] (the small rows' products, summed
+// over rows).  dot[k] += V[r, k] AP2[r, k] when want_dot.  The lanes' column
+// sums go to s_col[warp] (kSmall x K).
+template <int K, int VS>
+__device__ __forceinline__ void dense_rows(const Params &a, const double *V, const double *s_ps,
+                                           double *s_col, double (&dot)[K], bool want_dot)
+{
+    const int lane = threadIdx.x & 31, half = lane >> 4, j = lane & 15;
+    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t W = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double psj[K], col[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        psj[k] = j < a.ns ? s_ps[j * K + k] : 0.0;
+        col[k] = 0.0;
+    }
+    for (int64_t r2 = 2 * gw; r2 < a.Lb; r2 += 2 * W) {        // warp-uniform trips
+        const int64_t r = r2 + half;
+        const bool in = r < a.Lb;
+        const double b = in ? __ldcs(a.cross + r * kSmall + j) : 0.0;
+        double pr[K], t[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            pr[k] = in ? V[r * VS + k] : 0.0;
+            t[k] = b * psj[k];
+            col[k] += b * pr[k];
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) t[k] += __shfl_xor_sync(kFull, t[k], o);
+        if (in && j == 0) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                a.AP2[r * K + k] = t[k];
+                if (want_dot) dot[k] += pr[k] * t[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) col[k] += __shfl_xor_sync(kFull, col[k], 16);
+    if (lane < kSmall) {
+#pragma unroll
+        for (int k = 0; k < K; k++) s_col[(threadIdx.x >> 5) * kSmall * K + lane * K + k] = col[k];
+    }
+}
+
+// This CTA's column sums (over its warps, in order) to partials qc .. qc +
+// ns K - 1; with want_dot, thread k adds this CTA's share of the small rows'
+// p'Ap, ps . (its column sums) (CTA 0: also ps . small ps), to dot[k].
+template <int K>
+__device__ __forceinline__ void dense_partials(const Params &a, const double *s_ps,
+                                               double *s_col, double *s_cta, int qc, int nb,
+                                               double (&dot)[K], bool want_dot)
+{
+    __syncthreads();
+    const int t = threadIdx.x, nw = blockDim.x >> 5;
+    if (t < a.ns * K) {
+        double c = 0.0;
+        for (int w = 0; w < nw; w++) c += s_col[w * kSmall * K + t];
+        s_cta[t] = c;
+        a.part[(int64_t)(qc + t) * nb + blockIdx.x] = c;
+    }
+    __syncthreads();
+    if (want_dot && t < K) {
+        double e = 0.0;
+        for (int j = 0; j < a.ns; j++) e += s_ps[j * K + t] * s_cta[j * K + t];
+        if (blockIdx.x == 0) {
+            for (int j = 0; j < a.ns; j++) {
+                double q = 0.0;
+                for (int i = 0; i < a.ns; i++) q += a.small[j * a.ns + i] * s_ps[i * K + t];
+                e += s_ps[j * K + t] * q;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            if (t == k) dot[k] += e;
+    }
+}
+
+// After the grid barrier: s_aps[j * K + k] = (S V)[Lb + j, k], the column
+// sums over all CTAs (fixed order) plus small . ps, in every CTA.
+template <int K>
+__device__ __forceinline__ void dense_small_rows(const Params &a, const double *s_ps, int qc,
+                                                 double *s_aps)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int t = warp; t < a.ns * K; t += nw) {
+        const double v = reduce_part(a.part, qc + t);
+        if (lane == 0) s_aps[t] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < a.ns * K) {
+        const int j = threadIdx.x / K, k = threadIdx.x % K;
+        double q = 0.0;
+        for (int i = 0; i < a.ns; i++) q += a.small[j * a.ns + i] * s_ps[i * K + k];
+        s_aps[threadIdx.x] += q;
+    }
+    __syncthreads();
+}
+
 template <int K>
 __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 {
     constexpr int KP = Stride<K>::P;
     __shared__ double s_red[4 * K];
     __shared__ double s_scratch[kMaxWarps * 3 * K];
+    // the dense small block: its vector entries, this CTA's column sums, the
+    // small rows' products, and the warps' column sums
+    __shared__ double s_ps[kSmall * K], s_cta[kSmall * K], s_aps[kSmall * K];
+    __shared__ double s_col[kMaxWarps * kSmall * K];
+    constexpr int kQc = 4 * K;          // first partial of the column sums
     GridBarrier gb{a.bar};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -482,7 +624,13 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
     for (int k = 0; k < K; k++) dot[k] = 0.0;
     if (a.X0 != nullptr) {
         spmm_range<K, K, 1, double>(a, a.data, a.X0, a.AP, a.carry, dot, false);
+        if (a.ns > 0) {
+            load_small<K, K>(a, a.X0, s_ps);
+            dense_rows<K, K>(a, a.X0, s_ps, s_col, dot, false);
+            dense_partials<K>(a, s_ps, s_col, s_cta, kQc, nb, dot, false);
+        }
         if (!gb.sync()) return;
+        if (a.ns > 0) dense_small_rows<K>(a, s_ps, kQc, s_aps);
     }
     {
         double sb[K], sr[K], sz[K];
@@ -511,13 +659,23 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
             if (a.X0 != nullptr && (a.cut[r] & 1)) continue;
             const bool empty = (a.cut[r] & 2) != 0;
 #pragma unroll
-            for (int k = 0; k < K; k++) ap[k] = (a.X0 != nullptr && !empty) ? a.AP[r * K + k] : 0.0;
+            for (int k = 0; k < K; k++) {
+                ap[k] = (a.X0 != nullptr && !empty) ? a.AP[r * K + k] : 0.0;
+                if (a.X0 != nullptr && a.ns > 0)
+                    ap[k] = r < a.Lb ? ap[k] + a.AP2[r * K + k] : s_aps[(r - a.Lb) * K + k];
+            }
             setup_row(r, ap);
         }
         if (a.X0 != nullptr) {
             int64_t r;
             double ap[K];
-            if (finish_cut_row<K, double>(a, a.carry, r, ap) && lane == 0) setup_row(r, ap);
+            if (finish_cut_row<K, double>(a, a.carry, r, ap) && lane == 0) {
+                if (a.ns > 0) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) ap[k] += a.AP2[r * K + k];
+                }
+                setup_row(r, ap);
+            }
         }
         {
             double v[3 * K];
@@ -560,6 +718,11 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
             // rows for k = 3, 4
             spmm_range<K, KP, (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1), double>(
                 a, a.data, a.P, a.AP, a.carry, dot, true);
+            if (a.ns > 0) {
+                load_small<K, KP>(a, a.P, s_ps);
+                dense_rows<K, KP>(a, a.P, s_ps, s_col, dot, true);
+                dense_partials<K>(a, s_ps, s_col, s_cta, kQc, nb, dot, true);
+            }
             block_partials<K>(dot, s_scratch, a.part, 0, nb);
             if (!gb.sync()) return;
             if (warp == 0) {
@@ -569,6 +732,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                 }
             }
             __syncthreads();
+            if (a.ns > 0) dense_small_rows<K>(a, s_ps, kQc, s_aps);
             double alpha[K];
 #pragma unroll
             for (int k = 0; k < K; k++) {
@@ -586,7 +750,8 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                 for (int k = 0; k < K; k++) {
                     const double p = a.P[r * KP + k];
                     a.X[r * K + k] += alpha[k] * p;
-                    const double res = a.R[r * K + k] - alpha[k] * ap[k];
+                    const double apk = a.ns > 0 ? ap[k] + a.AP2[r * K + k] : ap[k];
+                    const double res = a.R[r * K + k] - alpha[k] * apk;
                     a.R[r * K + k] = res;
                     sr[k] += res * res;
                     sz[k] += res * res * di;
@@ -610,6 +775,9 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                     for (int k = 0; k < K; k++) {
                         p[u][k] = use ? a.P[r * KP + k] : 0.0;
                         ap[u][k] = (use && !empty) ? a.AP[r * K + k] : 0.0;
+                        if (use && a.ns > 0)
+                            ap[u][k] = r < a.Lb ? ap[u][k] + a.AP2[r * K + k]
+                                                : s_aps[(r - a.Lb) * K + k];
                         x[u][k] = use ? a.X[r * K + k] : 0.0;
                         rr[u][k] = use ? a.R[r * K + k] : 0.0;
                     }
@@ -1340,33 +1508,31 @@ extern "C" int64_t hdfe_pcg_workspace_bytes(int64_t L, int64_t nnz, int32_t k)
     return pcg::layout(L, k, blocks).total;
 }
 
-extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *data,
-                              int64_t L, int64_t nnz, const double *dinv, const double *B,
-                              int32_t k, const uint8_t *zero, const double *X0, double tol,
-                              int64_t maxiter, double *X, void *workspace,
-                              int64_t workspace_bytes, hdfe_pcg_info *info, void *stream)
+namespace {
+
+int solve_registers(const int64_t *indptr, const int32_t *indices, const double *data, int64_t L,
+                    int64_t nnz, int64_t small_first, int32_t small_count, const double *cross,
+                    const double *small, const double *dinv, const double *B, int32_t k,
+                    const uint8_t *zero, const double *X0, double tol, int64_t maxiter, double *X,
+                    void *workspace, int64_t workspace_bytes, hdfe_pcg_info *info,
+                    cudaStream_t s)
 {
-    if (k < 1 || k > HDFE_PCG_MAX_K || L < 1 || nnz < 0 || !indptr || !dinv || !B || !X ||
-        !info || !workspace || maxiter < 0 || (nnz > 0 && (!indices || !data)))
-        return hdfe_set_arg_error("hdfe_pcg_solve: bad argument");
-    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
-        return hdfe_set_arg_error("hdfe_pcg_solve: workspace must be 256-byte aligned");
-    cudaStream_t s = (cudaStream_t)stream;
-    if (pcg::use_lanes(k)) return pcg::solve_lanes(indptr, indices, data, L, nnz, dinv, B, k, zero,
-                                                   X0, tol, maxiter, X, workspace,
-                                                   workspace_bytes, info, s);
     int blocks = pcg::grid_blocks_for(k);
     if (blocks < 1) return hdfe_set_cuda_error(cudaGetLastError());
     pcg::Layout lay = pcg::layout(L, k, blocks);
     if (workspace_bytes < lay.total)
         return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_pcg_solve: workspace too small");
     char *ws = (char *)workspace;
-    pcg::Params p;
+    pcg::Params p{};
     p.indptr = indptr;
     p.indices = indices;
     p.data = data;
     p.L = L;
     p.nnz = nnz;
+    p.Lb = small_count > 0 ? small_first : L;
+    p.ns = small_count;
+    p.cross = cross;
+    p.small = small;
     const int64_t warps = (int64_t)blocks * (pcg::threads_for(k) / 32);
     p.nwarps = warps;
     p.dinv = dinv;
@@ -1379,6 +1545,7 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     p.R = (double *)(ws + lay.r);
     p.P = (double *)(ws + lay.p);
     p.AP = (double *)(ws + lay.ap);
+    p.AP2 = (double *)(ws + lay.ap2);
     p.carry = (double *)(ws + lay.carry);
     p.part = (double *)(ws + lay.part);
     p.wfirst = (int64_t *)(ws + lay.wfirst);
@@ -1405,6 +1572,48 @@ extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, con
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(3);
     return HDFE_OK;
+}
+
+}  // namespace
+
+extern "C" int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *data,
+                              int64_t L, int64_t nnz, const double *dinv, const double *B,
+                              int32_t k, const uint8_t *zero, const double *X0, double tol,
+                              int64_t maxiter, double *X, void *workspace,
+                              int64_t workspace_bytes, hdfe_pcg_info *info, void *stream)
+{
+    if (k < 1 || k > HDFE_PCG_MAX_K || L < 1 || nnz < 0 || !indptr || !dinv || !B || !X ||
+        !info || !workspace || maxiter < 0 || (nnz > 0 && (!indices || !data)))
+        return hdfe_set_arg_error("hdfe_pcg_solve: bad argument");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return hdfe_set_arg_error("hdfe_pcg_solve: workspace must be 256-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (pcg::use_lanes(k)) return pcg::solve_lanes(indptr, indices, data, L, nnz, dinv, B, k, zero,
+                                                   X0, tol, maxiter, X, workspace,
+                                                   workspace_bytes, info, s);
+    return solve_registers(indptr, indices, data, L, nnz, L, 0, nullptr, nullptr, dinv, B, k, zero,
+                           X0, tol, maxiter, X, workspace, workspace_bytes, info, s);
+}
+
+extern "C" int hdfe_pcg_solve_small(const int64_t *indptr, const int32_t *indices,
+                                    const double *data, int64_t L, int64_t nnz,
+                                    int64_t small_first, int32_t small_count,
+                                    const double *cross, const double *small, const double *dinv,
+                                    const double *B, int32_t k, const uint8_t *zero,
+                                    const double *X0, double tol, int64_t maxiter, double *X,
+                                    void *workspace, int64_t workspace_bytes,
+                                    hdfe_pcg_info *info, void *stream)
+{
+    if (k < 1 || k > HDFE_PCG_SMALL_MAX_K || L < 1 || nnz < 0 || !indptr || !dinv || !B || !X ||
+        !info || !workspace || maxiter < 0 || (nnz > 0 && (!indices || !data)) ||
+        small_count < 1 || small_count > HDFE_SMALL_MAX_LEVELS || small_first < 0 ||
+        small_first + small_count != L || !cross || !small)
+        return hdfe_set_arg_error("hdfe_pcg_solve_small: bad argument");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return hdfe_set_arg_error("hdfe_pcg_solve_small: workspace must be 256-byte aligned");
+    return solve_registers(indptr, indices, data, L, nnz, small_first, small_count, cross, small,
+                           dinv, B, k, zero, X0, tol, maxiter, X, workspace, workspace_bytes,
+                           info, (cudaStream_t)stream);
 }
 
 // ------------------------------------------------ allocation-free variant

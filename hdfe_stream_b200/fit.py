@@ -21,7 +21,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from .gpu import BlockSolver, DeviceCSR
+from .gpu import BlockSolver, DeviceCSR, small_levels
 
 RHS_ZERO_TOL = 1e-11        # core/solve.py:44
 
@@ -282,12 +282,15 @@ class FitResult:
 
 def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
           x0=None, normalize_fe=True, timer=None, precision="fp64", comps=None,
-          solver="explicit", names=None) -> FitResult:
+          solver="explicit", names=None, small_block=True) -> FitResult:
     """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
     right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
     zero, block PCG per `rhs_block` columns, then `_normalize`.  `comps`:
     the first dimension's components from `components_async`, else computed
-    here.  `names`: the variables' names, for info["fe_spanned"].  The info
+    here.  `names`: the variables' names, for info["fe_spanned"].
+    `small_block`: when the trailing dimensions have at most 16 levels in
+    all (the years), the FP64 solve takes S with those levels' rows and
+    columns stored densely (`gpu.SmallSplit`, `hdfe_pcg_solve_small`).  The info
     dict has the keys of core/solve.py:370-381 `_solve_info` (iterations,
     converged, blocks; max_rel_residual unless NaN; fe_spanned, the names
     of the variables the fixed effects span, only when there are any) and
@@ -300,7 +303,8 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
         from .gpu import StreamSolver
         solver = StreamSolver(cells, dinv, tol, maxiter)
     elif solver == "explicit":
-        solver = BlockSolver(S, dinv, tol, maxiter, precision=precision)
+        small = small_levels(cells.n_levels) if small_block and precision == "fp64" else None
+        solver = BlockSolver(S, dinv, tol, maxiter, precision=precision, small=small)
         solver.timer = timer
     else:
         raise ValueError("solver must be 'explicit' or 'stream_cg'")
@@ -335,6 +339,9 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
             "n_components": int(n_comp[0])}
     if not np.isnan(rel):
         info["max_rel_residual"] = rel
+    if explicit and getattr(solver, "split", None) is not None:
+        sp = solver.split
+        info["small_block"] = {"first": sp.first, "count": sp.count, "big_nnz": sp.S_big.nnz}
     names = list(names) if names else [f"v{j}" for j in range(m)]
     spanned = [names[j] for j in range(m) if zero_all[j]]
     if spanned:
@@ -407,33 +414,64 @@ def _copy_stream(dev):
     return _COPY_STREAMS[key]
 
 
+V_CHUNKS = (4, 3, 2, 1)     # relative sizes of the outcome's upload chunks, last smallest
+
+
+def _group_cuts(gcode, weights):
+    """Row offsets 0 < c_1 < ... < N cutting the sorted host `gcode` into
+    pieces of about the given relative sizes, each cut at a group's first
+    row (so no group is split)."""
+    g = gcode.numpy() if hasattr(gcode, "numpy") else np.asarray(gcode)
+    N = len(g)
+    tot = float(sum(weights))
+    cuts, acc = [0], 0.0
+    for wgt in weights[:-1]:
+        acc += wgt
+        t = min(int(N * acc / tot), N - 1)
+        c = int(np.searchsorted(g, g[t], side="left")) if N else 0
+        if cuts[-1] < c < N:
+            cuts.append(c)
+    cuts.append(N)
+    return cuts
+
+
 def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_block=8,
-             timer=None, precision="fp64") -> FitResult:
+             timer=None, precision="fp64", names=None, v_chunks=V_CHUNKS) -> FitResult:
     """The fit from host tensors in pass 0's layout -- gcode (N,) int32,
     codes (N, D) int32, V (m, N) float64, w (N,) float64 or None, pinned for
-    the copies to overlap -- with the upload overlapped with the work that
-    needs no outcome: the group and level structure (and the weights) are
-    copied first; while V follows on a copy stream, pass 1 runs on the
-    structure alone (m = 0: cells, counts, diag) and S is built from it; then
-    pass 1 runs again with V for the right-hand sides and the solve follows.
-    S depends on the structure only and comes out identical to `fit`'s; the
-    right-hand sides are pass 1's own (its level sums are atomic, so their
-    last bits vary from run to run exactly as they do in `fit`)."""
+    the copies to overlap -- with the upload overlapped with the work: the
+    group and level structure (and the weights) are copied first; while V
+    follows on a copy stream, pass 1 runs on the structure alone (m = 0:
+    cells, counts, diag) and S is built from it; V crosses in chunks of
+    whole groups (relative sizes `v_chunks`, the last the smallest), and as
+    each lands pass 1 runs on that chunk's rows for its right-hand sides
+    (sums over its groups, so they add up across chunks; the variables' sums
+    of squares combine by the parallel-variance rule).  After the last byte
+    only the last chunk's pass and the solve remain.  S depends on the
+    structure only and comes out identical to `fit`'s; the right-hand sides
+    agree with `fit`'s to rounding (another grouping of the same sums)."""
     torch = _torch()
     timer = timer or _NoTimer()
     dev = torch.device("cuda", torch.cuda.current_device())
     compute = torch.cuda.current_stream(dev)
     copy = _copy_stream(dev)
+    m = int(V.shape[0])
+    cuts = _group_cuts(gcode, list(v_chunks) or [1])
     copy.wait_stream(compute)       # the buffers it writes may be freed memory of compute's
+    chunks = []
     with torch.cuda.stream(copy):
         g_d = gcode.to(dev, non_blocking=True)
         c_d = codes.to(dev, non_blocking=True)
         w_d = None if w is None else w.to(dev, non_blocking=True)
         structure = torch.cuda.Event()
         structure.record(copy)
-        V_d = V.to(dev, non_blocking=True)
-        values = torch.cuda.Event()
-        values.record(copy)
+        for lo, hi in zip(cuts[:-1], cuts[1:]):
+            Vc = torch.empty((m, hi - lo), dtype=torch.float64, device=dev)
+            for j in range(m):
+                Vc[j].copy_(V[j, lo:hi], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(copy)
+            chunks.append((lo, hi, Vc, ev))
     compute.wait_event(structure)
     for t in (g_d, c_d, w_d):
         if t is not None:
@@ -445,14 +483,38 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
     comps = components_async(shape)         # the structure is all it reads
     with timer("sbuild"):
         S = build_s(shape)
-    del shape
-    compute.wait_event(values)
-    V_d.record_stream(compute)
+    rhs, n_tot, mean, m2 = None, 0, None, None
     with timer("pass1"):
-        cells = pass1(DeviceRows(g_d, c_d, V_d, w_d, n_levels))
+        for lo, hi, Vc, ev in chunks:
+            compute.wait_event(ev)
+            Vc.record_stream(compute)
+            part = pass1(DeviceRows(g_d[lo:hi], c_d[lo:hi], Vc,
+                                    None if w_d is None else w_d[lo:hi], n_levels))
+            nb = hi - lo
+            if rhs is None:
+                rhs, n_tot, mean, m2 = part.rhs, nb, part.means.clone(), part.raw_ss.clone()
+            else:
+                rhs = rhs + part.rhs
+                delta = part.means - mean
+                n_new = n_tot + nb
+                m2 = m2 + part.raw_ss + delta * delta * (n_tot * nb / n_new)
+                mean = mean + delta * (nb / n_new)
+                n_tot = n_new
+            del part
+    del chunks
+    import dataclasses
+    cells = dataclasses.replace(shape, rhs=rhs, means=mean, raw_ss=m2)
     with timer("solve"):
         return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
-                     comps=comps)
+                     comps=comps, names=names)
+
+
+def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):
+    """The fit from host rows (pass 0's layout, `simulate.Rows`): upload,
+    solve on the device, and the normalised fixed effects back on the host.
+    Returns (gamma (L, m) numpy, info)."""
+    res = fit(DeviceRows.from_rows(rows), tol, maxiter, rhs_block)
+    return res.gamma.cpu().numpy(), res.info
 
 
 BATCH_ROWS = 4_000_000      # rows per streamed batch (core/passes.py batch_rows)
@@ -576,11 +638,3 @@ def fit_stream(batches, n_levels, tol=1e-10, maxiter=5000, rhs_block=8, names=No
                     comps=comps, names=names)
     res.info["batches"] = len(batches)
     return res
-
-
-def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):
-    """The fit from host rows (pass 0's layout, `simulate.Rows`): upload,
-    solve on the device, and the normalised fixed effects back on the host.
-    Returns (gamma (L, m) numpy, info)."""
-    res = fit(DeviceRows.from_rows(rows), tol, maxiter, rhs_block)
-    return res.gamma.cpu().numpy(), res.info

@@ -74,6 +74,56 @@ class DeviceCSR:
         return self.nnz * 12 + (self.L + 1) * 8
 
 
+def small_levels(n_levels):
+    """(first, count) of the dense small block for levels stacked by
+    dimension (`n_levels`): the trailing dimensions whose levels total at
+    most SMALL_MAX_LEVELS, behind at least one big level; None if none."""
+    n = [int(v) for v in n_levels]
+    count, d = 0, len(n)
+    while d > 1 and count + n[d - 1] <= _lib.SMALL_MAX_LEVELS:
+        count += n[d - 1]
+        d -= 1
+    first = sum(n[:d])
+    return (first, count) if count > 0 and first > 0 else None
+
+
+class SmallSplit:
+    """S split for `hdfe_pcg_solve_small`: the big levels' block in CSR
+    (`S_big`), cross (first, 16) = S[r, first + j] and small (count, count)
+    (`hdfe_small_split`)."""
+
+    def __init__(self, S: DeviceCSR, first: int, count: int, stream=None):
+        import torch
+        lib = _lib.lib()
+        dev = S.indptr.device
+        L = S.L
+        self.first, self.count = int(first), int(count)
+        indptr = torch.empty(L + 1, dtype=torch.int64, device=dev)
+        indices = torch.empty(max(S.nnz, 1), dtype=torch.int32, device=dev)
+        data = torch.empty(max(S.nnz, 1), dtype=torch.float64, device=dev)
+        self.cross = torch.empty((self.first, _lib.SMALL_MAX_LEVELS), dtype=torch.float64,
+                                 device=dev)
+        self.small = torch.empty((self.count, self.count), dtype=torch.float64, device=dev)
+        out = torch.zeros(2, dtype=torch.int64, device=dev)       # nnz, status
+        ws = torch.empty(int(lib.hdfe_small_split_workspace_bytes(L)), dtype=torch.uint8,
+                         device=dev)
+        _lib.check(lib.hdfe_small_split(
+            S.indptr.data_ptr(), S.indices.data_ptr(), S.data.data_ptr(), L, self.first,
+            self.count, indptr.data_ptr(), indices.data_ptr(), data.data_ptr(),
+            self.cross.data_ptr(), self.small.data_ptr(), out.data_ptr(),
+            out.data_ptr() + 8, ws.data_ptr(), ws.numel(), _lib.stream_handle(stream)))
+        nnz, status = (int(v) for v in out.cpu())
+        if status & 0xFFFFFFFF:
+            raise _lib.HDFEError(_lib.HDFE_ERR_BAD_CODE,
+                                 "small split: a big row holds only small-level entries "
+                                 "or a column is out of range")
+        self.S_big = DeviceCSR(indptr, indices[:nnz], data[:nnz], L, nnz)
+
+    @property
+    def nbytes(self) -> int:
+        return self.S_big.nbytes + (self.cross.numel() + self.small.numel()) * 8
+
+
 class BlockSolver:
     """`solve(b, zero, x0) -> (X, iterations, converged, rel)` on the device.
 
@@ -82,10 +132,12 @@ class BlockSolver:
     exactly as the reference's `solve` (core/gpu.py:194-196)."""
 
     def __init__(self, S: DeviceCSR, dinv, tol: float, maxiter: int, debug=None,
-                 precision: str = "fp64", inner_tol: float = 1e-6):
+                 precision: str = "fp64", inner_tol: float = 1e-6, small=None):
         """precision "fp64" is the reference's solve; "mixed" runs the inner
         CG in FP32 with FP64 iterative refinement (hdfe_pcg_solve_mixed),
-        stopping on the same FP64 relative residual `tol`."""
+        stopping on the same FP64 relative residual `tol`.  small: (first,
+        count) of a dense small block (`small_levels`), used by the FP64
+        solves of at most PCG_SMALL_MAX_K columns (`hdfe_pcg_solve_small`)."""
         import torch
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
@@ -100,6 +152,15 @@ class BlockSolver:
         self._info = torch.zeros(3, dtype=torch.float64, device=self.dev)   # 24 bytes
         self._zero = torch.zeros(_lib.PCG_MAX_K, dtype=torch.uint8, device=self.dev)
         self.stats = {"launches": 0, "iterations": 0}     # solves so far (for the roofline)
+        self.split = None
+        if small is not None and precision == "fp64":
+            try:
+                self.split = SmallSplit(S, *small)
+            except _lib.HDFEError as e:
+                # a level whose row of S meets only the small levels: solve
+                # on the whole CSR instead
+                if e.code != _lib.HDFE_ERR_BAD_CODE:
+                    raise
 
     def _workspace(self, k):
         import torch
@@ -122,6 +183,15 @@ class BlockSolver:
             self._zero[:k].copy_(torch.from_numpy(np.asarray(zero, bool).astype(np.uint8)))
             zp = self._zero.data_ptr()
         x0p = None if X0 is None else X0.data_ptr()
+        if self.split is not None and k <= _lib.PCG_SMALL_MAX_K:
+            sp = self.split
+            _lib.check(_lib.lib().hdfe_pcg_solve_small(
+                sp.S_big.indptr.data_ptr(), sp.S_big.indices.data_ptr(),
+                sp.S_big.data.data_ptr(), sp.S_big.L, sp.S_big.nnz, sp.first, sp.count,
+                sp.cross.data_ptr(), sp.small.data_ptr(), self.dinv.data_ptr(), B.data_ptr(),
+                k, zp, x0p, self.tol, self.maxiter, X.data_ptr(), ws.data_ptr(), ws.numel(),
+                self._info.data_ptr(), _lib.stream_handle(stream)))
+            return
         if self.precision == "mixed":
             _lib.check(_lib.lib().hdfe_pcg_solve_mixed(
                 self.S.indptr.data_ptr(), self.S.indices.data_ptr(), self.S.data.data_ptr(),

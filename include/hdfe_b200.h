@@ -526,6 +526,48 @@ int hdfe_pcg_solve(const int64_t *indptr, const int32_t *indices, const double *
                    double *X, void *workspace, int64_t workspace_bytes,
                    hdfe_pcg_info *info, void *stream);
 
+/* ------------------------------------------- the dense small block
+ *
+ * A dimension with few levels (the years) meets nearly every level of the
+ * others, so its rows and columns of S are nearly dense (on the 5M-worker
+ * panel: 7.28M of the 7.50M firm-year entries exist, 64% of S's nonzeros).
+ * When those levels are S's last `small_count` <= HDFE_SMALL_MAX_LEVELS
+ * levels [small_first, L), the solve can take S split in three:
+ *   the CSR of S[big, big] (rows >= small_first empty), columns < small_first;
+ *   cross (small_first x HDFE_SMALL_MAX_LEVELS, row-major, zero-padded):
+ *     cross[r * 16 + j] = S[r, small_first + j];
+ *   small (small_count x small_count): S[small_first + i, small_first + j].
+ * hdfe_small_split makes this form from S's CSR (columns sorted in each row):
+ * indptr_out (L+1), indices_out / data_out (at most nnz entries), cross and
+ * small as above, the big block's nonzero count to *nnz_out (a DEVICE
+ * pointer), and status to *status_out (DEVICE): HDFE_OK, or
+ * HDFE_ERR_BAD_CODE when a big row holds small-level entries but none of
+ * the big block (the split would lose it from the row walk).
+ * hdfe_pcg_solve_small is hdfe_pcg_solve (k <= HDFE_PCG_SMALL_MAX_K, the
+ * same workspace size) on the split form: the big rows' products with the
+ * small levels are coalesced rows of cross, the small rows' products the
+ * column sums of cross reduced with p'Ap, no index round trips.  The
+ * reference stores all of S in CSR (core/solve.py:148-194); the algorithm
+ * (core/solve.py:66-140) is unchanged, only the order of the additions in
+ * S P differs. */
+#define HDFE_SMALL_MAX_LEVELS 16
+#define HDFE_PCG_SMALL_MAX_K 4
+
+int64_t hdfe_small_split_workspace_bytes(int64_t L);
+
+int hdfe_small_split(const int64_t *indptr, const int32_t *indices, const double *data,
+                     int64_t L, int64_t small_first, int32_t small_count, int64_t *indptr_out,
+                     int32_t *indices_out, double *data_out, double *cross, double *small,
+                     int64_t *nnz_out, int32_t *status_out, void *workspace,
+                     int64_t workspace_bytes, void *stream);
+
+int hdfe_pcg_solve_small(const int64_t *indptr, const int32_t *indices, const double *data,
+                         int64_t L, int64_t nnz, int64_t small_first, int32_t small_count,
+                         const double *cross, const double *small, const double *dinv,
+                         const double *B, int32_t k, const uint8_t *zero, const double *X0,
+                         double tol, int64_t maxiter, double *X, void *workspace,
+                         int64_t workspace_bytes, hdfe_pcg_info *info, void *stream);
+
 /* Mixed precision: the same solve with the inner CG in FP32 and iterative
  * refinement in FP64 -- the outer residual B - S X (S's FP64 values in
  * `data`), the update X += D and every dot product and norm are FP64; the

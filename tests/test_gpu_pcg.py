@@ -299,3 +299,73 @@ def test_solver_handle_matches_block_solver(device):
                                      ctypes.byref(info), _lib.stream_handle()) != _lib.HDFE_OK
     finally:
         assert lib.hdfe_solver_destroy(handle) == _lib.HDFE_OK
+
+
+def _small_cases():
+    from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
+    out = []
+    for name in GOLDEN_PANELS:
+        g = load_golden(name)
+        out.append((name, (g["S_indptr"], g["S_indices"], g["S_data"]), g["diag"],
+                    list(g["n_levels"])))
+    rows = pass0_layout(simulate_panel(20_000, 2_000, 10, spell=(2, 10), p_move=0.1,
+                                       weights=True, seed=9))
+    c = orc.pass1(rows)
+    out.append(("weighted_20k", orc.build_explicit(c), c.diag, list(c.n_levels)))
+    return out
+
+
+SMALL_CASES = _small_cases()
+
+
+@pytest.mark.parametrize("case", SMALL_CASES, ids=[c[0] for c in SMALL_CASES])
+def test_small_block_split_and_solve(device, case):
+    """S with its trailing small dimension (the years) stored densely
+    (`hdfe_small_split` + `hdfe_pcg_solve_small`): the split reproduces S's
+    entries exactly (big block in CSR with the entries' order kept, cross
+    and small dense), and the solve matches the oracle's CG on the whole S
+    for 1, 3 and 4 columns, with a zero column and a warm start."""
+    import scipy.sparse as sp
+    import torch
+    from hdfe_stream_b200 import gpu
+    _, S, diag, n_levels = case
+    small = gpu.small_levels(n_levels)
+    assert small is not None
+    first, count = small
+    A = gpu.DeviceCSR.from_host(*S)
+    split = gpu.SmallSplit(A, first, count)
+    dense = sp.csr_matrix((S[2], S[1], S[0]), shape=(A.L, A.L))
+    big = dense[:first, :first].tocsr()
+    big.sort_indices()
+    ip = split.S_big.indptr.cpu().numpy()
+    assert np.array_equal(ip[:first + 1], big.indptr) and np.all(ip[first:] == big.nnz)
+    assert np.array_equal(split.S_big.indices.cpu().numpy(), big.indices)
+    assert np.array_equal(split.S_big.data.cpu().numpy(), big.data)
+    cross = split.cross.cpu().numpy()
+    assert np.array_equal(cross[:, :count], dense[:first, first:].toarray())
+    assert np.all(cross[:, count:] == 0.0)
+    assert np.array_equal(split.small.cpu().numpy(), dense[first:, first:].toarray())
+
+    dinv = orc.jacobi(diag)
+    plain = gpu.BlockSolver(A, dinv, 1e-10, 5000)
+    solver = gpu.BlockSolver(A, dinv, 1e-10, 5000, small=small)
+    rng = np.random.default_rng(first)
+    for k in (1, 3, 4):
+        b = orc.csr_matmat(S, rng.standard_normal((A.L, k)))
+        zero = np.zeros(k, bool)
+        if k > 1:
+            zero[1] = True
+        x0 = 0.3 * rng.standard_normal((A.L, k))
+        for guess in (None, x0):
+            X_ref, it_ref, ok_ref, _ = orc.pcg(S, dinv, b, zero, guess, 1e-10)
+            X, it, ok, rel = solver(b, zero, guess)
+            Xp, itp, _, _ = plain(b, zero, guess)
+            assert ok and ok_ref and abs(it - it_ref) <= 1 and rel <= 1e-10, (k, it, it_ref)
+            assert np.all(X[:, zero] == 0.0)
+            assert np.max(np.abs(X - X_ref)) < 1e-8 * np.max(np.abs(X_ref))
+            assert np.max(np.abs(X - Xp)) < 1e-9 * np.max(np.abs(Xp)) and abs(it - itp) <= 1
+    # deterministic: the same bits twice
+    b = orc.csr_matmat(S, rng.standard_normal((A.L, 3)))
+    X1, *_ = solver(b)
+    X2, *_ = solver(b)
+    assert np.array_equal(X1, X2)
