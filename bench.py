@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-jla", dest="jla", action="store_false",
                     help="skip the KSS-JLA leverage measurement")
+    ap.add_argument("--kss-workload", default="kss_1m",
+                    help="panel of the KSS measurement (kss_100k: a small case for profiling)")
+    ap.add_argument("--parts", default="all",
+                    help="comma list of the measurements besides the fit to run: accuracy, "
+                         "kss, adjoint, batched, e2e, streamed (default all; for profiling)")
     return ap.parse_args()
 
 
@@ -65,8 +70,8 @@ def describe(name):
             f"spells of {lo}-{hi} years, p_move {p['p_move']}")
     if p.get("weights"):
         text += ", weights U[0.5, 2]"
-    restriction = {"akm_5m": "largest connected set with min_degree=2",
-                   "kss_1m": "leave-one-out connected set"}.get(name)
+    restriction = "leave-one-out connected set" if name.startswith("kss_") else \
+        {"akm_5m": "largest connected set with min_degree=2"}.get(name)
     return text + (f", {restriction}" if restriction else "")
 
 
@@ -227,16 +232,20 @@ def run_ours(args, rank, world, local_rank):
     # tolerance whose fixed effects are within 1e-8 (relative, max norm) of an
     # FP64 solve at 1e-13, and the solve's time at that tolerance (components,
     # PCG, normalisation on the same cells and S)
-    accuracy = equal_error_solves(res.cells, res.S, max(args.steps, 3))
+    parts = set(("accuracy,kss,adjoint,batched,e2e,streamed" if args.parts == "all"
+                 else args.parts).split(","))
+    accuracy = equal_error_solves(res.cells, res.S, max(args.steps, 3)) \
+        if "accuracy" in parts else None
     # KSS-JLA: p = 256 Rademacher probes through A S^- A' on the 1M-worker panel
-    jla = run_jla(args, rank, world, dist) if args.jla else None
-    adjoint = run_adjoint(args, rank) if args.jla else None
-    batched = run_batched(args, rank) if args.jla else None
+    jla = run_jla(args, rank, world, dist) if args.jla and "kss" in parts else None
+    adjoint = run_adjoint(args, rank) if args.jla and "adjoint" in parts else None
+    batched = run_batched(args, rank) if args.jla and "batched" in parts else None
 
     # e2e through the public call: pinned host rows up, fixed effects back
-    e2e = run_e2e(args, rows, dist)
+    e2e = run_e2e(args, rows, dist) if "e2e" in parts else None
     # the same fit with the rows streamed through the device in 4M-row batches
-    streamed = run_streamed(args, rows, res.gamma, dist) if args.jla else None
+    streamed = run_streamed(args, rows, res.gamma, dist) \
+        if args.jla and "streamed" in parts else None
 
     out = None
     if rank == 0:
@@ -334,7 +343,7 @@ def run_jla(args, rank, world, dist):
 
     # under torchrun the ranks share ONE job: the same panel, the probes and
     # draws split over the ranks (one all-reduce of the moment sums each)
-    rows = prepare("kss_1m", seed=100)
+    rows = prepare(args.kss_workload, seed=100)
     drows = fit.DeviceRows.from_rows(rows)
     res = fit.fit(drows, tol=args.tol)
     S = res.S
@@ -411,8 +420,8 @@ def run_jla(args, rank, world, dist):
 
     def finite(x):
         return [float(v) if np.isfinite(v) else None for v in x]
-    out = {"workload": "kss_1m: 1M workers, 100k firms, 10 years, leave-one-out connected set; "
-                       "log_earn ~ age_squared + age_cubed | worker_id + firm_id",
+    out = {"workload": describe(args.kss_workload) + "; log_earn ~ age_squared + age_cubed | "
+                       "worker_id + firm_id",
            "rows": rows.n_rows, "levels": int(sum(rows.n_levels)), "S_nnz": S.nnz, "draws": p,
            "block": 32, "ms": round(ms, 3), "ms_leverages": round(ms_jla, 3),
            "ms_trace": round(ms_tr, 3), "ms_steps34": round(phases["steps34"], 3),

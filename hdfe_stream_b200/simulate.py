@@ -261,6 +261,10 @@ PANELS = {
     # 1M workers, 100k firms, 10 years, ~8.5 rows per worker (~8.5M rows)
     "kss_1m": dict(n_workers=1_000_000, n_firms=100_000, n_years=10, spell=(7, 10),
                    p_move=0.1),
+    # 100k workers, 10k firms, 10 years (~850k rows): the 1M-worker panel's
+    # shape at a tenth of the size, for kernel profiles
+    "kss_100k": dict(n_workers=100_000, n_firms=10_000, n_years=10, spell=(7, 10),
+                     p_move=0.1),
     # 400k workers, 40k firms, 10 years (~3.4M rows), weights U[0.5, 2]
     "akm_400k_w": dict(n_workers=400_000, n_firms=40_000, n_years=10, spell=(7, 10),
                        p_move=0.1, weights=True),
@@ -277,6 +281,6 @@ def prepare(name: str, seed: int = 0):
     panel = simulate_panel(seed=seed, **spec)
     if name == "akm_5m":
         return pass0_layout(panel, restrict_connected(panel, (2, 2)))
-    if name == "kss_1m":
+    if name.startswith("kss_"):
         return pass0_layout(panel, restrict_leave_one_out(panel), year_fe=False)
     return pass0_layout(panel)
