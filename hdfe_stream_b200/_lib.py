@@ -49,6 +49,14 @@ SIGNATURES = {
     "hdfe_sbuild_fill": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _vp, _i64,
                                     _i64, _vp, _vp, _vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp,
                                     _vp]),
+    "hdfe_sbuild_analyze_split": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp,
+                                             _vp, _i64, _i32, _vp, _i64, _vp, _vp]),
+    "hdfe_sbuild_count_split": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _vp,
+                                           _i64, _i64, _i64, _i32, _vp, _vp, _vp, _vp, _i64,
+                                           _vp, _i64, _vp, _i64, _vp, _vp]),
+    "hdfe_sbuild_fill_split": (_c.c_int, [_vp, _i64, _vp, _i32, _vp, _vp, _i64, _vp, _vp, _vp,
+                                          _i64, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
+                                          _i64, _vp, _vp]),
     "hdfe_components_workspace_bytes": (_i64, []),
     "hdfe_components": (_c.c_int, [_vp, _i64, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i64, _vp]),
     "hdfe_normalize_workspace_bytes": (_i64, [_i64, _i32]),

@@ -63,7 +63,7 @@ class FixedEffectsSolve:
                        None if X is None else X.detach(),
                        None if w is None else w.detach().to(torch.float64).contiguous(),
                        n_levels)
-        res = _fit.fit(rows, tol=tol)
+        res = _fit.fit(rows, tol=tol, small_block=False)     # the backward pass needs S whole
         op = InverseOperator(rows, res.cells, res.S, None if X is None else rows.V[1:].T,
                              tol=tol)
         A = op.residual_moments(res.gamma).cpu().numpy()

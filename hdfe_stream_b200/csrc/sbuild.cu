@@ -30,6 +30,12 @@
 //             each wide row is the compaction of its dense row (S is
 //             symmetric: the narrow rows' entries at the wide column), in
 //             column segments processed in parallel.
+// Split form (the *_split entry points, for hdfe_pcg_solve_small): the
+// trailing small dimensions' levels [small_first, L) are the wide rows, by
+// force; a narrow row adds its items at those columns into 16 direct slots
+// instead of the hash (the same additions in the same order) and writes them
+// as its row of `cross`; the wide x wide block goes to `small`; no wide row
+// is written to the CSR, which holds the big block only.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -106,7 +112,14 @@ struct Args {
     int64_t *indptr;
     int32_t *indices;
     double *data;
+    // split form: levels >= small_first are the small levels (L: no split)
+    int64_t small_first;
+    int ns;
+    double *cross;              // (small_first, kCross)
+    double *smallb;             // (ns, ns)
 };
+
+constexpr int kCross = HDFE_SMALL_MAX_LEVELS;     // cross's row stride
 
 __device__ __forceinline__ int level_dim(const Args &a, int64_t r)
 {
@@ -156,6 +169,12 @@ __global__ void __launch_bounds__(kThreads) k_classify(Args a)
         else if (cap <= kWarpSlots * 3 / 4 && lc <= kWarpListCap) k = kKindWarp;
         else if (cap <= kBlockSlots * 3 / 4 && lc <= kBlockListCap) k = kKindBlock;
         else k = kKindWide;
+        if (r >= a.small_first) {
+            k = kKindWide;                  // the split form's small levels
+        } else if (k == kKindWide && a.small_first < a.L) {
+            // a big row too wide for a narrow row: the split form cannot be built
+            atomicCAS(a.status, 0u, (unsigned)HDFE_ERR_CAPACITY);
+        }
         if (k == kKindWarp) {
             if (cap <= kSmallSlots * 3 / 4 && lc <= kSmallListCap)   // small rows from the front
                 a.warp_rows[atomicAdd((unsigned long long *)(a.ctr + 1), 1ull)] = (int32_t)r;
@@ -363,6 +382,7 @@ __device__ __forceinline__ void warp_sort(int32_t *key, double *val, int n, int 
 }
 
 struct RowSmem {
+    double *xs;         // kCross direct slots: the split form's small columns
     int32_t *keys;
     double *vals;
     int32_t *list;      // the row's groups
@@ -383,7 +403,9 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
     int bits = ceil_log2((cap * 4 + 2) / 3);
     bits = bits < 5 ? 5 : (bits > max_bits ? max_bits : bits);
     const int slots = 1 << bits;
+    const bool split = a.small_first < a.L;
     for (int i = lane; i < slots; i += 32) { sm.keys[i] = kEmptyKey; sm.vals[i] = 0.0; }
+    if (lane < kCross) sm.xs[lane] = 0.0;
     // the row's groups, ascending
     const int64_t l0 = a.lptr[r];
     const int nl = (int)(a.lptr[r + 1] - l0);
@@ -444,7 +466,11 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
             const int leader = __ffs(peers) - 1;
             sm.stage[lane] = v;
             __syncwarp();
-            if (valid && lane == leader) {
+            if (valid && lane == leader && split && col >= a.small_first) {
+                double sum = 0.0;
+                for (unsigned p = peers; p; p &= p - 1) sum += sm.stage[__ffs(p) - 1];
+                sm.xs[col - a.small_first] += sum;      // a direct slot, not the hash
+            } else if (valid && lane == leader) {
                 double sum = 0.0;
                 for (unsigned p = peers; p; p &= p - 1) sum += sm.stage[__ffs(p) - 1];
                 uint32_t h = slot_of(col, bits);
@@ -493,6 +519,7 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
             a.dval[(int64_t)k * a.L + r] = sm.vals[i];
         }
     }
+    if (split && lane < kCross) a.cross[r * kCross + lane] = sm.xs[lane];
     if (lane == 0) a.rnnz[r] = cnt;
     __syncwarp();
 }
@@ -500,6 +527,7 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
 // small warp rows (the front of warp_rows): 256-slot tables, 8 warps per CTA
 __global__ void __launch_bounds__(kSmallWarpsPerCta * 32) k_small_rows(Args a)
 {
+    __shared__ double s_xs[kSmallWarpsPerCta][kCross];
     __shared__ int32_t s_keys[kSmallWarpsPerCta][kSmallSlots];
     __shared__ double s_vals[kSmallWarpsPerCta][kSmallSlots];
     __shared__ int32_t s_list[kSmallWarpsPerCta][kSmallListCap];
@@ -509,7 +537,8 @@ __global__ void __launch_bounds__(kSmallWarpsPerCta * 32) k_small_rows(Args a)
     __shared__ double s_stage[kSmallWarpsPerCta][32];
     __shared__ int s_cnt[kSmallWarpsPerCta];
     const int w = threadIdx.x >> 5;
-    RowSmem sm{s_keys[w], s_vals[w], s_list[w], s_loff[w], s_gs[w], s_wv[w], s_stage[w], &s_cnt[w]};
+    RowSmem sm{s_xs[w], s_keys[w], s_vals[w], s_list[w], s_loff[w], s_gs[w], s_wv[w], s_stage[w],
+               &s_cnt[w]};
     const int64_t nrows = a.ctr[1];
     for (int64_t k = (int64_t)blockIdx.x * kSmallWarpsPerCta + w; k < nrows;
          k += (int64_t)gridDim.x * kSmallWarpsPerCta)
@@ -519,6 +548,7 @@ __global__ void __launch_bounds__(kSmallWarpsPerCta * 32) k_small_rows(Args a)
 // the other warp rows (the back of warp_rows): 512-slot tables
 __global__ void __launch_bounds__(kWarpsPerCta * 32) k_warp_rows(Args a)
 {
+    __shared__ double s_xs[kWarpsPerCta][kCross];
     __shared__ int32_t s_keys[kWarpsPerCta][kWarpSlots];
     __shared__ double s_vals[kWarpsPerCta][kWarpSlots];
     __shared__ int32_t s_list[kWarpsPerCta][kWarpListCap];
@@ -528,7 +558,8 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) k_warp_rows(Args a)
     __shared__ double s_stage[kWarpsPerCta][32];
     __shared__ int s_cnt[kWarpsPerCta];
     const int w = threadIdx.x >> 5;
-    RowSmem sm{s_keys[w], s_vals[w], s_list[w], s_loff[w], s_gs[w], s_wv[w], s_stage[w], &s_cnt[w]};
+    RowSmem sm{s_xs[w], s_keys[w], s_vals[w], s_list[w], s_loff[w], s_gs[w], s_wv[w], s_stage[w],
+               &s_cnt[w]};
     const int64_t nrows = a.ctr[6];
     for (int64_t k = (int64_t)blockIdx.x * kWarpsPerCta + w; k < nrows;
          k += (int64_t)gridDim.x * kWarpsPerCta)
@@ -546,8 +577,9 @@ __global__ void __launch_bounds__(32) k_block_rows(Args a)
     int32_t *list = keys + kBlockSlots;
     int32_t *loff = list + kBlockListCap;
     __shared__ double s_stage[32];
+    __shared__ double s_xs[kCross];
     __shared__ int s_cnt;
-    RowSmem sm{keys, vals, list, loff, gs, wv, s_stage, &s_cnt};
+    RowSmem sm{s_xs, keys, vals, list, loff, gs, wv, s_stage, &s_cnt};
     const int64_t nrows = a.ctr[2];
     for (int64_t k = blockIdx.x; k < nrows; k += gridDim.x)
         narrow_row(a, a.block_rows[k], sm, 13);
@@ -740,6 +772,10 @@ __global__ void __launch_bounds__(kThreads) k_wide_block_reduce(Args a)
         }
         sum = warp_sum(sum);
         p = __any_sync(0xffffffffu, p != 0);
+        if (a.small_first < a.L) {          // split form: the dense small block
+            if (lane == 0) a.smallb[en] = sum + a.wcross[en];
+            continue;
+        }
         if (!p || lane != 0) continue;
         const int64_t wa = en / a.W, wb = en % a.W;
         const int64_t lb = a.wide_list[wb];
@@ -939,6 +975,7 @@ int setup(Ctx &c, const int64_t *starts, int64_t G, const uint32_t *codes, int32
     }
     if (L >= INT32_MAX) return hdfe_set_arg_error("hdfe_sbuild: more than 2^31 levels");
     a.L = L;
+    a.small_first = L;
     Layout lay = layout(L, M, D);
     if (ws_bytes < lay.total) return hdfe_set_error(HDFE_ERR_WORKSPACE, "hdfe_sbuild: workspace too small");
     char *b = (char *)ws;
@@ -1004,6 +1041,24 @@ int scan_exclusive(Ctx &c, int64_t *x, int64_t n, int64_t *out, int64_t *total)
     return HDFE_OK;
 }
 
+// the split form: levels [small_first, L) (the trailing dimensions' levels,
+// at most kCross of them) are the small levels
+int set_split(Ctx &c, int64_t small_first, int32_t small_count, double *cross, double *small)
+{
+    Args &a = c.a;
+    bool at_dim = false;
+    for (int d = 0; d < a.D; d++) at_dim |= a.offs[d] == small_first;
+    if (small_count < 1 || small_count > kCross || small_first < 1 ||
+        small_first + small_count != a.L || !at_dim)
+        return hdfe_set_arg_error("hdfe_sbuild_*_split: the small levels must be the trailing "
+                                  "dimensions' levels, 1 to 16 of them, after at least one other");
+    a.small_first = small_first;
+    a.ns = small_count;
+    a.cross = cross;
+    a.smallb = small;
+    return HDFE_OK;
+}
+
 inline unsigned grid_for(int64_t items, int per_cta, int cap)
 {
     int64_t b = (items + per_cta - 1) / per_cta;
@@ -1034,18 +1089,20 @@ extern "C" int64_t hdfe_sbuild_wide_workspace_bytes(int64_t L, int64_t n_cells, 
     return wide_layout(n_wide, L, n_cells, D, wide_ctas_for(sms)).total;
 }
 
-extern "C" int hdfe_sbuild_analyze(const int64_t *starts, int64_t n_groups,
-                                   const uint32_t *codes, int32_t D, const double *n,
-                                   const double *group_n, int64_t n_cells,
-                                   const int64_t *n_levels, const int32_t *lcount,
-                                   const int64_t *work, void *workspace,
-                                   int64_t workspace_bytes, hdfe_sbuild_info *info, void *stream)
+static int analyze_impl(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                        int32_t D, const double *n, const double *group_n, int64_t n_cells,
+                        const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                        void *workspace, int64_t workspace_bytes, hdfe_sbuild_info *info,
+                        void *stream, int64_t small_first, int32_t small_count)
 {
     Ctx c;
     c.s = (cudaStream_t)stream;
     int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
                    workspace, workspace_bytes);
     if (st != HDFE_OK) return st;
+    if (small_count > 0 &&
+        (st = set_split(c, small_first, small_count, nullptr, nullptr)) != HDFE_OK)
+        return st;
     Args &a = c.a;
     Layout lay = layout(a.L, n_cells, D);
     char *b = (char *)workspace;
@@ -1074,28 +1131,65 @@ extern "C" int hdfe_sbuild_analyze(const int64_t *starts, int64_t n_groups,
     return HDFE_OK;
 }
 
-extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
-                                 int32_t D, const double *n, const double *group_n,
-                                 int64_t n_cells, const int64_t *n_levels, const int32_t *lcount,
-                                 const int64_t *work, int64_t n_wide, int64_t temp_len,
-                                 int64_t *indptr, void *workspace, int64_t workspace_bytes,
-                                 void *wide_workspace, int64_t wide_workspace_bytes, void *temp,
-                                 int64_t temp_bytes, hdfe_sbuild_info *info, void *stream)
+extern "C" int hdfe_sbuild_analyze(const int64_t *starts, int64_t n_groups,
+                                   const uint32_t *codes, int32_t D, const double *n,
+                                   const double *group_n, int64_t n_cells,
+                                   const int64_t *n_levels, const int32_t *lcount,
+                                   const int64_t *work, void *workspace,
+                                   int64_t workspace_bytes, hdfe_sbuild_info *info, void *stream)
+{
+    return analyze_impl(starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                        workspace, workspace_bytes, info, stream, 0, 0);
+}
+
+extern "C" int hdfe_sbuild_analyze_split(const int64_t *starts, int64_t n_groups,
+                                         const uint32_t *codes, int32_t D, const double *n,
+                                         const double *group_n, int64_t n_cells,
+                                         const int64_t *n_levels, const int32_t *lcount,
+                                         const int64_t *work, int64_t small_first,
+                                         int32_t small_count, void *workspace,
+                                         int64_t workspace_bytes, hdfe_sbuild_info *info,
+                                         void *stream)
+{
+    if (small_count < 1) return hdfe_set_arg_error("hdfe_sbuild_analyze_split: small_count < 1");
+    return analyze_impl(starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                        workspace, workspace_bytes, info, stream, small_first, small_count);
+}
+
+static int count_impl(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                      const double *n, const double *group_n, int64_t n_cells,
+                      const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                      int64_t n_wide, int64_t temp_len, int64_t *indptr, void *workspace,
+                      int64_t workspace_bytes, void *wide_workspace, int64_t wide_workspace_bytes,
+                      void *temp, int64_t temp_bytes, hdfe_sbuild_info *info, void *stream,
+                      int64_t small_first, int32_t small_count, double *cross, double *small)
 {
     Ctx c;
     c.s = (cudaStream_t)stream;
     int st = setup(c, starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
                    workspace, workspace_bytes);
     if (st != HDFE_OK) return st;
+    const bool split = small_count > 0;
+    if (split) {
+        if ((st = set_split(c, small_first, small_count, cross, small)) != HDFE_OK) return st;
+        if (!cross || !small || n_wide != small_count)
+            return hdfe_set_arg_error("hdfe_sbuild_count_split: cross / small missing, or "
+                                      "n_wide is not the number of small levels");
+    }
     if ((st = set_wide(c, n_wide, wide_workspace, wide_workspace_bytes)) != HDFE_OK) return st;
     if ((st = set_temp(c, temp, temp_bytes, temp_len)) != HDFE_OK) return st;
     if (!indptr) return hdfe_set_arg_error("hdfe_sbuild_count: indptr is null");
     Args &a = c.a;
     a.indptr = indptr;
     int launched = 0;
+    if (split) {
+        HDFE_CUDA_TRY(cudaMemsetAsync(cross, 0, small_first * kCross * 8, c.s));
+        HDFE_CUDA_TRY(cudaMemsetAsync(small, 0, (int64_t)small_count * small_count * 8, c.s));
+    }
     if (n_wide > 0) {
         WideLayout wl = wide_layout(n_wide, a.L, a.M, a.D, a.wide_ctas);
-        HDFE_CUDA_TRY(cudaMemsetAsync(wide_workspace, 0, wl.dpres + n_wide * a.L, c.s));
+        if (!split)     // the dense wide rows (the split form writes cross instead)
+            HDFE_CUDA_TRY(cudaMemsetAsync(wide_workspace, 0, wl.dpres + n_wide * a.L, c.s));
         HDFE_CUDA_TRY(cudaMemsetAsync((char *)wide_workspace + wl.wcross, 0,
                                       n_wide * n_wide * 8, c.s));
         k_cell_widx<<<grid_for(a.M * a.D, kThreads, c.sms * 8), kThreads, 0, c.s>>>(a);
@@ -1126,8 +1220,10 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
             k_wide_block_atomic<<<(unsigned)(c.sms * 8), kThreads, 0, c.s>>>(a);
             launched++;
         }
-        k_wide_count<<<grid_for(n_wide * a.nseg, 1, c.sms * 8), kThreads, 0, c.s>>>(a);
-        launched++;
+        if (!split) {
+            k_wide_count<<<grid_for(n_wide * a.nseg, 1, c.sms * 8), kThreads, 0, c.s>>>(a);
+            launched++;
+        }
     }
     HDFE_CUDA_TRY(cudaGetLastError());
     if ((st = scan_exclusive(c, a.rnnz, a.L, indptr, a.ctr + 4)) != HDFE_OK) return st;
@@ -1137,14 +1233,45 @@ extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const 
     return HDFE_OK;
 }
 
-extern "C" int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
-                                int32_t D, const double *n, const double *group_n,
-                                int64_t n_cells, const int64_t *n_levels, const int32_t *lcount,
-                                const int64_t *work, int64_t n_wide, int64_t temp_len,
-                                const int64_t *indptr, int32_t *indices, double *data,
-                                void *workspace, int64_t workspace_bytes, void *wide_workspace,
-                                int64_t wide_workspace_bytes, void *temp, int64_t temp_bytes,
-                                hdfe_sbuild_info *info, void *stream)
+extern "C" int hdfe_sbuild_count(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                                 int32_t D, const double *n, const double *group_n,
+                                 int64_t n_cells, const int64_t *n_levels, const int32_t *lcount,
+                                 const int64_t *work, int64_t n_wide, int64_t temp_len,
+                                 int64_t *indptr, void *workspace, int64_t workspace_bytes,
+                                 void *wide_workspace, int64_t wide_workspace_bytes, void *temp,
+                                 int64_t temp_bytes, hdfe_sbuild_info *info, void *stream)
+{
+    return count_impl(starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                      n_wide, temp_len, indptr, workspace, workspace_bytes, wide_workspace,
+                      wide_workspace_bytes, temp, temp_bytes, info, stream, 0, 0, nullptr,
+                      nullptr);
+}
+
+extern "C" int hdfe_sbuild_count_split(const int64_t *starts, int64_t n_groups,
+                                       const uint32_t *codes, int32_t D, const double *n,
+                                       const double *group_n, int64_t n_cells,
+                                       const int64_t *n_levels, const int32_t *lcount,
+                                       const int64_t *work, int64_t n_wide, int64_t temp_len,
+                                       int64_t small_first, int32_t small_count, int64_t *indptr,
+                                       double *cross, double *small, void *workspace,
+                                       int64_t workspace_bytes, void *wide_workspace,
+                                       int64_t wide_workspace_bytes, void *temp,
+                                       int64_t temp_bytes, hdfe_sbuild_info *info, void *stream)
+{
+    if (small_count < 1) return hdfe_set_arg_error("hdfe_sbuild_count_split: small_count < 1");
+    return count_impl(starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                      n_wide, temp_len, indptr, workspace, workspace_bytes, wide_workspace,
+                      wide_workspace_bytes, temp, temp_bytes, info, stream, small_first,
+                      small_count, cross, small);
+}
+
+static int fill_impl(const int64_t *starts, int64_t n_groups, const uint32_t *codes, int32_t D,
+                     const double *n, const double *group_n, int64_t n_cells,
+                     const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                     int64_t n_wide, int64_t temp_len, const int64_t *indptr, int32_t *indices,
+                     double *data, void *workspace, int64_t workspace_bytes, void *wide_workspace,
+                     int64_t wide_workspace_bytes, void *temp, int64_t temp_bytes,
+                     hdfe_sbuild_info *info, void *stream, bool split)
 {
     Ctx c;
     c.s = (cudaStream_t)stream;
@@ -1160,7 +1287,7 @@ extern "C" int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const u
     a.data = data;
     k_copy_narrow<<<(unsigned)(c.sms * 8), kThreads, 0, c.s>>>(a);
     int launched = 1;
-    if (n_wide > 0) {
+    if (n_wide > 0 && !split) {
         k_wide_fill<<<grid_for(n_wide * a.nseg, 1, c.sms * 8), kThreads, 0, c.s>>>(a);
         launched++;
     }
@@ -1168,4 +1295,34 @@ extern "C" int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const u
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(launched + 1);
     return HDFE_OK;
+}
+
+extern "C" int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                                int32_t D, const double *n, const double *group_n,
+                                int64_t n_cells, const int64_t *n_levels, const int32_t *lcount,
+                                const int64_t *work, int64_t n_wide, int64_t temp_len,
+                                const int64_t *indptr, int32_t *indices, double *data,
+                                void *workspace, int64_t workspace_bytes, void *wide_workspace,
+                                int64_t wide_workspace_bytes, void *temp, int64_t temp_bytes,
+                                hdfe_sbuild_info *info, void *stream)
+{
+    return fill_impl(starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                     n_wide, temp_len, indptr, indices, data, workspace, workspace_bytes,
+                     wide_workspace, wide_workspace_bytes, temp, temp_bytes, info, stream, false);
+}
+
+extern "C" int hdfe_sbuild_fill_split(const int64_t *starts, int64_t n_groups,
+                                      const uint32_t *codes, int32_t D, const double *n,
+                                      const double *group_n, int64_t n_cells,
+                                      const int64_t *n_levels, const int32_t *lcount,
+                                      const int64_t *work, int64_t n_wide, int64_t temp_len,
+                                      const int64_t *indptr, int32_t *indices, double *data,
+                                      void *workspace, int64_t workspace_bytes,
+                                      void *wide_workspace, int64_t wide_workspace_bytes,
+                                      void *temp, int64_t temp_bytes, hdfe_sbuild_info *info,
+                                      void *stream)
+{
+    return fill_impl(starts, n_groups, codes, D, n, group_n, n_cells, n_levels, lcount, work,
+                     n_wide, temp_len, indptr, indices, data, workspace, workspace_bytes,
+                     wide_workspace, wide_workspace_bytes, temp, temp_bytes, info, stream, true);
 }

@@ -21,7 +21,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from .gpu import BlockSolver, DeviceCSR, small_levels
+from .gpu import BlockSolver, DeviceCSR, SmallSplit, small_levels
 
 RHS_ZERO_TOL = 1e-11        # core/solve.py:44
 
@@ -191,6 +191,68 @@ def build_s(cells: DeviceCells, stream=None) -> DeviceCSR:
     return S
 
 
+def build_s_split(cells: DeviceCells, first: int, count: int, stream=None):
+    """S in the split form (`gpu.SmallSplit`: the big levels' block in CSR,
+    the dense cross and small blocks) built directly from the identifying
+    cells, with the values `build_s` followed by `hdfe_small_split` would
+    give; None when a big level is too wide for the build's narrow rows
+    (then build S whole and split it)."""
+    torch = _torch()
+    lib = _lib.lib()
+    dev = cells.starts.device
+    G = int(cells.starts.shape[0]) - 1
+    M = int(cells.codes.shape[0])
+    D = len(cells.n_levels)
+    L = cells.L
+    nlev = np.asarray(cells.n_levels, dtype=np.int64)
+    sh = _lib.stream_handle(stream)
+    ws = torch.empty(int(lib.hdfe_sbuild_workspace_bytes(L, M, D)), dtype=torch.uint8, device=dev)
+    info = torch.zeros(8, dtype=torch.int64, device=dev)
+    lc = None if cells.lcount is None else cells.lcount.data_ptr()
+    wk = None if cells.work is None else cells.work.data_ptr()
+    args = (cells.starts.data_ptr(), G, cells.codes.data_ptr(), D, cells.n.data_ptr(),
+            cells.group_n.data_ptr(), M, nlev.ctypes.data, lc, wk)
+    _lib.check(lib.hdfe_sbuild_analyze_split(*args, first, count, ws.data_ptr(), ws.numel(),
+                                             info.data_ptr(), sh))
+    inf = _lib.read_struct(_lib.SbuildInfo, info)
+    if inf.status == _lib.HDFE_ERR_CAPACITY:
+        return None
+    if inf.status != _lib.HDFE_OK:
+        raise _lib.HDFEError(inf.status, "S build: a level code is out of range")
+    W, T = int(inf.n_wide), int(inf.temp_len)
+    wide = torch.empty(max(int(lib.hdfe_sbuild_wide_workspace_bytes(L, M, D, W)), 256),
+                       dtype=torch.uint8, device=dev)
+    temp = torch.empty(max(T * 12, 16), dtype=torch.uint8, device=dev)
+    indptr = torch.empty(L + 1, dtype=torch.int64, device=dev)
+    cross = torch.empty((first, _lib.SMALL_MAX_LEVELS), dtype=torch.float64, device=dev)
+    small = torch.empty((count, count), dtype=torch.float64, device=dev)
+    _lib.check(lib.hdfe_sbuild_count_split(*args, W, T, first, count, indptr.data_ptr(),
+                                           cross.data_ptr(), small.data_ptr(), ws.data_ptr(),
+                                           ws.numel(), wide.data_ptr(), wide.numel(),
+                                           temp.data_ptr(), temp.numel(), info.data_ptr(), sh))
+    nnz = int(_lib.read_struct(_lib.SbuildInfo, info).nnz)
+    indices = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    data = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+    _lib.check(lib.hdfe_sbuild_fill_split(*args, W, T, indptr.data_ptr(), indices.data_ptr(),
+                                          data.data_ptr(), ws.data_ptr(), ws.numel(),
+                                          wide.data_ptr(), wide.numel(), temp.data_ptr(),
+                                          temp.numel(), info.data_ptr(), sh))
+    return SmallSplit.from_parts(DeviceCSR(indptr, indices[:nnz], data[:nnz], L, nnz), cross,
+                                 small, first, count)
+
+
+def build_fit_s(cells: DeviceCells, m: int, small_block=True):
+    """What the fit's solve takes: (S, split).  With a small trailing
+    dimension and at most PCG_SMALL_MAX_K variables, only the split form
+    (S None: `FitResult.S` builds the whole CSR when asked); else S whole."""
+    small = small_levels(cells.n_levels) if small_block else None
+    if small is not None and m <= _lib.PCG_SMALL_MAX_K:
+        split = build_s_split(cells, *small)
+        if split is not None:
+            return None, split
+    return build_s(cells), None
+
+
 def jacobi(diag):
     """core/solve.py:142-146 `_jacobi` on the device."""
     torch = _torch()
@@ -269,20 +331,26 @@ def normalize(gamma, cells: DeviceCells, root, stream=None):
     return gamma
 
 
-@dataclass
 class FitResult:
-    """Step 2's output for the estimator's own variables."""
+    """Step 2's output for the estimator's own variables: gamma (L, m) on
+    the device, normalised; info; the cells; S (the whole CSR: built on
+    first use when the solve ran on the split form only); the first
+    dimension's component roots; split (`gpu.SmallSplit`) or None."""
 
-    gamma: object               # (L, m) device tensor, normalised
-    info: dict
-    cells: DeviceCells
-    S: DeviceCSR
-    root: object
+    def __init__(self, gamma, info, cells: DeviceCells, S, root, split=None):
+        self.gamma, self.info, self.cells, self.root, self.split = gamma, info, cells, root, split
+        self._S = S
+
+    @property
+    def S(self) -> DeviceCSR:
+        if self._S is None:
+            self._S = build_s(self.cells)
+        return self._S
 
 
 def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8,
           x0=None, normalize_fe=True, timer=None, precision="fp64", comps=None,
-          solver="explicit", names=None, small_block=True) -> FitResult:
+          solver="explicit", names=None, small_block=True, split=None) -> FitResult:
     """`_SolveMixin._solve` (core/solve.py:294-368) on the device: zero
     right-hand sides (norm <= 1e-11 sqrt(total sum of squares)) solved by
     zero, block PCG per `rhs_block` columns, then `_normalize`.  `comps`:
@@ -290,7 +358,8 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     here.  `names`: the variables' names, for info["fe_spanned"].
     `small_block`: when the trailing dimensions have at most 16 levels in
     all (the years), the FP64 solve takes S with those levels' rows and
-    columns stored densely (`gpu.SmallSplit`, `hdfe_pcg_solve_small`).  The info
+    columns stored densely (`gpu.SmallSplit`, `hdfe_pcg_solve_small`);
+    `split`: that form already built (`build_fit_s`), S then may be None.  The info
     dict has the keys of core/solve.py:370-381 `_solve_info` (iterations,
     converged, blocks; max_rel_residual unless NaN; fe_spanned, the names
     of the variables the fixed effects span, only when there are any) and
@@ -304,7 +373,12 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
         solver = StreamSolver(cells, dinv, tol, maxiter)
     elif solver == "explicit":
         small = small_levels(cells.n_levels) if small_block and precision == "fp64" else None
-        solver = BlockSolver(S, dinv, tol, maxiter, precision=precision, small=small)
+        if split is not None or S is None:
+            small = None
+        if S is None and (split is None or precision != "fp64"):
+            S = build_s(cells)
+        solver = BlockSolver(S, dinv, tol, maxiter, precision=precision, small=small,
+                             split=split if precision == "fp64" else None)
         solver.timer = timer
     else:
         raise ValueError("solver must be 'explicit' or 'stream_cg'")
@@ -330,23 +404,28 @@ def solve(cells: DeviceCells, S: DeviceCSR, tol=1e-10, maxiter=5000, rhs_block=8
     n_comp = ncomp.cpu().numpy()
     if int(n_comp[1]) != _lib.HDFE_OK:
         raise _lib.HDFEError(int(n_comp[1]), "components: union-find failed")
-    explicit = S is not None and not hasattr(solver, "matvec")
+    explicit = not hasattr(solver, "matvec")
+    sp = getattr(solver, "split", None)
+    if explicit and S is not None:
+        nnz, mb = S.nnz, round(S.nbytes / 1e6, 1)
+    elif explicit:          # the split form only (its big block in info["small_block"])
+        nnz, mb = None, round(sp.nbytes / 1e6, 1)
+    else:
+        nnz = mb = None
     info = {"solver": "explicit" if explicit else "stream_cg", "device": "cuda",
             "iterations": its if len(its) > 1 else its[0],
             "converged": conv, "blocks": len(its),
-            "S_nnz": S.nnz if explicit else None,
-            "S_mb": round(S.nbytes / 1e6, 1) if explicit else None,
+            "S_nnz": nnz, "S_mb": mb,
             "n_components": int(n_comp[0])}
     if not np.isnan(rel):
         info["max_rel_residual"] = rel
-    if explicit and getattr(solver, "split", None) is not None:
-        sp = solver.split
+    if explicit and sp is not None:
         info["small_block"] = {"first": sp.first, "count": sp.count, "big_nnz": sp.S_big.nnz}
     names = list(names) if names else [f"v{j}" for j in range(m)]
     spanned = [names[j] for j in range(m) if zero_all[j]]
     if spanned:
         info["fe_spanned"] = spanned
-    return FitResult(gamma=gamma, info=info, cells=cells, S=S, root=root)
+    return FitResult(gamma=gamma, info=info, cells=cells, S=S, root=root, split=sp)
 
 
 class PhaseTimer:
@@ -388,19 +467,21 @@ class _NoTimer:
 
 
 def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None,
-        precision="fp64") -> FitResult:
+        precision="fp64", small_block=True) -> FitResult:
     """Pass 1, the S build and step 2 on the device, for device rows.
     precision "mixed": the PCG's inner iterations in FP32 with FP64
-    refinement to the same FP64 tolerance."""
+    refinement to the same FP64 tolerance.  small_block: with a trailing
+    dimension of at most 16 levels (the years) and at most 4 variables, S
+    is built in the split form the solve takes (`build_fit_s`)."""
     timer = timer or _NoTimer()
     with timer("pass1"):
         cells = pass1(rows)
     comps = components_async(cells)         # beside the S build
     with timer("sbuild"):
-        S = build_s(cells)
+        S, split = build_fit_s(cells, rows.m, small_block and precision == "fp64")
     with timer("solve"):
         return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
-                     comps=comps, names=rows.names)
+                     comps=comps, names=rows.names, split=split)
 
 
 _COPY_STREAMS = {}
@@ -482,7 +563,7 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
         shape = pass1(DeviceRows(g_d, c_d, empty, w_d, n_levels))
     comps = components_async(shape)         # the structure is all it reads
     with timer("sbuild"):
-        S = build_s(shape)
+        S, split = build_fit_s(shape, m, precision == "fp64")
     rhs, n_tot, mean, m2 = None, 0, None, None
     with timer("pass1"):
         for lo, hi, Vc, ev in chunks:
@@ -506,7 +587,7 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
     cells = dataclasses.replace(shape, rhs=rhs, means=mean, raw_ss=m2)
     with timer("solve"):
         return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
-                     comps=comps, names=names)
+                     comps=comps, names=names, split=split)
 
 
 def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):
@@ -632,9 +713,9 @@ def fit_stream(batches, n_levels, tol=1e-10, maxiter=5000, rhs_block=8, names=No
         del parts
     comps = components_async(cells)
     with timer("sbuild"):
-        S = build_s(cells)
+        S, split = build_fit_s(cells, int(cells.rhs.shape[1]), precision == "fp64")
     with timer("solve"):
         res = solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
-                    comps=comps, names=names)
+                    comps=comps, names=names, split=split)
     res.info["batches"] = len(batches)
     return res

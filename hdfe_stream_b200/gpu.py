@@ -92,6 +92,14 @@ class SmallSplit:
     (`S_big`), cross (first, 16) = S[r, first + j] and small (count, count)
     (`hdfe_small_split`)."""
 
+    @classmethod
+    def from_parts(cls, S_big: DeviceCSR, cross, small, first: int, count: int):
+        """The split form as built directly (`fit.build_s_split`)."""
+        self = cls.__new__(cls)
+        self.S_big, self.cross, self.small = S_big, cross, small
+        self.first, self.count = int(first), int(count)
+        return self
+
     def __init__(self, S: DeviceCSR, first: int, count: int, stream=None):
         import torch
         lib = _lib.lib()
@@ -132,19 +140,21 @@ class BlockSolver:
     exactly as the reference's `solve` (core/gpu.py:194-196)."""
 
     def __init__(self, S: DeviceCSR, dinv, tol: float, maxiter: int, debug=None,
-                 precision: str = "fp64", inner_tol: float = 1e-6, small=None):
+                 precision: str = "fp64", inner_tol: float = 1e-6, small=None, split=None):
         """precision "fp64" is the reference's solve; "mixed" runs the inner
         CG in FP32 with FP64 iterative refinement (hdfe_pcg_solve_mixed),
         stopping on the same FP64 relative residual `tol`.  small: (first,
         count) of a dense small block (`small_levels`), used by the FP64
-        solves of at most PCG_SMALL_MAX_K columns (`hdfe_pcg_solve_small`)."""
+        solves of at most PCG_SMALL_MAX_K columns (`hdfe_pcg_solve_small`);
+        split: that form already built (`SmallSplit`), in which case S may be
+        None when no solve is wider than PCG_SMALL_MAX_K columns."""
         import torch
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.precision, self.inner_tol = precision, float(inner_tol)
         self.S = S
         self._data32 = S.data.float() if precision == "mixed" else None
-        self.dev = S.indptr.device
+        self.dev = (S if S is not None else split.S_big).indptr.device
         self.dinv = torch.as_tensor(np.asarray(dinv, dtype=np.float64)).to(self.dev) \
             if not torch.is_tensor(dinv) else dinv.to(self.dev, torch.float64).contiguous()
         self.tol, self.maxiter, self.debug = float(tol), int(maxiter), debug
@@ -152,8 +162,8 @@ class BlockSolver:
         self._info = torch.zeros(3, dtype=torch.float64, device=self.dev)   # 24 bytes
         self._zero = torch.zeros(_lib.PCG_MAX_K, dtype=torch.uint8, device=self.dev)
         self.stats = {"launches": 0, "iterations": 0}     # solves so far (for the roofline)
-        self.split = None
-        if small is not None and precision == "fp64":
+        self.split = split if precision == "fp64" else None
+        if self.split is None and small is not None and precision == "fp64":
             try:
                 self.split = SmallSplit(S, *small)
             except _lib.HDFEError as e:
@@ -167,7 +177,8 @@ class BlockSolver:
         if k not in self._ws:
             size = (_lib.lib().hdfe_pcg_mixed_workspace_bytes if self.precision == "mixed"
                     else _lib.lib().hdfe_pcg_workspace_bytes)
-            nbytes = size(self.S.L, self.S.nnz, k)
+            A = self.S if self.S is not None else self.split.S_big
+            nbytes = size(A.L, A.nnz, k)
             if nbytes < 0:
                 raise _lib.HDFEError(_lib.HDFE_ERR_CUDA, "could not size the PCG workspace")
             self._ws[k] = torch.empty(int(nbytes), dtype=torch.uint8, device=self.dev)
@@ -192,6 +203,9 @@ class BlockSolver:
                 k, zp, x0p, self.tol, self.maxiter, X.data_ptr(), ws.data_ptr(), ws.numel(),
                 self._info.data_ptr(), _lib.stream_handle(stream)))
             return
+        if self.S is None:
+            raise ValueError(f"a {k}-column solve needs S's CSR; this solver holds only the "
+                             "split form")
         if self.precision == "mixed":
             _lib.check(_lib.lib().hdfe_pcg_solve_mixed(
                 self.S.indptr.data_ptr(), self.S.indices.data_ptr(), self.S.data.data_ptr(),

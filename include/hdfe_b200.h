@@ -135,6 +135,41 @@ int hdfe_sbuild_fill(const int64_t *starts, int64_t n_groups, const uint32_t *co
                      void *wide_workspace, int64_t wide_workspace_bytes, void *temp,
                      int64_t temp_bytes, hdfe_sbuild_info *info, void *stream);
 
+/* The same build in the split form hdfe_pcg_solve_small takes (see the
+ * dense small block below): the levels [small_first, L), the trailing
+ * dimensions' levels (1 .. HDFE_SMALL_MAX_LEVELS of them), are the wide rows
+ * by force; the CSR (indptr over all L rows, rows >= small_first empty)
+ * holds S's big block only, cross (small_first x HDFE_SMALL_MAX_LEVELS) and
+ * small (small_count x small_count) the rest, with the very values of the
+ * full build (the same additions in the same order).  n_wide must be
+ * small_count.  info->status is HDFE_ERR_CAPACITY when a big level is too
+ * wide for a narrow row (then build the full CSR and split it with
+ * hdfe_small_split).  The workspaces are sized as for the full build. */
+int hdfe_sbuild_analyze_split(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                              int32_t D, const double *n, const double *group_n,
+                              int64_t n_cells, const int64_t *n_levels, const int32_t *lcount,
+                              const int64_t *work, int64_t small_first, int32_t small_count,
+                              void *workspace, int64_t workspace_bytes, hdfe_sbuild_info *info,
+                              void *stream);
+
+int hdfe_sbuild_count_split(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                            int32_t D, const double *n, const double *group_n, int64_t n_cells,
+                            const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                            int64_t n_wide, int64_t temp_len, int64_t small_first,
+                            int32_t small_count, int64_t *indptr, double *cross, double *small,
+                            void *workspace, int64_t workspace_bytes, void *wide_workspace,
+                            int64_t wide_workspace_bytes, void *temp, int64_t temp_bytes,
+                            hdfe_sbuild_info *info, void *stream);
+
+int hdfe_sbuild_fill_split(const int64_t *starts, int64_t n_groups, const uint32_t *codes,
+                           int32_t D, const double *n, const double *group_n, int64_t n_cells,
+                           const int64_t *n_levels, const int32_t *lcount, const int64_t *work,
+                           int64_t n_wide, int64_t temp_len, const int64_t *indptr,
+                           int32_t *indices, double *data, void *workspace,
+                           int64_t workspace_bytes, void *wide_workspace,
+                           int64_t wide_workspace_bytes, void *temp, int64_t temp_bytes,
+                           hdfe_sbuild_info *info, void *stream);
+
 /* ------------------------------------------------ components, normalisation
  *
  * hdfe_components: union-find over dimension `col` of the identifying cells

@@ -268,3 +268,33 @@ def test_fit_stream_matches_one_pass(device, name, batch_rows):
     ref = orc.pass1(rows)
     g_ref, _ = orc.solve(ref, orc.build_explicit(ref), tol=1e-12)
     assert np.max(np.abs(g - g_ref)) / np.max(np.abs(g_ref)) < 1e-8
+
+
+@pytest.mark.parametrize("name,rows", PANELS, ids=[p[0] for p in PANELS])
+def test_split_build_equals_split_of_whole_s(device, name, rows):
+    """The S build in the split form (`fit.build_s_split`: the years' levels
+    forced wide, their columns of the firm rows summed in direct slots) gives
+    bit for bit what the whole build followed by `hdfe_small_split` gives,
+    and the fit on it matches the fit on the whole S."""
+    import torch
+    from hdfe_stream_b200 import fit, gpu
+    cells = fit.pass1(fit.DeviceRows.from_rows(rows))
+    small = gpu.small_levels(cells.n_levels)
+    assert small is not None
+    direct = fit.build_s_split(cells, *small)
+    assert direct is not None
+    whole = gpu.SmallSplit(fit.build_s(cells), *small)
+    for a, b in ((direct.S_big.indptr, whole.S_big.indptr),
+                 (direct.S_big.indices, whole.S_big.indices),
+                 (direct.S_big.data, whole.S_big.data), (direct.cross, whole.cross)):
+        assert torch.equal(a, b)
+    # the years' own block: when the whole build takes the years as narrow
+    # rows (small panels), their entries are summed in another order
+    d = float((direct.small - whole.small).abs().max() / whole.small.abs().max())
+    assert d < 1e-13, d
+    res = fit.fit(fit.DeviceRows.from_rows(rows), tol=1e-12)
+    assert res.split is not None and res.info["small_block"]["count"] == small[1]
+    plain = fit.fit(fit.DeviceRows.from_rows(rows), tol=1e-12, small_block=False)
+    assert plain.split is None
+    assert float((res.gamma - plain.gamma).abs().max() / plain.gamma.abs().max()) < 1e-9
+    assert torch.equal(res.S.indices, plain.S.indices)       # the lazily built whole S
