@@ -157,9 +157,10 @@ def phase_bytes(rows, counts, S, iterations, m=3, small=None):
     design notes): pass 1 reads each row once and writes the identifying
     cells and level arrays; the S build reads the cells and writes S; one
     PCG iteration reads S and streams the L x k vectors.  small: the fit's
-    info["small_block"] when the PCG ran on the split S -- the big block's
-    CSR, the dense cross block (first x 16 doubles) read once, and the big
-    rows' products with the small levels written and read back (16 L m)."""
+    info["small_block"] when S was built and solved in the split form -- the
+    build writes the big block's CSR and the dense cross block (first x 16
+    doubles); an iteration reads them once and writes and reads back the big
+    rows' products with the small levels (16 first m)."""
     N, D, L = rows.n_rows, rows.codes.shape[1], int(sum(rows.n_levels))
     M, G = counts["n_ident_cells"], counts["n_ident_groups"]
     w = 0 if rows.w is None else 8
@@ -167,6 +168,8 @@ def phase_bytes(rows, counts, S, iterations, m=3, small=None):
     sb = M * (4 * D + 8) + G * 16 + S.nnz * 12 + (L + 1) * 8
     per_it = 12 * S.nnz + 8 * (L + 1) + 8 * L * m * 9
     if small:
+        sb = (M * (4 * D + 8) + G * 16 + small["big_nnz"] * 12 + (L + 1) * 8
+              + 8 * 16 * small["first"])
         per_it = (12 * small["big_nnz"] + 8 * (L + 1) + 8 * 16 * small["first"]
                   + 8 * L * m * 9 + 16 * small["first"] * m)
     return {"pass1": p1, "sbuild": sb, "pcg_kernel": per_it * max(iterations, 1)}
