@@ -154,12 +154,26 @@ __host__ __device__ inline int stage_doubles(int D, int c) { return (BP * D + 1)
 
 // dynamic shared memory of the staged passes, in doubles: C (kMaxCov x 32),
 // the sub-warps' covariate sums ([SUBS][kMaxCov][BP]: lane j of a sub-warp owns
-// column j of its slot, so no two lanes add to one entry), then the staging
+// column j of its slot, so no two lanes add to one entry), the staging, then
+// each sub-warp's window slots ([kWin][BP + 1]: the window's gathered values,
+// lane j reading and writing only its own column, so the loop over the
+// window's rows need not be unrolled to keep them in registers -- the
+// unrolled bodies overflowed the instruction cache)
 template <int BP>
 __host__ __device__ inline int pass_smem_bytes(int D, int c)
 {
-    return (kMaxCov * 32 + kPassThreads * kMaxCov + (kPassThreads / BP) * stage_doubles<BP>(D, c)) *
+    return (kMaxCov * 32 + kPassThreads * kMaxCov + (kPassThreads / BP) * stage_doubles<BP>(D, c) +
+            (kPassThreads / BP) * kWin * (BP + 1)) *
            8;
+}
+
+// this lane's window slots: slot u at [u * (BP + 1)]
+template <int BP>
+__device__ __forceinline__ double *win_slots(const Args &a, double *s_dyn)
+{
+    constexpr int SUBS = kPassThreads / BP;
+    return s_dyn + kMaxCov * 32 + kPassThreads * kMaxCov + SUBS * stage_doubles<BP>(a.D, a.c) +
+           (threadIdx.x / BP) * kWin * (BP + 1) + threadIdx.x % BP;
 }
 
 template <int BP>
@@ -235,6 +249,7 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_reduce(Args a)
     const Lanes<BP> ln(a.B);
     const Stage st = stage_area<BP>(a, s_dyn);
     double *ax = cov_slot<BP>(s_dyn);
+    double *ws = win_slots<BP>(a, s_dyn);
     cov_zero(s_dyn);
     __syncthreads();
     const int64_t g0 = (int64_t)blockIdx.x * SUBS + threadIdx.x / BP;
@@ -264,22 +279,24 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_reduce(Args a)
             if (c0 > 0) __syncwarp(ln.mask);
             const double wl = stage_rows<BP>(a, ln, st, s + c0, m, nullptr);
             for (int q0 = 0; q0 < m; q0 += kWin) {
-                double r[kWin];
+                if (!a.streamed) {                   // explicit rows: every load first
+                    double r[kWin];
 #pragma unroll
-                for (int u = 0; u < kWin; u++) {     // explicit rows: every load first
-                    const int q = q0 + u;
-                    r[u] = rho;
-                    if (!a.streamed) r[u] = (q < m && ln.on) ? __ldg(a.R + (s + c0 + q) * a.B + ln.j)
-                                                             : 0.0;
+                    for (int u = 0; u < kWin; u++) {
+                        const int q = q0 + u;
+                        r[u] = (q < m && ln.on) ? __ldg(a.R + (s + c0 + q) * a.B + ln.j) : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < kWin; u++) ws[u * (BP + 1)] = r[u];
                 }
-#pragma unroll
-                for (int u = 0; u < kWin; u++) {
+                const int nw = min(kWin, m - q0);
+#pragma unroll 1
+                for (int u = 0; u < nw; u++) {
                     const int q = q0 + u;
-                    if (q >= m) break;
                     const double wi = __shfl_sync(ln.mask, wl, q, BP);
                     uint32_t c[HDFE_MAX_DIMS];
                     staged_codes(a, st, q, c);
-                    const double v = wi * r[u];
+                    const double v = wi * (a.streamed ? rho : ws[u * (BP + 1)]);
                     run_add(a, run, c, v, ln.j, ln.on);
                     gs += v;
                     for (int cc = 0; cc < a.c; cc++) ax[cc * BP] += st.x[q * a.c + cc] * v;
@@ -306,12 +323,15 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_project_coef(Args a)
     const Lanes<BP> ln(a.B);
     const Stage st = stage_area<BP>(a, s_dyn);
     double *ax = cov_slot<BP>(s_dyn);
+    double *ws = win_slots<BP>(a, s_dyn);
     cov_zero(s_dyn);
     for (int k = threadIdx.x; k < a.c * a.B; k += kPassThreads) s_C[k] = a.C[k];
     __syncthreads();
     const int64_t g0 = (int64_t)blockIdx.x * SUBS + threadIdx.x / BP;
     const int64_t gstep = (int64_t)gridDim.x * SUBS;
-    auto gather = [&](int q0, int m, double (&h)[kWin]) {
+    // the window's U sums into this lane's slots, every gather issued first
+    auto gather = [&](int q0, int m) {
+        double h[kWin];
 #pragma unroll
         for (int u = 0; u < kWin; u++) {
             const int q = q0 + u;
@@ -322,6 +342,8 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_project_coef(Args a)
             }
             h[u] = v;
         }
+#pragma unroll
+        for (int u = 0; u < kWin; u++) ws[u * (BP + 1)] = h[u];
     };
     auto h_cov = [&](int q) {
         double v = 0.0;
@@ -338,15 +360,14 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_project_coef(Args a)
             if (c0 > 0) __syncwarp(ln.mask);
             wl = stage_rows<BP>(a, ln, st, s + c0, m, &om);
             for (int q0 = 0; q0 < m; q0 += kWin) {
-                double h[kWin];
-                gather(q0, m, h);
-#pragma unroll
-                for (int u = 0; u < kWin; u++) {
+                gather(q0, m);
+                const int nw = min(kWin, m - q0);
+#pragma unroll 1
+                for (int u = 0; u < nw; u++) {
                     const int q = q0 + u;
-                    if (q >= m) break;
                     const double wi = __shfl_sync(ln.mask, wl, q, BP);
                     sw += wi;
-                    swh += wi * (h[u] + h_cov(q));
+                    swh += wi * (ws[u * (BP + 1)] + h_cov(q));
                 }
             }
         }
@@ -369,13 +390,12 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_project_coef(Args a)
                 wl = stage_rows<BP>(a, ln, st, s + c0, m, &om);
             }
             for (int q0 = 0; q0 < m; q0 += kWin) {
-                double h[kWin];
-                gather(q0, m, h);
-#pragma unroll
-                for (int u = 0; u < kWin; u++) {
+                gather(q0, m);
+                const int nw = min(kWin, m - q0);
+#pragma unroll 1
+                for (int u = 0; u < nw; u++) {
                     const int q = q0 + u;
-                    if (q >= m) break;
-                    const double o = h[u] + h_cov(q) + mean;
+                    const double o = ws[u * (BP + 1)] + h_cov(q) + mean;
                     const int64_t i = s + c0 + q;
                     if (a.rows && ln.on) a.rows[i * a.B + ln.j] = o;
                     if (a.collect) {

@@ -474,15 +474,20 @@ __device__ __forceinline__ void load_small(const Params &a, const double *V, dou
     __syncthreads();
 }
 
-// The big rows against the small levels, grid-strided two rows a warp, a lane
-// per small level (j = lane % 16): AP2[r] = cross[r] . ps (a 16-lane sum) and,
-// per lane, col[k] += cross[r, j] V[r, k] (the small rows' products, summed
-// over rows).  dot[k] += V[r, k] AP2[r, k] when want_dot.  The lanes' column
+// The big rows against the small levels, a lane per small level (j = lane %
+// 16), a half-warp per row: AP2[r] = cross[r] . ps (a 16-lane sum) and, per
+// lane, col[k] += cross[r, j] V[r, k] (the small rows' products, summed over
+// rows).  dot[k] += V[r, k] AP2[r, k] when want_dot.  A warp takes
+// dense_rows_per_trip(K) rows per trip (rows r0 + 2u + half), all their loads
+// issued before any is used; the trips are grid-strided.  The lanes' column
 // sums go to s_col[warp] (kSmall x K).
+__host__ __device__ constexpr int dense_rows_per_trip(int k) { return k <= 2 ? 2 : 8; }
 template <int K, int VS>
 __device__ __forceinline__ void dense_rows(const Params &a, const double *V, const double *s_ps,
                                            double *s_col, double (&dot)[K], bool want_dot)
 {
+    constexpr int kDenseRows = dense_rows_per_trip(K);
+    constexpr int RU = kDenseRows / 2;
     const int lane = threadIdx.x & 31, half = lane >> 4, j = lane & 15;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int64_t W = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -492,26 +497,35 @@ __device__ __forceinline__ void dense_rows(const Params &a, const double *V, con
         psj[k] = j < a.ns ? s_ps[j * K + k] : 0.0;
         col[k] = 0.0;
     }
-    for (int64_t r2 = 2 * gw; r2 < a.Lb; r2 += 2 * W) {        // warp-uniform trips
-        const int64_t r = r2 + half;
-        const bool in = r < a.Lb;
-        const double b = in ? __ldcs(a.cross + r * kSmall + j) : 0.0;
-        double pr[K], t[K];
+    for (int64_t r0 = kDenseRows * gw; r0 < a.Lb; r0 += kDenseRows * W) {   // warp-uniform
+        double b[RU], pr[RU][K];
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            pr[k] = in ? V[r * VS + k] : 0.0;
-            t[k] = b * psj[k];
-            col[k] += b * pr[k];
+        for (int u = 0; u < RU; u++) {
+            const int64_t r = r0 + 2 * u + half;
+            const bool in = r < a.Lb;
+            b[u] = in ? __ldcs(a.cross + r * kSmall + j) : 0.0;
+#pragma unroll
+            for (int k = 0; k < K; k++) pr[u][k] = in ? V[r * VS + k] : 0.0;
         }
 #pragma unroll
-        for (int k = 0; k < K; k++)
-#pragma unroll
-            for (int o = 8; o > 0; o >>= 1) t[k] += __shfl_xor_sync(kFull, t[k], o);
-        if (in && j == 0) {
+        for (int u = 0; u < RU; u++) {
+            const int64_t r = r0 + 2 * u + half;
+            double t[K];
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                a.AP2[r * K + k] = t[k];
-                if (want_dot) dot[k] += pr[k] * t[k];
+                t[k] = b[u] * psj[k];
+                col[k] += b[u] * pr[u][k];
+            }
+#pragma unroll
+            for (int k = 0; k < K; k++)
+#pragma unroll
+                for (int o = 8; o > 0; o >>= 1) t[k] += __shfl_xor_sync(kFull, t[k], o);
+            if (r < a.Lb && j == 0) {
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    a.AP2[r * K + k] = t[k];
+                    if (want_dot) dot[k] += pr[u][k] * t[k];
+                }
             }
         }
     }

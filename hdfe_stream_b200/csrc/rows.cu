@@ -307,7 +307,11 @@ __global__ void __launch_bounds__(kPassThreads) k_center(Args a)
 // covariates to shared memory, the weight to a register) and walked in windows
 // of kWin rows: the window's U gathers (one coalesced BP-wide row of U each)
 // are all issued before any is used, so a sub-warp has kWin gathers in flight
-// instead of one dependent gather per row.  The JLA sums go through a
+// instead of one dependent gather per row; their sums are parked in the
+// window's shared-memory slots (each lane its own), so the loop over the
+// window's rows runs without unrolling (the unrolled body did not fit the
+// instruction cache: most issue slots were lost waiting for instructions).
+// The JLA sums go through a
 // shared-memory transpose per window: each lane stores its P and M for the
 // window's rows, then lane t sums row t's values over the draws in draw order
 // and adds them to the running moments, whose old values it loaded when the
@@ -370,9 +374,11 @@ __global__ void __launch_bounds__(kProjThreads, 4) k_project(Args a)
         __syncwarp(ln.mask);
         return w;
     };
-    // sum_d U[level_d(q), j] for the window's rows q0 .. q0 + kWin - 1 (< m),
-    // every gather issued before the first is used
-    auto gather = [&](int q0, int m, double (&hU)[kWin]) {
+    // sum_d U[level_d(q), j] for the window's rows q0 .. q0 + kWin - 1 (< m)
+    // into slot u of hs (this lane's column), every gather issued before the
+    // first is used
+    auto gather = [&](int q0, int m, double *hs) {
+        double hU[kWin];
 #pragma unroll
         for (int u = 0; u < kWin; u++) {
             const int q = q0 + u;
@@ -383,6 +389,8 @@ __global__ void __launch_bounds__(kProjThreads, 4) k_project(Args a)
             }
             hU[u] = h;
         }
+#pragma unroll
+        for (int u = 0; u < kWin; u++) hs[u * (BP + 1) + ln.j] = hU[u];
     };
     auto h_cov = [&](int q) {
         double h = 0.0;
@@ -406,16 +414,17 @@ __global__ void __launch_bounds__(kProjThreads, 4) k_project(Args a)
             const double wl = stage(s + c0, m);
             const double irl = inv_root(a, wl);
             for (int q0 = 0; q0 < m; q0 += kWin) {
-                double hU[kWin];
-                gather(q0, m, hU);
-#pragma unroll
-                for (int u = 0; u < kWin; u++) {
+                gather(q0, m, s_P);
+                const int nw = min(kWin, m - q0);
+#pragma unroll 1
+                for (int u = 0; u < nw; u++) {
                     const int q = q0 + u;
-                    if (q >= m) break;
                     const double wi = __shfl_sync(ln.mask, wl, q, BP);
                     const double ir = __shfl_sync(ln.mask, irl, q, BP);
                     sw += wi;
-                    if (ln.on) tot += wi * (draw(s + c0 + q) * ir - (hU[u] + h_cov(q)));
+                    if (ln.on)
+                        tot += wi * (draw(s + c0 + q) * ir -
+                                     (s_P[u * (BP + 1) + ln.j] + h_cov(q)));
                 }
             }
             if (c0 + BP < n) __syncwarp(ln.mask);   // the next chunk reuses the staging
@@ -440,16 +449,14 @@ __global__ void __launch_bounds__(kProjThreads, 4) k_project(Args a)
 #pragma unroll
                     for (int k = 0; k < 5; k++) mom[k] = a.moments[k * a.N + ir];
                 }
-                double hU[kWin];
-                gather(q0, m, hU);
-#pragma unroll
-                for (int u = 0; u < kWin; u++) {
+                gather(q0, m, s_P);
+#pragma unroll 1
+                for (int u = 0; u < nw; u++) {
                     const int q = q0 + u;
-                    if (q >= m) break;
                     const double wi = __shfl_sync(ln.mask, wl, q, BP);
                     if (!ln.on) continue;
                     const int64_t i = s + c0 + q;
-                    double o = hU[u] + h_cov(q) + mean;
+                    double o = s_P[u * (BP + 1) + ln.j] + h_cov(q) + mean;
                     if (a.sqrt_weights) o *= sqrt(wi);
                     if (a.out) a.out[i * a.B + ln.j] = o;
                     if (a.moments) {

@@ -10,7 +10,7 @@
 //           big entries copied (coalesced), the small-column entries of big
 //           rows scattered into cross, the small rows' small-column entries
 //           into small (their big-column entries are cross transposed: S is
-//           symmetric).
+//           symmetric; columns are sorted, so those are a prefix of the row).
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -144,10 +144,18 @@ __global__ void __launch_bounds__(kThreads) k_fill(const int64_t *indptr, const 
                 done += __popc(m);
             }
         } else {
-            for (int64_t e = st + lane; e < en; e += 32) {
+            // a small row: its small-column entries are the row's tail (sorted
+            // columns), found by a binary search rather than a walk over the
+            // row's big columns (a year meets every firm)
+            int64_t lo = st, hi = en;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (indices[mid] < Lb) lo = mid + 1; else hi = mid;
+            }
+            for (int64_t e = lo + lane; e < en; e += 32) {
                 const int32_t c = indices[e];
                 if (c >= Lb && c < Lb + ns) small[(r - Lb) * ns + (c - Lb)] = data[e];
-                else if (c < 0 || c >= Lb + ns) atomicExch(status, (int32_t)HDFE_ERR_BAD_CODE);
+                else atomicExch(status, (int32_t)HDFE_ERR_BAD_CODE);
             }
         }
     }
