@@ -71,7 +71,8 @@ def describe(name):
     if p.get("weights"):
         text += ", weights U[0.5, 2]"
     restriction = "leave-one-out connected set" if name.startswith("kss_") else \
-        {"akm_5m": "largest connected set with min_degree=2"}.get(name)
+        {"akm_5m": "largest connected set with min_degree=2",
+         "akm_2m": "largest connected set with min_degree=2"}.get(name)
     return text + (f", {restriction}" if restriction else "")
 
 

@@ -258,6 +258,10 @@ PANELS = {
     # 5M workers, 500k firms, 15 years, ~8.5 rows per worker (~42M rows)
     "akm_5m": dict(n_workers=5_000_000, n_firms=500_000, n_years=15, spell=(5, 12),
                    p_move=0.08),
+    # 2M workers, 200k firms, 15 years: the 5M-worker panel's shape at 2/5 of
+    # the size (S and the vectors still larger than L2), for kernel profiles
+    "akm_2m": dict(n_workers=2_000_000, n_firms=200_000, n_years=15, spell=(5, 12),
+                   p_move=0.08),
     # 1M workers, 100k firms, 10 years, ~8.5 rows per worker (~8.5M rows)
     "kss_1m": dict(n_workers=1_000_000, n_firms=100_000, n_years=10, spell=(7, 10),
                    p_move=0.1),
@@ -279,7 +283,7 @@ def prepare(name: str, seed: int = 0):
     age_cubed | worker_id + firm_id)."""
     spec = dict(PANELS[name])
     panel = simulate_panel(seed=seed, **spec)
-    if name == "akm_5m":
+    if name in ("akm_5m", "akm_2m"):
         return pass0_layout(panel, restrict_connected(panel, (2, 2)))
     if name.startswith("kss_"):
         return pass0_layout(panel, restrict_leave_one_out(panel), year_fe=False)
