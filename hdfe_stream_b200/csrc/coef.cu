@@ -138,276 +138,135 @@ __device__ __forceinline__ void run_add(const Args &a, Runs &run, const uint32_t
     run.v += v;
 }
 
-// Rows staged per sub-warp, BP at a time (lane t: row i0 + t): codes and
-// covariates in shared memory, the weight and omega in registers; the group's
-// rows are then walked from there, so a row costs no dependent global load.
-constexpr int kPassThreads = 256;
-constexpr int kWin = 8;         // rows whose U gathers are in flight together
-
-struct Stage {
-    uint32_t *codes;    // [BP][D]
-    double *x;          // [BP][c]
-};
-
-template <int BP>
-__host__ __device__ inline int stage_doubles(int D, int c) { return (BP * D + 1) / 2 + BP * c; }
-
-// dynamic shared memory of the staged passes, in doubles: C (kMaxCov x 32),
-// the sub-warps' covariate sums ([SUBS][kMaxCov][BP]: lane j of a sub-warp owns
-// column j of its slot, so no two lanes add to one entry), the staging, then
-// each sub-warp's window slots ([kWin][BP + 1]: the window's gathered values,
-// lane j reading and writing only its own column, so the loop over the
-// window's rows need not be unrolled to keep them in registers -- the
-// unrolled bodies overflowed the instruction cache)
-template <int BP>
-__host__ __device__ inline int pass_smem_bytes(int D, int c)
+// the covariate block: per thread, then per CTA, then one add per entry
+__device__ __forceinline__ void flush_cov(const Args &a, const double (&ax)[kMaxCov], double *s_ax,
+                                          int j, bool on)
 {
-    return (kMaxCov * 32 + kPassThreads * kMaxCov + (kPassThreads / BP) * stage_doubles<BP>(D, c) +
-            (kPassThreads / BP) * kWin * (BP + 1)) *
-           8;
-}
-
-// this lane's window slots: slot u at [u * (BP + 1)]
-template <int BP>
-__device__ __forceinline__ double *win_slots(const Args &a, double *s_dyn)
-{
-    constexpr int SUBS = kPassThreads / BP;
-    return s_dyn + kMaxCov * 32 + kPassThreads * kMaxCov + SUBS * stage_doubles<BP>(a.D, a.c) +
-           (threadIdx.x / BP) * kWin * (BP + 1) + threadIdx.x % BP;
-}
-
-template <int BP>
-__device__ __forceinline__ Stage stage_area(const Args &a, double *s_dyn)
-{
-    double *area = s_dyn + kMaxCov * 32 + kPassThreads * kMaxCov +
-                   (threadIdx.x / BP) * stage_doubles<BP>(a.D, a.c);
-    return Stage{reinterpret_cast<uint32_t *>(area), area + (BP * a.D + 1) / 2};
-}
-
-// this lane's covariate sums: slot [sub-warp][c][lane]
-template <int BP>
-__device__ __forceinline__ double *cov_slot(double *s_dyn)
-{
-    return s_dyn + kMaxCov * 32 + (threadIdx.x / BP) * kMaxCov * BP + threadIdx.x % BP;
-}
-
-__device__ __forceinline__ void cov_zero(double *s_dyn)
-{
-    for (int k = threadIdx.x; k < kPassThreads * kMaxCov; k += kPassThreads)
-        s_dyn[kMaxCov * 32 + k] = 0.0;
-}
-
-// acc_x[c, j] += the CTA's sums, over its sub-warps in a fixed order
-template <int BP>
-__device__ __forceinline__ void cov_flush(const Args &a, const double *s_dyn)
-{
-    constexpr int SUBS = kPassThreads / BP;
+    for (int k = threadIdx.x; k < a.c * a.B; k += kThreads) s_ax[k] = 0.0;
     __syncthreads();
-    for (int k = threadIdx.x; k < a.c * a.B; k += kPassThreads) {
-        const int c = k / a.B, j = k % a.B;
-        double t = 0.0;
-        for (int q = 0; q < SUBS; q++) t += s_dyn[kMaxCov * 32 + (q * kMaxCov + c) * BP + j];
-        if (t != 0.0) atomicAdd(a.acc_x + k, t);
-    }
-}
-
-// load rows i0 .. i0 + m - 1; returns this lane's row weight (and omega)
-template <int BP>
-__device__ __forceinline__ double stage_rows(const Args &a, const Lanes<BP> &ln, const Stage &st,
-                                             int64_t i0, int m, double *omega)
-{
-    double w = 1.0;
-    if (omega) *omega = 1.0;
-    if (ln.j < m) {
-        const int64_t i = i0 + ln.j;
-        if (a.w) w = __ldg(a.w + i);
-        if (omega && a.omega) *omega = __ldg(a.omega + i);
-        uint32_t c[HDFE_MAX_DIMS];
-        row_codes(a, i, c);
-        for (int d = 0; d < a.D; d++) st.codes[ln.j * a.D + d] = c[d];
-        for (int cc = 0; cc < a.c; cc++) st.x[ln.j * a.c + cc] = __ldg(a.X + i * a.c + cc);
-    }
-    __syncwarp(ln.mask);
-    return w;
-}
-
-__device__ __forceinline__ void staged_codes(const Args &a, const Stage &st, int q,
-                                             uint32_t (&c)[HDFE_MAX_DIMS])
-{
+    if (on) {
 #pragma unroll
-    for (int d = 0; d < HDFE_MAX_DIMS; d++) {
-        if (d >= a.D) break;
-        c[d] = st.codes[q * a.D + d];
+        for (int c = 0; c < kMaxCov; c++) {
+            if (c >= a.c) break;
+            atomicAdd(s_ax + c * a.B + j, ax[c]);
+        }
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < a.c * a.B; k += kThreads)
+        if (s_ax[k] != 0.0) atomicAdd(a.acc_x + k, s_ax[k]);
 }
 
 template <int BP>
-__global__ void __launch_bounds__(kPassThreads, 4) k_reduce(Args a)
+__global__ void __launch_bounds__(kThreads) k_reduce(Args a)
 {
-    constexpr int SUBS = kPassThreads / BP;
-    extern __shared__ double s_dyn[];
+    constexpr int SUBS = kThreads / BP;
+    __shared__ double s_ax[kMaxCov * 32];
     const Lanes<BP> ln(a.B);
-    const Stage st = stage_area<BP>(a, s_dyn);
-    double *ax = cov_slot<BP>(s_dyn);
-    double *ws = win_slots<BP>(a, s_dyn);
-    cov_zero(s_dyn);
-    __syncthreads();
     const int64_t g0 = (int64_t)blockIdx.x * SUBS + threadIdx.x / BP;
     const int64_t gstep = (int64_t)gridDim.x * SUBS;
+    double ax[kMaxCov];
+#pragma unroll
+    for (int c = 0; c < kMaxCov; c++) ax[c] = 0.0;
     for (int64_t g = g0; g < a.G; g += gstep) {
-        const int64_t s = __ldg(a.starts + g), e = __ldg(a.starts + g + 1);
-        const int n = (int)(e - s);
-        // rho: the streamed value spread over the group by its weight
-        double sw = 0.0;
+        const int64_t s = a.starts[g], e = a.starts[g + 1];
+        double rho = 0.0;
         if (a.streamed) {
-            if (a.w) {
-                for (int c0 = 0; c0 < n; c0 += BP) {
-                    double wl = (c0 + ln.j < n) ? __ldg(a.w + s + c0 + ln.j) : 0.0;
-                    for (int o = BP / 2; o > 0; o >>= 1) wl += __shfl_xor_sync(ln.mask, wl, o, BP);
-                    sw += wl;
-                }
-            } else {
-                sw = (double)n;
-            }
+            const double sw = group_weight(a, s, e);
+            rho = (ln.on && sw > 0.0) ? a.streamed[g * a.B + ln.j] / sw : 0.0;
         }
-        const double rho = (a.streamed && ln.on && sw > 0.0) ? __ldg(a.streamed + g * a.B + ln.j) / sw
-                                                            : 0.0;
         Runs run{};
         double gs = 0.0;
-        for (int c0 = 0; c0 < n; c0 += BP) {
-            const int m = min(BP, n - c0);
-            if (c0 > 0) __syncwarp(ln.mask);
-            const double wl = stage_rows<BP>(a, ln, st, s + c0, m, nullptr);
-            for (int q0 = 0; q0 < m; q0 += kWin) {
-                if (!a.streamed) {                   // explicit rows: every load first
-                    double r[kWin];
+        for (int64_t i = s; i < e; i++) {
+            uint32_t c[HDFE_MAX_DIMS];
+            row_codes(a, i, c);
+            const double wi = a.w ? __ldg(a.w + i) : 1.0;
+            const double r = a.streamed ? rho : (ln.on ? a.R[i * a.B + ln.j] : 0.0);
+            const double v = wi * r;
+            run_add(a, run, c, v, ln.j, ln.on);
+            gs += v;
 #pragma unroll
-                    for (int u = 0; u < kWin; u++) {
-                        const int q = q0 + u;
-                        r[u] = (q < m && ln.on) ? __ldg(a.R + (s + c0 + q) * a.B + ln.j) : 0.0;
-                    }
-#pragma unroll
-                    for (int u = 0; u < kWin; u++) ws[u * (BP + 1)] = r[u];
-                }
-                const int nw = min(kWin, m - q0);
-#pragma unroll 1
-                for (int u = 0; u < nw; u++) {
-                    const int q = q0 + u;
-                    const double wi = __shfl_sync(ln.mask, wl, q, BP);
-                    uint32_t c[HDFE_MAX_DIMS];
-                    staged_codes(a, st, q, c);
-                    const double v = wi * (a.streamed ? rho : ws[u * (BP + 1)]);
-                    run_add(a, run, c, v, ln.j, ln.on);
-                    gs += v;
-                    for (int cc = 0; cc < a.c; cc++) ax[cc * BP] += st.x[q * a.c + cc] * v;
-                }
+            for (int cc = 0; cc < kMaxCov; cc++) {
+                if (cc >= a.c) break;
+                ax[cc] += __ldg(a.X + i * a.c + cc) * v;
             }
         }
         if (run.have && ln.on) run_flush(a, run, ln.j);
         if (a.gsum && ln.on) a.gsum[g * a.B + ln.j] = gs;
-        __syncwarp(ln.mask);
     }
-    if (a.acc_x && a.c > 0) cov_flush<BP>(a, s_dyn);
+    if (a.acc_x && a.c > 0) flush_cov(a, ax, s_ax, ln.j, ln.on);
 }
 
-// h_ij = sum_d U[level_d(i), j] + X_i . C[:, j]; pass 1: u0[g, j] = rho - the
-// weighted group mean of h; pass 2: the rows' (A u)_ij = h + u0 and the
-// collect sink, both from the staged rows, the U gathers of kWin rows issued
-// together.
 template <int BP>
-__global__ void __launch_bounds__(kPassThreads, 4) k_project_coef(Args a)
+__global__ void __launch_bounds__(kThreads) k_project_coef(Args a)
 {
-    constexpr int SUBS = kPassThreads / BP;
-    extern __shared__ double s_dyn[];
-    double *s_C = s_dyn;
+    constexpr int SUBS = kThreads / BP;
+    __shared__ double s_ax[kMaxCov * 32];
+    __shared__ double s_C[kMaxCov * 32];
     const Lanes<BP> ln(a.B);
-    const Stage st = stage_area<BP>(a, s_dyn);
-    double *ax = cov_slot<BP>(s_dyn);
-    double *ws = win_slots<BP>(a, s_dyn);
-    cov_zero(s_dyn);
-    for (int k = threadIdx.x; k < a.c * a.B; k += kPassThreads) s_C[k] = a.C[k];
+    for (int k = threadIdx.x; k < a.c * a.B; k += kThreads) s_C[k] = a.C[k];
     __syncthreads();
     const int64_t g0 = (int64_t)blockIdx.x * SUBS + threadIdx.x / BP;
     const int64_t gstep = (int64_t)gridDim.x * SUBS;
-    // the window's U sums into this lane's slots, every gather issued first
-    auto gather = [&](int q0, int m) {
-        double h[kWin];
+    double ax[kMaxCov];
 #pragma unroll
-        for (int u = 0; u < kWin; u++) {
-            const int q = q0 + u;
-            double v = 0.0;
-            if (q < m && ln.on) {
-                for (int d = 0; d < a.D; d++)
-                    v += __ldg(a.U + (a.offs[d] + st.codes[q * a.D + d]) * a.B + ln.j);
-            }
-            h[u] = v;
-        }
+    for (int c = 0; c < kMaxCov; c++) ax[c] = 0.0;
+    auto h_of = [&](int64_t i, const uint32_t (&c)[HDFE_MAX_DIMS], double &hU, Runs &key) {
+        // sum_d U[level_d(i), j], read again only when the codes change
+        if (!key.have || !same(a, key.codes, c)) {
+            hU = 0.0;
+            if (ln.on) {
 #pragma unroll
-        for (int u = 0; u < kWin; u++) ws[u * (BP + 1)] = h[u];
-    };
-    auto h_cov = [&](int q) {
-        double v = 0.0;
-        for (int cc = 0; cc < a.c; cc++) v += st.x[q * a.c + cc] * s_C[cc * a.B + ln.j];
-        return v;
-    };
-    for (int64_t g = g0; g < a.G; g += gstep) {
-        const int64_t s = __ldg(a.starts + g), e = __ldg(a.starts + g + 1);
-        const int n = (int)(e - s);
-        // pass 1: the group's weight and weighted sum of h
-        double sw = 0.0, swh = 0.0, wl = 1.0, om = 1.0;
-        for (int c0 = 0; c0 < n; c0 += BP) {
-            const int m = min(BP, n - c0);
-            if (c0 > 0) __syncwarp(ln.mask);
-            wl = stage_rows<BP>(a, ln, st, s + c0, m, &om);
-            for (int q0 = 0; q0 < m; q0 += kWin) {
-                gather(q0, m);
-                const int nw = min(kWin, m - q0);
-#pragma unroll 1
-                for (int u = 0; u < nw; u++) {
-                    const int q = q0 + u;
-                    const double wi = __shfl_sync(ln.mask, wl, q, BP);
-                    sw += wi;
-                    swh += wi * (ws[u * (BP + 1)] + h_cov(q));
+                for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+                    if (d >= a.D) break;
+                    hU += a.U[(a.offs[d] + c[d]) * a.B + ln.j];
                 }
             }
+#pragma unroll
+            for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+                if (d >= a.D) break;
+                key.codes[d] = c[d];
+            }
+            key.have = true;
         }
-        const double rho = (a.streamed && ln.on && sw > 0.0) ? __ldg(a.streamed + g * a.B + ln.j) / sw
-                                                            : 0.0;
-        const double mean = sw > 0.0 ? rho - swh / sw : 0.0;
+        double h = hU;
+        if (ln.on)
+            for (int cc = 0; cc < a.c; cc++) h += __ldg(a.X + i * a.c + cc) * s_C[cc * a.B + ln.j];
+        return h;
+    };
+    for (int64_t g = g0; g < a.G; g += gstep) {
+        const int64_t s = a.starts[g], e = a.starts[g + 1];
+        const double sw = group_weight(a, s, e);
+        const double rho = (a.streamed && ln.on && sw > 0.0) ? a.streamed[g * a.B + ln.j] / sw : 0.0;
+        // pass 1: the group's mean of rho - h
+        double tot = 0.0, hU = 0.0;
+        Runs key{};
+        for (int64_t i = s; i < e; i++) {
+            uint32_t c[HDFE_MAX_DIMS];
+            row_codes(a, i, c);
+            const double wi = a.w ? __ldg(a.w + i) : 1.0;
+            tot += wi * (rho - h_of(i, c, hU, key));
+        }
+        const double mean = sw > 0.0 ? tot / sw : 0.0;
         if (a.groups && ln.on) a.groups[g * a.B + ln.j] = mean;
-        if (!a.rows && !a.collect) {
-            __syncwarp(ln.mask);
-            continue;
-        }
-        // pass 2: the rows, and the collect sink (a group of one chunk keeps
-        // its staged rows)
+        if (!a.rows && !a.collect) continue;
+        // pass 2: the rows, and the collect sink
+        key.have = false;
         Runs run{};
         double gs = 0.0;
-        for (int c0 = 0; c0 < n; c0 += BP) {
-            const int m = min(BP, n - c0);
-            if (n > BP) {
-                __syncwarp(ln.mask);
-                wl = stage_rows<BP>(a, ln, st, s + c0, m, &om);
-            }
-            for (int q0 = 0; q0 < m; q0 += kWin) {
-                gather(q0, m);
-                const int nw = min(kWin, m - q0);
-#pragma unroll 1
-                for (int u = 0; u < nw; u++) {
-                    const int q = q0 + u;
-                    const double o = ws[u * (BP + 1)] + h_cov(q) + mean;
-                    const int64_t i = s + c0 + q;
-                    if (a.rows && ln.on) a.rows[i * a.B + ln.j] = o;
-                    if (a.collect) {
-                        const double wi = __shfl_sync(ln.mask, wl, q, BP);
-                        const double oi = __shfl_sync(ln.mask, om, q, BP);
-                        const double v = wi * oi * o;
-                        uint32_t c[HDFE_MAX_DIMS];
-                        staged_codes(a, st, q, c);
-                        run_add(a, run, c, v, ln.j, ln.on);
-                        gs += v;
-                        for (int cc = 0; cc < a.c; cc++) ax[cc * BP] += st.x[q * a.c + cc] * v;
-                    }
+        for (int64_t i = s; i < e; i++) {
+            uint32_t c[HDFE_MAX_DIMS];
+            row_codes(a, i, c);
+            const double o = h_of(i, c, hU, key) + mean;
+            if (a.rows && ln.on) a.rows[i * a.B + ln.j] = o;
+            if (a.collect) {
+                const double wi = a.w ? __ldg(a.w + i) : 1.0;
+                const double v = wi * (a.omega ? __ldg(a.omega + i) : 1.0) * o;
+                run_add(a, run, c, v, ln.j, ln.on);
+                gs += v;
+#pragma unroll
+                for (int cc = 0; cc < kMaxCov; cc++) {
+                    if (cc >= a.c) break;
+                    ax[cc] += __ldg(a.X + i * a.c + cc) * v;
                 }
             }
         }
@@ -415,9 +274,8 @@ __global__ void __launch_bounds__(kPassThreads, 4) k_project_coef(Args a)
             if (run.have && ln.on) run_flush(a, run, ln.j);
             if (a.gsum && ln.on) a.gsum[g * a.B + ln.j] = gs;
         }
-        __syncwarp(ln.mask);
     }
-    if (a.collect && a.acc_x && a.c > 0) cov_flush<BP>(a, s_dyn);
+    if (a.collect && a.acc_x && a.c > 0) flush_cov(a, ax, s_ax, ln.j, ln.on);
 }
 
 // ---------------------------------------------------------- trace moments
@@ -553,29 +411,6 @@ inline unsigned grid_for(int64_t G, int Bp)
     return (unsigned)(b > 0 ? b : 1);
 }
 
-// the staged passes' grid: two waves of four resident CTAs per SM at most
-// (the rest grid-stride)
-inline unsigned pass_grid(int64_t G, int Bp)
-{
-    const int64_t per = kPassThreads / Bp;
-    int64_t b = (G + per - 1) / per;
-    if (b > 148 * 8) b = 148 * 8;
-    return (unsigned)(b > 0 ? b : 1);
-}
-
-template <int BP>
-void launch_reduce(const Args &a, cudaStream_t s)
-{
-    k_reduce<BP><<<pass_grid(a.G, BP), kPassThreads, pass_smem_bytes<BP>(a.D, a.c), s>>>(a);
-}
-
-template <int BP>
-void launch_project_coef(const Args &a, cudaStream_t s)
-{
-    k_project_coef<BP><<<pass_grid(a.G, BP), kPassThreads, pass_smem_bytes<BP>(a.D, a.c), s>>>(
-        a);
-}
-
 }  // namespace coef
 }  // namespace hdfe
 
@@ -600,9 +435,10 @@ extern "C" int hdfe_rows_reduce(const int64_t *starts, int64_t n_groups, const u
     a.acc_x = acc_x;
     a.gsum = group_sums;
     cudaStream_t s = (cudaStream_t)stream;
-    if (a.Bp == 8) coef::launch_reduce<8>(a, s);
-    else if (a.Bp == 16) coef::launch_reduce<16>(a, s);
-    else coef::launch_reduce<32>(a, s);
+    const unsigned grid = coef::grid_for(n_groups, a.Bp);
+    if (a.Bp == 8) coef::k_reduce<8><<<grid, coef::kThreads, 0, s>>>(a);
+    else if (a.Bp == 16) coef::k_reduce<16><<<grid, coef::kThreads, 0, s>>>(a);
+    else coef::k_reduce<32><<<grid, coef::kThreads, 0, s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
     return HDFE_OK;
@@ -632,9 +468,10 @@ extern "C" int hdfe_rows_project_coef(const int64_t *starts, int64_t n_groups,
     a.acc_x = acc_x;
     a.gsum = group_sums;
     cudaStream_t s = (cudaStream_t)stream;
-    if (a.Bp == 8) coef::launch_project_coef<8>(a, s);
-    else if (a.Bp == 16) coef::launch_project_coef<16>(a, s);
-    else coef::launch_project_coef<32>(a, s);
+    const unsigned grid = coef::grid_for(n_groups, a.Bp);
+    if (a.Bp == 8) coef::k_project_coef<8><<<grid, coef::kThreads, 0, s>>>(a);
+    else if (a.Bp == 16) coef::k_project_coef<16><<<grid, coef::kThreads, 0, s>>>(a);
+    else coef::k_project_coef<32><<<grid, coef::kThreads, 0, s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
     return HDFE_OK;
@@ -725,9 +562,10 @@ extern "C" int hdfe_stream_matvec(const int64_t *starts, int64_t n_groups, const
     a.acc = out;
     cudaStream_t s = (cudaStream_t)stream;
     HDFE_CUDA_TRY(cudaMemsetAsync(out, 0, a.L * k * 8, s));
-    if (a.Bp == 8) coef::launch_project_coef<8>(a, s);
-    else if (a.Bp == 16) coef::launch_project_coef<16>(a, s);
-    else coef::launch_project_coef<32>(a, s);
+    const unsigned grid = coef::grid_for(n_groups, a.Bp);
+    if (a.Bp == 8) coef::k_project_coef<8><<<grid, coef::kThreads, 0, s>>>(a);
+    else if (a.Bp == 16) coef::k_project_coef<16><<<grid, coef::kThreads, 0, s>>>(a);
+    else coef::k_project_coef<32><<<grid, coef::kThreads, 0, s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
     return HDFE_OK;

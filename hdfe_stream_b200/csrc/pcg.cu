@@ -329,12 +329,19 @@ __device__ __forceinline__ void finish_row(int64_t row, const T (&acc)[K], int64
 
 // out = S V over this warp's range of nonzeros (rows inside the range),
 // partial sums of cut rows to the carry slots, dot[k] += V[r] . (S V)[r]
-// (in FP64 whatever T is).  vals are S's values in T.
-template <int K, int VS, int VW, typename T>
+// (in FP64 whatever T is).  vals are S's values in T.  Short rows go LPR
+// lanes each, 32 / LPR rows side by side: a short row costs two dependent
+// round trips (its indices and values, then its gathers) whatever its length
+// up to LPR x the unroll, so matrices of short rows (S's big block once the
+// years are split off: ~16 nonzeros a row) run with 4 lanes a row and twice
+// the rows in flight.
+template <int K, int VS, int VW, typename T, int LPR = 8>
 __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T *__restrict__ V,
                            T *__restrict__ out, T *carry, double (&dot)[K], bool want_dot)
 {
-    const int lane = threadIdx.x & 31, sub = lane >> 3, sl = lane & 7;
+    static_assert(LPR == 4 || LPR == 8, "short rows take 4 or 8 lanes");
+    constexpr int RPS = 32 / LPR;       // short rows per step
+    const int lane = threadIdx.x & 31, sub = lane / LPR, sl = lane % LPR;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int64_t lo = a.wlo[gw];
     const int64_t hi = a.wlo[gw + 1];
@@ -373,10 +380,10 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
                                      dot, want_dot);
                 j++;
             } else {
-                // up to four short rows, one per 8-lane subgroup, up to the next long row
+                // up to RPS short rows, one per LPR-lane subgroup, up to the next long row
                 const unsigned ahead = longmask & (0xffffffffu << j);
-                int batch = ahead ? (__ffs(ahead) - 1 - j) : 4;
-                batch = min(min(batch, 4), nrows - j);
+                int batch = ahead ? (__ffs(ahead) - 1 - j) : RPS;
+                batch = min(min(batch, RPS), nrows - j);
                 const int src = min(j + sub, 31);
                 const bool mine = sub < batch;
                 const int64_t rs = __shfl_sync(kFull, cs, src), re = __shfl_sync(kFull, ce, src);
@@ -389,13 +396,11 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
                 T acc[K];
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = T(0);
-                if (mine) row_products<K, VS, VW, 8, T>(a, vals, V, rs + sl, re, acc);
+                if (mine) row_products<K, VS, VW, LPR, T>(a, vals, V, rs + sl, re, acc);
 #pragma unroll
-                for (int k = 0; k < K; k++) {
-                    acc[k] += __shfl_xor_sync(kFull, acc[k], 4);
-                    acc[k] += __shfl_xor_sync(kFull, acc[k], 2);
-                    acc[k] += __shfl_xor_sync(kFull, acc[k], 1);
-                }
+                for (int k = 0; k < K; k++)
+#pragma unroll
+                    for (int o = LPR / 2; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(kFull, acc[k], o);
                 if (mine && sl == 0 && re > rs)
                     finish_row<K, T>(r0 + j + sub, acc, row_st, row_en, lo, hi, gw, vrow, out,
                                      carry, dot, want_dot);
@@ -591,7 +596,7 @@ __device__ __forceinline__ void dense_small_rows(const Params &a, const double *
     __syncthreads();
 }
 
-template <int K>
+template <int K, int LPR = 8>
 __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 {
     constexpr int KP = Stride<K>::P;
@@ -637,7 +642,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 #pragma unroll
     for (int k = 0; k < K; k++) dot[k] = 0.0;
     if (a.X0 != nullptr) {
-        spmm_range<K, K, 1, double>(a, a.data, a.X0, a.AP, a.carry, dot, false);
+        spmm_range<K, K, 1, double, LPR>(a, a.data, a.X0, a.AP, a.carry, dot, false);
         if (a.ns > 0) {
             load_small<K, K>(a, a.X0, s_ps);
             dense_rows<K, K>(a, a.X0, s_ps, s_col, dot, false);
@@ -730,7 +735,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
             for (int k = 0; k < K; k++) dot[k] = 0.0;
             // P's rows are KP wide from a 256-byte aligned workspace: 32-byte
             // rows for k = 3, 4
-            spmm_range<K, KP, (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1), double>(
+            spmm_range<K, KP, (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1), double, LPR>(
                 a, a.data, a.P, a.AP, a.carry, dot, true);
             if (a.ns > 0) {
                 load_small<K, KP>(a, a.P, s_ps);
@@ -939,13 +944,16 @@ int grid_blocks_for(int k)
     return cache[dev][k];
 }
 
-template <int K>
+template <int K, int LPR = 8>
 cudaError_t launch(Params p, int blocks, cudaStream_t s)
 {
     void *args[] = {&p};
-    return cudaLaunchCooperativeKernel((const void *)pcg_kernel<K>, dim3(blocks), dim3(threads_for(K)),
-                                       args, 0, s);
+    return cudaLaunchCooperativeKernel((const void *)pcg_kernel<K, LPR>, dim3(blocks),
+                                       dim3(threads_for(K)), args, 0, s);
 }
+
+// 4 lanes a short row when S's rows average at most this many nonzeros
+constexpr int64_t kShortRowNnz = 24;
 
 // ------------------------------------------------ one column per lane
 //
@@ -1571,11 +1579,12 @@ int solve_registers(const int64_t *indptr, const int32_t *indices, const double 
     pcg::k_partition<<<(unsigned)((p.nwarps + 256) / 256), 256, 0, s>>>(indptr, L, nnz, p.nwarps,
                                                                       pcg::kRowCost, (int64_t *)p.wlo);
     cudaError_t e = cudaErrorInvalidValue;
+    const bool short_rows = nnz <= pcg::kShortRowNnz * L;
     switch (k) {
-    case 1: e = pcg::launch<1>(p, blocks, s); break;
-    case 2: e = pcg::launch<2>(p, blocks, s); break;
-    case 3: e = pcg::launch<3>(p, blocks, s); break;
-    case 4: e = pcg::launch<4>(p, blocks, s); break;
+    case 1: e = short_rows ? pcg::launch<1, 4>(p, blocks, s) : pcg::launch<1>(p, blocks, s); break;
+    case 2: e = short_rows ? pcg::launch<2, 4>(p, blocks, s) : pcg::launch<2>(p, blocks, s); break;
+    case 3: e = short_rows ? pcg::launch<3, 4>(p, blocks, s) : pcg::launch<3>(p, blocks, s); break;
+    case 4: e = short_rows ? pcg::launch<4, 4>(p, blocks, s) : pcg::launch<4>(p, blocks, s); break;
     case 5: e = pcg::launch<5>(p, blocks, s); break;
     case 6: e = pcg::launch<6>(p, blocks, s); break;
     case 7: e = pcg::launch<7>(p, blocks, s); break;

@@ -298,192 +298,157 @@ __global__ void __launch_bounds__(kPassThreads) k_center(Args a)
     }
 }
 
-// `_nb_project_rows` and the JLA sink, one sub-warp of BP lanes per group
-// (lane j: draw j).  h_ij = sum_d U[level_d(i), j] + X_i . C[:, j]; pass 1:
-// the weighted group mean of r - h; pass 2: the projection o_ij (times
-// sqrt(w_i) in the square-root weight metric), written to out and/or turned
-// into the sink's P = o^2 and M = (r - o)^2.
-//   The group's rows are staged BP at a time (lane t loads row t: codes and
-// covariates to shared memory, the weight to a register) and walked in windows
-// of kWin rows: the window's U gathers (one coalesced BP-wide row of U each)
-// are all issued before any is used, so a sub-warp has kWin gathers in flight
-// instead of one dependent gather per row; their sums are parked in the
-// window's shared-memory slots (each lane its own), so the loop over the
-// window's rows runs without unrolling (the unrolled body did not fit the
-// instruction cache: most issue slots were lost waiting for instructions).
-// The JLA sums go through a
-// shared-memory transpose per window: each lane stores its P and M for the
-// window's rows, then lane t sums row t's values over the draws in draw order
-// and adds them to the running moments, whose old values it loaded when the
-// window began.
-constexpr int kProjThreads = 256;
-constexpr int kWin = 8;
-
-struct ProjLayout {     // dynamic shared memory of k_project, in doubles
-    int chunk;          // per sub-warp: staged codes (BP x D u32) and covariates (BP x c)
-    int win;            // per sub-warp: P and M of one window, [2][kWin][BP + 1]
-    int c_off;          // C (c x B) first, then the sub-warps' areas
-    int total_bytes;
-};
-
+// `_nb_project_rows` and the JLA sink, one sub-warp of BP lanes per group.
+// h_ij = sum_d U[level_d(i), j] (loaded once per run of equal codes) +
+// X_i . C[:, j]; pass 1: the weighted group mean of r - h; pass 2: the
+// projection o_ij (times sqrt(w_i) in the square-root weight metric), written
+// to out and/or turned into the sink's P = o^2 and M = (r - o)^2.  The five
+// per-row sums over the block's draws go through shared memory: each lane
+// stores its P and M for up to MR rows, then lane t sums row t's values in
+// draw order and adds them to the running moments.
 template <int BP>
-__host__ __device__ inline ProjLayout proj_layout(int D, int c)
+__global__ void __launch_bounds__(kPassThreads) k_project(Args a)
 {
-    ProjLayout o;
-    o.chunk = (BP * D + 1) / 2 + BP * c;
-    o.win = 2 * kWin * (BP + 1);
-    o.c_off = kMaxCov * 32;
-    o.total_bytes = (o.c_off + (kProjThreads / BP) * (o.chunk + o.win)) * 8;
-    return o;
-}
-
-template <int BP>
-__global__ void __launch_bounds__(kProjThreads, 4) k_project(Args a)
-{
-    constexpr int SUBS = kProjThreads / BP;
+    constexpr int SUBS = kPassThreads / BP;
+    constexpr int MR = BP < 16 ? BP : 16;                 // rows per moment flush
     extern __shared__ double s_dyn[];
     const Lanes<BP> ln(a.B);
     const int subw = threadIdx.x / BP;
-    const ProjLayout lay = proj_layout<BP>(a.D, a.c);
-    double *s_C = s_dyn;
-    double *area = s_dyn + lay.c_off + subw * (lay.chunk + lay.win);
-    uint32_t *s_codes = reinterpret_cast<uint32_t *>(area);          // [BP][D]
-    double *s_x = area + (BP * a.D + 1) / 2;                          // [BP][c]
-    double *s_P = area + lay.chunk;                                   // [kWin][BP + 1]
-    double *s_M = s_P + kWin * (BP + 1);
-    for (int k = threadIdx.x; k < a.c * a.B; k += kProjThreads) s_C[k] = a.C[k];
+    double *s_C = s_dyn;                                   // (c, B)
+    double *s_mom = s_dyn + kMaxCov * 32 + subw * (MR * (BP + 1) * 2);   // [2][MR][BP+1]
+    char *s_chunks = reinterpret_cast<char *>(s_dyn + kMaxCov * 32 + SUBS * MR * (BP + 1) * 2);
+    Chunk<BP> ch;
+    ch.codes = reinterpret_cast<uint32_t *>(s_chunks + subw * Chunk<BP>::kBytes);
+    ch.x = reinterpret_cast<double *>(s_chunks + subw * Chunk<BP>::kBytes + BP * HDFE_MAX_DIMS * 4);
+    for (int k = threadIdx.x; k < a.c * a.B; k += kPassThreads) s_C[k] = a.C[k];
     __syncthreads();
     const uint64_t dterm = (uint64_t)(a.first_draw + ln.j) * kDrawMul;
-
-    // stage rows i0 .. i0 + m - 1 (lane t: row i0 + t); returns the lane's weight
-    auto stage = [&](int64_t i0, int m) -> double {
-        double w = 1.0;
-        if (ln.j < m) {
-            const int64_t i = i0 + ln.j;
-            if (a.w) w = __ldg(a.w + i);
-            for (int d = 0; d < a.D; d++) {
-                uint32_t code = __ldg(a.codes + i * a.D + d);
-                if ((int64_t)code >= a.nlev[d]) {
-                    if (a.status) atomicCAS(a.status, 0u, (unsigned)HDFE_ERR_BAD_CODE);
-                    code = 0;
-                }
-                s_codes[ln.j * a.D + d] = code;
-            }
-            for (int c = 0; c < a.c; c++) s_x[ln.j * a.c + c] = __ldg(a.X + i * a.c + c);
-        }
-        __syncwarp(ln.mask);
-        return w;
-    };
-    // sum_d U[level_d(q), j] for the window's rows q0 .. q0 + kWin - 1 (< m)
-    // into slot u of hs (this lane's column), every gather issued before the
-    // first is used
-    auto gather = [&](int q0, int m, double *hs) {
-        double hU[kWin];
+    double *pp_buf = s_mom, *mm_buf = s_mom + MR * (BP + 1);
+    auto hU_of = [&](const uint32_t (&codes)[HDFE_MAX_DIMS]) {
+        double h = 0.0;
+        if (ln.on) {
 #pragma unroll
-        for (int u = 0; u < kWin; u++) {
-            const int q = q0 + u;
-            double h = 0.0;
-            if (q < m && ln.on) {
-                for (int d = 0; d < a.D; d++)
-                    h += __ldg(a.U + (a.offs[d] + s_codes[q * a.D + d]) * a.B + ln.j);
+            for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+                if (d >= a.D) break;
+                h += a.U[(a.offs[d] + codes[d]) * a.B + ln.j];
             }
-            hU[u] = h;
         }
-#pragma unroll
-        for (int u = 0; u < kWin; u++) hs[u * (BP + 1) + ln.j] = hU[u];
+        return h;
     };
     auto h_cov = [&](int q) {
         double h = 0.0;
-        for (int c = 0; c < a.c; c++) h += s_x[q * a.c + c] * s_C[c * a.B + ln.j];
+        for (int c = 0; c < a.c; c++) h += ch.x[q * a.c + c] * s_C[c * a.B + ln.j];
         return h;
     };
-    // the draw of row i (unscaled +-1, or the explicit vector)
-    auto draw = [&](int64_t i) -> double {
-        if (a.R) return ln.on ? __ldg(a.R + i * a.B + ln.j) : 0.0;
-        return rad_negative(a.seed, (uint64_t)(a.ordinal0 + i) * kRowMul, dterm) ? -1.0 : 1.0;
+    // lane t < nrow adds the sums of row i0 + t to the moments
+    auto flush_moments = [&](int64_t i0, int nrow) {
+        __syncwarp(ln.mask);
+        if (ln.j < nrow) {
+            double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
+            const double *pr = pp_buf + ln.j * (BP + 1), *mr = mm_buf + ln.j * (BP + 1);
+            for (int k = 0; k < a.B; k++) {
+                const double P = pr[k], M = mr[k];
+                m0 += P;
+                m1 += M;
+                m2 += P * P;
+                m3 += M * M;
+                m4 += P * M;
+            }
+            const int64_t i = i0 + ln.j;
+            a.moments[0 * a.N + i] += m0;
+            a.moments[1 * a.N + i] += m1;
+            a.moments[2 * a.N + i] += m2;
+            a.moments[3 * a.N + i] += m3;
+            a.moments[4 * a.N + i] += m4;
+        }
+        __syncwarp(ln.mask);
     };
-
     const int64_t g0 = (int64_t)blockIdx.x * SUBS + subw, gstep = (int64_t)gridDim.x * SUBS;
     for (int64_t g = g0; g < a.G; g += gstep) {
-        const int64_t s = __ldg(a.starts + g), e = __ldg(a.starts + g + 1);
+        const int64_t s = a.starts[g], e = a.starts[g + 1];
         const int n = (int)(e - s);
-        // pass 1: the weighted group mean of r - h
+        // pass 1
         double sw = 0.0, tot = 0.0;
+        uint32_t bits = 0;
+        double wl = 1.0, irl = 1.0;
+        uint32_t prev[HDFE_MAX_DIMS] = {0, 0, 0, 0};
+        bool have = false;
+        double hU = 0.0;
         for (int c0 = 0; c0 < n; c0 += BP) {
             const int m = min(BP, n - c0);
-            const double wl = stage(s + c0, m);
-            const double irl = inv_root(a, wl);
-            for (int q0 = 0; q0 < m; q0 += kWin) {
-                gather(q0, m, s_P);
-                const int nw = min(kWin, m - q0);
-#pragma unroll 1
-                for (int u = 0; u < nw; u++) {
-                    const int q = q0 + u;
-                    const double wi = __shfl_sync(ln.mask, wl, q, BP);
-                    const double ir = __shfl_sync(ln.mask, irl, q, BP);
-                    sw += wi;
-                    if (ln.on)
-                        tot += wi * (draw(s + c0 + q) * ir -
-                                     (s_P[u * (BP + 1) + ln.j] + h_cov(q)));
+            wl = load_chunk<BP>(a, ln, ch, s + c0, m);
+            irl = inv_root(a, wl);
+            for (int q = 0; q < m; q++) {
+                const double wi = __shfl_sync(ln.mask, wl, q, BP);
+                const double ir = __shfl_sync(ln.mask, irl, q, BP);
+                sw += wi;
+                if (!have || !same_codes(a, ch.codes, q, prev)) {
+                    take_codes(a, ch.codes, q, prev);
+                    hU = hU_of(prev);
+                    have = true;
                 }
+                if (!ln.on) continue;
+                const int64_t i = s + c0 + q;
+                double r;
+                if (a.R) {
+                    r = a.R[i * a.B + ln.j] * ir;
+                } else {
+                    const bool neg = rad_negative(a.seed, (uint64_t)(a.ordinal0 + i) * kRowMul, dterm);
+                    if (c0 == 0 && neg) bits |= 1u << q;
+                    r = neg ? -ir : ir;
+                }
+                tot += wi * (r - (hU + h_cov(q)));
             }
-            if (c0 + BP < n) __syncwarp(ln.mask);   // the next chunk reuses the staging
+            if (c0 + BP < n) __syncwarp(ln.mask);
         }
         const double mean = sw > 0.0 ? tot / sw : 0.0;
-        // pass 2: the projection and the JLA sums (a group of one chunk keeps
-        // its staged rows)
+        // pass 2
+        have = false;
+        int nbuf = 0;               // rows in the moment buffer
+        int64_t buf0 = s;           // the first of them
         for (int c0 = 0; c0 < n; c0 += BP) {
             const int m = min(BP, n - c0);
-            double wl = 1.0;
             if (n > BP) {
                 __syncwarp(ln.mask);
-                wl = stage(s + c0, m);
-            } else if (ln.j < m && a.w) {
-                wl = __ldg(a.w + s + ln.j);
+                wl = load_chunk<BP>(a, ln, ch, s + c0, m);
             }
-            for (int q0 = 0; q0 < m; q0 += kWin) {
-                const int nw = min(kWin, m - q0);
-                double mom[5] = {0, 0, 0, 0, 0};
-                const int64_t ir = s + c0 + q0 + ln.j;          // the row this lane sums
-                if (a.moments && ln.j < nw) {
-#pragma unroll
-                    for (int k = 0; k < 5; k++) mom[k] = a.moments[k * a.N + ir];
+            for (int q = 0; q < m; q++) {
+                const double wi = __shfl_sync(ln.mask, wl, q, BP);
+                if (!have || !same_codes(a, ch.codes, q, prev)) {
+                    take_codes(a, ch.codes, q, prev);
+                    hU = hU_of(prev);
+                    have = true;
                 }
-                gather(q0, m, s_P);
-#pragma unroll 1
-                for (int u = 0; u < nw; u++) {
-                    const int q = q0 + u;
-                    const double wi = __shfl_sync(ln.mask, wl, q, BP);
-                    if (!ln.on) continue;
-                    const int64_t i = s + c0 + q;
-                    double o = s_P[u * (BP + 1) + ln.j] + h_cov(q) + mean;
+                const int64_t i = s + c0 + q;
+                double P = 0.0, M = 0.0;
+                if (ln.on) {
+                    double o = hU + h_cov(q) + mean;
                     if (a.sqrt_weights) o *= sqrt(wi);
                     if (a.out) a.out[i * a.B + ln.j] = o;
-                    if (a.moments) {
-                        const double rr = draw(i);
-                        s_P[u * (BP + 1) + ln.j] = o * o;
-                        s_M[u * (BP + 1) + ln.j] = (rr - o) * (rr - o);
+                    double rr;       // the sink's unscaled draw
+                    if (a.R) {
+                        rr = a.R[i * a.B + ln.j];
+                    } else {
+                        const bool neg =
+                            c0 == 0 ? ((bits >> q) & 1u) != 0
+                                    : rad_negative(a.seed, (uint64_t)(a.ordinal0 + i) * kRowMul, dterm);
+                        rr = neg ? -1.0 : 1.0;
                     }
+                    P = o * o;
+                    M = (rr - o) * (rr - o);
                 }
                 if (a.moments) {
-                    __syncwarp(ln.mask);
-                    if (ln.j < nw) {
-                        const double *pr = s_P + ln.j * (BP + 1), *mr = s_M + ln.j * (BP + 1);
-                        for (int k = 0; k < a.B; k++) {
-                            const double P = pr[k], M = mr[k];
-                            mom[0] += P;
-                            mom[1] += M;
-                            mom[2] += P * P;
-                            mom[3] += M * M;
-                            mom[4] += P * M;
-                        }
-#pragma unroll
-                        for (int k = 0; k < 5; k++) a.moments[k * a.N + ir] = mom[k];
+                    pp_buf[nbuf * (BP + 1) + ln.j] = P;
+                    mm_buf[nbuf * (BP + 1) + ln.j] = M;
+                    if (++nbuf == MR) {
+                        flush_moments(buf0, nbuf);
+                        nbuf = 0;
+                        buf0 = i + 1;
                     }
-                    __syncwarp(ln.mask);
                 }
             }
         }
+        if (a.moments && nbuf > 0) flush_moments(buf0, nbuf);
         __syncwarp(ln.mask);
     }
 }
@@ -604,20 +569,10 @@ inline unsigned grid_for(int64_t G, int Bp)
 }
 
 template <int BP>
-constexpr int project_smem_max()
+constexpr int project_smem()
 {
-    return (kMaxCov * 32 + (kProjThreads / BP) * ((BP * HDFE_MAX_DIMS + 1) / 2 + BP * kMaxCov +
-                                                   2 * kWin * (BP + 1))) * 8;
-}
-
-// k_project's grid: its groups spread over every SM, two waves of its four
-// resident CTAs per SM at most (the rest grid-stride)
-inline unsigned project_grid(int64_t G, int Bp)
-{
-    const int64_t groups_per_cta = kProjThreads / Bp;
-    int64_t b = (G + groups_per_cta - 1) / groups_per_cta;
-    if (b > 148 * 8) b = 148 * 8;
-    return (unsigned)(b > 0 ? b : 1);
+    constexpr int subs = kPassThreads / BP, mr = BP < 16 ? BP : 16;
+    return (kMaxCov * 32 + subs * mr * (BP + 1) * 2) * 8 + subs * Chunk<BP>::kBytes;
 }
 
 template <int BP>
@@ -636,9 +591,9 @@ bool set_smem_limits()
     if (cudaFuncSetAttribute(k_center<8>, at, kSmallBytes + center_chunk_smem<8>()) != cudaSuccess ||
         cudaFuncSetAttribute(k_center<16>, at, kSmallBytes + center_chunk_smem<16>()) != cudaSuccess ||
         cudaFuncSetAttribute(k_center<32>, at, kSmallBytes + center_chunk_smem<32>()) != cudaSuccess ||
-        cudaFuncSetAttribute(k_project<8>, at, project_smem_max<8>()) != cudaSuccess ||
-        cudaFuncSetAttribute(k_project<16>, at, project_smem_max<16>()) != cudaSuccess ||
-        cudaFuncSetAttribute(k_project<32>, at, project_smem_max<32>()) != cudaSuccess)
+        cudaFuncSetAttribute(k_project<8>, at, project_smem<8>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_project<16>, at, project_smem<16>()) != cudaSuccess ||
+        cudaFuncSetAttribute(k_project<32>, at, project_smem<32>()) != cudaSuccess)
         return false;
     done[dev] = true;
     return true;
@@ -738,16 +693,13 @@ extern "C" int hdfe_rows_project(const int64_t *starts, int64_t n_groups, const 
     a.N = n_rows;
     cudaStream_t s = (cudaStream_t)stream;
     if (!rows::set_smem_limits()) return hdfe_set_cuda_error(cudaGetLastError());
-    const unsigned grid = rows::project_grid(n_groups, a.Bp);
+    const unsigned grid = rows::grid_for(n_groups, a.Bp);
     if (a.Bp == 8)
-        rows::k_project<8><<<grid, rows::kProjThreads,
-                             rows::proj_layout<8>(D, c).total_bytes, s>>>(a);
+        rows::k_project<8><<<grid, rows::kPassThreads, rows::project_smem<8>(), s>>>(a);
     else if (a.Bp == 16)
-        rows::k_project<16><<<grid, rows::kProjThreads,
-                              rows::proj_layout<16>(D, c).total_bytes, s>>>(a);
+        rows::k_project<16><<<grid, rows::kPassThreads, rows::project_smem<16>(), s>>>(a);
     else
-        rows::k_project<32><<<grid, rows::kProjThreads,
-                              rows::proj_layout<32>(D, c).total_bytes, s>>>(a);
+        rows::k_project<32><<<grid, rows::kPassThreads, rows::project_smem<32>(), s>>>(a);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(1);
     return HDFE_OK;

@@ -481,7 +481,7 @@ def fit(rows: DeviceRows, tol=1e-10, maxiter=5000, rhs_block=8, timer=None,
         S, split = build_fit_s(cells, rows.m, small_block and precision == "fp64")
     with timer("solve"):
         return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
-                     comps=comps, names=rows.names, split=split)
+                     comps=comps, names=rows.names, split=split, small_block=small_block)
 
 
 _COPY_STREAMS = {}
