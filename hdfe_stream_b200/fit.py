@@ -516,29 +516,33 @@ def _group_cuts(gcode, weights):
     return cuts
 
 
-def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_block=8,
-             timer=None, precision="fp64", names=None, v_chunks=V_CHUNKS) -> FitResult:
-    """The fit from host tensors in pass 0's layout -- gcode (N,) int32,
-    codes (N, D) int32, V (m, N) float64, w (N,) float64 or None, pinned for
-    the copies to overlap -- with the upload overlapped with the work: the
-    group and level structure (and the weights) are copied first; while V
-    follows on a copy stream, pass 1 runs on the structure alone (m = 0:
-    cells, counts, diag) and S is built from it; V crosses in chunks of
-    whole groups (relative sizes `v_chunks`, the last the smallest), and as
-    each lands pass 1 runs on that chunk's rows for its right-hand sides
-    (sums over its groups, so they add up across chunks; the variables' sums
-    of squares combine by the parallel-variance rule).  After the last byte
-    only the last chunk's pass and the solve remain.  S depends on the
-    structure only and comes out identical to `fit`'s; the right-hand sides
-    agree with `fit`'s to rounding (another grouping of the same sums)."""
+@dataclass
+class HostUpload:
+    """Rows in flight to the device (`upload_host`): device tensors being
+    filled on the copy stream and the events that say when."""
+
+    gcode: object
+    codes: object
+    w: object
+    chunks: list                # (first row, last row + 1, V chunk (m, rows), event)
+    structure: object           # event: gcode, codes and w have landed
+    m: int
+
+
+def upload_host(gcode, codes, V, w=None, v_chunks=V_CHUNKS) -> HostUpload:
+    """Start the upload of host rows in pass 0's layout -- gcode (N,) int32,
+    codes (N, D) int32, V (m, N) float64, w (N,) float64 or None, pinned --
+    on the copy stream, and return at once: the group and level structure
+    (and the weights) first, then V in chunks of whole groups (relative sizes
+    `v_chunks`, the last the smallest).  No wait on the compute stream: the
+    copies write fresh blocks of the copy stream's own pool (the caching
+    allocator never hands a block freed on one stream to another), so a
+    caller can upload the next fit's rows while this one computes."""
     torch = _torch()
-    timer = timer or _NoTimer()
     dev = torch.device("cuda", torch.cuda.current_device())
-    compute = torch.cuda.current_stream(dev)
     copy = _copy_stream(dev)
     m = int(V.shape[0])
     cuts = _group_cuts(gcode, list(v_chunks) or [1])
-    copy.wait_stream(compute)       # the buffers it writes may be freed memory of compute's
     chunks = []
     with torch.cuda.stream(copy):
         g_d = gcode.to(dev, non_blocking=True)
@@ -553,7 +557,25 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
             ev = torch.cuda.Event()
             ev.record(copy)
             chunks.append((lo, hi, Vc, ev))
-    compute.wait_event(structure)
+    return HostUpload(g_d, c_d, w_d, chunks, structure, m)
+
+
+def fit_uploaded(up: HostUpload, n_levels, tol=1e-10, maxiter=5000, rhs_block=8, timer=None,
+                 precision="fp64", names=None) -> FitResult:
+    """The fit of rows `upload_host` is bringing over, overlapped with their
+    arrival: pass 1 runs on the structure alone (m = 0: cells, counts,
+    diag) as soon as it lands, then the components and S are built while V
+    is still on the bus; as each V chunk lands, pass 1 runs on that chunk's
+    rows for its right-hand sides (sums over its groups, so they add up
+    across chunks; the variables' sums of squares combine by the
+    parallel-variance rule).  After the last byte only the last chunk's
+    pass and the solve remain."""
+    torch = _torch()
+    timer = timer or _NoTimer()
+    dev = up.gcode.device
+    compute = torch.cuda.current_stream(dev)
+    compute.wait_event(up.structure)
+    g_d, c_d, w_d, m = up.gcode, up.codes, up.w, up.m
     for t in (g_d, c_d, w_d):
         if t is not None:
             t.record_stream(compute)
@@ -566,7 +588,7 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
         S, split = build_fit_s(shape, m, precision == "fp64")
     rhs, n_tot, mean, m2 = None, 0, None, None
     with timer("pass1"):
-        for lo, hi, Vc, ev in chunks:
+        for lo, hi, Vc, ev in up.chunks:
             compute.wait_event(ev)
             Vc.record_stream(compute)
             part = pass1(DeviceRows(g_d[lo:hi], c_d[lo:hi], Vc,
@@ -582,12 +604,24 @@ def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_blo
                 mean = mean + delta * (nb / n_new)
                 n_tot = n_new
             del part
-    del chunks
     import dataclasses
     cells = dataclasses.replace(shape, rhs=rhs, means=mean, raw_ss=m2)
     with timer("solve"):
         return solve(cells, S, tol, maxiter, rhs_block, timer=timer, precision=precision,
                      comps=comps, names=names, split=split)
+
+
+def fit_host(gcode, codes, V, n_levels, w=None, tol=1e-10, maxiter=5000, rhs_block=8,
+             timer=None, precision="fp64", names=None, v_chunks=V_CHUNKS) -> FitResult:
+    """The fit from host tensors in pass 0's layout (pinned for the copies to
+    overlap): `upload_host` then `fit_uploaded`.  S depends on the structure
+    only and comes out identical to `fit`'s; the right-hand sides agree with
+    `fit`'s to rounding (another grouping of the same sums).  A caller
+    fitting one panel after another overlaps the next upload with this
+    fit's work by calling `upload_host` for the next rows before
+    `fit_uploaded` for these."""
+    return fit_uploaded(upload_host(gcode, codes, V, w, v_chunks), n_levels, tol, maxiter,
+                        rhs_block, timer, precision, names)
 
 
 def fit_rows(rows, tol=1e-10, maxiter=5000, rhs_block=8):
@@ -657,8 +691,7 @@ def fit_stream(batches, n_levels, tol=1e-10, maxiter=5000, rhs_block=8, names=No
     copy = _copy_stream(dev)
     n_levels = list(n_levels)
 
-    def upload(b):
-        copy.wait_stream(compute)
+    def upload(b):              # no wait on compute: see fit_host
         with torch.cuda.stream(copy):
             ts = tuple(None if t is None else t.to(dev, non_blocking=True) for t in b)
             ev = torch.cuda.Event()

@@ -298,3 +298,29 @@ def test_split_build_equals_split_of_whole_s(device, name, rows):
     assert plain.split is None
     assert float((res.gamma - plain.gamma).abs().max() / plain.gamma.abs().max()) < 1e-9
     assert torch.equal(res.S.indices, plain.S.indices)       # the lazily built whole S
+
+
+def test_pipelined_host_fits(device):
+    """Back-to-back fits with the next rows' upload issued before this fit
+    (`fit.upload_host` then `fit.fit_uploaded`): every fit equals its own
+    `fit.fit_host`, whatever was in flight beside it."""
+    import torch
+    from hdfe_stream_b200 import fit
+
+    def pin(rows):
+        return (torch.from_numpy(rows.gcode.astype(np.uint32).view(np.int32)).pin_memory(),
+                torch.from_numpy(np.ascontiguousarray(rows.codes.astype(np.uint32))
+                                 .view(np.int32)).pin_memory(),
+                torch.from_numpy(np.ascontiguousarray(rows.V.T)).pin_memory(),
+                None if rows.w is None else torch.from_numpy(rows.w.astype(np.float64))
+                .pin_memory())
+    panels = [dict(PANELS)[n] for n in ("akm_20k", "weighted", "akm_20k", "weighted")]
+    host = [pin(r) for r in panels]
+    want = [fit.fit_host(g, c, V, r.n_levels, w=w, tol=1e-12).gamma.cpu()
+            for (g, c, V, w), r in zip(host, panels)]
+    up = fit.upload_host(*host[0][:3], w=host[0][3])
+    for i, r in enumerate(panels):
+        nxt = fit.upload_host(*host[i + 1][:3], w=host[i + 1][3]) if i + 1 < len(panels) else None
+        got = fit.fit_uploaded(up, r.n_levels, tol=1e-12).gamma.cpu()
+        assert float((got - want[i]).abs().max() / want[i].abs().max()) < 1e-10, i
+        up = nxt
