@@ -173,7 +173,9 @@ def phase_bytes(rows, counts, S, iterations, m=3, small=None):
               + 8 * 16 * small["first"])
         per_it = (12 * small["big_nnz"] + 8 * (L + 1) + 8 * 16 * small["first"]
                   + 8 * L * m * 9 + 16 * small["first"] * m)
-    return {"pass1": p1, "sbuild": sb, "pcg_kernel": per_it * max(iterations, 1)}
+    whole = (12 * S.nnz + 8 * (L + 1) + 8 * L * m * 9) * max(iterations, 1)
+    return {"pass1": p1, "sbuild": sb, "pcg_kernel": per_it * max(iterations, 1),
+            "pcg_kernel_whole_csr": whole}
 
 
 # DRAM bytes (read + write) of one PCG iteration on the 5M-worker panel, from
@@ -264,6 +266,13 @@ def run_ours(args, rank, world, local_rank):
                 gbs = by[name] / (avg_ms / 1e3) / 1e9
                 roof[name] = {"ms": round(avg_ms, 4), "bytes": int(by[name]),
                               "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+                if name == "pcg_kernel" and info.get("small_block"):
+                    # the same iterations' bytes on the whole CSR (the layout the
+                    # reference streams), for comparison with that layout's solve
+                    wg = by["pcg_kernel_whole_csr"] / (avg_ms / 1e3) / 1e9
+                    roof[name]["whole_csr_bytes"] = int(by["pcg_kernel_whole_csr"])
+                    roof[name]["whole_csr_equivalent_gbs"] = round(wg, 1)
+                    roof[name]["whole_csr_equivalent_frac"] = round(wg / peak, 4)
         # the dominant single kernel is the PCG (one launch per fit); the S
         # build and pass 1 are phases of several kernels, reported alongside
         dom = "pcg_kernel"
