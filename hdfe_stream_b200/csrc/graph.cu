@@ -228,8 +228,8 @@ extern "C" int hdfe_components(const int64_t *starts, int64_t n_groups, const ui
                                void *stream)
 {
     if (D < 1 || D > HDFE_MAX_DIMS || col < 0 || col >= D || n_levels < 1 ||
-        n_levels >= INT32_MAX || n_groups < 0 || !starts || !codes || !root || !n_components ||
-        !workspace || workspace_bytes < 256)
+        n_levels >= INT32_MAX || n_groups < 0 || !starts || (n_groups > 0 && !codes) || !root ||
+        !n_components || !workspace || workspace_bytes < 256)
         return hdfe_set_arg_error("hdfe_components: bad argument");
     cudaStream_t s = (cudaStream_t)stream;
     unsigned *status = (unsigned *)workspace;

@@ -633,9 +633,11 @@ __global__ void __launch_bounds__(kThreads) k_cell_widx(Args a)
 // the same group and level combined by __match_any_sync in lane order); then
 // each lane owns W^2 / 32 entries and adds the 32 groups' (u_a / N_g) u_b in
 // group order, lanes a < W add the diagonal's u_a, and the pattern is the
-// union of the groups' level masks.  Cells with two wide levels (two small
-// dimensions) add their off-diagonal C into its own array.  Warps and CTAs
-// are summed in a fixed order, so the block is deterministic.
+// union of the groups' level masks.  Cells with two or more wide levels
+// (several small dimensions) add their off-diagonal C, for every pair of
+// their wide levels, into its own array by atomic adds (exact for counts;
+// in atomic order for weighted n).  Warps and CTAs are summed in a fixed
+// order, so the rest of the block is deterministic.
 constexpr int kWideThreads = 128;
 constexpr int kWideWarps = kWideThreads / 32;
 
@@ -688,7 +690,7 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
                 gq = lo;
                 ni = a.n[i];
             }
-            int k0 = -1;
+            int ks[HDFE_MAX_DIMS], nk = 0;      // the cell's wide levels so far
             for (int d = 0; d < a.D; d++) {
                 const int32_t k = valid ? a.cell_widx[i * a.D + d] : -1;
                 const int key = k >= 0 ? gq * 32 + k : -1 - lane;
@@ -701,12 +703,13 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
                     u[gq][k] += sum;
                 }
                 if (k >= 0) {
-                    if (k0 < 0) k0 = k;
-                    else {
-                        // a cell with two wide levels: C(k0, k) and C(k, k0)
-                        atomicAdd(a.wcross + (int64_t)k0 * W + k, ni);
-                        atomicAdd(a.wcross + (int64_t)k * W + k0, ni);
+                    // a cell with several wide levels: C(a, k) and C(k, a) for
+                    // each wide level a of its earlier dimensions
+                    for (int q = 0; q < nk; q++) {
+                        atomicAdd(a.wcross + (int64_t)ks[q] * W + k, ni);
+                        atomicAdd(a.wcross + (int64_t)k * W + ks[q], ni);
                     }
+                    ks[nk++] = k;
                 }
                 __syncwarp();
             }
@@ -954,8 +957,9 @@ int setup(Ctx &c, const int64_t *starts, int64_t G, const uint32_t *codes, int32
           const double *n, const double *group_n, int64_t M, const int64_t *n_levels,
           const int32_t *lcount, const int64_t *work, void *ws, int64_t ws_bytes)
 {
-    if (D < 1 || D > HDFE_MAX_DIMS || G < 0 || M < 0 || !starts || !codes || !n || !group_n ||
-        !n_levels || !ws || ((lcount == nullptr) != (work == nullptr)))
+    // empty arrays may come as null pointers (no identifying group or cell)
+    if (D < 1 || D > HDFE_MAX_DIMS || G < 0 || M < 0 || !starts || (M > 0 && (!codes || !n)) ||
+        (G > 0 && !group_n) || !n_levels || !ws || ((lcount == nullptr) != (work == nullptr)))
         return hdfe_set_arg_error("hdfe_sbuild: bad argument");
     Args &a = c.a;
     a = Args{};
