@@ -681,10 +681,10 @@ def run_e2e(args, rows, dist):
     buffers: every step copies its rows host->device and its fixed effects
     back, inside the timed region.  A stream of fits runs as a pipeline
     (`fit.upload_host` for step i+1 is issued before `fit.fit_uploaded` of
-    step i, so the next rows cross the bus while this fit computes; within a
-    step the structure goes first and the outcome's chunks are passed
-    through pass 1 as they land); `serial` is the same with one
-    `fit.fit_host` at a time."""
+    step i, so the next rows cross the bus while this fit computes, into
+    the device buffers of step i - 1; within a step the structure goes first
+    and the outcome's chunks are passed through pass 1 as they land);
+    `serial` is the same with one `fit.fit_host` at a time."""
     import torch
     from hdfe_stream_b200 import fit, replicas
 
@@ -699,8 +699,9 @@ def run_e2e(args, rows, dist):
     out_host = None
     d2h = 0
 
-    def upload():
-        return fit.upload_host(pinned["gcode"], pinned["codes"], pinned["V"], w=pinned.get("w"))
+    def upload(reuse=None):
+        return fit.upload_host(pinned["gcode"], pinned["codes"], pinned["V"], w=pinned.get("w"),
+                               reuse=reuse)
 
     def finish(res):
         nonlocal out_host, d2h
@@ -725,11 +726,13 @@ def run_e2e(args, rows, dist):
         return replicas.max_over_ranks(a.elapsed_time(b), dist, "cuda")
 
     def pipeline():
-        up = upload()
+        # two sets of device buffers in turn: step i + 1's rows go into the
+        # buffers of step i - 1, whose fit has returned
+        up, prev = upload(), None
         for i in range(args.steps):
-            nxt = upload() if i + 1 < args.steps else None
+            nxt = upload(reuse=prev) if i + 1 < args.steps else None
             finish(fit.fit_uploaded(up, rows.n_levels, tol=args.tol))
-            up = nxt
+            prev, up = up, nxt
 
     def serial():
         for _ in range(args.steps):

@@ -527,9 +527,10 @@ class HostUpload:
     chunks: list                # (first row, last row + 1, V chunk (m, rows), event)
     structure: object           # event: gcode, codes and w have landed
     m: int
+    done: object = None         # event on the compute stream: the fit has read them all
 
 
-def upload_host(gcode, codes, V, w=None, v_chunks=V_CHUNKS) -> HostUpload:
+def upload_host(gcode, codes, V, w=None, v_chunks=V_CHUNKS, reuse=None) -> HostUpload:
     """Start the upload of host rows in pass 0's layout -- gcode (N,) int32,
     codes (N, D) int32, V (m, N) float64, w (N,) float64 or None, pinned --
     on the copy stream, and return at once: the group and level structure
@@ -537,21 +538,37 @@ def upload_host(gcode, codes, V, w=None, v_chunks=V_CHUNKS) -> HostUpload:
     `v_chunks`, the last the smallest).  No wait on the compute stream: the
     copies write fresh blocks of the copy stream's own pool (the caching
     allocator never hands a block freed on one stream to another), so a
-    caller can upload the next fit's rows while this one computes."""
+    caller can upload the next fit's rows while this one computes.  `reuse`:
+    an earlier upload of rows of the same shape whose fit has returned; its
+    device buffers are written again (after that fit's last read of them),
+    so a pipeline of fits cycles two sets of buffers instead of allocating."""
     torch = _torch()
     dev = torch.device("cuda", torch.cuda.current_device())
     copy = _copy_stream(dev)
     m = int(V.shape[0])
     cuts = _group_cuts(gcode, list(v_chunks) or [1])
+    same = (reuse is not None and reuse.done is not None and reuse.m == m and
+            tuple(reuse.gcode.shape) == tuple(gcode.shape) and
+            tuple(reuse.codes.shape) == tuple(codes.shape) and (reuse.w is None) == (w is None)
+            and [(lo, hi) for lo, hi, _, _ in reuse.chunks] == list(zip(cuts[:-1], cuts[1:])))
     chunks = []
     with torch.cuda.stream(copy):
-        g_d = gcode.to(dev, non_blocking=True)
-        c_d = codes.to(dev, non_blocking=True)
-        w_d = None if w is None else w.to(dev, non_blocking=True)
+        if same:
+            copy.wait_event(reuse.done)
+            g_d, c_d, w_d = reuse.gcode, reuse.codes, reuse.w
+            g_d.copy_(gcode, non_blocking=True)
+            c_d.copy_(codes, non_blocking=True)
+            if w_d is not None:
+                w_d.copy_(w, non_blocking=True)
+        else:
+            g_d = gcode.to(dev, non_blocking=True)
+            c_d = codes.to(dev, non_blocking=True)
+            w_d = None if w is None else w.to(dev, non_blocking=True)
         structure = torch.cuda.Event()
         structure.record(copy)
-        for lo, hi in zip(cuts[:-1], cuts[1:]):
-            Vc = torch.empty((m, hi - lo), dtype=torch.float64, device=dev)
+        for q, (lo, hi) in enumerate(zip(cuts[:-1], cuts[1:])):
+            Vc = reuse.chunks[q][2] if same else torch.empty((m, hi - lo), dtype=torch.float64,
+                                                             device=dev)
             for j in range(m):
                 Vc[j].copy_(V[j, lo:hi], non_blocking=True)
             ev = torch.cuda.Event()
@@ -604,6 +621,8 @@ def fit_uploaded(up: HostUpload, n_levels, tol=1e-10, maxiter=5000, rhs_block=8,
                 mean = mean + delta * (nb / n_new)
                 n_tot = n_new
             del part
+    up.done = torch.cuda.Event()        # every read of the upload's buffers is enqueued
+    up.done.record(compute)
     import dataclasses
     cells = dataclasses.replace(shape, rhs=rhs, means=mean, raw_ss=m2)
     with timer("solve"):

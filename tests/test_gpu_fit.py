@@ -302,8 +302,9 @@ def test_split_build_equals_split_of_whole_s(device, name, rows):
 
 def test_pipelined_host_fits(device):
     """Back-to-back fits with the next rows' upload issued before this fit
-    (`fit.upload_host` then `fit.fit_uploaded`): every fit equals its own
-    `fit.fit_host`, whatever was in flight beside it."""
+    (`fit.upload_host` then `fit.fit_uploaded`), two sets of device buffers
+    in turn: every fit equals its own `fit.fit_host`, whatever was in flight
+    beside it."""
     import torch
     from hdfe_stream_b200 import fit
 
@@ -318,9 +319,13 @@ def test_pipelined_host_fits(device):
     host = [pin(r) for r in panels]
     want = [fit.fit_host(g, c, V, r.n_levels, w=w, tol=1e-12).gamma.cpu()
             for (g, c, V, w), r in zip(host, panels)]
-    up = fit.upload_host(*host[0][:3], w=host[0][3])
+    up, prev = fit.upload_host(*host[0][:3], w=host[0][3]), None
     for i, r in enumerate(panels):
-        nxt = fit.upload_host(*host[i + 1][:3], w=host[i + 1][3]) if i + 1 < len(panels) else None
+        # step i + 1 reuses step i - 1's buffers (the same panel shape)
+        nxt = fit.upload_host(*host[i + 1][:3], w=host[i + 1][3], reuse=prev) \
+            if i + 1 < len(panels) else None
+        if i >= 1 and nxt is not None:
+            assert nxt.gcode is prev.gcode
         got = fit.fit_uploaded(up, r.n_levels, tol=1e-12).gamma.cpu()
         assert float((got - want[i]).abs().max() / want[i].abs().max()) < 1e-10, i
-        up = nxt
+        prev, up = up, nxt
