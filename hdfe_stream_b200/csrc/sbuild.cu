@@ -640,6 +640,7 @@ __global__ void __launch_bounds__(kThreads) k_cell_widx(Args a)
 // order, so the rest of the block is deterministic.
 constexpr int kWideThreads = 128;
 constexpr int kWideWarps = kWideThreads / 32;
+constexpr int kWideRounds = 4;          // rounds of 32 cells whose loads are in flight together
 
 __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
 {
@@ -676,23 +677,45 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
         for (int q = lane; q < 32 * (kWideWarp + 1); q += 32) (&u[0][0])[q] = 0.0;
         __syncwarp();
         const int64_t c0 = gs[0], c1 = gs[ng];
-        for (int64_t i0 = c0; i0 < c1; i0 += 32) {
-            const int64_t i = i0 + lane;
+        // the chunk's cells, kWideRounds rounds of 32 at a time: every round's
+        // loads (n and the wide indices) issued before the first is used
+        for (int64_t b0 = c0; b0 < c1; b0 += 32 * kWideRounds) {
+          int gqr[kWideRounds];
+          double nir[kWideRounds];
+          int32_t kr[kWideRounds][HDFE_MAX_DIMS];
+#pragma unroll
+          for (int t = 0; t < kWideRounds; t++) {
+            const int64_t i = b0 + 32 * t + lane;
             const bool valid = i < c1;
-            int gq = 0;
-            double ni = 0.0;
+            gqr[t] = 0;
+            nir[t] = 0.0;
+#pragma unroll
+            for (int d = 0; d < HDFE_MAX_DIMS; d++) kr[t][d] = -1;
             if (valid) {
                 int lo = 0, hi = ng;        // last group with start <= i
                 while (hi - lo > 1) {
                     const int mid = (lo + hi) >> 1;
                     if (gs[mid] <= i) lo = mid; else hi = mid;
                 }
-                gq = lo;
-                ni = a.n[i];
+                gqr[t] = lo;
+                nir[t] = a.n[i];
+#pragma unroll
+                for (int d = 0; d < HDFE_MAX_DIMS; d++)
+                    if (d < a.D) kr[t][d] = a.cell_widx[i * a.D + d];
             }
+          }
+#pragma unroll
+          for (int t = 0; t < kWideRounds; t++) {
+            if (b0 + 32 * t >= c1) break;               // warp-uniform
+            const int64_t i = b0 + 32 * t + lane;
+            const bool valid = i < c1;
+            const int gq = gqr[t];
+            const double ni = nir[t];
             int ks[HDFE_MAX_DIMS], nk = 0;      // the cell's wide levels so far
-            for (int d = 0; d < a.D; d++) {
-                const int32_t k = valid ? a.cell_widx[i * a.D + d] : -1;
+#pragma unroll
+            for (int d = 0; d < HDFE_MAX_DIMS; d++) {
+                if (d >= a.D) break;
+                const int32_t k = valid ? kr[t][d] : -1;
                 const int key = k >= 0 ? gq * 32 + k : -1 - lane;
                 const unsigned peers = __match_any_sync(0xffffffffu, key);
                 s_stage[wl][lane] = ni;
@@ -713,6 +736,7 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
                 }
                 __syncwarp();
             }
+          }
         }
         __syncwarp();
         // each group's u / N_g and level mask
