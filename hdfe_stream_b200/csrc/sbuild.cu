@@ -381,8 +381,6 @@ __device__ __forceinline__ void warp_sort(int32_t *key, double *val, int n, int 
     else warp_bitonic(key, val, n, lane);
 }
 
-constexpr int kRowRounds = 2;           // a narrow row's rounds of 32 items loaded together
-
 struct RowSmem {
     double *xs;         // kCross direct slots: the split form's small columns
     int32_t *keys;
@@ -396,7 +394,7 @@ struct RowSmem {
 };
 
 // One narrow row by one warp: accumulate, compact, sort, park in temp.
-__device__ __forceinline__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_bits)
+__device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_bits)
 {
     const int lane = threadIdx.x & 31;
     const int dr = level_dim(a, r);
@@ -446,51 +444,24 @@ __device__ __forceinline__ void narrow_row(const Args &a, int64_t r, const RowSm
     if (lane == 0) sm.loff[nl] = carry;
     __syncwarp();
     const int32_t items = carry;
-    // the items kRowRounds rounds of 32 at a time: every round's cell loads
-    // issued before the first is used (the additions keep their order)
-    for (int32_t b0 = 0; b0 < items; b0 += 32 * kRowRounds) {
-      double nir[kRowRounds], wvr[kRowRounds];
-      uint32_t cr[kRowRounds][HDFE_MAX_DIMS];
-#pragma unroll
-      for (int t = 0; t < kRowRounds; t++) {
-        const int32_t j = b0 + 32 * t + lane;
-        nir[t] = 0.0;
-        wvr[t] = 0.0;
-#pragma unroll
-        for (int d = 0; d < HDFE_MAX_DIMS; d++) cr[t][d] = 0;
-        if (j < items) {
+    for (int32_t base = 0; base < items; base += 32) {
+        const int32_t j = base + lane;
+        const bool valid = j < items;
+        int64_t i = 0;
+        double v = 0.0;
+        if (valid) {
             int lo = 0, hi = nl;            // last group with loff <= j
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
                 if (sm.loff[mid] <= j) lo = mid; else hi = mid;
             }
-            const int64_t i = sm.gs[lo] + (j - sm.loff[lo]);
-            nir[t] = a.n[i];
-            wvr[t] = sm.wv[lo];
-#pragma unroll
-            for (int d = 0; d < HDFE_MAX_DIMS; d++)
-                if (d < a.D) cr[t][d] = a.codes[i * a.D + d];
+            i = sm.gs[lo] + (j - sm.loff[lo]);
+            const double ni = a.n[i];
+            v -= ni * sm.wv[lo];
+            if (a.codes[i * a.D + dr] == lr) v += ni;
         }
-      }
-#pragma unroll
-      for (int t = 0; t < kRowRounds; t++) {
-        const int32_t base = b0 + 32 * t;
-        if (base >= items) break;                       // warp-uniform
-        const bool valid = base + lane < items;
-        double v = 0.0;
-        if (valid) {
-            const double ni = nir[t];
-            v -= ni * wvr[t];
-            uint32_t cdr = cr[t][0];
-#pragma unroll
-            for (int d = 1; d < HDFE_MAX_DIMS; d++)
-                if (d == dr) cdr = cr[t][d];
-            if (cdr == lr) v += ni;
-        }
-#pragma unroll
-        for (int d = 0; d < HDFE_MAX_DIMS; d++) {
-            if (d >= a.D) break;
-            const int32_t col = valid ? (int32_t)(a.offs[d] + cr[t][d]) : -1;
+        for (int d = 0; d < a.D; d++) {
+            const int32_t col = valid ? (int32_t)(a.offs[d] + a.codes[i * a.D + d]) : -1;
             const unsigned peers = __match_any_sync(0xffffffffu, col);
             const int leader = __ffs(peers) - 1;
             sm.stage[lane] = v;
@@ -515,7 +486,6 @@ __device__ __forceinline__ void narrow_row(const Args &a, int64_t r, const RowSm
             }
             __syncwarp();
         }
-      }
     }
     __syncwarp();
     const int cnt = *sm.cnt;
@@ -555,7 +525,7 @@ __device__ __forceinline__ void narrow_row(const Args &a, int64_t r, const RowSm
 }
 
 // small warp rows (the front of warp_rows): 256-slot tables, 8 warps per CTA
-__global__ void __launch_bounds__(kSmallWarpsPerCta * 32, 4) k_small_rows(Args a)
+__global__ void __launch_bounds__(kSmallWarpsPerCta * 32) k_small_rows(Args a)
 {
     __shared__ double s_xs[kSmallWarpsPerCta][kCross];
     __shared__ int32_t s_keys[kSmallWarpsPerCta][kSmallSlots];
