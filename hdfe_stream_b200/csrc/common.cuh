@@ -35,6 +35,17 @@ __device__ __forceinline__ void st_release(unsigned *p, unsigned v)
     asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
+// fetch-and-add with release semantics at GPU scope: the writes this thread
+// has made or observed (the CTA's, after its __syncthreads) are visible to
+// whoever acquires the result
+__device__ __forceinline__ unsigned atom_add_release(unsigned *p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;"
+                 : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Grid barrier state: bar[0] arrivals, bar[1] generation, bar[2] error code.
 // Zeroed by the host (or a set-up kernel) before the launch that uses it.
 struct GridBarrier {
@@ -43,29 +54,34 @@ struct GridBarrier {
     // Returns false when the kernel must stop (an error was recorded, by this
     // CTA on a timeout or by another one).  All threads of the CTA return the
     // same value.
+    //   Arrival is one release fetch-and-add (it orders the CTA's writes,
+    // made visible to thread 0 by the __syncthreads, before it); the last CTA
+    // resets the count and publishes the next generation with a release
+    // store; the others spin on the generation alone with acquire loads,
+    // looking at the error word and the clock every 32 polls (the wait stays
+    // bounded by kSpinLimitNs, give or take 32 polls).
     __device__ bool sync() const
     {
         __shared__ int s_ok;
         __syncthreads();
         if (threadIdx.x == 0) {
             int ok = 1;
-            unsigned gen = ld_acquire(bar + 1);
-            __threadfence();
-            unsigned arrived = atomicAdd(bar, 1u);
+            const unsigned gen = ld_acquire(bar + 1);
+            const unsigned arrived = atom_add_release(bar, 1u);
             if (arrived == gridDim.x - 1) {
-                bar[0] = 0;
-                __threadfence();
+                bar[0] = 0;                 // ordered before the release below
                 st_release(bar + 1, gen + 1);
             } else {
-                unsigned long long t0 = global_ns();
-                while (ld_acquire(bar + 1) == gen) {
-                    if (ld_acquire(bar + 2) != 0) { ok = 0; break; }
-                    if (global_ns() - t0 > kSpinLimitNs) {
-                        atomicCAS(bar + 2, 0u, (unsigned)HDFE_ERR_SPIN_LIMIT);
-                        ok = 0;
-                        break;
+                const unsigned long long t0 = global_ns();
+                for (unsigned polls = 1; ld_acquire(bar + 1) == gen; polls++) {
+                    if ((polls & 31u) == 0) {
+                        if (ld_acquire(bar + 2) != 0) { ok = 0; break; }
+                        if (global_ns() - t0 > kSpinLimitNs) {
+                            atomicCAS(bar + 2, 0u, (unsigned)HDFE_ERR_SPIN_LIMIT);
+                            ok = 0;
+                            break;
+                        }
                     }
-                    __nanosleep(64);
                 }
             }
             if (ok && ld_acquire(bar + 2) != 0) ok = 0;
