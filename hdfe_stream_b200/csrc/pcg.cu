@@ -50,7 +50,10 @@ namespace pcg {
 __host__ __device__ constexpr int threads_for(int k) { return k >= HDFE_PCG_WIDE_K ? 512 : 1024; }
 constexpr int kMaxWarps = 32;
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kLong = 64;           // nonzeros in a warp's range that make a row "long"
+#ifndef HDFE_PCG_LONG
+#define HDFE_PCG_LONG 64
+#endif
+constexpr int kLong = HDFE_PCG_LONG;    // nonzeros in a warp's range that make a row "long"
 // rows per thread per trip in the vector phases (their loads all issued
 // before the updates), as many as fit the registers without spills
 __host__ __device__ constexpr int row_batch(int k) { return k <= 3 ? 2 : 1; }
@@ -339,7 +342,7 @@ template <int K, int VS, int VW, typename T, int LPR = 8>
 __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T *__restrict__ V,
                            T *__restrict__ out, T *carry, double (&dot)[K], bool want_dot)
 {
-    static_assert(LPR == 4 || LPR == 8, "short rows take 4 or 8 lanes");
+    static_assert(LPR == 2 || LPR == 4 || LPR == 8, "short rows take 2, 4 or 8 lanes");
     constexpr int RPS = 32 / LPR;       // short rows per step
     const int lane = threadIdx.x & 31, sub = lane / LPR, sl = lane % LPR;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -952,8 +955,16 @@ cudaError_t launch(Params p, int blocks, cudaStream_t s)
                                        dim3(threads_for(K)), args, 0, s);
 }
 
-// 4 lanes a short row when S's rows average at most this many nonzeros
-constexpr int64_t kShortRowNnz = 24;
+// HDFE_PCG_SHORT_LPR lanes a short row when S's rows average at most this
+// many nonzeros (8 otherwise)
+#ifndef HDFE_PCG_SHORT_ROW_NNZ
+#define HDFE_PCG_SHORT_ROW_NNZ 24
+#endif
+#ifndef HDFE_PCG_SHORT_LPR
+#define HDFE_PCG_SHORT_LPR 4
+#endif
+constexpr int64_t kShortRowNnz = HDFE_PCG_SHORT_ROW_NNZ;
+constexpr int kShortLpr = HDFE_PCG_SHORT_LPR;
 
 // ------------------------------------------------ one column per lane
 //
@@ -1581,10 +1592,10 @@ int solve_registers(const int64_t *indptr, const int32_t *indices, const double 
     cudaError_t e = cudaErrorInvalidValue;
     const bool short_rows = nnz <= pcg::kShortRowNnz * L;
     switch (k) {
-    case 1: e = short_rows ? pcg::launch<1, 4>(p, blocks, s) : pcg::launch<1>(p, blocks, s); break;
-    case 2: e = short_rows ? pcg::launch<2, 4>(p, blocks, s) : pcg::launch<2>(p, blocks, s); break;
-    case 3: e = short_rows ? pcg::launch<3, 4>(p, blocks, s) : pcg::launch<3>(p, blocks, s); break;
-    case 4: e = short_rows ? pcg::launch<4, 4>(p, blocks, s) : pcg::launch<4>(p, blocks, s); break;
+    case 1: e = short_rows ? pcg::launch<1, pcg::kShortLpr>(p, blocks, s) : pcg::launch<1>(p, blocks, s); break;
+    case 2: e = short_rows ? pcg::launch<2, pcg::kShortLpr>(p, blocks, s) : pcg::launch<2>(p, blocks, s); break;
+    case 3: e = short_rows ? pcg::launch<3, pcg::kShortLpr>(p, blocks, s) : pcg::launch<3>(p, blocks, s); break;
+    case 4: e = short_rows ? pcg::launch<4, pcg::kShortLpr>(p, blocks, s) : pcg::launch<4>(p, blocks, s); break;
     case 5: e = pcg::launch<5>(p, blocks, s); break;
     case 6: e = pcg::launch<6>(p, blocks, s); break;
     case 7: e = pcg::launch<7>(p, blocks, s); break;
