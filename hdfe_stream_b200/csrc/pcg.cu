@@ -69,11 +69,13 @@ struct Stride {
 // ns <= kSmall of S ("small levels" [Lb, L)), S's CSR holds only the block of
 // the other ("big") levels, and the rest is dense: cross (Lb x kSmall,
 // row-major, zero-padded) = S[r, Lb + j] and small (ns x ns) = S[Lb + i, Lb + j].
-// A big row's product with the small levels is then a coalesced 128-byte row
-// of cross against ns values held in shared memory, and the small rows'
-// products are the columns of cross summed against P's big rows, reduced
-// with the p'Ap partials: no index round trips, and cross is read once for
-// both halves of the symmetric block.
+// A big row's product with the small levels is then its 128-byte row of
+// cross, loaded beside the row's own indices and values in the SpMM's row
+// walk (the same round trips), against ns values held in shared memory; the
+// small rows' products are the columns of cross summed against P's big rows
+// in the same walk, reduced with the p'Ap partials: no index round trips for
+// the small levels, and cross is read once for both halves of the symmetric
+// block.
 constexpr int kSmall = HDFE_SMALL_MAX_LEVELS;
 
 struct Params {
@@ -85,7 +87,6 @@ struct Params {
     int ns;                     // small levels, 0 .. kSmall
     const double *cross;        // (Lb, kSmall) S[r, Lb + j]
     const double *small;        // (ns, ns) S[Lb + i, Lb + j]
-    double *AP2;                // (L, K) the big rows' products with the small levels
     const int64_t *wlo;     // (warps + 1) first nonzero of each warp's range
     int64_t nwarps;
     const double *dinv;
@@ -106,7 +107,7 @@ struct Params {
 // Workspace layout in bytes: R (L*K), P (L*KP), AP (L*K), carry, part,
 // wfirst, cut flags, then the barrier words.
 struct Layout {
-    int64_t r, p, ap, ap2, carry, part, wfirst, wlo, cut, bar, total;
+    int64_t r, p, ap, carry, part, wfirst, wlo, cut, bar, total;
 };
 
 inline Layout layout(int64_t L, int k, int64_t blocks)
@@ -118,7 +119,6 @@ inline Layout layout(int64_t L, int k, int64_t blocks)
     o.r = take(L * k * 8);
     o.p = take(L * kp * 8);
     o.ap = take(L * k * 8);
-    o.ap2 = take(L * k * 8);
     const int64_t warps = blocks * (threads_for(k) / 32);
     o.carry = take(warps * 2 * k * 8);
     // partials: p'Ap, ||R||^2, R'dinv R, ||B||^2 per column, then the dense
@@ -338,16 +338,31 @@ __device__ __forceinline__ void finish_row(int64_t row, const T (&acc)[K], int64
 // up to LPR x the unroll, so matrices of short rows (S's big block once the
 // years are split off: ~16 nonzeros a row) run with 4 lanes a row and twice
 // the rows in flight.
-template <int K, int VS, int VW, typename T, int LPR = 8>
+//   DENSE (S in the split form, see kSmall): a big row's products with the
+// small levels ride the same round trips -- the row's 16 values of `cross`
+// (JPL a lane: one vector load) are loaded beside its indices and values,
+// multiplied by the small levels' entries of V (s_ps, shared memory) into
+// the row's sum, and multiplied by the row's own V into the small rows'
+// products, which are summed over the subgroups of each step and added, in
+// step order, to this warp's slots s_colw (kSmall x K, zeroed here).  Only
+// the warp holding a row's first nonzero does this for the row.
+template <int K, int VS, int VW, typename T, int LPR = 8, bool DENSE = false>
 __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T *__restrict__ V,
-                           T *__restrict__ out, T *carry, double (&dot)[K], bool want_dot)
+                           T *__restrict__ out, T *carry, double (&dot)[K], bool want_dot,
+                           const double *s_ps = nullptr, double *s_colw = nullptr)
 {
     static_assert(LPR == 2 || LPR == 4 || LPR == 8, "short rows take 2, 4 or 8 lanes");
+    static_assert(!DENSE || sizeof(T) == 8, "the dense block is FP64");
     constexpr int RPS = 32 / LPR;       // short rows per step
+    constexpr int JPL = kSmall / LPR;   // a short row's small levels a lane
     const int lane = threadIdx.x & 31, sub = lane / LPR, sl = lane % LPR;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int64_t lo = a.wlo[gw];
     const int64_t hi = a.wlo[gw + 1];
+    if constexpr (DENSE) {
+        for (int t = lane; t < kSmall * K; t += 32) s_colw[t] = 0.0;
+        __syncwarp();
+    }
     if (lo >= hi) return;
     int64_t r0 = a.wfirst[gw];
     for (;;) {
@@ -367,17 +382,30 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
             if ((longmask >> j) & 1u) {
                 // one long row, the whole warp
                 const int64_t rs = __shfl_sync(kFull, cs, j), re = __shfl_sync(kFull, ce, j);
+                const int64_t row_st = __shfl_sync(kFull, st, j), row_en = __shfl_sync(kFull, en, j);
+                // DENSE: lanes 0..15 take one small level each
+                const bool dense = DENSE && r0 + j < a.Lb && row_st >= lo && lane < kSmall;
                 T vrow[K];
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    vrow[k] = (want_dot && lane == 0) ? V[(r0 + j) * VS + k] : T(0);
+                    vrow[k] = ((want_dot && lane == 0) || dense) ? V[(r0 + j) * VS + k] : T(0);
+                const double cv1 = dense ? __ldcs(a.cross + (r0 + j) * kSmall + lane) : 0.0;
                 T acc[K];
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = T(0);
                 row_products<K, VS, VW, 32, T>(a, vals, V, rs + lane, re, acc);
+                if constexpr (DENSE) {
+                    if (dense) {
+#pragma unroll
+                        for (int k = 0; k < K; k++) {
+                            acc[k] += cv1 * s_ps[lane * K + k];
+                            s_colw[lane * K + k] += cv1 * vrow[k];
+                        }
+                    }
+                    __syncwarp();
+                }
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = warp_sum(acc[k]);
-                const int64_t row_st = __shfl_sync(kFull, st, j), row_en = __shfl_sync(kFull, en, j);
                 if (lane == 0)
                     finish_row<K, T>(r0 + j, acc, row_st, row_en, lo, hi, gw, vrow, out, carry,
                                      dot, want_dot);
@@ -392,14 +420,48 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
                 const int64_t rs = __shfl_sync(kFull, cs, src), re = __shfl_sync(kFull, ce, src);
                 const int64_t row_st = __shfl_sync(kFull, st, src);
                 const int64_t row_en = __shfl_sync(kFull, en, src);
+                const int64_t row = r0 + j + sub;
+                // DENSE: this lane's JPL small levels of the row, loaded with
+                // its indices and values
+                const bool dense = DENSE && mine && row < a.Lb && row_st >= lo;
                 T vrow[K];
 #pragma unroll
                 for (int k = 0; k < K; k++)
-                    vrow[k] = (want_dot && mine && sl == 0) ? V[(r0 + j + sub) * VS + k] : T(0);
+                    vrow[k] = ((want_dot && mine && sl == 0) || dense) ? V[row * VS + k] : T(0);
+                double cv[DENSE ? JPL : 1];
+                if constexpr (DENSE) {
+                    const double2 *cp =
+                        reinterpret_cast<const double2 *>(a.cross + row * kSmall + sl * JPL);
+#pragma unroll
+                    for (int q = 0; q < JPL / 2; q++) {
+                        const double2 t2 = dense ? __ldcs(cp + q) : make_double2(0.0, 0.0);
+                        cv[2 * q] = t2.x;
+                        cv[2 * q + 1] = t2.y;
+                    }
+                }
                 T acc[K];
 #pragma unroll
                 for (int k = 0; k < K; k++) acc[k] = T(0);
                 if (mine) row_products<K, VS, VW, LPR, T>(a, vals, V, rs + sl, re, acc);
+                if constexpr (DENSE) {
+#pragma unroll
+                    for (int q = 0; q < JPL; q++)
+#pragma unroll
+                        for (int k = 0; k < K; k++) acc[k] += cv[q] * s_ps[(sl * JPL + q) * K + k];
+                    // the small rows' products: this step's rows summed over the
+                    // subgroups, then added to the warp's slots by lanes 0..LPR-1
+#pragma unroll
+                    for (int q = 0; q < JPL; q++) {
+#pragma unroll
+                        for (int k = 0; k < K; k++) {
+                            double pc = cv[q] * vrow[k];
+#pragma unroll
+                            for (int o = LPR; o < 32; o <<= 1) pc += __shfl_xor_sync(kFull, pc, o);
+                            if (lane < LPR) s_colw[(sl * JPL + q) * K + k] += pc;
+                        }
+                    }
+                    __syncwarp();
+                }
 #pragma unroll
                 for (int k = 0; k < K; k++)
 #pragma unroll
@@ -475,74 +537,11 @@ __device__ __forceinline__ void block_partials(double (&v)[N], double *scratch, 
 template <int K, int VS>
 __device__ __forceinline__ void load_small(const Params &a, const double *V, double *s_ps)
 {
-    if ((int)threadIdx.x < a.ns * K) {
+    if ((int)threadIdx.x < kSmall * K) {        // zeros past the small levels
         const int j = threadIdx.x / K, k = threadIdx.x % K;
-        s_ps[threadIdx.x] = V[(a.Lb + j) * VS + k];
+        s_ps[threadIdx.x] = j < a.ns ? V[(a.Lb + j) * VS + k] : 0.0;
     }
     __syncthreads();
-}
-
-// The big rows against the small levels, a lane per small level (j = lane %
-// 16), a half-warp per row: AP2[r] = cross[r] . ps (a 16-lane sum) and, per
-// lane, col[k] += cross[r, j] V[r, k] (the small rows' products, summed over
-// rows).  dot[k] += V[r, k] AP2[r, k] when want_dot.  A warp takes
-// dense_rows_per_trip(K) rows per trip (rows r0 + 2u + half), all their loads
-// issued before any is used; the trips are grid-strided.  The lanes' column
-// sums go to s_col[warp] (kSmall x K).
-__host__ __device__ constexpr int dense_rows_per_trip(int k) { return k <= 2 ? 2 : 8; }
-template <int K, int VS>
-__device__ __forceinline__ void dense_rows(const Params &a, const double *V, const double *s_ps,
-                                           double *s_col, double (&dot)[K], bool want_dot)
-{
-    constexpr int kDenseRows = dense_rows_per_trip(K);
-    constexpr int RU = kDenseRows / 2;
-    const int lane = threadIdx.x & 31, half = lane >> 4, j = lane & 15;
-    const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int64_t W = (int64_t)gridDim.x * (blockDim.x >> 5);
-    double psj[K], col[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        psj[k] = j < a.ns ? s_ps[j * K + k] : 0.0;
-        col[k] = 0.0;
-    }
-    for (int64_t r0 = kDenseRows * gw; r0 < a.Lb; r0 += kDenseRows * W) {   // warp-uniform
-        double b[RU], pr[RU][K];
-#pragma unroll
-        for (int u = 0; u < RU; u++) {
-            const int64_t r = r0 + 2 * u + half;
-            const bool in = r < a.Lb;
-            b[u] = in ? __ldcs(a.cross + r * kSmall + j) : 0.0;
-#pragma unroll
-            for (int k = 0; k < K; k++) pr[u][k] = in ? V[r * VS + k] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < RU; u++) {
-            const int64_t r = r0 + 2 * u + half;
-            double t[K];
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-                t[k] = b[u] * psj[k];
-                col[k] += b[u] * pr[u][k];
-            }
-#pragma unroll
-            for (int k = 0; k < K; k++)
-#pragma unroll
-                for (int o = 8; o > 0; o >>= 1) t[k] += __shfl_xor_sync(kFull, t[k], o);
-            if (r < a.Lb && j == 0) {
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    a.AP2[r * K + k] = t[k];
-                    if (want_dot) dot[k] += pr[u][k] * t[k];
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < K; k++) col[k] += __shfl_xor_sync(kFull, col[k], 16);
-    if (lane < kSmall) {
-#pragma unroll
-        for (int k = 0; k < K; k++) s_col[(threadIdx.x >> 5) * kSmall * K + lane * K + k] = col[k];
-    }
 }
 
 // This CTA's column sums (over its warps, in order) to partials qc .. qc +
@@ -599,7 +598,9 @@ __device__ __forceinline__ void dense_small_rows(const Params &a, const double *
     __syncthreads();
 }
 
-template <int K, int LPR = 8>
+// SPLIT: S in the split form (a.ns > 0); the kernels for the whole CSR carry
+// none of its code (and none of its registers)
+template <int K, int LPR = 8, bool SPLIT = false>
 __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 {
     constexpr int KP = Stride<K>::P;
@@ -645,14 +646,16 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 #pragma unroll
     for (int k = 0; k < K; k++) dot[k] = 0.0;
     if (a.X0 != nullptr) {
-        spmm_range<K, K, 1, double, LPR>(a, a.data, a.X0, a.AP, a.carry, dot, false);
-        if (a.ns > 0) {
+        if ((SPLIT && a.ns > 0)) {
             load_small<K, K>(a, a.X0, s_ps);
-            dense_rows<K, K>(a, a.X0, s_ps, s_col, dot, false);
+            spmm_range<K, K, 1, double, LPR, true>(a, a.data, a.X0, a.AP, a.carry, dot, false,
+                                                   s_ps, s_col + warp * kSmall * K);
             dense_partials<K>(a, s_ps, s_col, s_cta, kQc, nb, dot, false);
+        } else {
+            spmm_range<K, K, 1, double, LPR>(a, a.data, a.X0, a.AP, a.carry, dot, false);
         }
         if (!gb.sync()) return;
-        if (a.ns > 0) dense_small_rows<K>(a, s_ps, kQc, s_aps);
+        if ((SPLIT && a.ns > 0)) dense_small_rows<K>(a, s_ps, kQc, s_aps);
     }
     {
         double sb[K], sr[K], sz[K];
@@ -683,21 +686,14 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 ap[k] = (a.X0 != nullptr && !empty) ? a.AP[r * K + k] : 0.0;
-                if (a.X0 != nullptr && a.ns > 0)
-                    ap[k] = r < a.Lb ? ap[k] + a.AP2[r * K + k] : s_aps[(r - a.Lb) * K + k];
+                if (a.X0 != nullptr && (SPLIT && a.ns > 0) && r >= a.Lb) ap[k] = s_aps[(r - a.Lb) * K + k];
             }
             setup_row(r, ap);
         }
         if (a.X0 != nullptr) {
             int64_t r;
             double ap[K];
-            if (finish_cut_row<K, double>(a, a.carry, r, ap) && lane == 0) {
-                if (a.ns > 0) {
-#pragma unroll
-                    for (int k = 0; k < K; k++) ap[k] += a.AP2[r * K + k];
-                }
-                setup_row(r, ap);
-            }
+            if (finish_cut_row<K, double>(a, a.carry, r, ap) && lane == 0) setup_row(r, ap);
         }
         {
             double v[3 * K];
@@ -738,12 +734,14 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
             for (int k = 0; k < K; k++) dot[k] = 0.0;
             // P's rows are KP wide from a 256-byte aligned workspace: 32-byte
             // rows for k = 3, 4
-            spmm_range<K, KP, (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1), double, LPR>(
-                a, a.data, a.P, a.AP, a.carry, dot, true);
-            if (a.ns > 0) {
+            constexpr int VWP = (KP == 4) ? 4 : ((KP % 2 == 0) ? 2 : 1);
+            if ((SPLIT && a.ns > 0)) {
                 load_small<K, KP>(a, a.P, s_ps);
-                dense_rows<K, KP>(a, a.P, s_ps, s_col, dot, true);
+                spmm_range<K, KP, VWP, double, LPR, true>(a, a.data, a.P, a.AP, a.carry, dot,
+                                                          true, s_ps, s_col + warp * kSmall * K);
                 dense_partials<K>(a, s_ps, s_col, s_cta, kQc, nb, dot, true);
+            } else {
+                spmm_range<K, KP, VWP, double, LPR>(a, a.data, a.P, a.AP, a.carry, dot, true);
             }
             block_partials<K>(dot, s_scratch, a.part, 0, nb);
             if (!gb.sync()) return;
@@ -754,7 +752,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                 }
             }
             __syncthreads();
-            if (a.ns > 0) dense_small_rows<K>(a, s_ps, kQc, s_aps);
+            if ((SPLIT && a.ns > 0)) dense_small_rows<K>(a, s_ps, kQc, s_aps);
             double alpha[K];
 #pragma unroll
             for (int k = 0; k < K; k++) {
@@ -772,8 +770,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                 for (int k = 0; k < K; k++) {
                     const double p = a.P[r * KP + k];
                     a.X[r * K + k] += alpha[k] * p;
-                    const double apk = a.ns > 0 ? ap[k] + a.AP2[r * K + k] : ap[k];
-                    const double res = a.R[r * K + k] - alpha[k] * apk;
+                    const double res = a.R[r * K + k] - alpha[k] * ap[k];
                     a.R[r * K + k] = res;
                     sr[k] += res * res;
                     sz[k] += res * res * di;
@@ -797,9 +794,7 @@ __global__ void __launch_bounds__(threads_for(K), 1) pcg_kernel(Params a)
                     for (int k = 0; k < K; k++) {
                         p[u][k] = use ? a.P[r * KP + k] : 0.0;
                         ap[u][k] = (use && !empty) ? a.AP[r * K + k] : 0.0;
-                        if (use && a.ns > 0)
-                            ap[u][k] = r < a.Lb ? ap[u][k] + a.AP2[r * K + k]
-                                                : s_aps[(r - a.Lb) * K + k];
+                        if (use && (SPLIT && a.ns > 0) && r >= a.Lb) ap[u][k] = s_aps[(r - a.Lb) * K + k];
                         x[u][k] = use ? a.X[r * K + k] : 0.0;
                         rr[u][k] = use ? a.R[r * K + k] : 0.0;
                     }
@@ -951,8 +946,9 @@ template <int K, int LPR = 8>
 cudaError_t launch(Params p, int blocks, cudaStream_t s)
 {
     void *args[] = {&p};
-    return cudaLaunchCooperativeKernel((const void *)pcg_kernel<K, LPR>, dim3(blocks),
-                                       dim3(threads_for(K)), args, 0, s);
+    const void *fn = p.ns > 0 ? (const void *)pcg_kernel<K, LPR, true>
+                              : (const void *)pcg_kernel<K, LPR, false>;
+    return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads_for(K)), args, 0, s);
 }
 
 // HDFE_PCG_SHORT_LPR lanes a short row when S's rows average at most this
@@ -1578,7 +1574,6 @@ int solve_registers(const int64_t *indptr, const int32_t *indices, const double 
     p.R = (double *)(ws + lay.r);
     p.P = (double *)(ws + lay.p);
     p.AP = (double *)(ws + lay.ap);
-    p.AP2 = (double *)(ws + lay.ap2);
     p.carry = (double *)(ws + lay.carry);
     p.part = (double *)(ws + lay.part);
     p.wfirst = (int64_t *)(ws + lay.wfirst);
