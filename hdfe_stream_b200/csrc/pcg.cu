@@ -308,6 +308,40 @@ __device__ __forceinline__ void row_products(const Params &a, const T *vals, con
     }
 }
 
+// The small rows' products of one step of short rows (DENSE spmm_range):
+// lane (subgroup, sl) holds cv[q] = cross[row, sl JPL + q] of its subgroup's
+// row and that row's V; the K products per q are summed over the subgroups
+// by a reduce-scatter (the two top subgroup bits halve the K <= 4 values
+// between partner lanes, the rest of the subgroup bits sum the one value
+// left), and one lane per (small level, column) adds the total to the warp's
+// slot: 2 + 1 + (log2(32 / LPR) - 2) shuffles per q instead of K
+// log2(32 / LPR).  A fixed tree, so the sums are deterministic.
+template <int K, int LPR, int JPL>
+__device__ __forceinline__ void col_step(const double (&cv)[JPL], const double (&vrow)[K],
+                                         double *s_colw, int lane, int sl)
+{
+    static_assert(K <= 4 && LPR <= 8, "four columns, at least four subgroups");
+    const bool h = (lane >> 4) & 1, g = (lane >> 3) & 1;
+    constexpr int kLowMask = 7 & ~(LPR - 1);       // subgroup bits below bit 3
+    const int vi = 2 * (int)h + (int)g;             // the value this lane ends with
+#pragma unroll
+    for (int q = 0; q < JPL; q++) {
+        const double v0 = cv[q] * vrow[0];
+        const double v1 = K > 1 ? cv[q] * vrow[K > 1 ? 1 : 0] : 0.0;
+        const double v2 = K > 2 ? cv[q] * vrow[K > 2 ? 2 : 0] : 0.0;
+        const double v3 = K > 3 ? cv[q] * vrow[K > 3 ? 3 : 0] : 0.0;
+        // lanes with bit 4 set keep values 2, 3; the others 0, 1
+        double k0 = h ? v2 : v0, k1 = h ? v3 : v1;
+        k0 += __shfl_xor_sync(kFull, h ? v0 : v2, 16);
+        k1 += __shfl_xor_sync(kFull, h ? v1 : v3, 16);
+        // then bit 3 picks one of the two
+        double b = (g ? k1 : k0) + __shfl_xor_sync(kFull, g ? k0 : k1, 8);
+#pragma unroll
+        for (int o = 4; o >= LPR; o >>= 1) b += __shfl_xor_sync(kFull, b, o);
+        if (vi < K && (lane & kLowMask) == 0) s_colw[(sl * JPL + q) * K + vi] += b;
+    }
+}
+
 // vrow: V[row, 0..K), loaded before the row's products (for p'Ap)
 template <int K, typename T>
 __device__ __forceinline__ void finish_row(int64_t row, const T (&acc)[K], int64_t row_st,
@@ -449,17 +483,8 @@ __device__ void spmm_range(const Params &a, const T *__restrict__ vals, const T 
 #pragma unroll
                         for (int k = 0; k < K; k++) acc[k] += cv[q] * s_ps[(sl * JPL + q) * K + k];
                     // the small rows' products: this step's rows summed over the
-                    // subgroups, then added to the warp's slots by lanes 0..LPR-1
-#pragma unroll
-                    for (int q = 0; q < JPL; q++) {
-#pragma unroll
-                        for (int k = 0; k < K; k++) {
-                            double pc = cv[q] * vrow[k];
-#pragma unroll
-                            for (int o = LPR; o < 32; o <<= 1) pc += __shfl_xor_sync(kFull, pc, o);
-                            if (lane < LPR) s_colw[(sl * JPL + q) * K + k] += pc;
-                        }
-                    }
+                    // subgroups and added to the warp's slots
+                    if constexpr (K <= 4) col_step<K, LPR, JPL>(cv, vrow, s_colw, lane, sl);
                     __syncwarp();
                 }
 #pragma unroll
@@ -946,8 +971,10 @@ template <int K, int LPR = 8>
 cudaError_t launch(Params p, int blocks, cudaStream_t s)
 {
     void *args[] = {&p};
-    const void *fn = p.ns > 0 ? (const void *)pcg_kernel<K, LPR, true>
-                              : (const void *)pcg_kernel<K, LPR, false>;
+    const void *fn = (const void *)pcg_kernel<K, LPR, false>;
+    if constexpr (K <= HDFE_PCG_SMALL_MAX_K) {
+        if (p.ns > 0) fn = (const void *)pcg_kernel<K, LPR, true>;
+    }
     return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(threads_for(K)), args, 0, s);
 }
 
