@@ -88,12 +88,14 @@ struct Args {
     int64_t *lptr;              // (L+1)
     int32_t *fillpos;
     int32_t *lgrp;
+    double *lwv;                // beside lgrp: u_r / N_g of the (level r, group g) pair
     int64_t *rnnz;              // (L+1) row nnz
     int64_t *toff;              // (L+1) temp offsets of the narrow rows
     int32_t *wide_list;         // wide index -> level
     int32_t *warp_rows, *block_rows;
     int64_t *tiles;             // scan partials
     int64_t *ctr;               // [0] W, [1] warp rows, [2] block rows, [3] lgrp len,
+                                // [7] bit d: dimension d has narrow levels,
                                 // [4] nnz, [5] temp len
     unsigned *status;
     // wide workspace
@@ -155,6 +157,7 @@ __global__ void __launch_bounds__(kThreads) k_level_stats(Args a)
 
 __global__ void __launch_bounds__(kThreads) k_classify(Args a)
 {
+    unsigned dims = 0;          // dimensions of this thread's narrow levels
     for (int64_t r = (int64_t)blockIdx.x * kThreads + threadIdx.x; r < a.L;
          r += (int64_t)gridDim.x * kThreads) {
         const unsigned long long w = a.work[r];
@@ -192,7 +195,11 @@ __global__ void __launch_bounds__(kThreads) k_classify(Args a)
         const bool narrow = k == kKindWarp || k == kKindBlock;
         a.lptr[r] = narrow ? lc : 0;
         a.toff[r] = narrow ? cap : 0;   // capacity of the row in the temp buffer
+        if (narrow) dims |= 1u << level_dim(a, r);
     }
+    dims = __reduce_or_sync(0xffffffffu, dims);
+    if ((threadIdx.x & 31) == 0 && dims != 0)
+        atomicOr(reinterpret_cast<unsigned long long *>(a.ctr + 7), (unsigned long long)dims);
 }
 
 // the wide list in level order, so wide indices do not depend on atomics
@@ -277,30 +284,107 @@ __global__ void __launch_bounds__(kThreads) k_scan_apply(const int64_t *x, int64
 
 // ------------------------------------------------------- group lists
 
-__global__ void __launch_bounds__(kThreads) k_fill_lists(Args a)
+// A thread per group.  Per dimension, each level's first cell in the group
+// appends the group to the level's list, with u_r / N_g beside it (u_r = n
+// summed over the group's cells at the level, in cell order).  When the
+// group's codes in the dimension are nondecreasing (pass 0's layout), a run
+// start is its level's first cell and the run holds all of the level's
+// cells; otherwise the group's cells are walked for both.  A warp takes 32
+// consecutive groups at a time and first stages their cells' codes and n in
+// shared memory by coalesced loads (a chunk of more than kListCap cells is
+// read in place), so each cell is fetched once.
+constexpr int kListWarps = 4;
+constexpr int kListCap = 384;                   // cells staged per warp
+
+inline size_t list_smem(int D) { return (size_t)kListWarps * kListCap * (8 + 4 * (size_t)D); }
+
+__device__ __forceinline__ void list_append(const Args &a, int64_t lv, int64_t g, double u)
 {
-    for (int64_t g = (int64_t)blockIdx.x * kThreads + threadIdx.x; g < a.G;
-         g += (int64_t)gridDim.x * kThreads) {
-        const int64_t s = a.starts[g], e = a.starts[g + 1];
-        for (int d = 0; d < a.D; d++) {
-            uint32_t prev = 0xffffffffu;
-            for (int64_t i = s; i < e; i++) {
-                const uint32_t c = a.codes[i * a.D + d];
-                if (c == prev || (int64_t)c >= a.nlev[d]) continue;    // a run of one level
-                prev = c;
-                const int64_t lv = a.offs[d] + c;
-                const int32_t k = a.kind[lv];
-                if (k != kKindWarp && k != kKindBlock) continue;        // no list for wide rows
-                bool first = true;
-                for (int64_t j = s; j < i; j++)
-                    if (a.codes[j * a.D + d] == c) { first = false; break; }
-                if (!first) continue;
-                {
-                    const int32_t at = atomicAdd(a.fillpos + lv, 1);
-                    if (a.lptr[lv] + at < a.lptr[lv + 1]) a.lgrp[a.lptr[lv] + at] = (int32_t)g;
+    const int32_t at = atomicAdd(a.fillpos + lv, 1);
+    if (a.lptr[lv] + at < a.lptr[lv + 1]) {
+        a.lgrp[a.lptr[lv] + at] = (int32_t)g;
+        a.lwv[a.lptr[lv] + at] = u / a.group_n[g];
+    }
+}
+
+__device__ __forceinline__ bool listed(const Args &a, int64_t lv)
+{
+    const int32_t k = a.kind[lv];
+    return k == kKindWarp || k == kKindBlock;       // no list for wide rows
+}
+
+// the group's lists from codes cd (stride D) and weights nw, both indexed
+// from the group's first cell
+__device__ void group_lists(const Args &a, int64_t g, int cells, const uint32_t *cd,
+                            const double *nw)
+{
+    const int D = a.D;
+    const int64_t dims = a.ctr[7];
+    for (int d = 0; d < D; d++) {
+        if (!((dims >> d) & 1)) continue;           // no narrow level in this dimension
+        bool sorted = true;
+        for (int i = 1; i < cells; i++) sorted &= cd[(i - 1) * D + d] <= cd[i * D + d];
+        if (sorted) {
+            for (int i = 0; i < cells;) {
+                const uint32_t c = cd[i * D + d];
+                int j = i + 1;
+                while (j < cells && cd[j * D + d] == c) j++;
+                if ((int64_t)c < a.nlev[d] && listed(a, a.offs[d] + c)) {
+                    double u = nw[i];
+                    for (int q = i + 1; q < j; q++) u += nw[q];
+                    list_append(a, a.offs[d] + c, g, u);
                 }
+                i = j;
             }
+            continue;
         }
+        uint32_t prev = 0xffffffffu;
+        for (int i = 0; i < cells; i++) {
+            const uint32_t c = cd[i * D + d];
+            if (c == prev || (int64_t)c >= a.nlev[d]) continue;        // a run of one level
+            prev = c;
+            const int64_t lv = a.offs[d] + c;
+            if (!listed(a, lv)) continue;
+            bool first = true;
+            for (int j = 0; j < i; j++)
+                if (cd[j * D + d] == c) { first = false; break; }
+            if (!first) continue;
+            double u = 0.0;
+            for (int j = i; j < cells; j++)
+                if (cd[j * D + d] == c) u += nw[j];
+            list_append(a, lv, g, u);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kListWarps * 32) k_fill_lists(Args a)
+{
+    extern __shared__ double s_list_raw[];
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int D = a.D;
+    double *sn = s_list_raw + (size_t)wl * kListCap;
+    uint32_t *sc = reinterpret_cast<uint32_t *>(s_list_raw + (size_t)kListWarps * kListCap) +
+                   (size_t)wl * kListCap * D;
+    const int64_t chunks = (a.G + 31) / 32;
+    const int64_t wstep = (int64_t)gridDim.x * kListWarps;
+    for (int64_t ch = (int64_t)blockIdx.x * kListWarps + wl; ch < chunks; ch += wstep) {
+        const int64_t g0 = ch * 32;
+        const int ng = (int)min((int64_t)32, a.G - g0);
+        const int64_t g = g0 + lane;
+        const int64_t s = lane < ng ? a.starts[g] : 0, e = lane < ng ? a.starts[g + 1] : 0;
+        const int64_t c0 = __shfl_sync(0xffffffffu, s, 0);
+        const int64_t c1 = __shfl_sync(0xffffffffu, e, ng - 1);
+        const bool staged = c1 - c0 <= kListCap;            // warp-uniform
+        if (staged) {
+            for (int64_t q = lane; q < (c1 - c0) * D; q += 32) sc[q] = a.codes[c0 * D + q];
+            for (int64_t q = lane; q < c1 - c0; q += 32) sn[q] = a.n[c0 + q];
+        }
+        __syncwarp();
+        if (lane < ng) {
+            if (staged) group_lists(a, g, (int)(e - s), sc + (s - c0) * D, sn + (s - c0));
+            else group_lists(a, g, (int)(e - s), a.codes + s * D, a.n + s);
+        }
+        __syncwarp();
     }
 }
 
@@ -375,9 +459,25 @@ __device__ void warp_rank_sort(int32_t *key, double *val, int n, int lane)
     __syncwarp();
 }
 
+// The same for n <= 32 keys: one key a lane.
+__device__ void warp_rank_sort32(int32_t *key, double *val, int n, int lane)
+{
+    const int32_t k = lane < n ? key[lane] : INT32_MAX;
+    const double v = (val && lane < n) ? val[lane] : 0.0;
+    int rank = 0;
+    for (int j = 0; j < n; j++) rank += __shfl_sync(0xffffffffu, k, j) < k;
+    __syncwarp();
+    if (lane < n) {
+        key[rank] = k;
+        if (val) val[rank] = v;
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ void warp_sort(int32_t *key, double *val, int n, int lane)
 {
-    if (n <= 128) warp_rank_sort(key, val, n, lane);
+    if (n <= 32) warp_rank_sort32(key, val, n, lane);
+    else if (n <= 128) warp_rank_sort(key, val, n, lane);
     else warp_bitonic(key, val, n, lane);
 }
 
@@ -409,20 +509,18 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
     // the row's groups, ascending
     const int64_t l0 = a.lptr[r];
     const int nl = (int)(a.lptr[r + 1] - l0);
-    for (int i = lane; i < nl; i += 32) sm.list[i] = a.lgrp[l0 + i];
-    if (lane == 0) *sm.cnt = 0;
+    for (int i = lane; i < nl; i += 32) {
+        sm.list[i] = a.lgrp[l0 + i];
+        sm.wv[i] = a.lwv[l0 + i];
+    }
     __syncwarp();
-    warp_sort(sm.list, nullptr, nl, lane);
-    // per group: first cell, cell count, u_r / N_g (one lane per group)
+    warp_sort(sm.list, sm.wv, nl, lane);
+    // per group: first cell and cell count (u_r / N_g came with the list)
     for (int k = lane; k < nl; k += 32) {
         const int64_t g = sm.list[k];
         const int64_t s = a.starts[g], e = a.starts[g + 1];
-        double ur = 0.0;
-        for (int64_t i = s; i < e; i++)
-            if (a.codes[i * a.D + dr] == lr) ur += a.n[i];
         sm.gs[k] = s;
         sm.loff[k] = (int32_t)(e - s);
-        sm.wv[k] = ur / a.group_n[g];
     }
     __syncwarp();
     // exclusive offsets of the groups' cells (the row's items)
@@ -473,11 +571,13 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
             } else if (valid && lane == leader) {
                 double sum = 0.0;
                 for (unsigned p = peers; p; p &= p - 1) sum += sm.stage[__ffs(p) - 1];
+                // the leaders' columns are distinct, so a slot found holding col
+                // is this lane's alone; an empty one is claimed by a CAS
                 uint32_t h = slot_of(col, bits);
                 for (int probe = 0; probe < slots; probe++) {
-                    const int32_t old = atomicCAS(sm.keys + h, kEmptyKey, col);
+                    int32_t old = sm.keys[h];
+                    if (old == kEmptyKey) old = atomicCAS(sm.keys + h, kEmptyKey, col);
                     if (old == kEmptyKey || old == col) {
-                        if (old == kEmptyKey) atomicAdd(sm.cnt, 1);
                         sm.vals[h] += sum;
                         break;
                     }
@@ -487,10 +587,7 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
             __syncwarp();
         }
     }
-    __syncwarp();
-    const int cnt = *sm.cnt;
-    // compact the table to its first cnt slots (entries never overtake unread slots)
-    __syncwarp();
+    // compact the table to its first slots (entries never overtake unread slots)
     if (lane == 0) *sm.cnt = 0;
     __syncwarp();
     for (int base = 0; base < slots; base += 32) {
@@ -507,6 +604,7 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
         if (lane == 0) *sm.cnt = at0 + __popc(m);
         __syncwarp();
     }
+    const int cnt = *sm.cnt;
     warp_sort(sm.keys, sm.vals, cnt, lane);
     const int64_t t0 = a.toff[r];
     for (int i = lane; i < cnt; i += 32) {
@@ -921,7 +1019,7 @@ __global__ void k_write_info(Args a, hdfe_sbuild_info *info)
 // --------------------------------------------------------------- host
 
 struct Layout {
-    int64_t lcount, work, kind, lptr, fillpos, lgrp, rnnz, toff, wide_list, warp_rows,
+    int64_t lcount, work, kind, lptr, fillpos, lgrp, lwv, rnnz, toff, wide_list, warp_rows,
         block_rows, tiles, ctr, status, total;
 };
 
@@ -936,6 +1034,7 @@ inline Layout layout(int64_t L, int64_t M, int D)
     o.lptr = take((L + 1) * 8);
     o.fillpos = take(L * 4);
     o.lgrp = take(M * (int64_t)D * 4);
+    o.lwv = take(M * (int64_t)D * 8);
     o.rnnz = take((L + 1) * 8);
     o.toff = take((L + 1) * 8);
     o.wide_list = take(L * 4);
@@ -1015,6 +1114,7 @@ int setup(Ctx &c, const int64_t *starts, int64_t G, const uint32_t *codes, int32
     a.lptr = (int64_t *)(b + lay.lptr);
     a.fillpos = (int32_t *)(b + lay.fillpos);
     a.lgrp = (int32_t *)(b + lay.lgrp);
+    a.lwv = (double *)(b + lay.lwv);
     a.rnnz = (int64_t *)(b + lay.rnnz);
     a.toff = (int64_t *)(b + lay.toff);
     a.wide_list = (int32_t *)(b + lay.wide_list);
@@ -1152,7 +1252,17 @@ static int analyze_impl(const int64_t *starts, int64_t n_groups, const uint32_t 
     HDFE_CUDA_TRY(cudaGetLastError());
     if ((st = scan_exclusive(c, a.lptr, a.L, a.lptr, a.ctr + 3)) != HDFE_OK) return st;
     if ((st = scan_exclusive(c, a.toff, a.L, a.toff, a.ctr + 5)) != HDFE_OK) return st;
-    k_fill_lists<<<grid_for(a.G, kThreads, cap), kThreads, 0, c.s>>>(a);
+    {
+        const size_t smem = list_smem(a.D);
+        HDFE_CUDA_TRY(cudaFuncSetAttribute(k_fill_lists,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per = 0;
+        HDFE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fill_lists,
+                                                                  kListWarps * 32, smem));
+        const int64_t ctas = ((a.G + 31) / 32 + kListWarps - 1) / kListWarps;
+        k_fill_lists<<<grid_for(ctas, 1, c.sms * (per > 0 ? per : 1)), kListWarps * 32, smem,
+                       c.s>>>(a);
+    }
     k_write_info<<<1, 32, 0, c.s>>>(a, info);
     HDFE_CUDA_TRY(cudaGetLastError());
     hdfe_add_launches(launched + 11);
