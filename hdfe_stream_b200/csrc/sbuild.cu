@@ -95,7 +95,8 @@ struct Args {
     int32_t *warp_rows, *block_rows;
     int64_t *tiles;             // scan partials
     int64_t *ctr;               // [0] W, [1] warp rows, [2] block rows, [3] lgrp len,
-                                // [7] bit d: dimension d has narrow levels,
+                                // [7] bit d: dimension d has narrow levels, bit 8 + d:
+                                // wide levels,
                                 // [4] nnz, [5] temp len
     unsigned *status;
     // wide workspace
@@ -196,6 +197,7 @@ __global__ void __launch_bounds__(kThreads) k_classify(Args a)
         a.lptr[r] = narrow ? lc : 0;
         a.toff[r] = narrow ? cap : 0;   // capacity of the row in the temp buffer
         if (narrow) dims |= 1u << level_dim(a, r);
+        if (k >= 0) dims |= 1u << (8 + level_dim(a, r));
     }
     dims = __reduce_or_sync(0xffffffffu, dims);
     if ((threadIdx.x & 31) == 0 && dims != 0)
@@ -764,6 +766,7 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
         eb[t] = en < E ? en % W : 0;
     }
     double dsum = 0.0;          // lane a < W: sum of u_a
+    const int wdims = (int)(a.ctr[7] >> 8) & 0xff;     // dimensions with wide levels
     unsigned pat = 0;           // lane a < W: levels sharing a group with a
     const int64_t chunks = (a.G + 31) / 32;
     const int64_t wstep = (int64_t)gridDim.x * kWideWarps;
@@ -776,7 +779,7 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
         __syncwarp();
         const int64_t c0 = gs[0], c1 = gs[ng];
         // the chunk's cells, kWideRounds rounds of 32 at a time: every round's
-        // loads (n and the wide indices) issued before the first is used
+        // loads (n, the codes and their levels' wide indices) issued before the first is used
         for (int64_t b0 = c0; b0 < c1; b0 += 32 * kWideRounds) {
           int gqr[kWideRounds];
           double nir[kWideRounds];
@@ -799,7 +802,11 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
                 nir[t] = a.n[i];
 #pragma unroll
                 for (int d = 0; d < HDFE_MAX_DIMS; d++)
-                    if (d < a.D) kr[t][d] = a.cell_widx[i * a.D + d];
+                    if (d < a.D && ((wdims >> d) & 1)) {
+                        const uint32_t c = a.codes[i * a.D + d];
+                        const int32_t k = (int64_t)c < a.nlev[d] ? a.kind[a.offs[d] + c] : -1;
+                        kr[t][d] = k >= 0 ? k : -1;
+                    }
             }
           }
 #pragma unroll
@@ -813,6 +820,7 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
 #pragma unroll
             for (int d = 0; d < HDFE_MAX_DIMS; d++) {
                 if (d >= a.D) break;
+                if (!((wdims >> d) & 1)) continue;      // no wide level in this dimension
                 const int32_t k = valid ? kr[t][d] : -1;
                 const int key = k >= 0 ? gq * 32 + k : -1 - lane;
                 const unsigned peers = __match_any_sync(0xffffffffu, key);
@@ -1330,8 +1338,10 @@ static int count_impl(const int64_t *starts, int64_t n_groups, const uint32_t *c
             HDFE_CUDA_TRY(cudaMemsetAsync(wide_workspace, 0, wl.dpres + n_wide * a.L, c.s));
         HDFE_CUDA_TRY(cudaMemsetAsync((char *)wide_workspace + wl.wcross, 0,
                                       n_wide * n_wide * 8, c.s));
-        k_cell_widx<<<grid_for(a.M * a.D, kThreads, c.sms * 8), kThreads, 0, c.s>>>(a);
-        launched++;
+        if (n_wide > kWideWarp) {       // the atomic wide block reads each cell's wide index
+            k_cell_widx<<<grid_for(a.M * a.D, kThreads, c.sms * 8), kThreads, 0, c.s>>>(a);
+            launched++;
+        }
     }
     HDFE_CUDA_TRY(cudaMemsetAsync(a.rnnz, 0, (a.L + 1) * 8, c.s));
     // one wave: as many CTAs as stay resident (the rows are grid-strided, so a
