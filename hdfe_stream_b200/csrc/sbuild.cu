@@ -501,11 +501,20 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
     const int lane = threadIdx.x & 31;
     const int dr = level_dim(a, r);
     const uint32_t lr = (uint32_t)(r - a.offs[dr]);
-    const int64_t cap = a.toff[r + 1] - a.toff[r];
+    const bool split = a.small_first < a.L;
+    // the table holds the row's hashed columns: all of them, or in the split
+    // form the big levels' alone (the small ones go to direct slots)
+    int64_t cap = a.toff[r + 1] - a.toff[r];
+    if (split) {
+        const int64_t w = (int64_t)a.work[r];
+        int64_t cb = 0;
+        for (int d = 0; d < a.D; d++)
+            if (a.offs[d] < a.small_first) cb += w < a.nlev[d] ? w : a.nlev[d];
+        cap = cb < cap ? cb : cap;
+    }
     int bits = ceil_log2((cap * 4 + 2) / 3);
     bits = bits < 5 ? 5 : (bits > max_bits ? max_bits : bits);
     const int slots = 1 << bits;
-    const bool split = a.small_first < a.L;
     for (int i = lane; i < slots; i += 32) { sm.keys[i] = kEmptyKey; sm.vals[i] = 0.0; }
     if (lane < kCross) sm.xs[lane] = 0.0;
     // the row's groups, ascending
@@ -613,7 +622,7 @@ __device__ void narrow_row(const Args &a, int64_t r, const RowSmem &sm, int max_
         const int32_t c = sm.keys[i];
         a.tcol[t0 + i] = c;
         a.tval[t0 + i] = sm.vals[i];
-        const int32_t k = a.kind[c];
+        const int32_t k = split ? -1 : a.kind[c];     // the split form has no wide column here
         if (k >= 0) {
             a.dpres[(int64_t)k * a.L + r] = 1;
             a.dval[(int64_t)k * a.L + r] = sm.vals[i];
