@@ -53,8 +53,7 @@ constexpr int kWarpListCap = 128;               // groups per warp row
 constexpr int kBlockListCap = 2048;             // groups per block row
 constexpr int32_t kEmptyKey = -1;
 constexpr int32_t kKindEmpty = -1, kKindWarp = -2, kKindBlock = -3, kKindWide = -100;
-constexpr int kWideWarp = 16;                   // wide x wide in warp registers up to this W
-constexpr int kWideEntries = (kWideWarp * kWideWarp + 31) / 32;   // entries per lane
+constexpr int kWideWarp = 16;                   // wide x wide on one warp's tiles up to this W
 constexpr int kScanTile = 4096;
 constexpr int64_t kSeg = 16384;                 // columns per wide-row segment
 constexpr int kWarpsPerCta = 4;
@@ -740,13 +739,24 @@ __global__ void __launch_bounds__(kThreads) k_cell_widx(Args a)
 // takes 32 consecutive groups at a time: their cells are read coalesced (one
 // per lane) and summed into the groups' u rows in shared memory (lanes with
 // the same group and level combined by __match_any_sync in lane order); then
-// each lane owns W^2 / 32 entries and adds the 32 groups' (u_a / N_g) u_b in
-// group order, lanes a < W add the diagonal's u_a, and the pattern is the
+// the 32 groups' (u_a / N_g) u_b are added as a 16 x 32 by 32 x 16 product on
+// the FP64 tensor cores (mma m8n8k4 tiles), lanes a < W add the diagonal's
+// u_a, and the pattern is the
 // union of the groups' level masks.  Cells with two or more wide levels
 // (several small dimensions) add their off-diagonal C, for every pair of
 // their wide levels, into its own array by atomic adds (exact for counts;
 // in atomic order for weighted n).  Warps and CTAs are summed in a fixed
 // order, so the rest of the block is deterministic.
+// D += A B for one 8 x 8 x 4 FP64 tile, the whole warp: A row-major (this lane
+// holds row lane / 4, column lane % 4), B column-major (row lane % 4, column
+// lane / 4), D (row lane / 4, columns 2 (lane % 4) and 2 (lane % 4) + 1)
+__device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
 constexpr int kWideThreads = 128;
 constexpr int kWideWarps = kWideThreads / 32;
 constexpr int kWideRounds = 4;          // rounds of 32 cells whose loads are in flight together
@@ -765,15 +775,10 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
     double (*u)[kWideWarp + 1] = s_u[wl];
     double (*wv)[kWideWarp + 1] = s_w[wl];
     int64_t *gs = s_gs[wl];
-    double acc[kWideEntries];
-    int ea[kWideEntries], eb[kWideEntries];
-#pragma unroll
-    for (int t = 0; t < kWideEntries; t++) {
-        acc[t] = 0.0;
-        const int en = lane + 32 * t;
-        ea[t] = en < E ? en / W : 0;
-        eb[t] = en < E ? en % W : 0;
-    }
+    // sum over groups of (u_a / N_g) u_b as 8 x 8 tiles (ta, tb) of the 16 x 16
+    // block: this lane holds entries (8 ta + lane / 4, 8 tb + 2 (lane % 4) + i)
+    double acc[2][2][2] = {};
+    const int r8 = lane >> 2, c4 = lane & 3;
     double dsum = 0.0;          // lane a < W: sum of u_a
     const int wdims = (int)(a.ctr[7] >> 8) & 0xff;     // dimensions with wide levels
     unsigned pat = 0;           // lane a < W: levels sharing a group with a
@@ -854,12 +859,13 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
           }
         }
         __syncwarp();
-        // each group's u / N_g and level mask
+        // each group's u / N_g and level mask; rows past the chunk's groups
+        // and columns past W are zeros (the tiles below read them)
         unsigned mask = 0;
-        if (lane < ng) {
-            const double inv = 1.0 / a.group_n[g0 + lane];
-            for (int k = 0; k < W; k++) {
-                const double x = u[lane][k];
+        {
+            const double inv = lane < ng ? 1.0 / a.group_n[g0 + lane] : 0.0;
+            for (int k = 0; k < kWideWarp; k++) {
+                const double x = (lane < ng && k < W) ? u[lane][k] : 0.0;
                 wv[lane][k] = x * inv;
                 if (x > 0.0) mask |= 1u << k;
             }
@@ -871,17 +877,32 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_block_warp(Args a)
                 if ((mq >> lane) & 1u) pat |= mq;
                 dsum += u[q][lane];
             }
+        }
+        // the chunk's products on the FP64 tensor cores: A (a x group) = u / N_g
+        // transposed, B (group x b) = u, four groups a step
 #pragma unroll
-            for (int t = 0; t < kWideEntries; t++) acc[t] += wv[q][ea[t]] * u[q][eb[t]];
+        for (int ks = 0; ks < 8; ks++) {
+            if (ks * 4 >= ng) break;                    // warp-uniform
+            const int q = ks * 4 + c4;
+            const double a0 = wv[q][r8], a1 = wv[q][8 + r8];
+            const double b0 = u[q][r8], b1 = u[q][8 + r8];
+            dmma_m8n8k4(acc[0][0], a0, b0);
+            dmma_m8n8k4(acc[0][1], a0, b1);
+            dmma_m8n8k4(acc[1][0], a1, b0);
+            dmma_m8n8k4(acc[1][1], a1, b1);
         }
         __syncwarp();
     }
     // the warp's entries, then the CTA's warps summed in order
 #pragma unroll
-    for (int t = 0; t < kWideEntries; t++) {
-        const int en = lane + 32 * t;
-        if (en < E) s_acc[wl][en] = -acc[t];
-    }
+    for (int ta = 0; ta < 2; ta++)
+#pragma unroll
+        for (int tb = 0; tb < 2; tb++)
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int ra = 8 * ta + r8, rb = 8 * tb + 2 * c4 + i;
+                if (ra < W && rb < W) s_acc[wl][ra * W + rb] = -acc[ta][tb][i];
+            }
     if (lane < W) s_pat[wl][lane] = pat;
     __syncwarp();
     if (lane < W) s_acc[wl][lane * W + lane] += dsum;
