@@ -180,8 +180,8 @@ def phase_bytes(rows, counts, S, iterations, m=3, small=None):
 
 # DRAM bytes (read + write) of one PCG iteration on the 5M-worker panel, from
 # an ncu capture of pcg_kernel<3, 4> (the split form of S) in this bench's
-# own command: 3.91 GB over 19 iterations and the set-up
-PCG_DRAM_BYTES_PER_ITER = (3279237888 + 631930368) / 19
+# own command: 3.22 GB over 19 iterations and the set-up
+PCG_DRAM_BYTES_PER_ITER = (3140617472 + 80062976) / 19
 
 
 def measured_peak():

@@ -14,7 +14,8 @@
 //             -> each level's class: "warp" rows (one warp, a shared hash of
 //             32-512 slots), "block" rows (one CTA, up to 8192 slots), or
 //             "wide" rows (levels of small dimensions such as years, present
-//             in most groups); the groups of each narrow level (lists).
+//             in most groups); the groups of each narrow level (lists),
+//             each with the pair's u_r / N_g.
 //   count     narrow rows, ONE pass: a warp sorts the row's groups (fixed
 //             summation order), flattens the row's (group, cell) items over
 //             all 32 lanes, and adds each item's v into the hash slot of each
