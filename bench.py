@@ -157,25 +157,27 @@ def phase_bytes(rows, counts, S, iterations, m=3, small=None):
     """Compulsory DRAM bytes per launch of each phase (written out in the
     design notes): pass 1 reads each row once and writes the identifying
     cells and level arrays; the S build reads the cells and writes S; one
-    PCG iteration reads S and streams the L x k vectors.  small: the fit's
-    info["small_block"] when S was built and solved in the split form -- the
-    build writes the big block's CSR and the dense cross block (first x 16
-    doubles); an iteration reads them once and writes and reads back the big
-    rows' products with the small levels (16 first m)."""
+    PCG iteration reads S and streams the L x k vectors: 12 nnz + 4 (L+1) +
+    72 L k on the whole S, the algorithm's figure whatever layout solves it
+    (the roofline's `achieved`).  small: the fit's info["small_block"] when S
+    was built and solved in the split form -- the build writes the big
+    block's CSR and the dense cross block (first x 16 doubles); that layout's
+    own iteration reads them once and writes and reads back the big rows'
+    products with the small levels (16 first m), fewer bytes than the whole
+    S's (reported beside, as "pcg_kernel_split")."""
     N, D, L = rows.n_rows, rows.codes.shape[1], int(sum(rows.n_levels))
     M, G = counts["n_ident_cells"], counts["n_ident_groups"]
     w = 0 if rows.w is None else 8
     p1 = N * (4 + 4 * D + 8 * m + w) + M * (4 * D + 8) + G * 16 + L * 8 * (3 + m)
     sb = M * (4 * D + 8) + G * 16 + S.nnz * 12 + (L + 1) * 8
-    per_it = 12 * S.nnz + 8 * (L + 1) + 8 * L * m * 9
+    per_it = 12 * S.nnz + 4 * (L + 1) + 8 * L * m * 9
+    out = {"pass1": p1, "sbuild": sb, "pcg_kernel": per_it * max(iterations, 1)}
     if small:
-        sb = (M * (4 * D + 8) + G * 16 + small["big_nnz"] * 12 + (L + 1) * 8
-              + 8 * 16 * small["first"])
-        per_it = (12 * small["big_nnz"] + 8 * (L + 1) + 8 * 16 * small["first"]
-                  + 8 * L * m * 9 + 16 * small["first"] * m)
-    whole = (12 * S.nnz + 8 * (L + 1) + 8 * L * m * 9) * max(iterations, 1)
-    return {"pass1": p1, "sbuild": sb, "pcg_kernel": per_it * max(iterations, 1),
-            "pcg_kernel_whole_csr": whole}
+        out["sbuild"] = (M * (4 * D + 8) + G * 16 + small["big_nnz"] * 12 + (L + 1) * 8
+                         + 8 * 16 * small["first"])
+        out["pcg_kernel_split"] = (12 * small["big_nnz"] + 8 * (L + 1) + 8 * 16 * small["first"]
+                                   + 8 * L * m * 9 + 16 * small["first"] * m) * max(iterations, 1)
+    return out
 
 
 # DRAM bytes (read + write) of one PCG iteration on the 5M-worker panel, from
@@ -266,13 +268,12 @@ def run_ours(args, rank, world, local_rank):
                 gbs = by[name] / (avg_ms / 1e3) / 1e9
                 roof[name] = {"ms": round(avg_ms, 4), "bytes": int(by[name]),
                               "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
-                if name == "pcg_kernel" and info.get("small_block"):
-                    # the same iterations' bytes on the whole CSR (the layout the
-                    # reference streams), for comparison with that layout's solve
-                    wg = by["pcg_kernel_whole_csr"] / (avg_ms / 1e3) / 1e9
-                    roof[name]["whole_csr_bytes"] = int(by["pcg_kernel_whole_csr"])
-                    roof[name]["whole_csr_equivalent_gbs"] = round(wg, 1)
-                    roof[name]["whole_csr_equivalent_frac"] = round(wg / peak, 4)
+                if name == "pcg_kernel" and "pcg_kernel_split" in by:
+                    # the split form's own (smaller) bytes for the same iterations
+                    sg = by["pcg_kernel_split"] / (avg_ms / 1e3) / 1e9
+                    roof[name]["split_form_bytes"] = int(by["pcg_kernel_split"])
+                    roof[name]["split_form_gbs"] = round(sg, 1)
+                    roof[name]["split_form_frac"] = round(sg / peak, 4)
         # the dominant single kernel is the PCG (one launch per fit); the S
         # build and pass 1 are phases of several kernels, reported alongside
         dom = "pcg_kernel"
