@@ -322,21 +322,53 @@ __device__ void group_lists(const Args &a, int64_t g, int cells, const uint32_t 
 {
     const int D = a.D;
     const int64_t dims = a.ctr[7];
+    const double gn = a.group_n[g];
     for (int d = 0; d < D; d++) {
         if (!((dims >> d) & 1)) continue;           // no narrow level in this dimension
         bool sorted = true;
         for (int i = 1; i < cells; i++) sorted &= cd[(i - 1) * D + d] <= cd[i * D + d];
         if (sorted) {
+            // kRuns runs at a time: their levels' kinds, then their list slots,
+            // each set of loads and atomics issued together
+            constexpr int kRuns = 4;
             for (int i = 0; i < cells;) {
-                const uint32_t c = cd[i * D + d];
-                int j = i + 1;
-                while (j < cells && cd[j * D + d] == c) j++;
-                if ((int64_t)c < a.nlev[d] && listed(a, a.offs[d] + c)) {
-                    double u = nw[i];
-                    for (int q = i + 1; q < j; q++) u += nw[q];
-                    list_append(a, a.offs[d] + c, g, u);
+                int64_t lv[kRuns];
+                double u[kRuns];
+                int nr = 0;
+#pragma unroll
+                for (int t = 0; t < kRuns; t++) {
+                    lv[t] = -1;
+                    u[t] = 0.0;
+                    if (i < cells) {
+                        const uint32_t c = cd[i * D + d];
+                        double su = nw[i];
+                        int j = i + 1;
+                        for (; j < cells && cd[j * D + d] == c; j++) su += nw[j];
+                        if ((int64_t)c < a.nlev[d]) lv[t] = a.offs[d] + c;
+                        u[t] = su;
+                        i = j;
+                        nr = t + 1;
+                    }
                 }
-                i = j;
+                int32_t kk[kRuns];
+#pragma unroll
+                for (int t = 0; t < kRuns; t++) kk[t] = lv[t] >= 0 ? a.kind[lv[t]] : kKindEmpty;
+                int32_t at[kRuns];
+                int64_t l0[kRuns], l1[kRuns];
+#pragma unroll
+                for (int t = 0; t < kRuns; t++) {
+                    const bool on = t < nr && (kk[t] == kKindWarp || kk[t] == kKindBlock);
+                    at[t] = on ? atomicAdd(a.fillpos + lv[t], 1) : -1;
+                    l0[t] = on ? a.lptr[lv[t]] : 0;
+                    l1[t] = on ? a.lptr[lv[t] + 1] : 0;
+                }
+#pragma unroll
+                for (int t = 0; t < kRuns; t++) {
+                    if (at[t] >= 0 && l0[t] + at[t] < l1[t]) {
+                        a.lgrp[l0[t] + at[t]] = (int32_t)g;
+                        a.lwv[l0[t] + at[t]] = u[t] / gn;
+                    }
+                }
             }
             continue;
         }
