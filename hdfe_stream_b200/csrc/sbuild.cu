@@ -729,17 +729,21 @@ __global__ void __launch_bounds__(32) k_block_rows(Args a)
 constexpr size_t kBlockSmem = (size_t)kBlockSlots * 12 + (size_t)kBlockListCap * (8 + 8 + 4 + 4) + 16;
 
 // narrow rows from the temp buffer to their place in the CSR
+// (kCopyLanes lanes a row, so a warp has several rows' dependent loads --
+// the row, its offsets, then its entries -- in flight at once)
+constexpr int kCopyLanes = 8;
+
 __global__ void __launch_bounds__(kThreads) k_copy_narrow(Args a)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t gw = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * kThreads) >> 5;
+    const int64_t t = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    const int sl = (int)(t % kCopyLanes);
+    const int64_t gs = t / kCopyLanes, ns = ((int64_t)gridDim.x * kThreads) / kCopyLanes;
     const int64_t n1 = a.ctr[1], n6 = a.ctr[6], n2 = a.ctr[2];
-    for (int64_t k = gw; k < n1 + n6 + n2; k += nw) {
+    for (int64_t k = gs; k < n1 + n6 + n2; k += ns) {
         const int64_t r = k < n1 ? a.warp_rows[k]
                         : k < n1 + n6 ? a.warp_rows[a.L - 1 - (k - n1)] : a.block_rows[k - n1 - n6];
         const int64_t src = a.toff[r], dst = a.indptr[r], cnt = a.rnnz[r];
-        for (int64_t i = lane; i < cnt; i += 32) {
+        for (int64_t i = sl; i < cnt; i += kCopyLanes) {
             a.indices[dst + i] = a.tcol[src + i];
             a.data[dst + i] = a.tval[src + i];
         }
