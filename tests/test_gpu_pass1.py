@@ -37,6 +37,19 @@ def three_dim_rows(seed=5, regions=7):
                 names=r.names)
 
 
+def years_first_rows(seed=8):
+    """The year before the firm (`| worker + year + firm`): pass 0 orders a
+    group's rows by year, so the firms' codes within a group are not sorted
+    and their level lists take the walk over the group's cells."""
+    from hdfe_stream_b200.simulate import Rows, pass0_layout, simulate_panel
+    r = pass0_layout(simulate_panel(4_000, 400, 8, spell=(2, 8), p_move=0.25, seed=seed))
+    codes = np.ascontiguousarray(r.codes[:, ::-1])
+    order = np.lexsort((r.V[:, 2], r.V[:, 1], r.V[:, 0], codes[:, 1], codes[:, 0], r.gcode))
+    return Rows(gcode=r.gcode[order], codes=np.ascontiguousarray(codes[order]),
+                V=r.V[order], w=None, n_levels=r.n_levels[::-1], n_groups=r.n_groups,
+                names=r.names)
+
+
 def panels():
     from hdfe_stream_b200.simulate import pass0_layout, simulate_panel
     out = [(n, golden_rows(load_golden(n))) for n in GOLDEN_PANELS]
@@ -47,6 +60,11 @@ def panels():
     out.append(("three_dims", three_dim_rows()))
     # more than 16 wide rows: the wide x wide block takes its atomic path
     out.append(("many_wide", three_dim_rows(seed=6, regions=30)))
+    out.append(("years_first", years_first_rows()))
+    # 20 cells a group: 32 groups' cells exceed what the list pass stages in
+    # shared memory, so it reads them in place
+    out.append(("long_groups", pass0_layout(simulate_panel(3_000, 300, 20, spell=(20, 20),
+                                                            p_move=0.15, seed=13))))
     return out
 
 
