@@ -96,7 +96,8 @@ int hdfe_pass1(const uint32_t *gcode, const uint32_t *codes, int32_t D, const do
  * `_nb_row_nnz`, `_nb_row_fill`), plain case.  Three calls on one workspace
  * (hdfe_sbuild_workspace_bytes), because the sizes are data-dependent; the
  * caller reads info (a DEVICE pointer) between them:
- *   analyze  levels' classes and group lists; info->n_wide (wide rows) and
+ *   analyze  levels' classes and group lists (each entry with its group's
+ *            u_r / N_g for the level); info->n_wide (wide rows) and
  *            info->temp_len (entries of the temp buffer)
  *   count    needs the wide workspace (hdfe_sbuild_wide_workspace_bytes with
  *            n_wide) and a temp buffer of temp_len * 12 bytes; writes indptr
