@@ -202,27 +202,30 @@ constexpr int kRedLoads = 8;            // CTAs per lane in reduce_range: grids 
 
 // s_red[q] = sum over CTAs of partial q, for q in [q0, q1): one warp per
 // quantity, the same fixed order in every CTA
+// LOADS partials a lane (grids up to 32 LOADS CTAs), QW quantities a warp at
+// a time: LOADS x QW doubles in flight a lane
+template <int LOADS = kRedLoads, int QW = 4>
 __device__ __forceinline__ void reduce_range(const double *part, int q0, int q1, double *s_red)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int nb = gridDim.x;
-    for (int qb = q0 + warp; qb < q1; qb += 4 * nw) {
-        // four quantities per warp at a time, every load issued before the sums
-        double v[4][kRedLoads];
+    for (int qb = q0 + warp; qb < q1; qb += QW * nw) {
+        // QW quantities per warp at a time, every load issued before the sums
+        double v[QW][LOADS];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
+        for (int i = 0; i < QW; i++) {
             const int q = qb + i * nw;
 #pragma unroll
-            for (int u = 0; u < kRedLoads; u++) {
+            for (int u = 0; u < LOADS; u++) {
                 const int b = lane + 32 * u;
                 v[i][u] = (q < q1 && b < nb) ? __ldcg(part + (int64_t)q * nb + b) : 0.0;
             }
         }
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
+        for (int i = 0; i < QW; i++) {
             double t = 0.0;
 #pragma unroll
-            for (int u = 0; u < kRedLoads; u++) t += v[i][u];
+            for (int u = 0; u < LOADS; u++) t += v[i][u];
             t = warp_sum(t);
             const int q = qb + i * nw;
             if (lane == 0 && q < q1) s_red[q] = t;
@@ -1017,10 +1020,23 @@ constexpr int kShortLpr = HDFE_PCG_SHORT_LPR;
 __host__ __device__ constexpr int lane_threads(int K) { return K >= 32 ? 256 : 512; }
 __host__ __device__ constexpr int lane_ru(int K) { return K >= 32 ? 4 : 2; }  // vector elements per trip
 constexpr int kLaneStages = 3;          // windows of 32 nonzeros in flight per warp
+// The FP64 block of 32 columns keeps one window in flight: its CTAs (8 warps,
+// at most 128 registers a thread) then fit two to an SM, which hides more of
+// the gathers' latency than two more windows do (the 32-probe block solve of
+// the KSS call: 103 -> 92 ms on the 1M-worker panel).
+__host__ __device__ constexpr int lane_stages(int K) { return K >= 32 ? 1 : kLaneStages; }
+__host__ __device__ constexpr int lane_ctas(int K) { return K >= 32 ? 2 : 1; }
+// its reduce_range: partials a lane (grids up to 32 x this CTAs), quantities
+// a warp at a time
+__host__ __device__ constexpr int lane_red_loads(int K) { return K >= 32 ? 16 : kRedLoads; }
+__host__ __device__ constexpr int lane_red_qw(int K) { return K >= 32 ? 2 : 4; }
 constexpr uint8_t kRowCut = 1, kRowEmpty = 2;   // per-row flags
 // dynamic shared memory: per warp, kLaneStages x 32 gathered rows of K values
 // and their 32 matrix values
-inline int lane_smem_bytes(int K) { return (lane_threads(K) / 32) * kLaneStages * 32 * (K + 1) * 8; }
+inline int lane_smem_bytes(int K, int ns = kLaneStages)
+{
+    return (lane_threads(K) / 32) * ns * 32 * (K + 1) * 8;
+}
 
 inline bool use_lanes(int k) { return k >= HDFE_PCG_LANE_FROM || k > 8; }
 inline int lane_width(int k) { return k <= 8 ? 8 : (k <= 16 ? 16 : 32); }
@@ -1106,11 +1122,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // plus the window's matrix values, and keeps kLaneStages windows in flight,
 // so the bytes in flight per SM do not depend on registers.  Row walk and
 // flushes as described above; V[r] for p'Ap is loaded as row r begins.
-template <int K, typename T>
+template <int K, typename T, int NS = kLaneStages>
 __device__ void lane_spmm(const Params &a, const T *__restrict__ mvals, const T *__restrict__ V,
                           T *__restrict__ out, T *carry, double &dot, bool want_dot, T *stage)
 {
-    constexpr int H = 32 / K, NS = kLaneStages;
+    constexpr int H = 32 / K;
     const int lane = threadIdx.x & 31, col = lane % K, sub = lane / K;
     const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int64_t lo = a.wlo[gw];
@@ -1255,7 +1271,7 @@ __device__ __forceinline__ void column_partials(double (&v)[N], double *scratch,
 }
 
 template <int K>
-__global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, LaneArgs x)
+__global__ void __launch_bounds__(lane_threads(K), lane_ctas(K)) lane_kernel(Params a, LaneArgs x)
 {
     constexpr int RU = lane_ru(K);
     extern __shared__ double s_stage[];
@@ -1272,7 +1288,7 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
     const int kc = x.k;
     double *Xw = x.Xw;
     const bool zero_c = col >= kc || (a.zero != nullptr && a.zero[col] != 0);
-    double *stage = s_stage + (threadIdx.x >> 5) * kLaneStages * 32 * (K + 1);
+    double *stage = s_stage + (threadIdx.x >> 5) * lane_stages(K) * 32 * (K + 1);
 
     // ---- set-up: each warp's first row and the cut flags
     {
@@ -1292,7 +1308,7 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
         for (int64_t t = gtid; t < LK; t += gstride)
             Xw[t] = zero_c ? 0.0 : a.X0[(t / K) * kc + col];
         if (!gb.sync()) return;
-        lane_spmm<K, double>(a, a.data, Xw, a.AP, a.carry, dot, false, stage);
+        lane_spmm<K, double, lane_stages(K)>(a, a.data, Xw, a.AP, a.carry, dot, false, stage);
         if (!gb.sync()) return;
     }
     double rel_c = 0.0, rz_c, bnorm_c;
@@ -1325,7 +1341,7 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
         }
         column_partials<K, 3>(v, s_scratch, a.part, 0, nb);
         if (!gb.sync()) return;
-        reduce_range(a.part, 0, 3 * K, s_red);
+        reduce_range<lane_red_loads(K), lane_red_qw(K)>(a.part, 0, 3 * K, s_red);
         const double bn = sqrt(s_red[col]);
         bnorm_c = bn == 0.0 ? 1.0 : bn;
         rz_c = s_red[2 * K + col];
@@ -1348,13 +1364,13 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
         for (it = 1; it <= a.maxiter; it++) {
             // ---- A: AP = S P, p'Ap
             dot = 0.0;
-            lane_spmm<K, double>(a, a.data, a.P, a.AP, a.carry, dot, true, stage);
+            lane_spmm<K, double, lane_stages(K)>(a, a.data, a.P, a.AP, a.carry, dot, true, stage);
             {
                 double v[1] = {dot};
                 column_partials<K, 1>(v, s_scratch, a.part, 0, nb);
             }
             if (!gb.sync()) return;
-            reduce_range(a.part, 0, K, s_red);
+            reduce_range<lane_red_loads(K), lane_red_qw(K)>(a.part, 0, K, s_red);
             const double pap = s_red[col];
             const double alpha = (active_c && pap > 0.0) ? rz_c / pap : 0.0;
             // ---- B: X += alpha P, R -= alpha AP, sums of R^2, R^2 dinv
@@ -1404,7 +1420,7 @@ __global__ void __launch_bounds__(lane_threads(K), 1) lane_kernel(Params a, Lane
             }
             column_partials<K, 2>(v, s_scratch, a.part, 1, nb);
             if (!gb.sync()) return;
-            reduce_range(a.part, K, 3 * K, s_red);
+            reduce_range<lane_red_loads(K), lane_red_qw(K)>(a.part, K, 3 * K, s_red);
             // ---- C: convergence, beta, P = dinv R + beta P
             rel_c = sqrt(s_red[K + col]) / bnorm_c;
             active_c = rel_c > a.tol;
@@ -1464,14 +1480,17 @@ int lane_grid()
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
     if (cudaFuncSetAttribute(lane_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             lane_smem_bytes(K)) != cudaSuccess)
+                             lane_smem_bytes(K, lane_stages(K))) != cudaSuccess)
         return -1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lane_kernel<K>, lane_threads(K),
-                                                      lane_smem_bytes(K)) != cudaSuccess)
+                                                      lane_smem_bytes(K, lane_stages(K))) !=
+        cudaSuccess)
         return -1;
-    // one CTA per SM, at most as many as reduce_range sums (32 lanes x
-    // kRedLoads partials each): a larger part runs fewer CTAs than SMs
-    return per_sm < 1 ? -1 : (sms < 32 * kRedLoads ? sms : 32 * kRedLoads);
+    // lane_ctas(K) CTAs per SM (fewer if they do not fit), at most as many as
+    // reduce_range sums (32 lanes x lane_red_loads(K) partials each)
+    const int want = sms * (per_sm < lane_ctas(K) ? per_sm : lane_ctas(K));
+    const int most = 32 * lane_red_loads(K);
+    return per_sm < 1 ? -1 : (want < most ? want : most);
 }
 
 int lane_grid_for(int kw)
@@ -1490,7 +1509,8 @@ cudaError_t launch_lanes(Params p, LaneArgs x, int blocks, cudaStream_t s)
 {
     void *args[] = {&p, &x};
     return cudaLaunchCooperativeKernel((const void *)lane_kernel<K>, dim3(blocks),
-                                       dim3(lane_threads(K)), args, lane_smem_bytes(K), s);
+                                       dim3(lane_threads(K)), args,
+                                       lane_smem_bytes(K, lane_stages(K)), s);
 }
 
 int solve_lanes(const int64_t *indptr, const int32_t *indices, const double *data, int64_t L,
